@@ -1,0 +1,423 @@
+"""Benchmark of the TurboNeRF training hot path on B200: samples/s of the full train step.
+
+Workload (one step): 2^14 synthetic rays (origins on a radius-4 sphere, directions toward
+the centre + N(0, 0.05)) through a 5-cascade 128^3 occupancy grid built from an 8-blob
+Gaussian field (base size 1: extents 1..16) -> march count + batch cut at 2^18 samples ->
+march emit -> field (network stand-in) -> reconstruction + distortion (lambda 1e-3) loss
+forward/backward with the gradient merge -> occupancy EMA (decay 0.95, threshold 0.01,
+2^16 random cells re-sampled) -> Adam (beta1 0.9, beta2 0.99, eps 1e-15, lr 1e-2) over
+16 x 2^19 x 2 hash-grid + 7168 MLP parameters with fixed sparse synthetic gradients.
+
+Prints ONE JSON line. `value` = samples/s of the fused, CUDA-graph-captured step with
+inputs resident in HBM; `e2e` = the same through Trainer.train_step_rays() with host rays
+copied in and the metrics read back every step; `plain` = the one-kernel-per-stage path.
+`--impl reference` times the CPU restatement of the reference (the oracle) instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "train-step samples/s fused vs plain on 1 B200 (grad err ≤1e-4); % HBM roofline"
+WORKLOAD = "full single-scene train step, CUDA graph: 5x128^3 cascades, 2^18 samples/step from 2^14 rays"
+BATCH = 1 << 18
+RAYS = 1 << 14
+OCC_CELLS = 1 << 16
+N_GRID = 16 * (1 << 19) * 2
+N_MLP = 7168
+LAMBDA = 1e-3
+THRESHOLD = 0.01
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _scene(seed):
+    from turbonerf_b200 import scenes
+    return scenes.march_scene_cascaded(seed=seed, n_rays=64, n_levels=5)
+
+
+def _trainer(scene, path, seed):
+    from turbonerf_b200.trainer import SyntheticNeRF, Trainer
+    tr = Trainer(SyntheticNeRF.from_scene(scene), path=path, use_cuda_graph=(path == "fused"), n_rays_per_step=RAYS,
+                 occupancy_cells_per_step=OCC_CELLS, distortion_lambda=LAMBDA, occupancy_threshold=THRESHOLD,
+                 n_grid_params=N_GRID, n_mlp_params=N_MLP, beta2=0.99, seed=seed)
+    tr.use_distortion_loss = True
+    tr.setup_data(batch_size=BATCH, synthetic_grad_std=1e-3)
+    return tr
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def stage_bytes(n_rays_gen, n_rays, n_samples, n_touched, levels=5, volume=128 ** 3):
+    """Algorithmic HBM bytes of each fused stage for one step (what the stage must move)."""
+    P = N_GRID + N_MLP
+    return {
+        "rays": n_rays_gen * (12 + 12 + 16 + 12 + 9),                    # write ori, dir, target, bg, t, t_max, alive
+        "march_count": n_rays_gen * (24 + 8 + 1 + 4),                    # read o, d, t, t_max, alive; write count
+        "march_emit": n_rays_gen * 37 + n_samples * 40,                  # ray reads + 10 floats per sample
+        "network_forward": n_samples * (12 + 16),                        # read pos, write sigma + rgb
+        "losses": n_samples * (4 + 12 + 4 + 4 + 4 + 4 + 8 + 12) + n_rays * 36,
+        "network_backward": 0,
+        "occupancy": levels * volume * 8 + volume + OCC_CELLS * 48,      # sweep RMW + bits + scatter inputs
+        "adam": 4 * P + 32 * (n_touched + N_MLP),                        # gradient read + RMW of touched params
+    }
+
+
+STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "network_backward", "occupancy", "adam"]
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = _env_rank()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    seed = 0x7B0 + 7919 * rank
+
+    scene = _scene(0x7B0)
+    tr = _trainer(scene, "fused", seed)
+    stream = torch.cuda.ExternalStream(tr.stream_handle())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        tr.train_step_async()
+    tr.sync_metrics()
+    s0 = tr.stat(3)
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            tr.train_step_async()
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    last = tr.sync_metrics()
+    samples = tr.stat(3) - s0
+    rays_used = last.n_rays
+    kernels_per_step = tr.stat(0)
+    t = torch.tensor([ms], device=dev)
+    tot = torch.tensor([float(samples)], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    value = float(tot.item()) / (ms_max / 1e3)
+
+    # per-stage timing (eager step with events between stages), averaged
+    prof = []
+    for _ in range(5):
+        prof.append(tr.profile_step())
+    stage_ms = [float(np.median([p[i] for p in prof])) for i in range(len(STAGES))]
+    m = tr.sync_metrics()
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        sb = stage_bytes(RAYS, m.n_rays, m.n_samples, tr.n_touched_grads)
+        stages = {}
+        for i, name in enumerate(STAGES):
+            b = sb[name]
+            gbs = b / (stage_ms[i] / 1e3) / 1e9 if stage_ms[i] > 0 else 0.0
+            stages[name] = {"ms": round(stage_ms[i], 4), "alg_bytes": int(b), "achieved_gbs": round(gbs, 1),
+                            "frac": round(gbs / peak, 4)}
+        dom = max(STAGES, key=lambda k: stages[k]["ms"])
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": stages[dom]["achieved_gbs"], "peak": peak,
+                    "unit": "GB/s", "frac": round(stages[dom]["achieved_gbs"] / peak, 4), "traffic": None,
+                    "peak_source": peak_kind}
+        result = dict(value=value, ms=ms_max, samples=samples, rays=rays_used, kernels=kernels_per_step,
+                      clocks=clk.summary(), stages=stages, roofline=roofline, n_touched=tr.n_touched_grads,
+                      last=dict(n_rays=m.n_rays, n_samples=m.n_samples, loss=m.loss))
+
+    # e2e: public API with host rays (pinned) copied in and metrics read back every step
+    from turbonerf_b200 import scenes
+    rng = np.random.default_rng(seed + 1)
+    n_batches = 4
+    host = []
+    for _ in range(n_batches):
+        r = scenes.sphere_rays(rng, RAYS)
+        tgt = np.concatenate([rng.uniform(0, 1, 3 * RAYS), np.ones(RAYS)]).astype(np.float32)
+        bg = rng.uniform(0, 1, 3 * RAYS).astype(np.float32)
+        host.append([torch.from_numpy(a).pin_memory() for a in (r.ori, r.dir, tgt, bg)])
+    for i in range(max(args.warmup, 3)):
+        tr.train_step_rays(*host[i % n_batches])
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0 = tr.stat(3)
+    e0.record(stream)
+    wall0 = time.perf_counter()
+    for i in range(args.steps):
+        tr.train_step_rays(*host[i % n_batches])
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - wall0
+    e_ms = e0.elapsed_time(e1)
+    e_samples = tr.stat(3) - s0
+    te = torch.tensor([max(e_ms, wall * 1e3)], device=dev)
+    ts = torch.tensor([float(e_samples)], device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+    e2e_value = float(ts.item()) / (float(te.item()) / 1e3)
+    tr.teardown()
+
+    # plain path (reference launch structure) on the same workload
+    plain = None
+    if rank == 0 and not args.no_plain:
+        trp = _trainer(scene, "plain", seed)
+        for _ in range(max(args.warmup, 3)):
+            trp.train_step()
+        torch.cuda.synchronize()
+        ps = torch.cuda.ExternalStream(trp.stream_handle())
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ss0 = trp.stat(3)
+        k_plain = max(5, args.steps // 4)
+        p0.record(ps)
+        for _ in range(k_plain):
+            trp.train_step()
+        p1.record(ps)
+        p1.synchronize()
+        p_ms = p0.elapsed_time(p1)
+        p_samples = trp.stat(3) - ss0
+        plain = {"value": p_samples / (p_ms / 1e3), "ms_per_step": p_ms / k_plain, "steps": k_plain}
+        trp.teardown()
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    cpu = None if args.no_cpu else cpu_baseline(seconds=args.cpu_seconds)
+    bi = RAYS * 4 * (3 + 3 + 4 + 3)
+    line = {
+        "metric": METRIC, "value": round(result["value"], 1), "unit": "samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(result["ms"] / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "batch_size_samples": BATCH, "rays_per_step": RAYS, "cascades": 5,
+                   "grid": "128^3", "occupancy_cells_per_step": OCC_CELLS, "hash_params": N_GRID, "mlp_params": N_MLP,
+                   "distortion_lambda": LAMBDA, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (Adam state 268 MB + grid 42 MB touched per step)",
+                   "samples_last_step": result["last"]["n_samples"], "rays_last_step": result["last"]["n_rays"],
+                   "touched_hash_grads": result["n_touched"]},
+        "e2e": {"value": round(e2e_value, 1), "unit": "samples/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": 68},
+        "gpu_launches": int(result["kernels"]) * args.steps,
+        "roofline": result["roofline"],
+        "stages": result["stages"],
+        "clocks": result["clocks"],
+        "plain": plain,
+        "speedup_vs_plain": round(result["value"] / plain["value"], 2) if plain else None,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# CPU: the oracle's restatement of the reference, one train step of the same workload
+# ---------------------------------------------------------------------------------------
+class CpuStep:
+    def __init__(self, seed=0x7B0):
+        import oracle
+        from turbonerf_b200 import scenes
+        self.o = oracle
+        self.sc = _scene(0x7B0)
+        self.rng = np.random.default_rng(seed)
+        P = N_GRID + N_MLP
+        g = np.zeros(P, np.float32)
+        # same sparsity class as the GPU run: a fixed random half of the hash entries touched
+        touched = self.rng.random(N_GRID) < 0.5
+        g[:N_GRID][touched] = self.rng.normal(0, 1e-3, int(touched.sum())).astype(np.float32)
+        g[N_GRID:] = self.rng.normal(0, 1e-3, N_MLP).astype(np.float32)
+        self.grad = g
+        self.adam = dict(w=self.rng.uniform(-1e-4, 1e-4, P), m=np.zeros(P), v=np.zeros(P),
+                         steps=np.zeros(P, np.uint32))
+        self.density = self.sc.grid.density.copy()
+        self.bits = self.sc.grid.bitfield.copy()
+        self.k = 0
+
+    def step(self):
+        from turbonerf_b200 import scenes
+        o, sc = self.o, self.sc
+        rays = scenes.rays_init_bbox(scenes.sphere_rays(self.rng, RAYS), sc.bbox)
+        grid = dict(n_levels=5, res=128, base=1.0, bitfield=self.bits)
+        march = dict(bbox=sc.bbox, cone=sc.cone_angle, dt_min=sc.dt_min, dt_max=sc.dt_max, max_steps=0)
+        ns, alive, _ = o.march_count(rays.as_dict(), grid, march)
+        st, off, nr, nsamp = o.scan_cut(ns, BATCH)
+        em = o.march_emit(rays.as_dict(), grid, march, off, ns, alive, nr, BATCH, 1.0 / sc.aabb_size)
+        sig, rgb = o.blob_field(em["pos"], BATCH, BATCH, sc.aabb_size, sc.field.blobs, sc.field.waves)
+        tgt = np.concatenate([self.rng.uniform(0, 1, 3 * nr), np.ones(nr)]).astype(np.float32)
+        bg = self.rng.uniform(0, 1, 3 * nr).astype(np.float32)
+        counts = ns[:nr]
+        rec = o.recon_fwd_bwd(counts, off[:nr], sig.astype(np.float32), rgb.astype(np.float32), em["dt"], tgt, bg,
+                              nr, BATCH)
+        _, ddist = o.distortion_fwd_bwd(counts, off[:nr], sig.astype(np.float32), em["m_norm"], em["dt_norm"], LAMBDA,
+                                        BATCH)
+        o.grad_epilogue(nsamp, 1.0, rec["dL_ddensity"][:nsamp], ddist[:nsamp], em["t"][:nsamp], np.zeros(nsamp))
+        lv = self.rng.integers(0, 5, OCC_CELLS).astype(np.int32)
+        cells = self.rng.integers(0, 128 ** 3, OCC_CELLS).astype(np.uint32)
+        r3 = self.rng.random(3 * OCC_CELLS).astype(np.float32)
+        pos = o.occupancy_sample_points(lv, cells, r3, OCC_CELLS, 128, 1.0, 1.0 / sc.aabb_size, OCC_CELLS)
+        vals, _ = o.blob_field(pos, OCC_CELLS, OCC_CELLS, sc.aabb_size, sc.field.blobs, sc.field.waves, want_rgb=False)
+        self.density, self.bits, _ = o.occupancy_update(self.density, self.bits, 5, 128, lv, cells,
+                                                        vals.astype(np.float32), self.rng.random(OCC_CELLS).astype(
+                                                            np.float32), sample_all=self.k < 256,
+                                                        threshold=THRESHOLD)
+        lr = 1e-2 / (1.0 + 3.3e-5 * self.k)
+        o.adam_step(self.adam, self.grad, N_GRID, N_MLP, lr=lr, beta2=0.99)
+        self.k += 1
+        return nsamp
+
+
+def cpu_baseline(seconds=12.0):
+    import oracle
+    oracle.build()
+    cs = CpuStep()
+    cs.step()  # warm-up (first touch of the buffers)
+    t0 = time.perf_counter()
+    samples, steps = 0, 0
+    while True:
+        samples += cs.step()
+        steps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": round(samples / el, 1), "unit": "samples/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{steps} full train steps of the same workload on the CPU oracle (OpenMP), {el:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    cs = CpuStep()
+    for _ in range(max(args.warmup, 1)):
+        cs.step()
+    t0 = time.perf_counter()
+    samples = 0
+    k = max(1, args.steps)
+    for _ in range(k):
+        samples += cs.step()
+    el = time.perf_counter() - t0
+    v = samples / el
+    cores = oracle.num_threads()
+    line = {
+        "metric": METRIC, "value": round(v, 1), "unit": "samples/s", "n_gpus": world, "steps": k,
+        "warmup": args.warmup, "ms_per_step": round(el / k * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "batch_size_samples": BATCH, "rays_per_step": RAYS, "cascades": 5,
+                   "parallelism": "cpu"},
+        "cpu_baseline": {"value": round(v, 1), "unit": "samples/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} full train steps on the CPU oracle (OpenMP, {cores} threads)"},
+        "e2e": {"value": round(v, 1), "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,413 @@
+/*
+ * turbo_hot.h — C ABI of the B200 (sm_100a) TurboNeRF training hot path.
+ *
+ * Conventions
+ *  - Every entry point returns int: TN_OK (0) or a negative TN_E_* status. No C++
+ *    exception crosses this boundary; tn_last_error() gives a message for the calling
+ *    thread.
+ *  - All buffers are device pointers owned by the caller, in the reference's
+ *    structure-of-arrays layout: component c of item i lives at buf[c * stride + i]
+ *    (reference: src/workspaces/training-workspace.cuh:87-112). Ray buffers use
+ *    `ray_stride`, per-sample buffers `sample_stride`.
+ *  - Every compute call takes a cudaStream_t (passed as tn_stream_t, the same type) and
+ *    only enqueues work: no host synchronisation, except the functions of the "plain"
+ *    family and the *_sync helpers, which reproduce the reference's blocking structure.
+ *  - The library owns only the opaque tn_ctx (scratch buffers, device error flags,
+ *    tuning table). One context per stream/thread.
+ */
+#ifndef TURBO_HOT_H
+#define TURBO_HOT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* tn_stream_t; /* identical to cudaStream_t */
+
+#define TN_OK 0
+#define TN_E_INVALID (-1)     /* an argument is out of range */
+#define TN_E_NULL (-2)        /* a required pointer is NULL */
+#define TN_E_CAPACITY (-3)    /* a size exceeds a capacity or limit */
+#define TN_E_CUDA (-4)        /* a CUDA runtime call failed */
+#define TN_E_NO_RAYS (-5)     /* the batch cut found no ray (reference: trainer.cu:162-164) */
+#define TN_E_NO_SAMPLES (-6)  /* the batch cut found no sample (reference: trainer.cu:181-183) */
+#define TN_E_LEVELS (-7)      /* cascade count outside 1..8 */
+#define TN_E_DEVICE (-8)      /* a kernel raised a device-side error flag (see tn_ctx_check) */
+#define TN_E_STATE (-9)       /* call not valid in the current state (e.g. during capture) */
+
+/* Device-side error bits reported by tn_ctx_check. */
+#define TN_FLAG_GUARD 1u      /* a march loop hit max_iterations */
+#define TN_FLAG_CAPACITY 2u   /* an offset + count exceeded the sample capacity */
+#define TN_FLAG_NO_RAYS 4u
+#define TN_FLAG_NO_SAMPLES 8u
+#define TN_FLAG_SPIN 16u      /* a bounded spin-wait gave up */
+
+/* Compositor input activation. */
+#define TN_ACT_SIGMA 0        /* input is sigma; d sigma / d input = 1 */
+#define TN_ACT_DENSITY 1      /* input is the network density: sigma = exp(min(d,12)-1),
+                                 reference density_to_sigma, common-network-kernels.cuh:7-10 */
+
+/* Axis-aligned box; same POD layout as the reference's BoundingBox
+ * (src/models/bounding-box.cuh:8-16). contains() is inclusive on both faces. */
+typedef struct tn_bbox {
+    float min_x, min_y, min_z;
+    float max_x, max_y, max_z;
+} tn_bbox;
+
+/* Cascaded occupancy grid (reference OccupancyGrid, src/core/occupancy-grid.cuh:22-287).
+ * Level k covers the cube [-base*2^k/2, base*2^k/2]^3 with resolution^3 cells; the
+ * bitfield holds one byte per Morton-ordered cell, bit k = level k; density holds
+ * [n_levels][resolution^3] floats. base_size = 1 reproduces the reference exactly
+ * (level extent 2^k, occupancy-grid.cuh:139-141). */
+typedef struct tn_grid_desc {
+    int32_t n_levels;    /* 1..8 */
+    int32_t resolution;  /* power of two, 2..1024 (the reference uses 128) */
+    float base_size;     /* extent of level 0 in world units */
+    int32_t reserved;
+} tn_grid_desc;
+
+/* Step control of the march (reference get_dt, src/utils/raymarching-utils.cuh:7-14,
+ * called with dt_max = aabb_size * dt_min at src/core/trainer.cu:102-104). */
+typedef struct tn_march_desc {
+    float cone_angle;        /* reference NeRFConstants::cone_angle = 1/256 */
+    float dt_min;            /* reference min_step_size = sqrt(3)/1024 */
+    float dt_max;
+    uint32_t max_steps;      /* 0 = unlimited (reference); otherwise samples per ray are capped */
+    uint32_t max_iterations; /* loop guard per ray; 0 selects 1<<22. Exceeding it raises TN_FLAG_GUARD */
+} tn_march_desc;
+
+/* Per-ray sample ranges of a packed batch. n_rays bounds the launch; when n_rays_dev is
+ * non-NULL the kernels read the live ray count from that device word (<= n_rays), so a
+ * batch cut computed on the device needs no host round trip. */
+typedef struct tn_ray_batch {
+    uint32_t n_rays;
+    uint32_t ray_stride;
+    uint32_t sample_stride;
+    uint32_t reserved;
+    const uint32_t* counts;      /* [ray] samples per ray */
+    const uint32_t* offsets;     /* [ray] first sample of each ray (exclusive scan of counts) */
+    const uint32_t* n_rays_dev;  /* optional device count */
+} tn_ray_batch;
+
+typedef struct tn_ctx tn_ctx;
+
+/* ---- library / context ------------------------------------------------------------ */
+int tn_version(void);
+const char* tn_last_error(void);
+/* Creates a context on the current CUDA device. */
+int tn_ctx_create(tn_ctx** out);
+int tn_ctx_destroy(tn_ctx* ctx);
+/* Grows the context scratch for batches of up to max_rays rays / max_samples samples
+ * (call before stream capture; kernels never allocate). */
+int tn_ctx_reserve(tn_ctx* ctx, uint32_t max_rays, uint32_t max_samples);
+/* Synchronises `stream`, returns the device error bits raised since the last check in
+ * *flags_out and clears them. */
+int tn_ctx_check(tn_ctx* ctx, tn_stream_t stream, uint32_t* flags_out);
+/* Device pointer of the context's error word (for graph users that read it themselves). */
+int tn_ctx_flags_ptr(tn_ctx* ctx, uint32_t** flags_dev);
+
+/* ---- ray set-up (a 'next' stage of the reference path) ---------------------------- */
+/* Bounding-box clip of initialize_training_rays_and_pixels_kernel
+ * (reference src/utils/training-batch-kernels.cuh:122-150): t = max(0, tmin + 1e-5),
+ * t_max = min(t_far, tmax), alive = hit && t <= t_max. */
+int tn_rays_init_bbox(tn_stream_t stream, uint32_t n_rays, uint32_t ray_stride, const tn_bbox* bbox,
+                      float t_far, const float* ori, const float* dir, float* t, float* t_max,
+                      uint8_t* alive);
+
+/* ---- fused march + compaction --------------------------------------------------- */
+/* Count pass (reference march_and_count_steps_per_ray_kernel,
+ * src/utils/training-batch-kernels.cuh:212-298) fused with the batch cut of
+ * src/core/trainer.cu:133-183: writes n_steps[ray], clears alive for rays with no step,
+ * and writes batch_info[0] = n_rays_cut (rays [0, n_rays_cut) fill the batch),
+ * batch_info[1] = n_samples = offsets[n_rays_cut], where offsets is the exclusive scan of
+ * n_steps, and batch_info[2] = total samples of all n_rays rays. The offsets themselves are
+ * written by tn_march_emit. batch_size is the sample capacity (reference batch_size);
+ * batch_size = UINT32_MAX disables the cut (render use: every ray is kept and
+ * batch_info = {n_rays, total, total}). */
+int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, const uint8_t* bitfield,
+                   const tn_bbox* bbox, const tn_march_desc* march, uint32_t n_rays, uint32_t ray_stride,
+                   const uint32_t* n_rays_dev, const float* ori, const float* dir, const float* ray_t,
+                   const float* ray_t_max, uint8_t* alive, uint32_t* n_steps, uint32_t batch_size,
+                   uint32_t* batch_info);
+
+/* Emit pass (reference march_and_generate_network_positions_kernel,
+ * src/utils/training-batch-kernels.cuh:339-481): for rays [0, batch_info[0]) writes
+ * offsets[ray] and, per sample at offsets[ray] + j: t, pos[3] (normalised to [0,1]),
+ * dir[3] (0.5*d+0.5), dt (= dt/aabb_size, the compositor's dt), m_norm, dt_norm and
+ * img_id (optional, from ray_img_id). Rays at or beyond the cut get offsets = total
+ * so that downstream kernels see empty ranges. */
+int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, const uint8_t* bitfield,
+                  const tn_bbox* bbox, const tn_march_desc* march, float inv_aabb_size, uint32_t n_rays,
+                  uint32_t ray_stride, uint32_t sample_stride, const uint32_t* batch_info,
+                  const uint32_t* ray_img_id, const float* ori, const float* dir, const float* ray_t,
+                  const uint8_t* alive, const uint32_t* n_steps, uint32_t* offsets,
+                  uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir, float* out_dt,
+                  float* out_m_norm, float* out_dt_norm);
+
+/* Exclusive scan + batch cut of arbitrary counts (reference trainer.cu:146-183 with
+ * find_last_lt_presorted, src/utils/parallel-utils.cuh:31-58). batch_info as above. */
+int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,
+                    uint32_t batch_size, uint32_t* batch_info);
+
+/* Ascending list of the indices i < n with values[i] != 0 (reference
+ * generate_nonzero_compaction_indices, src/utils/stream-compaction.cuh:120-139);
+ * *count_dev receives the list length. */
+int tn_compact_nonzero(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* values, int32_t* out,
+                       uint32_t* count_dev);
+
+/* ---- compositor (a warp per ray, warp-shuffle scans) ----------------------------- */
+/* Forward (reference density_to_ray_rgba_forward, training-kernels-fused.cuh:227-264):
+ * rgba[4][ray_stride]; optional per-ray saved state for the backward: depth[ray]
+ * (optical depth up to the transmittance cut) and n_used[ray] (samples composited). */
+int tn_composite_fwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                     float min_transmittance, const float* density, const float* rgb, const float* dt,
+                     float* rgba, float* depth, uint32_t* n_used);
+
+/* Vector-Jacobian product of tn_composite_fwd: given grad_rgba[4][ray_stride], writes
+ * dL/d density [sample] and dL/d rgb [3][sample_stride] (zero past each ray's cut).
+ * Transmittance is recomputed by a reverse scan from the saved per-ray depth and n_used;
+ * no per-sample state from the forward is read. */
+int tn_composite_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                     const float* density, const float* rgb, const float* dt, const float* depth,
+                     const uint32_t* n_used, const float* grad_rgba, float* dL_ddensity, float* dL_drgb);
+
+/* Reconstruction loss forward + backward in one pass (reference
+ * fused_reconstruction_forward_backward_kernel, training-kernels-fused.cuh:381-498):
+ * composite, random-background blend of target and prediction, smooth-L1 loss,
+ * dL/dR_c = inv_nrays * huber'(d_c); writes dL/d density and grad_scale * dL/d rgb
+ * (zero past the cut). Optional outputs: ray_rgba[4][ray_stride], loss[4][ray_stride],
+ * loss_sum[1] (device: inv_nrays * sum over rays of the 4 channel losses). */
+int tn_recon_loss_fwd_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                          float min_transmittance, float inv_nrays, float grad_scale, const float* density,
+                          const float* rgb, const float* dt, const float* target_rgba, const float* bg_rgb,
+                          float* ray_rgba, float* loss, float* loss_sum, float* dL_ddensity, float* dL_drgb);
+
+/* mip-NeRF 360 distortion loss forward (+ backward when dL_ddensity != NULL)
+ * (reference mipNeRF360_distortion_loss_forward/backward_kernel,
+ * training-kernels-fused.cuh:13-224). ray_loss[ray] = lambda/N * (dt w^2 / 3 + 2 * cross
+ * terms); loss_sum[1] = mean over rays; grad_ray (optional) scales each ray's gradient
+ * (the reference uses 1). */
+int tn_distortion_fwd_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                          float lambda, const float* density, const float* m_norm, const float* dt_norm,
+                          const float* grad_ray, float* ray_loss, float* loss_sum, float* dL_ddensity);
+
+/* Gradient merge (reference nerf-network.cu:734-758): grad_out[i] += loss_scale *
+ * (dL_rec[i] + dL_dist[i]) then *= t[i]^2 where t[i] < 1 (apply_gradient_distance_scaling,
+ * training-kernels-fused.cuh:500-515). dL_dist and t may be NULL. n_samples_dev, when
+ * non-NULL, holds the live sample count (<= n_samples). */
+int tn_grad_epilogue(tn_stream_t stream, uint32_t n_samples, const uint32_t* n_samples_dev, float loss_scale,
+                     const float* dL_rec, const float* dL_dist, const float* t, float* grad_out);
+
+/* Everything between the network forward and backward in one kernel: reconstruction
+ * loss fwd/bwd, distortion loss fwd/bwd (lambda > 0) and the gradient merge into
+ * grad_density (accumulated, then distance-scaled when t != NULL). dL_drgb receives
+ * grad_scale * dL/d rgb. loss_sums[0] = reconstruction loss, loss_sums[1] = distortion. */
+int tn_train_losses(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                    float min_transmittance, float inv_nrays, const uint32_t* inv_nrays_from_dev,
+                    float grad_scale, float lambda, const float* density, const float* rgb,
+                    const float* dt, const float* m_norm, const float* dt_norm, const float* t,
+                    const float* target_rgba, const float* bg_rgb, float* ray_rgba, float* grad_density,
+                    float* dL_drgb, float* loss_sums);
+
+/* ---- occupancy grid ------------------------------------------------------------- */
+/* Network sample points for (level, cell) pairs (reference
+ * generate_grid_cell_network_sample_points_kernel, occupancy-grid-kernels.cu:38-76):
+ * out_pos[3][pos_stride] = (cell corner + rand * voxel) * inv_aabb + 0.5. */
+int tn_occupancy_sample_points(tn_stream_t stream, const tn_grid_desc* grid, uint32_t n, const int32_t* levels,
+                               const uint32_t* cells, const float* rand3, uint32_t rand_stride,
+                               float inv_aabb_size, float* out_pos, uint32_t pos_stride);
+
+/* Decay, max-update of the listed (level, cell) pairs and bitfield rebuild in two
+ * kernels (reference occupancy-grid-kernels.cu:16-141, trainer.cu:221-311):
+ * density *= decay everywhere; for each update u whose selection passes
+ * (sample_all, or rand_select[u] < 0.25, or rand_select[u] <= 0.5 and the cell is
+ * occupied at its level) density = max(density, act(values[u])); bits = density >
+ * threshold; *n_occupied_dev = popcount of the bitfield (optional). */
+int tn_occupancy_update(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, float* density,
+                        uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
+                        const float* values, const float* rand_select, int activation, int sample_all,
+                        float decay, float threshold, uint32_t* n_occupied_dev);
+
+/* Number of set bits in n_bytes bytes (reference count_1s, src/utils/bit-utils.cuh:52-94). */
+int tn_popcount(tn_ctx* ctx, tn_stream_t stream, uint64_t n_bytes, const uint8_t* bytes, uint32_t* out_dev);
+
+/* ---- Adam ---------------------------------------------------------------------- */
+/* Reference ngp_adam_step (src/core/adam-optimizer.cuh:48-96), vectorised by 4: params
+ * [0, n_grid) are the hash grid (a zero gradient skips the parameter: no moment decay,
+ * no step), [n_grid, n_grid+n_mlp) get L2 regularisation. lr is the already-decayed rate
+ * (reference 1e-2 / (1 + 3.3e-5 * step), nerf-network.cu:256). weights_copy (optional)
+ * receives the updated weights again (the network-precision copy). */
+int tn_adam_step(tn_stream_t stream, uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_scale, float lr,
+                 float beta1, float beta2, float epsilon, float l2_reg, float* weights, float* weights_copy,
+                 const float* gradients, float* first_moments, float* second_moments, uint32_t* param_steps);
+
+/* ---- plain path: one kernel per stage, one thread per ray --------------------------
+ * The reference's launch structure, kept as the baseline the fused path is measured
+ * against: thrust scans, blocking device->host reads, memsets, dense launches. */
+int tn_plain_march_count(tn_stream_t stream, const tn_grid_desc* grid, const uint8_t* bitfield,
+                         const tn_bbox* bbox, const tn_march_desc* march, uint32_t n_rays, uint32_t ray_stride,
+                         const float* ori, const float* dir, const float* ray_t, const float* ray_t_max,
+                         uint8_t* alive, uint32_t* n_steps);
+/* thrust exclusive_scan + reverse find_if + device->host copy + stream synchronise. */
+int tn_plain_scan_cut_sync(tn_stream_t stream, uint32_t n, const uint32_t* n_steps, uint32_t* offsets,
+                           uint32_t batch_size, uint32_t* n_rays_out, uint32_t* n_samples_out);
+int tn_plain_march_emit(tn_stream_t stream, const tn_grid_desc* grid, const uint8_t* bitfield,
+                        const tn_bbox* bbox, const tn_march_desc* march, float inv_aabb_size, uint32_t n_rays,
+                        uint32_t ray_stride, uint32_t sample_stride, const uint32_t* ray_img_id,
+                        const float* ori, const float* dir, const float* ray_t, const uint32_t* offsets,
+                        const uint8_t* alive, const uint32_t* n_steps, uint32_t* out_img_id, float* out_t,
+                        float* out_pos, float* out_dir, float* out_dt, float* out_m_norm, float* out_dt_norm);
+/* memsets + one thread per ray + thrust::reduce with a blocking read of the loss. */
+int tn_plain_recon_loss_sync(tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                             float min_transmittance, float inv_nrays, float grad_scale, const float* density,
+                             const float* rgb, const float* dt, const float* target_rgba, const float* bg_rgb,
+                             float* loss, float* dL_ddensity, float* dL_drgb, float* loss_out);
+/* memset + forward kernel + backward kernel (per-sample w_cs/wm_cs scratch, caller
+ * provided: 2 * sample_stride floats and 5 * ray_stride floats) + thrust::reduce. */
+int tn_plain_distortion_sync(tn_stream_t stream, const tn_ray_batch* batch, int activation, float lambda,
+                             const float* density, const float* m_norm, const float* dt_norm, float* ray_scratch,
+                             float* sample_scratch, float* ray_loss, float* dL_ddensity, float* loss_out);
+int tn_plain_grad_epilogue(tn_stream_t stream, uint32_t n_samples, float loss_scale, const float* dL_rec,
+                           const float* dL_dist, const float* t, float* grad_out);
+int tn_plain_occupancy_update_sync(tn_stream_t stream, const tn_grid_desc* grid, float* density,
+                                   uint8_t* bitfield, uint32_t n_updates, const int32_t* levels,
+                                   const uint32_t* cells, const float* values, const float* rand_select,
+                                   int activation, int sample_all, float decay, float threshold,
+                                   uint8_t* count_scratch, uint32_t* n_occupied_out);
+int tn_plain_adam_step(tn_stream_t stream, uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_scale,
+                       float lr, float beta1, float beta2, float epsilon, float l2_reg, float* weights,
+                       float* weights_copy, const float* gradients, float* first_moments, float* second_moments,
+                       uint32_t* param_steps);
+
+/* ---- synthetic producer (stand-in for the tiny-cuda-nn network) ------------------ */
+/* Gaussian-blob density and sinusoid colour at normalised positions pos[3][pos_stride]
+ * (world = (pos - 0.5) * aabb_size). blobs[n_blobs][5] = (cx, cy, cz, std, peak),
+ * waves[3][4] = (ax, ay, az, phase) are device arrays. n_dev optional live count. */
+int tn_synth_field(tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t pos_stride, const float* pos,
+                   float aabb_size, uint32_t n_blobs, const float* blobs, const float* waves, float* sigma,
+                   float* rgb, uint32_t out_stride);
+
+/* ---- trainer: the controller surface ----------------------------------------------
+ * Mirrors the reference's NeRFTrainingController / Trainer (src/controllers/
+ * nerf-training-controller.h:23-89, src/core/trainer.cuh:21-70): setup, train_step(),
+ * update_occupancy_grid(step), with the TrainingMetrics / OccupancyGridMetrics structs
+ * of nerf-training-controller.h:25-51. The network between the march and the losses is
+ * pluggable (tn_network); without one the trainer uses its built-in synthetic scene (a
+ * Gaussian-blob field for sigma/rgb and fixed sparse hash-grid gradients). */
+#define TN_PATH_FUSED 0 /* fused kernels, device batch cut, optional CUDA graph */
+#define TN_PATH_PLAIN 1 /* one kernel per stage, thrust, blocking reads (reference structure) */
+
+/* Producer/consumer of per-sample network values (the tiny-cuda-nn boundary). Every
+ * callback only enqueues work on `stream`; n is the buffer capacity, n_dev (device) the
+ * live count. Positions are normalised to [0,1]^3, [3][stride]. */
+typedef struct tn_network {
+    void* user;
+    int activation; /* TN_ACT_SIGMA or TN_ACT_DENSITY: what `forward` writes into density */
+    int (*forward)(void* user, tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t stride,
+                   const float* pos, const float* dir, float* density, float* rgb);
+    /* dL/d density (merged, scaled) and dL/d rgb -> parameter gradients; may be NULL */
+    int (*backward)(void* user, tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t stride,
+                    const float* pos, const float* dir, const float* dL_ddensity, const float* dL_drgb,
+                    float* param_grads);
+    /* density only, for occupancy updates */
+    int (*density)(void* user, tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t stride,
+                   const float* pos, float* density);
+} tn_network;
+
+typedef struct tn_trainer_desc {
+    tn_grid_desc grid;
+    tn_bbox bbox;                       /* training box; aabb size = max_x - min_x */
+    uint32_t batch_size;                /* sample capacity per step (reference batch_size) */
+    uint32_t n_rays_per_step;           /* rays generated and marched per step */
+    float min_step_size;                /* reference NeRFConstants::min_step_size */
+    float cone_angle;                   /* reference NeRFConstants::cone_angle */
+    uint32_t max_steps_per_ray;         /* 0 = unlimited */
+    float min_transmittance;            /* 1e-4 */
+    int32_t use_distortion_loss;
+    float distortion_lambda;            /* reference 0.01 */
+    float loss_scale;                   /* reference LOSS_SCALE (1 with fp32 network values) */
+    float occupancy_decay;              /* 0.95 */
+    float occupancy_threshold;          /* reference 0.01 * min_step_size */
+    uint32_t occupancy_cells_per_step;  /* > 0: re-sample this many random cells in every step */
+    uint32_t n_grid_params;             /* parameter layout [hash grid | MLP] */
+    uint32_t n_mlp_params;
+    float learning_rate;                /* 1e-2, decayed as lr / (1 + decay * step) */
+    float learning_rate_decay;          /* 3.3e-5 */
+    float beta1, beta2, epsilon, l2_reg;
+    int32_t path;                       /* TN_PATH_FUSED or TN_PATH_PLAIN */
+    int32_t use_cuda_graph;             /* fused path: capture the step once, replay after */
+    uint32_t seed;
+    float ray_radius;                   /* synthetic rays: origin sphere radius */
+    float ray_jitter;                   /* synthetic rays: direction jitter */
+} tn_trainer_desc;
+
+typedef struct tn_training_metrics {
+    uint32_t step;
+    uint32_t n_rays;
+    uint32_t n_samples;
+    float loss;
+} tn_training_metrics;
+
+typedef struct tn_occupancy_metrics {
+    uint32_t n_occupied;
+    uint32_t n_total;
+} tn_occupancy_metrics;
+
+typedef struct tn_trainer tn_trainer;
+
+/* Fills `out` with the reference defaults. */
+int tn_trainer_default_desc(tn_trainer_desc* out);
+/* Creates the trainer on the current device: allocates every buffer once (no allocation
+ * during steps), initialises the grid like the reference (all bits set, densities 0) and
+ * the parameters. `net` may be NULL (built-in synthetic scene). */
+int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_network* net);
+int tn_trainer_destroy(tn_trainer* tr);
+/* Synthetic scene of the built-in network: n_blobs x (cx, cy, cz, std, peak) and 3 x
+ * (ax, ay, az, phase), host arrays. */
+int tn_trainer_set_synthetic_field(tn_trainer* tr, uint32_t n_blobs, const float* blobs, const float* waves);
+/* Copies a grid state from host memory (density [n_levels][res^3], bitfield [res^3]). */
+int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bitfield);
+/* Fills the parameter gradient buffer with N(0, std) values on the hash-grid entries that
+ * one step's samples touch (and on every MLP weight), zero elsewhere; the built-in
+ * network then leaves it unchanged, so every step feeds Adam the same sparse gradients. */
+int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_touched_out);
+/* One training step (reference NeRFTrainingController::train_step,
+ * nerf-training-controller.cu:185-212). With metrics == NULL the fused path only enqueues
+ * (no host synchronisation); otherwise the call waits and fills the metrics. */
+int tn_trainer_train_step(tn_trainer* tr, tn_training_metrics* metrics);
+/* The same step on rays supplied by the caller in host memory (pinned for asynchronous
+ * copies): ori/dir [3][n_rays], target_rgba [4][n_rays], bg_rgb [3][n_rays]; n_rays must
+ * equal n_rays_per_step. Stands in for the reference's camera/image ray generation
+ * (training-batch-kernels.cuh:82-187); the box clip runs on the device. */
+int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori, const float* dir,
+                               const float* target_rgba, const float* bg_rgb, tn_training_metrics* metrics);
+/* Runs one fused step eagerly with events between its stages and writes the stage times
+ * (ms): rays, march count, march emit, network forward, losses, network backward,
+ * occupancy, Adam. */
+int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages);
+/* 0/1: kernel nodes in the captured step graph (synthetic / caller rays), 2: graph nodes,
+ * 3: samples processed so far, 4: rays used so far, 5: steps (3-5 synchronise). */
+int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out);
+/* Reference NeRFTrainingController::update_occupancy_grid (nerf-training-controller.cu:
+ * 214-226, trainer.cu:221-311): decay, every cell of every level re-sampled through the
+ * network (all selected while training_step < 256), bits, popcount. Synchronous. */
+int tn_trainer_update_occupancy_grid(tn_trainer* tr, uint32_t training_step, tn_occupancy_metrics* metrics);
+/* Waits for the trainer's stream and reads the last step's metrics. */
+int tn_trainer_sync_metrics(tn_trainer* tr, tn_training_metrics* metrics);
+int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out);
+/* Device pointers of the trainer's state, for inspection and tests:
+ * 0 weights, 1 gradients, 2 first moments, 3 second moments, 4 param steps, 5 grid
+ * density, 6 bitfield, 7 sample t, 8 sample pos, 9 sample dt, 10 ray offsets,
+ * 11 ray n_steps, 12 batch_info[4], 13 network density, 14 network rgb,
+ * 15 grad density, 16 dL/drgb, 17 ray origins, 18 ray directions, 19 ray t,
+ * 20 ray t_max, 21 ray alive, 22 target rgba, 23 background rgb, 24 m_norm, 25 dt_norm. */
+int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TURBO_HOT_H */

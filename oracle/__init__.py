@@ -1,0 +1,291 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings to the CPU oracle (oracle/oracle.cpp).
+
+The oracle restates the reference kernels of TurboNeRF's training hot path on the CPU
+(FP32 with the reference's operation order for integer outputs, FP64 for float
+outputs). Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only as the checker or the timed CPU baseline. Parity is UNPINNED:
+the reference ships no tests or golden vectors and cannot be built here.
+
+All arrays are numpy arrays in the reference's structure-of-arrays layout
+(component c of item i at buf[c * stride + i]).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "_build", "liboracle.so")
+
+_lib = None
+
+
+class Bbox(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")]
+
+
+def build() -> str:
+    """Compile oracle.cpp with the committed Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _SO
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(os.path.join(_HERE, "oracle.cpp")):
+            build()
+        _lib = ctypes.CDLL(_SO)
+        _declare(_lib)
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _declare(L):
+    i64, i32, u32, f32, f64, vp = (ctypes.c_int64, ctypes.c_int, ctypes.c_uint32,
+                                   ctypes.c_float, ctypes.c_double, ctypes.c_void_p)
+    sig = {
+        "orc_morton3d": (u32, [u32, u32, u32]),
+        "orc_morton3d_invert": (u32, [u32]),
+        "orc_fdiv_ru": (f32, [f32, f32]),
+        "orc_num_threads": (i32, []),
+        "orc_set_num_threads": (None, [i32]),
+        "orc_rays_init_bbox": (None, [i64, i64, ctypes.POINTER(Bbox), f32, vp, vp, vp, vp, vp]),
+        "orc_march_count": (i64, [i64, i64, ctypes.POINTER(Bbox), i32, i32, f32, vp, f32, f32, f32, u32, u32,
+                                  vp, vp, vp, vp, vp, vp]),
+        "orc_scan_cut": (i32, [i64, vp, u32, vp, ctypes.POINTER(u32), ctypes.POINTER(u32)]),
+        "orc_march_emit": (None, [i64, i64, i64, ctypes.POINTER(Bbox), f32, i32, i32, f32, vp, f32, f32, f32,
+                                  vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "orc_compact_nonzero": (i64, [i64, vp, vp]),
+        "orc_recon_fwd_bwd": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, vp, vp, f64, f64, f64, f64,
+                                     vp, vp, vp, vp, vp, vp]),
+        "orc_recon_loss_rgb": (f64, [i64, i64, i64, vp, vp, i32, vp, vp, vp, vp, vp, f64, f64, vp]),
+        "orc_composite_fwd": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, f64, vp, vp]),
+        "orc_composite_vjp": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, f64, vp, vp, vp]),
+        "orc_distortion_fwd_bwd": (None, [i64, vp, vp, i32, vp, vp, vp, f64, vp, vp, vp]),
+        "orc_distortion_loss_sum": (f64, [i64, vp, vp, i32, vp, vp, vp, f64]),
+        "orc_grad_epilogue": (None, [i64, f64, vp, vp, vp, vp]),
+        "orc_occupancy_sample_points": (None, [i64, i32, f32, vp, vp, vp, i64, f32, vp, i64]),
+        "orc_occupancy_update": (ctypes.c_uint64, [i32, i32, vp, vp, i64, vp, vp, vp, vp, i32, i32, f32, f32]),
+        "orc_popcount": (ctypes.c_uint64, [i64, vp]),
+        "orc_adam_step": (None, [i64, i64, i64, f64, f64, f64, f64, f64, f64, vp, vp, vp, vp, vp, vp]),
+        "orc_blob_field": (None, [i64, i64, vp, f32, i32, vp, vp, vp, vp, i64]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def bbox_struct(bbox):
+    b = [float(v) for v in bbox]
+    return Bbox(*b)
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+def morton3d(x, y, z) -> int:
+    return lib().orc_morton3d(int(x), int(y), int(z))
+
+
+def morton3d_invert(v) -> int:
+    return lib().orc_morton3d_invert(int(v))
+
+
+def fdiv_ru(a, b) -> float:
+    return lib().orc_fdiv_ru(float(a), float(b))
+
+
+def rays_init_bbox(ori, dir_, stride, n, bbox, t_far=3.0e38):
+    ori, dir_ = _c(ori, np.float32), _c(dir_, np.float32)
+    t = np.zeros(n, np.float32)
+    tmax = np.zeros(n, np.float32)
+    alive = np.zeros(n, np.uint8)
+    b = bbox_struct(bbox)
+    lib().orc_rays_init_bbox(n, stride, ctypes.byref(b), t_far, _p(ori), _p(dir_), _p(t), _p(tmax), _p(alive))
+    return t, tmax, alive
+
+
+def march_count(rays, grid, march, max_iters=1 << 24):
+    """rays: dict(ori, dir, t, t_max, alive, stride, n); grid: dict(n_levels, res, base, bitfield);
+    march: dict(bbox, cone, dt_min, dt_max, max_steps). Returns (n_steps, alive, n_guard)."""
+    n, stride = rays["n"], rays["stride"]
+    alive = _c(rays["alive"], np.uint8).copy()
+    n_steps = np.zeros(n, np.uint32)
+    b = bbox_struct(march["bbox"])
+    bits = _c(grid["bitfield"], np.uint8)
+    ori, dir_ = _c(rays["ori"], np.float32), _c(rays["dir"], np.float32)
+    t, tmax = _c(rays["t"], np.float32), _c(rays["t_max"], np.float32)
+    guard = lib().orc_march_count(n, stride, ctypes.byref(b), grid["n_levels"], grid["res"], grid["base"],
+                                  _p(bits), march["cone"], march["dt_min"], march["dt_max"],
+                                  march.get("max_steps", 0), max_iters, _p(ori), _p(dir_), _p(t), _p(tmax),
+                                  _p(alive), _p(n_steps))
+    return n_steps, alive, guard
+
+
+def scan_cut(n_steps, batch_size):
+    n_steps = _c(n_steps, np.uint32)
+    offsets = np.zeros(len(n_steps), np.uint32)
+    nr, ns = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    st = lib().orc_scan_cut(len(n_steps), _p(n_steps), batch_size, _p(offsets), ctypes.byref(nr), ctypes.byref(ns))
+    return st, offsets, nr.value, ns.value
+
+
+def march_emit(rays, grid, march, offsets, n_steps, alive, n_rays, sample_stride, inv_aabb, img_id=None):
+    stride = rays["stride"]
+    ss = sample_stride
+    out = {
+        "img_id": np.zeros(ss, np.uint32), "t": np.zeros(ss, np.float32), "pos": np.zeros(3 * ss, np.float32),
+        "dir": np.zeros(3 * ss, np.float32), "dt": np.zeros(ss, np.float32), "m_norm": np.zeros(ss, np.float32),
+        "dt_norm": np.zeros(ss, np.float32),
+    }
+    b = bbox_struct(march["bbox"])
+    bits = _c(grid["bitfield"], np.uint8)
+    ori, dir_ = _c(rays["ori"], np.float32), _c(rays["dir"], np.float32)
+    t = _c(rays["t"], np.float32)
+    img = _c(img_id, np.uint32) if img_id is not None else None
+    lib().orc_march_emit(n_rays, stride, ss, ctypes.byref(b), inv_aabb, grid["n_levels"], grid["res"], grid["base"],
+                         _p(bits), march["cone"], march["dt_min"], march["dt_max"], _p(img), _p(ori), _p(dir_), _p(t),
+                         _p(_c(offsets, np.uint32)), _p(_c(alive, np.uint8)), _p(_c(n_steps, np.uint32)),
+                         _p(out["img_id"]), _p(out["t"]), _p(out["pos"]), _p(out["dir"]), _p(out["dt"]),
+                         _p(out["m_norm"]), _p(out["dt_norm"]))
+    return out
+
+
+def compact_nonzero(values):
+    values = _c(values, np.uint32)
+    out = np.zeros(len(values), np.int32)
+    c = lib().orc_compact_nonzero(len(values), _p(values), _p(out))
+    return out[:c]
+
+
+def recon_fwd_bwd(counts, offsets, density, rgb, dt, target_rgba, bg_rgb, ray_stride, sample_stride,
+                  act=0, inv_nrays=None, grad_scale=1.0, min_t=1e-4, amb_eps=1e-4):
+    n = len(counts)
+    if inv_nrays is None:
+        inv_nrays = 1.0 / max(n, 1)
+    ray_rgba = np.zeros(4 * ray_stride)
+    loss = np.zeros(4 * ray_stride)
+    dd = np.zeros(sample_stride)
+    drgb = np.zeros(3 * sample_stride)
+    used = np.zeros(n, np.uint32)
+    amb = np.zeros(n, np.uint8)
+    lib().orc_recon_fwd_bwd(n, ray_stride, sample_stride, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
+                            _p(_c(density, np.float32)), _p(_c(rgb, np.float32)), _p(_c(dt, np.float32)),
+                            _p(_c(target_rgba, np.float32)), _p(_c(bg_rgb, np.float32)), inv_nrays, grad_scale,
+                            min_t, amb_eps, _p(ray_rgba), _p(loss), _p(dd), _p(drgb), _p(used), _p(amb))
+    return dict(ray_rgba=ray_rgba, loss=loss, dL_ddensity=dd, dL_drgb=drgb, n_used=used, ambiguous=amb)
+
+
+def recon_loss_rgb(counts, offsets, density, rgb, dt, target_rgba, bg_rgb, ray_stride, sample_stride,
+                   act=0, inv_nrays=None, min_t=1e-4, fixed_used=None):
+    n = len(counts)
+    if inv_nrays is None:
+        inv_nrays = 1.0 / max(n, 1)
+    fu = _c(fixed_used, np.uint32) if fixed_used is not None else None
+    return lib().orc_recon_loss_rgb(n, ray_stride, sample_stride, _p(_c(counts, np.uint32)),
+                                    _p(_c(offsets, np.uint32)), act, _p(_c(density, np.float64)),
+                                    _p(_c(rgb, np.float64)), _p(_c(dt, np.float64)), _p(_c(target_rgba, np.float64)),
+                                    _p(_c(bg_rgb, np.float64)), inv_nrays, min_t, _p(fu))
+
+
+def composite_fwd(counts, offsets, density, rgb, dt, ray_stride, sample_stride, act=0, min_t=1e-4):
+    n = len(counts)
+    rgba = np.zeros(4 * ray_stride)
+    used = np.zeros(n, np.uint32)
+    lib().orc_composite_fwd(n, ray_stride, sample_stride, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
+                            _p(_c(density, np.float32)), _p(_c(rgb, np.float32)), _p(_c(dt, np.float32)), min_t,
+                            _p(rgba), _p(used))
+    return rgba, used
+
+
+def composite_vjp(counts, offsets, density, rgb, dt, grad_rgba, ray_stride, sample_stride, act=0, min_t=1e-4):
+    n = len(counts)
+    dd = np.zeros(sample_stride)
+    drgb = np.zeros(3 * sample_stride)
+    lib().orc_composite_vjp(n, ray_stride, sample_stride, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
+                            _p(_c(density, np.float32)), _p(_c(rgb, np.float32)), _p(_c(dt, np.float32)), min_t,
+                            _p(_c(grad_rgba, np.float64)), _p(dd), _p(drgb))
+    return dd, drgb
+
+
+def distortion_fwd_bwd(counts, offsets, density, m_norm, dt_norm, lam, n_samples, act=0, grad_ray=None):
+    n = len(counts)
+    loss = np.zeros(n)
+    dd = np.zeros(max(n_samples, 1))
+    gr = _c(grad_ray, np.float64) if grad_ray is not None else None
+    lib().orc_distortion_fwd_bwd(n, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
+                                 _p(_c(density, np.float32)), _p(_c(m_norm, np.float32)), _p(_c(dt_norm, np.float32)),
+                                 lam, _p(gr), _p(loss), _p(dd))
+    return loss, dd
+
+
+def distortion_loss_sum(counts, offsets, density, m_norm, dt_norm, lam, act=0):
+    return lib().orc_distortion_loss_sum(len(counts), _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
+                                         _p(_c(density, np.float64)), _p(_c(m_norm, np.float64)),
+                                         _p(_c(dt_norm, np.float64)), lam)
+
+
+def grad_epilogue(n_samples, loss_scale, dL_rec, dL_dist, sample_t, grad_in):
+    g = _c(grad_in, np.float64).copy()
+    lib().orc_grad_epilogue(n_samples, loss_scale, _p(_c(dL_rec, np.float64)),
+                            _p(_c(dL_dist, np.float64) if dL_dist is not None else None),
+                            _p(_c(sample_t, np.float32) if sample_t is not None else None), _p(g))
+    return g
+
+
+def occupancy_sample_points(levels, cells, rand3, rand_stride, res, base, inv_aabb, pos_stride):
+    n = len(levels)
+    out = np.zeros(3 * pos_stride, np.float32)
+    lib().orc_occupancy_sample_points(n, res, base, _p(_c(levels, np.int32)), _p(_c(cells, np.uint32)),
+                                      _p(_c(rand3, np.float32)), rand_stride, inv_aabb, _p(out), pos_stride)
+    return out
+
+
+def occupancy_update(density, bitfield, n_levels, res, levels, cells, values, rand_select, act=0,
+                     sample_all=False, decay=0.95, threshold=0.01):
+    d = _c(density, np.float32).copy()
+    b = _c(bitfield, np.uint8).copy()
+    n = len(levels)
+    occ = lib().orc_occupancy_update(n_levels, res, _p(d), _p(b), n, _p(_c(levels, np.int32)),
+                                     _p(_c(cells, np.uint32)), _p(_c(values, np.float32)),
+                                     _p(_c(rand_select, np.float32)), act, int(bool(sample_all)), decay, threshold)
+    return d, b, int(occ)
+
+
+def popcount(bytes_):
+    b = _c(bytes_, np.uint8)
+    return int(lib().orc_popcount(len(b), _p(b)))
+
+
+def adam_step(state, grad, n_grid, n_mlp, loss_scale=1.0, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-15, l2=1e-6):
+    """state: dict(w=f64, m=f64, v=f64, steps=u32), updated in place."""
+    n = len(state["w"])
+    lib().orc_adam_step(n, n_grid, n_mlp, loss_scale, lr, beta1, beta2, eps, l2, _p(state["w"]),
+                        _p(_c(grad, np.float32)), _p(state["m"]), _p(state["v"]), _p(state["steps"]), None)
+    return state
+
+
+def blob_field(pos, stride, n, aabb_size, blobs, waves, out_stride=None, want_rgb=True):
+    out_stride = out_stride or n
+    sig = np.zeros(n)
+    rgb = np.zeros(3 * out_stride) if want_rgb else None
+    lib().orc_blob_field(n, stride, _p(_c(pos, np.float32)), aabb_size, len(blobs), _p(_c(blobs, np.float32)),
+                         _p(_c(waves, np.float32)), _p(sig), _p(rgb), out_stride)
+    return sig, rgb

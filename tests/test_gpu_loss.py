@@ -1,0 +1,160 @@
+"""Parity of the CUDA compositor, reconstruction loss, distortion loss and gradient merge
+against the FP64 oracle.
+
+Tolerances: composited RGBA per element within 1e-5 relative; loss sums within 1e-5
+relative; gradient vectors within 1e-4 in the normwise relative error (max |g - ref| /
+max |ref|), for the whole batch and, where the upstream gradient is fixed, for every ray
+(see tests/helpers.py for why entries are not checked one by one)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import (RTOL_COMPOSITE, RTOL_GRAD, assert_close, assert_norm_close, assert_per_ray_norm_close,
+                           dev, expand_rays, host, i32)
+from turbonerf_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(n_samples, mean, seed=0x7B1):
+    return scenes.make_sample_batch(seed, n_samples, mean=mean)
+
+
+def _rb(sb, counts_t, offsets_t):
+    from turbonerf_b200.hotpath import ray_batch
+    return ray_batch(counts_t, offsets_t, sb.n_rays, sb.n_rays, sb.n_samples)
+
+
+def _rgb_ok(ref_rgba, gpu_rgba, n_rays, mask):
+    for c in range(4):
+        assert_close(gpu_rgba[c * n_rays:(c + 1) * n_rays], ref_rgba[c * n_rays:(c + 1) * n_rays], RTOL_COMPOSITE,
+                     f"rgba[{c}]", mask=mask)
+
+
+@pytest.mark.parametrize("mean,n_samples", [(48, 1 << 18), (3, 4096), (700, 1 << 16)])
+def test_composite_forward_and_vjp(mean, n_samples):
+    from turbonerf_b200 import hotpath as hp
+    sb = _batch(n_samples, mean)
+    n, ss = sb.n_rays, sb.n_samples
+    ctx = hp.Context()
+    counts, offsets = i32(sb.counts), i32(sb.offsets)
+    rb = _rb(sb, counts, offsets)
+    sig, rgb, dt = dev(sb.sigma), dev(sb.rgb), dev(sb.dt)
+    out = hp.composite_fwd(ctx, rb, sig, rgb, dt)
+    ref_rgba, ref_used = oracle.composite_fwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, n, ss)
+    # rays whose transmittance check sits at the threshold within FP32 rounding may cut one
+    # sample apart; they are identified by the oracle and checked separately
+    rec = oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss,
+                               amb_eps=1e-5)
+    ok = rec["ambiguous"] == 0
+    assert ok.mean() > 0.97
+    _rgb_ok(ref_rgba, host(out["rgba"]), n, ok)
+    used = host(out["n_used"]).view(np.uint32)
+    assert np.array_equal(used[ok], ref_used[ok])
+    g = np.random.default_rng(1).normal(size=4 * n)
+    dd, drgb = hp.composite_bwd(ctx, rb, sig, rgb, dt, out["depth"], out["n_used"], dev(g.astype(np.float32)))
+    ref_dd, ref_drgb = oracle.composite_vjp(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt,
+                                            g.astype(np.float32).astype(np.float64), n, ss)
+    sm = expand_rays(ok, sb.counts, sb.offsets, ss)
+    assert_per_ray_norm_close(host(dd), ref_dd, sb.counts, sb.offsets, RTOL_GRAD, "dL/dsigma", ray_mask=ok)
+    for c in range(3):
+        assert_per_ray_norm_close(host(drgb)[c * ss:(c + 1) * ss], ref_drgb[c * ss:(c + 1) * ss], sb.counts, sb.offsets,
+                                  RTOL_GRAD, f"dL/drgb[{c}]", ray_mask=ok)
+    assert_norm_close(host(dd), ref_dd, RTOL_GRAD, "dL/dsigma (batch)", mask=sm)
+    assert ctx.check() == 0
+
+
+@pytest.mark.parametrize("act", [0, 1])
+def test_recon_loss_fused_and_plain(act):
+    from turbonerf_b200 import hotpath as hp
+    sb = _batch(1 << 18, 48, seed=0x7B2)
+    n, ss = sb.n_rays, sb.n_samples
+    dens = sb.sigma if act == 0 else np.log(np.maximum(sb.sigma, 1e-6)).astype(np.float32) + 1.0
+    ctx = hp.Context()
+    counts, offsets = i32(sb.counts), i32(sb.offsets)
+    rb = _rb(sb, counts, offsets)
+    args = (dev(dens), dev(sb.rgb), dev(sb.dt), dev(sb.target_rgba), dev(sb.bg_rgb))
+    out = hp.recon_loss_fwd_bwd(ctx, rb, *args, inv_nrays=1.0 / n, grad_scale=1.0, activation=act)
+    ref = oracle.recon_fwd_bwd(sb.counts, sb.offsets, dens, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss, act=act)
+    ok = ref["ambiguous"] == 0
+    _rgb_ok(ref["ray_rgba"], host(out["ray_rgba"]), n, ok)
+    for c in range(4):
+        assert_norm_close(host(out["loss"])[c * n:(c + 1) * n], ref["loss"][c * n:(c + 1) * n], 1e-4, f"loss[{c}]",
+                          mask=ok)
+    ref_sum = ref["loss"][:4 * n].sum() / n
+    assert abs(float(host(out["loss_sum"])[0]) - ref_sum) <= 1e-5 * abs(ref_sum)
+    sm = expand_rays(ok, sb.counts, sb.offsets, ss)
+    assert_norm_close(host(out["dL_ddensity"]), ref["dL_ddensity"], RTOL_GRAD, "dL/ddensity", mask=sm)
+    assert_norm_close(host(out["dL_drgb"]), ref["dL_drgb"], RTOL_GRAD, "dL/drgb", mask=np.tile(sm, 3))
+    # the plain path (reference structure, one thread per ray, FP32 suffix subtraction)
+    loss, dd, drgb, lsum = hp.plain_recon_loss(rb, *args, inv_nrays=1.0 / n, grad_scale=1.0, activation=act)
+    assert abs(lsum - ref_sum) <= 1e-4 * abs(ref_sum)
+    assert_norm_close(host(dd), ref["dL_ddensity"], 1e-3, "plain dL/ddensity", mask=sm)
+    assert ctx.check() == 0
+
+
+@pytest.mark.parametrize("mean,n_samples", [(48, 1 << 18), (2, 2048), (1024, 1 << 16)])
+def test_distortion_fused_and_plain(mean, n_samples):
+    from turbonerf_b200 import hotpath as hp
+    sb = _batch(n_samples, mean, seed=0x7B3)
+    n, ss = sb.n_rays, sb.n_samples
+    lam = 1e-3
+    ctx = hp.Context()
+    counts, offsets = i32(sb.counts), i32(sb.offsets)
+    rb = _rb(sb, counts, offsets)
+    out = hp.distortion_fwd_bwd(ctx, rb, dev(sb.sigma), dev(sb.m_norm), dev(sb.dt_norm), lam)
+    ref_loss, ref_dd = oracle.distortion_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.m_norm, sb.dt_norm, lam, ss)
+    assert_norm_close(host(out["ray_loss"])[:n], ref_loss, 1e-4, "ray distortion loss")
+    assert abs(float(host(out["loss_sum"])[0]) - ref_loss.mean()) <= 1e-5 * abs(ref_loss.mean())
+    assert_norm_close(host(out["dL_ddensity"]), ref_dd, RTOL_GRAD, "dLdist/dsigma")
+    assert_per_ray_norm_close(host(out["dL_ddensity"]), ref_dd, sb.counts, sb.offsets, RTOL_GRAD,
+                              "dLdist/dsigma per ray")
+    ray_loss, dd, lsum = hp.plain_distortion(rb, dev(sb.sigma), dev(sb.m_norm), dev(sb.dt_norm), lam)
+    assert abs(lsum - ref_loss.mean()) <= 1e-3 * abs(ref_loss.mean())
+    assert ctx.check() == 0
+
+
+def test_train_losses_fused_matches_oracle_chain():
+    """One kernel = reconstruction fwd/bwd + distortion fwd/bwd + gradient merge with
+    distance scaling, against the oracle's separate stages."""
+    from turbonerf_b200 import hotpath as hp
+    sb = _batch(1 << 18, 48, seed=0x7B4)
+    n, ss = sb.n_rays, sb.n_samples
+    lam, scale = 1e-3, 1.0
+    t_world = (sb.t * 0.9).astype(np.float32)  # part of the samples below t = 1
+    grad_in = np.random.default_rng(2).normal(0, 1e-3, ss).astype(np.float32)
+    ctx = hp.Context()
+    counts, offsets = i32(sb.counts), i32(sb.offsets)
+    rb = _rb(sb, counts, offsets)
+    gd = dev(grad_in.copy())
+    ray_rgba = dev(np.zeros(4 * n, np.float32))
+    gd, drgb, sums = hp.train_losses(ctx, rb, dev(sb.sigma), dev(sb.rgb), dev(sb.dt), dev(sb.m_norm), dev(sb.dt_norm),
+                                     dev(t_world), dev(sb.target_rgba), dev(sb.bg_rgb), gd, inv_nrays=1.0 / n,
+                                     grad_scale=scale, lam=lam, ray_rgba=ray_rgba)
+    rec = oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss,
+                               grad_scale=scale)
+    dl, ddist = oracle.distortion_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.m_norm, sb.dt_norm, lam, ss)
+    ref_g = oracle.grad_epilogue(ss, scale, rec["dL_ddensity"], ddist, t_world, grad_in.astype(np.float64))
+    ok = rec["ambiguous"] == 0
+    sm = expand_rays(ok, sb.counts, sb.offsets, ss)
+    assert_norm_close(host(gd), ref_g, RTOL_GRAD, "merged density gradient", mask=sm)
+    assert_norm_close(host(drgb), rec["dL_drgb"], RTOL_GRAD, "dL/drgb", mask=np.tile(sm, 3))
+    _rgb_ok(rec["ray_rgba"], host(ray_rgba), n, ok)
+    s = host(sums)
+    assert abs(s[0] - rec["loss"][:4 * n].sum() / n) <= 1e-5 * abs(rec["loss"][:4 * n].sum() / n)
+    assert abs(s[1] - dl.mean()) <= 1e-5 * abs(dl.mean())
+    assert ctx.check() == 0
+
+
+def test_grad_epilogue_fused_and_plain():
+    from turbonerf_b200 import hotpath as hp
+    rng = np.random.default_rng(9)
+    n = 100003
+    rec, dist = rng.normal(size=n).astype(np.float32), rng.normal(size=n).astype(np.float32)
+    t = rng.uniform(0, 2, n).astype(np.float32)
+    g0 = rng.normal(size=n).astype(np.float32)
+    ref = oracle.grad_epilogue(n, 128.0, rec.astype(np.float64), dist.astype(np.float64), t, g0.astype(np.float64))
+    a = hp.grad_epilogue(n, 128.0, dev(rec), dev(dist), dev(t), dev(g0.copy()))
+    b = hp.plain_grad_epilogue(n, 128.0, dev(rec), dev(dist), dev(t), dev(g0.copy()))
+    assert_norm_close(host(a), ref, 1e-6, "fused epilogue")
+    assert_norm_close(host(b), ref, 1e-6, "plain epilogue")

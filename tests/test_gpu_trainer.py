@@ -1,0 +1,147 @@
+"""The C++ training controller on the GPU: one fused train step checked stage by stage
+against the oracle, fused vs plain path, graph replay vs eager, and the full-grid
+occupancy update of the reference API."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import RTOL_GRAD, assert_bitwise, assert_norm_close, expand_rays
+from turbonerf_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+R, B = 4096, 1 << 16
+
+
+def _make(path="fused", graph=True, cells=4096, seed=0x7B0):
+    from turbonerf_b200.trainer import SyntheticNeRF, Trainer
+    sc = scenes.march_scene_cascaded(n_rays=8, n_levels=5)
+    tr = Trainer(SyntheticNeRF.from_scene(sc), path=path, use_cuda_graph=graph, n_rays_per_step=R,
+                 occupancy_cells_per_step=cells, distortion_lambda=1e-3, occupancy_threshold=0.01,
+                 n_grid_params=16 * (1 << 15) * 2, n_mlp_params=7168, beta2=0.99, seed=seed)
+    tr.use_distortion_loss = True
+    tr.setup_data(batch_size=B)
+    return sc, tr
+
+
+def _h(t, dtype=np.float32):
+    return t.cpu().numpy().view(dtype) if t.dtype.itemsize == np.dtype(dtype).itemsize else t.cpu().numpy()
+
+
+def test_fused_step_matches_oracle_stage_by_stage():
+    sc, tr = _make()
+    import torch
+    w0 = tr.buffer(0).clone()
+    m = tr.train_step()
+    torch.cuda.synchronize()
+    rays = scenes.RayBatch(R, R, _h(tr.buffer(17)), _h(tr.buffer(18)), _h(tr.buffer(19)), _h(tr.buffer(20)),
+                           _h(tr.buffer(21, np.uint8)))
+    march = dict(bbox=sc.bbox, cone=sc.cone_angle, dt_min=sc.dt_min, dt_max=sc.dt_max, max_steps=0)
+    # the rays' box clip
+    t_o, tm_o, a_o = oracle.rays_init_bbox(rays.ori, rays.dir, R, R, sc.bbox)
+    assert_bitwise(rays.t, t_o, "ray t")
+    assert_bitwise(rays.t_max, tm_o, "ray t_max")
+    # march on the grid as it was before the step's occupancy update
+    ns, alive, _ = oracle.march_count(dict(rays.as_dict(), alive=a_o), sc.grid.as_dict(), march)
+    st, off, nr, nsamp = oracle.scan_cut(ns, B)
+    assert st == 0
+    assert (m.n_rays, m.n_samples) == (nr, nsamp)
+    assert_bitwise(_h(tr.buffer(11), np.uint32), ns, "n_steps")
+    assert_bitwise(_h(tr.buffer(10), np.uint32), off, "offsets")
+    em = oracle.march_emit(dict(rays.as_dict(), alive=a_o), sc.grid.as_dict(), march, off, ns, alive, nr, B,
+                           1.0 / sc.aabb_size)
+    for idx, key in ((7, "t"), (9, "dt"), (24, "m_norm"), (25, "dt_norm")):
+        assert_bitwise(_h(tr.buffer(idx))[:nsamp], em[key][:nsamp], key)
+    assert_bitwise(_h(tr.buffer(8)).reshape(3, B)[:, :nsamp], em["pos"].reshape(3, B)[:, :nsamp], "pos")
+    # losses and the merged gradient on the trainer's own network outputs
+    sig, rgb = _h(tr.buffer(13)), _h(tr.buffer(14))
+    tgt = _h(tr.buffer(22))
+    bg = _h(tr.buffer(23))
+    tgt_c = np.concatenate([tgt[c * R:c * R + nr] for c in range(4)])
+    bg_c = np.concatenate([bg[c * R:c * R + nr] for c in range(3)])
+    rec = oracle.recon_fwd_bwd(ns[:nr], off[:nr], sig, rgb, em["dt"], tgt_c, bg_c, nr, B)
+    dl, ddist = oracle.distortion_fwd_bwd(ns[:nr], off[:nr], sig, em["m_norm"], em["dt_norm"], 1e-3, B)
+    ref_g = oracle.grad_epilogue(nsamp, 1.0, rec["dL_ddensity"][:nsamp], ddist[:nsamp], em["t"][:nsamp],
+                                 np.zeros(nsamp))
+    ok = rec["ambiguous"] == 0
+    sm = expand_rays(ok, ns[:nr], off[:nr], nsamp)
+    assert_norm_close(_h(tr.buffer(15))[:nsamp], ref_g, RTOL_GRAD, "merged density gradient", mask=sm)
+    ref_loss = rec["loss"][:4 * nr].sum() / nr + dl.mean()
+    assert abs(m.loss - ref_loss) <= 1e-5 * abs(ref_loss)
+    # Adam on the fixed synthetic gradients
+    g = _h(tr.buffer(1))
+    state = dict(w=_h(w0).astype(np.float64), m=np.zeros(len(g)), v=np.zeros(len(g)),
+                 steps=np.zeros(len(g), np.uint32))
+    f32 = lambda x: float(np.float32(x))  # noqa: E731
+    oracle.adam_step(state, g, 16 * (1 << 15) * 2, 7168, lr=f32(1e-2), beta1=f32(0.9), beta2=f32(0.99),
+                     eps=f32(1e-15), l2=f32(1e-6))
+    w = _h(tr.buffer(0)).astype(np.float64)
+    moved = np.abs(state["w"] - _h(w0))
+    t = state["steps"] > 0
+    assert float((np.abs(w - state["w"])[t] / moved[t]).max()) <= 1e-4
+    assert_bitwise(_h(tr.buffer(4), np.uint32), state["steps"], "param steps")
+    tr.teardown()
+
+
+def test_fused_and_plain_paths_agree():
+    sc, f = _make("fused")
+    _, p = _make("plain")
+    for _ in range(3):
+        mf = f.train_step()
+        mp = p.train_step()
+        assert (mf.step, mf.n_rays, mf.n_samples) == (mp.step, mp.n_rays, mp.n_samples)
+        assert abs(mf.loss - mp.loss) <= 1e-3 * abs(mp.loss)
+    assert_bitwise(_h(f.buffer(6, np.uint8)), _h(p.buffer(6, np.uint8)), "bitfield after 3 steps")
+    assert_bitwise(_h(f.buffer(5)), _h(p.buffer(5)), "grid density after 3 steps")
+    assert_norm_close(_h(f.buffer(0)), _h(p.buffer(0)), 1e-5, "weights after 3 steps")
+    assert_bitwise(_h(f.buffer(4), np.uint32), _h(p.buffer(4), np.uint32), "param steps")
+    f.teardown()
+    p.teardown()
+
+
+def test_graph_replay_matches_eager_bitwise():
+    _, a = _make("fused", graph=True)
+    _, b = _make("fused", graph=False)
+    for _ in range(4):
+        a.train_step_async()
+        b.train_step_async()
+    ma, mb = a.sync_metrics(), b.sync_metrics()
+    assert (ma.step, ma.n_rays, ma.n_samples) == (mb.step, mb.n_rays, mb.n_samples) == (4, ma.n_rays, ma.n_samples)
+    assert ma.loss == mb.loss
+    for idx in (0, 2, 3, 5, 15, 16):
+        assert_bitwise(_h(a.buffer(idx)), _h(b.buffer(idx)), f"buffer {idx}")
+    assert_bitwise(_h(a.buffer(6, np.uint8)), _h(b.buffer(6, np.uint8)), "bitfield")
+    assert a.stat(0) >= 10  # kernels captured in one step graph
+    assert a.stat(3) > 0  # samples processed so far
+    a.teardown()
+    b.teardown()
+
+
+def test_update_occupancy_grid_fused_and_plain():
+    _, f = _make("fused", cells=0)
+    _, p = _make("plain", cells=0)
+    for step in (3, 300):
+        mf = f.update_occupancy_grid(step)
+        mp = p.update_occupancy_grid(step)
+        assert mf.n_total == mp.n_total == 5 * 128 ** 3
+        assert mf.n_occupied == mp.n_occupied
+        assert_bitwise(_h(f.buffer(5)), _h(p.buffer(5)), f"density after update at step {step}")
+        assert_bitwise(_h(f.buffer(6, np.uint8)), _h(p.buffer(6, np.uint8)), "bitfield")
+        assert oracle.popcount(_h(f.buffer(6, np.uint8))) == mf.n_occupied
+    f.teardown()
+    p.teardown()
+
+
+def test_train_step_rays_host_input():
+    import torch
+    sc, tr = _make()
+    rng = np.random.default_rng(3)
+    r = scenes.sphere_rays(rng, R)
+    tgt = np.concatenate([rng.uniform(0, 1, 3 * R), np.ones(R)]).astype(np.float32)
+    bg = rng.uniform(0, 1, 3 * R).astype(np.float32)
+    host = [torch.from_numpy(a).pin_memory() for a in (r.ori, r.dir, tgt, bg)]
+    m1 = tr.train_step_rays(*host)
+    m2 = tr.train_step_rays(*host)  # second call replays the captured graph
+    assert m1.n_samples > 0 and m2.step == 2
+    assert_bitwise(_h(tr.buffer(17)), r.ori, "uploaded origins")
+    tr.teardown()

@@ -1,0 +1,953 @@
+// Volume-rendering compositor, reconstruction loss and mip-NeRF 360 distortion loss,
+// forward and backward (sm_100a).
+//
+// Layout: one warp per ray (grid-stride over rays, static assignment so reductions are
+// deterministic); the ray's samples are walked in chunks of 32, one sample per lane, with
+// coalesced loads of the structure-of-arrays inputs. Running quantities along the ray
+// (optical depth, weight sums) are warp-shuffle prefix scans carried across chunks.
+//
+// Backward passes walk the chunks from the last to the first and obtain every suffix sum
+// (sum over later samples) by a reverse scan, instead of subtracting a running prefix from
+// the ray total as the reference does (src/utils/training-kernels-fused.cuh:204-208, 310-313).
+// Compositor transmittance is recomputed in the backward from the saved per-ray optical
+// depth S and the reverse scan of sigma*dt: T_{j+1} = exp(-(S - sum_{i>j} x_i)). No
+// per-sample transmittance or weight is stored between forward and backward.
+//
+// The distortion loss runs without a transmittance cut, so its optical depth can be large;
+// its prefix quantities are therefore recomputed in the forward direction from per-chunk
+// carries (held in lane registers for the first 64 chunks) rather than by subtraction.
+#include <thrust/device_ptr.h>
+#include <thrust/execution_policy.h>
+#include <thrust/reduce.h>
+
+#include "tn_internal.cuh"
+
+namespace tn {
+
+constexpr int LOSS_WARPS = 8;
+constexpr int LOSS_THREADS = LOSS_WARPS * WARP;
+constexpr int SAVED_CHUNKS = 64;  // distortion chunk carries kept in registers (2 per lane)
+
+__device__ __forceinline__ float act_sigma(int act, float d) { return act == 0 ? d : expf(fminf(d, 12.0f) - 1.0f); }
+__device__ __forceinline__ float act_dsigma(int act, float sigma) { return act == 0 ? 1.0f : sigma; }
+
+// Exclusive value from an inclusive warp scan: lane 0 gets `carry`.
+__device__ __forceinline__ float shift_up(float incl, int lane, float carry) {
+    const float v = __shfl_up_sync(FULL_MASK, incl, 1);
+    return lane == 0 ? carry : v;
+}
+// Exclusive value from an inclusive suffix scan: lane 31 gets `carry`.
+__device__ __forceinline__ float shift_down(float incl, int lane, float carry) {
+    const float v = __shfl_down_sync(FULL_MASK, incl, 1);
+    return lane == WARP - 1 ? carry : v;
+}
+
+struct Samples {
+    const float* __restrict__ density;
+    const float* __restrict__ rgb;
+    const float* __restrict__ dt;
+    const float* __restrict__ m_norm;
+    const float* __restrict__ dt_norm;
+    const float* __restrict__ t;
+    uint32_t ss;
+    int act;
+};
+
+// Per-ray result of the compositor forward.
+struct CompFwd {
+    float r, g, b, a;
+    float depth;   // optical depth up to and including the last composited sample
+    uint32_t used; // samples composited (reference: loop index at the transmittance break + 1)
+};
+
+// density_to_ray_rgba_forward, src/utils/training-kernels-fused.cuh:227-264, with
+// T_j = exp(-sum_{i<j} sigma_i dt_i) and alpha_j = -expm1(-sigma_j dt_j). Sample j is
+// composited while T_j >= min_t, i.e. up to and including the first sample after which
+// the transmittance drops below min_t.
+__device__ CompFwd composite_forward_ray(const Samples& S, uint32_t o, uint32_t n, float min_t, int lane) {
+    float carry = 0.0f, t_prev = 1.0f;
+    float ar = 0.0f, ag = 0.0f, ab = 0.0f, aa = 0.0f;
+    CompFwd out;
+    out.used = n;
+    out.depth = 0.0f;
+    bool done = false;
+    for (uint32_t base = 0; base < n && !done; base += WARP) {
+        const uint32_t j = base + lane;
+        const bool valid = j < n;
+        float x = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+        if (valid) {
+            const size_t s = (size_t)o + j;
+            x = act_sigma(S.act, S.density[s]) * S.dt[s];
+            cr = S.rgb[s];
+            cg = S.rgb[s + S.ss];
+            cb = S.rgb[s + 2 * (size_t)S.ss];
+        }
+        const float incl = warp_inclusive_sum(x, lane) + carry;
+        const float tn = expf(-incl);
+        const float tj = shift_up(tn, lane, t_prev);
+        const float w = tj * -expm1f(-x);
+        const unsigned term = __ballot_sync(FULL_MASK, valid && tn < min_t);
+        const int first = term ? __ffs(term) - 1 : WARP;
+        if (valid && lane <= first) {
+            ar += w * cr;
+            ag += w * cg;
+            ab += w * cb;
+            aa += w;
+        }
+        if (term) {
+            out.used = base + first + 1;
+            out.depth = __shfl_sync(FULL_MASK, incl, first);
+            done = true;
+        } else {
+            carry = __shfl_sync(FULL_MASK, incl, WARP - 1);
+            t_prev = __shfl_sync(FULL_MASK, tn, WARP - 1);
+        }
+    }
+    if (!done) out.depth = carry;
+    out.r = warp_sum(ar);
+    out.g = warp_sum(ag);
+    out.b = warp_sum(ab);
+    out.a = warp_sum(aa);
+    return out;
+}
+
+// Reverse-scan vector-Jacobian product of the compositor for one ray over samples
+// [0, used): dL/dsigma_j = dt_j * sum_c g_c (T_{j+1} c_j - sum_{i>j} w_i c_i)
+//                        + dt_j * g_a (T_{j+1} - sum_{i>j} w_i);   dL/dc_j = cscale * g_c * w_j.
+// The callback `emit(j, valid, dsigma_density, drgb_r, drgb_g, drgb_b, chunk_base)` consumes
+// each chunk's gradients (dsigma already multiplied by d sigma / d input).
+template <typename Emit>
+__device__ __forceinline__ void composite_vjp_chunk(const Samples& S, uint32_t o, uint32_t used, float depth,
+                                                    float gr, float gg, float gb, float ga, float cscale,
+                                                    uint32_t base, int lane, float& sx, float& sr, float& sg,
+                                                    float& sb, float& sa, Emit&& emit) {
+    const uint32_t j = base + lane;
+    const bool valid = j < used;
+    float x = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f, dtv = 0.0f, sigma = 0.0f;
+    if (valid) {
+        const size_t s = (size_t)o + j;
+        sigma = act_sigma(S.act, S.density[s]);
+        dtv = S.dt[s];
+        x = sigma * dtv;
+        cr = S.rgb[s];
+        cg = S.rgb[s + S.ss];
+        cb = S.rgb[s + 2 * (size_t)S.ss];
+    }
+    const float xs_incl = warp_inclusive_suffix_sum(x, lane) + sx;  // sum_{i>=j} x_i
+    const float xs_excl = shift_down(xs_incl, lane, sx);             // sum_{i>j} x_i
+    const float tj = expf(-fmaxf(depth - xs_incl, 0.0f));
+    const float tn = expf(-fmaxf(depth - xs_excl, 0.0f));
+    const float w = valid ? tj * -expm1f(-x) : 0.0f;
+    const float wr = w * cr, wg = w * cg, wb = w * cb;
+    const float r_incl = warp_inclusive_suffix_sum(wr, lane) + sr;
+    const float g_incl = warp_inclusive_suffix_sum(wg, lane) + sg;
+    const float b_incl = warp_inclusive_suffix_sum(wb, lane) + sb;
+    const float a_incl = warp_inclusive_suffix_sum(w, lane) + sa;
+    const float r_ex = shift_down(r_incl, lane, sr);
+    const float g_ex = shift_down(g_incl, lane, sg);
+    const float b_ex = shift_down(b_incl, lane, sb);
+    const float a_ex = shift_down(a_incl, lane, sa);
+    const float ds = dtv * (gr * (tn * cr - r_ex) + gg * (tn * cg - g_ex) + gb * (tn * cb - b_ex) + ga * (tn - a_ex));
+    emit(j, valid, ds * act_dsigma(S.act, sigma), cscale * gr * w, cscale * gg * w, cscale * gb * w);
+    sx = __shfl_sync(FULL_MASK, xs_incl, 0);
+    sr = __shfl_sync(FULL_MASK, r_incl, 0);
+    sg = __shfl_sync(FULL_MASK, g_incl, 0);
+    sb = __shfl_sync(FULL_MASK, b_incl, 0);
+    sa = __shfl_sync(FULL_MASK, a_incl, 0);
+}
+
+__device__ __forceinline__ void zero_tail(float* __restrict__ dd, float* __restrict__ drgb, uint32_t ss, uint32_t o,
+                                          uint32_t from, uint32_t n, int lane) {
+    for (uint32_t j = from + lane; j < n; j += WARP) {
+        const size_t s = (size_t)o + j;
+        if (dd) dd[s] = 0.0f;
+        if (drgb) {
+            drgb[s] = 0.0f;
+            drgb[s + ss] = 0.0f;
+            drgb[s + 2 * (size_t)ss] = 0.0f;
+        }
+    }
+}
+
+// smooth-L1 (beta 1) helpers, src/utils/training-kernels-fused.cuh:344-356
+__device__ __forceinline__ float huber(float x) { const float a = fabsf(x); return a < 1.0f ? 0.5f * x * x : a - 0.5f; }
+__device__ __forceinline__ float huber_grad(float x) { return fabsf(x) < 1.0f ? x : copysignf(1.0f, x); }
+
+// Reconstruction loss of one ray given its composite (training-kernels-fused.cuh:434-477).
+// Returns the sum of the four channel losses; sets the VJP weights g4 of the compositor.
+struct ReconGrad { float gr, gg, gb, ga; float l[4]; };
+
+__device__ __forceinline__ ReconGrad recon_loss_ray(const CompFwd& c, const float* __restrict__ target,
+                                                   const float* __restrict__ bg, uint32_t r, uint32_t rs,
+                                                   float inv_nrays) {
+    const float gt_r = target[r], gt_g = target[r + rs], gt_b = target[r + 2 * (size_t)rs], gt_a = target[r + 3 * (size_t)rs];
+    const float br = bg[r], bgc = bg[r + rs], bb = bg[r + 2 * (size_t)rs];
+    const float gt_ac = 1.0f - gt_a;
+    const float gtr = gt_r * gt_a + br * gt_ac, gtg = gt_g * gt_a + bgc * gt_ac, gtb = gt_b * gt_a + bb * gt_ac;
+    const float ac = 1.0f - c.a;
+    const float pr = c.r * c.a + br * ac, pg = c.g * c.a + bgc * ac, pb = c.b * c.a + bb * ac;
+    const float dr = pr - gtr, dg = pg - gtg, db = pb - gtb, da = ac - gt_ac;
+    ReconGrad g;
+    g.l[0] = huber(dr); g.l[1] = huber(dg); g.l[2] = huber(db); g.l[3] = huber(da);
+    const float lr = inv_nrays * huber_grad(dr), lg = inv_nrays * huber_grad(dg), lb = inv_nrays * huber_grad(db);
+    // pred'_c = R_c A + bg_c (1 - A): d pred'_c = A dR_c + (R_c - bg_c) dA
+    // (density_to_ray_rgba_backward, training-kernels-fused.cuh:320-322)
+    g.gr = lr * c.a;
+    g.gg = lg * c.a;
+    g.gb = lb * c.a;
+    g.ga = lr * (c.r - br) + lg * (c.g - bgc) + lb * (c.b - bb);
+    return g;
+}
+
+// ---- distortion -------------------------------------------------------------------------
+struct DistCarry { float x, w, wm; };
+
+struct DistChunk {
+    float dtn, m, w, wm, t_next, w_incl, w_excl, wm_incl, wm_excl, sigma;
+    bool valid;
+};
+
+__device__ __forceinline__ DistChunk dist_chunk_forward(const Samples& S, uint32_t o, uint32_t n, uint32_t base,
+                                                        int lane, const DistCarry& c, DistCarry& next) {
+    DistChunk d;
+    const uint32_t j = base + lane;
+    d.valid = j < n;
+    float x = 0.0f;
+    d.dtn = 0.0f; d.m = 0.0f; d.sigma = 0.0f;
+    if (d.valid) {
+        const size_t s = (size_t)o + j;
+        d.sigma = act_sigma(S.act, S.density[s]);
+        d.dtn = S.dt_norm[s];
+        d.m = S.m_norm[s];
+        x = d.sigma * d.dtn;
+    }
+    const float x_incl = warp_inclusive_sum(x, lane) + c.x;
+    const float x_excl = shift_up(x_incl, lane, c.x);
+    const float em = expm1f(-x);
+    const float tj = expf(-x_excl);
+    d.w = d.valid ? tj * -em : 0.0f;
+    d.t_next = tj * (1.0f + em);  // T_j (1 - alpha_j)
+    d.wm = d.w * d.m;
+    d.w_incl = warp_inclusive_sum(d.w, lane) + c.w;
+    d.w_excl = shift_up(d.w_incl, lane, c.w);
+    d.wm_incl = warp_inclusive_sum(d.wm, lane) + c.wm;
+    d.wm_excl = shift_up(d.wm_incl, lane, c.wm);
+    next.x = __shfl_sync(FULL_MASK, x_incl, WARP - 1);
+    next.w = __shfl_sync(FULL_MASK, d.w_incl, WARP - 1);
+    next.wm = __shfl_sync(FULL_MASK, d.wm_incl, WARP - 1);
+    return d;
+}
+
+// Chunk carries of the distortion forward, distributed over lanes: chunk c lives in lane
+// (c % 32), slot c / 32 (two slots).
+struct DistCarryStore {
+    DistCarry s0, s1;
+    __device__ __forceinline__ void put(uint32_t c, int lane, const DistCarry& v) {
+        if ((uint32_t)lane == (c & 31u)) {
+            if (c < 32u) s0 = v; else if (c < 64u) s1 = v;
+        }
+    }
+    __device__ __forceinline__ DistCarry get(uint32_t c) const {
+        const int src = (int)(c & 31u);
+        const DistCarry& s = c < 32u ? s0 : s1;
+        DistCarry v;
+        v.x = __shfl_sync(FULL_MASK, s.x, src);
+        v.w = __shfl_sync(FULL_MASK, s.w, src);
+        v.wm = __shfl_sync(FULL_MASK, s.wm, src);
+        return v;
+    }
+};
+
+struct DistFwd { float loss, k; };
+
+__device__ __forceinline__ DistFwd dist_forward_ray(const Samples& S, uint32_t o, uint32_t n, float lambda, int lane,
+                                                    DistCarryStore& store) {
+    DistCarry c{0.0f, 0.0f, 0.0f};
+    float uni = 0.0f, b0 = 0.0f, b1 = 0.0f;
+    uint32_t ci = 0;
+    for (uint32_t base = 0; base < n; base += WARP, ++ci) {
+        store.put(ci, lane, c);
+        DistCarry nx;
+        const DistChunk d = dist_chunk_forward(S, o, n, base, lane, c, nx);
+        uni += d.dtn * d.w * d.w;
+        b0 += d.wm * d.w_excl;
+        b1 += d.w * d.wm_excl;
+        c = nx;
+    }
+    uni = warp_sum(uni);
+    b0 = warp_sum(b0);
+    b1 = warp_sum(b1);
+    DistFwd f;
+    f.k = n ? lambda / (float)n : 0.0f;
+    f.loss = f.k * ((1.0f / 3.0f) * uni + 2.0f * (b0 - b1));
+    return f;
+}
+
+// Carry at the start of chunk `ci` (>= SAVED_CHUNKS): replay the forward from the last
+// saved chunk.
+__device__ DistCarry dist_replay_carry(const Samples& S, uint32_t o, uint32_t n, uint32_t ci, int lane,
+                                       const DistCarryStore& store) {
+    DistCarry c = store.get(SAVED_CHUNKS - 1);
+    for (uint32_t k = SAVED_CHUNKS - 1; k < ci; ++k) {
+        DistCarry nx;
+        (void)dist_chunk_forward(S, o, n, k * WARP, lane, c, nx);
+        c = nx;
+    }
+    return c;
+}
+
+struct DistSuffix { float wm, wmW, w, wWM, dtw2; };
+
+// mipNeRF360_distortion_loss_backward_kernel gradient (training-kernels-fused.cuh:188-223)
+// for one chunk, with the suffix sums obtained by reverse scans.
+__device__ __forceinline__ float dist_chunk_backward(const DistChunk& d, float k, int lane, DistSuffix& suf) {
+    const float a1 = d.wm, a2 = d.wm * d.w_excl, a3 = d.w, a4 = d.w * d.wm_excl, a5 = d.dtn * d.w * d.w;
+    const float i1 = warp_inclusive_suffix_sum(a1, lane) + suf.wm;
+    const float i2 = warp_inclusive_suffix_sum(a2, lane) + suf.wmW;
+    const float i3 = warp_inclusive_suffix_sum(a3, lane) + suf.w;
+    const float i4 = warp_inclusive_suffix_sum(a4, lane) + suf.wWM;
+    const float i5 = warp_inclusive_suffix_sum(a5, lane) + suf.dtw2;
+    const float s_wm = shift_down(i1, lane, suf.wm);
+    const float s_wmW = shift_down(i2, lane, suf.wmW);
+    const float s_w = shift_down(i3, lane, suf.w);
+    const float s_wWM = shift_down(i4, lane, suf.wWM);
+    const float s_dtw2 = shift_down(i5, lane, suf.dtw2);
+    suf.wm = __shfl_sync(FULL_MASK, i1, 0);
+    suf.wmW = __shfl_sync(FULL_MASK, i2, 0);
+    suf.w = __shfl_sync(FULL_MASK, i3, 0);
+    suf.wWM = __shfl_sync(FULL_MASK, i4, 0);
+    suf.dtw2 = __shfl_sync(FULL_MASK, i5, 0);
+    const float dw = d.dtn * d.t_next;
+    const float dwm = d.m * dw;
+    const float tw = d.t_next;
+    const float db0 = dwm * d.w_excl + d.dtn * (s_wm * (d.w_incl + tw) - 2.0f * s_wmW);
+    const float db1 = dw * d.wm_excl + d.dtn * (s_w * (d.m * tw + d.wm_incl) - 2.0f * s_wWM);
+    const float du = 2.0f * d.dtn * (d.dtn * d.w * tw - s_dtw2);
+    return k * (2.0f * (db0 - db1) + (1.0f / 3.0f) * du);
+}
+
+// ---- block-level deterministic sums (per-block partials, last block adds them) ---------
+// out[k] = scale[k] * (block-summed v[k]), additionally divided by the live ray count
+// *n_dev for the components whose bit is set in dev_mask.
+struct FinishScale {
+    float s[2];
+    const uint32_t* n_dev;
+    uint32_t n_host;
+    uint32_t dev_mask;
+};
+
+template <int NV>
+__device__ void block_sum_and_finish(float (&v)[NV], float* partials, uint32_t* ticket, float* out,
+                                     const FinishScale fs) {
+    __shared__ float red[LOSS_WARPS][NV];
+    __shared__ bool is_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const float s = warp_sum(v[k]);
+        if (lane == 0) red[wid][k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            float s = 0.0f;
+            for (int w = 0; w < LOSS_WARPS; ++w) s += red[w][k];
+            partials[(size_t)blockIdx.x * NV + k] = s;
+        }
+        __threadfence();
+        is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    float acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0f;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += *((volatile float*)(partials + (size_t)b * NV + k));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const float s = warp_sum(acc[k]);
+        if (lane == 0) red[wid][k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t nn = fs.n_dev ? min(*fs.n_dev, fs.n_host) : fs.n_host;
+        const float inv_n = nn ? 1.0f / (float)nn : 0.0f;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            float s = 0.0f;
+            for (int w = 0; w < LOSS_WARPS; ++w) s += red[w][k];
+            s *= fs.s[k];
+            if ((fs.dev_mask >> k) & 1u) s *= inv_n;
+            if (out) out[k] = s;
+        }
+        *ticket = 0u;
+    }
+}
+
+__device__ __forceinline__ uint32_t live_rays(uint32_t n_rays, const uint32_t* n_dev) {
+    return n_dev ? min(*n_dev, n_rays) : n_rays;
+}
+
+// ---- kernels ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(LOSS_THREADS)
+composite_fwd_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
+                     const uint32_t* __restrict__ offsets, float min_t, float* __restrict__ rgba,
+                     float* __restrict__ depth, uint32_t* __restrict__ n_used) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t nw = gridDim.x * LOSS_WARPS;
+    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
+        const CompFwd c = composite_forward_ray(S, offsets[r], counts[r], min_t, lane);
+        if (lane == 0) {
+            rgba[r] = c.r; rgba[r + rs] = c.g; rgba[r + 2 * (size_t)rs] = c.b; rgba[r + 3 * (size_t)rs] = c.a;
+            if (depth) depth[r] = c.depth;
+            if (n_used) n_used[r] = c.used;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(LOSS_THREADS)
+composite_bwd_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
+                     const uint32_t* __restrict__ offsets, const float* __restrict__ depth,
+                     const uint32_t* __restrict__ n_used, const float* __restrict__ grad_rgba,
+                     float* __restrict__ dd, float* __restrict__ drgb) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t nw = gridDim.x * LOSS_WARPS;
+    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
+        const uint32_t o = offsets[r], n = counts[r];
+        const uint32_t used = min(n_used[r], n);
+        const float dep = depth[r];
+        const float gr = grad_rgba[r], gg = grad_rgba[r + rs], gb = grad_rgba[r + 2 * (size_t)rs],
+                    ga = grad_rgba[r + 3 * (size_t)rs];
+        zero_tail(dd, drgb, S.ss, o, used, n, lane);
+        float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
+        if (used == 0) continue;
+        for (int base = (int)(((used - 1) / WARP) * WARP); base >= 0; base -= WARP) {
+            composite_vjp_chunk(S, o, used, dep, gr, gg, gb, ga, 1.0f, (uint32_t)base, lane, sx, sr, sg, sb, sa,
+                                [&](uint32_t j, bool valid, float ds, float xr, float xg, float xb) {
+                                    if (!valid) return;
+                                    const size_t s = (size_t)o + j;
+                                    dd[s] = ds;
+                                    drgb[s] = xr;
+                                    drgb[s + S.ss] = xg;
+                                    drgb[s + 2 * (size_t)S.ss] = xb;
+                                });
+        }
+    }
+}
+
+__global__ void __launch_bounds__(LOSS_THREADS)
+recon_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
+             const uint32_t* __restrict__ offsets, float min_t, float inv_nrays, float grad_scale,
+             const float* __restrict__ target, const float* __restrict__ bg, float* __restrict__ ray_rgba,
+             float* __restrict__ loss, float* loss_sum, float* __restrict__ dd, float* __restrict__ drgb,
+             float* partials, uint32_t* ticket) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t nw = gridDim.x * LOSS_WARPS;
+    float acc[1] = {0.0f};
+    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
+        const uint32_t o = offsets[r], n = counts[r];
+        const CompFwd c = composite_forward_ray(S, o, n, min_t, lane);
+        const ReconGrad g = recon_loss_ray(c, target, bg, r, rs, inv_nrays);
+        if (lane == 0) {
+            if (ray_rgba) {
+                ray_rgba[r] = c.r; ray_rgba[r + rs] = c.g; ray_rgba[r + 2 * (size_t)rs] = c.b;
+                ray_rgba[r + 3 * (size_t)rs] = c.a;
+            }
+            if (loss) {
+                loss[r] = g.l[0]; loss[r + rs] = g.l[1]; loss[r + 2 * (size_t)rs] = g.l[2]; loss[r + 3 * (size_t)rs] = g.l[3];
+            }
+            acc[0] += g.l[0] + g.l[1] + g.l[2] + g.l[3];
+        }
+        zero_tail(dd, drgb, S.ss, o, c.used, n, lane);
+        float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
+        if (c.used == 0) continue;
+        for (int base = (int)(((c.used - 1) / WARP) * WARP); base >= 0; base -= WARP) {
+            composite_vjp_chunk(S, o, c.used, c.depth, g.gr, g.gg, g.gb, g.ga, grad_scale, (uint32_t)base, lane, sx, sr,
+                                sg, sb, sa, [&](uint32_t j, bool valid, float ds, float xr, float xg, float xb) {
+                                    if (!valid) return;
+                                    const size_t s = (size_t)o + j;
+                                    dd[s] = ds;
+                                    drgb[s] = xr;
+                                    drgb[s + S.ss] = xg;
+                                    drgb[s + 2 * (size_t)S.ss] = xb;
+                                });
+        }
+    }
+    if (loss_sum) block_sum_and_finish<1>(acc, partials, ticket, loss_sum, FinishScale{{inv_nrays, 0.0f}, nullptr, 0u, 0u});
+}
+
+__global__ void __launch_bounds__(LOSS_THREADS)
+distortion_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, const uint32_t* __restrict__ counts,
+                  const uint32_t* __restrict__ offsets, float lambda, const float* __restrict__ grad_ray,
+                  float* __restrict__ ray_loss, float* loss_sum, float* __restrict__ dd, float* partials,
+                  uint32_t* ticket) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t nw = gridDim.x * LOSS_WARPS;
+    float acc[1] = {0.0f};
+    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
+        const uint32_t o = offsets[r], n = counts[r];
+        DistCarryStore store;
+        const DistFwd f = dist_forward_ray(S, o, n, lambda, lane, store);
+        if (lane == 0) {
+            if (ray_loss) ray_loss[r] = f.loss;
+            acc[0] += f.loss;
+        }
+        if (!dd || n == 0) continue;
+        const float gscale = grad_ray ? grad_ray[r] : 1.0f;
+        DistSuffix suf{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        const uint32_t nch = (n + WARP - 1) / WARP;
+        for (int ci = (int)nch - 1; ci >= 0; --ci) {
+            const DistCarry c = ci < SAVED_CHUNKS ? store.get((uint32_t)ci)
+                                                  : dist_replay_carry(S, o, n, (uint32_t)ci, lane, store);
+            DistCarry nx;
+            const DistChunk d = dist_chunk_forward(S, o, n, (uint32_t)ci * WARP, lane, c, nx);
+            const float g = dist_chunk_backward(d, f.k, lane, suf);
+            if (d.valid) dd[(size_t)o + (uint32_t)ci * WARP + lane] = gscale * g * act_dsigma(S.act, d.sigma);
+        }
+    }
+    if (loss_sum) block_sum_and_finish<1>(acc, partials, ticket, loss_sum, FinishScale{{1.0f, 0.0f}, n_dev, n_rays, 1u});
+}
+
+// Reconstruction + distortion forward/backward + gradient merge, one warp per ray.
+__global__ void __launch_bounds__(LOSS_THREADS)
+train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
+                    const uint32_t* __restrict__ offsets, float min_t, float inv_nrays_host,
+                    const uint32_t* __restrict__ inv_from, float grad_scale, float lambda,
+                    const float* __restrict__ target, const float* __restrict__ bg, float* __restrict__ ray_rgba,
+                    float* __restrict__ grad_density, float* __restrict__ drgb, float* loss_sums, float* partials,
+                    uint32_t* ticket) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    float inv_nrays = inv_nrays_host;
+    if (inv_from) { const uint32_t nn = *inv_from; inv_nrays = nn ? 1.0f / (float)nn : 0.0f; }
+    const uint32_t nw = gridDim.x * LOSS_WARPS;
+    const bool use_dist = lambda > 0.0f;
+    float acc[2] = {0.0f, 0.0f};
+    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
+        const uint32_t o = offsets[r], n = counts[r];
+        const CompFwd c = composite_forward_ray(S, o, n, min_t, lane);
+        const ReconGrad g = recon_loss_ray(c, target, bg, r, rs, inv_nrays);
+        DistCarryStore store;
+        DistFwd f{0.0f, 0.0f};
+        if (use_dist) f = dist_forward_ray(S, o, n, lambda, lane, store);
+        if (lane == 0) {
+            if (ray_rgba) {
+                ray_rgba[r] = c.r; ray_rgba[r + rs] = c.g; ray_rgba[r + 2 * (size_t)rs] = c.b;
+                ray_rgba[r + 3 * (size_t)rs] = c.a;
+            }
+            acc[0] += g.l[0] + g.l[1] + g.l[2] + g.l[3];
+            acc[1] += f.loss;
+        }
+        if (n == 0) continue;
+        float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
+        DistSuffix suf{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        const uint32_t nch = (n + WARP - 1) / WARP;
+        for (int ci = (int)nch - 1; ci >= 0; --ci) {
+            const uint32_t base = (uint32_t)ci * WARP;
+            const uint32_t j = base + lane;
+            float g_rec = 0.0f, xr = 0.0f, xg = 0.0f, xb = 0.0f;
+            if (base < c.used) {
+                composite_vjp_chunk(S, o, c.used, c.depth, g.gr, g.gg, g.gb, g.ga, grad_scale, base, lane, sx, sr, sg,
+                                    sb, sa, [&](uint32_t, bool valid, float ds, float a, float b, float cc) {
+                                        if (valid) { g_rec = ds; xr = a; xg = b; xb = cc; }
+                                    });
+            }
+            float g_dist = 0.0f;
+            if (use_dist) {
+                const DistCarry cc = ci < SAVED_CHUNKS ? store.get((uint32_t)ci)
+                                                       : dist_replay_carry(S, o, n, (uint32_t)ci, lane, store);
+                DistCarry nx;
+                const DistChunk d = dist_chunk_forward(S, o, n, base, lane, cc, nx);
+                g_dist = dist_chunk_backward(d, f.k, lane, suf) * act_dsigma(S.act, d.sigma);
+            }
+            if (j < n) {
+                const size_t s = (size_t)o + j;
+                // copy_gradients_kernel<1,true> twice + apply_gradient_distance_scaling_kernel
+                // (src/core/nerf-network.cu:734-758); the loss scale is grad_scale.
+                float gd = grad_density[s] + grad_scale * g_rec + grad_scale * g_dist;
+                if (S.t) { const float tt = S.t[s]; if (tt < 1.0f) gd *= tt * tt; }
+                grad_density[s] = gd;
+                drgb[s] = xr;
+                drgb[s + S.ss] = xg;
+                drgb[s + 2 * (size_t)S.ss] = xb;
+            }
+        }
+    }
+    if (loss_sums) {
+        acc[0] *= inv_nrays;
+        block_sum_and_finish<2>(acc, partials, ticket, loss_sums, FinishScale{{1.0f, 1.0f}, n_dev, n_rays, 2u});
+    }
+}
+
+__global__ void grad_epilogue_kernel(uint32_t n, const uint32_t* __restrict__ n_dev, float scale,
+                                     const float* __restrict__ rec, const float* __restrict__ dist,
+                                     const float* __restrict__ t, float* __restrict__ out) {
+    const uint32_t n_live = n_dev ? min(*n_dev, n) : n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_live; i += gridDim.x * blockDim.x) {
+        float g = out[i] + scale * rec[i];
+        if (dist) g += scale * dist[i];
+        if (t) { const float tt = t[i]; if (tt < 1.0f) g *= tt * tt; }
+        out[i] = g;
+    }
+}
+
+// ---- plain path: one thread per ray, reference structure --------------------------------
+__device__ __forceinline__ float plain_sigma(int act, float d) { return act == 0 ? d : __expf(fminf(d, 12.0f) - 1.0f); }
+
+__global__ void plain_recon_kernel(uint32_t n_rays, uint32_t rs, uint32_t ss, int act, float min_t, float inv_nrays,
+                                   float grad_scale, const uint32_t* __restrict__ counts,
+                                   const uint32_t* __restrict__ offsets, const float* __restrict__ bg,
+                                   const float* __restrict__ target, const float* __restrict__ density,
+                                   const float* __restrict__ rgb, const float* __restrict__ dtb,
+                                   float* __restrict__ loss, float* __restrict__ dd, float* __restrict__ drgb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rays) return;
+    const uint32_t o = offsets[i], n = counts[i];
+    const float* sr = rgb + o;
+    const float* sg = rgb + o + ss;
+    const float* sb = rgb + o + 2 * (size_t)ss;
+    const float* sd = density + o;
+    const float* sdt = dtb + o;
+    float r = 0, g = 0, b = 0, a = 0, trans = 1.0f;
+    for (uint32_t k = 0; k < n; ++k) {
+        const float alpha = 1.0f - __expf(-plain_sigma(act, sd[k]) * sdt[k]);
+        const float w = trans * alpha;
+        r += w * sr[k]; g += w * sg[k]; b += w * sb[k]; a += w;
+        trans *= (1.0f - alpha);
+        if (trans < min_t) break;
+    }
+    const float gt_r = target[i], gt_g = target[i + rs], gt_b = target[i + 2 * (size_t)rs], gt_a = target[i + 3 * (size_t)rs];
+    const float br = bg[i], bgc = bg[i + rs], bb = bg[i + 2 * (size_t)rs];
+    const float gac = 1.0f - gt_a;
+    const float gtr = gt_r * gt_a + br * gac, gtg = gt_g * gt_a + bgc * gac, gtb = gt_b * gt_a + bb * gac;
+    const float ac = 1.0f - a;
+    const float pr = r * a + br * ac, pg = g * a + bgc * ac, pb = b * a + bb * ac;
+    const float dr = pr - gtr, dg = pg - gtg, db = pb - gtb, da = ac - gac;
+    loss[i] = huber(dr); loss[i + rs] = huber(dg); loss[i + 2 * (size_t)rs] = huber(db); loss[i + 3 * (size_t)rs] = huber(da);
+    const float lr = inv_nrays * huber_grad(dr), lg = inv_nrays * huber_grad(dg), lb = inv_nrays * huber_grad(db);
+    const float cdr = r - br, cdg = g - bgc, cdb = b - bb;
+    float cr = r, cg = g, cb = b, ca = a;
+    trans = 1.0f;
+    for (uint32_t k = 0; k < n; ++k) {
+        const float sig = plain_sigma(act, sd[k]);
+        const float alpha = 1.0f - __expf(-sig * sdt[k]);
+        const float w = trans * alpha;
+        const float kk = trans - w;
+        cr -= w * sr[k]; cg -= w * sg[k]; cb -= w * sb[k]; ca -= w;
+        float dRr = sdt[k] * (kk * sr[k] - cr), dRg = sdt[k] * (kk * sg[k] - cg), dRb = sdt[k] * (kk * sb[k] - cb);
+        const float dRa = sdt[k] * (kk - ca);
+        dRr = dRr * a + cdr * dRa;
+        dRg = dRg * a + cdg * dRa;
+        dRb = dRb * a + cdb * dRa;
+        dd[o + k] = (lr * dRr + lg * dRg + lb * dRb) * (act == 0 ? 1.0f : sig);
+        const float dRc = w * a;
+        drgb[o + k] = grad_scale * lr * dRc;
+        drgb[o + k + ss] = grad_scale * lg * dRc;
+        drgb[o + k + 2 * (size_t)ss] = grad_scale * lb * dRc;
+        trans *= 1.0f - alpha;
+        if (trans < min_t) break;
+    }
+}
+
+__global__ void plain_dist_fwd_kernel(uint32_t n_rays, uint32_t rs, int act, float lambda,
+                                      const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                                      const float* __restrict__ density, const float* __restrict__ mb,
+                                      const float* __restrict__ dtb, float* __restrict__ ray5,
+                                      float* __restrict__ ray_loss, float* __restrict__ w_cs_b,
+                                      float* __restrict__ wm_cs_b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rays) return;
+    const uint32_t n = counts[i];
+    if (n == 0) {
+        ray_loss[i] = 0.0f;
+        for (int k = 0; k < 5; ++k) ray5[i + k * (size_t)rs] = 0.0f;
+        return;
+    }
+    const uint32_t o = offsets[i];
+    float cw = 0, cwm = 0, cdtw2 = 0, cwmw = 0, cwwm = 0, trans = 1.0f, pw = 0, pwm = 0, b0 = 0, b1 = 0, uni = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const float dt = dtb[o + k];
+        const float alpha = 1.0f - __expf(-plain_sigma(act, density[o + k]) * dt);
+        const float w = alpha * trans;
+        const float m = mb[o + k];
+        const float wm = w * m;
+        const float a0 = wm * pw, a1 = w * pwm, a2 = dt * w * w;
+        cw += w; cwm += wm; cdtw2 += a2; cwmw += a0; cwwm += a1;
+        w_cs_b[o + k] = cw;
+        wm_cs_b[o + k] = cwm;
+        b0 += a0; b1 += a1; uni += a2;
+        pw = cw; pwm = cwm;
+        trans *= (1.0f - alpha);
+    }
+    const float kk = lambda / (float)n;
+    ray_loss[i] = kk * ((1.0f / 3.0f) * uni + 2.0f * (b0 - b1));
+    ray5[i] = cdtw2; ray5[i + rs] = cw; ray5[i + 2 * (size_t)rs] = cwm; ray5[i + 3 * (size_t)rs] = cwmw;
+    ray5[i + 4 * (size_t)rs] = cwwm;
+}
+
+__global__ void plain_dist_bwd_kernel(uint32_t n_rays, uint32_t rs, int act, float lambda,
+                                      const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                                      const float* __restrict__ density, const float* __restrict__ ray5,
+                                      const float* __restrict__ mb, const float* __restrict__ dtb,
+                                      const float* __restrict__ w_cs_b, const float* __restrict__ wm_cs_b,
+                                      float* __restrict__ dd) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rays) return;
+    const uint32_t n = counts[i];
+    if (n == 0) return;
+    const uint32_t o = offsets[i];
+    float cdtw2 = ray5[i], cw = ray5[i + rs], cwm = ray5[i + 2 * (size_t)rs], cwmw = ray5[i + 3 * (size_t)rs],
+          cwwm = ray5[i + 4 * (size_t)rs];
+    float trans = 1.0f, pw = 0.0f, pwm = 0.0f;
+    const float kk = lambda / (float)n;
+    for (uint32_t k = 0; k < n; ++k) {
+        const float dt = dtb[o + k];
+        const float sig = plain_sigma(act, density[o + k]);
+        const float alpha = 1.0f - __expf(-sig * dt);
+        const float T = trans;
+        const float w = alpha * T;
+        const float m = mb[o + k];
+        const float wm = w * m;
+        const float wcs = w_cs_b[o + k], wmcs = wm_cs_b[o + k];
+        const float dw = T * (dt * (1.0f - alpha));
+        const float dwm = m * dw;
+        const float tw = T - w;
+        cw -= w; cwm -= wm; cdtw2 -= dt * w * w; cwmw -= wm * pw; cwwm -= w * pwm;
+        const float db0 = dwm * pw + dt * (cwm * (wcs + tw) - 2.0f * cwmw);
+        const float db1 = dw * pwm + dt * (cw * (m * tw + wmcs) - 2.0f * cwwm);
+        const float du = 2.0f * dt * (dt * w * tw - cdtw2);
+        dd[o + k] = kk * (2.0f * (db0 - db1) + (1.0f / 3.0f) * du) * (act == 0 ? 1.0f : sig);
+        pw = wcs; pwm = wmcs;
+        trans *= (1.0f - alpha);
+    }
+}
+
+__global__ void plain_copy_gradients_kernel(uint32_t n, float scale, const float* __restrict__ in, float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = scale * in[i] + out[i];
+}
+
+__global__ void plain_distance_scaling_kernel(uint32_t n, const float* __restrict__ t, float* __restrict__ g) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float tt = t[i];
+    if (tt >= 1.0f) return;
+    g[i] *= tt * tt;
+}
+
+static int loss_grid(const void* kernel, uint32_t n_rays) {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, LOSS_THREADS, 0);
+        if (per_sm <= 0) per_sm = 1;
+    }
+    const uint32_t want = (n_rays + LOSS_WARPS - 1) / LOSS_WARPS;
+    const uint32_t cap = (uint32_t)(num_sms() * per_sm);
+    return (int)max(1u, min(want, cap));
+}
+
+static int check_batch(const tn_ray_batch* b) {
+    TN_REQUIRE(b != nullptr, TN_E_NULL, "ray batch is NULL");
+    TN_NONNULL(b->counts);
+    TN_NONNULL(b->offsets);
+    TN_REQUIRE(b->ray_stride >= b->n_rays, TN_E_INVALID, "ray_stride %u < n_rays %u", b->ray_stride, b->n_rays);
+    return TN_OK;
+}
+
+}  // namespace tn
+
+using namespace tn;
+
+extern "C" {
+
+int tn_composite_fwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                     float min_transmittance, const float* density, const float* rgb, const float* dt,
+                     float* rgba, float* depth, uint32_t* n_used) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(rgba);
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
+    const int grid = loss_grid((const void*)composite_fwd_kernel, batch->n_rays);
+    composite_fwd_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
+                                                            batch->counts, batch->offsets, min_transmittance, rgba,
+                                                            depth, n_used);
+    return check_launch("tn_composite_fwd");
+}
+
+int tn_composite_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                     const float* density, const float* rgb, const float* dt, const float* depth,
+                     const uint32_t* n_used, const float* grad_rgba, float* dL_ddensity, float* dL_drgb) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(depth); TN_NONNULL(n_used);
+    TN_NONNULL(grad_rgba); TN_NONNULL(dL_ddensity); TN_NONNULL(dL_drgb);
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
+    const int grid = loss_grid((const void*)composite_bwd_kernel, batch->n_rays);
+    composite_bwd_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
+                                                            batch->counts, batch->offsets, depth, n_used, grad_rgba,
+                                                            dL_ddensity, dL_drgb);
+    return check_launch("tn_composite_bwd");
+}
+
+int tn_recon_loss_fwd_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                          float min_transmittance, float inv_nrays, float grad_scale, const float* density,
+                          const float* rgb, const float* dt, const float* target_rgba, const float* bg_rgb,
+                          float* ray_rgba, float* loss, float* loss_sum, float* dL_ddensity, float* dL_drgb) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
+    TN_NONNULL(dL_ddensity); TN_NONNULL(dL_drgb);
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
+    const int grid = loss_grid((const void*)recon_kernel, batch->n_rays);
+    st = ensure_block_f32(ctx, (size_t)grid * 2);
+    if (st != TN_OK) return st;
+    recon_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, batch->counts,
+                                                    batch->offsets, min_transmittance, inv_nrays, grad_scale,
+                                                    target_rgba, bg_rgb, ray_rgba, loss, loss_sum, dL_ddensity,
+                                                    dL_drgb, ctx->block_f32, ctx->tickets + TICKET_RECON);
+    return check_launch("tn_recon_loss_fwd_bwd");
+}
+
+int tn_distortion_fwd_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation, float lambda,
+                          const float* density, const float* m_norm, const float* dt_norm, const float* grad_ray,
+                          float* ray_loss, float* loss_sum, float* dL_ddensity) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(m_norm); TN_NONNULL(dt_norm);
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, nullptr, nullptr, m_norm, dt_norm, nullptr, batch->sample_stride, activation};
+    const int grid = loss_grid((const void*)distortion_kernel, batch->n_rays);
+    st = ensure_block_f32(ctx, (size_t)grid * 2);
+    if (st != TN_OK) return st;
+    distortion_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->counts,
+                                                         batch->offsets, lambda, grad_ray, ray_loss, loss_sum,
+                                                         dL_ddensity, ctx->block_f32, ctx->tickets + TICKET_DIST);
+    return check_launch("tn_distortion_fwd_bwd");
+}
+
+int tn_grad_epilogue(tn_stream_t stream, uint32_t n_samples, const uint32_t* n_samples_dev, float loss_scale,
+                     const float* dL_rec, const float* dL_dist, const float* t, float* grad_out) {
+    TN_NONNULL(dL_rec); TN_NONNULL(grad_out);
+    if (n_samples == 0) return TN_OK;
+    const int grid = (int)min((n_samples + 255u) / 256u, (uint32_t)num_sms() * 8u);
+    grad_epilogue_kernel<<<grid, 256, 0, stream>>>(n_samples, n_samples_dev, loss_scale, dL_rec, dL_dist, t, grad_out);
+    return check_launch("tn_grad_epilogue");
+}
+
+int tn_train_losses(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                    float min_transmittance, float inv_nrays, const uint32_t* inv_nrays_from_dev, float grad_scale,
+                    float lambda, const float* density, const float* rgb, const float* dt, const float* m_norm,
+                    const float* dt_norm, const float* t, const float* target_rgba, const float* bg_rgb,
+                    float* ray_rgba, float* grad_density, float* dL_drgb, float* loss_sums) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
+    TN_NONNULL(grad_density); TN_NONNULL(dL_drgb);
+    if (lambda > 0.0f) { TN_NONNULL(m_norm); TN_NONNULL(dt_norm); }
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, rgb, dt, m_norm, dt_norm, t, batch->sample_stride, activation};
+    const int grid = loss_grid((const void*)train_losses_kernel, batch->n_rays);
+    st = ensure_block_f32(ctx, (size_t)grid * 2);
+    if (st != TN_OK) return st;
+    train_losses_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
+                                                           batch->counts, batch->offsets, min_transmittance, inv_nrays,
+                                                           inv_nrays_from_dev, grad_scale, lambda, target_rgba, bg_rgb,
+                                                           ray_rgba, grad_density, dL_drgb, loss_sums, ctx->block_f32,
+                                                           ctx->tickets + TICKET_TRAIN);
+    return check_launch("tn_train_losses");
+}
+
+// fused_reconstruction_loss_forward_backward launch structure (src/core/nerf-network.cu:547-602):
+// two memsets, one thread per ray, thrust::reduce of the 4 x n_rays losses, blocking read.
+int tn_plain_recon_loss_sync(tn_stream_t stream, const tn_ray_batch* batch, int activation, float min_transmittance,
+                             float inv_nrays, float grad_scale, const float* density, const float* rgb, const float* dt,
+                             const float* target_rgba, const float* bg_rgb, float* loss, float* dL_ddensity,
+                             float* dL_drgb, float* loss_out) {
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
+    TN_NONNULL(loss); TN_NONNULL(dL_ddensity); TN_NONNULL(dL_drgb); TN_NONNULL(loss_out);
+    TN_REQUIRE(batch->n_rays_dev == nullptr, TN_E_INVALID, "plain path takes a host ray count");
+    const uint32_t n = batch->n_rays, rs = batch->ray_stride, ss = batch->sample_stride;
+    st = cuda_status(cudaMemsetAsync(dL_ddensity, 0, (size_t)ss * sizeof(float), stream), "plain recon memset");
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(dL_drgb, 0, 3 * (size_t)ss * sizeof(float), stream), "plain recon memset");
+    if (st != TN_OK) return st;
+    if (n == 0) { *loss_out = 0.0f; return TN_OK; }
+    plain_recon_kernel<<<(n + 127) / 128, 128, 0, stream>>>(n, rs, ss, activation, min_transmittance, inv_nrays,
+                                                            grad_scale, batch->counts, batch->offsets, bg_rgb,
+                                                            target_rgba, density, rgb, dt, loss, dL_ddensity, dL_drgb);
+    st = check_launch("tn_plain_recon_loss_sync");
+    if (st != TN_OK) return st;
+    float total = 0.0f;
+    for (int c = 0; c < 4; ++c) {
+        thrust::device_ptr<float> p(loss + (size_t)c * rs);
+        total += thrust::reduce(thrust::cuda::par.on(stream), p, p + n, 0.0f, thrust::plus<float>());
+    }
+    *loss_out = inv_nrays * total;
+    return TN_OK;
+}
+
+// mipNeRF360_distortion_loss_forward_backward launch structure (src/core/nerf-network.cu:605-666).
+int tn_plain_distortion_sync(tn_stream_t stream, const tn_ray_batch* batch, int activation, float lambda,
+                             const float* density, const float* m_norm, const float* dt_norm, float* ray_scratch,
+                             float* sample_scratch, float* ray_loss, float* dL_ddensity, float* loss_out) {
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(m_norm); TN_NONNULL(dt_norm); TN_NONNULL(ray_scratch); TN_NONNULL(sample_scratch);
+    TN_NONNULL(ray_loss); TN_NONNULL(dL_ddensity); TN_NONNULL(loss_out);
+    TN_REQUIRE(batch->n_rays_dev == nullptr, TN_E_INVALID, "plain path takes a host ray count");
+    const uint32_t n = batch->n_rays, rs = batch->ray_stride, ss = batch->sample_stride;
+    st = cuda_status(cudaMemsetAsync(dL_ddensity, 0, (size_t)ss * sizeof(float), stream), "plain distortion memset");
+    if (st != TN_OK) return st;
+    if (n == 0) { *loss_out = 0.0f; return TN_OK; }
+    const uint32_t nb = (n + 127) / 128;
+    plain_dist_fwd_kernel<<<nb, 128, 0, stream>>>(n, rs, activation, lambda, batch->counts, batch->offsets, density,
+                                                  m_norm, dt_norm, ray_scratch, ray_loss, sample_scratch,
+                                                  sample_scratch + ss);
+    plain_dist_bwd_kernel<<<nb, 128, 0, stream>>>(n, rs, activation, lambda, batch->counts, batch->offsets, density,
+                                                  ray_scratch, m_norm, dt_norm, sample_scratch, sample_scratch + ss,
+                                                  dL_ddensity);
+    st = check_launch("tn_plain_distortion_sync");
+    if (st != TN_OK) return st;
+    thrust::device_ptr<float> p(ray_loss);
+    const float total = thrust::reduce(thrust::cuda::par.on(stream), p, p + n, 0.0f, thrust::plus<float>());
+    *loss_out = (1.0f / (float)n) * total;
+    return TN_OK;
+}
+
+int tn_plain_grad_epilogue(tn_stream_t stream, uint32_t n_samples, float loss_scale, const float* dL_rec,
+                           const float* dL_dist, const float* t, float* grad_out) {
+    TN_NONNULL(dL_rec); TN_NONNULL(grad_out);
+    if (n_samples == 0) return TN_OK;
+    const uint32_t nb = (n_samples + 127) / 128;
+    plain_copy_gradients_kernel<<<nb, 128, 0, stream>>>(n_samples, loss_scale, dL_rec, grad_out);
+    if (dL_dist) plain_copy_gradients_kernel<<<nb, 128, 0, stream>>>(n_samples, loss_scale, dL_dist, grad_out);
+    if (t) plain_distance_scaling_kernel<<<nb, 128, 0, stream>>>(n_samples, t, grad_out);
+    return check_launch("tn_plain_grad_epilogue");
+}
+
+}  // extern "C"

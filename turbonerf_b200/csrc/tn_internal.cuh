@@ -1,0 +1,96 @@
+// Host-side internals shared by the library's translation units: the context, error
+// reporting and argument checks.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "tn_common.cuh"
+
+struct tn_ctx {
+    int device = 0;
+    uint32_t* flags = nullptr;          // device error word (TN_FLAG_*)
+    uint32_t* tickets = nullptr;        // [16] last-block counters, always left at zero
+    uint32_t* block_u32 = nullptr;      // per-block u32 aggregates / prefixes
+    size_t block_u32_cap = 0;
+    float* block_f32 = nullptr;         // per-block float partials
+    size_t block_f32_cap = 0;
+};
+
+namespace tn {
+
+enum Ticket : int {
+    TICKET_MARCH = 0,
+    TICKET_SCAN = 1,
+    TICKET_RECON = 2,
+    TICKET_DIST = 3,
+    TICKET_TRAIN = 4,
+    TICKET_POPCOUNT = 5,
+    TICKET_COMPACT = 6,
+    TICKET_COUNT = 16,
+};
+
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* what);
+int check_launch(const char* what);
+int ensure_block_u32(tn_ctx* ctx, size_t n);
+int ensure_block_f32(tn_ctx* ctx, size_t n);
+bool stream_capturing(cudaStream_t s);
+int num_sms();
+
+inline GridView make_grid_view(const tn_grid_desc& d, const uint8_t* bits) {
+    GridView g;
+    g.n_levels = d.n_levels;
+    g.res = d.resolution;
+    g.res_f = (float)d.resolution;
+    g.inv_res = 1.0f / g.res_f;
+    g.base = d.base_size;
+    g.bits = bits;
+    return g;
+}
+
+int validate_grid(const tn_grid_desc* grid);
+
+// Internal launchers (device-side parameters for graph replays).
+int launch_adam(cudaStream_t stream, bool plain, uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_scale,
+                float lr, const float* lr_dev, float beta1, float beta2, float epsilon, float l2_reg, float* weights,
+                float* weights_copy, const float* gradients, float* first_moments, float* second_moments,
+                uint32_t* param_steps);
+int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc* grid, float* density,
+                            uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
+                            const float* values, const float* rand_select, int activation, int sample_all,
+                            const uint32_t* sample_all_dev, const uint32_t* n_dev, float decay, float threshold,
+                            uint32_t* n_occupied_dev);
+int launch_occupancy_scatter(cudaStream_t stream, const tn_grid_desc* grid, float* density, const uint8_t* bitfield,
+                             uint32_t n_updates, const int32_t* levels, const uint32_t* cells, const float* values,
+                             const float* rand_select, int activation, int sample_all, float decay);
+int launch_occupancy_sweep(cudaStream_t stream, const tn_grid_desc* grid, float* density, uint8_t* bitfield,
+                           float decay, float threshold, uint32_t* n_occupied_dev);
+int launch_plain_occ_decay(cudaStream_t stream, const tn_grid_desc* grid, float* density, float decay);
+int launch_plain_occ_update(cudaStream_t stream, const tn_grid_desc* grid, float* density, const uint8_t* bitfield,
+                            uint32_t n_updates, const int32_t* levels, const uint32_t* cells, const float* values,
+                            const float* rand_select, int activation, int sample_all);
+int launch_plain_occ_bits_sync(cudaStream_t stream, const tn_grid_desc* grid, const float* density, uint8_t* bitfield,
+                               float threshold, uint8_t* count_scratch, uint32_t* n_occupied_out);
+int launch_synth_rays(cudaStream_t stream, uint32_t n, uint32_t rs, uint32_t seed, const uint32_t* step_dev,
+                      float radius, float jitter, const tn_bbox& b, float t_far, float* ori, float* dir, float* target,
+                      float* bg, float* ray_t, float* ray_t_max, uint8_t* alive);
+int launch_synth_cells(cudaStream_t stream, uint32_t n, uint32_t seed, const uint32_t* step_dev, int n_levels,
+                       uint32_t volume, int32_t* levels, uint32_t* cells, float* rand3, uint32_t rand_stride,
+                       float* rand_sel);
+int launch_synth_level_cells(cudaStream_t stream, uint32_t n, uint32_t start, int level, uint32_t seed, uint32_t salt,
+                             int32_t* levels, uint32_t* cells, float* rand3, uint32_t rand_stride, float* rand_sel);
+int launch_synth_hash_grads(cudaStream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t ps, const float* pos,
+                            int n_levels, uint32_t log2_table, int n_features, float base_res, float per_level_scale,
+                            uint32_t seed, float std, float* grads);
+int launch_synth_params(cudaStream_t stream, uint32_t n, uint32_t n_grid, uint32_t seed, float* w);
+
+}  // namespace tn
+
+#define TN_REQUIRE(cond, code, ...) \
+    do { if (!(cond)) return tn::fail((code), __VA_ARGS__); } while (0)
+#define TN_NONNULL(p) TN_REQUIRE((p) != nullptr, TN_E_NULL, "%s: %s is NULL", __func__, #p)

@@ -1,0 +1,711 @@
+// Training-step controller (reference NeRFTrainingController + Trainer,
+// src/controllers/nerf-training-controller.cu:27-226, src/core/trainer.cu:39-349).
+//
+// One step = rays -> march count + device batch cut -> march emit -> network forward ->
+// reconstruction + distortion losses with the gradient merge -> network backward ->
+// [occupancy re-sampling of random cells] -> Adam.
+//
+// Fused path: every stage is one of the library's fused kernels; every step-dependent
+// scalar (step index, learning rate, occupancy selection policy, ray and sample counts)
+// lives in device memory, so the whole step is captured once into a CUDA graph and
+// replayed without any host synchronisation.
+// Plain path: the reference's launch structure (thrust scans, blocking device->host reads of
+// the sample count and the losses, separate memsets and epilogue kernels, dense Adam).
+#include <cstring>
+#include <vector>
+
+#include "tn_internal.cuh"
+
+namespace tn {
+
+struct StepState {
+    unsigned long long samples_total;  // samples processed by all steps so far
+    unsigned long long rays_total;     // rays used by all steps so far
+    uint32_t step_count;   // completed steps
+    uint32_t cur_step;     // index of the running step
+    float lr;              // decayed learning rate of the running step
+    uint32_t sample_all;   // occupancy selection policy: 1 while cur_step < 256
+    uint32_t batch_info[4];
+    uint32_t n_occupied;
+    float loss_sums[2];
+    uint32_t pad;
+};
+
+__global__ void step_end_kernel(StepState* s) {
+    s->samples_total += s->batch_info[1];
+    s->rays_total += s->batch_info[0];
+}
+
+__global__ void step_begin_kernel(StepState* s, float base_lr, float lr_decay) {
+    const uint32_t k = s->step_count;
+    s->cur_step = k;
+    s->lr = base_lr / (1.0f + lr_decay * (float)k);
+    s->sample_all = k < 256u ? 1u : 0u;
+    s->step_count = k + 1u;
+}
+
+// Built-in synthetic network: blob field forward, fixed gradients backward.
+struct SynthNet {
+    float* blobs = nullptr;
+    float* waves = nullptr;
+    uint32_t n_blobs = 0;
+    float aabb = 1.0f;
+};
+
+static int synth_forward(void* user, tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t stride,
+                         const float* pos, const float*, float* density, float* rgb) {
+    SynthNet* s = static_cast<SynthNet*>(user);
+    if (!s->blobs) return fail(TN_E_STATE, "synthetic network has no field (call tn_trainer_set_synthetic_field)");
+    return tn_synth_field(stream, n, n_dev, stride, pos, s->aabb, s->n_blobs, s->blobs, s->waves, density, rgb, stride);
+}
+
+static int synth_density(void* user, tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t stride,
+                         const float* pos, float* density) {
+    SynthNet* s = static_cast<SynthNet*>(user);
+    if (!s->blobs) return fail(TN_E_STATE, "synthetic network has no field (call tn_trainer_set_synthetic_field)");
+    return tn_synth_field(stream, n, n_dev, stride, pos, s->aabb, s->n_blobs, s->blobs, s->waves, density, nullptr,
+                          stride);
+}
+
+}  // namespace tn
+
+using namespace tn;
+
+struct tn_trainer {
+    tn_trainer_desc d{};
+    tn_network net{};
+    SynthNet synth;
+    cudaStream_t stream = nullptr;
+    tn_ctx* ctx = nullptr;
+    std::vector<void*> allocs;
+    uint32_t R = 0, B = 0, V = 0, P = 0, M = 0, chunk = 0;
+    float aabb = 1.0f;
+    // rays
+    float *ori, *dir, *ray_t, *ray_tmax, *target, *bg;
+    uint8_t* alive;
+    uint32_t *n_steps, *offsets;
+    // samples
+    float *s_t, *s_pos, *s_dir, *s_dt, *s_mnorm, *s_dtnorm;
+    float *net_density, *net_rgb, *grad_density, *dl_drgb;
+    // plain-path scratch
+    float *loss4, *dl_rec, *dl_dist, *ray5, *sample2, *ray_loss;
+    uint8_t* count_scratch;
+    // grid
+    float* density;
+    uint8_t* bits;
+    // occupancy re-sampling
+    int32_t* occ_levels;
+    uint32_t* occ_cells;
+    float *occ_rand3, *occ_rsel, *occ_pos, *occ_values;
+    // params
+    float *w, *g, *m, *v;
+    uint32_t* steps;
+    // step state
+    StepState* state = nullptr;
+    StepState* state_host = nullptr;  // pinned
+    cudaGraph_t graph[2] = {nullptr, nullptr};           // [synthetic rays, caller rays]
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    uint32_t graph_kernels[2] = {0, 0};
+    uint32_t graph_nodes[2] = {0, 0};
+    uint32_t fused_steps_enqueued = 0;
+    uint32_t host_step = 0;
+    tn_training_metrics last{};
+
+    template <typename T>
+    int alloc(T*& p, size_t n) {
+        p = nullptr;
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        if (e != cudaSuccess) return fail(TN_E_CUDA, "tn_trainer: cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
+        allocs.push_back(p);
+        return cudaMemsetAsync(p, 0, n * sizeof(T), stream) == cudaSuccess ? TN_OK : fail(TN_E_CUDA, "memset");
+    }
+
+    tn_grid_desc grid() const { return d.grid; }
+    // dt_max = aabb_size * dt_min (reference src/core/trainer.cu:102-104)
+    tn_march_desc march() const {
+        tn_march_desc m{d.cone_angle, d.min_step_size, aabb * d.min_step_size, d.max_steps_per_ray, 0};
+        return m;
+    }
+};
+
+namespace {
+
+// Stage boundaries of one fused step (for per-stage timing with events).
+enum Stage : int { ST_RAYS = 0, ST_COUNT, ST_EMIT, ST_FORWARD, ST_LOSSES, ST_BACKWARD, ST_OCCUPANCY, ST_ADAM, ST_N };
+
+int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
+    const tn_trainer_desc& d = tr->d;
+    cudaStream_t s = tr->stream;
+    const tn_grid_desc grid = tr->grid();
+    const tn_march_desc march = tr->march();
+    auto mark = [&](int k) { if (ev) cudaEventRecord(ev[k + 1], s); };
+    if (ev) cudaEventRecord(ev[0], s);
+    step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
+    int st = check_launch("step_begin");
+    if (st == TN_OK) {
+        if (external_rays)
+            st = tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax,
+                                   tr->alive);
+        else
+            st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
+                                   3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+    }
+    mark(ST_RAYS);
+    uint32_t* info = tr->state->batch_info;
+    if (st == TN_OK)
+        st = tn_march_count(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, tr->ori, tr->dir,
+                            tr->ray_t, tr->ray_tmax, tr->alive, tr->n_steps, tr->B, info);
+    mark(ST_COUNT);
+    if (st == TN_OK)
+        st = tn_march_emit(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B, info,
+                           nullptr, tr->ori, tr->dir, tr->ray_t, tr->alive, tr->n_steps, tr->offsets, nullptr, tr->s_t,
+                           tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
+    mark(ST_EMIT);
+    if (st == TN_OK)
+        st = tr->net.forward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
+                             tr->net_rgb);
+    mark(ST_FORWARD);
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->grad_density, 0, (size_t)tr->B * 4, s), "grad memset");
+    tn_ray_batch rb{tr->R, tr->R, tr->B, 0, tr->n_steps, tr->offsets, info};
+    if (st == TN_OK)
+        st = tn_train_losses(tr->ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, info, d.loss_scale,
+                             d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb,
+                             tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, tr->target, tr->bg, nullptr,
+                             tr->grad_density, tr->dl_drgb, tr->state->loss_sums);
+    mark(ST_LOSSES);
+    if (st == TN_OK && tr->net.backward)
+        st = tr->net.backward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->grad_density,
+                              tr->dl_drgb, tr->g);
+    mark(ST_BACKWARD);
+    if (st == TN_OK && tr->M > 0) {
+        st = launch_synth_cells(s, tr->M, d.seed, &tr->state->cur_step, grid.n_levels, tr->V, tr->occ_levels,
+                                tr->occ_cells, tr->occ_rand3, tr->M, tr->occ_rsel);
+        if (st == TN_OK)
+            st = tn_occupancy_sample_points(s, &grid, tr->M, tr->occ_levels, tr->occ_cells, tr->occ_rand3, tr->M,
+                                            1.0f / tr->aabb, tr->occ_pos, tr->M);
+        if (st == TN_OK) st = tr->net.density(tr->net.user, s, tr->M, nullptr, tr->M, tr->occ_pos, tr->occ_values);
+        if (st == TN_OK)
+            st = launch_occupancy_update(tr->ctx, s, &grid, tr->density, tr->bits, tr->M, tr->occ_levels, tr->occ_cells,
+                                         tr->occ_values, tr->occ_rsel, tr->net.activation, 0, &tr->state->sample_all,
+                                         nullptr, d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied);
+    }
+    mark(ST_OCCUPANCY);
+    if (st == TN_OK)
+        st = launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate,
+                         &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
+                         tr->steps);
+    if (st == TN_OK) {
+        step_end_kernel<<<1, 1, 0, s>>>(tr->state);
+        st = check_launch("step_end");
+    }
+    mark(ST_ADAM);
+    return st;
+}
+
+int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out) {
+    const tn_trainer_desc& d = tr->d;
+    cudaStream_t s = tr->stream;
+    const tn_grid_desc grid = tr->grid();
+    const tn_march_desc march = tr->march();
+    const uint32_t k = tr->host_step;
+    const float lr = d.learning_rate / (1.0f + d.learning_rate_decay * (float)k);
+    step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
+    int st = check_launch("step_begin");
+    if (st == TN_OK) {
+        if (external_rays)
+            st = tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax,
+                                   tr->alive);
+        else
+            st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
+                                   3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+    }
+    if (st == TN_OK)
+        st = tn_plain_march_count(s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, tr->ori, tr->dir, tr->ray_t,
+                                  tr->ray_tmax, tr->alive, tr->n_steps);
+    uint32_t nr = 0, ns = 0;
+    if (st == TN_OK) st = tn_plain_scan_cut_sync(s, tr->R, tr->n_steps, tr->offsets, tr->B, &nr, &ns);
+    if (st == TN_OK)
+        st = tn_plain_march_emit(s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, nr, tr->R, tr->B, nullptr,
+                                 tr->ori, tr->dir, tr->ray_t, tr->offsets, tr->alive, tr->n_steps, nullptr, tr->s_t,
+                                 tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
+    if (st == TN_OK)
+        st = tr->net.forward(tr->net.user, s, ns, nullptr, tr->B, tr->s_pos, tr->s_dir, tr->net_density, tr->net_rgb);
+    tn_ray_batch rb{nr, tr->R, tr->B, 0, tr->n_steps, tr->offsets, nullptr};
+    float rec = 0.0f, dist = 0.0f;
+    if (st == TN_OK)
+        st = tn_plain_recon_loss_sync(s, &rb, tr->net.activation, d.min_transmittance, 1.0f / (float)nr, d.loss_scale,
+                                      tr->net_density, tr->net_rgb, tr->s_dt, tr->target, tr->bg, tr->loss4,
+                                      tr->dl_rec, tr->dl_drgb, &rec);
+    if (st == TN_OK && d.use_distortion_loss)
+        st = tn_plain_distortion_sync(s, &rb, tr->net.activation, d.distortion_lambda, tr->net_density, tr->s_mnorm,
+                                      tr->s_dtnorm, tr->ray5, tr->sample2, tr->ray_loss, tr->dl_dist, &dist);
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->grad_density, 0, (size_t)tr->B * 4, s), "grad memset");
+    if (st == TN_OK)
+        st = tn_plain_grad_epilogue(s, ns, d.loss_scale, tr->dl_rec, d.use_distortion_loss ? tr->dl_dist : nullptr,
+                                    tr->s_t, tr->grad_density);
+    if (st == TN_OK && tr->net.backward)
+        st = tr->net.backward(tr->net.user, s, ns, nullptr, tr->B, tr->s_pos, tr->s_dir, tr->grad_density, tr->dl_drgb,
+                              tr->g);
+    if (st == TN_OK && tr->M > 0) {
+        st = launch_synth_cells(s, tr->M, d.seed, &tr->state->cur_step, grid.n_levels, tr->V, tr->occ_levels,
+                                tr->occ_cells, tr->occ_rand3, tr->M, tr->occ_rsel);
+        if (st == TN_OK)
+            st = tn_occupancy_sample_points(s, &grid, tr->M, tr->occ_levels, tr->occ_cells, tr->occ_rand3, tr->M,
+                                            1.0f / tr->aabb, tr->occ_pos, tr->M);
+        if (st == TN_OK) st = tr->net.density(tr->net.user, s, tr->M, nullptr, tr->M, tr->occ_pos, tr->occ_values);
+        uint32_t nocc = 0;
+        if (st == TN_OK)
+            st = tn_plain_occupancy_update_sync(s, &grid, tr->density, tr->bits, tr->M, tr->occ_levels, tr->occ_cells,
+                                                tr->occ_values, tr->occ_rsel, tr->net.activation, k < 256 ? 1 : 0,
+                                                d.occupancy_decay, d.occupancy_threshold, tr->count_scratch, &nocc);
+    }
+    if (st == TN_OK)
+        st = launch_adam(s, true, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, lr, nullptr, d.beta1, d.beta2,
+                         d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v, tr->steps);
+    if (st == TN_OK) {
+        uint32_t info[2] = {nr, ns};
+        st = cuda_status(cudaMemcpyAsync(tr->state->batch_info, info, sizeof(info), cudaMemcpyHostToDevice, s),
+                         "batch info");
+        if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "plain info sync");
+        if (st == TN_OK) {
+            step_end_kernel<<<1, 1, 0, s>>>(tr->state);
+            st = check_launch("step_end");
+        }
+    }
+    if (st != TN_OK) return st;
+    tr->host_step = k + 1;
+    tr->last.step = k + 1;
+    tr->last.n_rays = nr;
+    tr->last.n_samples = ns;
+    tr->last.loss = rec + dist;
+    if (out) {
+        st = cuda_status(cudaStreamSynchronize(s), "plain step sync");
+        *out = tr->last;
+    }
+    return st;
+}
+
+int read_state(tn_trainer* tr, tn_training_metrics* out) {
+    int st = cuda_status(cudaMemcpyAsync(tr->state_host, tr->state, sizeof(StepState), cudaMemcpyDeviceToHost, tr->stream),
+                         "state read");
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "state sync");
+    if (st != TN_OK) return st;
+    uint32_t flags = 0;
+    st = tn_ctx_check(tr->ctx, tr->stream, &flags);
+    if (st != TN_OK) return st;
+    if (flags & TN_FLAG_NO_RAYS) return fail(TN_E_NO_RAYS, "No rays were generated for this training batch");
+    if (flags & TN_FLAG_NO_SAMPLES) return fail(TN_E_NO_SAMPLES, "No samples were generated for this training batch");
+    if (flags) return fail(TN_E_DEVICE, "device error flags 0x%x", flags);
+    const StepState& h = *tr->state_host;
+    tr->last.step = h.step_count;
+    tr->last.n_rays = h.batch_info[0];
+    tr->last.n_samples = h.batch_info[1];
+    tr->last.loss = h.loss_sums[0] + h.loss_sums[1];
+    if (out) *out = tr->last;
+    return TN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tn_trainer_default_desc(tn_trainer_desc* o) {
+    TN_NONNULL(o);
+    std::memset(o, 0, sizeof(*o));
+    o->grid = tn_grid_desc{1, 128, 1.0f, 0};
+    o->bbox = tn_bbox{-0.5f, -0.5f, -0.5f, 0.5f, 0.5f, 0.5f};
+    o->batch_size = 2u << 21;            // NeRFConstants::batch_size
+    o->n_rays_per_step = 1u << 14;
+    o->min_step_size = 0.00169145586f;   // NeRFConstants::min_step_size
+    o->cone_angle = 1.0f / 256.0f;       // NeRFConstants::cone_angle
+    o->max_steps_per_ray = 0;
+    o->min_transmittance = 1e-4f;        // NeRFConstants::min_transmittance
+    o->use_distortion_loss = 0;
+    o->distortion_lambda = 0.01f;        // NeRFConstants::mipNeRF360_distortion_loss_lambda
+    o->loss_scale = 1.0f;
+    o->occupancy_decay = 0.95f;          // NeRFConstants::occupancy_decay
+    o->occupancy_threshold = 0.01f * 0.00169145586f;  // NeRFConstants::occupancy_threshold
+    o->occupancy_cells_per_step = 0;
+    o->n_grid_params = 16u * (1u << 19) * 2u;
+    o->n_mlp_params = 7168;
+    o->learning_rate = 1e-2f;            // nerf-network.cu:173-178
+    o->learning_rate_decay = 3.3e-5f;    // NeRFConstants::learning_rate_decay
+    o->beta1 = 0.9f;
+    o->beta2 = 0.999f;                   // adam-optimizer.cuh:240
+    o->epsilon = 1e-15f;
+    o->l2_reg = 1e-6f;
+    o->path = TN_PATH_FUSED;
+    o->use_cuda_graph = 1;
+    o->seed = 0x7B0u;
+    o->ray_radius = 4.0f;
+    o->ray_jitter = 0.05f;
+    return TN_OK;
+}
+
+int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_network* net) {
+    TN_NONNULL(out);
+    TN_NONNULL(desc);
+    *out = nullptr;
+    int st = validate_grid(&desc->grid);
+    if (st != TN_OK) return st;
+    TN_REQUIRE(desc->path == TN_PATH_FUSED || desc->path == TN_PATH_PLAIN, TN_E_INVALID, "unknown path %d", desc->path);
+    TN_REQUIRE(desc->batch_size >= 2 && desc->n_rays_per_step >= 2, TN_E_INVALID, "batch_size and n_rays_per_step must be >= 2");
+    TN_REQUIRE(desc->bbox.max_x > desc->bbox.min_x, TN_E_INVALID, "empty bounding box");
+    if (net) {
+        TN_REQUIRE(net->forward && net->density, TN_E_NULL, "tn_network needs forward and density callbacks");
+    }
+    tn_trainer* tr = new tn_trainer();
+    tr->d = *desc;
+    tr->aabb = desc->bbox.max_x - desc->bbox.min_x;
+    tr->synth.aabb = tr->aabb;
+    if (net) {
+        tr->net = *net;
+    } else {
+        tr->net.user = &tr->synth;
+        tr->net.activation = TN_ACT_SIGMA;
+        tr->net.forward = synth_forward;
+        tr->net.backward = nullptr;
+        tr->net.density = synth_density;
+    }
+    st = cuda_status(cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking), "stream");
+    if (st == TN_OK) st = tn_ctx_create(&tr->ctx);
+    const uint32_t R = desc->n_rays_per_step, B = desc->batch_size;
+    const uint32_t res = (uint32_t)desc->grid.resolution;
+    const uint32_t V = res * res * res, L = (uint32_t)desc->grid.n_levels;
+    const uint32_t P = desc->n_grid_params + desc->n_mlp_params;
+    tr->R = R; tr->B = B; tr->V = V; tr->P = P; tr->M = desc->occupancy_cells_per_step;
+    tr->chunk = std::min(B, V);
+    const uint32_t occ_n = std::max(tr->M, tr->chunk);
+    if (st == TN_OK) st = tn_ctx_reserve(tr->ctx, R, B);
+#define ALLOC(p, n) if (st == TN_OK) st = tr->alloc(p, (size_t)(n))
+    ALLOC(tr->ori, 3 * R); ALLOC(tr->dir, 3 * R); ALLOC(tr->ray_t, R); ALLOC(tr->ray_tmax, R); ALLOC(tr->target, 4 * R);
+    ALLOC(tr->bg, 3 * R); ALLOC(tr->alive, R); ALLOC(tr->n_steps, R); ALLOC(tr->offsets, R);
+    ALLOC(tr->s_t, B); ALLOC(tr->s_pos, 3 * B); ALLOC(tr->s_dir, 3 * B); ALLOC(tr->s_dt, B); ALLOC(tr->s_mnorm, B);
+    ALLOC(tr->s_dtnorm, B); ALLOC(tr->net_density, B); ALLOC(tr->net_rgb, 3 * B); ALLOC(tr->grad_density, B);
+    ALLOC(tr->dl_drgb, 3 * B);
+    if (desc->path == TN_PATH_PLAIN) {
+        ALLOC(tr->loss4, 4 * R); ALLOC(tr->dl_rec, B); ALLOC(tr->dl_dist, B); ALLOC(tr->ray5, 5 * R);
+        ALLOC(tr->sample2, 2 * B); ALLOC(tr->ray_loss, R);
+    }
+    ALLOC(tr->count_scratch, V / 4);
+    ALLOC(tr->density, (size_t)L * V); ALLOC(tr->bits, V);
+    ALLOC(tr->occ_levels, occ_n); ALLOC(tr->occ_cells, occ_n); ALLOC(tr->occ_rand3, 3 * (size_t)occ_n);
+    ALLOC(tr->occ_rsel, occ_n); ALLOC(tr->occ_pos, 3 * (size_t)occ_n); ALLOC(tr->occ_values, occ_n);
+    ALLOC(tr->w, P); ALLOC(tr->g, P); ALLOC(tr->m, P); ALLOC(tr->v, P); ALLOC(tr->steps, P);
+    ALLOC(tr->state, 1);
+#undef ALLOC
+    if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->state_host, sizeof(StepState)), "pinned state");
+    // reference initial grid: every bit set, densities zero (occupancy-grid.cuh:81-85)
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->bits, 0xFF, V, tr->stream), "bitfield init");
+    if (st == TN_OK) st = launch_synth_params(tr->stream, P, desc->n_grid_params, desc->seed, tr->w);
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "trainer init");
+    if (st != TN_OK) {
+        tn_trainer_destroy(tr);
+        return st;
+    }
+    *out = tr;
+    return TN_OK;
+}
+
+int tn_trainer_destroy(tn_trainer* tr) {
+    if (!tr) return TN_OK;
+    if (tr->stream) cudaStreamSynchronize(tr->stream);
+    for (int i = 0; i < 2; ++i) {
+        if (tr->graph_exec[i]) cudaGraphExecDestroy(tr->graph_exec[i]);
+        if (tr->graph[i]) cudaGraphDestroy(tr->graph[i]);
+    }
+    for (void* p : tr->allocs) cudaFree(p);
+    if (tr->synth.blobs) cudaFree(tr->synth.blobs);
+    if (tr->synth.waves) cudaFree(tr->synth.waves);
+    if (tr->state_host) cudaFreeHost(tr->state_host);
+    if (tr->ctx) tn_ctx_destroy(tr->ctx);
+    if (tr->stream) cudaStreamDestroy(tr->stream);
+    delete tr;
+    return TN_OK;
+}
+
+int tn_trainer_set_synthetic_field(tn_trainer* tr, uint32_t n_blobs, const float* blobs, const float* waves) {
+    TN_NONNULL(tr); TN_NONNULL(blobs); TN_NONNULL(waves);
+    TN_REQUIRE(n_blobs >= 1 && n_blobs <= 256, TN_E_INVALID, "n_blobs %u outside 1..256", n_blobs);
+    TN_REQUIRE(tr->graph_exec[0] == nullptr && tr->graph_exec[1] == nullptr, TN_E_STATE,
+               "the field must be set before the first captured step");
+    if (tr->synth.blobs) cudaFree(tr->synth.blobs);
+    if (tr->synth.waves) cudaFree(tr->synth.waves);
+    tr->synth.blobs = tr->synth.waves = nullptr;
+    int st = cuda_status(cudaMalloc(&tr->synth.blobs, 5 * n_blobs * sizeof(float)), "blobs");
+    if (st == TN_OK) st = cuda_status(cudaMalloc(&tr->synth.waves, 12 * sizeof(float)), "waves");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy(tr->synth.blobs, blobs, 5 * n_blobs * sizeof(float), cudaMemcpyHostToDevice), "blobs copy");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy(tr->synth.waves, waves, 12 * sizeof(float), cudaMemcpyHostToDevice), "waves copy");
+    tr->synth.n_blobs = n_blobs;
+    return st;
+}
+
+int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bitfield) {
+    TN_NONNULL(tr);
+    const size_t L = (size_t)tr->d.grid.n_levels;
+    int st = TN_OK;
+    if (density) st = cuda_status(cudaMemcpyAsync(tr->density, density, L * tr->V * sizeof(float), cudaMemcpyHostToDevice, tr->stream), "density copy");
+    if (st == TN_OK && bitfield) st = cuda_status(cudaMemcpyAsync(tr->bits, bitfield, tr->V, cudaMemcpyHostToDevice, tr->stream), "bits copy");
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "set_grid sync");
+    return st;
+}
+
+int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_touched_out) {
+    TN_NONNULL(tr);
+    const tn_trainer_desc& d = tr->d;
+    cudaStream_t s = tr->stream;
+    const tn_grid_desc grid = tr->grid();
+    const tn_march_desc march = tr->march();
+    // one batch of samples from the current grid (rays of step 0)
+    int st = cuda_status(cudaMemsetAsync(tr->state, 0, sizeof(StepState), s), "state clear");
+    if (st == TN_OK)
+        st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
+                               3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+    uint32_t* info = tr->state->batch_info;
+    if (st == TN_OK)
+        st = tn_march_count(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, tr->ori, tr->dir,
+                            tr->ray_t, tr->ray_tmax, tr->alive, tr->n_steps, tr->B, info);
+    if (st == TN_OK)
+        st = tn_march_emit(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B, info,
+                           nullptr, tr->ori, tr->dir, tr->ray_t, tr->alive, tr->n_steps, tr->offsets, nullptr, tr->s_t,
+                           tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->g, 0, (size_t)tr->P * 4, s), "grad clear");
+    // the reference's encoding: 16 levels, 2 features, 2^19 entries, base 16, max 2048 * aabb
+    const int levels = 16, feats = 2;
+    uint32_t log2_t = 19;
+    while (log2_t > 0 && (uint64_t)levels * feats * (1ull << log2_t) > d.n_grid_params) --log2_t;
+    const double n_max = 2048.0 * std::max(1.0, (double)tr->aabb);
+    const float scale = (float)std::exp((std::log(n_max) - std::log(16.0)) / 15.0);
+    if (st == TN_OK)
+        st = launch_synth_hash_grads(s, tr->B, info + 1, tr->B, tr->s_pos, levels, log2_t, feats, 16.0f, scale, d.seed,
+                                     std, tr->g);
+    // every MLP weight gets a gradient too
+    if (st == TN_OK && d.n_mlp_params) {
+        std::vector<float> hg(d.n_mlp_params);
+        uint32_t x = d.seed * 2654435761u + 1u;
+        for (auto& v : hg) {
+            x ^= x << 13; x ^= x >> 17; x ^= x << 5;
+            v = std * (((float)(x >> 8) / 16777216.0f) * 2.0f - 1.0f) * 1.7320508f;
+        }
+        st = cuda_status(cudaMemcpyAsync(tr->g + d.n_grid_params, hg.data(), hg.size() * 4, cudaMemcpyHostToDevice, s), "mlp grads");
+        if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "mlp grads sync");
+    }
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->state, 0, sizeof(StepState), s), "state clear");
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "init grads sync");
+    if (st == TN_OK && n_touched_out) {
+        std::vector<float> hg(d.n_grid_params);
+        st = cuda_status(cudaMemcpy(hg.data(), tr->g, hg.size() * 4, cudaMemcpyDeviceToHost), "grad read");
+        uint32_t c = 0;
+        for (float v : hg) c += v != 0.0f;
+        *n_touched_out = c;
+    }
+    uint32_t flags = 0;
+    if (st == TN_OK) st = tn_ctx_check(tr->ctx, s, &flags);
+    return st;
+}
+
+static int train_step_impl(tn_trainer* tr, bool external, tn_training_metrics* metrics) {
+    if (tr->d.path == TN_PATH_PLAIN) return run_plain_step(tr, external, metrics);
+    int st = TN_OK;
+    const int gi = external ? 1 : 0;
+    // The first step runs eagerly (it also warms up every lazily initialised resource);
+    // later steps replay a graph captured once per ray source.
+    if (tr->d.use_cuda_graph && tr->fused_steps_enqueued >= 1) {
+        if (!tr->graph_exec[gi]) {
+            st = cuda_status(cudaStreamBeginCapture(tr->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            if (st == TN_OK) {
+                const int est = enqueue_fused_step(tr, external, nullptr);
+                cudaGraph_t g = nullptr;
+                const cudaError_t e = cudaStreamEndCapture(tr->stream, &g);
+                if (est != TN_OK) { if (g) cudaGraphDestroy(g); return est; }
+                st = cuda_status(e, "end capture");
+                if (st == TN_OK) tr->graph[gi] = g;
+            }
+            if (st == TN_OK) st = cuda_status(cudaGraphInstantiate(&tr->graph_exec[gi], tr->graph[gi], 0), "instantiate");
+            if (st == TN_OK) {
+                size_t n_nodes = 0;
+                cudaGraphGetNodes(tr->graph[gi], nullptr, &n_nodes);
+                std::vector<cudaGraphNode_t> nodes(n_nodes);
+                cudaGraphGetNodes(tr->graph[gi], nodes.data(), &n_nodes);
+                uint32_t kernels = 0;
+                for (auto nd : nodes) {
+                    cudaGraphNodeType t;
+                    cudaGraphNodeGetType(nd, &t);
+                    kernels += t == cudaGraphNodeTypeKernel;
+                }
+                tr->graph_kernels[gi] = kernels;
+                tr->graph_nodes[gi] = (uint32_t)n_nodes;
+            }
+            if (st != TN_OK) return st;
+        }
+        st = cuda_status(cudaGraphLaunch(tr->graph_exec[gi], tr->stream), "graph launch");
+    } else {
+        st = enqueue_fused_step(tr, external, nullptr);
+    }
+    if (st != TN_OK) return st;
+    ++tr->fused_steps_enqueued;
+    if (metrics) return read_state(tr, metrics);
+    return TN_OK;
+}
+
+int tn_trainer_train_step(tn_trainer* tr, tn_training_metrics* metrics) {
+    TN_NONNULL(tr);
+    return train_step_impl(tr, false, metrics);
+}
+
+int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori, const float* dir,
+                               const float* target_rgba, const float* bg_rgb, tn_training_metrics* metrics) {
+    TN_NONNULL(tr); TN_NONNULL(ori); TN_NONNULL(dir); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
+    TN_REQUIRE(n_rays == tr->R, TN_E_INVALID, "tn_trainer_train_step_rays: n_rays must equal n_rays_per_step (%u)", tr->R);
+    cudaStream_t s = tr->stream;
+    const size_t row = (size_t)n_rays * sizeof(float);
+    int st = cuda_status(cudaMemcpy2DAsync(tr->ori, row, ori, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(tr->dir, row, dir, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(tr->target, row, target_rgba, row, row, 4, cudaMemcpyHostToDevice, s), "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(tr->bg, row, bg_rgb, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
+    if (st != TN_OK) return st;
+    return train_step_impl(tr, true, metrics);
+}
+
+int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages) {
+    TN_NONNULL(tr); TN_NONNULL(stage_ms);
+    TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "stage timing covers the fused path");
+    cudaEvent_t ev[ST_N + 1];
+    for (auto& e : ev) cudaEventCreate(&e);
+    int st = enqueue_fused_step(tr, false, ev);
+    if (st == TN_OK) st = cuda_status(cudaEventSynchronize(ev[ST_N]), "profile sync");
+    const uint32_t n = std::min<uint32_t>(max_stages, ST_N);
+    for (uint32_t k = 0; k < n && st == TN_OK; ++k) cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    ++tr->fused_steps_enqueued;
+    if (n_stages) *n_stages = n;
+    return st;
+}
+
+int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out) {
+    TN_NONNULL(tr); TN_NONNULL(out);
+    switch (which) {
+        case 0: *out = tr->graph_kernels[0]; return TN_OK;
+        case 1: *out = tr->graph_kernels[1]; return TN_OK;
+        case 2: *out = tr->graph_nodes[0]; return TN_OK;
+        case 3:
+        case 4:
+        case 5: {
+            int st = cuda_status(cudaMemcpyAsync(tr->state_host, tr->state, sizeof(StepState), cudaMemcpyDeviceToHost,
+                                                 tr->stream), "stat");
+            if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "stat sync");
+            if (st != TN_OK) return st;
+            *out = which == 3 ? tr->state_host->samples_total
+                 : which == 4 ? tr->state_host->rays_total : tr->state_host->step_count;
+            return TN_OK;
+        }
+        default: return fail(TN_E_INVALID, "unknown trainer stat %d", which);
+    }
+}
+
+int tn_trainer_sync_metrics(tn_trainer* tr, tn_training_metrics* metrics) {
+    TN_NONNULL(tr);
+    if (tr->d.path == TN_PATH_PLAIN) {
+        int st = cuda_status(cudaStreamSynchronize(tr->stream), "sync");
+        if (metrics) *metrics = tr->last;
+        return st;
+    }
+    return read_state(tr, metrics);
+}
+
+int tn_trainer_update_occupancy_grid(tn_trainer* tr, uint32_t training_step, tn_occupancy_metrics* metrics) {
+    TN_NONNULL(tr);
+    const tn_trainer_desc& d = tr->d;
+    cudaStream_t s = tr->stream;
+    const tn_grid_desc grid = tr->grid();
+    const int sample_all = training_step < 256 ? 1 : 0;
+    const bool plain = d.path == TN_PATH_PLAIN;
+    int st = TN_OK;
+    if (plain) st = launch_plain_occ_decay(s, &grid, tr->density, d.occupancy_decay);
+    for (int level = 0; level < grid.n_levels && st == TN_OK; ++level) {
+        for (uint32_t start = 0; start < tr->V && st == TN_OK; start += tr->chunk) {
+            const uint32_t n = std::min(tr->chunk, tr->V - start);
+            st = launch_synth_level_cells(s, n, start, level, d.seed, 0x20000000u + training_step, tr->occ_levels,
+                                          tr->occ_cells, tr->occ_rand3, n, tr->occ_rsel);
+            if (st == TN_OK)
+                st = tn_occupancy_sample_points(s, &grid, n, tr->occ_levels, tr->occ_cells, tr->occ_rand3, n,
+                                                1.0f / tr->aabb, tr->occ_pos, n);
+            if (st == TN_OK) st = tr->net.density(tr->net.user, s, n, nullptr, n, tr->occ_pos, tr->occ_values);
+            if (st == TN_OK) {
+                st = plain ? launch_plain_occ_update(s, &grid, tr->density, tr->bits, n, tr->occ_levels, tr->occ_cells,
+                                                     tr->occ_values, tr->occ_rsel, tr->net.activation, sample_all)
+                           : launch_occupancy_scatter(s, &grid, tr->density, tr->bits, n, tr->occ_levels, tr->occ_cells,
+                                                      tr->occ_values, tr->occ_rsel, tr->net.activation, sample_all,
+                                                      d.occupancy_decay);
+            }
+        }
+    }
+    uint32_t nocc = 0;
+    if (st == TN_OK) {
+        if (plain) {
+            st = launch_plain_occ_bits_sync(s, &grid, tr->density, tr->bits, d.occupancy_threshold, tr->count_scratch,
+                                            &nocc);
+        } else {
+            st = launch_occupancy_sweep(s, &grid, tr->density, tr->bits, d.occupancy_decay, d.occupancy_threshold,
+                                        &tr->state->n_occupied);
+            if (st == TN_OK)
+                st = cuda_status(cudaMemcpyAsync(&tr->state_host->n_occupied, &tr->state->n_occupied, 4,
+                                                 cudaMemcpyDeviceToHost, s), "n_occupied");
+            if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "occupancy sync");
+            nocc = tr->state_host->n_occupied;
+        }
+    }
+    if (st == TN_OK && metrics) {
+        metrics->n_occupied = nocc;
+        metrics->n_total = (uint32_t)grid.n_levels * tr->V;  // reference: n_levels * 128^3
+    }
+    return st;
+}
+
+int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out) {
+    TN_NONNULL(tr); TN_NONNULL(out);
+    *out = tr->stream;
+    return TN_OK;
+}
+
+int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes) {
+    TN_NONNULL(tr); TN_NONNULL(ptr);
+    const uint64_t R = tr->R, B = tr->B, V = tr->V, P = tr->P, L = (uint64_t)tr->d.grid.n_levels;
+    void* p = nullptr;
+    uint64_t n = 0;
+    switch (which) {
+        case 0: p = tr->w; n = 4 * P; break;
+        case 1: p = tr->g; n = 4 * P; break;
+        case 2: p = tr->m; n = 4 * P; break;
+        case 3: p = tr->v; n = 4 * P; break;
+        case 4: p = tr->steps; n = 4 * P; break;
+        case 5: p = tr->density; n = 4 * L * V; break;
+        case 6: p = tr->bits; n = V; break;
+        case 7: p = tr->s_t; n = 4 * B; break;
+        case 8: p = tr->s_pos; n = 12 * B; break;
+        case 9: p = tr->s_dt; n = 4 * B; break;
+        case 10: p = tr->offsets; n = 4 * R; break;
+        case 11: p = tr->n_steps; n = 4 * R; break;
+        case 12: p = tr->state->batch_info; n = 16; break;
+        case 13: p = tr->net_density; n = 4 * B; break;
+        case 14: p = tr->net_rgb; n = 12 * B; break;
+        case 15: p = tr->grad_density; n = 4 * B; break;
+        case 16: p = tr->dl_drgb; n = 12 * B; break;
+        case 17: p = tr->ori; n = 12 * R; break;
+        case 18: p = tr->dir; n = 12 * R; break;
+        case 19: p = tr->ray_t; n = 4 * R; break;
+        case 20: p = tr->ray_tmax; n = 4 * R; break;
+        case 21: p = tr->alive; n = R; break;
+        case 22: p = tr->target; n = 16 * R; break;
+        case 23: p = tr->bg; n = 12 * R; break;
+        case 24: p = tr->s_mnorm; n = 4 * B; break;
+        case 25: p = tr->s_dtnorm; n = 4 * B; break;
+        default: return fail(TN_E_INVALID, "unknown trainer buffer %d", which);
+    }
+    *ptr = p;
+    if (bytes) *bytes = n;
+    return TN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,358 @@
+"""Tensor-level entry points of the training hot path (thin wrappers over the C ABI).
+
+Every function takes CUDA tensors in the reference's structure-of-arrays layout and
+enqueues work on torch's current stream; nothing here computes on the CPU. Tensors must be
+contiguous with the dtypes named in each docstring.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import native
+from .native import Bbox, GridDesc, MarchDesc, RayBatchDesc, call
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("turbo_hot tensors must live on a CUDA device")
+    if not t.is_contiguous():
+        raise ValueError("turbo_hot tensors must be contiguous")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Context:
+    """Owns a tn_ctx (scratch, device error word) on the current CUDA device."""
+
+    def __init__(self, max_rays: int = 0, max_samples: int = 0):
+        h = ctypes.c_void_p()
+        call("tn_ctx_create", ctypes.byref(h))
+        self.handle = h
+        if max_rays or max_samples:
+            self.reserve(max_rays, max_samples)
+
+    def reserve(self, max_rays: int, max_samples: int) -> None:
+        call("tn_ctx_reserve", self.handle, max_rays, max_samples)
+
+    def check(self) -> int:
+        """Synchronises the stream; returns and clears the device error bits."""
+        f = ctypes.c_uint32(0)
+        call("tn_ctx_check", self.handle, _stream(), ctypes.byref(f))
+        return f.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            native.lib().tn_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class GridSpec:
+    n_levels: int
+    resolution: int = 128
+    base_size: float = 1.0
+
+    def desc(self) -> GridDesc:
+        return GridDesc(self.n_levels, self.resolution, float(self.base_size), 0)
+
+    @property
+    def volume(self) -> int:
+        return self.resolution ** 3
+
+
+@dataclass
+class MarchSpec:
+    cone_angle: float
+    dt_min: float
+    dt_max: float
+    max_steps: int = 0
+    max_iterations: int = 0
+
+    def desc(self) -> MarchDesc:
+        return MarchDesc(self.cone_angle, self.dt_min, self.dt_max, self.max_steps, self.max_iterations)
+
+
+def bbox_desc(b) -> Bbox:
+    return Bbox(*[float(v) for v in b])
+
+
+def ray_batch(counts: torch.Tensor, offsets: torch.Tensor, n_rays: int, ray_stride: int, sample_stride: int,
+              n_rays_dev: torch.Tensor | None = None) -> RayBatchDesc:
+    return RayBatchDesc(n_rays, ray_stride, sample_stride, 0, _ptr(counts), _ptr(offsets), _ptr(n_rays_dev))
+
+
+# ---- rays -------------------------------------------------------------------------------
+def rays_init_bbox(ori, dir_, n_rays, ray_stride, bbox, t_far=3.0e38):
+    dev = ori.device
+    t = torch.zeros(ray_stride, dtype=torch.float32, device=dev)
+    tmax = torch.zeros(ray_stride, dtype=torch.float32, device=dev)
+    alive = torch.zeros(ray_stride, dtype=torch.uint8, device=dev)
+    b = bbox_desc(bbox)
+    call("tn_rays_init_bbox", _stream(), n_rays, ray_stride, ctypes.byref(b), t_far, _ptr(ori), _ptr(dir_), _ptr(t),
+         _ptr(tmax), _ptr(alive))
+    return t, tmax, alive
+
+
+# ---- march ------------------------------------------------------------------------------
+def march_count(ctx: Context, grid: GridSpec, bitfield, bbox, march: MarchSpec, n_rays: int, ray_stride: int,
+                ori, dir_, ray_t, ray_t_max, alive, batch_size: int, n_rays_dev=None, n_steps=None, batch_info=None):
+    """Fused count pass + device batch cut. `alive` (uint8) is updated in place.
+    Returns (n_steps uint32[ray_stride], batch_info uint32[3] = n_rays_cut, n_samples, total)."""
+    dev = ori.device
+    if n_steps is None:
+        n_steps = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    if batch_info is None:
+        batch_info = torch.zeros(4, dtype=torch.int32, device=dev)
+    g, b, m = grid.desc(), bbox_desc(bbox), march.desc()
+    call("tn_march_count", ctx.handle, _stream(), ctypes.byref(g), _ptr(bitfield), ctypes.byref(b), ctypes.byref(m),
+         n_rays, ray_stride, _ptr(n_rays_dev), _ptr(ori), _ptr(dir_), _ptr(ray_t), _ptr(ray_t_max), _ptr(alive),
+         _ptr(n_steps), batch_size, _ptr(batch_info))
+    return n_steps, batch_info
+
+
+def alloc_samples(sample_stride: int, device) -> dict:
+    f = dict(dtype=torch.float32, device=device)
+    return dict(img_id=torch.zeros(sample_stride, dtype=torch.int32, device=device),
+                t=torch.zeros(sample_stride, **f), pos=torch.zeros(3 * sample_stride, **f),
+                dir=torch.zeros(3 * sample_stride, **f), dt=torch.zeros(sample_stride, **f),
+                m_norm=torch.zeros(sample_stride, **f), dt_norm=torch.zeros(sample_stride, **f))
+
+
+def march_emit(ctx: Context, grid: GridSpec, bitfield, bbox, march: MarchSpec, inv_aabb: float, n_rays: int,
+               ray_stride: int, sample_stride: int, batch_info, ori, dir_, ray_t, alive, n_steps, ray_img_id=None,
+               offsets=None, samples=None):
+    dev = ori.device
+    if offsets is None:
+        offsets = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    if samples is None:
+        samples = alloc_samples(sample_stride, dev)
+    g, b, m = grid.desc(), bbox_desc(bbox), march.desc()
+    call("tn_march_emit", ctx.handle, _stream(), ctypes.byref(g), _ptr(bitfield), ctypes.byref(b), ctypes.byref(m),
+         inv_aabb, n_rays, ray_stride, sample_stride, _ptr(batch_info), _ptr(ray_img_id), _ptr(ori), _ptr(dir_),
+         _ptr(ray_t), _ptr(alive), _ptr(n_steps), _ptr(offsets), _ptr(samples["img_id"]), _ptr(samples["t"]),
+         _ptr(samples["pos"]), _ptr(samples["dir"]), _ptr(samples["dt"]), _ptr(samples["m_norm"]),
+         _ptr(samples["dt_norm"]))
+    return offsets, samples
+
+
+def scan_offsets(ctx: Context, counts, batch_size: int):
+    n = counts.numel()
+    offsets = torch.zeros(n, dtype=torch.int32, device=counts.device)
+    info = torch.zeros(4, dtype=torch.int32, device=counts.device)
+    call("tn_scan_offsets", ctx.handle, _stream(), n, _ptr(counts), _ptr(offsets), batch_size, _ptr(info))
+    return offsets, info
+
+
+def compact_nonzero(ctx: Context, values):
+    n = values.numel()
+    out = torch.zeros(n, dtype=torch.int32, device=values.device)
+    cnt = torch.zeros(1, dtype=torch.int32, device=values.device)
+    call("tn_compact_nonzero", ctx.handle, _stream(), n, _ptr(values), _ptr(out), _ptr(cnt))
+    return out, cnt
+
+
+# ---- plain march ------------------------------------------------------------------------
+def plain_march_count(grid, bitfield, bbox, march, n_rays, ray_stride, ori, dir_, ray_t, ray_t_max, alive):
+    n_steps = torch.zeros(ray_stride, dtype=torch.int32, device=ori.device)
+    g, b, m = grid.desc(), bbox_desc(bbox), march.desc()
+    call("tn_plain_march_count", _stream(), ctypes.byref(g), _ptr(bitfield), ctypes.byref(b), ctypes.byref(m), n_rays,
+         ray_stride, _ptr(ori), _ptr(dir_), _ptr(ray_t), _ptr(ray_t_max), _ptr(alive), _ptr(n_steps))
+    return n_steps
+
+
+def plain_scan_cut(n, n_steps, batch_size, offsets=None):
+    if offsets is None:
+        offsets = torch.zeros(n_steps.numel(), dtype=torch.int32, device=n_steps.device)
+    nr, ns = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    call("tn_plain_scan_cut_sync", _stream(), n, _ptr(n_steps), _ptr(offsets), batch_size, ctypes.byref(nr),
+         ctypes.byref(ns))
+    return offsets, nr.value, ns.value
+
+
+def plain_march_emit(grid, bitfield, bbox, march, inv_aabb, n_rays, ray_stride, sample_stride, ori, dir_, ray_t,
+                     offsets, alive, n_steps, ray_img_id=None, samples=None):
+    if samples is None:
+        samples = alloc_samples(sample_stride, ori.device)
+    g, b, m = grid.desc(), bbox_desc(bbox), march.desc()
+    call("tn_plain_march_emit", _stream(), ctypes.byref(g), _ptr(bitfield), ctypes.byref(b), ctypes.byref(m), inv_aabb,
+         n_rays, ray_stride, sample_stride, _ptr(ray_img_id), _ptr(ori), _ptr(dir_), _ptr(ray_t), _ptr(offsets),
+         _ptr(alive), _ptr(n_steps), _ptr(samples["img_id"]), _ptr(samples["t"]), _ptr(samples["pos"]),
+         _ptr(samples["dir"]), _ptr(samples["dt"]), _ptr(samples["m_norm"]), _ptr(samples["dt_norm"]))
+    return samples
+
+
+# ---- compositor / losses ------------------------------------------------------------------
+def composite_fwd(ctx, rb: RayBatchDesc, density, rgb, dt, activation=0, min_t=1e-4, out=None):
+    dev = density.device
+    rs = rb.ray_stride
+    if out is None:
+        out = dict(rgba=torch.zeros(4 * rs, dtype=torch.float32, device=dev),
+                   depth=torch.zeros(rs, dtype=torch.float32, device=dev),
+                   n_used=torch.zeros(rs, dtype=torch.int32, device=dev))
+    call("tn_composite_fwd", ctx.handle, _stream(), ctypes.byref(rb), activation, min_t, _ptr(density), _ptr(rgb),
+         _ptr(dt), _ptr(out["rgba"]), _ptr(out["depth"]), _ptr(out["n_used"]))
+    return out
+
+
+def composite_bwd(ctx, rb: RayBatchDesc, density, rgb, dt, depth, n_used, grad_rgba, activation=0):
+    dev = density.device
+    ss = rb.sample_stride
+    dd = torch.zeros(ss, dtype=torch.float32, device=dev)
+    drgb = torch.zeros(3 * ss, dtype=torch.float32, device=dev)
+    call("tn_composite_bwd", ctx.handle, _stream(), ctypes.byref(rb), activation, _ptr(density), _ptr(rgb), _ptr(dt),
+         _ptr(depth), _ptr(n_used), _ptr(grad_rgba), _ptr(dd), _ptr(drgb))
+    return dd, drgb
+
+
+def recon_loss_fwd_bwd(ctx, rb: RayBatchDesc, density, rgb, dt, target_rgba, bg_rgb, inv_nrays, grad_scale=1.0,
+                       activation=0, min_t=1e-4):
+    dev = density.device
+    rs, ss = rb.ray_stride, rb.sample_stride
+    out = dict(ray_rgba=torch.zeros(4 * rs, dtype=torch.float32, device=dev),
+               loss=torch.zeros(4 * rs, dtype=torch.float32, device=dev),
+               loss_sum=torch.zeros(1, dtype=torch.float32, device=dev),
+               dL_ddensity=torch.zeros(ss, dtype=torch.float32, device=dev),
+               dL_drgb=torch.zeros(3 * ss, dtype=torch.float32, device=dev))
+    call("tn_recon_loss_fwd_bwd", ctx.handle, _stream(), ctypes.byref(rb), activation, min_t, inv_nrays, grad_scale,
+         _ptr(density), _ptr(rgb), _ptr(dt), _ptr(target_rgba), _ptr(bg_rgb), _ptr(out["ray_rgba"]), _ptr(out["loss"]),
+         _ptr(out["loss_sum"]), _ptr(out["dL_ddensity"]), _ptr(out["dL_drgb"]))
+    return out
+
+
+def distortion_fwd_bwd(ctx, rb: RayBatchDesc, density, m_norm, dt_norm, lam, activation=0, grad_ray=None,
+                       backward=True):
+    dev = density.device
+    out = dict(ray_loss=torch.zeros(rb.ray_stride, dtype=torch.float32, device=dev),
+               loss_sum=torch.zeros(1, dtype=torch.float32, device=dev),
+               dL_ddensity=torch.zeros(rb.sample_stride, dtype=torch.float32, device=dev) if backward else None)
+    call("tn_distortion_fwd_bwd", ctx.handle, _stream(), ctypes.byref(rb), activation, lam, _ptr(density),
+         _ptr(m_norm), _ptr(dt_norm), _ptr(grad_ray), _ptr(out["ray_loss"]), _ptr(out["loss_sum"]),
+         _ptr(out["dL_ddensity"]))
+    return out
+
+
+def grad_epilogue(n_samples, loss_scale, dL_rec, dL_dist, t, grad_out, n_samples_dev=None):
+    call("tn_grad_epilogue", _stream(), n_samples, _ptr(n_samples_dev), loss_scale, _ptr(dL_rec), _ptr(dL_dist), _ptr(t),
+         _ptr(grad_out))
+    return grad_out
+
+
+def train_losses(ctx, rb: RayBatchDesc, density, rgb, dt, m_norm, dt_norm, t, target_rgba, bg_rgb, grad_density,
+                 inv_nrays=0.0, inv_nrays_from=None, grad_scale=1.0, lam=0.0, activation=0, min_t=1e-4,
+                 ray_rgba=None, dL_drgb=None, loss_sums=None):
+    dev = density.device
+    if dL_drgb is None:
+        dL_drgb = torch.zeros(3 * rb.sample_stride, dtype=torch.float32, device=dev)
+    if loss_sums is None:
+        loss_sums = torch.zeros(2, dtype=torch.float32, device=dev)
+    call("tn_train_losses", ctx.handle, _stream(), ctypes.byref(rb), activation, min_t, inv_nrays,
+         _ptr(inv_nrays_from), grad_scale, lam, _ptr(density), _ptr(rgb), _ptr(dt), _ptr(m_norm), _ptr(dt_norm),
+         _ptr(t), _ptr(target_rgba), _ptr(bg_rgb), _ptr(ray_rgba), _ptr(grad_density), _ptr(dL_drgb), _ptr(loss_sums))
+    return grad_density, dL_drgb, loss_sums
+
+
+def plain_recon_loss(rb, density, rgb, dt, target_rgba, bg_rgb, inv_nrays, grad_scale=1.0, activation=0, min_t=1e-4):
+    dev = density.device
+    rs, ss = rb.ray_stride, rb.sample_stride
+    loss = torch.zeros(4 * rs, dtype=torch.float32, device=dev)
+    dd = torch.zeros(ss, dtype=torch.float32, device=dev)
+    drgb = torch.zeros(3 * ss, dtype=torch.float32, device=dev)
+    out = ctypes.c_float(0)
+    call("tn_plain_recon_loss_sync", _stream(), ctypes.byref(rb), activation, min_t, inv_nrays, grad_scale,
+         _ptr(density), _ptr(rgb), _ptr(dt), _ptr(target_rgba), _ptr(bg_rgb), _ptr(loss), _ptr(dd), _ptr(drgb),
+         ctypes.byref(out))
+    return loss, dd, drgb, out.value
+
+
+def plain_distortion(rb, density, m_norm, dt_norm, lam, activation=0):
+    dev = density.device
+    rs, ss = rb.ray_stride, rb.sample_stride
+    ray_scratch = torch.zeros(5 * rs, dtype=torch.float32, device=dev)
+    sample_scratch = torch.zeros(2 * ss, dtype=torch.float32, device=dev)
+    ray_loss = torch.zeros(rs, dtype=torch.float32, device=dev)
+    dd = torch.zeros(ss, dtype=torch.float32, device=dev)
+    out = ctypes.c_float(0)
+    call("tn_plain_distortion_sync", _stream(), ctypes.byref(rb), activation, lam, _ptr(density), _ptr(m_norm),
+         _ptr(dt_norm), _ptr(ray_scratch), _ptr(sample_scratch), _ptr(ray_loss), _ptr(dd), ctypes.byref(out))
+    return ray_loss, dd, out.value
+
+
+def plain_grad_epilogue(n_samples, loss_scale, dL_rec, dL_dist, t, grad_out):
+    call("tn_plain_grad_epilogue", _stream(), n_samples, loss_scale, _ptr(dL_rec), _ptr(dL_dist), _ptr(t),
+         _ptr(grad_out))
+    return grad_out
+
+
+# ---- occupancy ------------------------------------------------------------------------------
+def occupancy_sample_points(grid: GridSpec, levels, cells, rand3, rand_stride, inv_aabb, pos_stride=None):
+    n = levels.numel()
+    pos_stride = pos_stride or n
+    out = torch.zeros(3 * pos_stride, dtype=torch.float32, device=levels.device)
+    g = grid.desc()
+    call("tn_occupancy_sample_points", _stream(), ctypes.byref(g), n, _ptr(levels), _ptr(cells), _ptr(rand3),
+         rand_stride, inv_aabb, _ptr(out), pos_stride)
+    return out
+
+
+def occupancy_update(ctx, grid: GridSpec, density, bitfield, levels, cells, values, rand_select, activation=0,
+                     sample_all=False, decay=0.95, threshold=0.01, n_occupied=None):
+    n = levels.numel() if levels is not None else 0
+    if n_occupied is None:
+        n_occupied = torch.zeros(1, dtype=torch.int32, device=density.device)
+    g = grid.desc()
+    call("tn_occupancy_update", ctx.handle, _stream(), ctypes.byref(g), _ptr(density), _ptr(bitfield), n,
+         _ptr(levels), _ptr(cells), _ptr(values), _ptr(rand_select), activation, int(bool(sample_all)), decay,
+         threshold, _ptr(n_occupied))
+    return n_occupied
+
+
+def plain_occupancy_update(grid: GridSpec, density, bitfield, levels, cells, values, rand_select, activation=0,
+                           sample_all=False, decay=0.95, threshold=0.01, count_scratch=None):
+    n = levels.numel() if levels is not None else 0
+    if count_scratch is None:
+        count_scratch = torch.zeros(grid.volume // 4, dtype=torch.uint8, device=density.device)
+    out = ctypes.c_uint32(0)
+    g = grid.desc()
+    call("tn_plain_occupancy_update_sync", _stream(), ctypes.byref(g), _ptr(density), _ptr(bitfield), n,
+         _ptr(levels), _ptr(cells), _ptr(values), _ptr(rand_select), activation, int(bool(sample_all)), decay,
+         threshold, _ptr(count_scratch), ctypes.byref(out))
+    return out.value
+
+
+def popcount(ctx, bytes_):
+    out = torch.zeros(1, dtype=torch.int32, device=bytes_.device)
+    call("tn_popcount", ctx.handle, _stream(), bytes_.numel(), _ptr(bytes_), _ptr(out))
+    return out
+
+
+# ---- Adam ---------------------------------------------------------------------------------
+def adam_step(weights, grads, m, v, steps, n_grid, n_mlp, lr, beta1=0.9, beta2=0.99, eps=1e-15, l2=1e-6,
+              loss_scale=1.0, weights_copy=None, plain=False):
+    name = "tn_plain_adam_step" if plain else "tn_adam_step"
+    call(name, _stream(), weights.numel(), n_grid, n_mlp, loss_scale, lr, beta1, beta2, eps, l2, _ptr(weights),
+         _ptr(weights_copy), _ptr(grads), _ptr(m), _ptr(v), _ptr(steps))
+
+
+# ---- synthetic producer -----------------------------------------------------------------
+def synth_field(pos, pos_stride, n, aabb_size, blobs, waves, n_dev=None, out_stride=None, want_rgb=True):
+    dev = pos.device
+    out_stride = out_stride or pos_stride
+    sigma = torch.zeros(out_stride, dtype=torch.float32, device=dev)
+    rgb = torch.zeros(3 * out_stride, dtype=torch.float32, device=dev) if want_rgb else None
+    call("tn_synth_field", _stream(), n, _ptr(n_dev), pos_stride, _ptr(pos), aabb_size, blobs.shape[0], _ptr(blobs),
+         _ptr(waves), _ptr(sigma), _ptr(rgb), out_stride)
+    return sigma, rgb

@@ -1,0 +1,244 @@
+"""Python surface of the training controller, named like the reference's `PyTurboNeRF`
+module (src/api/python_bindings.cu:240-255, 423-491): `BoundingBox`, `Trainer` with
+`setup_data(batch_size)`, `train_step()`, `update_occupancy_grid(training_step)`,
+`teardown()`, the `TrainingMetrics` / `OccupancyGridMetrics` results and the
+`min_step_size` / `use_distortion_loss` / alpha-selection attributes.
+
+The controller itself is C++ inside libturbo_hot.so (tn_trainer_*); this module only
+marshals arguments. The reference's `Trainer(nerf)` takes a NeRF proxy holding a dataset
+and a tiny-cuda-nn network; here `Trainer(scene)` takes a `SyntheticNeRF` (occupancy grid,
+bounding box and the synthetic blob field that stands in for the network).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native
+from .native import Bbox, GridDesc, OccupancyMetricsC, TrainerDesc, TrainingMetricsC, call
+
+MIN_STEP_SIZE = 0.00169145586  # NeRFConstants::min_step_size
+CONE_ANGLE = 1.0 / 256.0       # NeRFConstants::cone_angle
+
+
+class BoundingBox:
+    """Axis-aligned box, reference BoundingBox (src/models/bounding-box.cuh:8-23)."""
+
+    def __init__(self, size: float | None = None):
+        if size is None:
+            self.min_x = self.min_y = self.min_z = self.max_x = self.max_y = self.max_z = 0.0
+        else:
+            h = 0.5 * float(size)
+            self.min_x = self.min_y = self.min_z = -h
+            self.max_x = self.max_y = self.max_z = h
+
+    def size(self) -> float:
+        return self.max_x - self.min_x
+
+    def as_tuple(self):
+        return (self.min_x, self.min_y, self.min_z, self.max_x, self.max_y, self.max_z)
+
+    def __eq__(self, other):
+        return isinstance(other, BoundingBox) and self.as_tuple() == other.as_tuple()
+
+    def __ne__(self, other):
+        return not self == other
+
+
+@dataclass
+class TrainingMetrics:
+    step: int
+    loss: float
+    n_rays: int
+    n_samples: int
+
+
+@dataclass
+class OccupancyGridMetrics:
+    n_occupied: int
+    n_total: int
+
+
+@dataclass
+class SyntheticNeRF:
+    """What the trainer trains on: the cascaded occupancy grid (base size 1 = the reference's
+    2^k level extents), the training box, and the blob field standing in for the network."""
+    bounding_box: BoundingBox
+    n_levels: int
+    blobs: np.ndarray
+    waves: np.ndarray
+    density: np.ndarray | None = None   # [n_levels][res^3] float32 (None: zeros, like the reference)
+    bitfield: np.ndarray | None = None  # [res^3] uint8 (None: all bits set, like the reference)
+    resolution: int = 128
+    base_size: float = 1.0
+
+    @classmethod
+    def from_scene(cls, scene) -> "SyntheticNeRF":
+        b = BoundingBox()
+        b.min_x, b.min_y, b.min_z, b.max_x, b.max_y, b.max_z = [float(v) for v in scene.bbox]
+        g = scene.grid
+        return cls(b, g.n_levels, scene.field.blobs, scene.field.waves, g.density, g.bitfield, g.resolution,
+                   g.base_size)
+
+
+class Trainer:
+    """Training controller (reference NeRFTrainingController)."""
+
+    def __init__(self, nerf: SyntheticNeRF, path: str = "fused", use_cuda_graph: bool = True,
+                 n_rays_per_step: int = 1 << 14, occupancy_cells_per_step: int = 0,
+                 distortion_lambda: float = 0.01, occupancy_threshold: float = 0.01 * MIN_STEP_SIZE,
+                 n_grid_params: int = 16 * (1 << 19) * 2, n_mlp_params: int = 7168, beta2: float = 0.999,
+                 max_steps_per_ray: int = 0, seed: int = 0x7B0):
+        if path not in ("fused", "plain"):
+            raise ValueError("path must be 'fused' or 'plain'")
+        self.nerf = nerf
+        self.path = path
+        self.use_cuda_graph = use_cuda_graph
+        self.n_rays_per_step = n_rays_per_step
+        self.occupancy_cells_per_step = occupancy_cells_per_step
+        self.distortion_lambda = distortion_lambda
+        self.occupancy_threshold = occupancy_threshold
+        self.n_grid_params = n_grid_params
+        self.n_mlp_params = n_mlp_params
+        self.beta2 = beta2
+        self.max_steps_per_ray = max_steps_per_ray
+        self.seed = seed
+        # reference training settings (nerf-training-controller.h:75-78)
+        self.alpha_selection_threshold = 1.0
+        self.alpha_selection_probability = 1.0
+        self.min_step_size = MIN_STEP_SIZE
+        self.use_distortion_loss = False
+        self._h = None
+        self.n_touched_grads = 0
+
+    # -- lifecycle -----------------------------------------------------------------------
+    def setup_data(self, batch_size: int = 2 << 21, synthetic_grad_std: float = 1e-3) -> None:
+        """Allocates every buffer, uploads the grid and the synthetic field, and seeds the
+        parameter gradients (reference setup_data, nerf-training-controller.cu:27-85)."""
+        if self.alpha_selection_threshold < 1.0 and self.alpha_selection_probability < 1.0:
+            raise NotImplementedError("alpha selection acts on image alpha; the synthetic ray source has none")
+        self.teardown()
+        d = TrainerDesc()
+        call("tn_trainer_default_desc", ctypes.byref(d))
+        n = self.nerf
+        d.grid = GridDesc(n.n_levels, n.resolution, float(n.base_size), 0)
+        d.bbox = Bbox(*n.bounding_box.as_tuple())
+        d.batch_size = int(batch_size)
+        d.n_rays_per_step = int(self.n_rays_per_step)
+        d.min_step_size = float(self.min_step_size)
+        d.max_steps_per_ray = int(self.max_steps_per_ray)
+        d.use_distortion_loss = int(bool(self.use_distortion_loss))
+        d.distortion_lambda = float(self.distortion_lambda)
+        d.occupancy_threshold = float(self.occupancy_threshold)
+        d.occupancy_cells_per_step = int(self.occupancy_cells_per_step)
+        d.n_grid_params = int(self.n_grid_params)
+        d.n_mlp_params = int(self.n_mlp_params)
+        d.beta2 = float(self.beta2)
+        d.path = native.TN_PATH_FUSED if self.path == "fused" else native.TN_PATH_PLAIN
+        d.use_cuda_graph = int(bool(self.use_cuda_graph))
+        d.seed = int(self.seed)
+        h = ctypes.c_void_p()
+        call("tn_trainer_create", ctypes.byref(h), ctypes.byref(d), None)
+        self._h = h
+        blobs = np.ascontiguousarray(n.blobs, np.float32)
+        waves = np.ascontiguousarray(n.waves, np.float32)
+        call("tn_trainer_set_synthetic_field", h, blobs.shape[0], blobs.ctypes.data_as(ctypes.c_void_p),
+             waves.ctypes.data_as(ctypes.c_void_p))
+        dens = None if n.density is None else np.ascontiguousarray(n.density, np.float32)
+        bits = None if n.bitfield is None else np.ascontiguousarray(n.bitfield, np.uint8)
+        call("tn_trainer_set_grid", h, dens.ctypes.data_as(ctypes.c_void_p) if dens is not None else None,
+             bits.ctypes.data_as(ctypes.c_void_p) if bits is not None else None)
+        touched = ctypes.c_uint32(0)
+        call("tn_trainer_init_synthetic_gradients", h, float(synthetic_grad_std), ctypes.byref(touched))
+        self.n_touched_grads = touched.value
+
+    def teardown(self) -> None:
+        if self._h is not None:
+            native.lib().tn_trainer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.teardown()
+        except Exception:
+            pass
+
+    def _handle(self):
+        if self._h is None:
+            raise RuntimeError("call setup_data() first")
+        return self._h
+
+    # -- steps ---------------------------------------------------------------------------
+    def train_step(self) -> TrainingMetrics:
+        m = TrainingMetricsC()
+        call("tn_trainer_train_step", self._handle(), ctypes.byref(m))
+        return TrainingMetrics(m.step, m.loss, m.n_rays, m.n_samples)
+
+    def train_step_async(self) -> None:
+        """Enqueues one step without waiting (fused path: a graph replay)."""
+        call("tn_trainer_train_step", self._handle(), None)
+
+    def train_step_rays(self, ori, dir_, target_rgba, bg_rgb) -> TrainingMetrics:
+        """One step on caller rays held in (preferably pinned) host memory, each
+        [components][n_rays_per_step] float32; waits and returns the metrics."""
+        m = TrainingMetricsC()
+        arrs = [self._host_ptr(a) for a in (ori, dir_, target_rgba, bg_rgb)]
+        call("tn_trainer_train_step_rays", self._handle(), self.n_rays_per_step, *arrs, ctypes.byref(m))
+        return TrainingMetrics(m.step, m.loss, m.n_rays, m.n_samples)
+
+    @staticmethod
+    def _host_ptr(a):
+        try:
+            import torch
+            if isinstance(a, torch.Tensor):
+                if a.is_cuda or not a.is_contiguous() or a.dtype != torch.float32:
+                    raise ValueError("host rays must be contiguous float32 CPU tensors")
+                return ctypes.c_void_p(a.data_ptr())
+        except ImportError:
+            pass
+        a = np.ascontiguousarray(a, np.float32)
+        return a.ctypes.data_as(ctypes.c_void_p)
+
+    def sync_metrics(self) -> TrainingMetrics:
+        m = TrainingMetricsC()
+        call("tn_trainer_sync_metrics", self._handle(), ctypes.byref(m))
+        return TrainingMetrics(m.step, m.loss, m.n_rays, m.n_samples)
+
+    def update_occupancy_grid(self, training_step: int) -> OccupancyGridMetrics:
+        m = OccupancyMetricsC()
+        call("tn_trainer_update_occupancy_grid", self._handle(), int(training_step), ctypes.byref(m))
+        return OccupancyGridMetrics(m.n_occupied, m.n_total)
+
+    # -- introspection -------------------------------------------------------------------
+    def profile_step(self) -> list[float]:
+        out = (ctypes.c_float * 8)()
+        n = ctypes.c_uint32(0)
+        call("tn_trainer_profile_step", self._handle(), out, 8, ctypes.byref(n))
+        return [out[i] for i in range(n.value)]
+
+    def stat(self, which: int) -> int:
+        v = ctypes.c_uint64(0)
+        call("tn_trainer_stat", self._handle(), which, ctypes.byref(v))
+        return v.value
+
+    def stream_handle(self) -> int:
+        s = ctypes.c_void_p()
+        call("tn_trainer_stream", self._handle(), ctypes.byref(s))
+        return s.value or 0
+
+    def buffer(self, which: int, dtype=np.float32, count: int | None = None):
+        """A device buffer of the trainer as a torch tensor view (no copy)."""
+        import torch
+        p = ctypes.c_void_p()
+        nbytes = ctypes.c_uint64(0)
+        call("tn_trainer_buffer", self._handle(), which, ctypes.byref(p), ctypes.byref(nbytes))
+        itemsize = np.dtype(dtype).itemsize
+        n = count if count is not None else nbytes.value // itemsize
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (n,), "typestr": np.dtype(dtype).str, "data": (p.value, False),
+                                        "version": 3}
+
+        return torch.as_tensor(_View(), device="cuda")
