@@ -4,9 +4,9 @@ Workload (one step): 2^14 synthetic rays (origins on a radius-4 sphere, directio
 the centre + N(0, 0.05)) through a 5-cascade 128^3 occupancy grid built from an 8-blob
 Gaussian field (base size 1: extents 1..16) -> march count + batch cut at 2^18 samples ->
 march emit -> field (network stand-in) -> reconstruction + distortion (lambda 1e-3) loss
-forward/backward with the gradient merge -> occupancy EMA (decay 0.95, threshold 0.01,
-2^16 random cells re-sampled) -> Adam (beta1 0.9, beta2 0.99, eps 1e-15, lr 1e-2) over
-16 x 2^19 x 2 hash-grid + 7168 MLP parameters with fixed sparse synthetic gradients.
+forward/backward with the gradient merge -> Adam (beta1 0.9, beta2 0.99, eps 1e-15,
+lr 1e-2) over 16 x 2^19 x 2 hash-grid + 7168 MLP parameters with fixed sparse synthetic
+gradients -> occupancy EMA (decay 0.95, threshold 0.01, 2^16 random cells re-sampled).
 
 Prints ONE JSON line. `value` = samples/s of the fused, CUDA-graph-captured step with
 inputs resident in HBM; `e2e` = the same through Trainer.train_step_rays() with host rays
@@ -139,7 +139,7 @@ def stage_bytes(n_rays_gen, n_rays, n_samples, n_touched, levels=5, volume=128 *
     }
 
 
-STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "network_backward", "occupancy", "adam"]
+STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "network_backward", "adam", "occupancy"]
 
 
 def run_ours(args):

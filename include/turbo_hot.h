@@ -137,8 +137,9 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
  * src/utils/training-batch-kernels.cuh:339-481): for rays [0, batch_info[0]) writes
  * offsets[ray] and, per sample at offsets[ray] + j: t, pos[3] (normalised to [0,1]),
  * dir[3] (0.5*d+0.5), dt (= dt/aabb_size, the compositor's dt), m_norm, dt_norm and
- * img_id (optional, from ray_img_id). Rays at or beyond the cut get offsets = total
- * so that downstream kernels see empty ranges. */
+ * img_id (optional, from ray_img_id). offsets holds the exclusive scan of n_steps for all
+ * n_rays rays (rays at or beyond the cut emit nothing). Must follow tn_march_count on the
+ * same context with the same n_rays: it expands the step positions that pass recorded. */
 int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, const uint8_t* bitfield,
                   const tn_bbox* bbox, const tn_march_desc* march, float inv_aabb_size, uint32_t n_rays,
                   uint32_t ray_stride, uint32_t sample_stride, const uint32_t* batch_info,
@@ -386,7 +387,7 @@ int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori
                                const float* target_rgba, const float* bg_rgb, tn_training_metrics* metrics);
 /* Runs one fused step eagerly with events between its stages and writes the stage times
  * (ms): rays, march count, march emit, network forward, losses, network backward,
- * occupancy, Adam. */
+ * Adam, occupancy. */
 int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages);
 /* 0/1: kernel nodes in the captured step graph (synthetic / caller rays), 2: graph nodes,
  * 3: samples processed so far, 4: rays used so far, 5: steps (3-5 synchronise). */

@@ -78,10 +78,13 @@ def assert_norm_close(gpu, ref, rtol, what, mask=None):
     return err
 
 
-def assert_per_ray_norm_close(gpu, ref, counts, offsets, rtol, what, ray_mask=None):
-    """Normwise relative error of each ray's gradient vector (over that ray's samples)."""
+def assert_per_ray_norm_close(gpu, ref, counts, offsets, rtol, what, ray_mask=None, floor=FLOOR):
+    """Normwise relative error of each ray's gradient vector (over that ray's samples).
+    A ray whose whole gradient is below `floor` times the batch's largest entry (it
+    underflows in FP32) is measured against that floor instead."""
     g = np.asarray(gpu, dtype=np.float64)
     r = np.asarray(ref, dtype=np.float64)
+    batch_floor = floor * float(np.max(np.abs(r))) if r.size else 0.0
     worst = 0.0
     for i in range(len(counts)):
         if ray_mask is not None and not ray_mask[i]:
@@ -90,7 +93,7 @@ def assert_per_ray_norm_close(gpu, ref, counts, offsets, rtol, what, ray_mask=No
         if c == 0:
             continue
         rr = r[o:o + c]
-        m = np.max(np.abs(rr))
+        m = max(float(np.max(np.abs(rr))), batch_floor)
         if m == 0:
             continue
         worst = max(worst, float(np.max(np.abs(g[o:o + c] - rr)) / m))

@@ -1,0 +1,75 @@
+"""The CUDA library against the committed golden fixtures (tests/golden/*.npz, written by the
+oracle): march outputs and occupancy update bit-exact, losses and gradients within the
+parity tolerances. Runs without the oracle library."""
+import os
+
+import numpy as np
+import pytest
+
+from tests.helpers import RTOL_GRAD, assert_bitwise, assert_close, assert_norm_close, dev, expand_rays, host, i32
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _load(name):
+    return dict(np.load(os.path.join(HERE, name + ".npz")))
+
+
+def test_march_matches_golden():
+    from turbonerf_b200 import hotpath as hp
+    fx = _load("march_small")
+    n = fx["ori"].size // 3
+    g = hp.GridSpec(int(fx["n_levels"]), int(fx["res"]), float(fx["base"]))
+    m = hp.MarchSpec(float(fx["cone"]), float(fx["dt_min"]), float(fx["dt_max"]), 0)
+    bbox = tuple(float(v) for v in fx["bbox"])
+    batch = int(fx["batch"])
+    ctx = hp.Context()
+    alive = dev(fx["alive_in"].copy())
+    ori, dr, t, tmax = dev(fx["ori"]), dev(fx["dir"]), dev(fx["t"]), dev(fx["t_max"])
+    bits = dev(fx["bitfield"])
+    n_steps, info = hp.march_count(ctx, g, bits, bbox, m, n, n, ori, dr, t, tmax, alive, batch)
+    offsets, smp = hp.march_emit(ctx, g, bits, bbox, m, 0.25, n, n, batch + 1, info, ori, dr, t, alive, n_steps)
+    ctx.check()
+    info_h = host(info).view(np.uint32)
+    ns = int(fx["n_samples"])
+    assert (int(info_h[0]), int(info_h[1])) == (int(fx["n_rays"]), ns)
+    assert_bitwise(host(n_steps).view(np.uint32), fx["n_steps"], "n_steps")
+    assert_bitwise(host(alive), fx["alive"], "alive")
+    assert_bitwise(host(offsets).view(np.uint32), fx["offsets"], "offsets")
+    for k in ("t", "dt", "m_norm", "dt_norm"):
+        assert_bitwise(host(smp[k])[:ns], fx["s_" + k], k)
+    assert_bitwise(host(smp["pos"]).reshape(3, batch + 1)[:, :ns].ravel(), fx["s_pos"].ravel(), "pos")
+
+
+def test_losses_match_golden():
+    from turbonerf_b200 import hotpath as hp
+    fx = _load("loss_small")
+    n, ss = fx["counts"].size, fx["sigma"].size
+    ctx = hp.Context()
+    rb = hp.ray_batch(i32(fx["counts"]), i32(fx["offsets"]), n, n, ss)
+    out = hp.recon_loss_fwd_bwd(ctx, rb, dev(fx["sigma"]), dev(fx["rgb"]), dev(fx["dt"]), dev(fx["target"]),
+                                dev(fx["bg"]), inv_nrays=1.0 / n)
+    ok = fx["ambiguous"] == 0
+    for c in range(4):
+        assert_close(host(out["ray_rgba"])[c * n:(c + 1) * n], fx["ray_rgba"][c * n:(c + 1) * n], 1e-5, "rgba",
+                     mask=ok)
+    sm = expand_rays(ok, fx["counts"], fx["offsets"], ss)
+    assert_norm_close(host(out["dL_ddensity"]), fx["dL_ddensity"], RTOL_GRAD, "dL/ddensity", mask=sm)
+    assert_norm_close(host(out["dL_drgb"]), fx["dL_drgb"], RTOL_GRAD, "dL/drgb", mask=np.tile(sm, 3))
+    d = hp.distortion_fwd_bwd(ctx, rb, dev(fx["sigma"]), dev(fx["m_norm"]), dev(fx["dt_norm"]), 1e-3)
+    assert_norm_close(host(d["ray_loss"]), fx["dist_loss"], 1e-4, "distortion loss")
+    assert_norm_close(host(d["dL_ddensity"]), fx["dist_dd"], RTOL_GRAD, "distortion gradient")
+
+
+def test_occupancy_matches_golden():
+    from turbonerf_b200 import hotpath as hp
+    fx = _load("occupancy_small")
+    L, res = fx["density"].shape[0], 16
+    ctx = hp.Context()
+    d, b = dev(fx["density"].ravel().copy()), dev(fx["bitfield"].copy())
+    nocc = hp.occupancy_update(ctx, hp.GridSpec(L, res, 1.0), d, b, dev(fx["levels"]), i32(fx["cells"]),
+                               dev(fx["values"]), dev(fx["rsel"]))
+    assert_bitwise(host(d), fx["out_density"].ravel(), "density")
+    assert_bitwise(host(b), fx["out_bitfield"], "bitfield")
+    assert int(host(nocc)[0]) == int(fx["n_occupied"])

@@ -92,12 +92,15 @@ def test_adam_matches_fp64(plain):
                          l2=f32(1e-6))
         hp.adam_step(w, dev(g), m, v, steps, n_grid, n_mlp, lr=lr, beta2=0.99, weights_copy=wcopy, plain=plain)
     assert_bitwise(host(steps).view(np.uint32), state["steps"], "per-parameter steps")
-    # each weight moved by about 4 * lr: its error is measured against that displacement
-    err_w = np.abs(host(w).astype(np.float64) - state["w"]) / (np.abs(state["w"] - w0) + 1e-30)
-    touched = state["steps"] > 0
-    assert float(err_w[touched].max()) <= 1e-4, float(err_w[touched].max())
+    # Adam moves a weight by about lr per step whatever the gradient's scale: the weight error
+    # is measured against that step size (4 steps of lr = 1e-2)
+    err_w = np.abs(host(w).astype(np.float64) - state["w"]) / (4 * 1e-2)
+    assert float(err_w.max()) <= 1e-5, float(err_w.max())
     assert_norm_close(host(m), state["m"], 1e-5, "first moments")
     assert_norm_close(host(v), state["v"], 1e-5, "second moments")
     touched = state["steps"] > 0
     assert_bitwise(host(wcopy)[touched], host(w)[touched], "weights copy")
-    assert not np.any(host(wcopy)[~touched])  # never-updated parameters keep their old copy
+    # a never-updated parameter keeps its old copy (0 here) or, when it shares a 16-byte quad
+    # with updated ones, receives its unchanged weight
+    wc, ww = host(wcopy)[~touched], host(w)[~touched]
+    assert np.all((wc == 0) | (wc == ww))

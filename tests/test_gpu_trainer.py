@@ -76,9 +76,7 @@ def test_fused_step_matches_oracle_stage_by_stage():
     oracle.adam_step(state, g, 16 * (1 << 15) * 2, 7168, lr=f32(1e-2), beta1=f32(0.9), beta2=f32(0.99),
                      eps=f32(1e-15), l2=f32(1e-6))
     w = _h(tr.buffer(0)).astype(np.float64)
-    moved = np.abs(state["w"] - _h(w0))
-    t = state["steps"] > 0
-    assert float((np.abs(w - state["w"])[t] / moved[t]).max()) <= 1e-4
+    assert float(np.abs(w - state["w"]).max()) <= 1e-5 * 1e-2  # against one step of lr = 1e-2
     assert_bitwise(_h(tr.buffer(4), np.uint32), state["steps"], "param steps")
     tr.teardown()
 

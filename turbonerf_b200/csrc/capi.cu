@@ -66,6 +66,8 @@ static int ensure(T*& ptr, size_t& cap, size_t n, const char* what) {
 
 int ensure_block_u32(tn_ctx* ctx, size_t n) { return ensure(ctx->block_u32, ctx->block_u32_cap, n, "scratch(u32)"); }
 int ensure_block_f32(tn_ctx* ctx, size_t n) { return ensure(ctx->block_f32, ctx->block_f32_cap, n, "scratch(f32)"); }
+int ensure_mip(tn_ctx* ctx, size_t bytes) { return ensure(ctx->mip, ctx->mip_cap, bytes, "scratch(mip)"); }
+int ensure_slots(tn_ctx* ctx, size_t n) { return ensure(ctx->slots, ctx->slots_cap, n, "scratch(slots)"); }
 
 int validate_grid(const tn_grid_desc* grid) {
     TN_REQUIRE(grid != nullptr, TN_E_NULL, "grid descriptor is NULL");
@@ -112,6 +114,8 @@ int tn_ctx_destroy(tn_ctx* ctx) {
     cudaFree(ctx->tickets);
     cudaFree(ctx->block_u32);
     cudaFree(ctx->block_f32);
+    cudaFree(ctx->mip);
+    cudaFree(ctx->slots);
     delete ctx;
     return TN_OK;
 }
@@ -122,6 +126,14 @@ int tn_ctx_reserve(tn_ctx* ctx, uint32_t max_rays, uint32_t max_samples) {
     const size_t blocks = (size_t)max_rays / 64 + (size_t)max_samples / 1024 + 1024;
     int st = ensure_block_u32(ctx, 2 * blocks);
     if (st == TN_OK) st = ensure_block_f32(ctx, 8 * blocks);
+    // march scratch: the 128^3 coarse mip and the step-position slots (16 Mi floats at most)
+    if (st == TN_OK) st = ensure_mip(ctx, 32u * 1024u);
+    if (st == TN_OK && max_rays) {
+        size_t per = (16u << 20) / max_rays;
+        if (per > 1024) per = 1024;
+        if (per < 16) per = 16;
+        st = ensure_slots(ctx, per * max_rays);
+    }
     if (st == TN_OK) st = cuda_status(cudaDeviceSynchronize(), "tn_ctx_reserve");
     return st;
 }

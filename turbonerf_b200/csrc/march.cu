@@ -1,11 +1,14 @@
 // Occupancy-grid ray marching with sample compaction.
 //
-// Fused path (tn_march_count + tn_march_emit): two launches, no host round trip.
-//  * count: one thread per ray replays the reference's DDA loop exactly; each 128-ray block
-//    reduces its counts; the last block to finish (ticket) scans the block totals and
-//    performs the reference's batch cut on the device (batch_info).
-//  * emit: the same 128-ray blocks rebuild their rays' offsets from the block prefixes
-//    with a block scan, write them, and replay the march writing the packed samples.
+// Fused path (tn_march_count + tn_march_emit): no host round trip, one sequential march.
+//  * count: one thread per ray runs the reference's DDA loop exactly, with a coarse occupancy
+//    mip staged in shared memory to answer empty blocks without a global load, and records
+//    the t of every occupied step in a per-ray slot; each 128-ray block reduces its counts;
+//    the last block to finish (ticket) scans the block totals and performs the reference's
+//    batch cut on the device (batch_info).
+//  * emit: the same 128-ray blocks rebuild their rays' offsets with a block scan, then expand
+//    the recorded steps into the packed sample arrays, one warp per ray and one lane per
+//    sample (coalesced stores), instead of replaying the march.
 // Plain path (tn_plain_*): count kernel, thrust exclusive_scan, reverse find_if, a
 // blocking device->host read of the sample count, emit kernel -- the reference's launch
 // structure (src/core/trainer.cu:106-216).
@@ -28,9 +31,16 @@ struct MarchArgs {
     uint32_t max_steps, max_iters;
 };
 
-__device__ __forceinline__ bool occupied_at(const GridView& g, int k, float x, float y, float z) {
+// Occupancy test (OccupancyGrid::is_occupied_at, src/core/occupancy-grid.cuh:185-207). With a
+// coarse mip (one byte per 4x4x4 block of cells = 64 consecutive Morton indices, bit k set when
+// any cell of the block is occupied at level k) held in shared memory, an empty block answers
+// without touching the fine bitfield; the result is identical by construction.
+__device__ __forceinline__ bool occupied_at(const GridView& g, int k, float x, float y, float z,
+                                           const uint8_t* __restrict__ mip) {
     const uint32_t idx = voxel_morton(g, k, x, y, z);
-    return (__ldg(g.bits + idx) & (uint8_t)(1u << k)) != 0;
+    const uint8_t bit = (uint8_t)(1u << k);
+    if (mip && !(mip[idx >> 6] & bit)) return false;
+    return (__ldg(g.bits + idx) & bit) != 0;
 }
 
 __device__ __forceinline__ void load_ray(RayMarch& r, const float* __restrict__ ori, const float* __restrict__ dir,
@@ -42,8 +52,12 @@ __device__ __forceinline__ void load_ray(RayMarch& r, const float* __restrict__ 
     r.idz = __fdiv_rn(1.0f, r.dz);
 }
 
-// march_and_count_steps_per_ray_kernel loop, src/utils/training-batch-kernels.cuh:258-297
-__device__ uint32_t march_count_ray(const MarchArgs& a, RayMarch& r, float t_max, uint32_t* flags) {
+// march_and_count_steps_per_ray_kernel loop, src/utils/training-batch-kernels.cuh:258-297.
+// When `slots` is set, the t of the first `slot_cap` occupied steps is recorded so that the
+// emit pass can expand the samples without replaying the march.
+__device__ uint32_t march_count_ray(const MarchArgs& a, RayMarch& r, float t_max, uint32_t* flags,
+                                    const uint8_t* __restrict__ mip = nullptr, float* __restrict__ slots = nullptr,
+                                    uint32_t slot_cap = 0) {
     uint32_t n = 0, iters = 0;
     float t = r.t;
     while (t < t_max) {
@@ -53,7 +67,8 @@ __device__ uint32_t march_count_ray(const MarchArgs& a, RayMarch& r, float t_max
         if (!bbox_contains(a.bbox, x, y, z)) break;
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
         const int k = grid_level_at(a.g, x, y, z, dt);
-        if (occupied_at(a.g, k, x, y, z)) {
+        if (occupied_at(a.g, k, x, y, z, mip)) {
+            if (n < slot_cap) slots[n] = t;
             t = __fadd_rn(t, dt);
             ++n;
             if (a.max_steps != 0u && n >= a.max_steps) break;
@@ -113,7 +128,7 @@ __device__ void march_emit_ray(const MarchArgs& a, RayMarch& r, uint32_t n_steps
             continue;
         }
         const int k = grid_level_at(a.g, x, y, z, dt);
-        if (occupied_at(a.g, k, x, y, z)) {
+        if (occupied_at(a.g, k, x, y, z, nullptr)) {
             o.t[s] = t;
             o.m_norm[s] = __fadd_rn(t, __fmul_rn(0.5f, dt));
             o.dt_norm[s] = dt;
@@ -228,7 +243,15 @@ count_kernel(MarchArgs a, uint32_t n_rays, const uint32_t* __restrict__ n_rays_d
              const float* __restrict__ ori, const float* __restrict__ dir, const float* __restrict__ ray_t,
              const float* __restrict__ ray_t_max, uint8_t* __restrict__ alive, uint32_t* counts,
              uint32_t batch_size, uint32_t* batch_info, uint32_t* block_agg, uint32_t* block_prefix,
-             uint32_t* ticket, uint32_t* flags) {
+             uint32_t* ticket, uint32_t* flags, const uint8_t* __restrict__ mip_g, uint32_t mip_bytes,
+             float* __restrict__ slots, uint32_t slot_cap) {
+    extern __shared__ __align__(16) uint8_t mip_s[];
+    if (MARCH && mip_g) {
+        // stage the coarse occupancy mip (mip_bytes is a multiple of 16)
+        for (uint32_t k = threadIdx.x; k < mip_bytes / 16; k += MARCH_BLOCK)
+            reinterpret_cast<uint4*>(mip_s)[k] = __ldg(reinterpret_cast<const uint4*>(mip_g) + k);
+        __syncthreads();
+    }
     const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
     const uint32_t i = blockIdx.x * MARCH_BLOCK + threadIdx.x;
     uint32_t cnt = 0;
@@ -238,7 +261,8 @@ count_kernel(MarchArgs a, uint32_t n_rays, const uint32_t* __restrict__ n_rays_d
                 RayMarch r;
                 load_ray(r, ori, dir, i, rs);
                 r.t = ray_t[i];
-                cnt = march_count_ray(a, r, ray_t_max[i], flags);
+                cnt = march_count_ray(a, r, ray_t_max[i], flags, mip_g ? mip_s : nullptr,
+                                      slots ? slots + (size_t)i * slot_cap : nullptr, slots ? slot_cap : 0u);
                 if (cnt == 0) alive[i] = 0;
             }
             counts[i] = cnt;
@@ -291,6 +315,86 @@ emit_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __rest
     load_ray(r, ori, dir, i, rs);
     r.t = ray_t[i];
     march_emit_ray(a, r, cnt, off, img_id ? img_id[i] : 0u, inv_aabb, o);
+}
+
+// Emit pass from the recorded step positions: the 128-ray block of the count pass rebuilds its
+// offsets, then each warp expands one ray at a time with one lane per sample (coalesced
+// stores of the packed sample arrays). Every value is the one the reference's emit loop
+// (training-batch-kernels.cuh:412-480) computes from the same t: dt = get_dt(t), the position
+// o + t d, m = t + dt/2, the ray's span from its start t to the end of its last step.
+// Rays with more samples than slots fall back to replaying their march.
+__global__ void __launch_bounds__(MARCH_BLOCK)
+expand_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
+              const uint32_t* __restrict__ batch_info, const uint32_t* __restrict__ block_prefix,
+              const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
+              const float* __restrict__ ray_t, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ counts,
+              uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags, const float* __restrict__ slots,
+              uint32_t slot_cap) {
+    __shared__ uint32_t off_s[MARCH_BLOCK], cnt_s[MARCH_BLOCK];
+    const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
+    const uint32_t base = blockIdx.x * MARCH_BLOCK;
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t c = i < n_live ? counts[i] : 0u;
+    uint32_t tot;
+    const uint32_t off = block_exclusive_scan(c, &tot) + block_prefix[blockIdx.x];
+    const uint32_t n_cut = batch_info[0];
+    off_s[threadIdx.x] = off;
+    cnt_s[threadIdx.x] = (i < n_live && i < n_cut && c != 0 && alive[i]) ? c : 0u;
+    if (i < n_live) offsets[i] = off;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const size_t ss = o.ss;
+    for (int k = 0; k < WARP; ++k) {
+        const int local = wid * WARP + k;
+        const uint32_t n = cnt_s[local];
+        if (n == 0) continue;
+        const uint32_t r_i = base + local;
+        const uint32_t o0 = off_s[local];
+        if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
+            if (lane == 0) raise_flag(flags, ERR_CAPACITY);
+            continue;
+        }
+        RayMarch r;
+        load_ray(r, ori, dir, r_i, rs);
+        r.t = ray_t[r_i];
+        const uint32_t img = img_id ? img_id[r_i] : 0u;
+        if (n > slot_cap) {
+            if (lane == 0) march_emit_ray(a, r, n, o0, img, inv_aabb, o);
+            continue;
+        }
+        const float* sl = slots + (size_t)r_i * slot_cap;
+        const float t_last = sl[n - 1];
+        const float t_end = __fadd_rn(t_last, get_dt(t_last, a.cone, a.dt_min, a.dt_max));
+        const float t_span = fmaxf(__fadd_rn(t_end, -r.t), 1e-6f);
+        for (uint32_t j = lane; j < n; j += WARP) {
+            const float t = sl[j];
+            const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
+            float x, y, z;
+            ray_point(r, t, x, y, z);
+            const uint32_t s = o0 + j;
+            o.t[s] = t;
+            const float m = __fadd_rn(t, __fmul_rn(0.5f, dt));
+            o.m_norm[s] = clamp_ref(__fdiv_rn(__fadd_rn(m, -r.t), t_span), 0.0f, 1.0f);
+            o.dt_norm[s] = __fdiv_rn(dt, t_span);
+            if (o.img_id) o.img_id[s] = img;
+            write_sample(o, s, x, y, z, r, dt, inv_aabb);
+        }
+    }
+    (void)ss;
+}
+
+// Coarse occupancy mip: byte c = OR of the 64 fine bytes [64c, 64c + 64) (one 4x4x4 block).
+__global__ void build_mip_kernel(uint32_t n_coarse, const uint32_t* __restrict__ bits4, uint8_t* __restrict__ mip) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_coarse) return;
+    const uint4* p = reinterpret_cast<const uint4*>(bits4) + (size_t)c * 4;
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint4 q = __ldg(p + k);
+        v |= q.x | q.y | q.z | q.w;
+    }
+    mip[c] = (uint8_t)((v | (v >> 8) | (v >> 16) | (v >> 24)) & 0xFFu);
 }
 
 // ---- compaction: ascending indices of non-zero values ---------------------------------
@@ -394,6 +498,19 @@ __global__ void rays_init_kernel(uint32_t n, uint32_t rs, tn_bbox b, float t_far
     alive[i] = 1;
 }
 
+// Shared memory available for the coarse mip of the count pass (128^3 cells -> 32 KiB).
+constexpr uint32_t MIP_SMEM_MAX = 48u * 1024u;
+// Budget of the per-ray step-position slots (floats).
+constexpr size_t SLOT_BUDGET = 16u << 20;
+
+static uint32_t slot_capacity(uint32_t n_rays, uint32_t max_steps) {
+    size_t cap = SLOT_BUDGET / (n_rays ? n_rays : 1);
+    if (cap > 1024) cap = 1024;
+    if (max_steps && cap > max_steps) cap = max_steps;
+    if (cap < 16) cap = 16;
+    return (uint32_t)cap;
+}
+
 static int make_march_args(const tn_grid_desc* grid, const uint8_t* bitfield, const tn_bbox* bbox,
                            const tn_march_desc* march, MarchArgs& a) {
     int st = validate_grid(grid);
@@ -445,9 +562,31 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     const uint32_t nb = (n_rays + MARCH_BLOCK - 1) / MARCH_BLOCK;
     st = ensure_block_u32(ctx, 2 * (size_t)nb);
     if (st != TN_OK) return st;
-    count_kernel<true><<<nb, MARCH_BLOCK, 0, stream>>>(a, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t, ray_t_max,
-                                                       alive, n_steps, batch_size, batch_info, ctx->block_u32,
-                                                       ctx->block_u32 + nb, ctx->tickets + TICKET_MARCH, ctx->flags);
+    // coarse mip of the bitfield (staged in shared memory by the count pass)
+    const uint32_t volume = (uint32_t)grid->resolution * grid->resolution * grid->resolution;
+    const uint32_t mip_bytes = volume / 64;
+    const bool use_mip = grid->resolution >= 8 && mip_bytes <= MIP_SMEM_MAX;
+    if (use_mip) {
+        st = ensure_mip(ctx, mip_bytes);
+        if (st != TN_OK) return st;
+        TN_REQUIRE(((uintptr_t)bitfield & 15u) == 0, TN_E_INVALID, "bitfield must be 16-byte aligned");
+        build_mip_kernel<<<(mip_bytes + 255) / 256, 256, 0, stream>>>(mip_bytes, reinterpret_cast<const uint32_t*>(bitfield),
+                                                                      ctx->mip);
+        st = check_launch("tn_march_count(mip)");
+        if (st != TN_OK) return st;
+    }
+    // per-ray step positions for the emit pass
+    const uint32_t slot_cap = slot_capacity(n_rays, march->max_steps);
+    st = ensure_slots(ctx, (size_t)n_rays * slot_cap);
+    if (st != TN_OK) return st;
+    ctx->slot_cap = slot_cap;
+    ctx->slot_rays = n_rays;
+    const size_t smem = use_mip ? mip_bytes : 0;
+    count_kernel<true><<<nb, MARCH_BLOCK, smem, stream>>>(a, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t, ray_t_max,
+                                                          alive, n_steps, batch_size, batch_info, ctx->block_u32,
+                                                          ctx->block_u32 + nb, ctx->tickets + TICKET_MARCH, ctx->flags,
+                                                          use_mip ? ctx->mip : nullptr, use_mip ? mip_bytes : 0u,
+                                                          ctx->slots, slot_cap);
     return check_launch("tn_march_count");
 }
 
@@ -468,11 +607,12 @@ int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, con
     TN_REQUIRE(n_rays > 0, TN_E_NO_RAYS, "tn_march_emit: n_rays = 0");
     TN_REQUIRE(ray_stride >= n_rays, TN_E_INVALID, "ray_stride %u < n_rays %u", ray_stride, n_rays);
     const uint32_t nb = (n_rays + MARCH_BLOCK - 1) / MARCH_BLOCK;
-    TN_REQUIRE(ctx->block_u32_cap >= 2 * (size_t)nb, TN_E_STATE, "tn_march_emit must follow tn_march_count on the same context");
+    TN_REQUIRE(ctx->block_u32_cap >= 2 * (size_t)nb && ctx->slot_rays == n_rays, TN_E_STATE,
+               "tn_march_emit must follow tn_march_count on the same context with the same n_rays");
     SampleOut o{out_img_id, out_t, out_pos, out_dir, out_dt, out_m_norm, out_dt_norm, sample_stride};
-    emit_kernel<true><<<nb, MARCH_BLOCK, 0, stream>>>(a, inv_aabb_size, n_rays, nullptr, ray_stride, batch_info,
-                                                      ctx->block_u32 + nb, ray_img_id, ori, dir, ray_t, alive,
-                                                      n_steps, offsets, o, ctx->flags);
+    expand_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(a, inv_aabb_size, n_rays, nullptr, ray_stride, batch_info,
+                                                  ctx->block_u32 + nb, ray_img_id, ori, dir, ray_t, alive, n_steps,
+                                                  offsets, o, ctx->flags, ctx->slots, ctx->slot_cap);
     return check_launch("tn_march_emit");
 }
 
@@ -487,7 +627,8 @@ int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t*
     count_kernel<false><<<nb, MARCH_BLOCK, 0, stream>>>(a, n, nullptr, n, nullptr, nullptr, nullptr, nullptr, nullptr,
                                                         const_cast<uint32_t*>(counts), batch_size, batch_info,
                                                         ctx->block_u32, ctx->block_u32 + nb,
-                                                        ctx->tickets + TICKET_SCAN, ctx->flags);
+                                                        ctx->tickets + TICKET_SCAN, ctx->flags, nullptr, 0u, nullptr,
+                                                        0u);
     st = check_launch("tn_scan_offsets(count)");
     if (st != TN_OK) return st;
     SampleOut o{};

@@ -59,6 +59,11 @@ __host__ __device__ __forceinline__ uint32_t morton3d(uint32_t x, uint32_t y, ui
 // ------------------------------------------------------------------------------------
 // Grid / march arithmetic (exact FP32, no contraction)
 // ------------------------------------------------------------------------------------
+constexpr int MAX_LEVELS = 8;
+
+// Per-level constants are computed once on the host with the same IEEE operations the
+// reference performs inline (level size base * 2^k, its reciprocal 1.0f / size, half size,
+// cell size size * (1/R)), so the kernels read them instead of re-deriving them per step.
 struct GridView {
     int n_levels;
     int res;
@@ -66,11 +71,13 @@ struct GridView {
     float inv_res;     // 1.0f / res_f
     float base;        // level k covers base * 2^k
     const uint8_t* __restrict__ bits;
+    float ls[MAX_LEVELS];      // level size
+    float inv_ls[MAX_LEVELS];  // 1.0f / level size
+    float half[MAX_LEVELS];    // 0.5f * level size
+    float cell[MAX_LEVELS];    // level size * inv_res (== inv_res * level size)
 };
 
-__device__ __forceinline__ float level_size(const GridView& g, int k) {
-    return __fmul_rn(g.base, (float)(1 << k));
-}
+__device__ __forceinline__ float level_size(const GridView& g, int k) { return g.ls[k]; }
 
 // tcnn::clamp(val, lo, hi) = val < lo ? lo : (hi < val ? hi : val)
 __device__ __forceinline__ float clamp_ref(float v, float lo, float hi) {
@@ -97,18 +104,17 @@ __device__ __forceinline__ uint32_t cell_coord(float x, float s, float res_f, in
 }
 
 __device__ __forceinline__ uint32_t voxel_morton(const GridView& g, int k, float x, float y, float z) {
-    const float s = __fdiv_rn(1.0f, level_size(g, k));
+    const float s = g.inv_ls[k];
     return morton3d(cell_coord(x, s, g.res_f, g.res), cell_coord(y, s, g.res_f, g.res), cell_coord(z, s, g.res_f, g.res));
 }
 
 // get_grid_level_at, src/core/occupancy-grid.cuh:232-248
 __device__ __forceinline__ int grid_level_at(const GridView& g, float x, float y, float z, float dt) {
-    const float ax = fabsf(x), ay = fabsf(y), az = fabsf(z);
-    for (int k = 0; k < g.n_levels; ++k) {
-        const float ls = level_size(g, k);
-        const float half = __fmul_rn(0.5f, ls);
-        const float cell = __fmul_rn(ls, g.inv_res);
-        if (ax < half && ay < half && az < half && cell > dt) return k;
+    const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));  // all three < half  <=>  max < half
+#pragma unroll
+    for (int k = 0; k < MAX_LEVELS; ++k) {
+        if (k >= g.n_levels) break;
+        if (m < g.half[k] && g.cell[k] > dt) return k;
     }
     return g.n_levels - 1;
 }
@@ -118,12 +124,11 @@ __device__ __forceinline__ float dt_to_next_voxel(const GridView& g, float px, f
                                                   float dx, float dy, float dz,
                                                   float idx, float idy, float idz,
                                                   float dt_min, int level) {
-    const float ls = level_size(g, level);
-    const float ils = __fdiv_rn(1.0f, ls);
+    const float ils = g.inv_ls[level];
     const float x = __fmul_rn(__fadd_rn(__fmul_rn(px, ils), 0.5f), g.res_f);
     const float y = __fmul_rn(__fadd_rn(__fmul_rn(py, ils), 0.5f), g.res_f);
     const float z = __fmul_rn(__fadd_rn(__fmul_rn(pz, ils), 0.5f), g.res_f);
-    const float k = __fmul_rn(g.inv_res, ls);
+    const float k = g.cell[level];  // inv_res * level size
     const float tx = __fmul_rn(k, __fmul_rn(__fadd_rn(floorf(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, copysignf(1.0f, dx)), x), 0.5f)), -x), idx));
     const float ty = __fmul_rn(k, __fmul_rn(__fadd_rn(floorf(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, copysignf(1.0f, dy)), y), 0.5f)), -y), idy));
     const float tz = __fmul_rn(k, __fmul_rn(__fadd_rn(floorf(__fadd_rn(__fadd_rn(__fmul_rn(0.5f, copysignf(1.0f, dz)), z), 0.5f)), -z), idz));

@@ -18,6 +18,12 @@ struct tn_ctx {
     size_t block_u32_cap = 0;
     float* block_f32 = nullptr;         // per-block float partials
     size_t block_f32_cap = 0;
+    uint8_t* mip = nullptr;             // coarse occupancy mip built by tn_march_count
+    size_t mip_cap = 0;
+    float* slots = nullptr;             // per-ray step positions recorded by tn_march_count
+    size_t slots_cap = 0;
+    uint32_t slot_cap = 0;              // slots per ray of the last tn_march_count
+    uint32_t slot_rays = 0;             // n_rays of the last tn_march_count
 };
 
 namespace tn {
@@ -39,17 +45,29 @@ int cuda_status(cudaError_t e, const char* what);
 int check_launch(const char* what);
 int ensure_block_u32(tn_ctx* ctx, size_t n);
 int ensure_block_f32(tn_ctx* ctx, size_t n);
+int ensure_mip(tn_ctx* ctx, size_t bytes);
+int ensure_slots(tn_ctx* ctx, size_t n);
 bool stream_capturing(cudaStream_t s);
 int num_sms();
 
+// Host-side IEEE single arithmetic, identical to the device expressions they replace
+// (volatile keeps the compiler from folding or contracting them).
 inline GridView make_grid_view(const tn_grid_desc& d, const uint8_t* bits) {
-    GridView g;
+    GridView g{};
     g.n_levels = d.n_levels;
     g.res = d.resolution;
     g.res_f = (float)d.resolution;
-    g.inv_res = 1.0f / g.res_f;
+    volatile float one = 1.0f, halfc = 0.5f;
+    g.inv_res = one / g.res_f;
     g.base = d.base_size;
     g.bits = bits;
+    for (int k = 0; k < MAX_LEVELS; ++k) {
+        volatile float ls = g.base * (float)(1 << k);
+        g.ls[k] = ls;
+        g.inv_ls[k] = one / ls;
+        g.half[k] = halfc * ls;
+        g.cell[k] = ls * g.inv_res;
+    }
     return g;
 }
 

@@ -132,7 +132,7 @@ struct tn_trainer {
 namespace {
 
 // Stage boundaries of one fused step (for per-stage timing with events).
-enum Stage : int { ST_RAYS = 0, ST_COUNT, ST_EMIT, ST_FORWARD, ST_LOSSES, ST_BACKWARD, ST_OCCUPANCY, ST_ADAM, ST_N };
+enum Stage : int { ST_RAYS = 0, ST_COUNT, ST_EMIT, ST_FORWARD, ST_LOSSES, ST_BACKWARD, ST_ADAM, ST_OCCUPANCY, ST_N };
 
 int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
     const tn_trainer_desc& d = tr->d;
@@ -178,6 +178,14 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
         st = tr->net.backward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->grad_density,
                               tr->dl_drgb, tr->g);
     mark(ST_BACKWARD);
+    // Adam, then the occupancy update: the reference trains first and refreshes the grid after
+    // the step (update_occupancy_grid follows train_step, src/main.cu:157-166); the freshly
+    // written bitfield is then still in L2 for the next step's march.
+    if (st == TN_OK)
+        st = launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate,
+                         &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
+                         tr->steps);
+    mark(ST_ADAM);
     if (st == TN_OK && tr->M > 0) {
         st = launch_synth_cells(s, tr->M, d.seed, &tr->state->cur_step, grid.n_levels, tr->V, tr->occ_levels,
                                 tr->occ_cells, tr->occ_rand3, tr->M, tr->occ_rsel);
@@ -191,15 +199,10 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
                                          nullptr, d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied);
     }
     mark(ST_OCCUPANCY);
-    if (st == TN_OK)
-        st = launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate,
-                         &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
-                         tr->steps);
     if (st == TN_OK) {
         step_end_kernel<<<1, 1, 0, s>>>(tr->state);
         st = check_launch("step_end");
     }
-    mark(ST_ADAM);
     return st;
 }
 
@@ -247,6 +250,9 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
     if (st == TN_OK && tr->net.backward)
         st = tr->net.backward(tr->net.user, s, ns, nullptr, tr->B, tr->s_pos, tr->s_dir, tr->grad_density, tr->dl_drgb,
                               tr->g);
+    if (st == TN_OK)
+        st = launch_adam(s, true, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, lr, nullptr, d.beta1, d.beta2,
+                         d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v, tr->steps);
     if (st == TN_OK && tr->M > 0) {
         st = launch_synth_cells(s, tr->M, d.seed, &tr->state->cur_step, grid.n_levels, tr->V, tr->occ_levels,
                                 tr->occ_cells, tr->occ_rand3, tr->M, tr->occ_rsel);
@@ -260,9 +266,6 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
                                                 tr->occ_values, tr->occ_rsel, tr->net.activation, k < 256 ? 1 : 0,
                                                 d.occupancy_decay, d.occupancy_threshold, tr->count_scratch, &nocc);
     }
-    if (st == TN_OK)
-        st = launch_adam(s, true, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, lr, nullptr, d.beta1, d.beta2,
-                         d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v, tr->steps);
     if (st == TN_OK) {
         uint32_t info[2] = {nr, ns};
         st = cuda_status(cudaMemcpyAsync(tr->state->batch_info, info, sizeof(info), cudaMemcpyHostToDevice, s),
