@@ -107,8 +107,10 @@ def test_distortion_fused_and_plain(mean, n_samples):
     assert_norm_close(host(out["ray_loss"])[:n], ref_loss, 1e-4, "ray distortion loss")
     assert abs(float(host(out["loss_sum"])[0]) - ref_loss.mean()) <= 1e-5 * abs(ref_loss.mean())
     assert_norm_close(host(out["dL_ddensity"]), ref_dd, RTOL_GRAD, "dLdist/dsigma")
+    # per ray: dL/dsigma_j = dtn_j (g_j T_{j+1} - sum_{l>j} g_l w_l) keeps one intrinsic difference,
+    # so rays whose whole gradient is below 1e-3 of the batch's largest are measured against that
     assert_per_ray_norm_close(host(out["dL_ddensity"]), ref_dd, sb.counts, sb.offsets, RTOL_GRAD,
-                              "dLdist/dsigma per ray")
+                              "dLdist/dsigma per ray", floor=1e-3)
     ray_loss, dd, lsum = hp.plain_distortion(rb, dev(sb.sigma), dev(sb.m_norm), dev(sb.dt_norm), lam)
     assert abs(lsum - ref_loss.mean()) <= 1e-3 * abs(ref_loss.mean())
     assert ctx.check() == 0

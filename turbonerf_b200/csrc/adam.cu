@@ -6,6 +6,8 @@
 // four gradients are all zero is skipped without touching weights, moments or step
 // counters (the reference's per-parameter "zero gradient => return" rule, applied to whole
 // quads before any other load is issued). Mixed quads update only their active lanes.
+#include <cmath>
+
 #include "tn_internal.cuh"
 
 namespace tn {
@@ -13,17 +15,23 @@ namespace tn {
 struct AdamArgs {
     uint32_t n, n_grid, n_net_end;
     float inv_loss_scale, lr, beta1, beta2, eps, l2;
+    float log2_beta1, log2_beta2;  // log2 of beta1 / beta2 (host double, rounded once)
     const float* lr_dev;  // when set, the learning rate is read from device memory (graph replays)
 };
 
+// One parameter of ngp_adam_step (adam-optimizer.cuh:69-95). The bias corrections beta^step
+// are evaluated as exp2(step * log2(beta)) with log2(beta) prepared on the host, and the two
+// divisions of the update are merged into one.
 __device__ __forceinline__ void adam_one(const AdamArgs& a, float base_lr, uint32_t i, float g, float& w, float& m,
                                          float& v, uint32_t& step) {
     if (i >= a.n_grid && i < a.n_net_end) g += a.l2 * w;
     m = a.beta1 * m + (1.0f - a.beta1) * g;
     v = a.beta2 * v + (1.0f - a.beta2) * (g * g);
     step += 1u;
-    const float lr = base_lr * sqrtf(1.0f - powf(a.beta2, (float)step)) / (1.0f - powf(a.beta1, (float)step));
-    w = w - (lr / (sqrtf(v) + a.eps)) * m;
+    const float s = (float)step;
+    const float c1 = 1.0f - exp2f(s * a.log2_beta1);
+    const float c2 = 1.0f - exp2f(s * a.log2_beta2);
+    w = w - base_lr * sqrtf(c2) * m / (c1 * (sqrtf(v) + a.eps));
 }
 
 __global__ void __launch_bounds__(256)
@@ -117,6 +125,8 @@ static int adam_args(uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_sca
     a.beta2 = beta2;
     a.eps = eps;
     a.l2 = l2;
+    a.log2_beta1 = (float)std::log2((double)beta1);
+    a.log2_beta2 = (float)std::log2((double)beta2);
     a.lr_dev = nullptr;
     return TN_OK;
 }

@@ -200,10 +200,22 @@ __device__ __forceinline__ ReconGrad recon_loss_ray(const CompFwd& c, const floa
 }
 
 // ---- distortion -------------------------------------------------------------------------
-struct DistCarry { float x, w, wm; };
+// Loss of one ray (mipNeRF360_distortion_loss_forward_kernel, training-kernels-fused.cuh:13-120):
+//   L = lambda/N * ( (1/3) sum_j dtn_j w_j^2 + sum_{i,j} w_i w_j |m_i - m_j| )
+// with w_j = T_j alpha_j from sigma * dt_norm and no transmittance cut. The reference forms the
+// cross term as (sum wm_i W_{<i}) - (sum w_i WM_{<i}) and its gradient from suffix sums obtained
+// by subtraction (:204-212), which cancels catastrophically in FP32. Here the same quantities
+// are accumulated from non-negative terms only:
+//   A_j = sum_{l<j} w_l (m_j - m_l) = sum_{i<=j} (m_i - m_{i-1}) W_{<i}     (forward scan)
+//   B_j = sum_{l>j} w_l (m_l - m_j) = sum_{i>j}  (m_i - m_{i-1}) W_{>=i}    (reverse scan)
+//   cross = 2 sum_j w_j A_j,   dL/dw_j = lambda/N ((2/3) dtn_j w_j + 2 (A_j + B_j))
+//   dL/dsigma_j = dtn_j (dL/dw_j T_{j+1} - sum_{l>j} dL/dw_l w_l)
+// which is the reference's gradient (:188-223) written without cancelling sums (m is
+// non-decreasing along a ray, so every increment m_i - m_{i-1} is >= 0).
+struct DistCarry { float x, w, a, m; };
 
 struct DistChunk {
-    float dtn, m, w, wm, t_next, w_incl, w_excl, wm_incl, wm_excl, sigma;
+    float dtn, w, t_next, dm, a, sigma;
     bool valid;
 };
 
@@ -212,13 +224,13 @@ __device__ __forceinline__ DistChunk dist_chunk_forward(const Samples& S, uint32
     DistChunk d;
     const uint32_t j = base + lane;
     d.valid = j < n;
-    float x = 0.0f;
-    d.dtn = 0.0f; d.m = 0.0f; d.sigma = 0.0f;
+    float x = 0.0f, m = c.m;
+    d.dtn = 0.0f; d.sigma = 0.0f;
     if (d.valid) {
         const size_t s = (size_t)o + j;
         d.sigma = act_sigma(S.act, S.density[s]);
         d.dtn = S.dt_norm[s];
-        d.m = S.m_norm[s];
+        m = S.m_norm[s];
         x = d.sigma * d.dtn;
     }
     const float x_incl = warp_inclusive_sum(x, lane) + c.x;
@@ -227,14 +239,15 @@ __device__ __forceinline__ DistChunk dist_chunk_forward(const Samples& S, uint32
     const float tj = expf(-x_excl);
     d.w = d.valid ? tj * -em : 0.0f;
     d.t_next = tj * (1.0f + em);  // T_j (1 - alpha_j)
-    d.wm = d.w * d.m;
-    d.w_incl = warp_inclusive_sum(d.w, lane) + c.w;
-    d.w_excl = shift_up(d.w_incl, lane, c.w);
-    d.wm_incl = warp_inclusive_sum(d.wm, lane) + c.wm;
-    d.wm_excl = shift_up(d.wm_incl, lane, c.wm);
+    const float w_incl = warp_inclusive_sum(d.w, lane) + c.w;
+    const float w_excl = shift_up(w_incl, lane, c.w);
+    const float m_prev = shift_up(m, lane, c.m);
+    d.dm = d.valid ? fmaxf(m - m_prev, 0.0f) : 0.0f;
+    d.a = warp_inclusive_sum(d.dm * w_excl, lane) + c.a;  // A_j
     next.x = __shfl_sync(FULL_MASK, x_incl, WARP - 1);
-    next.w = __shfl_sync(FULL_MASK, d.w_incl, WARP - 1);
-    next.wm = __shfl_sync(FULL_MASK, d.wm_incl, WARP - 1);
+    next.w = __shfl_sync(FULL_MASK, w_incl, WARP - 1);
+    next.a = __shfl_sync(FULL_MASK, d.a, WARP - 1);
+    next.m = __shfl_sync(FULL_MASK, m, WARP - 1);
     return d;
 }
 
@@ -253,33 +266,39 @@ struct DistCarryStore {
         DistCarry v;
         v.x = __shfl_sync(FULL_MASK, s.x, src);
         v.w = __shfl_sync(FULL_MASK, s.w, src);
-        v.wm = __shfl_sync(FULL_MASK, s.wm, src);
+        v.a = __shfl_sync(FULL_MASK, s.a, src);
+        v.m = __shfl_sync(FULL_MASK, s.m, src);
         return v;
     }
 };
 
 struct DistFwd { float loss, k; };
 
+__device__ __forceinline__ DistCarry dist_first_carry(const Samples& S, uint32_t o, uint32_t n) {
+    // m_{-1} := m_0 so that the first increment is zero
+    DistCarry c{0.0f, 0.0f, 0.0f, 0.0f};
+    if (n) c.m = S.m_norm[o];
+    return c;
+}
+
 __device__ __forceinline__ DistFwd dist_forward_ray(const Samples& S, uint32_t o, uint32_t n, float lambda, int lane,
                                                     DistCarryStore& store) {
-    DistCarry c{0.0f, 0.0f, 0.0f};
-    float uni = 0.0f, b0 = 0.0f, b1 = 0.0f;
+    DistCarry c = dist_first_carry(S, o, n);
+    float uni = 0.0f, cross = 0.0f;
     uint32_t ci = 0;
     for (uint32_t base = 0; base < n; base += WARP, ++ci) {
         store.put(ci, lane, c);
         DistCarry nx;
         const DistChunk d = dist_chunk_forward(S, o, n, base, lane, c, nx);
         uni += d.dtn * d.w * d.w;
-        b0 += d.wm * d.w_excl;
-        b1 += d.w * d.wm_excl;
+        cross += d.w * d.a;
         c = nx;
     }
     uni = warp_sum(uni);
-    b0 = warp_sum(b0);
-    b1 = warp_sum(b1);
+    cross = warp_sum(cross);
     DistFwd f;
     f.k = n ? lambda / (float)n : 0.0f;
-    f.loss = f.k * ((1.0f / 3.0f) * uni + 2.0f * (b0 - b1));
+    f.loss = f.k * ((1.0f / 3.0f) * uni + 2.0f * cross);
     return f;
 }
 
@@ -296,34 +315,20 @@ __device__ DistCarry dist_replay_carry(const Samples& S, uint32_t o, uint32_t n,
     return c;
 }
 
-struct DistSuffix { float wm, wmW, w, wWM, dtw2; };
+// Reverse carries: W_{>=}, B (as the suffix sum of the increments' terms), sum g w.
+struct DistSuffix { float w, f, gw; };
 
-// mipNeRF360_distortion_loss_backward_kernel gradient (training-kernels-fused.cuh:188-223)
-// for one chunk, with the suffix sums obtained by reverse scans.
 __device__ __forceinline__ float dist_chunk_backward(const DistChunk& d, float k, int lane, DistSuffix& suf) {
-    const float a1 = d.wm, a2 = d.wm * d.w_excl, a3 = d.w, a4 = d.w * d.wm_excl, a5 = d.dtn * d.w * d.w;
-    const float i1 = warp_inclusive_suffix_sum(a1, lane) + suf.wm;
-    const float i2 = warp_inclusive_suffix_sum(a2, lane) + suf.wmW;
-    const float i3 = warp_inclusive_suffix_sum(a3, lane) + suf.w;
-    const float i4 = warp_inclusive_suffix_sum(a4, lane) + suf.wWM;
-    const float i5 = warp_inclusive_suffix_sum(a5, lane) + suf.dtw2;
-    const float s_wm = shift_down(i1, lane, suf.wm);
-    const float s_wmW = shift_down(i2, lane, suf.wmW);
-    const float s_w = shift_down(i3, lane, suf.w);
-    const float s_wWM = shift_down(i4, lane, suf.wWM);
-    const float s_dtw2 = shift_down(i5, lane, suf.dtw2);
-    suf.wm = __shfl_sync(FULL_MASK, i1, 0);
-    suf.wmW = __shfl_sync(FULL_MASK, i2, 0);
-    suf.w = __shfl_sync(FULL_MASK, i3, 0);
-    suf.wWM = __shfl_sync(FULL_MASK, i4, 0);
-    suf.dtw2 = __shfl_sync(FULL_MASK, i5, 0);
-    const float dw = d.dtn * d.t_next;
-    const float dwm = d.m * dw;
-    const float tw = d.t_next;
-    const float db0 = dwm * d.w_excl + d.dtn * (s_wm * (d.w_incl + tw) - 2.0f * s_wmW);
-    const float db1 = dw * d.wm_excl + d.dtn * (s_w * (d.m * tw + d.wm_incl) - 2.0f * s_wWM);
-    const float du = 2.0f * d.dtn * (d.dtn * d.w * tw - s_dtw2);
-    return k * (2.0f * (db0 - db1) + (1.0f / 3.0f) * du);
+    const float w_ge = warp_inclusive_suffix_sum(d.w, lane) + suf.w;       // W_{>=j}
+    const float f_incl = warp_inclusive_suffix_sum(d.dm * w_ge, lane) + suf.f;
+    const float b = shift_down(f_incl, lane, suf.f);                       // B_j
+    const float g = k * ((2.0f / 3.0f) * d.dtn * d.w + 2.0f * (d.a + b));   // dL/dw_j
+    const float gw_incl = warp_inclusive_suffix_sum(g * d.w, lane) + suf.gw;
+    const float gw_excl = shift_down(gw_incl, lane, suf.gw);               // sum_{l>j} g_l w_l
+    suf.w = __shfl_sync(FULL_MASK, w_ge, 0);
+    suf.f = __shfl_sync(FULL_MASK, f_incl, 0);
+    suf.gw = __shfl_sync(FULL_MASK, gw_incl, 0);
+    return d.valid ? d.dtn * (g * d.t_next - gw_excl) : 0.0f;
 }
 
 // ---- block-level deterministic sums (per-block partials, last block adds them) ---------
@@ -504,7 +509,7 @@ distortion_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, const uint3
         }
         if (!dd || n == 0) continue;
         const float gscale = grad_ray ? grad_ray[r] : 1.0f;
-        DistSuffix suf{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        DistSuffix suf{0.0f, 0.0f, 0.0f};
         const uint32_t nch = (n + WARP - 1) / WARP;
         for (int ci = (int)nch - 1; ci >= 0; --ci) {
             const DistCarry c = ci < SAVED_CHUNKS ? store.get((uint32_t)ci)
@@ -550,7 +555,7 @@ train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t 
         }
         if (n == 0) continue;
         float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
-        DistSuffix suf{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        DistSuffix suf{0.0f, 0.0f, 0.0f};
         const uint32_t nch = (n + WARP - 1) / WARP;
         for (int ci = (int)nch - 1; ci >= 0; --ci) {
             const uint32_t base = (uint32_t)ci * WARP;

@@ -81,6 +81,8 @@ __global__ void occ_scatter_kernel(uint32_t n, uint32_t volume, int n_levels, fl
 
 __device__ __forceinline__ float settle(float v, float decay) { return signbit(v) ? -v : v * decay; }
 
+// Issues every level's 16-byte load of the thread's four cells before using any of them, so
+// each thread keeps n_levels loads in flight.
 __global__ void __launch_bounds__(256)
 occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, uint8_t* __restrict__ bits,
                  float decay, float threshold, uint32_t* __restrict__ n_occupied) {
@@ -88,18 +90,25 @@ occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, ui
     uint32_t cnt = 0;
     if (i < volume4) {
         float4* d4 = reinterpret_cast<float4*>(density);
+        float4 v[MAX_LEVELS];
+#pragma unroll
+        for (int k = 0; k < MAX_LEVELS; ++k)
+            if (k < n_levels) v[k] = __ldcs(d4 + (size_t)k * volume4 + i);
         uint32_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
-        for (int k = 0; k < n_levels; ++k) {
-            float4 v = d4[(size_t)k * volume4 + i];
-            v.x = settle(v.x, decay);
-            v.y = settle(v.y, decay);
-            v.z = settle(v.z, decay);
-            v.w = settle(v.w, decay);
-            d4[(size_t)k * volume4 + i] = v;
-            b0 |= (uint32_t)(v.x > threshold) << k;
-            b1 |= (uint32_t)(v.y > threshold) << k;
-            b2 |= (uint32_t)(v.z > threshold) << k;
-            b3 |= (uint32_t)(v.w > threshold) << k;
+#pragma unroll
+        for (int k = 0; k < MAX_LEVELS; ++k) {
+            if (k < n_levels) {
+                float4 x = v[k];
+                x.x = settle(x.x, decay);
+                x.y = settle(x.y, decay);
+                x.z = settle(x.z, decay);
+                x.w = settle(x.w, decay);
+                __stcs(d4 + (size_t)k * volume4 + i, x);
+                b0 |= (uint32_t)(x.x > threshold) << k;
+                b1 |= (uint32_t)(x.y > threshold) << k;
+                b2 |= (uint32_t)(x.z > threshold) << k;
+                b3 |= (uint32_t)(x.w > threshold) << k;
+            }
         }
         const uint32_t packed = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
         reinterpret_cast<uint32_t*>(bits)[i] = packed;

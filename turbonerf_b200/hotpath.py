@@ -92,7 +92,11 @@ def bbox_desc(b) -> Bbox:
 
 def ray_batch(counts: torch.Tensor, offsets: torch.Tensor, n_rays: int, ray_stride: int, sample_stride: int,
               n_rays_dev: torch.Tensor | None = None) -> RayBatchDesc:
-    return RayBatchDesc(n_rays, ray_stride, sample_stride, 0, _ptr(counts), _ptr(offsets), _ptr(n_rays_dev))
+    """Descriptor of a packed batch. It holds references to the tensors whose device
+    pointers it carries, so they stay allocated for as long as the descriptor lives."""
+    rb = RayBatchDesc(n_rays, ray_stride, sample_stride, 0, _ptr(counts), _ptr(offsets), _ptr(n_rays_dev))
+    rb._keep = (counts, offsets, n_rays_dev)
+    return rb
 
 
 # ---- rays -------------------------------------------------------------------------------
