@@ -153,6 +153,19 @@ int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, con
 int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,
                     uint32_t batch_size, uint32_t* batch_info);
 
+/* Allocation-free variant of tn_scan_offsets, with the same outputs (offsets, batch_info),
+ * for callers that cannot allocate device memory and hold no tn_ctx: for instance a plugin
+ * whose host application owns every device allocation, or a loop that must not pay the
+ * device synchronisation of cudaMalloc. No counterpart in the reference (which has no such
+ * callers). Its scratch is a fixed array inside the library image, held by every device that
+ * loads the library until exit. Limit: n <= TN_SCAN_NOALLOC_MAX_COUNTS; larger n returns
+ * TN_E_CAPACITY. The first call on a device looks up the array's device address, so make
+ * that first call before any stream capture. All calls share the array: calls that overlap
+ * on the GPU race and must be serialised. */
+#define TN_SCAN_NOALLOC_MAX_COUNTS (1u << 21)
+int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,
+                            uint32_t batch_size, uint32_t* batch_info);
+
 /* Ascending list of the indices i < n with values[i] != 0 (reference
  * generate_nonzero_compaction_indices, src/utils/stream-compaction.cuh:120-139);
  * *count_dev receives the list length. */

@@ -18,6 +18,8 @@
 #include <thrust/scan.h>
 #include <thrust/device_ptr.h>
 
+#include <mutex>
+
 #include "tn_internal.cuh"
 
 namespace tn {
@@ -638,6 +640,43 @@ int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t*
     return check_launch("tn_scan_offsets(offsets)");
 }
 
+// ---- allocation-free scan + batch cut ------------------------------------------------
+// Some callers cannot allocate device memory: a plugin whose host application owns the
+// whole device heap and forbids extra allocations, or a loop that must not pay cudaMalloc's
+// implicit device synchronisation. For them this variant of tn_scan_offsets takes no tn_ctx:
+// its scratch (per-block totals and prefixes of the counts, the last-block ticket and an
+// error word) is a fixed array in device memory that lives in the library image itself and is
+// held by every device that loads the library until the process exits.
+//
+// Limit: at most TN_SCAN_NOALLOC_MAX_COUNTS counts per call (2 x 16,384 block entries =
+// 128 KiB of scratch). Every call uses the same array, so two calls that overlap on the GPU
+// (different streams, or different host threads on one device) race on it; serialise them.
+constexpr uint32_t NOALLOC_MAX_BLOCKS = TN_SCAN_NOALLOC_MAX_COUNTS / MARCH_BLOCK;
+constexpr uint32_t NOALLOC_WORDS = 2 * NOALLOC_MAX_BLOCKS + 64;  // [agg | prefix | ticket, flags, ...]
+static __device__ __align__(256) uint32_t g_scan_noalloc_scratch[NOALLOC_WORDS];
+
+// The array's name is a host-side stand-in in host code, not a device address: the device
+// address is looked up once per device (with that device current) and cached here.
+static uint32_t* g_scan_noalloc_ptr[64] = {};
+static std::mutex g_scan_noalloc_mutex;
+
+static int scan_noalloc_scratch(uint32_t** out) {
+    int dev = 0;
+    int st = cuda_status(cudaGetDevice(&dev), "tn_scan_offsets_noalloc: cudaGetDevice");
+    if (st != TN_OK) return st;
+    TN_REQUIRE(dev >= 0 && dev < 64, TN_E_INVALID, "tn_scan_offsets_noalloc: device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_scan_noalloc_mutex);
+    if (!g_scan_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        st = cuda_status(cudaGetSymbolAddress(&p, g_scan_noalloc_scratch),
+                         "tn_scan_offsets_noalloc: cudaGetSymbolAddress");
+        if (st != TN_OK) return st;
+        g_scan_noalloc_ptr[dev] = static_cast<uint32_t*>(p);
+    }
+    *out = g_scan_noalloc_ptr[dev];
+    return TN_OK;
+}
+
 int tn_compact_nonzero(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* values, int32_t* out,
                        uint32_t* count_dev) {
     TN_NONNULL(ctx); TN_NONNULL(values); TN_NONNULL(out); TN_NONNULL(count_dev);
@@ -651,6 +690,37 @@ int tn_compact_nonzero(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32
     if (st != TN_OK) return st;
     compact_write_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, values, ctx->block_u32 + nb, out);
     return check_launch("tn_compact_nonzero(write)");
+}
+
+int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,
+                            uint32_t batch_size, uint32_t* batch_info) {
+    TN_NONNULL(counts); TN_NONNULL(offsets); TN_NONNULL(batch_info);
+    TN_REQUIRE(n > 0, TN_E_NO_RAYS, "tn_scan_offsets_noalloc: n = 0");
+    TN_REQUIRE(n <= TN_SCAN_NOALLOC_MAX_COUNTS, TN_E_CAPACITY,
+               "tn_scan_offsets_noalloc: %u counts exceed the fixed scratch limit of %u (use tn_scan_offsets)", n,
+               (uint32_t)TN_SCAN_NOALLOC_MAX_COUNTS);
+    uint32_t* scratch = nullptr;
+    int st = scan_noalloc_scratch(&scratch);
+    if (st != TN_OK) return st;
+    uint32_t* block_agg = scratch;
+    uint32_t* block_prefix = scratch + NOALLOC_MAX_BLOCKS;
+    uint32_t* ticket = scratch + 2 * NOALLOC_MAX_BLOCKS;
+    uint32_t* flags = ticket + 1;
+    // the ticket must start at zero (the last block also leaves it at zero); clear the error word too
+    st = cuda_status(cudaMemsetAsync(ticket, 0, 2 * sizeof(uint32_t), stream), "tn_scan_offsets_noalloc: clear");
+    if (st != TN_OK) return st;
+    const uint32_t nb = (n + MARCH_BLOCK - 1) / MARCH_BLOCK;
+    MarchArgs a{};
+    count_kernel<false><<<nb, MARCH_BLOCK, 0, stream>>>(a, n, nullptr, n, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                        const_cast<uint32_t*>(counts), batch_size, batch_info,
+                                                        block_agg, block_prefix, ticket, flags, nullptr, 0u, nullptr,
+                                                        0u);
+    st = check_launch("tn_scan_offsets_noalloc(count)");
+    if (st != TN_OK) return st;
+    SampleOut o{};
+    emit_kernel<false><<<nb, MARCH_BLOCK, 0, stream>>>(a, 0.0f, n, nullptr, n, batch_info, block_prefix, nullptr,
+                                                       nullptr, nullptr, nullptr, nullptr, counts, offsets, o, flags);
+    return check_launch("tn_scan_offsets_noalloc(offsets)");
 }
 
 int tn_plain_march_count(tn_stream_t stream, const tn_grid_desc* grid, const uint8_t* bitfield, const tn_bbox* bbox,

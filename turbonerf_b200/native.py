@@ -125,6 +125,7 @@ SIGNATURES = {
     "tn_march_emit": [_vp, _vp, _P(GridDesc), _vp, _P(Bbox), _P(MarchDesc), _f32, _u32, _u32, _u32, _vp, _vp, _vp,
                       _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_scan_offsets": [_vp, _vp, _u32, _vp, _vp, _u32, _vp],
+    "tn_scan_offsets_noalloc": [_vp, _u32, _vp, _vp, _u32, _vp],
     "tn_compact_nonzero": [_vp, _vp, _u32, _vp, _vp, _vp],
     "tn_composite_fwd": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_composite_bwd": [_vp, _vp, _P(RayBatchDesc), _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
