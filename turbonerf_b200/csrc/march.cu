@@ -1,14 +1,16 @@
 // Occupancy-grid ray marching with sample compaction.
 //
 // Fused path (tn_march_count + tn_march_emit): no host round trip, one sequential march.
-//  * count: one thread per ray runs the reference's DDA loop exactly, with a coarse occupancy
-//    mip staged in shared memory to answer empty blocks without a global load, and records
-//    the t of every occupied step in a per-ray slot; each 128-ray block reduces its counts;
+//  * count: one thread per ray runs the reference's DDA loop with its exact arithmetic, written
+//    branch-free per step (both successors of t are computed, one is selected) so that a warp's
+//    rays never split. Shared memory holds a Morton spread table and a coarse occupancy mip
+//    that answers empty 4x4x4 blocks without a global load. A box holding every occupied cell
+//    ends each ray's loop where it leaves that box for good (the count cannot change after).
+//    The t of every occupied step goes to a per-ray slot. Each 64-ray block reduces its counts;
 //    the last block to finish (ticket) scans the block totals and performs the reference's
 //    batch cut on the device (batch_info).
-//  * emit: the same 128-ray blocks rebuild their rays' offsets with a block scan, then expand
-//    the recorded steps into the packed sample arrays, one warp per ray and one lane per
-//    sample (coalesced stores), instead of replaying the march.
+//  * emit: one warp per ray rebuilds the ray's offset and expands its recorded steps into the
+//    packed sample arrays, one lane per sample (coalesced stores), instead of replaying the march.
 // Plain path (tn_plain_*): count kernel, thrust exclusive_scan, reverse find_if, a
 // blocking device->host read of the sample count, emit kernel -- the reference's launch
 // structure (src/core/trainer.cu:106-216).
@@ -18,6 +20,7 @@
 #include <thrust/scan.h>
 #include <thrust/device_ptr.h>
 
+#include <cmath>
 #include <mutex>
 
 #include "tn_internal.cuh"
@@ -30,19 +33,14 @@ struct MarchArgs {
     GridView g;
     tn_bbox bbox;
     float cone, dt_min, dt_max;
+    float inv_dt_min;  // 1 / dt_min rounded to nearest (host division)
     uint32_t max_steps, max_iters;
 };
 
-// Occupancy test (OccupancyGrid::is_occupied_at, src/core/occupancy-grid.cuh:185-207). With a
-// coarse mip (one byte per 4x4x4 block of cells = 64 consecutive Morton indices, bit k set when
-// any cell of the block is occupied at level k) held in shared memory, an empty block answers
-// without touching the fine bitfield; the result is identical by construction.
-__device__ __forceinline__ bool occupied_at(const GridView& g, int k, float x, float y, float z,
-                                           const uint8_t* __restrict__ mip) {
+// Occupancy test (OccupancyGrid::is_occupied_at, src/core/occupancy-grid.cuh:185-207).
+__device__ __forceinline__ bool occupied_at(const GridView& g, int k, float x, float y, float z) {
     const uint32_t idx = voxel_morton(g, k, x, y, z);
-    const uint8_t bit = (uint8_t)(1u << k);
-    if (mip && !(mip[idx >> 6] & bit)) return false;
-    return (__ldg(g.bits + idx) & bit) != 0;
+    return (__ldg(g.bits + idx) & (1u << k)) != 0;
 }
 
 __device__ __forceinline__ void load_ray(RayMarch& r, const float* __restrict__ ori, const float* __restrict__ dir,
@@ -54,12 +52,9 @@ __device__ __forceinline__ void load_ray(RayMarch& r, const float* __restrict__ 
     r.idz = __fdiv_rn(1.0f, r.dz);
 }
 
-// march_and_count_steps_per_ray_kernel loop, src/utils/training-batch-kernels.cuh:258-297.
-// When `slots` is set, the t of the first `slot_cap` occupied steps is recorded so that the
-// emit pass can expand the samples without replaying the march.
-__device__ uint32_t march_count_ray(const MarchArgs& a, RayMarch& r, float t_max, uint32_t* flags,
-                                    const uint8_t* __restrict__ mip = nullptr, float* __restrict__ slots = nullptr,
-                                    uint32_t slot_cap = 0) {
+// march_and_count_steps_per_ray_kernel loop, src/utils/training-batch-kernels.cuh:258-297, in the
+// reference's form (plain path).
+__device__ uint32_t march_count_ray(const MarchArgs& a, const RayMarch& r, float t_max, uint32_t* flags) {
     uint32_t n = 0, iters = 0;
     float t = r.t;
     while (t < t_max) {
@@ -69,8 +64,7 @@ __device__ uint32_t march_count_ray(const MarchArgs& a, RayMarch& r, float t_max
         if (!bbox_contains(a.bbox, x, y, z)) break;
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
         const int k = grid_level_at(a.g, x, y, z, dt);
-        if (occupied_at(a.g, k, x, y, z, mip)) {
-            if (n < slot_cap) slots[n] = t;
+        if (occupied_at(a.g, k, x, y, z)) {
             t = __fadd_rn(t, dt);
             ++n;
             if (a.max_steps != 0u && n >= a.max_steps) break;
@@ -130,7 +124,7 @@ __device__ void march_emit_ray(const MarchArgs& a, RayMarch& r, uint32_t n_steps
             continue;
         }
         const int k = grid_level_at(a.g, x, y, z, dt);
-        if (occupied_at(a.g, k, x, y, z, nullptr)) {
+        if (occupied_at(a.g, k, x, y, z)) {
             o.t[s] = t;
             o.m_norm[s] = __fadd_rn(t, __fmul_rn(0.5f, dt));
             o.dt_norm[s] = dt;
@@ -153,15 +147,16 @@ __device__ void march_emit_ray(const MarchArgs& a, RayMarch& r, uint32_t n_steps
 
 // Block-wide exclusive scan of one u32 per thread (MARCH_BLOCK threads); returns the
 // exclusive prefix and the block total in *total.
+template <int BLOCK = MARCH_BLOCK>
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
-    __shared__ uint32_t warp_tot[MARCH_BLOCK / WARP];
+    __shared__ uint32_t warp_tot[BLOCK / WARP];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t inc = warp_inclusive_sum(v, lane);
     if (lane == 31) warp_tot[wid] = inc;
     __syncthreads();
     uint32_t before = 0, tot = 0;
 #pragma unroll
-    for (int w = 0; w < MARCH_BLOCK / WARP; ++w) {
+    for (int w = 0; w < BLOCK / WARP; ++w) {
         const uint32_t x = warp_tot[w];
         if (w < wid) before += x;
         tot += x;
@@ -174,6 +169,8 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
 // Last-block epilogue of the count pass: exclusive scan of the block totals into
 // block_prefix, then the reference batch cut (src/core/trainer.cu:133-183):
 // L = last ray index whose offset < batch_size; n_rays = L; n_samples = offset[L].
+// Run by one block of BLOCK threads; each entry of block_agg covers BLOCK rays.
+template <int BLOCK = MARCH_BLOCK>
 __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t* __restrict__ counts,
                                     uint32_t* block_agg, uint32_t* block_prefix, uint32_t batch_size,
                                     uint32_t* batch_info, uint32_t* flags) {
@@ -182,12 +179,12 @@ __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t
     __shared__ int last_ray_s;
     if (threadIdx.x == 0) { carry_s = 0ull; last_block_s = -1; last_ray_s = -1; }
     __syncthreads();
-    const uint32_t nb_live = (n_live + MARCH_BLOCK - 1) / MARCH_BLOCK;
-    for (uint32_t base = 0; base < nb; base += MARCH_BLOCK) {
+    const uint32_t nb_live = (n_live + BLOCK - 1) / BLOCK;
+    for (uint32_t base = 0; base < nb; base += BLOCK) {
         const uint32_t b = base + threadIdx.x;
         const uint32_t v = b < nb ? *((volatile uint32_t*)(block_agg + b)) : 0u;
         uint32_t tot;
-        const uint32_t ex = block_exclusive_scan(v, &tot);
+        const uint32_t ex = block_exclusive_scan<BLOCK>(v, &tot);
         const unsigned long long pre = carry_s + ex;
         if (b < nb) {
             block_prefix[b] = pre > 0xffffffffull ? 0xffffffffu : (uint32_t)pre;
@@ -213,10 +210,10 @@ __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t
         return;
     }
     if (lb >= 0) {
-        const uint32_t i = (uint32_t)lb * MARCH_BLOCK + threadIdx.x;
+        const uint32_t i = (uint32_t)lb * BLOCK + threadIdx.x;
         const uint32_t c = i < n_live ? *((volatile const uint32_t*)(counts + i)) : 0u;
         uint32_t tot;
-        const uint32_t ex = block_exclusive_scan(c, &tot);
+        const uint32_t ex = block_exclusive_scan<BLOCK>(c, &tot);
         const uint32_t off = block_prefix[lb] + ex;
         if (i < n_live && off < batch_size) atomicMax(&last_ray_s, (int)i);
         __syncthreads();
@@ -238,165 +235,395 @@ __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t
     }
 }
 
-// COUNT = true: march each ray; COUNT = false: counts are given (tn_scan_offsets).
-template <bool MARCH>
-__global__ void __launch_bounds__(MARCH_BLOCK)
-count_kernel(MarchArgs a, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
-             const float* __restrict__ ori, const float* __restrict__ dir, const float* __restrict__ ray_t,
-             const float* __restrict__ ray_t_max, uint8_t* __restrict__ alive, uint32_t* counts,
-             uint32_t batch_size, uint32_t* batch_info, uint32_t* block_agg, uint32_t* block_prefix,
-             uint32_t* ticket, uint32_t* flags, const uint8_t* __restrict__ mip_g, uint32_t mip_bytes,
-             float* __restrict__ slots, uint32_t slot_cap) {
-    extern __shared__ __align__(16) uint8_t mip_s[];
-    if (MARCH && mip_g) {
-        // stage the coarse occupancy mip (mip_bytes is a multiple of 16)
-        for (uint32_t k = threadIdx.x; k < mip_bytes / 16; k += MARCH_BLOCK)
-            reinterpret_cast<uint4*>(mip_s)[k] = __ldg(reinterpret_cast<const uint4*>(mip_g) + k);
-        __syncthreads();
-    }
-    const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
-    const uint32_t i = blockIdx.x * MARCH_BLOCK + threadIdx.x;
-    uint32_t cnt = 0;
-    if (i < n_live) {
-        if (MARCH) {
-            if (alive[i]) {
-                RayMarch r;
-                load_ray(r, ori, dir, i, rs);
-                r.t = ray_t[i];
-                cnt = march_count_ray(a, r, ray_t_max[i], flags, mip_g ? mip_s : nullptr,
-                                      slots ? slots + (size_t)i * slot_cap : nullptr, slots ? slot_cap : 0u);
-                if (cnt == 0) alive[i] = 0;
-            }
-            counts[i] = cnt;
-        } else {
-            cnt = counts[i];
-        }
-    }
-    // make this thread's count visible device-wide before the block reports completion
-    __threadfence();
+// ---- batch scan of given counts (tn_scan_offsets, tn_scan_offsets_noalloc) ---------------
+// Block totals of the counts; returns true in the last block to finish (ticket).
+template <int BLOCK>
+__device__ __forceinline__ bool block_total_and_ticket(uint32_t cnt, uint32_t* block_agg, uint32_t* ticket) {
     const int lane = threadIdx.x & 31;
-    uint32_t s = warp_sum(cnt);
-    __shared__ uint32_t wsum[MARCH_BLOCK / WARP];
+    const uint32_t s = warp_sum(cnt);
+    __shared__ uint32_t wsum[BLOCK / WARP];
+    __shared__ bool is_last;
     if (lane == 0) wsum[threadIdx.x >> 5] = s;
     __syncthreads();
-    __shared__ bool is_last;
     if (threadIdx.x == 0) {
         uint32_t tot = 0;
 #pragma unroll
-        for (int w = 0; w < MARCH_BLOCK / WARP; ++w) tot += wsum[w];
+        for (int w = 0; w < BLOCK / WARP; ++w) tot += wsum[w];
         block_agg[blockIdx.x] = tot;
         __threadfence();
         is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!is_last) return;
+    return is_last;
+}
+
+// Pass 1: per-block totals; the last block scans them and applies the batch cut.
+__global__ void __launch_bounds__(MARCH_BLOCK)
+scan_count_kernel(uint32_t n, const uint32_t* __restrict__ counts, uint32_t batch_size, uint32_t* batch_info,
+                  uint32_t* block_agg, uint32_t* block_prefix, uint32_t* ticket, uint32_t* flags) {
+    const uint32_t i = blockIdx.x * MARCH_BLOCK + threadIdx.x;
+    const uint32_t cnt = i < n ? counts[i] : 0u;
+    if (!block_total_and_ticket<MARCH_BLOCK>(cnt, block_agg, ticket)) return;
     __threadfence();
-    scan_blocks_and_cut(gridDim.x, n_live, counts, block_agg, block_prefix, batch_size, batch_info, flags);
+    scan_blocks_and_cut<MARCH_BLOCK>(gridDim.x, n, counts, block_agg, block_prefix, batch_size, batch_info, flags);
     if (threadIdx.x == 0) *ticket = 0u;
 }
 
-template <bool MARCH>
+// Pass 2: offsets = block scan + the block's prefix.
 __global__ void __launch_bounds__(MARCH_BLOCK)
-emit_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
-            const uint32_t* __restrict__ batch_info, const uint32_t* __restrict__ block_prefix,
-            const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
-            const float* __restrict__ ray_t, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ counts,
-            uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags) {
-    const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
+scan_offsets_kernel(uint32_t n, const uint32_t* __restrict__ counts, const uint32_t* __restrict__ block_prefix,
+                    uint32_t* __restrict__ offsets) {
     const uint32_t i = blockIdx.x * MARCH_BLOCK + threadIdx.x;
-    const uint32_t cnt = i < n_live ? counts[i] : 0u;
+    const uint32_t cnt = i < n ? counts[i] : 0u;
     uint32_t tot;
     const uint32_t off = block_exclusive_scan(cnt, &tot) + block_prefix[blockIdx.x];
-    if (i >= n_live) return;
-    offsets[i] = off;
-    if (!MARCH) return;
-    const uint32_t n_cut = batch_info[0];
-    if (i >= n_cut || cnt == 0 || !alive[i]) return;
-    if ((unsigned long long)off + cnt > (unsigned long long)o.ss) { raise_flag(flags, ERR_CAPACITY); return; }
-    RayMarch r;
-    load_ray(r, ori, dir, i, rs);
-    r.t = ray_t[i];
-    march_emit_ray(a, r, cnt, off, img_id ? img_id[i] : 0u, inv_aabb, o);
+    if (i < n) offsets[i] = off;
 }
 
-// Emit pass from the recorded step positions: the 128-ray block of the count pass rebuilds its
-// offsets, then each warp expands one ray at a time with one lane per sample (coalesced
-// stores of the packed sample arrays). Every value is the one the reference's emit loop
-// (training-batch-kernels.cuh:412-480) computes from the same t: dt = get_dt(t), the position
-// o + t d, m = t + dt/2, the ray's span from its start t to the end of its last step.
-// Rays with more samples than slots fall back to replaying their march.
-__global__ void __launch_bounds__(MARCH_BLOCK)
+// ---- fused march count ----------------------------------------------------------------
+// Rays per count block: 64 keeps every SM busy at the 2^14-ray batches of training, where
+// each warp is latency-bound on its own rays. block_agg / block_prefix hold one entry per group.
+constexpr int COUNT_GROUP = 64;
+// The coarse mip (one byte per 4x4x4 block) is staged in shared memory for 16 <= R <= 128.
+constexpr int MIP_MIN_RES = 16;
+constexpr int MIP_MAX_RES = 128;
+constexpr int BOX_INTS = 2 * MAX_LEVELS * 3;  // per level: lo block x,y,z | hi block + 1 x,y,z
+
+__device__ __forceinline__ float pow2i(int e) { return __int_as_float((127 + e) << 23); }
+
+// Level-0 constants of the count loop. Level k's half extent, cell size and reciprocal size are
+// level 0's times 2^k (2^-k): scaling by a power of two is exact in IEEE arithmetic, and the
+// host checks every level against the per-level table before launching.
+struct CountGrid {
+    float half0, cell0, inv_ls0, res_f, res_m1;
+    int res_shift;
+    const uint8_t* __restrict__ bits;
+};
+
+// get_grid_level_at (occupancy-grid.cuh:232-248): the finest level whose extent holds the point
+// (max |coordinate| < half extent) and whose cell is larger than dt, else the coarsest. Both
+// conditions only turn true as the level grows, so the level is the number of levels below the
+// coarsest that fail them: independent comparisons instead of a dependent search.
+template <int NL>
+__device__ __forceinline__ int count_level(float m, float dt, float half0, float cell0) {
+    int k = 0;
+#pragma unroll
+    for (int j = 0; j < NL - 1; ++j) {
+        const float s = pow2i(j);
+        k += (m < __fmul_rn(half0, s) && __fmul_rn(cell0, s) > dt) ? 0 : 1;
+    }
+    return k;
+}
+
+// a / b rounded toward +infinity for finite a >= b > 0 (the __fdiv_ru of get_dt_to_next_voxel,
+// occupancy-grid.cuh:281), from inv_b = 1/b rounded to nearest. q0 = a * inv_b is within two
+// ulps of a/b; one Newton correction with the residual a - q0*b (Markstein's division
+// refinement) puts q within half an ulp plus a negligible term. RU(a/b) is the smallest float q
+// with q*b >= a, so it is q, q's successor or q's predecessor; a fused multiply-add gives the
+// residual a - q*b with the sign of the exact residual (no underflow for these operands), which
+// decides between them. Infinite or NaN a passes through as the division would return it.
+__device__ __forceinline__ float div_ru_pos(float a, float b, float inv_b) {
+    const float q0 = __fmul_rn(a, inv_b);
+    float q = __fmaf_rn(__fmaf_rn(-q0, b, a), inv_b, q0);
+    if (__fmaf_rn(-q, b, a) > 0.0f) {
+        q = __uint_as_float(__float_as_uint(q) + 1u);
+    } else {
+        const float d = __uint_as_float(__float_as_uint(q) - 1u);
+        if (__fmaf_rn(-d, b, a) <= 0.0f) q = d;
+    }
+    return a <= 3.0e38f ? q : a;
+}
+
+// One axis of get_dt_to_next_voxel (occupancy-grid.cuh:270-278) from the scaled coordinate
+// f = (p / level size + 0.5) * R, which is also the cell coordinate before truncation.
+__device__ __forceinline__ float axis_dt(float f, float h, float inv_d, float kcell) {
+    return __fmul_rn(kcell, __fmul_rn(__fadd_rn(floorf(__fadd_rn(__fadd_rn(h, f), 0.5f)), -f), inv_d));
+}
+
+// The march loop of march_and_count_steps_per_ray_kernel (training-batch-kernels.cuh:258-297),
+// branch-free per step so that the 32 rays of a warp never split: both successors of t (the
+// occupied step t + dt and the DDA skip) are computed and one is selected. The scaled cell
+// coordinates are computed once per step and shared by the Morton lookup and the skip (the
+// reference computes the same expression in both, occupancy-grid.cuh:155-159 and :268-272).
+//  * t_stop: past it the ray stays outside every occupied cell, so the loop ends with the
+//    same count.
+//  * slots record the t of the first slot_cap occupied steps for the emit pass.
+template <int NL, bool MIP>
+__device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const RayMarch& r, float t_max, float t_stop,
+                              uint32_t* flags, const uint8_t* __restrict__ mip, const uint32_t* __restrict__ spread,
+                              float* __restrict__ slots, uint32_t slot_cap) {
+    const float hx = __fmul_rn(0.5f, copysignf(1.0f, r.dx));
+    const float hy = __fmul_rn(0.5f, copysignf(1.0f, r.dy));
+    const float hz = __fmul_rn(0.5f, copysignf(1.0f, r.dz));
+    const int cs = cg.res_shift - 2;
+    uint32_t n = 0, iters = 0;
+    float t = r.t;
+    while (t < t_max && t <= t_stop) {
+        if (++iters > a.max_iters) { raise_flag(flags, ERR_GUARD); break; }
+        float x, y, z;
+        ray_point(r, t, x, y, z);
+        if (!bbox_contains(a.bbox, x, y, z)) break;
+        const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
+        const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));
+        const int k = count_level<NL>(m, dt, cg.half0, cg.cell0);
+        const float ils = __fmul_rn(cg.inv_ls0, pow2i(-k));
+        const float fx = __fmul_rn(__fadd_rn(__fmul_rn(x, ils), 0.5f), cg.res_f);
+        const float fy = __fmul_rn(__fadd_rn(__fmul_rn(y, ils), 0.5f), cg.res_f);
+        const float fz = __fmul_rn(__fadd_rn(__fmul_rn(z, ils), 0.5f), cg.res_f);
+        // cell coordinates clamped to the grid (NaN -> 0), as cell_coord
+        const uint32_t cx = (uint32_t)fminf(fmaxf(fx, 0.0f), cg.res_m1);
+        const uint32_t cy = (uint32_t)fminf(fmaxf(fy, 0.0f), cg.res_m1);
+        const uint32_t cz = (uint32_t)fminf(fmaxf(fz, 0.0f), cg.res_m1);
+        const uint32_t bit = 1u << k;
+        uint32_t coarse = bit;
+        if (MIP) coarse = mip[(((((cz >> 2) << cs) | (cy >> 2)) << cs) | (cx >> 2))];
+        const uint32_t idx = spread[cx] | (spread[cy] << 1) | (spread[cz] << 2);
+        const uint32_t fine = (coarse & bit) ? (uint32_t)__ldg(cg.bits + idx) : 0u;
+        // DDA skip to the next cell boundary, in whole multiples of dt_min
+        const float kc = __fmul_rn(cg.cell0, pow2i(k));
+        const float tx = axis_dt(fx, hx, r.idx, kc);
+        const float ty = axis_dt(fy, hy, r.idy, kc);
+        const float tz = axis_dt(fz, hz, r.idz, kc);
+        const float t_target = fmaxf(a.dt_min, fminf(fminf(tx, ty), tz));
+        const float t_skip = __fadd_rn(t, __fmul_rn(div_ru_pos(t_target, a.dt_min, a.inv_dt_min), a.dt_min));
+        if (fine & bit) {
+            if (n < slot_cap) slots[n] = t;
+            t = __fadd_rn(t, dt);
+            ++n;
+            if (a.max_steps != 0u && n >= a.max_steps) break;
+        } else {
+            t = t_skip;
+        }
+    }
+    return n;
+}
+
+// World-space box that holds every occupied cell of every level: per level, the box of its
+// occupied 4x4x4 blocks padded by one cell of that level; points beyond the grid clamp to the
+// coarsest level's edge cells, so an occupied edge block of that level opens its side to
+// infinity. cut = 2 when no cell is occupied.
+__device__ void occupied_union(const CountGrid& cg, const int* __restrict__ box, int n_levels, float* u, int* cut) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int C = 1 << (cg.res_shift - 2);
+    bool any = false;
+    for (int k = 0; k < n_levels; ++k) {
+        if (box[MAX_LEVELS * 3 + k * 3] == 0) continue;  // no occupied block at this level
+        any = true;
+        const float ls = 2.0f * cg.half0 * pow2i(k), cw = cg.cell0 * pow2i(k);
+        for (int ax = 0; ax < 3; ++ax) {
+            const int l = box[k * 3 + ax], h = box[MAX_LEVELS * 3 + k * 3 + ax];
+            float wl = (4.0f * (float)l / cg.res_f - 0.5f) * ls - cw;
+            float wh = (4.0f * (float)h / cg.res_f - 0.5f) * ls + cw;
+            if (k == n_levels - 1) {
+                if (l == 0) wl = -INFINITY;
+                if (h == C) wh = INFINITY;
+            }
+            lo[ax] = fminf(lo[ax], wl);
+            hi[ax] = fmaxf(hi[ax], wh);
+        }
+    }
+    for (int ax = 0; ax < 3; ++ax) { u[ax] = lo[ax]; u[3 + ax] = hi[ax]; }
+    *cut = any ? 1 : 2;
+}
+
+// Slab test of the ray against the union box. Returns false when the ray misses it (so it
+// meets no occupied cell); otherwise *t_exit is where it leaves the box for good (infinity when
+// the test is degenerate). Rounding of o + t d grows with the coordinates: beyond `limit`
+// (65536 finest cells) it could exceed the one-cell padding, so such rays keep t_exit = infinity.
+__device__ __forceinline__ bool ray_box_exit(const RayMarch& r, const float* u, float t_max, float limit,
+                                             float* t_exit) {
+    *t_exit = INFINITY;
+    const float reach = fmaxf(fabsf(r.ox), fmaxf(fabsf(r.oy), fabsf(r.oz))) +
+                        fabsf(t_max) * fmaxf(fabsf(r.dx), fmaxf(fabsf(r.dy), fabsf(r.dz)));
+    if (!(reach <= limit)) return true;
+    const float o[3] = {r.ox, r.oy, r.oz}, d[3] = {r.dx, r.dy, r.dz}, inv[3] = {r.idx, r.idy, r.idz};
+    float te = -INFINITY, tx = INFINITY;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        if (d[ax] == 0.0f) {
+            if (!(o[ax] >= u[ax] && o[ax] <= u[3 + ax])) return false;
+            continue;
+        }
+        const float t1 = __fmul_rn(__fadd_rn(u[ax], -o[ax]), inv[ax]);
+        const float t2 = __fmul_rn(__fadd_rn(u[3 + ax], -o[ax]), inv[ax]);
+        if (t1 != t1 || t2 != t2) return true;
+        te = fmaxf(te, fminf(t1, t2));
+        tx = fminf(tx, fmaxf(t1, t2));
+    }
+    if (te > tx) return false;
+    *t_exit = tx;
+    return true;
+}
+
+// One thread per ray, COUNT_GROUP rays per block. Shared memory: the Morton spread table
+// (R words) and, with MIP, the coarse mip (R^3/64 bytes). The last block to finish scans the
+// group totals and applies the batch cut on the device.
+template <int NL, bool MIP>
+__global__ void __launch_bounds__(COUNT_GROUP)
+march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
+                   const float* __restrict__ ori, const float* __restrict__ dir, const float* __restrict__ ray_t,
+                   const float* __restrict__ ray_t_max, uint8_t* __restrict__ alive, uint32_t* counts,
+                   uint32_t batch_size, uint32_t* batch_info, uint32_t* block_agg, uint32_t* block_prefix,
+                   uint32_t* ticket, uint32_t* flags, const uint8_t* __restrict__ mip_g,
+                   const int* __restrict__ box_g, float* __restrict__ slots, uint32_t slot_cap) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint32_t* spread = reinterpret_cast<uint32_t*>(smem);
+    uint8_t* mip = smem + ((size_t)4 << cg.res_shift);
+    __shared__ float ubox_s[6];
+    __shared__ int cut_s;
+    const uint32_t res = 1u << cg.res_shift;
+    for (uint32_t c = threadIdx.x; c < res; c += COUNT_GROUP) spread[c] = part1by2(c);
+    if (MIP) {
+        const uint32_t n16 = (1u << (3 * (cg.res_shift - 2))) / 16;
+        const uint4* src = reinterpret_cast<const uint4*>(mip_g);
+        uint4* dst = reinterpret_cast<uint4*>(mip);
+#pragma unroll 8
+        for (uint32_t k = threadIdx.x; k < n16; k += COUNT_GROUP) dst[k] = __ldg(src + k);
+        if (threadIdx.x == 0) occupied_union(cg, box_g, a.g.n_levels, ubox_s, &cut_s);
+    }
+    __syncthreads();
+    const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
+    const uint32_t i = blockIdx.x * COUNT_GROUP + threadIdx.x;
+    uint32_t cnt = 0;
+    if (i < n_live) {
+        if (alive[i]) {
+            RayMarch r;
+            load_ray(r, ori, dir, i, rs);
+            r.t = ray_t[i];
+            const float t_max = ray_t_max[i];
+            float t_stop = INFINITY;
+            bool meets = true;
+            if (MIP) {
+                if (cut_s == 2) meets = false;
+                else meets = ray_box_exit(r, ubox_s, t_max, __fmul_rn(cg.cell0, 65536.0f), &t_stop);
+            }
+            if (meets)
+                cnt = count_ray<NL, MIP>(a, cg, r, t_max, t_stop, flags, mip, spread,
+                                         slots ? slots + (size_t)i * slot_cap : nullptr, slots ? slot_cap : 0u);
+            if (cnt == 0) alive[i] = 0;
+        }
+        counts[i] = cnt;
+    }
+    // make this thread's count visible device-wide before the block reports completion
+    __threadfence();
+    if (!block_total_and_ticket<COUNT_GROUP>(cnt, block_agg, ticket)) return;
+    __threadfence();
+    scan_blocks_and_cut<COUNT_GROUP>(gridDim.x, n_live, counts, block_agg, block_prefix, batch_size, batch_info,
+                                     flags);
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// Emit pass from the recorded step positions, one warp per ray, so that the rays inside the
+// batch (the first ones) spread over every SM. The warp rebuilds its ray's offset from the
+// group prefix of the count pass plus the counts of the group's earlier rays, writes it, and
+// expands the samples with one lane per sample (coalesced stores of the packed sample arrays).
+// Every value is the one the reference's emit loop (training-batch-kernels.cuh:412-480)
+// computes from the same t: dt = get_dt(t), the position o + t d, m = t + dt/2, the ray's span
+// from its start t to the end of its last step. Rays with more samples than slots fall back to
+// replaying their march.
+constexpr int EXPAND_WARPS = 8;
+
+__global__ void __launch_bounds__(EXPAND_WARPS * WARP)
 expand_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
               const uint32_t* __restrict__ batch_info, const uint32_t* __restrict__ block_prefix,
               const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
               const float* __restrict__ ray_t, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ counts,
               uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags, const float* __restrict__ slots,
               uint32_t slot_cap) {
-    __shared__ uint32_t off_s[MARCH_BLOCK], cnt_s[MARCH_BLOCK];
     const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
-    const uint32_t base = blockIdx.x * MARCH_BLOCK;
-    const uint32_t i = base + threadIdx.x;
-    const uint32_t c = i < n_live ? counts[i] : 0u;
-    uint32_t tot;
-    const uint32_t off = block_exclusive_scan(c, &tot) + block_prefix[blockIdx.x];
-    const uint32_t n_cut = batch_info[0];
-    off_s[threadIdx.x] = off;
-    cnt_s[threadIdx.x] = (i < n_live && i < n_cut && c != 0 && alive[i]) ? c : 0u;
-    if (i < n_live) offsets[i] = off;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const size_t ss = o.ss;
-    for (int k = 0; k < WARP; ++k) {
-        const int local = wid * WARP + k;
-        const uint32_t n = cnt_s[local];
-        if (n == 0) continue;
-        const uint32_t r_i = base + local;
-        const uint32_t o0 = off_s[local];
-        if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
-            if (lane == 0) raise_flag(flags, ERR_CAPACITY);
-            continue;
-        }
-        RayMarch r;
-        load_ray(r, ori, dir, r_i, rs);
-        r.t = ray_t[r_i];
-        const uint32_t img = img_id ? img_id[r_i] : 0u;
-        if (n > slot_cap) {
-            if (lane == 0) march_emit_ray(a, r, n, o0, img, inv_aabb, o);
-            continue;
-        }
-        const float* sl = slots + (size_t)r_i * slot_cap;
-        const float t_last = sl[n - 1];
-        const float t_end = __fadd_rn(t_last, get_dt(t_last, a.cone, a.dt_min, a.dt_max));
-        const float t_span = fmaxf(__fadd_rn(t_end, -r.t), 1e-6f);
-        for (uint32_t j = lane; j < n; j += WARP) {
-            const float t = sl[j];
-            const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
-            float x, y, z;
-            ray_point(r, t, x, y, z);
-            const uint32_t s = o0 + j;
-            o.t[s] = t;
-            const float m = __fadd_rn(t, __fmul_rn(0.5f, dt));
-            o.m_norm[s] = clamp_ref(__fdiv_rn(__fadd_rn(m, -r.t), t_span), 0.0f, 1.0f);
-            o.dt_norm[s] = __fdiv_rn(dt, t_span);
-            if (o.img_id) o.img_id[s] = img;
-            write_sample(o, s, x, y, z, r, dt, inv_aabb);
-        }
+    const int lane = threadIdx.x & 31;
+    const uint32_t r_i = blockIdx.x * EXPAND_WARPS + (threadIdx.x >> 5);
+    if (r_i >= n_live) return;
+    const uint32_t g0 = r_i / COUNT_GROUP * COUNT_GROUP;
+    uint32_t part = 0;
+    for (uint32_t j = g0 + lane; j < r_i; j += WARP) part += counts[j];
+    const uint32_t o0 = warp_sum(part) + block_prefix[r_i / COUNT_GROUP];
+    const uint32_t n = counts[r_i];
+    if (lane == 0) offsets[r_i] = o0;
+    if (r_i >= batch_info[0] || n == 0 || !alive[r_i]) return;
+    if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
+        if (lane == 0) raise_flag(flags, ERR_CAPACITY);
+        return;
     }
-    (void)ss;
+    RayMarch r;
+    load_ray(r, ori, dir, r_i, rs);
+    r.t = ray_t[r_i];
+    const uint32_t img = img_id ? img_id[r_i] : 0u;
+    if (n > slot_cap) {
+        if (lane == 0) march_emit_ray(a, r, n, o0, img, inv_aabb, o);
+        return;
+    }
+    const float* sl = slots + (size_t)r_i * slot_cap;
+    const float t_last = sl[n - 1];
+    const float t_end = __fadd_rn(t_last, get_dt(t_last, a.cone, a.dt_min, a.dt_max));
+    const float t_span = fmaxf(__fadd_rn(t_end, -r.t), 1e-6f);
+    for (uint32_t j = lane; j < n; j += WARP) {
+        const float t = sl[j];
+        const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
+        float x, y, z;
+        ray_point(r, t, x, y, z);
+        const uint32_t s = o0 + j;
+        o.t[s] = t;
+        const float m = __fadd_rn(t, __fmul_rn(0.5f, dt));
+        o.m_norm[s] = clamp_ref(__fdiv_rn(__fadd_rn(m, -r.t), t_span), 0.0f, 1.0f);
+        o.dt_norm[s] = __fdiv_rn(dt, t_span);
+        if (o.img_id) o.img_id[s] = img;
+        write_sample(o, s, x, y, z, r, dt, inv_aabb);
+    }
 }
 
-// Coarse occupancy mip: byte c = OR of the 64 fine bytes [64c, 64c + 64) (one 4x4x4 block).
-__global__ void build_mip_kernel(uint32_t n_coarse, const uint32_t* __restrict__ bits4, uint8_t* __restrict__ mip) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n_coarse) return;
-    const uint4* p = reinterpret_cast<const uint4*>(bits4) + (size_t)c * 4;
-    uint32_t v = 0;
+// Coarse occupancy mip, x-fastest: byte (cz*C + cy)*C + cx (C = R/4) is the OR of the 64 fine
+// bytes of that 4x4x4 block, Morton indices [64m, 64m + 64) with m = morton(cx, cy, cz). Also
+// reduces, per level, the box of occupied blocks into box[lo x,y,z per level | hi+1 x,y,z per
+// level] (lo starts at a large value, hi at 0), the input of the count pass's tail cut.
+__global__ void __launch_bounds__(256)
+build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8_t* __restrict__ mip, int* box) {
+    __shared__ int sbox[BOX_INTS];
+    if (threadIdx.x < BOX_INTS) sbox[threadIdx.x] = threadIdx.x < BOX_INTS / 2 ? 0x7fffffff : 0;
+    __syncthreads();
+    const uint32_t C = 1u << cshift;
+    const uint32_t c = blockIdx.x * 256 + threadIdx.x;
+    uint32_t v = 0, cx = 0, cy = 0, cz = 0;
+    if (c < C * C * C) {
+        cx = c & (C - 1);
+        cy = (c >> cshift) & (C - 1);
+        cz = c >> (2 * cshift);
+        const uint4* p = bits + (size_t)morton3d(cx, cy, cz) * 4;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint4 q = __ldg(p + k);
-        v |= q.x | q.y | q.z | q.w;
+        for (int k = 0; k < 4; ++k) {
+            const uint4 q = __ldg(p + k);
+            v |= q.x | q.y | q.z | q.w;
+        }
+        v = (v | (v >> 8) | (v >> 16) | (v >> 24)) & 0xFFu;
+        mip[c] = (uint8_t)v;
     }
-    mip[c] = (uint8_t)((v | (v >> 8) | (v >> 16) | (v >> 24)) & 0xFFu);
+    for (int k = 0; k < n_levels; ++k) {
+        const bool on = (v >> k) & 1u;
+        if (!__any_sync(FULL_MASK, on)) continue;
+        const int lx = __reduce_min_sync(FULL_MASK, on ? (int)cx : 0x7fffffff);
+        const int ly = __reduce_min_sync(FULL_MASK, on ? (int)cy : 0x7fffffff);
+        const int lz = __reduce_min_sync(FULL_MASK, on ? (int)cz : 0x7fffffff);
+        const int hx = __reduce_max_sync(FULL_MASK, on ? (int)cx + 1 : 0);
+        const int hy = __reduce_max_sync(FULL_MASK, on ? (int)cy + 1 : 0);
+        const int hz = __reduce_max_sync(FULL_MASK, on ? (int)cz + 1 : 0);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&sbox[k * 3 + 0], lx);
+            atomicMin(&sbox[k * 3 + 1], ly);
+            atomicMin(&sbox[k * 3 + 2], lz);
+            atomicMax(&sbox[BOX_INTS / 2 + k * 3 + 0], hx);
+            atomicMax(&sbox[BOX_INTS / 2 + k * 3 + 1], hy);
+            atomicMax(&sbox[BOX_INTS / 2 + k * 3 + 2], hz);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < BOX_INTS) {
+        const int val = sbox[threadIdx.x];
+        if (threadIdx.x < BOX_INTS / 2) {
+            if (val != 0x7fffffff) atomicMin(box + threadIdx.x, val);
+        } else if (val != 0) {
+            atomicMax(box + threadIdx.x, val);
+        }
+    }
 }
 
 // ---- compaction: ascending indices of non-zero values ---------------------------------
@@ -500,8 +727,6 @@ __global__ void rays_init_kernel(uint32_t n, uint32_t rs, tn_bbox b, float t_far
     alive[i] = 1;
 }
 
-// Shared memory available for the coarse mip of the count pass (128^3 cells -> 32 KiB).
-constexpr uint32_t MIP_SMEM_MAX = 48u * 1024u;
 // Budget of the per-ray step-position slots (floats).
 constexpr size_t SLOT_BUDGET = 16u << 20;
 
@@ -520,17 +745,58 @@ static int make_march_args(const tn_grid_desc* grid, const uint8_t* bitfield, co
     TN_NONNULL(bitfield);
     TN_NONNULL(bbox);
     TN_NONNULL(march);
-    TN_REQUIRE(march->dt_min > 0.0f && march->dt_max >= march->dt_min, TN_E_INVALID,
-               "march: need 0 < dt_min <= dt_max (got %g, %g)", march->dt_min, march->dt_max);
+    // dt_min >= 1e-30 keeps the residuals of the exact round-up division clear of underflow
+    TN_REQUIRE(march->dt_min >= 1e-30f && march->dt_max >= march->dt_min, TN_E_INVALID,
+               "march: need 1e-30 <= dt_min <= dt_max (got %g, %g)", march->dt_min, march->dt_max);
     TN_REQUIRE(march->cone_angle >= 0.0f, TN_E_INVALID, "march: cone_angle must be >= 0");
     a.g = make_grid_view(*grid, bitfield);
     a.bbox = *bbox;
     a.cone = march->cone_angle;
     a.dt_min = march->dt_min;
     a.dt_max = march->dt_max;
+    volatile float one = 1.0f;
+    a.inv_dt_min = one / a.dt_min;
     a.max_steps = march->max_steps;
     a.max_iters = march->max_iterations ? march->max_iterations : (1u << 22);
     return TN_OK;
+}
+
+// Level-0 constants of the fused count loop, checked against every level of the per-level table
+// (level k must be level 0 scaled by 2^k exactly; base sizes so extreme that this fails are
+// rejected).
+static int make_count_grid(const MarchArgs& a, CountGrid& cg) {
+    const GridView& g = a.g;
+    cg.half0 = g.half[0];
+    cg.cell0 = g.cell[0];
+    cg.inv_ls0 = g.inv_ls[0];
+    cg.res_f = g.res_f;
+    cg.res_m1 = (float)(g.res - 1);
+    cg.res_shift = 0;
+    while ((1 << cg.res_shift) < g.res) ++cg.res_shift;
+    cg.bits = g.bits;
+    for (int k = 0; k < g.n_levels; ++k) {
+        const float up = std::ldexp(1.0f, k), dn = std::ldexp(1.0f, -k);
+        TN_REQUIRE(g.half[k] == cg.half0 * up && g.cell[k] == cg.cell0 * up && g.inv_ls[k] == cg.inv_ls0 * dn,
+                   TN_E_INVALID, "march: base_size %g out of range for %d levels", g.base, g.n_levels);
+    }
+    return TN_OK;
+}
+
+template <int NL>
+static void launch_count_nl(bool mip, uint32_t nb, size_t smem, cudaStream_t stream, const MarchArgs& a,
+                            const CountGrid& cg, uint32_t n_rays, const uint32_t* n_rays_dev, uint32_t rs,
+                            const float* ori, const float* dir, const float* ray_t, const float* ray_t_max,
+                            uint8_t* alive, uint32_t* counts, uint32_t batch_size, uint32_t* batch_info,
+                            uint32_t* block_agg, uint32_t* block_prefix, uint32_t* ticket, uint32_t* flags,
+                            const uint8_t* mip_g, const int* box_g, float* slots, uint32_t slot_cap) {
+    if (mip)
+        march_count_kernel<NL, true><<<nb, COUNT_GROUP, smem, stream>>>(
+            a, cg, n_rays, n_rays_dev, rs, ori, dir, ray_t, ray_t_max, alive, counts, batch_size, batch_info,
+            block_agg, block_prefix, ticket, flags, mip_g, box_g, slots, slot_cap);
+    else
+        march_count_kernel<NL, false><<<nb, COUNT_GROUP, smem, stream>>>(
+            a, cg, n_rays, n_rays_dev, rs, ori, dir, ray_t, ray_t_max, alive, counts, batch_size, batch_info,
+            block_agg, block_prefix, ticket, flags, mip_g, box_g, slots, slot_cap);
 }
 
 }  // namespace tn
@@ -557,23 +823,33 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     MarchArgs a;
     int st = make_march_args(grid, bitfield, bbox, march, a);
     if (st != TN_OK) return st;
+    CountGrid cg;
+    st = make_count_grid(a, cg);
+    if (st != TN_OK) return st;
     TN_NONNULL(ori); TN_NONNULL(dir); TN_NONNULL(ray_t); TN_NONNULL(ray_t_max); TN_NONNULL(alive);
     TN_NONNULL(n_steps); TN_NONNULL(batch_info);
     TN_REQUIRE(n_rays > 0, TN_E_NO_RAYS, "tn_march_count: n_rays = 0");
     TN_REQUIRE(ray_stride >= n_rays, TN_E_INVALID, "ray_stride %u < n_rays %u", ray_stride, n_rays);
-    const uint32_t nb = (n_rays + MARCH_BLOCK - 1) / MARCH_BLOCK;
+    const uint32_t nb = (n_rays + COUNT_GROUP - 1) / COUNT_GROUP;
     st = ensure_block_u32(ctx, 2 * (size_t)nb);
     if (st != TN_OK) return st;
-    // coarse mip of the bitfield (staged in shared memory by the count pass)
-    const uint32_t volume = (uint32_t)grid->resolution * grid->resolution * grid->resolution;
-    const uint32_t mip_bytes = volume / 64;
-    const bool use_mip = grid->resolution >= 8 && mip_bytes <= MIP_SMEM_MAX;
+    // coarse mip of the bitfield and the per-level boxes of occupied blocks
+    const int res = grid->resolution;
+    const bool use_mip = res >= MIP_MIN_RES && res <= MIP_MAX_RES;
+    const uint32_t mip_bytes = use_mip ? (uint32_t)(res / 4) * (res / 4) * (res / 4) : 0u;
+    int* box = nullptr;
     if (use_mip) {
-        st = ensure_mip(ctx, mip_bytes);
+        st = ensure_mip(ctx, mip_bytes + BOX_INTS * sizeof(int));
         if (st != TN_OK) return st;
         TN_REQUIRE(((uintptr_t)bitfield & 15u) == 0, TN_E_INVALID, "bitfield must be 16-byte aligned");
-        build_mip_kernel<<<(mip_bytes + 255) / 256, 256, 0, stream>>>(mip_bytes, reinterpret_cast<const uint32_t*>(bitfield),
-                                                                      ctx->mip);
+        box = reinterpret_cast<int*>(ctx->mip + mip_bytes);
+        st = cuda_status(cudaMemsetAsync(box, 0x7f, BOX_INTS / 2 * sizeof(int), stream), "tn_march_count(box)");
+        if (st == TN_OK)
+            st = cuda_status(cudaMemsetAsync(box + BOX_INTS / 2, 0, BOX_INTS / 2 * sizeof(int), stream),
+                             "tn_march_count(box)");
+        if (st != TN_OK) return st;
+        build_mip_kernel<<<(mip_bytes + 255) / 256, 256, 0, stream>>>(
+            cg.res_shift - 2, grid->n_levels, reinterpret_cast<const uint4*>(bitfield), ctx->mip, box);
         st = check_launch("tn_march_count(mip)");
         if (st != TN_OK) return st;
     }
@@ -583,12 +859,18 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     if (st != TN_OK) return st;
     ctx->slot_cap = slot_cap;
     ctx->slot_rays = n_rays;
-    const size_t smem = use_mip ? mip_bytes : 0;
-    count_kernel<true><<<nb, MARCH_BLOCK, smem, stream>>>(a, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t, ray_t_max,
-                                                          alive, n_steps, batch_size, batch_info, ctx->block_u32,
-                                                          ctx->block_u32 + nb, ctx->tickets + TICKET_MARCH, ctx->flags,
-                                                          use_mip ? ctx->mip : nullptr, use_mip ? mip_bytes : 0u,
-                                                          ctx->slots, slot_cap);
+    const size_t smem = (size_t)4 * res + mip_bytes;
+#define TN_COUNT_CASE(NL)                                                                                          \
+    case NL:                                                                                                       \
+        launch_count_nl<NL>(use_mip, nb, smem, stream, a, cg, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t,     \
+                            ray_t_max, alive, n_steps, batch_size, batch_info, ctx->block_u32, ctx->block_u32 + nb, \
+                            ctx->tickets + TICKET_MARCH, ctx->flags, ctx->mip, box, ctx->slots, slot_cap);       \
+        break;
+    switch (grid->n_levels) {
+        TN_COUNT_CASE(1) TN_COUNT_CASE(2) TN_COUNT_CASE(3) TN_COUNT_CASE(4)
+        TN_COUNT_CASE(5) TN_COUNT_CASE(6) TN_COUNT_CASE(7) TN_COUNT_CASE(8)
+    }
+#undef TN_COUNT_CASE
     return check_launch("tn_march_count");
 }
 
@@ -608,11 +890,12 @@ int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, con
     TN_NONNULL(out_dt); TN_NONNULL(out_m_norm); TN_NONNULL(out_dt_norm);
     TN_REQUIRE(n_rays > 0, TN_E_NO_RAYS, "tn_march_emit: n_rays = 0");
     TN_REQUIRE(ray_stride >= n_rays, TN_E_INVALID, "ray_stride %u < n_rays %u", ray_stride, n_rays);
-    const uint32_t nb = (n_rays + MARCH_BLOCK - 1) / MARCH_BLOCK;
+    const uint32_t nb = (n_rays + COUNT_GROUP - 1) / COUNT_GROUP;
     TN_REQUIRE(ctx->block_u32_cap >= 2 * (size_t)nb && ctx->slot_rays == n_rays, TN_E_STATE,
                "tn_march_emit must follow tn_march_count on the same context with the same n_rays");
     SampleOut o{out_img_id, out_t, out_pos, out_dir, out_dt, out_m_norm, out_dt_norm, sample_stride};
-    expand_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(a, inv_aabb_size, n_rays, nullptr, ray_stride, batch_info,
+    const uint32_t n_blocks = (n_rays + EXPAND_WARPS - 1) / EXPAND_WARPS;
+    expand_kernel<<<n_blocks, EXPAND_WARPS * WARP, 0, stream>>>(a, inv_aabb_size, n_rays, nullptr, ray_stride, batch_info,
                                                   ctx->block_u32 + nb, ray_img_id, ori, dir, ray_t, alive, n_steps,
                                                   offsets, o, ctx->flags, ctx->slots, ctx->slot_cap);
     return check_launch("tn_march_emit");
@@ -625,18 +908,11 @@ int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t*
     const uint32_t nb = (n + MARCH_BLOCK - 1) / MARCH_BLOCK;
     int st = ensure_block_u32(ctx, 2 * (size_t)nb);
     if (st != TN_OK) return st;
-    MarchArgs a{};
-    count_kernel<false><<<nb, MARCH_BLOCK, 0, stream>>>(a, n, nullptr, n, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                                        const_cast<uint32_t*>(counts), batch_size, batch_info,
-                                                        ctx->block_u32, ctx->block_u32 + nb,
-                                                        ctx->tickets + TICKET_SCAN, ctx->flags, nullptr, 0u, nullptr,
-                                                        0u);
+    scan_count_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, batch_size, batch_info, ctx->block_u32,
+                                                      ctx->block_u32 + nb, ctx->tickets + TICKET_SCAN, ctx->flags);
     st = check_launch("tn_scan_offsets(count)");
     if (st != TN_OK) return st;
-    SampleOut o{};
-    emit_kernel<false><<<nb, MARCH_BLOCK, 0, stream>>>(a, 0.0f, n, nullptr, n, batch_info, ctx->block_u32 + nb,
-                                                       nullptr, nullptr, nullptr, nullptr, nullptr, counts, offsets,
-                                                       o, ctx->flags);
+    scan_offsets_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, ctx->block_u32 + nb, offsets);
     return check_launch("tn_scan_offsets(offsets)");
 }
 
@@ -710,16 +986,11 @@ int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* coun
     st = cuda_status(cudaMemsetAsync(ticket, 0, 2 * sizeof(uint32_t), stream), "tn_scan_offsets_noalloc: clear");
     if (st != TN_OK) return st;
     const uint32_t nb = (n + MARCH_BLOCK - 1) / MARCH_BLOCK;
-    MarchArgs a{};
-    count_kernel<false><<<nb, MARCH_BLOCK, 0, stream>>>(a, n, nullptr, n, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                                        const_cast<uint32_t*>(counts), batch_size, batch_info,
-                                                        block_agg, block_prefix, ticket, flags, nullptr, 0u, nullptr,
-                                                        0u);
+    scan_count_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, batch_size, batch_info, block_agg, block_prefix, ticket,
+                                                      flags);
     st = check_launch("tn_scan_offsets_noalloc(count)");
     if (st != TN_OK) return st;
-    SampleOut o{};
-    emit_kernel<false><<<nb, MARCH_BLOCK, 0, stream>>>(a, 0.0f, n, nullptr, n, batch_info, block_prefix, nullptr,
-                                                       nullptr, nullptr, nullptr, nullptr, counts, offsets, o, flags);
+    scan_offsets_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, block_prefix, offsets);
     return check_launch("tn_scan_offsets_noalloc(offsets)");
 }
 
