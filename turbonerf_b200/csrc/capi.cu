@@ -126,9 +126,9 @@ int tn_ctx_reserve(tn_ctx* ctx, uint32_t max_rays, uint32_t max_samples) {
     const size_t blocks = (size_t)max_rays / 64 + (size_t)max_samples / 1024 + 1024;
     int st = ensure_block_u32(ctx, 2 * blocks);
     if (st == TN_OK) st = ensure_block_f32(ctx, 8 * blocks);
-    // march scratch: the 128^3 coarse mip with its occupied boxes, and the step-position slots
-    // (16 Mi floats at most)
-    if (st == TN_OK) st = ensure_mip(ctx, 32u * 1024u + 256u);
+    // march scratch: the 128^3 coarse mip with its occupied boxes and 8 bit-planes (33,024 B +
+    // 8 x 256 KiB), and the step-position slots (16 Mi floats at most)
+    if (st == TN_OK) st = ensure_mip(ctx, 33024u + 8u * 262144u);
     if (st == TN_OK && max_rays) {
         size_t per = (16u << 20) / max_rays;
         if (per > 1024) per = 1024;

@@ -21,6 +21,7 @@
 #include <thrust/device_ptr.h>
 
 #include <cmath>
+#include <cstring>
 #include <mutex>
 
 #include "tn_internal.cuh"
@@ -295,24 +296,28 @@ __device__ __forceinline__ float pow2i(int e) { return __int_as_float((127 + e) 
 // level 0's times 2^k (2^-k): scaling by a power of two is exact in IEEE arithmetic, and the
 // host checks every level against the per-level table before launching.
 struct CountGrid {
-    float half0, cell0, inv_ls0, res_f, res_m1;
-    int res_shift;
-    const uint8_t* __restrict__ bits;
+    float cell0, inv_ls0, res_f;
+    int half0_bits, cell0_bits;  // bit patterns of the level-0 half extent and cell size
+    uint32_t res_m1;             // R - 1
+    int res_shift;               // log2 R
+    uint32_t plane_words;        // R^3 / 32: words per level of the bit-planes
+    const uint8_t* __restrict__ bits;     // the bitfield, one byte per cell (bit k = level k)
+    const uint32_t* __restrict__ planes;  // the same bits as one plane per level, 32 cells per word
 };
 
 // get_grid_level_at (occupancy-grid.cuh:232-248): the finest level whose extent holds the point
-// (max |coordinate| < half extent) and whose cell is larger than dt, else the coarsest. Both
-// conditions only turn true as the level grows, so the level is the number of levels below the
-// coarsest that fail them: independent comparisons instead of a dependent search.
+// (max |coordinate| m < half extent) and whose cell is larger than dt, else the coarsest. Each
+// condition turns true at some level and stays true above it, so the answer is the larger of
+// the two first levels. For positive floats the order of the values is the order of their bit
+// patterns, and level j's constant is level 0's pattern plus j << 23, so
+//   m < half0 * 2^j  <=>  j > (bits(m) - bits(half0)) / 2^23,
+//   cell0 * 2^j > dt  <=>  j > (bits(dt) - bits(cell0)) / 2^23,
+// and the first such j is the quotient (an arithmetic shift) plus one, at least 0.
 template <int NL>
-__device__ __forceinline__ int count_level(float m, float dt, float half0, float cell0) {
-    int k = 0;
-#pragma unroll
-    for (int j = 0; j < NL - 1; ++j) {
-        const float s = pow2i(j);
-        k += (m < __fmul_rn(half0, s) && __fmul_rn(cell0, s) > dt) ? 0 : 1;
-    }
-    return k;
+__device__ __forceinline__ int count_level(float m, float dt, int half0_bits, int cell0_bits) {
+    const int jp = (__float_as_int(m) - half0_bits) >> 23;
+    const int jd = (__float_as_int(dt) - cell0_bits) >> 23;
+    return min(max(max(jp, jd) + 1, 0), NL - 1);
 }
 
 // a / b rounded toward +infinity for finite a >= b > 0 (the __fdiv_ru of get_dt_to_next_voxel,
@@ -321,7 +326,8 @@ __device__ __forceinline__ int count_level(float m, float dt, float half0, float
 // refinement) puts q within half an ulp plus a negligible term. RU(a/b) is the smallest float q
 // with q*b >= a, so it is q, q's successor or q's predecessor; a fused multiply-add gives the
 // residual a - q*b with the sign of the exact residual (no underflow for these operands), which
-// decides between them. Infinite or NaN a passes through as the division would return it.
+// decides between them. (An infinite a, which only a direction of three zero components can
+// produce, yields NaN instead of infinity; either one ends the march loop the same way.)
 __device__ __forceinline__ float div_ru_pos(float a, float b, float inv_b) {
     const float q0 = __fmul_rn(a, inv_b);
     float q = __fmaf_rn(__fmaf_rn(-q0, b, a), inv_b, q0);
@@ -331,7 +337,7 @@ __device__ __forceinline__ float div_ru_pos(float a, float b, float inv_b) {
         const float d = __uint_as_float(__float_as_uint(q) - 1u);
         if (__fmaf_rn(-d, b, a) <= 0.0f) q = d;
     }
-    return a <= 3.0e38f ? q : a;
+    return q;
 }
 
 // One axis of get_dt_to_next_voxel (occupancy-grid.cuh:270-278) from the scaled coordinate
@@ -340,45 +346,53 @@ __device__ __forceinline__ float axis_dt(float f, float h, float inv_d, float kc
     return __fmul_rn(kcell, __fmul_rn(__fadd_rn(floorf(__fadd_rn(__fadd_rn(h, f), 0.5f)), -f), inv_d));
 }
 
+// Cell coordinate of get_voxel_morton_index, clamped to the grid: the conversion saturates
+// (negative and NaN give 0), then the upper edge clamps to R - 1.
+__device__ __forceinline__ uint32_t cell_of(float f, uint32_t res_m1) { return min(__float2uint_rz(f), res_m1); }
+
 // The march loop of march_and_count_steps_per_ray_kernel (training-batch-kernels.cuh:258-297),
 // branch-free per step so that the 32 rays of a warp never split: both successors of t (the
 // occupied step t + dt and the DDA skip) are computed and one is selected. The scaled cell
 // coordinates are computed once per step and shared by the Morton lookup and the skip (the
 // reference computes the same expression in both, occupancy-grid.cuh:155-159 and :268-272).
-//  * t_stop: past it the ray stays outside every occupied cell, so the loop ends with the
-//    same count.
+//  * t_lim = min(the float below t_max, t_stop) merges `t < t_max` with the tail cut: past
+//    t_stop the ray stays outside every occupied cell, so the loop ends with the same count.
+//  * max_steps is UINT32_MAX when unlimited.
+//  * spread holds three Morton spread tables, pre-shifted for x, y and z.
 //  * slots record the t of the first slot_cap occupied steps for the emit pass.
 template <int NL, bool MIP>
-__device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const RayMarch& r, float t_max, float t_stop,
-                              uint32_t* flags, const uint8_t* __restrict__ mip, const uint32_t* __restrict__ spread,
-                              float* __restrict__ slots, uint32_t slot_cap) {
+__device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const RayMarch& r, float t_lim,
+                              uint32_t max_steps, uint32_t* flags, const uint8_t* __restrict__ mip,
+                              const uint32_t* __restrict__ spread, float* __restrict__ slots, uint32_t slot_cap) {
     const float hx = __fmul_rn(0.5f, copysignf(1.0f, r.dx));
     const float hy = __fmul_rn(0.5f, copysignf(1.0f, r.dy));
     const float hz = __fmul_rn(0.5f, copysignf(1.0f, r.dz));
     const int cs = cg.res_shift - 2;
+    const uint32_t res = 1u << cg.res_shift;
     uint32_t n = 0, iters = 0;
     float t = r.t;
-    while (t < t_max && t <= t_stop) {
+    while (t <= t_lim) {
         if (++iters > a.max_iters) { raise_flag(flags, ERR_GUARD); break; }
         float x, y, z;
         ray_point(r, t, x, y, z);
         if (!bbox_contains(a.bbox, x, y, z)) break;
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
         const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));
-        const int k = count_level<NL>(m, dt, cg.half0, cg.cell0);
+        const int k = count_level<NL>(m, dt, cg.half0_bits, cg.cell0_bits);
         const float ils = __fmul_rn(cg.inv_ls0, pow2i(-k));
         const float fx = __fmul_rn(__fadd_rn(__fmul_rn(x, ils), 0.5f), cg.res_f);
         const float fy = __fmul_rn(__fadd_rn(__fmul_rn(y, ils), 0.5f), cg.res_f);
         const float fz = __fmul_rn(__fadd_rn(__fmul_rn(z, ils), 0.5f), cg.res_f);
-        // cell coordinates clamped to the grid (NaN -> 0), as cell_coord
-        const uint32_t cx = (uint32_t)fminf(fmaxf(fx, 0.0f), cg.res_m1);
-        const uint32_t cy = (uint32_t)fminf(fmaxf(fy, 0.0f), cg.res_m1);
-        const uint32_t cz = (uint32_t)fminf(fmaxf(fz, 0.0f), cg.res_m1);
-        const uint32_t bit = 1u << k;
-        uint32_t coarse = bit;
-        if (MIP) coarse = mip[(((((cz >> 2) << cs) | (cy >> 2)) << cs) | (cx >> 2))];
-        const uint32_t idx = spread[cx] | (spread[cy] << 1) | (spread[cz] << 2);
-        const uint32_t fine = (coarse & bit) ? (uint32_t)__ldg(cg.bits + idx) : 0u;
+        const uint32_t cx = cell_of(fx, cg.res_m1), cy = cell_of(fy, cg.res_m1), cz = cell_of(fz, cg.res_m1);
+        const uint32_t idx = spread[cx] | spread[res + cy] | spread[2 * res + cz];
+        bool occ;
+        if (MIP) {
+            const uint32_t coarse = mip[(((((cz >> 2) << cs) | (cy >> 2)) << cs) | (cx >> 2))];
+            const uint32_t word = ((coarse >> k) & 1u) ? __ldg(cg.planes + k * cg.plane_words + (idx >> 5)) : 0u;
+            occ = (word >> (idx & 31u)) & 1u;
+        } else {
+            occ = (__ldg(cg.bits + idx) >> k) & 1u;
+        }
         // DDA skip to the next cell boundary, in whole multiples of dt_min
         const float kc = __fmul_rn(cg.cell0, pow2i(k));
         const float tx = axis_dt(fx, hx, r.idx, kc);
@@ -386,11 +400,10 @@ __device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const Ray
         const float tz = axis_dt(fz, hz, r.idz, kc);
         const float t_target = fmaxf(a.dt_min, fminf(fminf(tx, ty), tz));
         const float t_skip = __fadd_rn(t, __fmul_rn(div_ru_pos(t_target, a.dt_min, a.inv_dt_min), a.dt_min));
-        if (fine & bit) {
+        if (occ) {
             if (n < slot_cap) slots[n] = t;
             t = __fadd_rn(t, dt);
-            ++n;
-            if (a.max_steps != 0u && n >= a.max_steps) break;
+            if (++n >= max_steps) break;
         } else {
             t = t_skip;
         }
@@ -409,7 +422,7 @@ __device__ void occupied_union(const CountGrid& cg, const int* __restrict__ box,
     for (int k = 0; k < n_levels; ++k) {
         if (box[MAX_LEVELS * 3 + k * 3] == 0) continue;  // no occupied block at this level
         any = true;
-        const float ls = 2.0f * cg.half0 * pow2i(k), cw = cg.cell0 * pow2i(k);
+        const float ls = __int_as_float(cg.half0_bits) * pow2i(k + 1), cw = cg.cell0 * pow2i(k);
         for (int ax = 0; ax < 3; ++ax) {
             const int l = box[k * 3 + ax], h = box[MAX_LEVELS * 3 + k * 3 + ax];
             float wl = (4.0f * (float)l / cg.res_f - 0.5f) * ls - cw;
@@ -455,9 +468,10 @@ __device__ __forceinline__ bool ray_box_exit(const RayMarch& r, const float* u, 
     return true;
 }
 
-// One thread per ray, COUNT_GROUP rays per block. Shared memory: the Morton spread table
-// (R words) and, with MIP, the coarse mip (R^3/64 bytes). The last block to finish scans the
-// group totals and applies the batch cut on the device.
+// One thread per ray, COUNT_GROUP rays per block. Shared memory: the three Morton spread tables
+// (3 R words) and, with MIP, the coarse mip (R^3/64 bytes); with MIP the fine test reads the
+// per-level bit-planes. The last block to finish scans the group totals and applies the batch
+// cut on the device.
 template <int NL, bool MIP>
 __global__ void __launch_bounds__(COUNT_GROUP)
 march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
@@ -468,11 +482,16 @@ march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* _
                    const int* __restrict__ box_g, float* __restrict__ slots, uint32_t slot_cap) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint32_t* spread = reinterpret_cast<uint32_t*>(smem);
-    uint8_t* mip = smem + ((size_t)4 << cg.res_shift);
+    uint8_t* mip = smem + ((size_t)12 << cg.res_shift);
     __shared__ float ubox_s[6];
     __shared__ int cut_s;
     const uint32_t res = 1u << cg.res_shift;
-    for (uint32_t c = threadIdx.x; c < res; c += COUNT_GROUP) spread[c] = part1by2(c);
+    for (uint32_t c = threadIdx.x; c < res; c += COUNT_GROUP) {
+        const uint32_t v = part1by2(c);
+        spread[c] = v;
+        spread[res + c] = v << 1;
+        spread[2 * res + c] = v << 2;
+    }
     if (MIP) {
         const uint32_t n16 = (1u << (3 * (cg.res_shift - 2))) / 16;
         const uint4* src = reinterpret_cast<const uint4*>(mip_g);
@@ -497,9 +516,13 @@ march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* _
                 if (cut_s == 2) meets = false;
                 else meets = ray_box_exit(r, ubox_s, t_max, __fmul_rn(cg.cell0, 65536.0f), &t_stop);
             }
+            // t < t_max  <=>  t <= the float just below t_max
+            const float below = nextafterf(t_max, -INFINITY);
+            const float t_lim = t_stop < below ? t_stop : below;  // a NaN t_max stays NaN
             if (meets)
-                cnt = count_ray<NL, MIP>(a, cg, r, t_max, t_stop, flags, mip, spread,
-                                         slots ? slots + (size_t)i * slot_cap : nullptr, slots ? slot_cap : 0u);
+                cnt = count_ray<NL, MIP>(a, cg, r, t_lim, a.max_steps ? a.max_steps : 0xffffffffu, flags, mip,
+                                         spread, slots ? slots + (size_t)i * slot_cap : nullptr,
+                                         slots ? slot_cap : 0u);
             if (cnt == 0) alive[i] = 0;
         }
         counts[i] = cnt;
@@ -572,12 +595,22 @@ expand_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __re
     }
 }
 
+// Bits k of the four bytes of x (cells 4j .. 4j+3) as four consecutive bits: the mask leaves
+// them at bit positions 0, 8, 16, 24, and the multiply by 1 + 2^7 + 2^14 + 2^21 moves them to
+// 21..24 without any two partial products meeting.
+__device__ __forceinline__ uint32_t gather_level_bits(uint32_t x, int k) {
+    return ((((x >> k) & 0x01010101u) * 0x00204081u) >> 21) & 0xFu;
+}
+
 // Coarse occupancy mip, x-fastest: byte (cz*C + cy)*C + cx (C = R/4) is the OR of the 64 fine
 // bytes of that 4x4x4 block, Morton indices [64m, 64m + 64) with m = morton(cx, cy, cz). Also
-// reduces, per level, the box of occupied blocks into box[lo x,y,z per level | hi+1 x,y,z per
-// level] (lo starts at a large value, hi at 0), the input of the count pass's tail cut.
+//  * writes the per-level bit-planes: bit j of word w of plane k is bit k of cell 32w + j
+//    (words 2m and 2m + 1 of every plane come from this block);
+//  * reduces, per level, the box of occupied blocks into box[lo x,y,z per level | hi+1 x,y,z
+//    per level] (lo starts at a large value, hi at 0), the input of the count pass's tail cut.
 __global__ void __launch_bounds__(256)
-build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8_t* __restrict__ mip, int* box) {
+build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8_t* __restrict__ mip, int* box,
+                 uint32_t* __restrict__ planes, uint32_t plane_words) {
     __shared__ int sbox[BOX_INTS];
     if (threadIdx.x < BOX_INTS) sbox[threadIdx.x] = threadIdx.x < BOX_INTS / 2 ? 0x7fffffff : 0;
     __syncthreads();
@@ -588,14 +621,28 @@ build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8
         cx = c & (C - 1);
         cy = (c >> cshift) & (C - 1);
         cz = c >> (2 * cshift);
-        const uint4* p = bits + (size_t)morton3d(cx, cy, cz) * 4;
+        const uint32_t m = morton3d(cx, cy, cz);
+        const uint4* p = bits + (size_t)m * 4;
+        uint32_t w[16];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint4 q = __ldg(p + k);
-            v |= q.x | q.y | q.z | q.w;
+        for (int q = 0; q < 4; ++q) {
+            const uint4 u = __ldg(p + q);
+            w[4 * q] = u.x; w[4 * q + 1] = u.y; w[4 * q + 2] = u.z; w[4 * q + 3] = u.w;
+            v |= u.x | u.y | u.z | u.w;
         }
         v = (v | (v >> 8) | (v >> 16) | (v >> 24)) & 0xFFu;
         mip[c] = (uint8_t)v;
+        for (int k = 0; k < n_levels; ++k) {
+            uint32_t lo = 0, hi = 0;
+            if ((v >> k) & 1u) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    lo |= gather_level_bits(w[j], k) << (4 * j);
+                    hi |= gather_level_bits(w[8 + j], k) << (4 * j);
+                }
+            }
+            *reinterpret_cast<uint2*>(planes + (size_t)k * plane_words + 2 * (size_t)m) = make_uint2(lo, hi);
+        }
     }
     for (int k = 0; k < n_levels; ++k) {
         const bool on = (v >> k) & 1u;
@@ -766,17 +813,22 @@ static int make_march_args(const tn_grid_desc* grid, const uint8_t* bitfield, co
 // rejected).
 static int make_count_grid(const MarchArgs& a, CountGrid& cg) {
     const GridView& g = a.g;
-    cg.half0 = g.half[0];
+    float half0 = g.half[0];
     cg.cell0 = g.cell[0];
     cg.inv_ls0 = g.inv_ls[0];
     cg.res_f = g.res_f;
-    cg.res_m1 = (float)(g.res - 1);
+    cg.res_m1 = (uint32_t)(g.res - 1);
+    std::memcpy(&cg.half0_bits, &half0, sizeof(int));
+    std::memcpy(&cg.cell0_bits, &cg.cell0, sizeof(int));
     cg.res_shift = 0;
     while ((1 << cg.res_shift) < g.res) ++cg.res_shift;
+    cg.plane_words = (uint32_t)(((uint64_t)g.res * g.res * g.res) / 32);
     cg.bits = g.bits;
+    cg.planes = nullptr;
     for (int k = 0; k < g.n_levels; ++k) {
         const float up = std::ldexp(1.0f, k), dn = std::ldexp(1.0f, -k);
-        TN_REQUIRE(g.half[k] == cg.half0 * up && g.cell[k] == cg.cell0 * up && g.inv_ls[k] == cg.inv_ls0 * dn,
+        TN_REQUIRE(g.half[k] == half0 * up && g.cell[k] == cg.cell0 * up && g.inv_ls[k] == cg.inv_ls0 * dn &&
+                       std::isnormal(half0 * up) && std::isnormal(cg.cell0 * up) && std::isnormal(cg.inv_ls0 * dn),
                    TN_E_INVALID, "march: base_size %g out of range for %d levels", g.base, g.n_levels);
     }
     return TN_OK;
@@ -833,23 +885,27 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     const uint32_t nb = (n_rays + COUNT_GROUP - 1) / COUNT_GROUP;
     st = ensure_block_u32(ctx, 2 * (size_t)nb);
     if (st != TN_OK) return st;
-    // coarse mip of the bitfield and the per-level boxes of occupied blocks
+    // coarse mip of the bitfield, the per-level boxes of occupied blocks and the bit-planes:
+    // ctx->mip = [mip (R^3/64 B) | box | planes (n_levels x R^3/8 B, 256-byte aligned)]
     const int res = grid->resolution;
     const bool use_mip = res >= MIP_MIN_RES && res <= MIP_MAX_RES;
     const uint32_t mip_bytes = use_mip ? (uint32_t)(res / 4) * (res / 4) * (res / 4) : 0u;
+    const size_t planes_off = ((size_t)mip_bytes + BOX_INTS * sizeof(int) + 255) & ~(size_t)255;
     int* box = nullptr;
     if (use_mip) {
-        st = ensure_mip(ctx, mip_bytes + BOX_INTS * sizeof(int));
+        st = ensure_mip(ctx, planes_off + (size_t)grid->n_levels * cg.plane_words * sizeof(uint32_t));
         if (st != TN_OK) return st;
         TN_REQUIRE(((uintptr_t)bitfield & 15u) == 0, TN_E_INVALID, "bitfield must be 16-byte aligned");
         box = reinterpret_cast<int*>(ctx->mip + mip_bytes);
+        cg.planes = reinterpret_cast<const uint32_t*>(ctx->mip + planes_off);
         st = cuda_status(cudaMemsetAsync(box, 0x7f, BOX_INTS / 2 * sizeof(int), stream), "tn_march_count(box)");
         if (st == TN_OK)
             st = cuda_status(cudaMemsetAsync(box + BOX_INTS / 2, 0, BOX_INTS / 2 * sizeof(int), stream),
                              "tn_march_count(box)");
         if (st != TN_OK) return st;
         build_mip_kernel<<<(mip_bytes + 255) / 256, 256, 0, stream>>>(
-            cg.res_shift - 2, grid->n_levels, reinterpret_cast<const uint4*>(bitfield), ctx->mip, box);
+            cg.res_shift - 2, grid->n_levels, reinterpret_cast<const uint4*>(bitfield), ctx->mip, box,
+            reinterpret_cast<uint32_t*>(ctx->mip + planes_off), cg.plane_words);
         st = check_launch("tn_march_count(mip)");
         if (st != TN_OK) return st;
     }
@@ -859,7 +915,7 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     if (st != TN_OK) return st;
     ctx->slot_cap = slot_cap;
     ctx->slot_rays = n_rays;
-    const size_t smem = (size_t)4 * res + mip_bytes;
+    const size_t smem = (size_t)12 * res + mip_bytes;
 #define TN_COUNT_CASE(NL)                                                                                          \
     case NL:                                                                                                       \
         launch_count_nl<NL>(use_mip, nb, smem, stream, a, cg, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t,     \
