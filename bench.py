@@ -134,12 +134,14 @@ def stage_bytes(n_rays_gen, n_rays, n_samples, n_touched, levels=5, volume=128 *
         "network_forward": n_samples * (12 + 16),                        # read pos, write sigma + rgb
         "losses": n_samples * (4 + 12 + 4 + 4 + 4 + 4 + 8 + 12) + n_rays * 36,
         "network_backward": 0,
+        "occupancy_query": OCC_CELLS * (4 + 4 + 12 + 4 + 12 + 4),       # cells, levels, rand3, select; pos; sigma
         "occupancy": levels * volume * 8 + volume + OCC_CELLS * 48,      # sweep RMW + bits + scatter inputs
         "adam": 4 * P + 32 * (n_touched + N_MLP),                        # gradient read + RMW of touched params
     }
 
 
-STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "network_backward", "adam", "occupancy"]
+STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "network_backward", "adam",
+          "occupancy_query", "occupancy"]
 
 
 def run_ours(args):

@@ -400,7 +400,7 @@ int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori
                                const float* target_rgba, const float* bg_rgb, tn_training_metrics* metrics);
 /* Runs one fused step eagerly with events between its stages and writes the stage times
  * (ms): rays, march count, march emit, network forward, losses, network backward,
- * Adam, occupancy. */
+ * Adam, occupancy query (cell sampling and the density network), occupancy update. */
 int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages);
 /* 0/1: kernel nodes in the captured step graph (synthetic / caller rays), 2: graph nodes,
  * 3: samples processed so far, 4: rays used so far, 5: steps (3-5 synchronise). */

@@ -116,11 +116,18 @@ def test_distortion_fused_and_plain(mean, n_samples):
     assert ctx.check() == 0
 
 
-def test_train_losses_fused_matches_oracle_chain():
+@pytest.mark.parametrize("mean,max_count,n_samples,sigma_scale", [
+    (48, 1024, 1 << 18, 1.0),      # the training mix: most rays in registers, a few long ones
+    (700, 1024, 1 << 16, 1.0),     # rays of 2-4 super-chunks, cut early by the transmittance
+    (700, 1024, 1 << 16, 1e-3),    # long composites that cross super-chunks
+    (6000, 9000, 1 << 16, 1e-4),   # rays beyond 32 super-chunks (distortion carries replayed)
+])
+def test_train_losses_fused_matches_oracle_chain(mean, max_count, n_samples, sigma_scale):
     """One kernel = reconstruction fwd/bwd + distortion fwd/bwd + gradient merge with
     distance scaling, against the oracle's separate stages."""
     from turbonerf_b200 import hotpath as hp
-    sb = _batch(1 << 18, 48, seed=0x7B4)
+    sb = scenes.make_sample_batch(0x7B4, n_samples, mean=mean, max_count=max_count)
+    sb.sigma = (sb.sigma * np.float32(sigma_scale)).astype(np.float32)
     n, ss = sb.n_rays, sb.n_samples
     lam, scale = 1e-3, 1.0
     t_world = (sb.t * 0.9).astype(np.float32)  # part of the samples below t = 1

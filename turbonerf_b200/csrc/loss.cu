@@ -20,6 +20,10 @@
 #include <thrust/execution_policy.h>
 #include <thrust/reduce.h>
 
+#include <mutex>
+#include <utility>
+#include <vector>
+
 #include "tn_internal.cuh"
 
 namespace tn {
@@ -523,8 +527,511 @@ distortion_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, const uint3
     if (loss_sum) block_sum_and_finish<1>(acc, partials, ticket, loss_sum, FinishScale{{1.0f, 0.0f}, n_dev, n_rays, 1u});
 }
 
-// Reconstruction + distortion forward/backward + gradient merge, one warp per ray.
-__global__ void __launch_bounds__(LOSS_THREADS)
+// ---- register-blocked rays -----------------------------------------------------------------
+// A ray of at most RB_MAX samples is held in registers, lane l owning the consecutive samples
+// [RB_SPL*l, RB_SPL*l + RB_SPL). Its inputs are read once, and each running sum along the ray is
+// a prefix inside the lane plus one warp scan of the lane totals (instead of one warp scan per
+// 32-sample chunk). Longer rays take the chunked path.
+constexpr int RB_SPL = 8;
+constexpr uint32_t RB_MAX = RB_SPL * WARP;
+
+// In place inclusive prefix along the ray plus `carry` (the sum before this block of samples);
+// returns the sum before the lane's first sample, so that the exclusive prefix of sample q is
+// (q ? v[q-1] : returned value).
+template <int K>
+__device__ __forceinline__ float blk_prefix(float (&v)[K], int lane, float carry = 0.0f) {
+#pragma unroll
+    for (int q = 1; q < K; ++q) v[q] += v[q - 1];
+    const float before = shift_up(warp_inclusive_sum(v[K - 1], lane), lane, 0.0f) + carry;
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] += before;
+    return before;
+}
+
+// In place inclusive suffix along the ray plus `carry` (the sum after this block of samples);
+// returns the sum after the lane's last sample, so that the exclusive suffix of sample q is
+// (q < K-1 ? v[q+1] : returned value).
+template <int K>
+__device__ __forceinline__ float blk_suffix(float (&v)[K], int lane, float carry = 0.0f) {
+#pragma unroll
+    for (int q = K - 2; q >= 0; --q) v[q] += v[q + 1];
+    const float after = shift_down(warp_inclusive_suffix_sum(v[0], lane), lane, 0.0f) + carry;
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] += after;
+    return after;
+}
+
+// One ray of the fused training losses (the same quantities as the chunked path below, with
+// the compositor's transmittance and weights kept from its forward instead of recomputed):
+// compositor forward (training-kernels-fused.cuh:227-264), reconstruction loss (:434-477),
+// compositor VJP (:269-341), distortion forward/backward in the non-cancelling form above, and
+// the gradient merge with the distance scaling (nerf-network.cu:734-758).
+__device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint32_t r, uint32_t o, uint32_t n,
+                                                         int lane, float min_t, float inv_nrays, float grad_scale,
+                                                         float lambda, const float* __restrict__ target,
+                                                         const float* __restrict__ bg, uint32_t rs,
+                                                         float* __restrict__ ray_rgba,
+                                                         float* __restrict__ grad_density, float* __restrict__ drgb,
+                                                         float& acc_rec, float& acc_dist) {
+    constexpr int K = RB_SPL;
+    const uint32_t j0 = (uint32_t)lane * K;
+    const size_t ss = S.ss;
+    float sig[K], dt[K], cr[K], cg[K], cb[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const uint32_t j = j0 + q;
+        const bool valid = j < n;
+        const size_t s = (size_t)o + j;
+        sig[q] = valid ? act_sigma(S.act, S.density[s]) : 0.0f;
+        dt[q] = valid ? S.dt[s] : 0.0f;
+        cr[q] = valid ? S.rgb[s] : 0.0f;
+        cg[q] = valid ? S.rgb[s + ss] : 0.0f;
+        cb[q] = valid ? S.rgb[s + 2 * ss] : 0.0f;
+    }
+    // ---- compositor forward: T after each sample, weights, the transmittance cut
+    float T[K], w[K];
+    uint32_t used = n;
+    float depth;
+    {
+        float p[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) p[q] = sig[q] * dt[q];
+        blk_prefix(p, lane);
+#pragma unroll
+        for (int q = 0; q < K; ++q) T[q] = expf(-p[q]);
+        const float t_in = shift_up(T[K - 1], lane, 1.0f);
+        int first_q = K;
+        float cut_depth = 0.0f;
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q) {
+            const float x = sig[q] * dt[q];
+            w[q] = (q ? T[q - 1] : t_in) * -expm1f(-x);
+            if (j0 + q < n && T[q] < min_t) { first_q = q; cut_depth = p[q]; }
+        }
+        const unsigned term = __ballot_sync(FULL_MASK, first_q < K);
+        if (term) {
+            const int fl = __ffs(term) - 1;
+            used = (uint32_t)fl * K + (uint32_t)__shfl_sync(FULL_MASK, first_q, fl) + 1u;
+            depth = __shfl_sync(FULL_MASK, cut_depth, fl);
+        } else {
+            depth = __shfl_sync(FULL_MASK, p[K - 1], WARP - 1);
+        }
+    }
+    float ar = 0.0f, ag = 0.0f, ab = 0.0f, aa = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        if (j0 + q >= used) w[q] = 0.0f;
+        ar += w[q] * cr[q];
+        ag += w[q] * cg[q];
+        ab += w[q] * cb[q];
+        aa += w[q];
+    }
+    CompFwd c;
+    c.r = warp_sum(ar); c.g = warp_sum(ag); c.b = warp_sum(ab); c.a = warp_sum(aa);
+    c.depth = depth;
+    c.used = used;
+    const ReconGrad g = recon_loss_ray(c, target, bg, r, rs, inv_nrays);
+    if (lane == 0) {
+        if (ray_rgba) {
+            ray_rgba[r] = c.r; ray_rgba[r + rs] = c.g; ray_rgba[r + 2 * (size_t)rs] = c.b;
+            ray_rgba[r + 3 * (size_t)rs] = c.a;
+        }
+        acc_rec += g.l[0] + g.l[1] + g.l[2] + g.l[3];
+    }
+    // ---- compositor VJP from suffix sums of w c and w over the composited samples
+    float ds[K];
+    {
+        float sr[K], sg[K], sb[K], sa[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) { sr[q] = w[q] * cr[q]; sg[q] = w[q] * cg[q]; sb[q] = w[q] * cb[q]; sa[q] = w[q]; }
+        const float ar_ = blk_suffix(sr, lane), ag_ = blk_suffix(sg, lane);
+        const float ab_ = blk_suffix(sb, lane), aa_ = blk_suffix(sa, lane);
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t j = j0 + q;
+            const float r_ex = q < K - 1 ? sr[q + 1] : ar_, g_ex = q < K - 1 ? sg[q + 1] : ag_;
+            const float b_ex = q < K - 1 ? sb[q + 1] : ab_, a_ex = q < K - 1 ? sa[q + 1] : aa_;
+            const float tn = T[q];
+            const float d = dt[q] * (g.gr * (tn * cr[q] - r_ex) + g.gg * (tn * cg[q] - g_ex) +
+                                     g.gb * (tn * cb[q] - b_ex) + g.ga * (tn - a_ex));
+            ds[q] = j < used ? grad_scale * d * act_dsigma(S.act, sig[q]) : 0.0f;
+            if (j < n) {
+                const size_t s = (size_t)o + j;
+                drgb[s] = grad_scale * g.gr * w[q];
+                drgb[s + ss] = grad_scale * g.gg * w[q];
+                drgb[s + 2 * ss] = grad_scale * g.gb * w[q];
+            }
+        }
+    }
+    // ---- distortion forward and backward (all n samples, no transmittance cut)
+    if (lambda > 0.0f) {
+        float dtn[K], mm[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t j = j0 + q;
+            const bool valid = j < n;
+            const size_t s = (size_t)o + j;
+            dtn[q] = valid ? S.dt_norm[s] : 0.0f;
+            mm[q] = valid ? S.m_norm[s] : 0.0f;
+        }
+        float wd[K], tnext[K], dm[K], A[K];
+        {
+            float p[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) p[q] = sig[q] * dtn[q];
+            const float before = blk_prefix(p, lane);
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const float x = sig[q] * dtn[q];
+                const float em = expm1f(-x);
+                const float tj = expf(-(q ? p[q - 1] : before));
+                wd[q] = j0 + q < n ? tj * -em : 0.0f;
+                tnext[q] = tj * (1.0f + em);  // T_j (1 - alpha_j)
+            }
+        }
+        {
+            float W[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) W[q] = wd[q];
+            const float w_before = blk_prefix(W, lane);
+            // m of the previous sample; the first sample's predecessor is itself (zero increment)
+            const float m_in = __shfl_up_sync(FULL_MASK, mm[K - 1], 1);
+            const float m0 = __shfl_sync(FULL_MASK, mm[0], 0);
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const float m_prev = q ? mm[q - 1] : (lane ? m_in : m0);
+                dm[q] = j0 + q < n ? fmaxf(mm[q] - m_prev, 0.0f) : 0.0f;
+                A[q] = dm[q] * (q ? W[q - 1] : w_before);
+            }
+            blk_prefix(A, lane);
+        }
+        float uni = 0.0f, cross = 0.0f;
+#pragma unroll
+        for (int q = 0; q < K; ++q) { uni += dtn[q] * wd[q] * wd[q]; cross += wd[q] * A[q]; }
+        uni = warp_sum(uni);
+        cross = warp_sum(cross);
+        const float k = n ? lambda / (float)n : 0.0f;
+        if (lane == 0) acc_dist += k * ((1.0f / 3.0f) * uni + 2.0f * cross);
+        float Wge[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) Wge[q] = wd[q];
+        blk_suffix(Wge, lane);
+        float f[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) f[q] = dm[q] * Wge[q];
+        const float f_after = blk_suffix(f, lane);
+        float gw[K], gq[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const float b = q < K - 1 ? f[q + 1] : f_after;  // B_j
+            gq[q] = k * ((2.0f / 3.0f) * dtn[q] * wd[q] + 2.0f * (A[q] + b));
+            gw[q] = gq[q] * wd[q];
+        }
+        const float gw_after = blk_suffix(gw, lane);
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const float gw_ex = q < K - 1 ? gw[q + 1] : gw_after;
+            if (j0 + q < n) ds[q] += grad_scale * dtn[q] * (gq[q] * tnext[q] - gw_ex) * act_dsigma(S.act, sig[q]);
+        }
+    }
+    // ---- gradient merge: copy_gradients_kernel<1,true> twice + apply_gradient_distance_scaling_kernel
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const uint32_t j = j0 + q;
+        if (j < n) {
+            const size_t s = (size_t)o + j;
+            float gd = grad_density[s] + ds[q];
+            if (S.t) { const float tt = S.t[s]; if (tt < 1.0f) gd *= tt * tt; }
+            grad_density[s] = gd;
+        }
+    }
+}
+
+// Rays longer than RB_MAX: the same computation over super-chunks of RB_MAX samples in the
+// blocked layout. The compositor forward carries its running sums from chunk to chunk; its VJP
+// walks the chunks from the last and rebuilds the transmittance from the ray's optical depth
+// and the suffix sums of sigma * dt, as the chunked path does. The distortion forward keeps each
+// chunk's starting carry (lane c holds chunk c for c < 32; later chunks replay from chunk 31),
+// and its backward recomputes each chunk's forward quantities from that carry.
+struct ScCarry { float x, w, a, m; };
+
+struct ScStore {
+    ScCarry s;
+    __device__ __forceinline__ void put(uint32_t c, int lane, const ScCarry& v) {
+        if (c < 32u && (uint32_t)lane == c) s = v;
+    }
+    __device__ __forceinline__ ScCarry get(uint32_t c) const {
+        const int src = (int)min(c, 31u);
+        ScCarry v;
+        v.x = __shfl_sync(FULL_MASK, s.x, src);
+        v.w = __shfl_sync(FULL_MASK, s.w, src);
+        v.a = __shfl_sync(FULL_MASK, s.a, src);
+        v.m = __shfl_sync(FULL_MASK, s.m, src);
+        return v;
+    }
+};
+
+// Distortion forward of one super-chunk from its carry: weights w_j, T_{j+1}, the increments of
+// m and A_j, and the next chunk's carry; adds the chunk's uni and cross terms (per lane).
+template <int K>
+__device__ __forceinline__ void sc_dist_forward(const float (&sig)[K], const float (&dtn)[K], const float (&mm)[K],
+                                                uint32_t j0, uint32_t n, int lane, const ScCarry& c, float (&wd)[K],
+                                                float (&tnext)[K], float (&dm)[K], float (&A)[K], ScCarry& next,
+                                                float& uni, float& cross) {
+    float p[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) p[q] = sig[q] * dtn[q];
+    const float before = blk_prefix(p, lane, c.x);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const float em = expm1f(-sig[q] * dtn[q]);
+        const float tj = expf(-(q ? p[q - 1] : before));
+        wd[q] = j0 + q < n ? tj * -em : 0.0f;
+        tnext[q] = tj * (1.0f + em);
+    }
+    float W[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) W[q] = wd[q];
+    const float w_before = blk_prefix(W, lane, c.w);
+    const float m_in = __shfl_up_sync(FULL_MASK, mm[K - 1], 1);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const float m_prev = q ? mm[q - 1] : (lane ? m_in : c.m);
+        dm[q] = j0 + q < n ? fmaxf(mm[q] - m_prev, 0.0f) : 0.0f;
+        A[q] = dm[q] * (q ? W[q - 1] : w_before);
+    }
+    blk_prefix(A, lane, c.a);
+#pragma unroll
+    for (int q = 0; q < K; ++q) { uni += dtn[q] * wd[q] * wd[q]; cross += wd[q] * A[q]; }
+    // only a chunk that is followed by another one passes its carry on, and such a chunk is full
+    next.x = __shfl_sync(FULL_MASK, p[K - 1], WARP - 1);
+    next.w = __shfl_sync(FULL_MASK, W[K - 1], WARP - 1);
+    next.a = __shfl_sync(FULL_MASK, A[K - 1], WARP - 1);
+    next.m = __shfl_sync(FULL_MASK, mm[K - 1], WARP - 1);
+}
+
+template <int K>
+__device__ __forceinline__ void sc_load_dist(const Samples& S, uint32_t o, uint32_t j0, uint32_t n, float (&sig)[K],
+                                             float (&dtn)[K], float (&mm)[K]) {
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const bool valid = j0 + q < n;
+        const size_t s = (size_t)o + j0 + q;
+        sig[q] = valid ? act_sigma(S.act, S.density[s]) : 0.0f;
+        dtn[q] = valid ? S.dt_norm[s] : 0.0f;
+        mm[q] = valid ? S.m_norm[s] : 0.0f;
+    }
+}
+
+__device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r, uint32_t o, uint32_t n, int lane,
+                                                   float min_t, float inv_nrays, float grad_scale, float lambda,
+                                                   const float* __restrict__ target, const float* __restrict__ bg,
+                                                   uint32_t rs, float* __restrict__ ray_rgba,
+                                                   float* __restrict__ grad_density, float* __restrict__ drgb,
+                                                   float& acc_rec, float& acc_dist) {
+    constexpr int K = RB_SPL;
+    const size_t ss = S.ss;
+    const uint32_t nch = (n + RB_MAX - 1) / RB_MAX;
+    // ---- compositor forward over the chunks up to the transmittance cut
+    float cx = 0.0f, tin = 1.0f;
+    float ar = 0.0f, ag = 0.0f, ab = 0.0f, aa = 0.0f;
+    uint32_t used = n;
+    float depth = 0.0f;
+    for (uint32_t c = 0; c < nch; ++c) {
+        const uint32_t j0 = c * RB_MAX + (uint32_t)lane * K;
+        float x[K], p[K], T[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const bool valid = j0 + q < n;
+            const size_t s = (size_t)o + j0 + q;
+            x[q] = valid ? act_sigma(S.act, S.density[s]) * S.dt[s] : 0.0f;
+            p[q] = x[q];
+        }
+        blk_prefix(p, lane, cx);
+#pragma unroll
+        for (int q = 0; q < K; ++q) T[q] = expf(-p[q]);
+        const float t_lane = shift_up(T[K - 1], lane, tin);
+        int first_q = K;
+        float cut_depth = 0.0f;
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q)
+            if (j0 + q < n && T[q] < min_t) { first_q = q; cut_depth = p[q]; }
+        const unsigned term = __ballot_sync(FULL_MASK, first_q < K);
+        uint32_t cut = n;
+        if (term) {
+            const int fl = __ffs(term) - 1;
+            cut = c * RB_MAX + (uint32_t)fl * K + (uint32_t)__shfl_sync(FULL_MASK, first_q, fl) + 1u;
+            depth = __shfl_sync(FULL_MASK, cut_depth, fl);
+        }
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t j = j0 + q;
+            if (j < cut) {
+                const size_t s = (size_t)o + j;
+                const float w = (q ? T[q - 1] : t_lane) * -expm1f(-x[q]);
+                ar += w * S.rgb[s]; ag += w * S.rgb[s + ss]; ab += w * S.rgb[s + 2 * ss]; aa += w;
+            }
+        }
+        if (term) { used = cut; break; }
+        cx = __shfl_sync(FULL_MASK, p[K - 1], WARP - 1);
+        tin = __shfl_sync(FULL_MASK, T[K - 1], WARP - 1);
+        depth = cx;
+    }
+    CompFwd cf;
+    cf.r = warp_sum(ar); cf.g = warp_sum(ag); cf.b = warp_sum(ab); cf.a = warp_sum(aa);
+    cf.depth = depth;
+    cf.used = used;
+    const ReconGrad g = recon_loss_ray(cf, target, bg, r, rs, inv_nrays);
+    if (lane == 0) {
+        if (ray_rgba) {
+            ray_rgba[r] = cf.r; ray_rgba[r + rs] = cf.g; ray_rgba[r + 2 * (size_t)rs] = cf.b;
+            ray_rgba[r + 3 * (size_t)rs] = cf.a;
+        }
+        acc_rec += g.l[0] + g.l[1] + g.l[2] + g.l[3];
+    }
+    // ---- distortion forward over all chunks, keeping each chunk's starting carry
+    ScStore store;
+    store.s = ScCarry{0.0f, 0.0f, 0.0f, 0.0f};
+    const float kd = lambda > 0.0f ? lambda / (float)n : 0.0f;
+    if (lambda > 0.0f) {
+        ScCarry c{0.0f, 0.0f, 0.0f, S.m_norm[o]};  // m_{-1} := m_0 (zero first increment)
+        float uni = 0.0f, cross = 0.0f;
+        for (uint32_t ci = 0; ci < nch; ++ci) {
+            store.put(ci, lane, c);
+            const uint32_t j0 = ci * RB_MAX + (uint32_t)lane * K;
+            float sig[K], dtn[K], mm[K], wd[K], tnext[K], dm[K], A[K];
+            sc_load_dist(S, o, j0, n, sig, dtn, mm);
+            ScCarry nx;
+            sc_dist_forward(sig, dtn, mm, j0, n, lane, c, wd, tnext, dm, A, nx, uni, cross);
+            c = nx;
+        }
+        uni = warp_sum(uni);
+        cross = warp_sum(cross);
+        if (lane == 0) acc_dist += kd * ((1.0f / 3.0f) * uni + 2.0f * cross);
+    }
+    // ---- backward over the chunks from the last
+    float sx = 0.0f;                                   // compositor: sum of x after the chunk
+    float sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;  // compositor: sums of w c, w after the chunk
+    float sw = 0.0f, sf = 0.0f, sgw = 0.0f;           // distortion suffix sums after the chunk
+    for (int ci = (int)nch - 1; ci >= 0; --ci) {
+        const uint32_t j0 = (uint32_t)ci * RB_MAX + (uint32_t)lane * K;
+        float ds[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) ds[q] = 0.0f;
+        if ((uint32_t)ci * RB_MAX < used) {
+            float sig[K], dt[K], cr[K], cg[K], cb[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const bool valid = j0 + q < used;
+                const size_t s = (size_t)o + j0 + q;
+                sig[q] = valid ? act_sigma(S.act, S.density[s]) : 0.0f;
+                dt[q] = valid ? S.dt[s] : 0.0f;
+                cr[q] = valid ? S.rgb[s] : 0.0f;
+                cg[q] = valid ? S.rgb[s + ss] : 0.0f;
+                cb[q] = valid ? S.rgb[s + 2 * ss] : 0.0f;
+            }
+            // T before / after sample j from the optical depth and the suffix sums of x
+            float xs[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) xs[q] = sig[q] * dt[q];
+            const float xs_after = blk_suffix(xs, lane, sx);
+            float w[K], ta[K], vr[K], vg[K], vb[K], va[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const float xs_ex = q < K - 1 ? xs[q + 1] : xs_after;
+                const float tj = expf(-fmaxf(depth - xs[q], 0.0f));
+                ta[q] = expf(-fmaxf(depth - xs_ex, 0.0f));
+                w[q] = j0 + q < used ? tj * -expm1f(-sig[q] * dt[q]) : 0.0f;
+                vr[q] = w[q] * cr[q]; vg[q] = w[q] * cg[q]; vb[q] = w[q] * cb[q]; va[q] = w[q];
+            }
+            const float ar_ = blk_suffix(vr, lane, sr), ag_ = blk_suffix(vg, lane, sg);
+            const float ab_ = blk_suffix(vb, lane, sb), aa_ = blk_suffix(va, lane, sa);
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const float r_ex = q < K - 1 ? vr[q + 1] : ar_, g_ex = q < K - 1 ? vg[q + 1] : ag_;
+                const float b_ex = q < K - 1 ? vb[q + 1] : ab_, a_ex = q < K - 1 ? va[q + 1] : aa_;
+                const float tn = ta[q];
+                const float d = dt[q] * (g.gr * (tn * cr[q] - r_ex) + g.gg * (tn * cg[q] - g_ex) +
+                                         g.gb * (tn * cb[q] - b_ex) + g.ga * (tn - a_ex));
+                if (j0 + q < used) ds[q] = grad_scale * d * act_dsigma(S.act, sig[q]);
+            }
+            sx = __shfl_sync(FULL_MASK, xs[0], 0);
+            sr = __shfl_sync(FULL_MASK, vr[0], 0); sg = __shfl_sync(FULL_MASK, vg[0], 0);
+            sb = __shfl_sync(FULL_MASK, vb[0], 0); sa = __shfl_sync(FULL_MASK, va[0], 0);
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                if (j0 + q < n) {
+                    const size_t s = (size_t)o + j0 + q;
+                    drgb[s] = grad_scale * g.gr * w[q];
+                    drgb[s + ss] = grad_scale * g.gg * w[q];
+                    drgb[s + 2 * ss] = grad_scale * g.gb * w[q];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                if (j0 + q < n) {
+                    const size_t s = (size_t)o + j0 + q;
+                    drgb[s] = 0.0f; drgb[s + ss] = 0.0f; drgb[s + 2 * ss] = 0.0f;
+                }
+            }
+        }
+        if (lambda > 0.0f) {
+            ScCarry c = store.get((uint32_t)ci);
+            float sig[K], dtn[K], mm[K], wd[K], tnext[K], dm[K], A[K];
+            for (uint32_t k = 31u; k < (uint32_t)ci; ++k) {  // chunks beyond 31: replay from chunk 31
+                const uint32_t jk = k * RB_MAX + (uint32_t)lane * K;
+                sc_load_dist(S, o, jk, n, sig, dtn, mm);
+                ScCarry nx;
+                float u0 = 0.0f, c0 = 0.0f;
+                sc_dist_forward(sig, dtn, mm, jk, n, lane, c, wd, tnext, dm, A, nx, u0, c0);
+                c = nx;
+            }
+            sc_load_dist(S, o, j0, n, sig, dtn, mm);
+            ScCarry nx;
+            float u0 = 0.0f, c0 = 0.0f;
+            sc_dist_forward(sig, dtn, mm, j0, n, lane, c, wd, tnext, dm, A, nx, u0, c0);
+            float Wge[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) Wge[q] = wd[q];
+            blk_suffix(Wge, lane, sw);
+            float f[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) f[q] = dm[q] * Wge[q];
+            const float f_after = blk_suffix(f, lane, sf);
+            float gw[K], gq[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const float b = q < K - 1 ? f[q + 1] : f_after;
+                gq[q] = kd * ((2.0f / 3.0f) * dtn[q] * wd[q] + 2.0f * (A[q] + b));
+                gw[q] = gq[q] * wd[q];
+            }
+            const float gw_after = blk_suffix(gw, lane, sgw);
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const float gw_ex = q < K - 1 ? gw[q + 1] : gw_after;
+                if (j0 + q < n) ds[q] += grad_scale * dtn[q] * (gq[q] * tnext[q] - gw_ex) * act_dsigma(S.act, sig[q]);
+            }
+            sw = __shfl_sync(FULL_MASK, Wge[0], 0);
+            sf = __shfl_sync(FULL_MASK, f[0], 0);
+            sgw = __shfl_sync(FULL_MASK, gw[0], 0);
+        }
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t j = j0 + q;
+            if (j < n) {
+                const size_t s = (size_t)o + j;
+                float gd = grad_density[s] + ds[q];
+                if (S.t) { const float tt = S.t[s]; if (tt < 1.0f) gd *= tt * tt; }
+                grad_density[s] = gd;
+            }
+        }
+    }
+}
+
+// Reconstruction + distortion forward/backward + gradient merge, one warp per ray; two blocks
+// per SM (128 registers a thread) keep 16 rays in flight per SM.
+__global__ void __launch_bounds__(LOSS_THREADS, 2)
 train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
                     const uint32_t* __restrict__ offsets, float min_t, float inv_nrays_host,
                     const uint32_t* __restrict__ inv_from, float grad_scale, float lambda,
@@ -540,6 +1047,14 @@ train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t 
     float acc[2] = {0.0f, 0.0f};
     for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
         const uint32_t o = offsets[r], n = counts[r];
+        if (n <= RB_MAX) {
+            train_losses_ray_blocked(S, r, o, n, lane, min_t, inv_nrays, grad_scale, use_dist ? lambda : 0.0f, target,
+                                     bg, rs, ray_rgba, grad_density, drgb, acc[0], acc[1]);
+        } else {
+            train_losses_ray_long(S, r, o, n, lane, min_t, inv_nrays, grad_scale, use_dist ? lambda : 0.0f, target,
+                                  bg, rs, ray_rgba, grad_density, drgb, acc[0], acc[1]);
+        }
+        continue;
         const CompFwd c = composite_forward_ray(S, o, n, min_t, lane);
         const ReconGrad g = recon_loss_ray(c, target, bg, r, rs, inv_nrays);
         DistCarryStore store;
@@ -751,12 +1266,22 @@ __global__ void plain_distance_scaling_kernel(uint32_t n, const float* __restric
     g[i] *= tt * tt;
 }
 
+// Resident blocks per SM of each loss kernel, queried once per kernel.
+static int blocks_per_sm(const void* kernel) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, int>> known;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto& kv : known)
+        if (kv.first == kernel) return kv.second;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, LOSS_THREADS, 0);
+    if (per_sm <= 0) per_sm = 1;
+    known.emplace_back(kernel, per_sm);
+    return per_sm;
+}
+
 static int loss_grid(const void* kernel, uint32_t n_rays) {
-    static int per_sm = 0;
-    if (per_sm == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, LOSS_THREADS, 0);
-        if (per_sm <= 0) per_sm = 1;
-    }
+    const int per_sm = blocks_per_sm(kernel);
     const uint32_t want = (n_rays + LOSS_WARPS - 1) / LOSS_WARPS;
     const uint32_t cap = (uint32_t)(num_sms() * per_sm);
     return (int)max(1u, min(want, cap));

@@ -76,6 +76,9 @@ struct tn_trainer {
     tn_network net{};
     SynthNet synth;
     cudaStream_t stream = nullptr;
+    // second stream of the captured step: occupancy query and update beside the training chain
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_emit = nullptr, ev_join = nullptr;
     tn_ctx* ctx = nullptr;
     std::vector<void*> allocs;
     uint32_t R = 0, B = 0, V = 0, P = 0, M = 0, chunk = 0;
@@ -132,17 +135,49 @@ struct tn_trainer {
 namespace {
 
 // Stage boundaries of one fused step (for per-stage timing with events).
-enum Stage : int { ST_RAYS = 0, ST_COUNT, ST_EMIT, ST_FORWARD, ST_LOSSES, ST_BACKWARD, ST_ADAM, ST_OCCUPANCY, ST_N };
+enum Stage : int { ST_RAYS = 0, ST_COUNT, ST_EMIT, ST_FORWARD, ST_LOSSES, ST_BACKWARD, ST_ADAM, ST_OCC_QUERY, ST_OCCUPANCY, ST_N };
 
+// Occupancy query of one step: random cells, their sample points, the density network.
+static int enqueue_occupancy_query(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid) {
+    const tn_trainer_desc& d = tr->d;
+    int st = launch_synth_cells(s, tr->M, d.seed, &tr->state->cur_step, grid.n_levels, tr->V, tr->occ_levels,
+                                tr->occ_cells, tr->occ_rand3, tr->M, tr->occ_rsel);
+    if (st == TN_OK)
+        st = tn_occupancy_sample_points(s, &grid, tr->M, tr->occ_levels, tr->occ_cells, tr->occ_rand3, tr->M,
+                                        1.0f / tr->aabb, tr->occ_pos, tr->M);
+    if (st == TN_OK) st = tr->net.density(tr->net.user, s, tr->M, nullptr, tr->M, tr->occ_pos, tr->occ_values);
+    return st;
+}
+
+// Occupancy update of one step: decay + max-update of the queried cells, bitfield rebuild.
+static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid) {
+    const tn_trainer_desc& d = tr->d;
+    return launch_occupancy_update(tr->ctx, s, &grid, tr->density, tr->bits, tr->M, tr->occ_levels, tr->occ_cells,
+                                   tr->occ_values, tr->occ_rsel, tr->net.activation, 0, &tr->state->sample_all,
+                                   nullptr, d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied);
+}
+
+// One fused step. Without stage events the occupancy work runs on a second stream beside the
+// training chain: its query (cell sampling and the density network) overlaps the march, and
+// its update (which rewrites the bitfield, so it waits for the emit pass, the last reader of
+// this step) overlaps the loss, backward and Adam stages; the main stream joins it before
+// step_end. With stage events (profiling) everything runs in order on one stream.
 int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream;
+    const bool side = ev == nullptr && tr->M > 0;
+    cudaStream_t so = side ? tr->aux : s;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
     auto mark = [&](int k) { if (ev) cudaEventRecord(ev[k + 1], s); };
     if (ev) cudaEventRecord(ev[0], s);
     step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
     int st = check_launch("step_begin");
+    if (st == TN_OK && side) {
+        st = cuda_status(cudaEventRecord(tr->ev_fork, s), "fork");
+        if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
+        if (st == TN_OK) st = enqueue_occupancy_query(tr, so, grid);
+    }
     if (st == TN_OK) {
         if (external_rays)
             st = tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax,
@@ -162,6 +197,12 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
                            nullptr, tr->ori, tr->dir, tr->ray_t, tr->alive, tr->n_steps, tr->offsets, nullptr, tr->s_t,
                            tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
     mark(ST_EMIT);
+    if (st == TN_OK && side) {
+        st = cuda_status(cudaEventRecord(tr->ev_emit, s), "emit done");
+        if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_emit, 0), "emit done");
+        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid);
+        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_join, so), "join");
+    }
     if (st == TN_OK)
         st = tr->net.forward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
                              tr->net_rgb);
@@ -186,19 +227,11 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
                          &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
                          tr->steps);
     mark(ST_ADAM);
-    if (st == TN_OK && tr->M > 0) {
-        st = launch_synth_cells(s, tr->M, d.seed, &tr->state->cur_step, grid.n_levels, tr->V, tr->occ_levels,
-                                tr->occ_cells, tr->occ_rand3, tr->M, tr->occ_rsel);
-        if (st == TN_OK)
-            st = tn_occupancy_sample_points(s, &grid, tr->M, tr->occ_levels, tr->occ_cells, tr->occ_rand3, tr->M,
-                                            1.0f / tr->aabb, tr->occ_pos, tr->M);
-        if (st == TN_OK) st = tr->net.density(tr->net.user, s, tr->M, nullptr, tr->M, tr->occ_pos, tr->occ_values);
-        if (st == TN_OK)
-            st = launch_occupancy_update(tr->ctx, s, &grid, tr->density, tr->bits, tr->M, tr->occ_levels, tr->occ_cells,
-                                         tr->occ_values, tr->occ_rsel, tr->net.activation, 0, &tr->state->sample_all,
-                                         nullptr, d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied);
-    }
+    if (st == TN_OK && !side && tr->M > 0) st = enqueue_occupancy_query(tr, s, grid);
+    mark(ST_OCC_QUERY);
+    if (st == TN_OK && !side && tr->M > 0) st = enqueue_occupancy_update(tr, s, grid);
     mark(ST_OCCUPANCY);
+    if (st == TN_OK && side) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_join, 0), "join");
     if (st == TN_OK) {
         step_end_kernel<<<1, 1, 0, s>>>(tr->state);
         st = check_launch("step_end");
@@ -372,6 +405,9 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
         tr->net.density = synth_density;
     }
     st = cuda_status(cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking), "stream");
+    if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->aux, cudaStreamNonBlocking), "aux stream");
+    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join})
+        if (st == TN_OK) st = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "step events");
     if (st == TN_OK) st = tn_ctx_create(&tr->ctx);
     const uint32_t R = desc->n_rays_per_step, B = desc->batch_size;
     const uint32_t res = (uint32_t)desc->grid.resolution;
@@ -423,6 +459,9 @@ int tn_trainer_destroy(tn_trainer* tr) {
     if (tr->synth.waves) cudaFree(tr->synth.waves);
     if (tr->state_host) cudaFreeHost(tr->state_host);
     if (tr->ctx) tn_ctx_destroy(tr->ctx);
+    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join})
+        if (e) cudaEventDestroy(e);
+    if (tr->aux) cudaStreamDestroy(tr->aux);
     if (tr->stream) cudaStreamDestroy(tr->stream);
     delete tr;
     return TN_OK;

@@ -213,9 +213,9 @@ class Trainer:
 
     # -- introspection -------------------------------------------------------------------
     def profile_step(self) -> list[float]:
-        out = (ctypes.c_float * 8)()
+        out = (ctypes.c_float * 16)()
         n = ctypes.c_uint32(0)
-        call("tn_trainer_profile_step", self._handle(), out, 8, ctypes.byref(n))
+        call("tn_trainer_profile_step", self._handle(), out, 16, ctypes.byref(n))
         return [out[i] for i in range(n.value)]
 
     def stat(self, which: int) -> int:
