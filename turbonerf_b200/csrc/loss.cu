@@ -20,6 +20,7 @@
 #include <thrust/execution_policy.h>
 #include <thrust/reduce.h>
 
+#include <algorithm>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -34,6 +35,7 @@ constexpr int SAVED_CHUNKS = 64;  // distortion chunk carries kept in registers 
 
 __device__ __forceinline__ float act_sigma(int act, float d) { return act == 0 ? d : expf(fminf(d, 12.0f) - 1.0f); }
 __device__ __forceinline__ float act_dsigma(int act, float sigma) { return act == 0 ? 1.0f : sigma; }
+
 
 // Exclusive value from an inclusive warp scan: lane 0 gets `carry`.
 __device__ __forceinline__ float shift_up(float incl, int lane, float carry) {
@@ -181,11 +183,8 @@ __device__ __forceinline__ float huber_grad(float x) { return fabsf(x) < 1.0f ? 
 // Returns the sum of the four channel losses; sets the VJP weights g4 of the compositor.
 struct ReconGrad { float gr, gg, gb, ga; float l[4]; };
 
-__device__ __forceinline__ ReconGrad recon_loss_ray(const CompFwd& c, const float* __restrict__ target,
-                                                   const float* __restrict__ bg, uint32_t r, uint32_t rs,
-                                                   float inv_nrays) {
-    const float gt_r = target[r], gt_g = target[r + rs], gt_b = target[r + 2 * (size_t)rs], gt_a = target[r + 3 * (size_t)rs];
-    const float br = bg[r], bgc = bg[r + rs], bb = bg[r + 2 * (size_t)rs];
+__device__ __forceinline__ ReconGrad recon_grad(const CompFwd& c, float gt_r, float gt_g, float gt_b, float gt_a,
+                                               float br, float bgc, float bb, float inv_nrays) {
     const float gt_ac = 1.0f - gt_a;
     const float gtr = gt_r * gt_a + br * gt_ac, gtg = gt_g * gt_a + bgc * gt_ac, gtb = gt_b * gt_a + bb * gt_ac;
     const float ac = 1.0f - c.a;
@@ -201,6 +200,13 @@ __device__ __forceinline__ ReconGrad recon_loss_ray(const CompFwd& c, const floa
     g.gb = lb * c.a;
     g.ga = lr * (c.r - br) + lg * (c.g - bgc) + lb * (c.b - bb);
     return g;
+}
+
+__device__ __forceinline__ ReconGrad recon_loss_ray(const CompFwd& c, const float* __restrict__ target,
+                                                   const float* __restrict__ bg, uint32_t r, uint32_t rs,
+                                                   float inv_nrays) {
+    return recon_grad(c, target[r], target[r + rs], target[r + 2 * (size_t)rs], target[r + 3 * (size_t)rs], bg[r],
+                      bg[r + rs], bg[r + 2 * (size_t)rs], inv_nrays);
 }
 
 // ---- distortion -------------------------------------------------------------------------
@@ -361,7 +367,7 @@ __device__ void block_sum_and_finish(float (&v)[NV], float* partials, uint32_t* 
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             float s = 0.0f;
-            for (int w = 0; w < LOSS_WARPS; ++w) s += red[w][k];
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w][k];
             partials[(size_t)blockIdx.x * NV + k] = s;
         }
         __threadfence();
@@ -390,7 +396,7 @@ __device__ void block_sum_and_finish(float (&v)[NV], float* partials, uint32_t* 
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             float s = 0.0f;
-            for (int w = 0; w < LOSS_WARPS; ++w) s += red[w][k];
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w][k];
             s *= fs.s[k];
             if ((fs.dev_mask >> k) & 1u) s *= inv_n;
             if (out) out[k] = s;
@@ -561,32 +567,88 @@ __device__ __forceinline__ float blk_suffix(float (&v)[K], int lane, float carry
     return after;
 }
 
+// ---- shared-memory staging of one ray's samples ----------------------------------------
+// Each input array of the ray is copied with cp.async (coalesced, one sample per lane per
+// step) into a per-warp buffer, all of them before a single wait, so the ray pays one memory
+// latency. Sample j sits at j + j/32: lane l then reads its consecutive samples 8l..8l+7
+// without bank conflicts. Results go back through the same buffers with coalesced stores.
+constexpr int RB_SKEW = RB_MAX + RB_MAX / WARP;
+enum StageArray : int { SA_SIG = 0, SA_DT, SA_R, SA_G, SA_B, SA_DTN, SA_M, SA_T, SA_GD, SA_N };
+constexpr int TL_WARPS = 4;  // warps (rays in flight) per block of the fused loss kernel
+constexpr int TL_THREADS = TL_WARPS * WARP;
+
+__device__ __forceinline__ uint32_t skew(uint32_t j) { return j + (j >> 5); }
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ void stage_segment(float* buf, const float* __restrict__ src, size_t o, uint32_t n,
+                                              int lane) {
+    for (uint32_t j = (uint32_t)lane; j < n; j += WARP) cp_async4(buf + skew(j), src + o + j);
+}
+
+__device__ __forceinline__ void store_segment(float* __restrict__ dst, const float* buf, size_t o, uint32_t n,
+                                              int lane) {
+    for (uint32_t j = (uint32_t)lane; j < n; j += WARP) dst[o + j] = buf[skew(j)];
+}
+
 // One ray of the fused training losses (the same quantities as the chunked path below, with
 // the compositor's transmittance and weights kept from its forward instead of recomputed):
 // compositor forward (training-kernels-fused.cuh:227-264), reconstruction loss (:434-477),
 // compositor VJP (:269-341), distortion forward/backward in the non-cancelling form above, and
-// the gradient merge with the distance scaling (nerf-network.cu:734-758).
+// the gradient merge with the distance scaling (nerf-network.cu:734-758). `sm` is the warp's
+// staging buffer, SA_N arrays of RB_SKEW floats.
 __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint32_t r, uint32_t o, uint32_t n,
                                                          int lane, float min_t, float inv_nrays, float grad_scale,
                                                          float lambda, const float* __restrict__ target,
                                                          const float* __restrict__ bg, uint32_t rs,
                                                          float* __restrict__ ray_rgba,
                                                          float* __restrict__ grad_density, float* __restrict__ drgb,
-                                                         float& acc_rec, float& acc_dist) {
+                                                         float& acc_rec, float& acc_dist, float* sm) {
     constexpr int K = RB_SPL;
     const uint32_t j0 = (uint32_t)lane * K;
     const size_t ss = S.ss;
+    float* const b_sig = sm + SA_SIG * RB_SKEW;
+    float* const b_dt = sm + SA_DT * RB_SKEW;
+    float* const b_r = sm + SA_R * RB_SKEW;
+    float* const b_g = sm + SA_G * RB_SKEW;
+    float* const b_b = sm + SA_B * RB_SKEW;
+    float* const b_dtn = sm + SA_DTN * RB_SKEW;
+    float* const b_m = sm + SA_M * RB_SKEW;
+    float* const b_t = sm + SA_T * RB_SKEW;
+    float* const b_gd = sm + SA_GD * RB_SKEW;
+    // every input of the ray in flight at once; the per-ray inputs of the loss meanwhile
+    __syncwarp();  // the previous ray's write-back reads of the buffers are done
+    stage_segment(b_sig, S.density, o, n, lane);
+    stage_segment(b_dt, S.dt, o, n, lane);
+    stage_segment(b_r, S.rgb, o, n, lane);
+    stage_segment(b_g, S.rgb + ss, o, n, lane);
+    stage_segment(b_b, S.rgb + 2 * ss, o, n, lane);
+    if (lambda > 0.0f) {
+        stage_segment(b_dtn, S.dt_norm, o, n, lane);
+        stage_segment(b_m, S.m_norm, o, n, lane);
+    }
+    if (S.t) stage_segment(b_t, S.t, o, n, lane);
+    stage_segment(b_gd, grad_density, o, n, lane);
+    const float gt_r = target[r], gt_g = target[r + rs], gt_b = target[r + 2 * (size_t)rs];
+    const float gt_a = target[r + 3 * (size_t)rs];
+    const float bg_r = bg[r], bg_g = bg[r + rs], bg_b = bg[r + 2 * (size_t)rs];
+    cp_async_wait_all();
+    __syncwarp();
     float sig[K], dt[K], cr[K], cg[K], cb[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) {
         const uint32_t j = j0 + q;
         const bool valid = j < n;
-        const size_t s = (size_t)o + j;
-        sig[q] = valid ? act_sigma(S.act, S.density[s]) : 0.0f;
-        dt[q] = valid ? S.dt[s] : 0.0f;
-        cr[q] = valid ? S.rgb[s] : 0.0f;
-        cg[q] = valid ? S.rgb[s + ss] : 0.0f;
-        cb[q] = valid ? S.rgb[s + 2 * ss] : 0.0f;
+        const uint32_t k = skew(j);
+        sig[q] = valid ? act_sigma(S.act, b_sig[k]) : 0.0f;
+        dt[q] = valid ? b_dt[k] : 0.0f;
+        cr[q] = valid ? b_r[k] : 0.0f;
+        cg[q] = valid ? b_g[k] : 0.0f;
+        cb[q] = valid ? b_b[k] : 0.0f;
     }
     // ---- compositor forward: T after each sample, weights, the transmittance cut
     float T[K], w[K];
@@ -630,7 +692,7 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
     c.r = warp_sum(ar); c.g = warp_sum(ag); c.b = warp_sum(ab); c.a = warp_sum(aa);
     c.depth = depth;
     c.used = used;
-    const ReconGrad g = recon_loss_ray(c, target, bg, r, rs, inv_nrays);
+    const ReconGrad g = recon_grad(c, gt_r, gt_g, gt_b, gt_a, bg_r, bg_g, bg_b, inv_nrays);
     if (lane == 0) {
         if (ray_rgba) {
             ray_rgba[r] = c.r; ray_rgba[r + rs] = c.g; ray_rgba[r + 2 * (size_t)rs] = c.b;
@@ -638,28 +700,29 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
         }
         acc_rec += g.l[0] + g.l[1] + g.l[2] + g.l[3];
     }
-    // ---- compositor VJP from suffix sums of w c and w over the composited samples
+    // ---- compositor VJP. The upstream weights gr, gg, gb, ga are the same for the whole ray, so
+    // the four suffix sums of w c and w enter only through sum_{i>j} w_i u_i with
+    // u = gr cr + gg cg + gb cb + ga: one suffix scan.
     float ds[K];
     {
-        float sr[K], sg[K], sb[K], sa[K];
+        float su[K], cu[K];
 #pragma unroll
-        for (int q = 0; q < K; ++q) { sr[q] = w[q] * cr[q]; sg[q] = w[q] * cg[q]; sb[q] = w[q] * cb[q]; sa[q] = w[q]; }
-        const float ar_ = blk_suffix(sr, lane), ag_ = blk_suffix(sg, lane);
-        const float ab_ = blk_suffix(sb, lane), aa_ = blk_suffix(sa, lane);
+        for (int q = 0; q < K; ++q) {
+            cu[q] = g.gr * cr[q] + g.gg * cg[q] + g.gb * cb[q] + g.ga;
+            su[q] = w[q] * cu[q];
+        }
+        const float su_after = blk_suffix(su, lane);
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             const uint32_t j = j0 + q;
-            const float r_ex = q < K - 1 ? sr[q + 1] : ar_, g_ex = q < K - 1 ? sg[q + 1] : ag_;
-            const float b_ex = q < K - 1 ? sb[q + 1] : ab_, a_ex = q < K - 1 ? sa[q + 1] : aa_;
-            const float tn = T[q];
-            const float d = dt[q] * (g.gr * (tn * cr[q] - r_ex) + g.gg * (tn * cg[q] - g_ex) +
-                                     g.gb * (tn * cb[q] - b_ex) + g.ga * (tn - a_ex));
+            const float u_ex = q < K - 1 ? su[q + 1] : su_after;
+            const float d = dt[q] * (T[q] * cu[q] - u_ex);
             ds[q] = j < used ? grad_scale * d * act_dsigma(S.act, sig[q]) : 0.0f;
             if (j < n) {
-                const size_t s = (size_t)o + j;
-                drgb[s] = grad_scale * g.gr * w[q];
-                drgb[s + ss] = grad_scale * g.gg * w[q];
-                drgb[s + 2 * ss] = grad_scale * g.gb * w[q];
+                const uint32_t k = skew(j);
+                b_r[k] = grad_scale * g.gr * w[q];
+                b_g[k] = grad_scale * g.gg * w[q];
+                b_b[k] = grad_scale * g.gb * w[q];
             }
         }
     }
@@ -670,9 +733,8 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
         for (int q = 0; q < K; ++q) {
             const uint32_t j = j0 + q;
             const bool valid = j < n;
-            const size_t s = (size_t)o + j;
-            dtn[q] = valid ? S.dt_norm[s] : 0.0f;
-            mm[q] = valid ? S.m_norm[s] : 0.0f;
+            dtn[q] = valid ? b_dtn[skew(j)] : 0.0f;
+            mm[q] = valid ? b_m[skew(j)] : 0.0f;
         }
         float wd[K], tnext[K], dm[K], A[K];
         {
@@ -739,12 +801,17 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
     for (int q = 0; q < K; ++q) {
         const uint32_t j = j0 + q;
         if (j < n) {
-            const size_t s = (size_t)o + j;
-            float gd = grad_density[s] + ds[q];
-            if (S.t) { const float tt = S.t[s]; if (tt < 1.0f) gd *= tt * tt; }
-            grad_density[s] = gd;
+            const uint32_t k = skew(j);
+            float gd = b_gd[k] + ds[q];
+            if (S.t) { const float tt = b_t[k]; if (tt < 1.0f) gd *= tt * tt; }
+            b_gd[k] = gd;
         }
     }
+    __syncwarp();
+    store_segment(grad_density, b_gd, o, n, lane);
+    store_segment(drgb, b_r, o, n, lane);
+    store_segment(drgb + ss, b_g, o, n, lane);
+    store_segment(drgb + 2 * ss, b_b, o, n, lane);
 }
 
 // Rays longer than RB_MAX: the same computation over super-chunks of RB_MAX samples in the
@@ -1029,79 +1096,32 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
     }
 }
 
-// Reconstruction + distortion forward/backward + gradient merge, one warp per ray; two blocks
-// per SM (128 registers a thread) keep 16 rays in flight per SM.
-__global__ void __launch_bounds__(LOSS_THREADS, 2)
+// Reconstruction + distortion forward/backward + gradient merge, one warp per ray with its own
+// staging buffer; four blocks of four warps per SM (128 registers a thread, 38 KB of shared
+// memory a block) keep 16 rays in flight per SM.
+__global__ void __launch_bounds__(TL_THREADS, 4)
 train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
                     const uint32_t* __restrict__ offsets, float min_t, float inv_nrays_host,
                     const uint32_t* __restrict__ inv_from, float grad_scale, float lambda,
                     const float* __restrict__ target, const float* __restrict__ bg, float* __restrict__ ray_rgba,
                     float* __restrict__ grad_density, float* __restrict__ drgb, float* loss_sums, float* partials,
                     uint32_t* ticket) {
-    const int lane = threadIdx.x & 31;
+    __shared__ float stage[TL_WARPS][SA_N * RB_SKEW];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_live = live_rays(n_rays, n_dev);
     float inv_nrays = inv_nrays_host;
     if (inv_from) { const uint32_t nn = *inv_from; inv_nrays = nn ? 1.0f / (float)nn : 0.0f; }
-    const uint32_t nw = gridDim.x * LOSS_WARPS;
-    const bool use_dist = lambda > 0.0f;
+    const uint32_t nw = gridDim.x * TL_WARPS;
+    const float lam = lambda > 0.0f ? lambda : 0.0f;
     float acc[2] = {0.0f, 0.0f};
-    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
+    for (uint32_t r = blockIdx.x * TL_WARPS + wid; r < n_live; r += nw) {
         const uint32_t o = offsets[r], n = counts[r];
-        if (n <= RB_MAX) {
-            train_losses_ray_blocked(S, r, o, n, lane, min_t, inv_nrays, grad_scale, use_dist ? lambda : 0.0f, target,
-                                     bg, rs, ray_rgba, grad_density, drgb, acc[0], acc[1]);
-        } else {
-            train_losses_ray_long(S, r, o, n, lane, min_t, inv_nrays, grad_scale, use_dist ? lambda : 0.0f, target,
-                                  bg, rs, ray_rgba, grad_density, drgb, acc[0], acc[1]);
-        }
-        continue;
-        const CompFwd c = composite_forward_ray(S, o, n, min_t, lane);
-        const ReconGrad g = recon_loss_ray(c, target, bg, r, rs, inv_nrays);
-        DistCarryStore store;
-        DistFwd f{0.0f, 0.0f};
-        if (use_dist) f = dist_forward_ray(S, o, n, lambda, lane, store);
-        if (lane == 0) {
-            if (ray_rgba) {
-                ray_rgba[r] = c.r; ray_rgba[r + rs] = c.g; ray_rgba[r + 2 * (size_t)rs] = c.b;
-                ray_rgba[r + 3 * (size_t)rs] = c.a;
-            }
-            acc[0] += g.l[0] + g.l[1] + g.l[2] + g.l[3];
-            acc[1] += f.loss;
-        }
-        if (n == 0) continue;
-        float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
-        DistSuffix suf{0.0f, 0.0f, 0.0f};
-        const uint32_t nch = (n + WARP - 1) / WARP;
-        for (int ci = (int)nch - 1; ci >= 0; --ci) {
-            const uint32_t base = (uint32_t)ci * WARP;
-            const uint32_t j = base + lane;
-            float g_rec = 0.0f, xr = 0.0f, xg = 0.0f, xb = 0.0f;
-            if (base < c.used) {
-                composite_vjp_chunk(S, o, c.used, c.depth, g.gr, g.gg, g.gb, g.ga, grad_scale, base, lane, sx, sr, sg,
-                                    sb, sa, [&](uint32_t, bool valid, float ds, float a, float b, float cc) {
-                                        if (valid) { g_rec = ds; xr = a; xg = b; xb = cc; }
-                                    });
-            }
-            float g_dist = 0.0f;
-            if (use_dist) {
-                const DistCarry cc = ci < SAVED_CHUNKS ? store.get((uint32_t)ci)
-                                                       : dist_replay_carry(S, o, n, (uint32_t)ci, lane, store);
-                DistCarry nx;
-                const DistChunk d = dist_chunk_forward(S, o, n, base, lane, cc, nx);
-                g_dist = dist_chunk_backward(d, f.k, lane, suf) * act_dsigma(S.act, d.sigma);
-            }
-            if (j < n) {
-                const size_t s = (size_t)o + j;
-                // copy_gradients_kernel<1,true> twice + apply_gradient_distance_scaling_kernel
-                // (src/core/nerf-network.cu:734-758); the loss scale is grad_scale.
-                float gd = grad_density[s] + grad_scale * g_rec + grad_scale * g_dist;
-                if (S.t) { const float tt = S.t[s]; if (tt < 1.0f) gd *= tt * tt; }
-                grad_density[s] = gd;
-                drgb[s] = xr;
-                drgb[s + S.ss] = xg;
-                drgb[s + 2 * (size_t)S.ss] = xb;
-            }
-        }
+        if (n <= RB_MAX)
+            train_losses_ray_blocked(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
+                                     grad_density, drgb, acc[0], acc[1], stage[wid]);
+        else
+            train_losses_ray_long(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
+                                  grad_density, drgb, acc[0], acc[1]);
     }
     if (loss_sums) {
         acc[0] *= inv_nrays;
@@ -1267,22 +1287,22 @@ __global__ void plain_distance_scaling_kernel(uint32_t n, const float* __restric
 }
 
 // Resident blocks per SM of each loss kernel, queried once per kernel.
-static int blocks_per_sm(const void* kernel) {
+static int blocks_per_sm(const void* kernel, int threads, size_t dyn_smem = 0) {
     static std::mutex mu;
     static std::vector<std::pair<const void*, int>> known;
     std::lock_guard<std::mutex> lock(mu);
     for (const auto& kv : known)
         if (kv.first == kernel) return kv.second;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, LOSS_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, dyn_smem);
     if (per_sm <= 0) per_sm = 1;
     known.emplace_back(kernel, per_sm);
     return per_sm;
 }
 
-static int loss_grid(const void* kernel, uint32_t n_rays) {
-    const int per_sm = blocks_per_sm(kernel);
-    const uint32_t want = (n_rays + LOSS_WARPS - 1) / LOSS_WARPS;
+static int loss_grid(const void* kernel, uint32_t n_rays, int threads = LOSS_THREADS) {
+    const int per_sm = blocks_per_sm(kernel, threads);
+    const uint32_t want = (n_rays + threads / WARP - 1) / (threads / WARP);
     const uint32_t cap = (uint32_t)(num_sms() * per_sm);
     return (int)max(1u, min(want, cap));
 }
@@ -1400,10 +1420,10 @@ int tn_train_losses(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, 
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, m_norm, dt_norm, t, batch->sample_stride, activation};
-    const int grid = loss_grid((const void*)train_losses_kernel, batch->n_rays);
+    const int grid = loss_grid((const void*)train_losses_kernel, batch->n_rays, TL_THREADS);
     st = ensure_block_f32(ctx, (size_t)grid * 2);
     if (st != TN_OK) return st;
-    train_losses_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
+    train_losses_kernel<<<grid, TL_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
                                                            batch->counts, batch->offsets, min_transmittance, inv_nrays,
                                                            inv_nrays_from_dev, grad_scale, lambda, target_rgba, bg_rgb,
                                                            ray_rgba, grad_density, dL_drgb, loss_sums, ctx->block_f32,
