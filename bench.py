@@ -143,6 +143,11 @@ def stage_bytes(n_rays_gen, n_rays, n_samples, n_touched, levels=5, volume=128 *
 STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "network_backward", "adam",
           "occupancy_query", "occupancy"]
 
+# DRAM bytes (read + write) of one launch of each stage's main kernel on this workload, measured
+# with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass, after the warm-up steps).
+NCU_TRAFFIC = {"march_count": 1_007_616, "march_emit": 1_285_376, "losses": 9_637_888, "adam": 304_766_208,
+               "occupancy": 50_338_304}
+
 
 def run_ours(args):
     import torch
@@ -212,8 +217,8 @@ def run_ours(args):
                             "frac": round(gbs / peak, 4)}
         dom = max(STAGES, key=lambda k: stages[k]["ms"])
         roofline = {"bound": "hbm", "kernel": dom, "achieved": stages[dom]["achieved_gbs"], "peak": peak,
-                    "unit": "GB/s", "frac": round(stages[dom]["achieved_gbs"] / peak, 4), "traffic": None,
-                    "peak_source": peak_kind}
+                    "unit": "GB/s", "frac": round(stages[dom]["achieved_gbs"] / peak, 4),
+                    "traffic": NCU_TRAFFIC.get(dom), "peak_source": peak_kind}
         result = dict(value=value, ms=ms_max, samples=samples, rays=rays_used, kernels=kernels_per_step,
                       clocks=clk.summary(), stages=stages, roofline=roofline, n_touched=tr.n_touched_grads,
                       last=dict(n_rays=m.n_rays, n_samples=m.n_samples, loss=m.loss))
