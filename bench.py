@@ -410,6 +410,67 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_backward_memory(args):
+    """Backward memory study: 2^22 samples over about 2^16 rays (truncated geometric counts,
+    mean 64, at most 1024; sigma and rgb as in the compositor workload), compositor + distortion
+    loss forward and backward, two ways:
+      * recompute: the compositor keeps only per-ray state (RGBA, optical depth, samples used)
+        and its backward rebuilds transmittance by a reverse scan; the distortion loss runs as
+        one fused forward/backward pass;
+      * store: the compositor forward also stores every sample's transmittance and weight and
+        its backward reads them; the distortion loss stores its per-sample running sums between
+        a forward and a backward kernel (the reference's structure).
+    Reports, per variant, the device memory its buffers add beyond the shared inputs (allocator
+    peak) and the time of forward + backward (CUDA events, after warm-up). Both variants'
+    gradients are checked against the FP64 oracle by tests/test_gpu_backward_memory.py."""
+    import torch
+    from turbonerf_b200 import hotpath as hp, scenes
+
+    torch.cuda.set_device(0)
+    sb = scenes.make_sample_batch(0x7B5, 1 << 22, mean=64.0, max_count=1024)
+    n, ss = sb.n_rays, sb.n_samples
+    lam = 1e-3
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    counts = dev(sb.counts.view(np.int32))
+    offsets = dev(sb.offsets.view(np.int32))
+    sig, rgb, dt, mn, dtn = (dev(a) for a in (sb.sigma, sb.rgb, sb.dt, sb.m_norm, sb.dt_norm))
+    g_rgba = dev(np.random.default_rng(5).normal(size=4 * n).astype(np.float32))
+    rb = hp.ray_batch(counts, offsets, n, n, ss)
+    ctx = hp.Context()
+    ctx.reserve(n, ss)
+    variants = {
+        "recompute": lambda: hp.backward_recompute(ctx, rb, sig, rgb, dt, mn, dtn, g_rgba, lam),
+        "store": lambda: hp.backward_store(ctx, rb, sig, rgb, dt, mn, dtn, g_rgba, lam),
+    }
+    result = {}
+    for name, fn in variants.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        base = torch.cuda.memory_allocated()
+        torch.cuda.reset_peak_memory_stats()
+        out = fn()
+        torch.cuda.synchronize()
+        extra = torch.cuda.max_memory_allocated() - base
+        del out
+        reps = max(args.steps // 10, 5)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        result[name] = {"extra_device_bytes": int(extra), "ms": round(ms, 4),
+                        "samples_per_s": round(ss / (ms / 1e3), 1)}
+    line = {"workload": "compositor + distortion backward, recompute vs store: 2^22 samples, "
+                        f"{n} rays (truncated geometric, mean 64, max 1024)",
+            "n_samples": ss, "n_rays": n, "dtype": "f32", "data": "synthetic",
+            "store_minus_recompute_bytes": result["store"]["extra_device_bytes"] -
+                                           result["recompute"]["extra_device_bytes"], **result}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -419,8 +480,12 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default="train-step", choices=["train-step", "backward-memory"],
+                    help="backward-memory: the recompute-vs-store study of the compositor and distortion backward")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "backward-memory":
+        run_backward_memory(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

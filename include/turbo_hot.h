@@ -188,6 +188,18 @@ int tn_composite_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch,
                      const float* density, const float* rgb, const float* dt, const float* depth,
                      const uint32_t* n_used, const float* grad_rgba, float* dL_ddensity, float* dL_drgb);
 
+/* The store-instead-of-recompute alternative of the pair above (for the memory study of the
+ * backward): the forward also writes, for every composited sample, the transmittance after
+ * it and its weight (t_saved, w_saved [sample_stride]); the backward reads them instead of
+ * recomputing them. Same results within FP32 rounding; 8 more bytes per sample of memory. */
+int tn_composite_fwd_store(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                           float min_transmittance, const float* density, const float* rgb, const float* dt,
+                           float* rgba, uint32_t* n_used, float* t_saved, float* w_saved);
+int tn_composite_bwd_stored(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                            const float* density, const float* rgb, const float* dt, const uint32_t* n_used,
+                            const float* t_saved, const float* w_saved, const float* grad_rgba, float* dL_ddensity,
+                            float* dL_drgb);
+
 /* Reconstruction loss forward + backward in one pass (reference
  * fused_reconstruction_forward_backward_kernel, training-kernels-fused.cuh:381-498):
  * composite, random-background blend of target and prediction, smooth-L1 loss,

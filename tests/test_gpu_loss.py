@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import (RTOL_COMPOSITE, RTOL_GRAD, assert_close, assert_norm_close, assert_per_ray_norm_close,
+from tests.helpers import (RTOL_COMPOSITE, RTOL_GRAD, assert_bitwise, assert_close, assert_norm_close, assert_per_ray_norm_close,
                            dev, expand_rays, host, i32)
 from turbonerf_b200 import scenes
 
@@ -61,6 +61,16 @@ def test_composite_forward_and_vjp(mean, n_samples):
         assert_per_ray_norm_close(host(drgb)[c * ss:(c + 1) * ss], ref_drgb[c * ss:(c + 1) * ss], sb.counts, sb.offsets,
                                   RTOL_GRAD, f"dL/drgb[{c}]", ray_mask=ok)
     assert_norm_close(host(dd), ref_dd, RTOL_GRAD, "dL/dsigma (batch)", mask=sm)
+    # the store-instead-of-recompute variant: same composite, same VJP
+    st = hp.composite_fwd_store(ctx, rb, sig, rgb, dt)
+    assert_bitwise(host(st["n_used"]).view(np.uint32), used, "n_used (store variant)")
+    _rgb_ok(ref_rgba, host(st["rgba"]), n, ok)
+    dd2, drgb2 = hp.composite_bwd_stored(ctx, rb, sig, rgb, dt, st["n_used"], st["t_saved"], st["w_saved"],
+                                         dev(g.astype(np.float32)))
+    assert_per_ray_norm_close(host(dd2), ref_dd, sb.counts, sb.offsets, RTOL_GRAD, "dL/dsigma (stored)", ray_mask=ok)
+    for c in range(3):
+        assert_per_ray_norm_close(host(drgb2)[c * ss:(c + 1) * ss], ref_drgb[c * ss:(c + 1) * ss], sb.counts,
+                                  sb.offsets, RTOL_GRAD, f"dL/drgb[{c}] (stored)", ray_mask=ok)
     assert ctx.check() == 0
 
 

@@ -70,7 +70,8 @@ struct CompFwd {
 // T_j = exp(-sum_{i<j} sigma_i dt_i) and alpha_j = -expm1(-sigma_j dt_j). Sample j is
 // composited while T_j >= min_t, i.e. up to and including the first sample after which
 // the transmittance drops below min_t.
-__device__ CompFwd composite_forward_ray(const Samples& S, uint32_t o, uint32_t n, float min_t, int lane) {
+__device__ CompFwd composite_forward_ray(const Samples& S, uint32_t o, uint32_t n, float min_t, int lane,
+                                         float* __restrict__ t_out = nullptr, float* __restrict__ w_out = nullptr) {
     float carry = 0.0f, t_prev = 1.0f;
     float ar = 0.0f, ag = 0.0f, ab = 0.0f, aa = 0.0f;
     CompFwd out;
@@ -99,6 +100,10 @@ __device__ CompFwd composite_forward_ray(const Samples& S, uint32_t o, uint32_t 
             ag += w * cg;
             ab += w * cb;
             aa += w;
+            if (t_out) {
+                t_out[(size_t)o + j] = tn;  // transmittance after the sample
+                w_out[(size_t)o + j] = w;
+            }
         }
         if (term) {
             out.used = base + first + 1;
@@ -413,12 +418,13 @@ __device__ __forceinline__ uint32_t live_rays(uint32_t n_rays, const uint32_t* n
 __global__ void __launch_bounds__(LOSS_THREADS)
 composite_fwd_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
                      const uint32_t* __restrict__ offsets, float min_t, float* __restrict__ rgba,
-                     float* __restrict__ depth, uint32_t* __restrict__ n_used) {
+                     float* __restrict__ depth, uint32_t* __restrict__ n_used, float* __restrict__ t_out,
+                     float* __restrict__ w_out) {
     const int lane = threadIdx.x & 31;
     const uint32_t n_live = live_rays(n_rays, n_dev);
     const uint32_t nw = gridDim.x * LOSS_WARPS;
     for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
-        const CompFwd c = composite_forward_ray(S, offsets[r], counts[r], min_t, lane);
+        const CompFwd c = composite_forward_ray(S, offsets[r], counts[r], min_t, lane, t_out, w_out);
         if (lane == 0) {
             rgba[r] = c.r; rgba[r + rs] = c.g; rgba[r + 2 * (size_t)rs] = c.b; rgba[r + 3 * (size_t)rs] = c.a;
             if (depth) depth[r] = c.depth;
@@ -454,6 +460,54 @@ composite_bwd_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t
                                     drgb[s + S.ss] = xg;
                                     drgb[s + 2 * (size_t)S.ss] = xb;
                                 });
+        }
+    }
+}
+
+// VJP of the compositor from the forward's stored per-sample transmittance (after the sample)
+// and weights, the alternative to recomputing them (composite_bwd_kernel): the same suffix
+// sums, read instead of rebuilt.
+__global__ void __launch_bounds__(LOSS_THREADS)
+composite_bwd_stored_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs,
+                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                            const uint32_t* __restrict__ n_used, const float* __restrict__ t_saved,
+                            const float* __restrict__ w_saved, const float* __restrict__ grad_rgba,
+                            float* __restrict__ dd, float* __restrict__ drgb) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t nw = gridDim.x * LOSS_WARPS;
+    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
+        const uint32_t o = offsets[r], n = counts[r];
+        const uint32_t used = min(n_used[r], n);
+        const float gr = grad_rgba[r], gg = grad_rgba[r + rs], gb = grad_rgba[r + 2 * (size_t)rs],
+                    ga = grad_rgba[r + 3 * (size_t)rs];
+        zero_tail(dd, drgb, S.ss, o, used, n, lane);
+        float su = 0.0f;  // sum over later chunks of w u, u = gr r + gg g + gb b + ga
+        if (used == 0) continue;
+        for (int base = (int)(((used - 1) / WARP) * WARP); base >= 0; base -= WARP) {
+            const uint32_t j = (uint32_t)base + lane;
+            const bool valid = j < used;
+            float u = 0.0f, w = 0.0f, tn = 0.0f, dtv = 0.0f, sigma = 0.0f;
+            float cr = 0.0f, cg = 0.0f, cb = 0.0f;
+            if (valid) {
+                const size_t s = (size_t)o + j;
+                sigma = act_sigma(S.act, S.density[s]);
+                dtv = S.dt[s];
+                cr = S.rgb[s]; cg = S.rgb[s + S.ss]; cb = S.rgb[s + 2 * (size_t)S.ss];
+                tn = t_saved[s];
+                w = w_saved[s];
+                u = gr * cr + gg * cg + gb * cb + ga;
+            }
+            const float incl = warp_inclusive_suffix_sum(w * u, lane) + su;
+            const float u_ex = shift_down(incl, lane, su);
+            if (valid) {
+                const size_t s = (size_t)o + j;
+                dd[s] = dtv * (tn * u - u_ex) * act_dsigma(S.act, sigma);
+                drgb[s] = gr * w;
+                drgb[s + S.ss] = gg * w;
+                drgb[s + 2 * (size_t)S.ss] = gb * w;
+            }
+            su = __shfl_sync(FULL_MASK, incl, 0);
         }
     }
 }
@@ -1334,8 +1388,45 @@ int tn_composite_fwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch,
     const int grid = loss_grid((const void*)composite_fwd_kernel, batch->n_rays);
     composite_fwd_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
                                                             batch->counts, batch->offsets, min_transmittance, rgba,
-                                                            depth, n_used);
+                                                            depth, n_used, nullptr, nullptr);
     return check_launch("tn_composite_fwd");
+}
+
+int tn_composite_fwd_store(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                           float min_transmittance, const float* density, const float* rgb, const float* dt,
+                           float* rgba, uint32_t* n_used, float* t_saved, float* w_saved) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(rgba); TN_NONNULL(n_used);
+    TN_NONNULL(t_saved); TN_NONNULL(w_saved);
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
+    const int grid = loss_grid((const void*)composite_fwd_kernel, batch->n_rays);
+    composite_fwd_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
+                                                            batch->counts, batch->offsets, min_transmittance, rgba,
+                                                            nullptr, n_used, t_saved, w_saved);
+    return check_launch("tn_composite_fwd_store");
+}
+
+int tn_composite_bwd_stored(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                            const float* density, const float* rgb, const float* dt, const uint32_t* n_used,
+                            const float* t_saved, const float* w_saved, const float* grad_rgba, float* dL_ddensity,
+                            float* dL_drgb) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(n_used); TN_NONNULL(t_saved);
+    TN_NONNULL(w_saved); TN_NONNULL(grad_rgba); TN_NONNULL(dL_ddensity); TN_NONNULL(dL_drgb);
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
+    const int grid = loss_grid((const void*)composite_bwd_stored_kernel, batch->n_rays);
+    composite_bwd_stored_kernel<<<grid, LOSS_THREADS, 0, stream>>>(
+        S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, batch->counts, batch->offsets, n_used, t_saved,
+        w_saved, grad_rgba, dL_ddensity, dL_drgb);
+    return check_launch("tn_composite_bwd_stored");
 }
 
 int tn_composite_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,

@@ -222,6 +222,33 @@ def composite_bwd(ctx, rb: RayBatchDesc, density, rgb, dt, depth, n_used, grad_r
     return dd, drgb
 
 
+def composite_fwd_store(ctx, rb: RayBatchDesc, density, rgb, dt, activation=0, min_t=1e-4, out=None):
+    """Compositor forward that also stores every composited sample's transmittance (after the
+    sample) and weight, for composite_bwd_stored."""
+    dev = density.device
+    rs, ss = rb.ray_stride, rb.sample_stride
+    if out is None:
+        out = dict(rgba=torch.zeros(4 * rs, dtype=torch.float32, device=dev),
+                   n_used=torch.zeros(rs, dtype=torch.int32, device=dev),
+                   t_saved=torch.empty(ss, dtype=torch.float32, device=dev),
+                   w_saved=torch.empty(ss, dtype=torch.float32, device=dev))
+    call("tn_composite_fwd_store", ctx.handle, _stream(), ctypes.byref(rb), activation, min_t, _ptr(density),
+         _ptr(rgb), _ptr(dt), _ptr(out["rgba"]), _ptr(out["n_used"]), _ptr(out["t_saved"]), _ptr(out["w_saved"]))
+    return out
+
+
+def composite_bwd_stored(ctx, rb: RayBatchDesc, density, rgb, dt, n_used, t_saved, w_saved, grad_rgba, activation=0,
+                         out=None):
+    dev = density.device
+    ss = rb.sample_stride
+    if out is None:
+        out = (torch.zeros(ss, dtype=torch.float32, device=dev), torch.zeros(3 * ss, dtype=torch.float32, device=dev))
+    dd, drgb = out
+    call("tn_composite_bwd_stored", ctx.handle, _stream(), ctypes.byref(rb), activation, _ptr(density), _ptr(rgb),
+         _ptr(dt), _ptr(n_used), _ptr(t_saved), _ptr(w_saved), _ptr(grad_rgba), _ptr(dd), _ptr(drgb))
+    return dd, drgb
+
+
 def recon_loss_fwd_bwd(ctx, rb: RayBatchDesc, density, rgb, dt, target_rgba, bg_rgb, inv_nrays, grad_scale=1.0,
                        activation=0, min_t=1e-4):
     dev = density.device
@@ -360,3 +387,25 @@ def synth_field(pos, pos_stride, n, aabb_size, blobs, waves, n_dev=None, out_str
     call("tn_synth_field", _stream(), n, _ptr(n_dev), pos_stride, _ptr(pos), aabb_size, blobs.shape[0], _ptr(blobs),
          _ptr(waves), _ptr(sigma), _ptr(rgb), out_stride)
     return sigma, rgb
+
+
+# ---- backward variants of the memory study -------------------------------------------------
+def backward_recompute(ctx, rb: RayBatchDesc, density, rgb, dt, m_norm, dt_norm, grad_rgba, lam, activation=0):
+    """Compositor forward (per-ray state only) + backward that recomputes transmittance, and the
+    fused distortion forward/backward. Returns (dL/d density of the compositor, dL/d rgb,
+    dL/d density of the distortion loss)."""
+    out = composite_fwd(ctx, rb, density, rgb, dt, activation=activation)
+    dd, drgb = composite_bwd(ctx, rb, density, rgb, dt, out["depth"], out["n_used"], grad_rgba, activation=activation)
+    d = distortion_fwd_bwd(ctx, rb, density, m_norm, dt_norm, lam, activation=activation)
+    return dd, drgb, d["dL_ddensity"]
+
+
+def backward_store(ctx, rb: RayBatchDesc, density, rgb, dt, m_norm, dt_norm, grad_rgba, lam, activation=0):
+    """Compositor forward that stores per-sample transmittance and weights + backward that reads
+    them, and the distortion loss as a forward kernel that stores per-sample running sums and a
+    backward kernel that reads them. Same returns as backward_recompute."""
+    st = composite_fwd_store(ctx, rb, density, rgb, dt, activation=activation)
+    dd, drgb = composite_bwd_stored(ctx, rb, density, rgb, dt, st["n_used"], st["t_saved"], st["w_saved"], grad_rgba,
+                                    activation=activation)
+    _, ddist, _ = plain_distortion(rb, density, m_norm, dt_norm, lam, activation=activation)
+    return dd, drgb, ddist

@@ -129,6 +129,8 @@ SIGNATURES = {
     "tn_compact_nonzero": [_vp, _vp, _u32, _vp, _vp, _vp],
     "tn_composite_fwd": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_composite_bwd": [_vp, _vp, _P(RayBatchDesc), _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "tn_composite_fwd_store": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "tn_composite_bwd_stored": [_vp, _vp, _P(RayBatchDesc), _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_recon_loss_fwd_bwd": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _f32, _f32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                               _vp, _vp, _vp],
     "tn_distortion_fwd_bwd": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
