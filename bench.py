@@ -471,6 +471,124 @@ def run_backward_memory(args):
     print(json.dumps(line), flush=True)
 
 
+def _multi_scene_gpu(params, resolution=128, threshold=THRESHOLD):
+    """Scenes of the multi-scene workload with their occupancy grids built on the device: per
+    level, the field's density at every cell centre (Morton order) thresholded into that
+    level's bit."""
+    import torch
+    from turbonerf_b200 import hotpath as hp, scenes
+    ms = scenes.make_multi_scene(params, resolution=resolution, grids=False)
+    V = resolution ** 3
+    m = np.arange(V, dtype=np.uint32)
+    unit = np.stack([(scenes.morton3d_invert(m >> np.uint32(c)).astype(np.float64) - resolution / 2 + 0.5) / resolution
+                     for c in range(3)])  # [3][V]: centres of a level of size 1
+    unit_d = torch.from_numpy(unit).cuda()
+    table, grids = [], []
+    for sc, b, p in zip(ms.scenes, ms.ray_begin, params):
+        base = float(np.float32(p["aabb"]) / np.float32(1 << (p["n_levels"] - 1)))
+        bits = torch.zeros(V, dtype=torch.uint8, device="cuda")
+        blobs = torch.from_numpy(sc.field.blobs).cuda()
+        waves = torch.from_numpy(sc.field.waves).cuda()
+        for k in range(p["n_levels"]):
+            ls = float(np.float32(base) * np.float32(1 << k))
+            pos = (unit_d * ls).float().contiguous().view(-1)
+            sigma, _ = hp.synth_field(pos, V, V, p["aabb"], blobs, waves, want_rgb=False)
+            bits |= (sigma > threshold).to(torch.uint8) << k
+        g = hp.GridSpec(p["n_levels"], resolution, base)
+        mk = hp.MarchSpec(sc.cone_angle, sc.dt_min, sc.dt_max, sc.max_steps)
+        table.append(dict(grid=g, bitfield=bits, bbox=sc.bbox, march=mk, inv_aabb=1.0 / sc.aabb_size,
+                          ray_begin=int(b), n_rays=sc.rays.n))
+    return ms, table
+
+
+def run_multi_scene(args):
+    """Batched multi-scene march: 16 scenes, each its own blob field (8-32 blobs), 1-5 cascades
+    of 128^3 and an AABB of size 0.5-16, ray counts log-uniform in 2^10..2^16, rays from a
+    sphere of radius 4A/3 toward the centre (cone stepping 1/256). Times the march count +
+    emit of every scene (no batch cut) two ways, each captured in a CUDA graph and replayed:
+      * persistent: one work-stealing count launch and one emit launch for all scenes;
+      * per-scene: tn_march_count + tn_march_emit once per scene.
+    A second workload scales every scene's ray count by one factor so that the batch holds
+    about 2^19 samples. Per-scene counts and samples of the persistent launch are checked
+    bit-exact against the oracle by tests/test_gpu_multi_scene.py."""
+    import torch
+    from turbonerf_b200 import hotpath as hp, scenes
+
+    torch.cuda.set_device(0)
+    params = scenes.multi_scene_params(seed=0x7C3, n_scenes=16, ray_lo=1 << 10, ray_hi=1 << 16)
+    out = {"workload": "batched multi-scene march count + emit: 16 scenes, 8-32 blobs, 1-5 cascades of 128^3, "
+                       "AABB 0.5-16, rays log-uniform 2^10..2^16", "dtype": "f32", "data": "synthetic"}
+    for label, scale in (("as_drawn", None), ("scaled_2e19_samples", 1 << 19)):
+        ps = [dict(p) for p in params]
+        if scale is not None:
+            f = scale / max(out["as_drawn"]["n_samples"], 1)
+            for p in ps:
+                p["n_rays"] = max(1, int(round(p["n_rays"] * f)))
+        ms, table_in = _multi_scene_gpu(ps)
+        table = hp.scene_table(table_in)
+        R = ms.rays.n
+        d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        ori, dr, t, tmax, alive = d(ms.rays.ori), d(ms.rays.dir), d(ms.rays.t), d(ms.rays.t_max), d(ms.rays.alive)
+        ctx = hp.Context()
+        n_steps, scene_samples, info = hp.multi_march_count(ctx, table, R, ori, dr, t, tmax, alive)
+        total = int(info[1].item())
+        per_scene = scene_samples.cpu().numpy().astype(np.int64)
+        ss = total + 64
+        samples = hp.alloc_samples(ss, "cuda")
+        offsets = torch.zeros(R, dtype=torch.int32, device="cuda")
+
+        def persistent():
+            hp.multi_march_count(ctx, table, R, ori, dr, t, tmax, alive, n_steps=n_steps, scene_samples=scene_samples,
+                                 info=info)
+            hp.multi_march_emit(ctx, table, R, ss, ori, dr, t, alive, n_steps, samples=samples, offsets=offsets)
+
+        ctx_s = hp.Context()
+        bufs = []
+        for sc_in, ns_k in zip(table_in, per_scene):
+            b, n = sc_in["ray_begin"], sc_in["n_rays"]
+            bufs.append(dict(b=b, n=n, ss=int(ns_k) + 64, samples=hp.alloc_samples(int(ns_k) + 64, "cuda"),
+                             n_steps=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                             offsets=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                             info=torch.zeros(4, dtype=torch.int32, device="cuda")))
+
+        def one_per_scene():
+            for sc_in, bf in zip(table_in, bufs):
+                b, n = bf["b"], bf["n"]
+                ns_k, inf = hp.march_count(ctx_s, sc_in["grid"], sc_in["bitfield"], sc_in["bbox"], sc_in["march"], n,
+                                           R, ori[b:], dr[b:], t[b:], tmax[b:], alive[b:], 0xFFFFFFFF,
+                                           n_steps=bf["n_steps"], batch_info=bf["info"])
+                hp.march_emit(ctx_s, sc_in["grid"], sc_in["bitfield"], sc_in["bbox"], sc_in["march"],
+                              sc_in["inv_aabb"], n, R, bf["ss"], inf, ori[b:], dr[b:], t[b:], alive[b:], ns_k,
+                              offsets=bf["offsets"], samples=bf["samples"])
+
+        res = {"n_rays": R, "n_samples": total, "rays_per_scene": [int(p["n_rays"]) for p in ps],
+               "samples_per_scene": [int(v) for v in per_scene]}
+        for name, fn in (("persistent", persistent), ("per_scene", one_per_scene)):
+            for _ in range(max(args.warmup, 3)):
+                fn()
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                fn()
+            reps = max(args.steps, 10)
+            for _ in range(3):
+                g.replay()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                g.replay()
+            e1.record()
+            e1.synchronize()
+            ms_ = e0.elapsed_time(e1) / reps
+            res[name] = {"ms": round(ms_, 4), "samples_per_s": round(total / (ms_ / 1e3), 1)}
+            del g
+        assert ctx.check() == 0 and ctx_s.check() == 0
+        res["persistent_speedup"] = round(res["per_scene"]["ms"] / res["persistent"]["ms"], 3)
+        out[label] = res
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -480,11 +598,14 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="train-step", choices=["train-step", "backward-memory"],
-                    help="backward-memory: the recompute-vs-store study of the compositor and distortion backward")
+    ap.add_argument("--workload", default="train-step", choices=["train-step", "backward-memory", "multi-scene"],
+                    help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "
+                         "multi-scene: the batched persistent march of 16 scenes against one launch per scene")
     args = ap.parse_args()
     if args.workload == "backward-memory":
         run_backward_memory(args)
+    elif args.workload == "multi-scene":
+        run_multi_scene(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -148,6 +148,37 @@ int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, con
                   uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir, float* out_dt,
                   float* out_m_norm, float* out_dt_norm);
 
+/* ---- several scenes in one launch (batched multi-scene training) -------------------
+ * No single reference call: the reference trains one scene per process. These entry points run
+ * the march count and emit of many scenes at once; per scene, counts, offsets and samples equal
+ * those of tn_march_count / tn_march_emit without a batch cut (batch_size = UINT32_MAX). */
+typedef struct tn_scene {
+    tn_grid_desc grid;
+    const uint8_t* bitfield;   /* device, R^3 bytes, 16-byte aligned */
+    tn_bbox bbox;
+    tn_march_desc march;
+    float inv_aabb_size;       /* emit: 1 / aabb size of the scene */
+    uint32_t ray_begin;        /* first ray of the scene in the shared ray arrays */
+    uint32_t n_rays;           /* scenes are given in ray order and do not overlap */
+} tn_scene;
+#define TN_MAX_SCENES 32
+
+/* Counts the steps of every ray of every scene in one persistent launch: blocks take 64-ray
+ * chunks of any scene from a shared counter (work stealing). Writes n_steps and alive for
+ * every scene ray, scene_samples[n_scenes] (device, optional: samples per scene) and
+ * batch_info[4] (device: total rays, total samples). Samples are packed scene after scene. */
+int tn_multi_march_count(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, const tn_scene* scenes,
+                         uint32_t ray_stride, const float* ori, const float* dir, const float* ray_t,
+                         const float* ray_t_max, uint8_t* alive, uint32_t* n_steps, uint32_t* scene_samples,
+                         uint32_t* batch_info);
+/* Offsets (exclusive scan over all scene rays, in scene order) and the samples of every scene
+ * (same outputs as tn_march_emit), after tn_multi_march_count on the same context and scenes. */
+int tn_multi_march_emit(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, const tn_scene* scenes,
+                        uint32_t ray_stride, uint32_t sample_stride, const uint32_t* ray_img_id, const float* ori,
+                        const float* dir, const float* ray_t, const uint8_t* alive, const uint32_t* n_steps,
+                        uint32_t* offsets, uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir,
+                        float* out_dt, float* out_m_norm, float* out_dt_norm);
+
 /* Exclusive scan + batch cut of arbitrary counts (reference trainer.cu:146-183 with
  * find_last_lt_presorted, src/utils/parallel-utils.cuh:31-58). batch_info as above. */
 int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,

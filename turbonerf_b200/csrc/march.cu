@@ -301,6 +301,7 @@ struct CountGrid {
     uint32_t res_m1;             // R - 1
     int res_shift;               // log2 R
     uint32_t plane_words;        // R^3 / 32: words per level of the bit-planes
+    int n_levels;
     const uint8_t* __restrict__ bits;     // the bitfield, one byte per cell (bit k = level k)
     const uint32_t* __restrict__ planes;  // the same bits as one plane per level, 32 cells per word
 };
@@ -313,11 +314,12 @@ struct CountGrid {
 //   m < half0 * 2^j  <=>  j > (bits(m) - bits(half0)) / 2^23,
 //   cell0 * 2^j > dt  <=>  j > (bits(dt) - bits(cell0)) / 2^23,
 // and the first such j is the quotient (an arithmetic shift) plus one, at least 0.
+// NL = 0: the level count is only known at run time (nl_rt).
 template <int NL>
-__device__ __forceinline__ int count_level(float m, float dt, int half0_bits, int cell0_bits) {
+__device__ __forceinline__ int count_level(float m, float dt, int half0_bits, int cell0_bits, int nl_rt) {
     const int jp = (__float_as_int(m) - half0_bits) >> 23;
     const int jd = (__float_as_int(dt) - cell0_bits) >> 23;
-    return min(max(max(jp, jd) + 1, 0), NL - 1);
+    return min(max(max(jp, jd) + 1, 0), (NL ? NL : nl_rt) - 1);
 }
 
 // a / b rounded toward +infinity for finite a >= b > 0 (the __fdiv_ru of get_dt_to_next_voxel,
@@ -378,7 +380,7 @@ __device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const Ray
         if (!bbox_contains(a.bbox, x, y, z)) break;
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
         const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));
-        const int k = count_level<NL>(m, dt, cg.half0_bits, cg.cell0_bits);
+        const int k = count_level<NL>(m, dt, cg.half0_bits, cg.cell0_bits, cg.n_levels);
         const float ils = __fmul_rn(cg.inv_ls0, pow2i(-k));
         const float fx = __fmul_rn(__fadd_rn(__fmul_rn(x, ils), 0.5f), cg.res_f);
         const float fy = __fmul_rn(__fadd_rn(__fmul_rn(y, ils), 0.5f), cg.res_f);
@@ -544,30 +546,13 @@ march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* _
 // computes from the same t: dt = get_dt(t), the position o + t d, m = t + dt/2, the ray's span
 // from its start t to the end of its last step. Rays with more samples than slots fall back to
 // replaying their march.
-constexpr int EXPAND_WARPS = 8;
-
-__global__ void __launch_bounds__(EXPAND_WARPS * WARP)
-expand_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
-              const uint32_t* __restrict__ batch_info, const uint32_t* __restrict__ block_prefix,
-              const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
-              const float* __restrict__ ray_t, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ counts,
-              uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags, const float* __restrict__ slots,
-              uint32_t slot_cap) {
-    const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
-    const int lane = threadIdx.x & 31;
-    const uint32_t r_i = blockIdx.x * EXPAND_WARPS + (threadIdx.x >> 5);
-    if (r_i >= n_live) return;
-    const uint32_t g0 = r_i / COUNT_GROUP * COUNT_GROUP;
-    uint32_t part = 0;
-    for (uint32_t j = g0 + lane; j < r_i; j += WARP) part += counts[j];
-    const uint32_t o0 = warp_sum(part) + block_prefix[r_i / COUNT_GROUP];
-    const uint32_t n = counts[r_i];
-    if (lane == 0) offsets[r_i] = o0;
-    if (r_i >= batch_info[0] || n == 0 || !alive[r_i]) return;
-    if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
-        if (lane == 0) raise_flag(flags, ERR_CAPACITY);
-        return;
-    }
+// Writes the n samples of ray r_i at o0.. from its recorded step positions (one lane per sample),
+// or, for a ray with more samples than slots, by replaying its march on lane 0.
+__device__ __forceinline__ void expand_ray(const MarchArgs& a, float inv_aabb, uint32_t r_i, uint32_t o0, uint32_t n,
+                                           uint32_t rs, const uint32_t* __restrict__ img_id,
+                                           const float* __restrict__ ori, const float* __restrict__ dir,
+                                           const float* __restrict__ ray_t, const SampleOut& o,
+                                           const float* __restrict__ slots, uint32_t slot_cap, int lane) {
     RayMarch r;
     load_ray(r, ori, dir, r_i, rs);
     r.t = ray_t[r_i];
@@ -595,6 +580,33 @@ expand_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __re
     }
 }
 
+constexpr int EXPAND_WARPS = 8;
+
+__global__ void __launch_bounds__(EXPAND_WARPS * WARP)
+expand_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
+              const uint32_t* __restrict__ batch_info, const uint32_t* __restrict__ block_prefix,
+              const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
+              const float* __restrict__ ray_t, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ counts,
+              uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags, const float* __restrict__ slots,
+              uint32_t slot_cap) {
+    const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
+    const int lane = threadIdx.x & 31;
+    const uint32_t r_i = blockIdx.x * EXPAND_WARPS + (threadIdx.x >> 5);
+    if (r_i >= n_live) return;
+    const uint32_t g0 = r_i / COUNT_GROUP * COUNT_GROUP;
+    uint32_t part = 0;
+    for (uint32_t j = g0 + lane; j < r_i; j += WARP) part += counts[j];
+    const uint32_t o0 = warp_sum(part) + block_prefix[r_i / COUNT_GROUP];
+    const uint32_t n = counts[r_i];
+    if (lane == 0) offsets[r_i] = o0;
+    if (r_i >= batch_info[0] || n == 0 || !alive[r_i]) return;
+    if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
+        if (lane == 0) raise_flag(flags, ERR_CAPACITY);
+        return;
+    }
+    expand_ray(a, inv_aabb, r_i, o0, n, rs, img_id, ori, dir, ray_t, o, slots, slot_cap, lane);
+}
+
 // Bits k of the four bytes of x (cells 4j .. 4j+3) as four consecutive bits: the mask leaves
 // them at bit positions 0, 8, 16, 24, and the multiply by 1 + 2^7 + 2^14 + 2^21 moves them to
 // 21..24 without any two partial products meeting.
@@ -608,14 +620,14 @@ __device__ __forceinline__ uint32_t gather_level_bits(uint32_t x, int k) {
 //    (words 2m and 2m + 1 of every plane come from this block);
 //  * reduces, per level, the box of occupied blocks into box[lo x,y,z per level | hi+1 x,y,z
 //    per level] (lo starts at a large value, hi at 0), the input of the count pass's tail cut.
-__global__ void __launch_bounds__(256)
-build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8_t* __restrict__ mip, int* box,
-                 uint32_t* __restrict__ planes, uint32_t plane_words) {
+__device__ __forceinline__ void build_mip_block(int cshift, int n_levels, const uint4* __restrict__ bits,
+                                                uint8_t* __restrict__ mip, int* box, uint32_t* __restrict__ planes,
+                                                uint32_t plane_words, uint32_t block) {
     __shared__ int sbox[BOX_INTS];
     if (threadIdx.x < BOX_INTS) sbox[threadIdx.x] = threadIdx.x < BOX_INTS / 2 ? 0x7fffffff : 0;
     __syncthreads();
     const uint32_t C = 1u << cshift;
-    const uint32_t c = blockIdx.x * 256 + threadIdx.x;
+    const uint32_t c = block * 256 + threadIdx.x;
     uint32_t v = 0, cx = 0, cy = 0, cz = 0;
     if (c < C * C * C) {
         cx = c & (C - 1);
@@ -671,6 +683,197 @@ build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8
             atomicMax(box + threadIdx.x, val);
         }
     }
+}
+
+__global__ void __launch_bounds__(256)
+build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8_t* __restrict__ mip, int* box,
+                 uint32_t* __restrict__ planes, uint32_t plane_words) {
+    build_mip_block(cshift, n_levels, bits, mip, box, planes, plane_words, blockIdx.x);
+}
+
+// ---- several scenes in one launch ---------------------------------------------------------
+// The scenes' rays sit in one set of ray arrays, scene after scene, and their samples are
+// packed the same way. Each scene keeps its own grid, bitfield, box and march parameters. The
+// count pass is one persistent launch: blocks take COUNT_GROUP-ray chunks of any scene from a
+// shared counter (work stealing) and stage a scene's coarse mip when they move to another scene.
+// The block that finishes the last chunk scans all chunk totals. The emit pass is one launch
+// with a warp per ray. The per-scene results equal those of a tn_march_count / tn_march_emit
+// call per scene without a batch cut.
+constexpr int MAX_SCENES = 32;
+
+struct SceneParams {
+    MarchArgs a;
+    CountGrid cg;
+    float inv_aabb;
+    uint32_t ray_begin, n_rays, chunk_begin;
+    int use_mip, cshift;
+    uint32_t mip_blocks;  // build_mip blocks of 256 coarse blocks
+    uint8_t* mip;
+    int* box;
+};
+
+struct MultiArgs {
+    uint32_t n_scenes, total_chunks, total_rays, spread_res;
+    SceneParams sp[MAX_SCENES];
+};
+
+__device__ __forceinline__ int scene_of_chunk(const MultiArgs& A, uint32_t chunk) {
+    int s = 0;
+    for (int k = 1; k < (int)A.n_scenes; ++k)
+        if (chunk >= A.sp[k].chunk_begin) s = k;
+    return s;
+}
+
+__device__ __forceinline__ int scene_of_ray(const MultiArgs& A, uint32_t ray) {
+    int s = 0;
+    for (int k = 1; k < (int)A.n_scenes; ++k)
+        if (ray >= A.sp[k].ray_begin) s = k;
+    return s;
+}
+
+// Per scene: the occupied-box reduction starts from lo = large, hi = 0.
+__global__ void multi_box_init_kernel(const __grid_constant__ MultiArgs A) {
+    const uint32_t s = blockIdx.x, i = threadIdx.x;
+    if (s < A.n_scenes && A.sp[s].use_mip && i < (uint32_t)BOX_INTS)
+        A.sp[s].box[i] = i < (uint32_t)BOX_INTS / 2 ? 0x7fffffff : 0;
+}
+
+__global__ void __launch_bounds__(256) multi_build_mip_kernel(const __grid_constant__ MultiArgs A) {
+    const SceneParams& sp = A.sp[blockIdx.y];
+    if (!sp.use_mip || blockIdx.x >= sp.mip_blocks) return;  // whole blocks leave together
+    build_mip_block(sp.cshift, sp.a.g.n_levels, reinterpret_cast<const uint4*>(sp.a.g.bits), sp.mip, sp.box,
+                    const_cast<uint32_t*>(sp.cg.planes), sp.cg.plane_words, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(COUNT_GROUP)
+multi_count_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const float* __restrict__ ori,
+                   const float* __restrict__ dir, const float* __restrict__ ray_t, const float* __restrict__ ray_t_max,
+                   uint8_t* __restrict__ alive, uint32_t* counts, uint32_t* block_agg, uint32_t* block_prefix,
+                   uint32_t* work, uint32_t* ticket, uint32_t* flags, float* __restrict__ slots, uint32_t slot_cap,
+                   uint32_t* __restrict__ scene_samples, uint32_t* batch_info) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint32_t* spread = reinterpret_cast<uint32_t*>(smem);
+    uint8_t* mip = smem + (size_t)12 * A.spread_res;
+    __shared__ float ubox_s[6];
+    __shared__ int cut_s;
+    __shared__ uint32_t chunk_s;
+    __shared__ uint32_t wsum[COUNT_GROUP / WARP];
+    __shared__ bool last_s;
+    const uint32_t res = A.spread_res;
+    for (uint32_t c = threadIdx.x; c < res; c += COUNT_GROUP) {
+        const uint32_t v = part1by2(c);
+        spread[c] = v;
+        spread[res + c] = v << 1;
+        spread[2 * res + c] = v << 2;
+    }
+    int staged = -1;
+    for (;;) {
+        if (threadIdx.x == 0) chunk_s = atomicAdd(work, 1u);
+        __syncthreads();
+        const uint32_t chunk = chunk_s;
+        if (chunk >= A.total_chunks) break;
+        const int s = scene_of_chunk(A, chunk);
+        const SceneParams& sp = A.sp[s];
+        if (s != staged) {
+            if (sp.use_mip) {
+                const uint32_t n16 = (1u << (3 * sp.cshift)) / 16;
+                const uint4* src = reinterpret_cast<const uint4*>(sp.mip);
+                uint4* dst = reinterpret_cast<uint4*>(mip);
+#pragma unroll 8
+                for (uint32_t k = threadIdx.x; k < n16; k += COUNT_GROUP) dst[k] = __ldg(src + k);
+                if (threadIdx.x == 0) occupied_union(sp.cg, sp.box, sp.a.g.n_levels, ubox_s, &cut_s);
+            }
+            staged = s;
+            __syncthreads();
+        }
+        const uint32_t local = (chunk - sp.chunk_begin) * COUNT_GROUP + threadIdx.x;
+        const uint32_t i = sp.ray_begin + local;
+        uint32_t cnt = 0;
+        if (local < sp.n_rays) {
+            if (alive[i]) {
+                RayMarch r;
+                load_ray(r, ori, dir, i, rs);
+                r.t = ray_t[i];
+                const float t_max = ray_t_max[i];
+                float t_stop = INFINITY;
+                bool meets = true;
+                if (sp.use_mip) {
+                    if (cut_s == 2) meets = false;
+                    else meets = ray_box_exit(r, ubox_s, t_max, __fmul_rn(sp.cg.cell0, 65536.0f), &t_stop);
+                }
+                const float below = nextafterf(t_max, -INFINITY);
+                const float t_lim = t_stop < below ? t_stop : below;
+                const uint32_t ms = sp.a.max_steps ? sp.a.max_steps : 0xffffffffu;
+                float* sl = slots ? slots + (size_t)i * slot_cap : nullptr;
+                const uint32_t sc = slots ? slot_cap : 0u;
+                if (meets) {
+                    if (sp.use_mip)
+                        cnt = count_ray<0, true>(sp.a, sp.cg, r, t_lim, ms, flags, mip, spread, sl, sc);
+                    else
+                        cnt = count_ray<0, false>(sp.a, sp.cg, r, t_lim, ms, flags, mip, spread, sl, sc);
+                }
+                if (cnt == 0) alive[i] = 0;
+            }
+            counts[i] = cnt;
+        }
+        __threadfence();
+        const uint32_t ws = warp_sum(cnt);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = ws;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t tot = 0;
+#pragma unroll
+            for (int w = 0; w < COUNT_GROUP / WARP; ++w) tot += wsum[w];
+            block_agg[chunk] = tot;
+            __threadfence();
+            last_s = atomicAdd(ticket, 1u) == A.total_chunks - 1;
+        }
+        __syncthreads();
+        if (last_s) {
+            __threadfence();
+            scan_blocks_and_cut<COUNT_GROUP>(A.total_chunks, A.total_rays, counts, block_agg, block_prefix,
+                                             0xffffffffu, batch_info, flags);
+            __syncthreads();
+            if (scene_samples && threadIdx.x < A.n_scenes) {
+                // a scene's samples start at its first chunk's prefix; scenes without rays at the
+                // end of the table start at the batch total
+                const uint32_t s0 = threadIdx.x;
+                const uint32_t cb = A.sp[s0].chunk_begin;
+                const uint32_t ce = s0 + 1 < A.n_scenes ? A.sp[s0 + 1].chunk_begin : A.total_chunks;
+                const uint32_t b = cb < A.total_chunks ? block_prefix[cb] : batch_info[2];
+                const uint32_t e = ce < A.total_chunks ? block_prefix[ce] : batch_info[2];
+                scene_samples[s0] = e - b;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(EXPAND_WARPS * WARP)
+multi_expand_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const uint32_t* __restrict__ block_prefix,
+                    const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
+                    const float* __restrict__ ray_t, const uint8_t* __restrict__ alive,
+                    const uint32_t* __restrict__ counts, uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags,
+                    const float* __restrict__ slots, uint32_t slot_cap) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t r_i = blockIdx.x * EXPAND_WARPS + (threadIdx.x >> 5);
+    const uint32_t last = A.sp[A.n_scenes - 1].ray_begin + A.sp[A.n_scenes - 1].n_rays;
+    if (r_i >= last) return;
+    const SceneParams& sp = A.sp[scene_of_ray(A, r_i)];
+    if (r_i - sp.ray_begin >= sp.n_rays) return;  // a gap between scenes
+    const uint32_t local = r_i - sp.ray_begin;
+    const uint32_t chunk = sp.chunk_begin + local / COUNT_GROUP;
+    const uint32_t g0 = sp.ray_begin + (local / COUNT_GROUP) * COUNT_GROUP;
+    uint32_t part = 0;
+    for (uint32_t j = g0 + lane; j < r_i; j += WARP) part += counts[j];
+    const uint32_t o0 = warp_sum(part) + block_prefix[chunk];
+    const uint32_t n = counts[r_i];
+    if (lane == 0) offsets[r_i] = o0;
+    if (n == 0 || !alive[r_i]) return;
+    if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
+        if (lane == 0) raise_flag(flags, ERR_CAPACITY);
+        return;
+    }
+    expand_ray(sp.a, sp.inv_aabb, r_i, o0, n, rs, img_id, ori, dir, ray_t, o, slots, slot_cap, lane);
 }
 
 // ---- compaction: ascending indices of non-zero values ---------------------------------
@@ -823,6 +1026,7 @@ static int make_count_grid(const MarchArgs& a, CountGrid& cg) {
     cg.res_shift = 0;
     while ((1 << cg.res_shift) < g.res) ++cg.res_shift;
     cg.plane_words = (uint32_t)(((uint64_t)g.res * g.res * g.res) / 32);
+    cg.n_levels = g.n_levels;
     cg.bits = g.bits;
     cg.planes = nullptr;
     for (int k = 0; k < g.n_levels; ++k) {
@@ -832,6 +1036,78 @@ static int make_count_grid(const MarchArgs& a, CountGrid& cg) {
                    TN_E_INVALID, "march: base_size %g out of range for %d levels", g.base, g.n_levels);
     }
     return TN_OK;
+}
+
+// Per-scene parameters of a multi-scene launch; scratch: per scene [mip | box | planes] in
+// ctx->mip, each part 256-byte aligned.
+static int make_multi_args(tn_ctx* ctx, uint32_t n_scenes, const tn_scene* scenes, uint32_t ray_stride,
+                           MultiArgs& A, bool build_scratch) {
+    TN_NONNULL(scenes);
+    TN_REQUIRE(n_scenes >= 1 && n_scenes <= (uint32_t)MAX_SCENES, TN_E_INVALID, "n_scenes = %u outside 1..%d", n_scenes,
+               MAX_SCENES);
+    std::memset(&A, 0, sizeof(A));
+    A.n_scenes = n_scenes;
+    uint32_t chunk = 0, prev_end = 0, max_res = 0;
+    size_t scratch = 0;
+    for (uint32_t s = 0; s < n_scenes; ++s) {
+        const tn_scene& sc = scenes[s];
+        SceneParams& sp = A.sp[s];
+        int st = make_march_args(&sc.grid, sc.bitfield, &sc.bbox, &sc.march, sp.a);
+        if (st != TN_OK) return st;
+        st = make_count_grid(sp.a, sp.cg);
+        if (st != TN_OK) return st;
+        TN_REQUIRE(sc.ray_begin >= prev_end, TN_E_INVALID, "scene %u: rays must follow the previous scene's", s);
+        TN_REQUIRE((uint64_t)sc.ray_begin + sc.n_rays <= ray_stride, TN_E_INVALID, "scene %u: rays beyond ray_stride", s);
+        prev_end = sc.ray_begin + sc.n_rays;
+        sp.inv_aabb = sc.inv_aabb_size;
+        sp.ray_begin = sc.ray_begin;
+        sp.n_rays = sc.n_rays;
+        sp.chunk_begin = chunk;
+        chunk += (sc.n_rays + COUNT_GROUP - 1) / COUNT_GROUP;
+        const int res = sc.grid.resolution;
+        max_res = std::max<uint32_t>(max_res, (uint32_t)res);
+        sp.use_mip = res >= MIP_MIN_RES && res <= MIP_MAX_RES;
+        sp.cshift = sp.cg.res_shift - 2;
+        if (sp.use_mip) {
+            TN_REQUIRE(((uintptr_t)sc.bitfield & 15u) == 0, TN_E_INVALID, "scene %u: bitfield must be 16-byte aligned", s);
+            const size_t mip_bytes = (size_t)1 << (3 * sp.cshift);
+            sp.mip_blocks = (uint32_t)((mip_bytes + 255) / 256);
+            const size_t box_off = (mip_bytes + 255) & ~(size_t)255;
+            const size_t planes_off = (box_off + BOX_INTS * sizeof(int) + 255) & ~(size_t)255;
+            const size_t end = planes_off + (size_t)sc.grid.n_levels * sp.cg.plane_words * sizeof(uint32_t);
+            // pointers are filled once the scratch is allocated
+            sp.mip = reinterpret_cast<uint8_t*>(scratch);
+            sp.box = reinterpret_cast<int*>(scratch + box_off);
+            sp.cg.planes = reinterpret_cast<const uint32_t*>(scratch + planes_off);
+            scratch += (end + 255) & ~(size_t)255;
+        }
+    }
+    A.total_chunks = chunk;
+    A.total_rays = prev_end;
+    A.spread_res = max_res;
+    if (build_scratch && scratch) {
+        const int st = ensure_mip(ctx, scratch);
+        if (st != TN_OK) return st;
+    }
+    const uintptr_t base = (uintptr_t)ctx->mip;
+    for (uint32_t s = 0; s < n_scenes; ++s) {
+        SceneParams& sp = A.sp[s];
+        if (!sp.use_mip) continue;
+        sp.mip = reinterpret_cast<uint8_t*>(base + (uintptr_t)sp.mip);
+        sp.box = reinterpret_cast<int*>(base + (uintptr_t)sp.box);
+        sp.cg.planes = reinterpret_cast<const uint32_t*>(base + (uintptr_t)sp.cg.planes);
+    }
+    return TN_OK;
+}
+
+// Per-ray step-position slots of a multi-scene launch (a larger budget than one scene's: the
+// batch holds many more rays).
+constexpr size_t MULTI_SLOT_BUDGET = 64u << 20;
+
+static uint32_t multi_slot_capacity(uint32_t n_rays) {
+    size_t cap = MULTI_SLOT_BUDGET / (n_rays ? n_rays : 1);
+    cap = std::min<size_t>(std::max<size_t>(cap, 16), 1024);
+    return (uint32_t)cap;
 }
 
 template <int NL>
@@ -955,6 +1231,72 @@ int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, con
                                                   ctx->block_u32 + nb, ray_img_id, ori, dir, ray_t, alive, n_steps,
                                                   offsets, o, ctx->flags, ctx->slots, ctx->slot_cap);
     return check_launch("tn_march_emit");
+}
+
+int tn_multi_march_count(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, const tn_scene* scenes,
+                         uint32_t ray_stride, const float* ori, const float* dir, const float* ray_t,
+                         const float* ray_t_max, uint8_t* alive, uint32_t* n_steps, uint32_t* scene_samples,
+                         uint32_t* batch_info) {
+    TN_NONNULL(ctx);
+    TN_NONNULL(ori); TN_NONNULL(dir); TN_NONNULL(ray_t); TN_NONNULL(ray_t_max); TN_NONNULL(alive);
+    TN_NONNULL(n_steps); TN_NONNULL(batch_info);
+    static MultiArgs A;  // large; built under the host lock of the calling thread's launch
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    int st = make_multi_args(ctx, n_scenes, scenes, ray_stride, A, true);
+    if (st != TN_OK) return st;
+    TN_REQUIRE(A.total_rays > 0, TN_E_NO_RAYS, "tn_multi_march_count: no rays");
+    st = ensure_block_u32(ctx, 2 * (size_t)A.total_chunks);
+    if (st != TN_OK) return st;
+    const uint32_t slot_cap = multi_slot_capacity(A.total_rays);
+    st = ensure_slots(ctx, (size_t)A.total_rays * slot_cap);
+    if (st != TN_OK) return st;
+    ctx->slot_cap = slot_cap;
+    ctx->slot_rays = A.total_rays;
+    st = cuda_status(cudaMemsetAsync(ctx->tickets + TICKET_MULTI, 0, 2 * sizeof(uint32_t), stream),
+                     "tn_multi_march_count(counters)");
+    if (st != TN_OK) return st;
+    uint32_t max_mip_blocks = 0;
+    for (uint32_t s = 0; s < n_scenes; ++s) max_mip_blocks = std::max(max_mip_blocks, A.sp[s].mip_blocks);
+    if (max_mip_blocks) {
+        multi_box_init_kernel<<<n_scenes, 64, 0, stream>>>(A);
+        multi_build_mip_kernel<<<dim3(max_mip_blocks, n_scenes), 256, 0, stream>>>(A);
+        st = check_launch("tn_multi_march_count(mip)");
+        if (st != TN_OK) return st;
+    }
+    const size_t smem = (size_t)12 * A.spread_res + (size_t)(MIP_MAX_RES / 4) * (MIP_MAX_RES / 4) * (MIP_MAX_RES / 4);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_count_kernel, COUNT_GROUP, smem);
+    const uint32_t grid = std::min<uint32_t>(A.total_chunks, (uint32_t)(num_sms() * std::max(per_sm, 1)));
+    multi_count_kernel<<<grid, COUNT_GROUP, smem, stream>>>(
+        A, ray_stride, ori, dir, ray_t, ray_t_max, alive, n_steps, ctx->block_u32, ctx->block_u32 + A.total_chunks,
+        ctx->tickets + TICKET_MULTI_WORK, ctx->tickets + TICKET_MULTI, ctx->flags, ctx->slots, slot_cap,
+        scene_samples, batch_info);
+    return check_launch("tn_multi_march_count");
+}
+
+int tn_multi_march_emit(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, const tn_scene* scenes,
+                        uint32_t ray_stride, uint32_t sample_stride, const uint32_t* ray_img_id, const float* ori,
+                        const float* dir, const float* ray_t, const uint8_t* alive, const uint32_t* n_steps,
+                        uint32_t* offsets, uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir,
+                        float* out_dt, float* out_m_norm, float* out_dt_norm) {
+    TN_NONNULL(ctx);
+    TN_NONNULL(ori); TN_NONNULL(dir); TN_NONNULL(ray_t); TN_NONNULL(alive); TN_NONNULL(n_steps);
+    TN_NONNULL(offsets); TN_NONNULL(out_t); TN_NONNULL(out_pos); TN_NONNULL(out_dir); TN_NONNULL(out_dt);
+    TN_NONNULL(out_m_norm); TN_NONNULL(out_dt_norm);
+    static MultiArgs A;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    int st = make_multi_args(ctx, n_scenes, scenes, ray_stride, A, false);
+    if (st != TN_OK) return st;
+    TN_REQUIRE(ctx->block_u32_cap >= 2 * (size_t)A.total_chunks && ctx->slot_rays == A.total_rays, TN_E_STATE,
+               "tn_multi_march_emit must follow tn_multi_march_count on the same context with the same scenes");
+    SampleOut o{out_img_id, out_t, out_pos, out_dir, out_dt, out_m_norm, out_dt_norm, sample_stride};
+    const uint32_t n_blocks = (A.total_rays + EXPAND_WARPS - 1) / EXPAND_WARPS;
+    multi_expand_kernel<<<n_blocks, EXPAND_WARPS * WARP, 0, stream>>>(
+        A, ray_stride, ctx->block_u32 + A.total_chunks, ray_img_id, ori, dir, ray_t, alive, n_steps, offsets, o,
+        ctx->flags, ctx->slots, ctx->slot_cap);
+    return check_launch("tn_multi_march_emit");
 }
 
 int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,

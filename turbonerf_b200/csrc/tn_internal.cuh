@@ -36,6 +36,8 @@ enum Ticket : int {
     TICKET_TRAIN = 4,
     TICKET_POPCOUNT = 5,
     TICKET_COMPACT = 6,
+    TICKET_MULTI = 7,        // multi-scene count: chunks finished
+    TICKET_MULTI_WORK = 8,   // multi-scene count: next chunk to take
     TICKET_COUNT = 16,
 };
 

@@ -199,6 +199,62 @@ def plain_march_emit(grid, bitfield, bbox, march, inv_aabb, n_rays, ray_stride, 
     return samples
 
 
+# ---- several scenes in one launch ----------------------------------------------------------
+def scene_table(scenes):
+    """scenes: sequence of dicts with grid (GridSpec), bitfield (device tensor), bbox, march
+    (MarchSpec), inv_aabb, ray_begin, n_rays. Returns a ctypes array of tn_scene (keeps the
+    bitfield tensors alive)."""
+    from .native import SceneDesc
+    arr = (SceneDesc * len(scenes))()
+    keep = []
+    for k, sc in enumerate(scenes):
+        arr[k].grid = sc["grid"].desc()
+        arr[k].bitfield = _ptr(sc["bitfield"])
+        arr[k].bbox = bbox_desc(sc["bbox"])
+        arr[k].march = sc["march"].desc()
+        arr[k].inv_aabb_size = float(sc["inv_aabb"])
+        arr[k].ray_begin = int(sc["ray_begin"])
+        arr[k].n_rays = int(sc["n_rays"])
+        keep.append(sc["bitfield"])
+    arr._keep = keep
+    return arr
+
+
+def multi_march_count(ctx, table, ray_stride, ori, dir_, ray_t, ray_t_max, alive, n_steps=None, scene_samples=None,
+                      info=None):
+    """Count pass of every scene of `table` in one persistent launch. Returns (n_steps
+    uint32[ray_stride], scene_samples uint32[n_scenes], info uint32[4] = total rays, total
+    samples)."""
+    n = len(table)
+    dev = ori.device
+    if n_steps is None:
+        n_steps = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    if scene_samples is None:
+        scene_samples = torch.zeros(n, dtype=torch.int32, device=dev)
+    if info is None:
+        info = torch.zeros(4, dtype=torch.int32, device=dev)
+    call("tn_multi_march_count", ctx.handle, _stream(), n, ctypes.addressof(table), ray_stride, _ptr(ori), _ptr(dir_), _ptr(ray_t),
+         _ptr(ray_t_max), _ptr(alive), _ptr(n_steps), _ptr(scene_samples), _ptr(info))
+    return n_steps, scene_samples, info
+
+
+def multi_march_emit(ctx, table, ray_stride, sample_stride, ori, dir_, ray_t, alive, n_steps, ray_img_id=None,
+                     samples=None, offsets=None):
+    """Offsets and samples of every scene of `table`, packed scene after scene, after
+    multi_march_count on the same context."""
+    dev = ori.device
+    if samples is None:
+        samples = alloc_samples(sample_stride, dev)
+    if offsets is None:
+        offsets = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    call("tn_multi_march_emit", ctx.handle, _stream(), len(table), ctypes.addressof(table), ray_stride, sample_stride,
+         _ptr(ray_img_id),
+         _ptr(ori), _ptr(dir_), _ptr(ray_t), _ptr(alive), _ptr(n_steps), _ptr(offsets), _ptr(samples["img_id"]),
+         _ptr(samples["t"]), _ptr(samples["pos"]), _ptr(samples["dir"]), _ptr(samples["dt"]), _ptr(samples["m_norm"]),
+         _ptr(samples["dt_norm"]))
+    return offsets, samples
+
+
 # ---- compositor / losses ------------------------------------------------------------------
 def composite_fwd(ctx, rb: RayBatchDesc, density, rgb, dt, activation=0, min_t=1e-4, out=None):
     dev = density.device

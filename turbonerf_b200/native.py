@@ -69,6 +69,12 @@ class MarchDesc(ctypes.Structure):
                 ("max_steps", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32)]
 
 
+class SceneDesc(ctypes.Structure):
+    """tn_scene: one scene of a multi-scene launch."""
+    _fields_ = [("grid", GridDesc), ("bitfield", ctypes.c_void_p), ("bbox", Bbox), ("march", MarchDesc),
+                ("inv_aabb_size", ctypes.c_float), ("ray_begin", ctypes.c_uint32), ("n_rays", ctypes.c_uint32)]
+
+
 class RayBatchDesc(ctypes.Structure):
     _fields_ = [("n_rays", ctypes.c_uint32), ("ray_stride", ctypes.c_uint32), ("sample_stride", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32), ("counts", ctypes.c_void_p), ("offsets", ctypes.c_void_p),
@@ -125,6 +131,9 @@ SIGNATURES = {
     "tn_march_emit": [_vp, _vp, _P(GridDesc), _vp, _P(Bbox), _P(MarchDesc), _f32, _u32, _u32, _u32, _vp, _vp, _vp,
                       _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_scan_offsets": [_vp, _vp, _u32, _vp, _vp, _u32, _vp],
+    "tn_multi_march_count": [_vp, _vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "tn_multi_march_emit": [_vp, _vp, _u32, _vp, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                            _vp, _vp, _vp],
     "tn_scan_offsets_noalloc": [_vp, _u32, _vp, _vp, _u32, _vp],
     "tn_compact_nonzero": [_vp, _vp, _u32, _vp, _vp, _vp],
     "tn_composite_fwd": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -331,3 +331,68 @@ def march_scene_cascaded(seed: int = SEED, n_rays: int = 1 << 14, n_levels: int 
     rays = rays_init_bbox(sphere_rays(rng, n_rays), bbox)
     dt = float(MIN_STEP_SIZE)
     return MarchScene(fld, grid, bbox, rays, 1.0 / 256.0, dt, float(np.float32(aabb) * np.float32(dt)), 0, aabb)
+
+
+# ---------------------------------------------------------------------------------------
+# Several scenes in one batch
+# ---------------------------------------------------------------------------------------
+@dataclass
+class MultiScene:
+    scenes: list           # MarchScene per scene (grid may be None until built)
+    ray_begin: np.ndarray  # [n_scenes] first ray of each scene in the shared arrays
+    rays: RayBatch         # all scenes' rays, scene after scene (box clip applied per scene)
+
+
+def multi_scene_params(seed: int = SEED, n_scenes: int = 16, ray_lo: int = 1 << 10, ray_hi: int = 1 << 16):
+    """Per-scene parameters of the batched multi-scene workload: a blob field of 8-32 blobs,
+    1-5 cascades, an AABB of size 0.5-16 (the coarsest level covers it), ray counts drawn
+    log-uniform in [ray_lo, ray_hi]. The field's geometry is the single-cascade scene's scaled
+    to the box: centres in +-A/3, standard deviations 0.1-0.3 A/3."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_scenes):
+        n_blobs = int(rng.integers(8, 33))
+        n_levels = int(rng.integers(1, 6))
+        aabb = float(np.float32(np.exp(rng.uniform(np.log(0.5), np.log(16.0)))))
+        n_rays = int(np.exp(rng.uniform(np.log(ray_lo), np.log(ray_hi))))
+        fld = make_blob_field(rng, n_blobs)
+        scale = aabb / 3.0
+        fld.blobs[:, :4] *= np.float32(scale)
+        out.append(dict(field=fld, n_levels=n_levels, aabb=aabb, n_rays=n_rays,
+                        seed=int(rng.integers(0, 2**31 - 1))))
+    return out
+
+
+def make_multi_scene(params, resolution: int = 32, grids: bool = True) -> MultiScene:
+    """Builds the scenes of multi_scene_params: grids (numpy, when grids is set), rays from a
+    sphere of radius 4A/3 toward the centre (the single-cascade scene's geometry scaled), box
+    clip, and the reference's cone stepping (dt = clamp(t/256, dt_min, max(A, 1) dt_min))."""
+    total = sum(p["n_rays"] for p in params)
+    ori = np.zeros(3 * total, np.float32)
+    dr = np.zeros(3 * total, np.float32)
+    t = np.zeros(total, np.float32)
+    tmax = np.zeros(total, np.float32)
+    alive = np.zeros(total, np.uint8)
+    scenes, begins = [], []
+    b = 0
+    dt = float(MIN_STEP_SIZE)
+    for p in params:
+        A = p["aabb"]
+        n_levels = p["n_levels"]
+        base = float(np.float32(A) / np.float32(1 << (n_levels - 1)))
+        h = A / 2
+        bbox = (-h, -h, -h, h, h, h)
+        rng = np.random.default_rng(p["seed"])
+        r = rays_init_bbox(sphere_rays(rng, p["n_rays"], radius=4.0 * A / 3.0), bbox)
+        n = p["n_rays"]
+        for c in range(3):
+            ori[c * total + b:c * total + b + n] = r.ori[c * n:(c + 1) * n]
+            dr[c * total + b:c * total + b + n] = r.dir[c * n:(c + 1) * n]
+        t[b:b + n], tmax[b:b + n], alive[b:b + n] = r.t[:n], r.t_max[:n], r.alive[:n]
+        grid = build_grid(p["field"], n_levels, base, resolution) if grids else None
+        dt_max = float(np.float32(max(A, 1.0)) * np.float32(dt))
+        scenes.append(MarchScene(p["field"], grid, bbox, r, 1.0 / 256.0, dt, dt_max, 1024, A))
+        begins.append(b)
+        b += n
+    rays = RayBatch(total, total, ori, dr, t, tmax, alive)
+    return MultiScene(scenes, np.asarray(begins, np.uint32), rays)
