@@ -165,6 +165,8 @@ def run_ours(args):
     scene = _scene(0x7B0)
     tr = _trainer(scene, "fused", seed)
     stream = torch.cuda.ExternalStream(tr.stream_handle())
+    # launch shapes of the march and the loss kernel, chosen on this trainer's own batch
+    tuned = tr.autotune() if not args.no_autotune else {"tuning": tr.tuning}
 
     def barrier():
         if world > 1:
@@ -294,7 +296,8 @@ def run_ours(args):
                    "distortion_lambda": LAMBDA, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (Adam state 268 MB + grid 42 MB touched per step)",
                    "samples_last_step": result["last"]["n_samples"], "rays_last_step": result["last"]["n_rays"],
-                   "touched_hash_grads": result["n_touched"]},
+                   "touched_hash_grads": result["n_touched"], "launch_shapes": tuned["tuning"],
+                   "autotuned": not args.no_autotune},
         "e2e": {"value": round(e2e_value, 1), "unit": "samples/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": 68},
         "gpu_launches": int(result["kernels"]) * args.steps,
         "roofline": result["roofline"],
@@ -536,6 +539,11 @@ def run_multi_scene(args):
         ss = total + 64
         samples = hp.alloc_samples(ss, "cuda")
         offsets = torch.zeros(R, dtype=torch.int32, device="cuda")
+        tune_rep = None
+        if not args.no_autotune:
+            *_, tune_rep = hp.autotune_multi(ctx, table, R, ss, ori, dr, t, tmax, alive, n_steps=n_steps,
+                                             scene_samples=scene_samples, info=info, offsets=offsets,
+                                             samples=samples)
 
         def persistent():
             hp.multi_march_count(ctx, table, R, ori, dr, t, tmax, alive, n_steps=n_steps, scene_samples=scene_samples,
@@ -543,6 +551,9 @@ def run_multi_scene(args):
             hp.multi_march_emit(ctx, table, R, ss, ori, dr, t, alive, n_steps, samples=samples, offsets=offsets)
 
         ctx_s = hp.Context()
+        tun = ctx.tuning  # the same launch shapes on both sides
+        ctx_s.tuning = dict(count_rays_per_block=tun["multi_chunk_rays"], emit_warps_per_block=tun["emit_warps_per_block"],
+                            emit_rays_per_warp=tun["emit_rays_per_warp"])
         bufs = []
         for sc_in, ns_k in zip(table_in, per_scene):
             b, n = sc_in["ray_begin"], sc_in["n_rays"]
@@ -562,7 +573,8 @@ def run_multi_scene(args):
                               offsets=bf["offsets"], samples=bf["samples"])
 
         res = {"n_rays": R, "n_samples": total, "rays_per_scene": [int(p["n_rays"]) for p in ps],
-               "samples_per_scene": [int(v) for v in per_scene]}
+               "samples_per_scene": [int(v) for v in per_scene], "launch_shapes": ctx.tuning,
+               "autotune": tune_rep}
         for name, fn in (("persistent", persistent), ("per_scene", one_per_scene)):
             for _ in range(max(args.warmup, 3)):
                 fn()
@@ -597,6 +609,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="train-step", choices=["train-step", "backward-memory", "multi-scene"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "

@@ -109,6 +109,38 @@ int tn_ctx_check(tn_ctx* ctx, tn_stream_t stream, uint32_t* flags_out);
 /* Device pointer of the context's error word (for graph users that read it themselves). */
 int tn_ctx_flags_ptr(tn_ctx* ctx, uint32_t** flags_dev);
 
+/* ---- launch shapes and the autotuner ---------------------------------------------------
+ * No reference counterpart: the reference fixes its launch shapes (tcnn's linear_kernel,
+ * 128 or 512 threads a block). Each field below only changes how the work is split over
+ * blocks, warps and lanes. Counts, offsets, samples, per-ray values and gradients are
+ * bit-identical for every valid shape; the scalar loss sums of tn_train_losses are the same
+ * per-ray terms summed in another order. A context starts with tn_tuning_default. */
+typedef struct tn_tuning {
+    uint32_t count_rays_per_block;  /* march count, one thread per ray: 32, 64, 128 or 256 (64) */
+    uint32_t emit_warps_per_block;  /* march emit: 1, 2, 4, 8 or 16 warps a block (8) */
+    uint32_t emit_rays_per_warp;    /* march emit: 1, 2 or 4 rays a warp = 32, 16 or 8 lanes a ray (1) */
+    uint32_t loss_rays_per_block;   /* fused losses, one warp per ray: 2, 4 or 8 (4) */
+    uint32_t compact_tile;          /* compaction: values a block, 128, 256, 512, 1024 or 2048 (128) */
+    uint32_t multi_chunk_rays;      /* multi-scene count: rays per work-stealing chunk, 32..256 (64) */
+} tn_tuning;
+
+void tn_tuning_default(tn_tuning* out);
+/* TN_OK when every field holds one of its listed values. */
+int tn_tuning_validate(const tn_tuning* t);
+/* Sets / reads the shapes later calls on this context use. A tn_march_emit uses the count
+ * block size of the tn_march_count before it, whatever the tuning is by then (likewise the
+ * multi-scene emit and chunk size). */
+int tn_ctx_set_tuning(tn_ctx* ctx, const tn_tuning* t);
+int tn_ctx_get_tuning(tn_ctx* ctx, tn_tuning* out);
+
+/* Result of one autotuner call: the candidates tried, the median time of one call with the
+ * shape the context had before and with the shape chosen (CUDA events on the caller's stream). */
+typedef struct tn_tune_report {
+    uint32_t n_candidates;
+    float before_ms;
+    float best_ms;
+} tn_tune_report;
+
 /* ---- ray set-up (a 'next' stage of the reference path) ---------------------------- */
 /* Bounding-box clip of initialize_training_rays_and_pixels_kernel
  * (reference src/utils/training-batch-kernels.cuh:122-150): t = max(0, tmin + 1e-5),
@@ -147,6 +179,20 @@ int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, con
                   const uint8_t* alive, const uint32_t* n_steps, uint32_t* offsets,
                   uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir, float* out_dt,
                   float* out_m_norm, float* out_dt_norm);
+/* Autotuner of the march (tn_tuning count_rays_per_block, then emit_warps_per_block x
+ * emit_rays_per_warp): times tn_march_count with every count block size on these rays, keeps
+ * the fastest, then tn_march_emit with every emit shape on the counts it produced. The
+ * arguments are those of tn_march_count (without n_rays_dev) and tn_march_emit together; on
+ * return they hold the outputs of one count + emit call with the chosen shapes. Synchronises
+ * the stream; not while it is being captured. Reports may be NULL. */
+int tn_autotune_march(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, const uint8_t* bitfield,
+                      const tn_bbox* bbox, const tn_march_desc* march, float inv_aabb_size, uint32_t n_rays,
+                      uint32_t ray_stride, const uint32_t* ray_img_id, const float* ori, const float* dir,
+                      const float* ray_t, const float* ray_t_max, uint8_t* alive, uint32_t* n_steps,
+                      uint32_t batch_size, uint32_t* batch_info, uint32_t sample_stride, uint32_t* offsets,
+                      uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir, float* out_dt,
+                      float* out_m_norm, float* out_dt_norm, tn_tune_report* count_report,
+                      tn_tune_report* emit_report);
 
 /* ---- several scenes in one launch (batched multi-scene training) -------------------
  * No single reference call: the reference trains one scene per process. These entry points run
@@ -178,6 +224,15 @@ int tn_multi_march_emit(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, cons
                         const float* dir, const float* ray_t, const uint8_t* alive, const uint32_t* n_steps,
                         uint32_t* offsets, uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir,
                         float* out_dt, float* out_m_norm, float* out_dt_norm);
+/* Autotuner of the multi-scene march (multi_chunk_rays, then the emit shape), as
+ * tn_autotune_march; the arguments are those of the two multi-scene calls together. */
+int tn_autotune_multi(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, const tn_scene* scenes,
+                      uint32_t ray_stride, const uint32_t* ray_img_id, const float* ori, const float* dir,
+                      const float* ray_t, const float* ray_t_max, uint8_t* alive, uint32_t* n_steps,
+                      uint32_t* scene_samples, uint32_t* batch_info, uint32_t sample_stride, uint32_t* offsets,
+                      uint32_t* out_img_id, float* out_t, float* out_pos, float* out_dir, float* out_dt,
+                      float* out_m_norm, float* out_dt_norm, tn_tune_report* count_report,
+                      tn_tune_report* emit_report);
 
 /* Exclusive scan + batch cut of arbitrary counts (reference trainer.cu:146-183 with
  * find_last_lt_presorted, src/utils/parallel-utils.cuh:31-58). batch_info as above. */
@@ -202,6 +257,9 @@ int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* coun
  * *count_dev receives the list length. */
 int tn_compact_nonzero(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* values, int32_t* out,
                        uint32_t* count_dev);
+/* Autotuner of the compaction tile (compact_tile), as tn_autotune_march. */
+int tn_autotune_compact(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* values, int32_t* out,
+                        uint32_t* count_dev, tn_tune_report* report);
 
 /* ---- compositor (a warp per ray, warp-shuffle scans) ----------------------------- */
 /* Forward (reference density_to_ray_rgba_forward, training-kernels-fused.cuh:227-264):
@@ -268,6 +326,15 @@ int tn_train_losses(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, 
                     const float* dt, const float* m_norm, const float* dt_norm, const float* t,
                     const float* target_rgba, const float* bg_rgb, float* ray_rgba, float* grad_density,
                     float* dL_drgb, float* loss_sums);
+/* Autotuner of the fused loss kernel's block size (loss_rays_per_block), as
+ * tn_autotune_march. grad_density is restored to its values on entry before every call, so
+ * on return it holds the result of one call. */
+int tn_autotune_losses(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, int activation,
+                       float min_transmittance, float inv_nrays, const uint32_t* inv_nrays_from_dev,
+                       float grad_scale, float lambda, const float* density, const float* rgb, const float* dt,
+                       const float* m_norm, const float* dt_norm, const float* t, const float* target_rgba,
+                       const float* bg_rgb, float* ray_rgba, float* grad_density, float* dL_drgb, float* loss_sums,
+                       tn_tune_report* report);
 
 /* ---- occupancy grid ------------------------------------------------------------- */
 /* Network sample points for (level, cell) pairs (reference
@@ -445,6 +512,16 @@ int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori
  * (ms): rays, march count, march emit, network forward, losses, network backward,
  * Adam, occupancy query (cell sampling and the density network), occupancy update. */
 int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages);
+/* Tunes the trainer's launch shapes on its own batch (the rays of the last step, or freshly
+ * generated synthetic rays before the first one): the march (count and emit) and the fused
+ * losses. Leaves weights, optimizer state and the occupancy grid untouched; the next step
+ * captures its graph again with the chosen shapes. reports[3] (may be NULL): count, emit,
+ * losses. Synchronous. */
+int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports);
+/* Launch shapes of the trainer's context; setting them (validated) makes the next step
+ * capture its graph again. */
+int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out);
+int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t);
 /* 0/1: kernel nodes in the captured step graph (synthetic / caller rays), 2: graph nodes,
  * 3: samples processed so far, 4: rays used so far, 5: steps (3-5 synchronise). */
 int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out);

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared():
     hdr = open(os.path.join(ROOT, "include", "turbo_hot.h")).read()
-    return re.findall(r"^\s*(?:int|const char\*)\s+(tn_\w+)\(", hdr, re.M)
+    return re.findall(r"^\s*(?:int|void|const char\*)\s+(tn_\w+)\(", hdr, re.M)
 
 
 def test_library_exports_every_declared_symbol():
@@ -51,3 +51,27 @@ def test_argument_errors_return_status_without_gpu():
         native.check(native.TN_E_INVALID)
     with pytest.raises(native.NoRaysError):
         native.check(native.TN_E_NO_RAYS)
+
+
+def test_tuning_defaults_and_validation_without_gpu():
+    """The launch-shape table: defaults, and every field outside its listed values rejected on
+    the host (tn_tuning_validate; tn_ctx_set_tuning runs the same check)."""
+    from turbonerf_b200 import native
+    L = native.lib()
+    t = native.Tuning()
+    L.tn_tuning_default(ctypes.byref(t))
+    assert t.as_dict() == {"count_rays_per_block": 64, "emit_warps_per_block": 8, "emit_rays_per_warp": 1,
+                           "loss_rays_per_block": 4, "compact_tile": 128, "multi_chunk_rays": 64}
+    assert L.tn_tuning_validate(ctypes.byref(t)) == native.TN_OK
+    allowed = {"count_rays_per_block": [32, 64, 128, 256], "emit_warps_per_block": [1, 2, 4, 8, 16],
+               "emit_rays_per_warp": [1, 2, 4], "loss_rays_per_block": [2, 4, 8],
+               "compact_tile": [128, 256, 512, 1024, 2048], "multi_chunk_rays": [32, 64, 128, 256]}
+    for field, values in allowed.items():
+        for v in range(0, 4097):
+            u = native.Tuning(**t.as_dict())
+            setattr(u, field, v)
+            st = L.tn_tuning_validate(ctypes.byref(u))
+            assert (st == native.TN_OK) == (v in values), (field, v, st)
+            if st != native.TN_OK:
+                assert st == native.TN_E_INVALID and field in L.tn_last_error().decode()
+    assert L.tn_tuning_validate(None) == native.TN_E_NULL

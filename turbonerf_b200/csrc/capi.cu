@@ -1,4 +1,6 @@
 // Context, error reporting and scratch management of the turbo_hot C ABI.
+#include <initializer_list>
+
 #include "tn_internal.cuh"
 
 namespace tn {
@@ -122,8 +124,8 @@ int tn_ctx_destroy(tn_ctx* ctx) {
 
 int tn_ctx_reserve(tn_ctx* ctx, uint32_t max_rays, uint32_t max_samples) {
     TN_NONNULL(ctx);
-    // One u32 per 128-ray block (march/scan) plus per-block float partials.
-    const size_t blocks = (size_t)max_rays / 64 + (size_t)max_samples / 1024 + 1024;
+    // One u32 per count block (32 rays at the smallest tuned size) plus per-block float partials.
+    const size_t blocks = (size_t)max_rays / 32 + (size_t)max_samples / 1024 + 1024;
     int st = ensure_block_u32(ctx, 2 * blocks);
     if (st == TN_OK) st = ensure_block_f32(ctx, 8 * blocks);
     // march scratch: the 128^3 coarse mip with its occupied boxes and 8 bit-planes (33,024 B +
@@ -153,6 +155,52 @@ int tn_ctx_flags_ptr(tn_ctx* ctx, uint32_t** flags_dev) {
     TN_NONNULL(ctx);
     TN_NONNULL(flags_dev);
     *flags_dev = ctx->flags;
+    return TN_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+void tn_tuning_default(tn_tuning* out) {
+    if (out) *out = tn_tuning{64, 8, 1, 4, 128, 64};
+}
+
+static bool one_of(uint32_t v, std::initializer_list<uint32_t> allowed) {
+    for (uint32_t a : allowed)
+        if (v == a) return true;
+    return false;
+}
+
+int tn_tuning_validate(const tn_tuning* t) {
+    TN_NONNULL(t);
+    TN_REQUIRE(one_of(t->count_rays_per_block, {32, 64, 128, 256}), TN_E_INVALID,
+               "tuning: count_rays_per_block %u not in {32, 64, 128, 256}", t->count_rays_per_block);
+    TN_REQUIRE(one_of(t->emit_warps_per_block, {1, 2, 4, 8, 16}), TN_E_INVALID,
+               "tuning: emit_warps_per_block %u not in {1, 2, 4, 8, 16}", t->emit_warps_per_block);
+    TN_REQUIRE(one_of(t->emit_rays_per_warp, {1, 2, 4}), TN_E_INVALID,
+               "tuning: emit_rays_per_warp %u not in {1, 2, 4}", t->emit_rays_per_warp);
+    TN_REQUIRE(one_of(t->loss_rays_per_block, {2, 4, 8}), TN_E_INVALID,
+               "tuning: loss_rays_per_block %u not in {2, 4, 8}", t->loss_rays_per_block);
+    TN_REQUIRE(one_of(t->compact_tile, {128, 256, 512, 1024, 2048}), TN_E_INVALID,
+               "tuning: compact_tile %u not in {128, 256, 512, 1024, 2048}", t->compact_tile);
+    TN_REQUIRE(one_of(t->multi_chunk_rays, {32, 64, 128, 256}), TN_E_INVALID,
+               "tuning: multi_chunk_rays %u not in {32, 64, 128, 256}", t->multi_chunk_rays);
+    return TN_OK;
+}
+
+int tn_ctx_set_tuning(tn_ctx* ctx, const tn_tuning* t) {
+    TN_NONNULL(ctx);
+    const int st = tn_tuning_validate(t);
+    if (st != TN_OK) return st;
+    ctx->tune = *t;
+    return TN_OK;
+}
+
+int tn_ctx_get_tuning(tn_ctx* ctx, tn_tuning* out) {
+    TN_NONNULL(ctx);
+    TN_NONNULL(out);
+    *out = ctx->tune;
     return TN_OK;
 }
 

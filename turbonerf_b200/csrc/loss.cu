@@ -628,8 +628,7 @@ __device__ __forceinline__ float blk_suffix(float (&v)[K], int lane, float carry
 // without bank conflicts. Results go back through the same buffers with coalesced stores.
 constexpr int RB_SKEW = RB_MAX + RB_MAX / WARP;
 enum StageArray : int { SA_SIG = 0, SA_DT, SA_R, SA_G, SA_B, SA_DTN, SA_M, SA_T, SA_GD, SA_N };
-constexpr int TL_WARPS = 4;  // warps (rays in flight) per block of the fused loss kernel
-constexpr int TL_THREADS = TL_WARPS * WARP;
+constexpr size_t TL_STAGE_BYTES = (size_t)SA_N * RB_SKEW * sizeof(float);  // one warp's staging buffer
 
 __device__ __forceinline__ uint32_t skew(uint32_t j) { return j + (j >> 5); }
 
@@ -1151,28 +1150,30 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
 }
 
 // Reconstruction + distortion forward/backward + gradient merge, one warp per ray with its own
-// staging buffer; four blocks of four warps per SM (128 registers a thread, 38 KB of shared
-// memory a block) keep 16 rays in flight per SM.
-__global__ void __launch_bounds__(TL_THREADS, 4)
+// staging buffer (dynamic shared memory, 9.3 KB a warp); W warps a block (tn_tuning
+// loss_rays_per_block: 2, 4 or 8) and 16 / W blocks an SM (128 registers a thread) keep 16 rays
+// in flight per SM.
+template <int W>
+__global__ void __launch_bounds__(W * WARP, 16 / W)
 train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
                     const uint32_t* __restrict__ offsets, float min_t, float inv_nrays_host,
                     const uint32_t* __restrict__ inv_from, float grad_scale, float lambda,
                     const float* __restrict__ target, const float* __restrict__ bg, float* __restrict__ ray_rgba,
                     float* __restrict__ grad_density, float* __restrict__ drgb, float* loss_sums, float* partials,
                     uint32_t* ticket) {
-    __shared__ float stage[TL_WARPS][SA_N * RB_SKEW];
+    extern __shared__ __align__(16) float stage[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_live = live_rays(n_rays, n_dev);
     float inv_nrays = inv_nrays_host;
     if (inv_from) { const uint32_t nn = *inv_from; inv_nrays = nn ? 1.0f / (float)nn : 0.0f; }
-    const uint32_t nw = gridDim.x * TL_WARPS;
+    const uint32_t nw = gridDim.x * W;
     const float lam = lambda > 0.0f ? lambda : 0.0f;
     float acc[2] = {0.0f, 0.0f};
-    for (uint32_t r = blockIdx.x * TL_WARPS + wid; r < n_live; r += nw) {
+    for (uint32_t r = blockIdx.x * W + wid; r < n_live; r += nw) {
         const uint32_t o = offsets[r], n = counts[r];
         if (n <= RB_MAX)
             train_losses_ray_blocked(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
-                                     grad_density, drgb, acc[0], acc[1], stage[wid]);
+                                     grad_density, drgb, acc[0], acc[1], stage + (size_t)wid * SA_N * RB_SKEW);
         else
             train_losses_ray_long(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
                                   grad_density, drgb, acc[0], acc[1]);
@@ -1354,11 +1355,32 @@ static int blocks_per_sm(const void* kernel, int threads, size_t dyn_smem = 0) {
     return per_sm;
 }
 
-static int loss_grid(const void* kernel, uint32_t n_rays, int threads = LOSS_THREADS) {
-    const int per_sm = blocks_per_sm(kernel, threads);
+static int loss_grid(const void* kernel, uint32_t n_rays, int threads = LOSS_THREADS, size_t dyn_smem = 0) {
+    const int per_sm = blocks_per_sm(kernel, threads, dyn_smem);
     const uint32_t want = (n_rays + threads / WARP - 1) / (threads / WARP);
     const uint32_t cap = (uint32_t)(num_sms() * per_sm);
     return (int)max(1u, min(want, cap));
+}
+
+template <int W>
+static int launch_train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_batch* batch, const Samples& S,
+                               float min_t, float inv_nrays, const uint32_t* inv_from, float grad_scale, float lambda,
+                               const float* target, const float* bg, float* ray_rgba, float* grad_density,
+                               float* drgb, float* loss_sums) {
+    const size_t smem = W * TL_STAGE_BYTES;
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        cudaFuncSetAttribute(train_losses_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
+    const int grid = loss_grid((const void*)train_losses_kernel<W>, batch->n_rays, W * WARP, smem);
+    int st = ensure_block_f32(ctx, (size_t)grid * 2);
+    if (st != TN_OK) return st;
+    train_losses_kernel<W><<<grid, W * WARP, smem, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
+                                                              batch->counts, batch->offsets, min_t, inv_nrays,
+                                                              inv_from, grad_scale, lambda, target, bg, ray_rgba,
+                                                              grad_density, drgb, loss_sums, ctx->block_f32,
+                                                              ctx->tickets + TICKET_TRAIN);
+    return check_launch("tn_train_losses");
 }
 
 static int check_batch(const tn_ray_batch* b) {
@@ -1511,15 +1533,18 @@ int tn_train_losses(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, 
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, m_norm, dt_norm, t, batch->sample_stride, activation};
-    const int grid = loss_grid((const void*)train_losses_kernel, batch->n_rays, TL_THREADS);
-    st = ensure_block_f32(ctx, (size_t)grid * 2);
-    if (st != TN_OK) return st;
-    train_losses_kernel<<<grid, TL_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
-                                                           batch->counts, batch->offsets, min_transmittance, inv_nrays,
-                                                           inv_nrays_from_dev, grad_scale, lambda, target_rgba, bg_rgb,
-                                                           ray_rgba, grad_density, dL_drgb, loss_sums, ctx->block_f32,
-                                                           ctx->tickets + TICKET_TRAIN);
-    return check_launch("tn_train_losses");
+    switch (ctx->tune.loss_rays_per_block) {
+        case 2: st = launch_train_losses<2>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
+                                            grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density, dL_drgb,
+                                            loss_sums); break;
+        case 8: st = launch_train_losses<8>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
+                                            grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density, dL_drgb,
+                                            loss_sums); break;
+        default: st = launch_train_losses<4>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
+                                             grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density, dL_drgb,
+                                             loss_sums); break;
+    }
+    return st;
 }
 
 // fused_reconstruction_loss_forward_backward launch structure (src/core/nerf-network.cu:547-602):

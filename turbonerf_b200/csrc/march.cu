@@ -146,18 +146,19 @@ __device__ void march_emit_ray(const MarchArgs& a, RayMarch& r, uint32_t n_steps
     }
 }
 
-// Block-wide exclusive scan of one u32 per thread (MARCH_BLOCK threads); returns the
-// exclusive prefix and the block total in *total.
+// Block-wide exclusive scan of one u32 per thread; returns the exclusive prefix and the block
+// total in *total. BLOCK bounds the block size; blockDim.x is any multiple of 32 up to it.
 template <int BLOCK = MARCH_BLOCK>
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
     __shared__ uint32_t warp_tot[BLOCK / WARP];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t inc = warp_inclusive_sum(v, lane);
     if (lane == 31) warp_tot[wid] = inc;
     __syncthreads();
     uint32_t before = 0, tot = 0;
 #pragma unroll
     for (int w = 0; w < BLOCK / WARP; ++w) {
+        if (w >= nw) break;
         const uint32_t x = warp_tot[w];
         if (w < wid) before += x;
         tot += x;
@@ -170,7 +171,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
 // Last-block epilogue of the count pass: exclusive scan of the block totals into
 // block_prefix, then the reference batch cut (src/core/trainer.cu:133-183):
 // L = last ray index whose offset < batch_size; n_rays = L; n_samples = offset[L].
-// Run by one block of BLOCK threads; each entry of block_agg covers BLOCK rays.
+// Run by one block of blockDim.x <= BLOCK threads; each entry of block_agg covers blockDim.x rays.
 template <int BLOCK = MARCH_BLOCK>
 __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t* __restrict__ counts,
                                     uint32_t* block_agg, uint32_t* block_prefix, uint32_t batch_size,
@@ -180,8 +181,9 @@ __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t
     __shared__ int last_ray_s;
     if (threadIdx.x == 0) { carry_s = 0ull; last_block_s = -1; last_ray_s = -1; }
     __syncthreads();
-    const uint32_t nb_live = (n_live + BLOCK - 1) / BLOCK;
-    for (uint32_t base = 0; base < nb; base += BLOCK) {
+    const uint32_t bs = blockDim.x;
+    const uint32_t nb_live = (n_live + bs - 1) / bs;
+    for (uint32_t base = 0; base < nb; base += bs) {
         const uint32_t b = base + threadIdx.x;
         const uint32_t v = b < nb ? *((volatile uint32_t*)(block_agg + b)) : 0u;
         uint32_t tot;
@@ -211,7 +213,7 @@ __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t
         return;
     }
     if (lb >= 0) {
-        const uint32_t i = (uint32_t)lb * BLOCK + threadIdx.x;
+        const uint32_t i = (uint32_t)lb * bs + threadIdx.x;
         const uint32_t c = i < n_live ? *((volatile const uint32_t*)(counts + i)) : 0u;
         uint32_t tot;
         const uint32_t ex = block_exclusive_scan<BLOCK>(c, &tot);
@@ -237,10 +239,11 @@ __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t
 }
 
 // ---- batch scan of given counts (tn_scan_offsets, tn_scan_offsets_noalloc) ---------------
-// Block totals of the counts; returns true in the last block to finish (ticket).
+// Block totals of the counts; returns true in the last block to finish (ticket). BLOCK bounds
+// the block size.
 template <int BLOCK>
 __device__ __forceinline__ bool block_total_and_ticket(uint32_t cnt, uint32_t* block_agg, uint32_t* ticket) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const uint32_t s = warp_sum(cnt);
     __shared__ uint32_t wsum[BLOCK / WARP];
     __shared__ bool is_last;
@@ -249,7 +252,8 @@ __device__ __forceinline__ bool block_total_and_ticket(uint32_t cnt, uint32_t* b
     if (threadIdx.x == 0) {
         uint32_t tot = 0;
 #pragma unroll
-        for (int w = 0; w < BLOCK / WARP; ++w) tot += wsum[w];
+        for (int w = 0; w < BLOCK / WARP; ++w)
+            if (w < nw) tot += wsum[w];
         block_agg[blockIdx.x] = tot;
         __threadfence();
         is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
@@ -284,7 +288,7 @@ scan_offsets_kernel(uint32_t n, const uint32_t* __restrict__ counts, const uint3
 // ---- fused march count ----------------------------------------------------------------
 // Rays per count block: 64 keeps every SM busy at the 2^14-ray batches of training, where
 // each warp is latency-bound on its own rays. block_agg / block_prefix hold one entry per group.
-constexpr int COUNT_GROUP = 64;
+constexpr int COUNT_GROUP_MAX = 256;  // largest count block (tn_tuning::count_rays_per_block)
 // The coarse mip (one byte per 4x4x4 block) is staged in shared memory for 16 <= R <= 128.
 constexpr int MIP_MIN_RES = 16;
 constexpr int MIP_MAX_RES = 128;
@@ -470,12 +474,12 @@ __device__ __forceinline__ bool ray_box_exit(const RayMarch& r, const float* u, 
     return true;
 }
 
-// One thread per ray, COUNT_GROUP rays per block. Shared memory: the three Morton spread tables
+// One thread per ray, blockDim.x rays per block (a tuning choice, 32..256). Shared memory: the three Morton spread tables
 // (3 R words) and, with MIP, the coarse mip (R^3/64 bytes); with MIP the fine test reads the
 // per-level bit-planes. The last block to finish scans the group totals and applies the batch
 // cut on the device.
 template <int NL, bool MIP>
-__global__ void __launch_bounds__(COUNT_GROUP)
+__global__ void __launch_bounds__(COUNT_GROUP_MAX)
 march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
                    const float* __restrict__ ori, const float* __restrict__ dir, const float* __restrict__ ray_t,
                    const float* __restrict__ ray_t_max, uint8_t* __restrict__ alive, uint32_t* counts,
@@ -488,7 +492,7 @@ march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* _
     __shared__ float ubox_s[6];
     __shared__ int cut_s;
     const uint32_t res = 1u << cg.res_shift;
-    for (uint32_t c = threadIdx.x; c < res; c += COUNT_GROUP) {
+    for (uint32_t c = threadIdx.x; c < res; c += blockDim.x) {
         const uint32_t v = part1by2(c);
         spread[c] = v;
         spread[res + c] = v << 1;
@@ -499,12 +503,12 @@ march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* _
         const uint4* src = reinterpret_cast<const uint4*>(mip_g);
         uint4* dst = reinterpret_cast<uint4*>(mip);
 #pragma unroll 8
-        for (uint32_t k = threadIdx.x; k < n16; k += COUNT_GROUP) dst[k] = __ldg(src + k);
+        for (uint32_t k = threadIdx.x; k < n16; k += blockDim.x) dst[k] = __ldg(src + k);
         if (threadIdx.x == 0) occupied_union(cg, box_g, a.g.n_levels, ubox_s, &cut_s);
     }
     __syncthreads();
     const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
-    const uint32_t i = blockIdx.x * COUNT_GROUP + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t cnt = 0;
     if (i < n_live) {
         if (alive[i]) {
@@ -531,9 +535,9 @@ march_count_kernel(MarchArgs a, CountGrid cg, uint32_t n_rays, const uint32_t* _
     }
     // make this thread's count visible device-wide before the block reports completion
     __threadfence();
-    if (!block_total_and_ticket<COUNT_GROUP>(cnt, block_agg, ticket)) return;
+    if (!block_total_and_ticket<COUNT_GROUP_MAX>(cnt, block_agg, ticket)) return;
     __threadfence();
-    scan_blocks_and_cut<COUNT_GROUP>(gridDim.x, n_live, counts, block_agg, block_prefix, batch_size, batch_info,
+    scan_blocks_and_cut<COUNT_GROUP_MAX>(gridDim.x, n_live, counts, block_agg, block_prefix, batch_size, batch_info,
                                      flags);
     if (threadIdx.x == 0) *ticket = 0u;
 }
@@ -552,7 +556,8 @@ __device__ __forceinline__ void expand_ray(const MarchArgs& a, float inv_aabb, u
                                            uint32_t rs, const uint32_t* __restrict__ img_id,
                                            const float* __restrict__ ori, const float* __restrict__ dir,
                                            const float* __restrict__ ray_t, const SampleOut& o,
-                                           const float* __restrict__ slots, uint32_t slot_cap, int lane) {
+                                           const float* __restrict__ slots, uint32_t slot_cap, int lane,
+                                           int lanes) {
     RayMarch r;
     load_ray(r, ori, dir, r_i, rs);
     r.t = ray_t[r_i];
@@ -565,7 +570,7 @@ __device__ __forceinline__ void expand_ray(const MarchArgs& a, float inv_aabb, u
     const float t_last = sl[n - 1];
     const float t_end = __fadd_rn(t_last, get_dt(t_last, a.cone, a.dt_min, a.dt_max));
     const float t_span = fmaxf(__fadd_rn(t_end, -r.t), 1e-6f);
-    for (uint32_t j = lane; j < n; j += WARP) {
+    for (uint32_t j = lane; j < n; j += lanes) {
         const float t = sl[j];
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
         float x, y, z;
@@ -580,31 +585,47 @@ __device__ __forceinline__ void expand_ray(const MarchArgs& a, float inv_aabb, u
     }
 }
 
-constexpr int EXPAND_WARPS = 8;
+constexpr int EXPAND_THREADS_MAX = 512;  // 16 warps (tn_tuning::emit_warps_per_block)
 
-__global__ void __launch_bounds__(EXPAND_WARPS * WARP)
+// Sum over the aligned group of L lanes (all 32 lanes take part).
+template <int L>
+__device__ __forceinline__ uint32_t group_sum(uint32_t v) {
+#pragma unroll
+    for (int d = L / 2; d > 0; d >>= 1) v += __shfl_xor_sync(FULL_MASK, v, d);
+    return v;
+}
+
+// RPW rays per warp (32 / RPW lanes per ray), blockDim.x / 32 warps per block; the count pass
+// grouped its rays by 2^group_shift (the block size it ran with).
+template <int RPW>
+__global__ void __launch_bounds__(EXPAND_THREADS_MAX)
 expand_kernel(MarchArgs a, float inv_aabb, uint32_t n_rays, const uint32_t* __restrict__ n_rays_dev, uint32_t rs,
-              const uint32_t* __restrict__ batch_info, const uint32_t* __restrict__ block_prefix,
-              const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
-              const float* __restrict__ ray_t, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ counts,
+              uint32_t group_shift, const uint32_t* __restrict__ batch_info,
+              const uint32_t* __restrict__ block_prefix, const uint32_t* __restrict__ img_id,
+              const float* __restrict__ ori, const float* __restrict__ dir, const float* __restrict__ ray_t,
+              const uint8_t* __restrict__ alive, const uint32_t* __restrict__ counts,
               uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags, const float* __restrict__ slots,
               uint32_t slot_cap) {
+    constexpr int L = WARP / RPW;
     const uint32_t n_live = n_rays_dev ? min(*n_rays_dev, n_rays) : n_rays;
-    const int lane = threadIdx.x & 31;
-    const uint32_t r_i = blockIdx.x * EXPAND_WARPS + (threadIdx.x >> 5);
-    if (r_i >= n_live) return;
-    const uint32_t g0 = r_i / COUNT_GROUP * COUNT_GROUP;
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1);
+    const uint32_t r_i = ((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * RPW) + (uint32_t)(lane / L);
+    const bool valid = r_i < n_live;
+    const uint32_t g0 = (r_i >> group_shift) << group_shift;
     uint32_t part = 0;
-    for (uint32_t j = g0 + lane; j < r_i; j += WARP) part += counts[j];
-    const uint32_t o0 = warp_sum(part) + block_prefix[r_i / COUNT_GROUP];
+    if (valid)
+        for (uint32_t j = g0 + sub; j < r_i; j += L) part += counts[j];
+    part = group_sum<L>(part);  // every lane of the warp takes part before any leaves
+    if (!valid) return;
+    const uint32_t o0 = part + block_prefix[r_i >> group_shift];
     const uint32_t n = counts[r_i];
-    if (lane == 0) offsets[r_i] = o0;
+    if (sub == 0) offsets[r_i] = o0;
     if (r_i >= batch_info[0] || n == 0 || !alive[r_i]) return;
     if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
-        if (lane == 0) raise_flag(flags, ERR_CAPACITY);
+        if (sub == 0) raise_flag(flags, ERR_CAPACITY);
         return;
     }
-    expand_ray(a, inv_aabb, r_i, o0, n, rs, img_id, ori, dir, ray_t, o, slots, slot_cap, lane);
+    expand_ray(a, inv_aabb, r_i, o0, n, rs, img_id, ori, dir, ray_t, o, slots, slot_cap, sub, L);
 }
 
 // Bits k of the four bytes of x (cells 4j .. 4j+3) as four consecutive bits: the mask leaves
@@ -694,11 +715,12 @@ build_mip_kernel(int cshift, int n_levels, const uint4* __restrict__ bits, uint8
 // ---- several scenes in one launch ---------------------------------------------------------
 // The scenes' rays sit in one set of ray arrays, scene after scene, and their samples are
 // packed the same way. Each scene keeps its own grid, bitfield, box and march parameters. The
-// count pass is one persistent launch: blocks take COUNT_GROUP-ray chunks of any scene from a
-// shared counter (work stealing) and stage a scene's coarse mip when they move to another scene.
-// The block that finishes the last chunk scans all chunk totals. The emit pass is one launch
-// with a warp per ray. The per-scene results equal those of a tn_march_count / tn_march_emit
-// call per scene without a batch cut.
+// count pass is one persistent launch: blocks take chunks of rays (tn_tuning::multi_chunk_rays,
+// one thread a ray) of any scene from a shared counter (work stealing) and stage a scene's
+// coarse mip when they move to another scene. The block that finishes the last chunk scans all
+// chunk totals. The emit pass is one launch over all scenes' rays with the single-scene emit's
+// shape. The per-scene results equal those of a tn_march_count / tn_march_emit call per scene
+// without a batch cut.
 constexpr int MAX_SCENES = 32;
 
 struct SceneParams {
@@ -714,6 +736,7 @@ struct SceneParams {
 
 struct MultiArgs {
     uint32_t n_scenes, total_chunks, total_rays, spread_res;
+    uint32_t chunk_shift;  // rays per work-stealing chunk = 2^chunk_shift = the count block size
     SceneParams sp[MAX_SCENES];
 };
 
@@ -745,7 +768,7 @@ __global__ void __launch_bounds__(256) multi_build_mip_kernel(const __grid_const
                     const_cast<uint32_t*>(sp.cg.planes), sp.cg.plane_words, blockIdx.x);
 }
 
-__global__ void __launch_bounds__(COUNT_GROUP)
+__global__ void __launch_bounds__(COUNT_GROUP_MAX)
 multi_count_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const float* __restrict__ ori,
                    const float* __restrict__ dir, const float* __restrict__ ray_t, const float* __restrict__ ray_t_max,
                    uint8_t* __restrict__ alive, uint32_t* counts, uint32_t* block_agg, uint32_t* block_prefix,
@@ -757,10 +780,10 @@ multi_count_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const float
     __shared__ float ubox_s[6];
     __shared__ int cut_s;
     __shared__ uint32_t chunk_s;
-    __shared__ uint32_t wsum[COUNT_GROUP / WARP];
+    __shared__ uint32_t wsum[COUNT_GROUP_MAX / WARP];
     __shared__ bool last_s;
     const uint32_t res = A.spread_res;
-    for (uint32_t c = threadIdx.x; c < res; c += COUNT_GROUP) {
+    for (uint32_t c = threadIdx.x; c < res; c += blockDim.x) {
         const uint32_t v = part1by2(c);
         spread[c] = v;
         spread[res + c] = v << 1;
@@ -780,13 +803,13 @@ multi_count_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const float
                 const uint4* src = reinterpret_cast<const uint4*>(sp.mip);
                 uint4* dst = reinterpret_cast<uint4*>(mip);
 #pragma unroll 8
-                for (uint32_t k = threadIdx.x; k < n16; k += COUNT_GROUP) dst[k] = __ldg(src + k);
+                for (uint32_t k = threadIdx.x; k < n16; k += blockDim.x) dst[k] = __ldg(src + k);
                 if (threadIdx.x == 0) occupied_union(sp.cg, sp.box, sp.a.g.n_levels, ubox_s, &cut_s);
             }
             staged = s;
             __syncthreads();
         }
-        const uint32_t local = (chunk - sp.chunk_begin) * COUNT_GROUP + threadIdx.x;
+        const uint32_t local = ((chunk - sp.chunk_begin) << A.chunk_shift) + threadIdx.x;
         const uint32_t i = sp.ray_begin + local;
         uint32_t cnt = 0;
         if (local < sp.n_rays) {
@@ -822,8 +845,10 @@ multi_count_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const float
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t tot = 0;
+            const int nw = blockDim.x >> 5;
 #pragma unroll
-            for (int w = 0; w < COUNT_GROUP / WARP; ++w) tot += wsum[w];
+            for (int w = 0; w < COUNT_GROUP_MAX / WARP; ++w)
+                if (w < nw) tot += wsum[w];
             block_agg[chunk] = tot;
             __threadfence();
             last_s = atomicAdd(ticket, 1u) == A.total_chunks - 1;
@@ -831,7 +856,7 @@ multi_count_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const float
         __syncthreads();
         if (last_s) {
             __threadfence();
-            scan_blocks_and_cut<COUNT_GROUP>(A.total_chunks, A.total_rays, counts, block_agg, block_prefix,
+            scan_blocks_and_cut<COUNT_GROUP_MAX>(A.total_chunks, A.total_rays, counts, block_agg, block_prefix,
                                              0xffffffffu, batch_info, flags);
             __syncthreads();
             if (scene_samples && threadIdx.x < A.n_scenes) {
@@ -848,41 +873,63 @@ multi_count_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const float
     }
 }
 
-__global__ void __launch_bounds__(EXPAND_WARPS * WARP)
+template <int RPW>
+__global__ void __launch_bounds__(EXPAND_THREADS_MAX)
 multi_expand_kernel(const __grid_constant__ MultiArgs A, uint32_t rs, const uint32_t* __restrict__ block_prefix,
                     const uint32_t* __restrict__ img_id, const float* __restrict__ ori, const float* __restrict__ dir,
                     const float* __restrict__ ray_t, const uint8_t* __restrict__ alive,
                     const uint32_t* __restrict__ counts, uint32_t* __restrict__ offsets, SampleOut o, uint32_t* flags,
                     const float* __restrict__ slots, uint32_t slot_cap) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t r_i = blockIdx.x * EXPAND_WARPS + (threadIdx.x >> 5);
+    constexpr int L = WARP / RPW;
+    const int lane = threadIdx.x & 31, sub = lane & (L - 1);
+    const uint32_t r_i = ((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * RPW) + (uint32_t)(lane / L);
     const uint32_t last = A.sp[A.n_scenes - 1].ray_begin + A.sp[A.n_scenes - 1].n_rays;
-    if (r_i >= last) return;
-    const SceneParams& sp = A.sp[scene_of_ray(A, r_i)];
-    if (r_i - sp.ray_begin >= sp.n_rays) return;  // a gap between scenes
+    const SceneParams& sp = A.sp[scene_of_ray(A, r_i < last ? r_i : 0u)];
+    // rays past the end and rays in a gap between scenes do nothing
+    const bool valid = r_i < last && r_i - sp.ray_begin < sp.n_rays;
     const uint32_t local = r_i - sp.ray_begin;
-    const uint32_t chunk = sp.chunk_begin + local / COUNT_GROUP;
-    const uint32_t g0 = sp.ray_begin + (local / COUNT_GROUP) * COUNT_GROUP;
+    const uint32_t chunk = sp.chunk_begin + (local >> A.chunk_shift);
+    const uint32_t g0 = sp.ray_begin + ((local >> A.chunk_shift) << A.chunk_shift);
     uint32_t part = 0;
-    for (uint32_t j = g0 + lane; j < r_i; j += WARP) part += counts[j];
-    const uint32_t o0 = warp_sum(part) + block_prefix[chunk];
+    if (valid)
+        for (uint32_t j = g0 + sub; j < r_i; j += L) part += counts[j];
+    part = group_sum<L>(part);  // every lane of the warp takes part before any leaves
+    if (!valid) return;
+    const uint32_t o0 = part + block_prefix[chunk];
     const uint32_t n = counts[r_i];
-    if (lane == 0) offsets[r_i] = o0;
+    if (sub == 0) offsets[r_i] = o0;
     if (n == 0 || !alive[r_i]) return;
     if ((unsigned long long)o0 + n > (unsigned long long)o.ss) {
-        if (lane == 0) raise_flag(flags, ERR_CAPACITY);
+        if (sub == 0) raise_flag(flags, ERR_CAPACITY);
         return;
     }
-    expand_ray(sp.a, sp.inv_aabb, r_i, o0, n, rs, img_id, ori, dir, ray_t, o, slots, slot_cap, lane);
+    expand_ray(sp.a, sp.inv_aabb, r_i, o0, n, rs, img_id, ori, dir, ray_t, o, slots, slot_cap, sub, L);
 }
 
 // ---- compaction: ascending indices of non-zero values ---------------------------------
-__global__ void __launch_bounds__(MARCH_BLOCK)
+// A tile of BLOCK x ITEMS values per block; each thread owns ITEMS consecutive values, so the
+// per-thread counts scanned in thread order give ascending output positions.
+template <int BLOCK, int ITEMS>
+__device__ __forceinline__ uint32_t tile_flags(uint32_t n, const uint32_t* __restrict__ values, uint32_t first,
+                                               uint32_t& bits) {
+    bits = 0u;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t i = first + (uint32_t)j;
+        if (i < n && __ldg(values + i) != 0u) bits |= 1u << j;
+    }
+    return (uint32_t)__popc(bits);
+}
+
+template <int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK)
 compact_count_kernel(uint32_t n, const uint32_t* __restrict__ values, uint32_t* block_agg, uint32_t* block_prefix,
                      uint32_t* count_dev, uint32_t* ticket) {
-    const uint32_t i = blockIdx.x * MARCH_BLOCK + threadIdx.x;
-    const uint32_t f = (i < n && values[i] != 0u) ? 1u : 0u;
-    const uint32_t s = __syncthreads_count(f);
+    const uint32_t first = (blockIdx.x * BLOCK + threadIdx.x) * ITEMS;
+    uint32_t bits;
+    const uint32_t f = tile_flags<BLOCK, ITEMS>(n, values, first, bits);
+    uint32_t s;
+    block_exclusive_scan<BLOCK>(f, &s);
     __shared__ bool is_last;
     if (threadIdx.x == 0) {
         block_agg[blockIdx.x] = s;
@@ -895,11 +942,11 @@ compact_count_kernel(uint32_t n, const uint32_t* __restrict__ values, uint32_t* 
     __shared__ uint32_t carry_s;
     if (threadIdx.x == 0) carry_s = 0u;
     __syncthreads();
-    for (uint32_t base = 0; base < gridDim.x; base += MARCH_BLOCK) {
+    for (uint32_t base = 0; base < gridDim.x; base += BLOCK) {
         const uint32_t b = base + threadIdx.x;
         const uint32_t v = b < gridDim.x ? *((volatile uint32_t*)(block_agg + b)) : 0u;
         uint32_t tot;
-        const uint32_t ex = block_exclusive_scan(v, &tot);
+        const uint32_t ex = block_exclusive_scan<BLOCK>(v, &tot);
         if (b < gridDim.x) block_prefix[b] = carry_s + ex;
         __syncthreads();
         if (threadIdx.x == 0) carry_s += tot;
@@ -911,14 +958,18 @@ compact_count_kernel(uint32_t n, const uint32_t* __restrict__ values, uint32_t* 
     }
 }
 
-__global__ void __launch_bounds__(MARCH_BLOCK)
+template <int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK)
 compact_write_kernel(uint32_t n, const uint32_t* __restrict__ values, const uint32_t* __restrict__ block_prefix,
                      int32_t* __restrict__ out) {
-    const uint32_t i = blockIdx.x * MARCH_BLOCK + threadIdx.x;
-    const uint32_t f = (i < n && values[i] != 0u) ? 1u : 0u;
+    const uint32_t first = (blockIdx.x * BLOCK + threadIdx.x) * ITEMS;
+    uint32_t bits;
+    const uint32_t f = tile_flags<BLOCK, ITEMS>(n, values, first, bits);
     uint32_t tot;
-    const uint32_t pos = block_exclusive_scan(f, &tot) + block_prefix[blockIdx.x];
-    if (f) out[pos] = (int32_t)i;
+    uint32_t pos = block_exclusive_scan<BLOCK>(f, &tot) + block_prefix[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j)
+        if ((bits >> j) & 1u) out[pos++] = (int32_t)(first + (uint32_t)j);
 }
 
 // ---- plain path kernels (one thread per ray, reference launch structure) -------------
@@ -1041,12 +1092,13 @@ static int make_count_grid(const MarchArgs& a, CountGrid& cg) {
 // Per-scene parameters of a multi-scene launch; scratch: per scene [mip | box | planes] in
 // ctx->mip, each part 256-byte aligned.
 static int make_multi_args(tn_ctx* ctx, uint32_t n_scenes, const tn_scene* scenes, uint32_t ray_stride,
-                           MultiArgs& A, bool build_scratch) {
+                           uint32_t chunk_rays, MultiArgs& A, bool build_scratch) {
     TN_NONNULL(scenes);
     TN_REQUIRE(n_scenes >= 1 && n_scenes <= (uint32_t)MAX_SCENES, TN_E_INVALID, "n_scenes = %u outside 1..%d", n_scenes,
                MAX_SCENES);
     std::memset(&A, 0, sizeof(A));
     A.n_scenes = n_scenes;
+    while ((1u << A.chunk_shift) < chunk_rays) ++A.chunk_shift;
     uint32_t chunk = 0, prev_end = 0, max_res = 0;
     size_t scratch = 0;
     for (uint32_t s = 0; s < n_scenes; ++s) {
@@ -1063,7 +1115,7 @@ static int make_multi_args(tn_ctx* ctx, uint32_t n_scenes, const tn_scene* scene
         sp.ray_begin = sc.ray_begin;
         sp.n_rays = sc.n_rays;
         sp.chunk_begin = chunk;
-        chunk += (sc.n_rays + COUNT_GROUP - 1) / COUNT_GROUP;
+        chunk += (sc.n_rays + chunk_rays - 1) >> A.chunk_shift;
         const int res = sc.grid.resolution;
         max_res = std::max<uint32_t>(max_res, (uint32_t)res);
         sp.use_mip = res >= MIP_MIN_RES && res <= MIP_MAX_RES;
@@ -1111,20 +1163,29 @@ static uint32_t multi_slot_capacity(uint32_t n_rays) {
 }
 
 template <int NL>
-static void launch_count_nl(bool mip, uint32_t nb, size_t smem, cudaStream_t stream, const MarchArgs& a,
+static void launch_count_nl(bool mip, uint32_t nb, uint32_t group, size_t smem, cudaStream_t stream, const MarchArgs& a,
                             const CountGrid& cg, uint32_t n_rays, const uint32_t* n_rays_dev, uint32_t rs,
                             const float* ori, const float* dir, const float* ray_t, const float* ray_t_max,
                             uint8_t* alive, uint32_t* counts, uint32_t batch_size, uint32_t* batch_info,
                             uint32_t* block_agg, uint32_t* block_prefix, uint32_t* ticket, uint32_t* flags,
                             const uint8_t* mip_g, const int* box_g, float* slots, uint32_t slot_cap) {
     if (mip)
-        march_count_kernel<NL, true><<<nb, COUNT_GROUP, smem, stream>>>(
+        march_count_kernel<NL, true><<<nb, group, smem, stream>>>(
             a, cg, n_rays, n_rays_dev, rs, ori, dir, ray_t, ray_t_max, alive, counts, batch_size, batch_info,
             block_agg, block_prefix, ticket, flags, mip_g, box_g, slots, slot_cap);
     else
-        march_count_kernel<NL, false><<<nb, COUNT_GROUP, smem, stream>>>(
+        march_count_kernel<NL, false><<<nb, group, smem, stream>>>(
             a, cg, n_rays, n_rays_dev, rs, ori, dir, ray_t, ray_t_max, alive, counts, batch_size, batch_info,
             block_agg, block_prefix, ticket, flags, mip_g, box_g, slots, slot_cap);
+}
+
+// The two passes of the compaction with a tile of BLOCK x ITEMS values.
+template <int BLOCK, int ITEMS>
+static void launch_compact(cudaStream_t stream, uint32_t nb, uint32_t n, const uint32_t* values, tn_ctx* ctx,
+                           int32_t* out, uint32_t* count_dev) {
+    compact_count_kernel<BLOCK, ITEMS><<<nb, BLOCK, 0, stream>>>(n, values, ctx->block_u32, ctx->block_u32 + nb,
+                                                                 count_dev, ctx->tickets + TICKET_COMPACT);
+    compact_write_kernel<BLOCK, ITEMS><<<nb, BLOCK, 0, stream>>>(n, values, ctx->block_u32 + nb, out);
 }
 
 }  // namespace tn
@@ -1158,7 +1219,8 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     TN_NONNULL(n_steps); TN_NONNULL(batch_info);
     TN_REQUIRE(n_rays > 0, TN_E_NO_RAYS, "tn_march_count: n_rays = 0");
     TN_REQUIRE(ray_stride >= n_rays, TN_E_INVALID, "ray_stride %u < n_rays %u", ray_stride, n_rays);
-    const uint32_t nb = (n_rays + COUNT_GROUP - 1) / COUNT_GROUP;
+    const uint32_t group = ctx->tune.count_rays_per_block;
+    const uint32_t nb = (n_rays + group - 1) / group;
     st = ensure_block_u32(ctx, 2 * (size_t)nb);
     if (st != TN_OK) return st;
     // coarse mip of the bitfield, the per-level boxes of occupied blocks and the bit-planes:
@@ -1194,7 +1256,7 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     const size_t smem = (size_t)12 * res + mip_bytes;
 #define TN_COUNT_CASE(NL)                                                                                          \
     case NL:                                                                                                       \
-        launch_count_nl<NL>(use_mip, nb, smem, stream, a, cg, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t,     \
+        launch_count_nl<NL>(use_mip, nb, group, smem, stream, a, cg, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t,     \
                             ray_t_max, alive, n_steps, batch_size, batch_info, ctx->block_u32, ctx->block_u32 + nb, \
                             ctx->tickets + TICKET_MARCH, ctx->flags, ctx->mip, box, ctx->slots, slot_cap);       \
         break;
@@ -1203,6 +1265,7 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
         TN_COUNT_CASE(5) TN_COUNT_CASE(6) TN_COUNT_CASE(7) TN_COUNT_CASE(8)
     }
 #undef TN_COUNT_CASE
+    ctx->count_group_used = group;
     return check_launch("tn_march_count");
 }
 
@@ -1222,14 +1285,25 @@ int tn_march_emit(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, con
     TN_NONNULL(out_dt); TN_NONNULL(out_m_norm); TN_NONNULL(out_dt_norm);
     TN_REQUIRE(n_rays > 0, TN_E_NO_RAYS, "tn_march_emit: n_rays = 0");
     TN_REQUIRE(ray_stride >= n_rays, TN_E_INVALID, "ray_stride %u < n_rays %u", ray_stride, n_rays);
-    const uint32_t nb = (n_rays + COUNT_GROUP - 1) / COUNT_GROUP;
+    const uint32_t group = ctx->count_group_used;
+    TN_REQUIRE(group != 0, TN_E_STATE, "tn_march_emit must follow tn_march_count on the same context");
+    const uint32_t nb = (n_rays + group - 1) / group;
     TN_REQUIRE(ctx->block_u32_cap >= 2 * (size_t)nb && ctx->slot_rays == n_rays, TN_E_STATE,
                "tn_march_emit must follow tn_march_count on the same context with the same n_rays");
     SampleOut o{out_img_id, out_t, out_pos, out_dir, out_dt, out_m_norm, out_dt_norm, sample_stride};
-    const uint32_t n_blocks = (n_rays + EXPAND_WARPS - 1) / EXPAND_WARPS;
-    expand_kernel<<<n_blocks, EXPAND_WARPS * WARP, 0, stream>>>(a, inv_aabb_size, n_rays, nullptr, ray_stride, batch_info,
-                                                  ctx->block_u32 + nb, ray_img_id, ori, dir, ray_t, alive, n_steps,
-                                                  offsets, o, ctx->flags, ctx->slots, ctx->slot_cap);
+    const uint32_t gshift = (uint32_t)__builtin_ctz(group);
+    const uint32_t warps = ctx->tune.emit_warps_per_block, rpw = ctx->tune.emit_rays_per_warp;
+    const uint32_t per_block = warps * rpw;
+    const uint32_t n_blocks = (n_rays + per_block - 1) / per_block;
+#define TN_EXPAND(RPW)                                                                                              \
+    expand_kernel<RPW><<<n_blocks, warps * WARP, 0, stream>>>(a, inv_aabb_size, n_rays, nullptr, ray_stride, gshift, \
+                                                             batch_info, ctx->block_u32 + nb, ray_img_id, ori, dir,  \
+                                                             ray_t, alive, n_steps, offsets, o, ctx->flags,          \
+                                                             ctx->slots, ctx->slot_cap)
+    if (rpw == 4) TN_EXPAND(4);
+    else if (rpw == 2) TN_EXPAND(2);
+    else TN_EXPAND(1);
+#undef TN_EXPAND
     return check_launch("tn_march_emit");
 }
 
@@ -1243,7 +1317,8 @@ int tn_multi_march_count(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, con
     static MultiArgs A;  // large; built under the host lock of the calling thread's launch
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
-    int st = make_multi_args(ctx, n_scenes, scenes, ray_stride, A, true);
+    const uint32_t chunk_rays = ctx->tune.multi_chunk_rays;
+    int st = make_multi_args(ctx, n_scenes, scenes, ray_stride, chunk_rays, A, true);
     if (st != TN_OK) return st;
     TN_REQUIRE(A.total_rays > 0, TN_E_NO_RAYS, "tn_multi_march_count: no rays");
     st = ensure_block_u32(ctx, 2 * (size_t)A.total_chunks);
@@ -1266,9 +1341,10 @@ int tn_multi_march_count(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, con
     }
     const size_t smem = (size_t)12 * A.spread_res + (size_t)(MIP_MAX_RES / 4) * (MIP_MAX_RES / 4) * (MIP_MAX_RES / 4);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_count_kernel, COUNT_GROUP, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_count_kernel, (int)chunk_rays, smem);
     const uint32_t grid = std::min<uint32_t>(A.total_chunks, (uint32_t)(num_sms() * std::max(per_sm, 1)));
-    multi_count_kernel<<<grid, COUNT_GROUP, smem, stream>>>(
+    ctx->multi_chunk_used = chunk_rays;
+    multi_count_kernel<<<grid, chunk_rays, smem, stream>>>(
         A, ray_stride, ori, dir, ray_t, ray_t_max, alive, n_steps, ctx->block_u32, ctx->block_u32 + A.total_chunks,
         ctx->tickets + TICKET_MULTI_WORK, ctx->tickets + TICKET_MULTI, ctx->flags, ctx->slots, slot_cap,
         scene_samples, batch_info);
@@ -1287,15 +1363,23 @@ int tn_multi_march_emit(tn_ctx* ctx, tn_stream_t stream, uint32_t n_scenes, cons
     static MultiArgs A;
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
-    int st = make_multi_args(ctx, n_scenes, scenes, ray_stride, A, false);
+    TN_REQUIRE(ctx->multi_chunk_used != 0, TN_E_STATE, "tn_multi_march_emit must follow tn_multi_march_count");
+    int st = make_multi_args(ctx, n_scenes, scenes, ray_stride, ctx->multi_chunk_used, A, false);
     if (st != TN_OK) return st;
     TN_REQUIRE(ctx->block_u32_cap >= 2 * (size_t)A.total_chunks && ctx->slot_rays == A.total_rays, TN_E_STATE,
                "tn_multi_march_emit must follow tn_multi_march_count on the same context with the same scenes");
     SampleOut o{out_img_id, out_t, out_pos, out_dir, out_dt, out_m_norm, out_dt_norm, sample_stride};
-    const uint32_t n_blocks = (A.total_rays + EXPAND_WARPS - 1) / EXPAND_WARPS;
-    multi_expand_kernel<<<n_blocks, EXPAND_WARPS * WARP, 0, stream>>>(
-        A, ray_stride, ctx->block_u32 + A.total_chunks, ray_img_id, ori, dir, ray_t, alive, n_steps, offsets, o,
-        ctx->flags, ctx->slots, ctx->slot_cap);
+    const uint32_t warps = ctx->tune.emit_warps_per_block, rpw = ctx->tune.emit_rays_per_warp;
+    const uint32_t per_block = warps * rpw;
+    const uint32_t n_blocks = (A.total_rays + per_block - 1) / per_block;
+#define TN_MULTI_EXPAND(RPW)                                                                                  \
+    multi_expand_kernel<RPW><<<n_blocks, warps * WARP, 0, stream>>>(A, ray_stride, ctx->block_u32 + A.total_chunks, \
+                                                                   ray_img_id, ori, dir, ray_t, alive, n_steps,    \
+                                                                   offsets, o, ctx->flags, ctx->slots, ctx->slot_cap)
+    if (rpw == 4) TN_MULTI_EXPAND(4);
+    else if (rpw == 2) TN_MULTI_EXPAND(2);
+    else TN_MULTI_EXPAND(1);
+#undef TN_MULTI_EXPAND
     return check_launch("tn_multi_march_emit");
 }
 
@@ -1355,15 +1439,18 @@ int tn_compact_nonzero(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32
                        uint32_t* count_dev) {
     TN_NONNULL(ctx); TN_NONNULL(values); TN_NONNULL(out); TN_NONNULL(count_dev);
     if (n == 0) return cuda_status(cudaMemsetAsync(count_dev, 0, sizeof(uint32_t), stream), "tn_compact_nonzero");
-    const uint32_t nb = (n + MARCH_BLOCK - 1) / MARCH_BLOCK;
+    const uint32_t tile = ctx->tune.compact_tile;
+    const uint32_t nb = (uint32_t)(((uint64_t)n + tile - 1) / tile);
     int st = ensure_block_u32(ctx, 2 * (size_t)nb);
     if (st != TN_OK) return st;
-    compact_count_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, values, ctx->block_u32, ctx->block_u32 + nb, count_dev,
-                                                          ctx->tickets + TICKET_COMPACT);
-    st = check_launch("tn_compact_nonzero(count)");
-    if (st != TN_OK) return st;
-    compact_write_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, values, ctx->block_u32 + nb, out);
-    return check_launch("tn_compact_nonzero(write)");
+    switch (tile) {
+        case 256: launch_compact<256, 1>(stream, nb, n, values, ctx, out, count_dev); break;
+        case 512: launch_compact<256, 2>(stream, nb, n, values, ctx, out, count_dev); break;
+        case 1024: launch_compact<256, 4>(stream, nb, n, values, ctx, out, count_dev); break;
+        case 2048: launch_compact<256, 8>(stream, nb, n, values, ctx, out, count_dev); break;
+        default: launch_compact<128, 1>(stream, nb, n, values, ctx, out, count_dev); break;
+    }
+    return check_launch("tn_compact_nonzero");
 }
 
 int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,

@@ -24,6 +24,9 @@ struct tn_ctx {
     size_t slots_cap = 0;
     uint32_t slot_cap = 0;              // slots per ray of the last tn_march_count
     uint32_t slot_rays = 0;             // n_rays of the last tn_march_count
+    tn_tuning tune{64, 8, 1, 4, 128, 64};  // launch shapes (tn_tuning_default)
+    uint32_t count_group_used = 0;      // rays per block of the last tn_march_count (its emit's grouping)
+    uint32_t multi_chunk_used = 0;      // rays per chunk of the last tn_multi_march_count
 };
 
 namespace tn {

@@ -625,6 +625,65 @@ int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages
     return st;
 }
 
+// Releases the captured step graphs; the next step captures them again (after a change of
+// launch shapes).
+static void drop_graphs(tn_trainer* tr) {
+    for (int i = 0; i < 2; ++i) {
+        if (tr->graph_exec[i]) cudaGraphExecDestroy(tr->graph_exec[i]);
+        if (tr->graph[i]) cudaGraphDestroy(tr->graph[i]);
+        tr->graph_exec[i] = nullptr;
+        tr->graph[i] = nullptr;
+    }
+}
+
+int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
+    TN_NONNULL(tr);
+    TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "tn_trainer_autotune: the fused path only");
+    cudaStream_t s = tr->stream;
+    const tn_trainer_desc& d = tr->d;
+    const tn_grid_desc grid = tr->grid();
+    const tn_march_desc march = tr->march();
+    int st = cuda_status(cudaStreamSynchronize(s), "tn_trainer_autotune");
+    // before the first step the ray buffers are empty: generate the first step's rays
+    if (st == TN_OK && tr->fused_steps_enqueued == 0)
+        st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
+                               3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+    uint32_t* info = tr->state->batch_info;
+    tn_tune_report rep[3] = {};
+    if (st == TN_OK)
+        st = tn_autotune_march(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, nullptr,
+                               tr->ori, tr->dir, tr->ray_t, tr->ray_tmax, tr->alive, tr->n_steps, tr->B, info, tr->B,
+                               tr->offsets, nullptr, tr->s_t, tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm,
+                               tr->s_dtnorm, &rep[0], &rep[1]);
+    if (st == TN_OK)
+        st = tr->net.forward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
+                             tr->net_rgb);
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->grad_density, 0, (size_t)tr->B * 4, s), "grad memset");
+    tn_ray_batch rb{tr->R, tr->R, tr->B, 0, tr->n_steps, tr->offsets, info};
+    if (st == TN_OK)
+        st = tn_autotune_losses(tr->ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, info, d.loss_scale,
+                                d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb,
+                                tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, tr->target, tr->bg, nullptr,
+                                tr->grad_density, tr->dl_drgb, tr->state->loss_sums, &rep[2]);
+    drop_graphs(tr);  // the captured step graphs hold the previous shapes
+    if (reports)
+        for (int k = 0; k < 3; ++k) reports[k] = rep[k];
+    return st;
+}
+
+int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out) {
+    TN_NONNULL(tr);
+    return tn_ctx_get_tuning(tr->ctx, out);
+}
+
+int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t) {
+    TN_NONNULL(tr);
+    int st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_set_tuning");
+    if (st == TN_OK) st = tn_ctx_set_tuning(tr->ctx, t);
+    if (st == TN_OK) drop_graphs(tr);
+    return st;
+}
+
 int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out) {
     TN_NONNULL(tr); TN_NONNULL(out);
     switch (which) {

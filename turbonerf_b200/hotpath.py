@@ -48,6 +48,21 @@ class Context:
         call("tn_ctx_check", self.handle, _stream(), ctypes.byref(f))
         return f.value
 
+    @property
+    def tuning(self) -> dict:
+        """Launch shapes used by later calls on this context (tn_tuning fields)."""
+        t = native.Tuning()
+        call("tn_ctx_get_tuning", self.handle, ctypes.byref(t))
+        return t.as_dict()
+
+    @tuning.setter
+    def tuning(self, values: dict) -> None:
+        t = native.Tuning()
+        call("tn_ctx_get_tuning", self.handle, ctypes.byref(t))
+        for k, v in values.items():
+            setattr(t, k, int(v))
+        call("tn_ctx_set_tuning", self.handle, ctypes.byref(t))
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             native.lib().tn_ctx_destroy(self.handle)
@@ -153,6 +168,48 @@ def march_emit(ctx: Context, grid: GridSpec, bitfield, bbox, march: MarchSpec, i
     return offsets, samples
 
 
+def default_tuning() -> dict:
+    t = native.Tuning()
+    native.lib().tn_tuning_default(ctypes.byref(t))
+    return t.as_dict()
+
+
+def autotune_march(ctx: Context, grid: GridSpec, bitfield, bbox, march: MarchSpec, inv_aabb: float, n_rays: int,
+                   ray_stride: int, ori, dir_, ray_t, ray_t_max, alive, batch_size: int, sample_stride: int,
+                   ray_img_id=None, n_steps=None, batch_info=None, offsets=None, samples=None):
+    """Autotuner of the march count block size and the emit shape on these rays. Returns
+    (n_steps, batch_info, offsets, samples, reports): the outputs of one count + emit with the
+    chosen shapes, and the count and emit tuning reports (dicts)."""
+    dev = ori.device
+    if n_steps is None:
+        n_steps = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    if batch_info is None:
+        batch_info = torch.zeros(4, dtype=torch.int32, device=dev)
+    if offsets is None:
+        offsets = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    if samples is None:
+        samples = alloc_samples(sample_stride, dev)
+    rc, re_ = native.TuneReport(), native.TuneReport()
+    g, b, m = grid.desc(), bbox_desc(bbox), march.desc()
+    call("tn_autotune_march", ctx.handle, _stream(), ctypes.byref(g), _ptr(bitfield), ctypes.byref(b),
+         ctypes.byref(m), inv_aabb, n_rays, ray_stride, _ptr(ray_img_id), _ptr(ori), _ptr(dir_), _ptr(ray_t),
+         _ptr(ray_t_max), _ptr(alive), _ptr(n_steps), batch_size, _ptr(batch_info), sample_stride, _ptr(offsets),
+         _ptr(samples["img_id"]), _ptr(samples["t"]), _ptr(samples["pos"]), _ptr(samples["dir"]),
+         _ptr(samples["dt"]), _ptr(samples["m_norm"]), _ptr(samples["dt_norm"]), ctypes.byref(rc),
+         ctypes.byref(re_))
+    return n_steps, batch_info, offsets, samples, {"count": rc.as_dict(), "emit": re_.as_dict()}
+
+
+def autotune_compact(ctx: Context, values):
+    """Autotuner of the compaction tile. Returns (indices, report)."""
+    n = values.numel()
+    out = torch.zeros(max(n, 1), dtype=torch.int32, device=values.device)
+    cnt = torch.zeros(1, dtype=torch.int32, device=values.device)
+    rep = native.TuneReport()
+    call("tn_autotune_compact", ctx.handle, _stream(), n, _ptr(values), _ptr(out), _ptr(cnt), ctypes.byref(rep))
+    return out[:int(cnt.item())], rep.as_dict()
+
+
 def scan_offsets(ctx: Context, counts, batch_size: int):
     n = counts.numel()
     offsets = torch.zeros(n, dtype=torch.int32, device=counts.device)
@@ -255,6 +312,30 @@ def multi_march_emit(ctx, table, ray_stride, sample_stride, ori, dir_, ray_t, al
     return offsets, samples
 
 
+def autotune_multi(ctx, table, ray_stride, sample_stride, ori, dir_, ray_t, ray_t_max, alive, ray_img_id=None,
+                   n_steps=None, scene_samples=None, info=None, offsets=None, samples=None):
+    """Autotuner of the multi-scene chunk size and emit shape. Returns (n_steps, scene_samples,
+    info, offsets, samples, reports) with the outputs of one count + emit with the chosen shapes."""
+    dev = ori.device
+    if n_steps is None:
+        n_steps = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    if scene_samples is None:
+        scene_samples = torch.zeros(len(table), dtype=torch.int32, device=dev)
+    if info is None:
+        info = torch.zeros(4, dtype=torch.int32, device=dev)
+    if offsets is None:
+        offsets = torch.zeros(ray_stride, dtype=torch.int32, device=dev)
+    if samples is None:
+        samples = alloc_samples(sample_stride, dev)
+    rc, re_ = native.TuneReport(), native.TuneReport()
+    call("tn_autotune_multi", ctx.handle, _stream(), len(table), ctypes.addressof(table), ray_stride,
+         _ptr(ray_img_id), _ptr(ori), _ptr(dir_), _ptr(ray_t), _ptr(ray_t_max), _ptr(alive), _ptr(n_steps),
+         _ptr(scene_samples), _ptr(info), sample_stride, _ptr(offsets), _ptr(samples["img_id"]), _ptr(samples["t"]),
+         _ptr(samples["pos"]), _ptr(samples["dir"]), _ptr(samples["dt"]), _ptr(samples["m_norm"]),
+         _ptr(samples["dt_norm"]), ctypes.byref(rc), ctypes.byref(re_))
+    return n_steps, scene_samples, info, offsets, samples, {"count": rc.as_dict(), "emit": re_.as_dict()}
+
+
 # ---- compositor / losses ------------------------------------------------------------------
 def composite_fwd(ctx, rb: RayBatchDesc, density, rgb, dt, activation=0, min_t=1e-4, out=None):
     dev = density.device
@@ -350,6 +431,24 @@ def train_losses(ctx, rb: RayBatchDesc, density, rgb, dt, m_norm, dt_norm, t, ta
          _ptr(inv_nrays_from), grad_scale, lam, _ptr(density), _ptr(rgb), _ptr(dt), _ptr(m_norm), _ptr(dt_norm),
          _ptr(t), _ptr(target_rgba), _ptr(bg_rgb), _ptr(ray_rgba), _ptr(grad_density), _ptr(dL_drgb), _ptr(loss_sums))
     return grad_density, dL_drgb, loss_sums
+
+
+def autotune_losses(ctx, rb: RayBatchDesc, density, rgb, dt, m_norm, dt_norm, t, target_rgba, bg_rgb, grad_density,
+                    inv_nrays=0.0, inv_nrays_from=None, grad_scale=1.0, lam=0.0, activation=0, min_t=1e-4,
+                    ray_rgba=None, dL_drgb=None, loss_sums=None):
+    """Autotuner of the fused loss kernel's block size; the outputs are those of one
+    train_losses call with the chosen shape. Returns (grad_density, dL_drgb, loss_sums, report)."""
+    dev = density.device
+    if dL_drgb is None:
+        dL_drgb = torch.zeros(3 * rb.sample_stride, dtype=torch.float32, device=dev)
+    if loss_sums is None:
+        loss_sums = torch.zeros(2, dtype=torch.float32, device=dev)
+    rep = native.TuneReport()
+    call("tn_autotune_losses", ctx.handle, _stream(), ctypes.byref(rb), activation, min_t, inv_nrays,
+         _ptr(inv_nrays_from), grad_scale, lam, _ptr(density), _ptr(rgb), _ptr(dt), _ptr(m_norm), _ptr(dt_norm),
+         _ptr(t), _ptr(target_rgba), _ptr(bg_rgb), _ptr(ray_rgba), _ptr(grad_density), _ptr(dL_drgb), _ptr(loss_sums),
+         ctypes.byref(rep))
+    return grad_density, dL_drgb, loss_sums, rep.as_dict()
 
 
 def plain_recon_loss(rb, density, rgb, dt, target_rgba, bg_rgb, inv_nrays, grad_scale=1.0, activation=0, min_t=1e-4):

@@ -81,6 +81,25 @@ class RayBatchDesc(ctypes.Structure):
                 ("n_rays_dev", ctypes.c_void_p)]
 
 
+class Tuning(ctypes.Structure):
+    """tn_tuning: launch shapes of the tunable kernels."""
+    _fields_ = [("count_rays_per_block", ctypes.c_uint32), ("emit_warps_per_block", ctypes.c_uint32),
+                ("emit_rays_per_warp", ctypes.c_uint32), ("loss_rays_per_block", ctypes.c_uint32),
+                ("compact_tile", ctypes.c_uint32), ("multi_chunk_rays", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+class TuneReport(ctypes.Structure):
+    """tn_tune_report: candidates tried, median ms before and with the chosen shape."""
+    _fields_ = [("n_candidates", ctypes.c_uint32), ("before_ms", ctypes.c_float), ("best_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {"n_candidates": int(self.n_candidates), "before_ms": float(self.before_ms),
+                "best_ms": float(self.best_ms)}
+
+
 TN_PATH_FUSED = 0
 TN_PATH_PLAIN = 1
 
@@ -125,6 +144,21 @@ SIGNATURES = {
     "tn_ctx_reserve": [_vp, _u32, _u32],
     "tn_ctx_check": [_vp, _vp, _P(_u32)],
     "tn_ctx_flags_ptr": [_vp, _P(_vp)],
+    "tn_tuning_default": [_P(Tuning)],
+    "tn_tuning_validate": [_P(Tuning)],
+    "tn_ctx_set_tuning": [_vp, _P(Tuning)],
+    "tn_ctx_get_tuning": [_vp, _P(Tuning)],
+    "tn_autotune_march": [_vp, _vp, _P(GridDesc), _vp, _P(Bbox), _P(MarchDesc), _f32, _u32, _u32, _vp, _vp, _vp,
+                          _vp, _vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                          _P(TuneReport), _P(TuneReport)],
+    "tn_autotune_multi": [_vp, _vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp,
+                          _vp, _vp, _vp, _vp, _vp, _vp, _P(TuneReport), _P(TuneReport)],
+    "tn_autotune_losses": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _f32, _vp, _f32, _f32, _vp, _vp, _vp, _vp, _vp,
+                           _vp, _vp, _vp, _vp, _vp, _vp, _vp, _P(TuneReport)],
+    "tn_autotune_compact": [_vp, _vp, _u32, _vp, _vp, _vp, _P(TuneReport)],
+    "tn_trainer_autotune": [_vp, _P(TuneReport)],
+    "tn_trainer_get_tuning": [_vp, _P(Tuning)],
+    "tn_trainer_set_tuning": [_vp, _P(Tuning)],
     "tn_rays_init_bbox": [_vp, _u32, _u32, _P(Bbox), _f32, _vp, _vp, _vp, _vp, _vp],
     "tn_march_count": [_vp, _vp, _P(GridDesc), _vp, _P(Bbox), _P(MarchDesc), _u32, _u32, _vp, _vp, _vp, _vp, _vp,
                        _vp, _vp, _u32, _vp],
@@ -178,7 +212,7 @@ SIGNATURES = {
     "tn_trainer_stream": [_vp, _P(_vp)],
     "tn_trainer_buffer": [_vp, _i32, _P(_vp), _P(_u64)],
 }
-_RESTYPE = {"tn_last_error": ctypes.c_char_p}
+_RESTYPE = {"tn_last_error": ctypes.c_char_p, "tn_tuning_default": None}
 
 _lib = None
 

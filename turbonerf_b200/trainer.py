@@ -17,7 +17,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import native
-from .native import Bbox, GridDesc, OccupancyMetricsC, TrainerDesc, TrainingMetricsC, call
+from .native import Bbox, GridDesc, OccupancyMetricsC, TrainerDesc, TrainingMetricsC, TuneReport, Tuning, call
 
 MIN_STEP_SIZE = 0.00169145586  # NeRFConstants::min_step_size
 CONE_ANGLE = 1.0 / 256.0       # NeRFConstants::cone_angle
@@ -210,6 +210,30 @@ class Trainer:
         m = OccupancyMetricsC()
         call("tn_trainer_update_occupancy_grid", self._handle(), int(training_step), ctypes.byref(m))
         return OccupancyGridMetrics(m.n_occupied, m.n_total)
+
+    # -- launch shapes -------------------------------------------------------------------
+    def autotune(self) -> dict:
+        """Tunes the march (count block size, emit shape) and the fused loss kernel's block size
+        on this trainer's batch; weights, optimizer state and the grid are left as they are.
+        Returns the reports of the three tuners and the chosen shapes."""
+        reps = (TuneReport * 3)()
+        call("tn_trainer_autotune", self._handle(), reps)
+        return {"count": reps[0].as_dict(), "emit": reps[1].as_dict(), "losses": reps[2].as_dict(),
+                "tuning": self.tuning}
+
+    @property
+    def tuning(self) -> dict:
+        t = Tuning()
+        call("tn_trainer_get_tuning", self._handle(), ctypes.byref(t))
+        return t.as_dict()
+
+    @tuning.setter
+    def tuning(self, values: dict) -> None:
+        t = Tuning()
+        call("tn_trainer_get_tuning", self._handle(), ctypes.byref(t))
+        for k, v in values.items():
+            setattr(t, k, int(v))
+        call("tn_trainer_set_tuning", self._handle(), ctypes.byref(t))
 
     # -- introspection -------------------------------------------------------------------
     def profile_step(self) -> list[float]:
