@@ -61,24 +61,65 @@ def _trainer(scene, path, seed):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
-
+    """SM clock and clock-event reasons sampled during the timed region (read only). NVML is
+    polled every 2 ms from a thread, so even a region of a few ms gets samples; without NVML,
+    nvidia-smi at its shortest interval. The device is found by its PCI bus id."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.samples = []  # (sm MHz, max MHz, set of reasons)
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.index)
+        bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except pynvml.NVMLError:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self.stop.is_set():
+            sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((sm, mx, {k for k, b in bits.items() if r & b}))
+            time.sleep(0.002)
 
     def __enter__(self):
         try:
+            nv, h = self._nvml_handle()
+            self.nvml = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.nvml.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 2.0:
+                time.sleep(0.001)
+            return self
+        except Exception:
+            self.nvml = None
+        try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "10"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0:
+                time.sleep(0.005)
         except OSError:
             self.proc = None
         return self
@@ -88,6 +129,9 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        if self.nvml:
+            self.stop.set()
+            self.nvml.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -97,7 +141,10 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s_mhz, m_mhz, rs in self.samples:
+            sm.append(s_mhz)
+            mx = max(mx, m_mhz)
+            reasons |= rs
         for ln in self.lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
@@ -107,11 +154,11 @@ class ClockSampler:
                 mx = max(mx, float(p[2]))
             except ValueError:
                 continue
-            for k, nm in enumerate(names):
+            for k, nm in enumerate(self.NAMES):
                 if p[5 + k].lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def _peaks():

@@ -122,6 +122,11 @@ typedef struct tn_tuning {
     uint32_t loss_rays_per_block;   /* fused losses, one warp per ray: 2, 4 or 8 (4) */
     uint32_t compact_tile;          /* compaction: values a block, 128, 256, 512, 1024 or 2048 (128) */
     uint32_t multi_chunk_rays;      /* multi-scene count: rays per work-stealing chunk, 32..256 (64) */
+    uint32_t side_sms;              /* 0 (default) or the SMs kept for work beside the march: every
+                                       count block then reserves over half an SM's shared memory,
+                                       so that blocks of kernels doing the same (the training
+                                       controller's Adam of the previous step) run on other SMs;
+                                       below the device's SM count */
 } tn_tuning;
 
 void tn_tuning_default(tn_tuning* out);
@@ -518,6 +523,12 @@ int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages
  * captures its graph again with the chosen shapes. reports[3] (may be NULL): count, emit,
  * losses. Synchronous. */
 int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports);
+/* Applies a pending Adam update and waits for the trainer's stream. With tn_tuning side_sms
+ * > 0 (the default when at least 16 SMs remain beside a march of 256-ray blocks) each step's
+ * Adam update runs at the start of the next step beside its march, so after
+ * tn_trainer_train_step the last step's update is pending. tn_trainer_buffer, the full
+ * occupancy update and stage timing apply it first. */
+int tn_trainer_flush(tn_trainer* tr);
 /* Launch shapes of the trainer's context; setting them (validated) makes the next step
  * capture its graph again. */
 int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out);

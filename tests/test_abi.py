@@ -61,11 +61,12 @@ def test_tuning_defaults_and_validation_without_gpu():
     t = native.Tuning()
     L.tn_tuning_default(ctypes.byref(t))
     assert t.as_dict() == {"count_rays_per_block": 64, "emit_warps_per_block": 8, "emit_rays_per_warp": 1,
-                           "loss_rays_per_block": 4, "compact_tile": 128, "multi_chunk_rays": 64}
+                           "loss_rays_per_block": 4, "compact_tile": 128, "multi_chunk_rays": 64, "side_sms": 0}
     assert L.tn_tuning_validate(ctypes.byref(t)) == native.TN_OK
     allowed = {"count_rays_per_block": [32, 64, 128, 256], "emit_warps_per_block": [1, 2, 4, 8, 16],
                "emit_rays_per_warp": [1, 2, 4], "loss_rays_per_block": [2, 4, 8],
-               "compact_tile": [128, 256, 512, 1024, 2048], "multi_chunk_rays": [32, 64, 128, 256]}
+               "compact_tile": [128, 256, 512, 1024, 2048], "multi_chunk_rays": [32, 64, 128, 256],
+               "side_sms": list(range(1024))}
     for field, values in allowed.items():
         for v in range(0, 4097):
             u = native.Tuning(**t.as_dict())

@@ -260,3 +260,40 @@ def test_trainer_autotune_trains_identically():
     for k, what in ((0, "weights"), (2, "first moments"), (3, "second moments"), (6, "bitfield")):
         dt = np.uint8 if k == 6 else np.float32
         assert_bitwise(host(a.buffer(k, dt)), host(b.buffer(k, dt)), what)
+
+
+def test_pipelined_adam_matches_in_order_adam():
+    """The default trainer runs each step's Adam update at the start of the next step, beside
+    its march, on SMs the march leaves free. Against a trainer that runs Adam in order at the
+    end of each step (side_sms = 0): identical metrics every step, and after the pending update
+    is applied (buffer access flushes it) bit-identical parameters, moments, step counters,
+    grid densities and bitfield. A second flush applies nothing more."""
+    from turbonerf_b200.trainer import SyntheticNeRF, Trainer
+    sc = scenes.march_scene_cascaded(n_rays=8, n_levels=5)
+
+    def make():
+        tr = Trainer(SyntheticNeRF.from_scene(sc), n_rays_per_step=4096, occupancy_cells_per_step=4096,
+                     distortion_lambda=1e-3, occupancy_threshold=0.01, n_grid_params=16 * (1 << 15) * 2,
+                     n_mlp_params=7168, beta2=0.99, seed=0x7B0)
+        tr.use_distortion_loss = True
+        tr.setup_data(batch_size=1 << 16)
+        return tr
+
+    a, b = make(), make()
+    assert a.tuning["side_sms"] > 0, "the trainer pipelines Adam by default"
+    b.tuning = dict(side_sms=0)
+    for _ in range(5):  # eager first step, then graph capture and replays
+        ma, mb = a.train_step(), b.train_step()
+        assert (ma.step, ma.n_rays, ma.n_samples) == (mb.step, mb.n_rays, mb.n_samples)
+        assert ma.loss == mb.loss
+    for k, what in ((0, "weights"), (2, "first moments"), (3, "second moments"), (4, "param steps"),
+                    (5, "grid density"), (6, "bitfield")):
+        dt = np.uint8 if k == 6 else (np.uint32 if k == 4 else np.float32)
+        assert_bitwise(host(a.buffer(k, dt)), host(b.buffer(k, dt)), what)
+    w1 = host(a.buffer(0)).copy()
+    a.flush()
+    assert_bitwise(host(a.buffer(0)), w1, "weights after a second flush")
+    # training goes on after a flush: the next step's graph skips the update already applied
+    ma, mb = a.train_step(), b.train_step()
+    assert ma.loss == mb.loss
+    assert_bitwise(host(a.buffer(0)), host(b.buffer(0)), "weights one step after the flush")

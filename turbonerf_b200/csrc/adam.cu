@@ -6,7 +6,11 @@
 // four gradients are all zero is skipped without touching weights, moments or step
 // counters (the reference's per-parameter "zero gradient => return" rule, applied to whole
 // quads before any other load is issued). Mixed quads update only their active lanes.
+// The kernel loops over the quads with a grid stride, so that the training controller can run
+// it on a subset of the SMs (a small grid of 1024-thread blocks) beside the next step's march.
+#include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "tn_internal.cuh"
 
@@ -17,6 +21,7 @@ struct AdamArgs {
     float inv_loss_scale, lr, beta1, beta2, eps, l2;
     float log2_beta1, log2_beta2;  // log2 of beta1 / beta2 (host double, rounded once)
     const float* lr_dev;  // when set, the learning rate is read from device memory (graph replays)
+    const uint32_t* enable;  // when set, the update runs only if *enable != 0 (a pending update)
 };
 
 // One parameter of ngp_adam_step (adam-optimizer.cuh:69-95). The bias corrections beta^step
@@ -34,12 +39,14 @@ __device__ __forceinline__ void adam_one(const AdamArgs& a, float base_lr, uint3
     w = w - base_lr * sqrtf(c2) * m / (c1 * (sqrtf(v) + a.eps));
 }
 
-__global__ void __launch_bounds__(256)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
 adam_vec4_kernel(AdamArgs a, float* __restrict__ w, float* __restrict__ wcopy, const float* __restrict__ grad,
                  float* __restrict__ m, float* __restrict__ v, uint32_t* __restrict__ steps) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a.enable && *a.enable == 0u) return;
+    const uint32_t stride = gridDim.x * BLOCK;
+    for (uint32_t q = blockIdx.x * BLOCK + threadIdx.x; q < (a.n + 3u) / 4u; q += stride) {
     const uint32_t i0 = q * 4u;
-    if (i0 >= a.n) return;
     if (i0 + 4u <= a.n) {
         float4 g = __ldcs(reinterpret_cast<const float4*>(grad) + q);
         g.x *= a.inv_loss_scale; g.y *= a.inv_loss_scale; g.z *= a.inv_loss_scale; g.w *= a.inv_loss_scale;
@@ -47,7 +54,7 @@ adam_vec4_kernel(AdamArgs a, float* __restrict__ w, float* __restrict__ wcopy, c
         const bool act1 = !(i0 + 1u < a.n_grid && g.y == 0.0f);
         const bool act2 = !(i0 + 2u < a.n_grid && g.z == 0.0f);
         const bool act3 = !(i0 + 3u < a.n_grid && g.w == 0.0f);
-        if (!(act0 | act1 | act2 | act3)) return;
+        if (!(act0 | act1 | act2 | act3)) continue;
         const float base_lr = a.lr_dev ? *a.lr_dev : a.lr;
         float4 wv = reinterpret_cast<float4*>(w)[q];
         float4 mv = reinterpret_cast<float4*>(m)[q];
@@ -74,13 +81,14 @@ adam_vec4_kernel(AdamArgs a, float* __restrict__ w, float* __restrict__ wcopy, c
             if (wcopy) wcopy[i] = wi;
         }
     }
+    }
 }
 
 __global__ void adam_scalar_kernel(AdamArgs a, float* __restrict__ w, float* __restrict__ wcopy,
                                    const float* __restrict__ grad, float* __restrict__ m, float* __restrict__ v,
                                    uint32_t* __restrict__ steps) {
     const uint32_t i = threadIdx.x + blockIdx.x * blockDim.x;
-    if (i >= a.n) return;
+    if (i >= a.n || (a.enable && *a.enable == 0u)) return;
     const float g = grad[i] * a.inv_loss_scale;
     if (i < a.n_grid && g == 0.0f) return;
     float wi = w[i], mi = m[i], vi = v[i];
@@ -128,19 +136,21 @@ static int adam_args(uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_sca
     a.log2_beta1 = (float)std::log2((double)beta1);
     a.log2_beta2 = (float)std::log2((double)beta2);
     a.lr_dev = nullptr;
+    a.enable = nullptr;
     return TN_OK;
 }
 
 int launch_adam(cudaStream_t stream, bool plain, uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_scale,
                 float lr, const float* lr_dev, float beta1, float beta2, float epsilon, float l2_reg, float* weights,
                 float* weights_copy, const float* gradients, float* first_moments, float* second_moments,
-                uint32_t* param_steps) {
+                uint32_t* param_steps, const AdamPlacement& place) {
     TN_NONNULL(weights); TN_NONNULL(gradients); TN_NONNULL(first_moments); TN_NONNULL(second_moments);
     TN_NONNULL(param_steps);
     AdamArgs a;
     int st = adam_args(n, n_grid, n_mlp, loss_scale, lr, beta1, beta2, epsilon, l2_reg, a);
     if (st != TN_OK) return st;
     a.lr_dev = lr_dev;
+    a.enable = place.enable;
     if (n == 0) return TN_OK;
     if (plain) {
         plain_adam_kernel<<<(n + 127) / 128, 128, 0, stream>>>(a, weights, weights_copy, gradients, first_moments,
@@ -149,10 +159,20 @@ int launch_adam(cudaStream_t stream, bool plain, uint32_t n, uint32_t n_grid, ui
     }
     const bool aligned = (((uintptr_t)weights | (uintptr_t)gradients | (uintptr_t)first_moments |
                            (uintptr_t)second_moments | (uintptr_t)param_steps | (uintptr_t)weights_copy) & 15u) == 0;
-    if (aligned) {
+    if (aligned && place.max_blocks) {
+        // a few large blocks, each alone on its SM when reserve_smem is over half an SM's shared memory
+        if (place.reserve_smem > 48 * 1024) {
+            static const int optin_status = allow_optin_smem((const void*)adam_vec4_kernel<1024>);
+            if (optin_status != TN_OK) return optin_status;
+        }
         const uint32_t quads = (n + 3) / 4;
-        adam_vec4_kernel<<<(quads + 255) / 256, 256, 0, stream>>>(a, weights, weights_copy, gradients, first_moments,
-                                                                  second_moments, param_steps);
+        const uint32_t blocks = std::max(1u, std::min(place.max_blocks, (quads + 1023) / 1024));
+        adam_vec4_kernel<1024><<<blocks, 1024, place.reserve_smem, stream>>>(a, weights, weights_copy, gradients,
+                                                                          first_moments, second_moments, param_steps);
+    } else if (aligned) {
+        const uint32_t quads = (n + 3) / 4;
+        adam_vec4_kernel<256><<<(quads + 255) / 256, 256, 0, stream>>>(a, weights, weights_copy, gradients,
+                                                                       first_moments, second_moments, param_steps);
     } else {
         adam_scalar_kernel<<<(n + 255) / 256, 256, 0, stream>>>(a, weights, weights_copy, gradients, first_moments,
                                                                 second_moments, param_steps);
@@ -170,14 +190,14 @@ int tn_adam_step(tn_stream_t stream, uint32_t n, uint32_t n_grid, uint32_t n_mlp
                  float beta1, float beta2, float epsilon, float l2_reg, float* weights, float* weights_copy,
                  const float* gradients, float* first_moments, float* second_moments, uint32_t* param_steps) {
     return launch_adam(stream, false, n, n_grid, n_mlp, loss_scale, lr, nullptr, beta1, beta2, epsilon, l2_reg,
-                       weights, weights_copy, gradients, first_moments, second_moments, param_steps);
+                       weights, weights_copy, gradients, first_moments, second_moments, param_steps, AdamPlacement{});
 }
 
 int tn_plain_adam_step(tn_stream_t stream, uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_scale, float lr,
                        float beta1, float beta2, float epsilon, float l2_reg, float* weights, float* weights_copy,
                        const float* gradients, float* first_moments, float* second_moments, uint32_t* param_steps) {
     return launch_adam(stream, true, n, n_grid, n_mlp, loss_scale, lr, nullptr, beta1, beta2, epsilon, l2_reg,
-                       weights, weights_copy, gradients, first_moments, second_moments, param_steps);
+                       weights, weights_copy, gradients, first_moments, second_moments, param_steps, AdamPlacement{});
 }
 
 }  // extern "C"

@@ -39,6 +39,30 @@ bool stream_capturing(cudaStream_t s) {
     return st != cudaStreamCaptureStatusNone;
 }
 
+int allow_optin_smem(const void* func) {
+    cudaFuncAttributes fa;
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaFuncGetAttributes(&fa, func);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    return cuda_status(e, "shared memory opt-in");
+}
+
+size_t exclusive_smem() {
+    static size_t cached = 0;
+    if (cached == 0) {
+        int dev = 0, per_sm = 0, reserved = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        // two blocks would need 2 * (excl + reserved) > per_sm
+        cached = (size_t)(per_sm - 2 * reserved) / 2 + 1024;
+    }
+    return cached;
+}
+
 int num_sms() {
     static int cached = 0;
     if (cached == 0) {
@@ -163,7 +187,7 @@ int tn_ctx_flags_ptr(tn_ctx* ctx, uint32_t** flags_dev) {
 extern "C" {
 
 void tn_tuning_default(tn_tuning* out) {
-    if (out) *out = tn_tuning{64, 8, 1, 4, 128, 64};
+    if (out) *out = tn_tuning{64, 8, 1, 4, 128, 64, 0};
 }
 
 static bool one_of(uint32_t v, std::initializer_list<uint32_t> allowed) {
@@ -186,6 +210,7 @@ int tn_tuning_validate(const tn_tuning* t) {
                "tuning: compact_tile %u not in {128, 256, 512, 1024, 2048}", t->compact_tile);
     TN_REQUIRE(one_of(t->multi_chunk_rays, {32, 64, 128, 256}), TN_E_INVALID,
                "tuning: multi_chunk_rays %u not in {32, 64, 128, 256}", t->multi_chunk_rays);
+    TN_REQUIRE(t->side_sms < 1024u, TN_E_INVALID, "tuning: side_sms %u not below 1024", t->side_sms);
     return TN_OK;
 }
 
@@ -193,6 +218,8 @@ int tn_ctx_set_tuning(tn_ctx* ctx, const tn_tuning* t) {
     TN_NONNULL(ctx);
     const int st = tn_tuning_validate(t);
     if (st != TN_OK) return st;
+    TN_REQUIRE(t->side_sms < (uint32_t)num_sms(), TN_E_INVALID, "tuning: side_sms %u leaves no SM of %d", t->side_sms,
+               num_sms());
     ctx->tune = *t;
     return TN_OK;
 }

@@ -1163,12 +1163,20 @@ static uint32_t multi_slot_capacity(uint32_t n_rays) {
 }
 
 template <int NL>
-static void launch_count_nl(bool mip, uint32_t nb, uint32_t group, size_t smem, cudaStream_t stream, const MarchArgs& a,
+static int launch_count_nl(bool mip, uint32_t nb, uint32_t group, size_t smem, cudaStream_t stream, const MarchArgs& a,
                             const CountGrid& cg, uint32_t n_rays, const uint32_t* n_rays_dev, uint32_t rs,
                             const float* ori, const float* dir, const float* ray_t, const float* ray_t_max,
                             uint8_t* alive, uint32_t* counts, uint32_t batch_size, uint32_t* batch_info,
                             uint32_t* block_agg, uint32_t* block_prefix, uint32_t* ticket, uint32_t* flags,
                             const uint8_t* mip_g, const int* box_g, float* slots, uint32_t slot_cap) {
+    if (smem > 48 * 1024) {
+        // the side_sms reservation: allow the device's opt-in shared memory (set once per kernel)
+        static const int optin_status = [] {
+            const int st = allow_optin_smem((const void*)march_count_kernel<NL, true>);
+            return st == TN_OK ? allow_optin_smem((const void*)march_count_kernel<NL, false>) : st;
+        }();
+        if (optin_status != TN_OK) return optin_status;
+    }
     if (mip)
         march_count_kernel<NL, true><<<nb, group, smem, stream>>>(
             a, cg, n_rays, n_rays_dev, rs, ori, dir, ray_t, ray_t_max, alive, counts, batch_size, batch_info,
@@ -1177,6 +1185,7 @@ static void launch_count_nl(bool mip, uint32_t nb, uint32_t group, size_t smem, 
         march_count_kernel<NL, false><<<nb, group, smem, stream>>>(
             a, cg, n_rays, n_rays_dev, rs, ori, dir, ray_t, ray_t_max, alive, counts, batch_size, batch_info,
             block_agg, block_prefix, ticket, flags, mip_g, box_g, slots, slot_cap);
+    return TN_OK;
 }
 
 // The two passes of the compaction with a tile of BLOCK x ITEMS values.
@@ -1253,10 +1262,12 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
     if (st != TN_OK) return st;
     ctx->slot_cap = slot_cap;
     ctx->slot_rays = n_rays;
-    const size_t smem = (size_t)12 * res + mip_bytes;
+    size_t smem = (size_t)12 * res + mip_bytes;
+    // with SMs kept for other work, each count block holds its SM alone (see exclusive_smem)
+    if (ctx->tune.side_sms) smem = std::max(smem, exclusive_smem());
 #define TN_COUNT_CASE(NL)                                                                                          \
     case NL:                                                                                                       \
-        launch_count_nl<NL>(use_mip, nb, group, smem, stream, a, cg, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t,     \
+        st = launch_count_nl<NL>(use_mip, nb, group, smem, stream, a, cg, n_rays, n_rays_dev, ray_stride, ori, dir, ray_t,     \
                             ray_t_max, alive, n_steps, batch_size, batch_info, ctx->block_u32, ctx->block_u32 + nb, \
                             ctx->tickets + TICKET_MARCH, ctx->flags, ctx->mip, box, ctx->slots, slot_cap);       \
         break;
@@ -1265,6 +1276,7 @@ int tn_march_count(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid, co
         TN_COUNT_CASE(5) TN_COUNT_CASE(6) TN_COUNT_CASE(7) TN_COUNT_CASE(8)
     }
 #undef TN_COUNT_CASE
+    if (st != TN_OK) return st;
     ctx->count_group_used = group;
     return check_launch("tn_march_count");
 }

@@ -24,7 +24,7 @@ struct tn_ctx {
     size_t slots_cap = 0;
     uint32_t slot_cap = 0;              // slots per ray of the last tn_march_count
     uint32_t slot_rays = 0;             // n_rays of the last tn_march_count
-    tn_tuning tune{64, 8, 1, 4, 128, 64};  // launch shapes (tn_tuning_default)
+    tn_tuning tune{64, 8, 1, 4, 128, 64, 0};  // launch shapes (tn_tuning_default)
     uint32_t count_group_used = 0;      // rays per block of the last tn_march_count (its emit's grouping)
     uint32_t multi_chunk_used = 0;      // rays per chunk of the last tn_multi_march_count
 };
@@ -78,11 +78,29 @@ inline GridView make_grid_view(const tn_grid_desc& d, const uint8_t* bits) {
 
 int validate_grid(const tn_grid_desc* grid);
 
+// Shared memory that a block reserves so that no second block reserving as much fits on its
+// SM: just over half of the SM's shared memory (blocks of the march count and of the kernels
+// that run beside it on other SMs).
+size_t exclusive_smem();
+// Lets kernel `func` take the device's opt-in shared memory (less its static shared memory) as
+// dynamic shared memory.
+int allow_optin_smem(const void* func);
+
+// Where the fused Adam runs: by default one 256-thread block per 1024 parameters over the whole
+// GPU; with max_blocks, at most that many 1024-thread blocks (a grid-stride loop), each
+// reserving reserve_smem bytes of shared memory. enable: a device flag; the update runs only
+// when it is non-zero.
+struct AdamPlacement {
+    uint32_t max_blocks = 0;
+    size_t reserve_smem = 0;
+    const uint32_t* enable = nullptr;
+};
+
 // Internal launchers (device-side parameters for graph replays).
 int launch_adam(cudaStream_t stream, bool plain, uint32_t n, uint32_t n_grid, uint32_t n_mlp, float loss_scale,
                 float lr, const float* lr_dev, float beta1, float beta2, float epsilon, float l2_reg, float* weights,
                 float* weights_copy, const float* gradients, float* first_moments, float* second_moments,
-                uint32_t* param_steps);
+                uint32_t* param_steps, const AdamPlacement& place = AdamPlacement{});
 int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc* grid, float* density,
                             uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
                             const float* values, const float* rand_select, int activation, int sample_all,

@@ -5,6 +5,13 @@
 // reconstruction + distortion losses with the gradient merge -> network backward ->
 // [occupancy re-sampling of random cells] -> Adam.
 //
+// Pipelined Adam (tn_tuning side_sms > 0, the trainer's default when the SMs allow it): a
+// step's Adam update is left pending and runs at the start of the next step on a second stream,
+// on side_sms SMs, beside that step's march (which holds the other SMs: see exclusive_smem);
+// the next network forward waits for it. The march reads no parameters, so every step computes
+// what the reference computes. A pending update is applied by tn_trainer_flush and before the
+// trainer's buffers are handed out, the full occupancy update and stage timing.
+//
 // Fused path: every stage is one of the library's fused kernels; every step-dependent
 // scalar (step index, learning rate, occupancy selection policy, ray and sample counts)
 // lives in device memory, so the whole step is captured once into a CUDA graph and
@@ -28,12 +35,16 @@ struct StepState {
     uint32_t batch_info[4];
     uint32_t n_occupied;
     float loss_sums[2];
+    float adam_lr;          // learning rate of the step whose Adam update is pending
+    uint32_t adam_pending;  // 1 while the last step's Adam update has not run
     uint32_t pad;
 };
 
-__global__ void step_end_kernel(StepState* s) {
+__global__ void step_end_kernel(StepState* s, uint32_t adam_left_pending) {
     s->samples_total += s->batch_info[1];
     s->rays_total += s->batch_info[0];
+    s->adam_lr = s->lr;
+    s->adam_pending = adam_left_pending;
 }
 
 __global__ void step_begin_kernel(StepState* s, float base_lr, float lr_decay) {
@@ -78,7 +89,7 @@ struct tn_trainer {
     cudaStream_t stream = nullptr;
     // second stream of the captured step: occupancy query and update beside the training chain
     cudaStream_t aux = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_emit = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_emit = nullptr, ev_join = nullptr, ev_adam = nullptr;
     tn_ctx* ctx = nullptr;
     std::vector<void*> allocs;
     uint32_t R = 0, B = 0, V = 0, P = 0, M = 0, chunk = 0;
@@ -157,15 +168,39 @@ static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_gri
                                    nullptr, d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied);
 }
 
-// One fused step. Without stage events the occupancy work runs on a second stream beside the
-// training chain: its query (cell sampling and the density network) overlaps the march, and
-// its update (which rewrites the bitfield, so it waits for the emit pass, the last reader of
-// this step) overlaps the loss, backward and Adam stages; the main stream joins it before
-// step_end. With stage events (profiling) everything runs in order on one stream.
+// The Adam update of the step whose gradients sit in tr->g. With a placement of the side SMs it
+// runs only while a pending update is flagged (the previous step's, at the start of the next).
+static int enqueue_adam(tn_trainer* tr, cudaStream_t s, const float* lr_dev, const AdamPlacement& place) {
+    const tn_trainer_desc& d = tr->d;
+    return launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate, lr_dev,
+                       d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v, tr->steps, place);
+}
+
+// Applies a pending Adam update (pipelined steps leave the last step's update pending).
+static int flush_adam(tn_trainer* tr) {
+    if (tr->d.path != TN_PATH_FUSED) return TN_OK;
+    AdamPlacement place;
+    place.enable = &tr->state->adam_pending;
+    int st = enqueue_adam(tr, tr->stream, &tr->state->adam_lr, place);
+    if (st == TN_OK)
+        st = cuda_status(cudaMemsetAsync(&tr->state->adam_pending, 0, sizeof(uint32_t), tr->stream), "flush");
+    return st;
+}
+
+// One fused step. Without stage events, work runs on a second stream beside the training chain:
+//  * pipelined (side_sms > 0): first the previous step's pending Adam update on side_sms SMs,
+//    beside this step's rays and march (the network forward waits for it);
+//  * the occupancy query (cell sampling and the density network; after that Adam update, since
+//    the network reads the parameters), beside the march;
+//  * the occupancy update, which rewrites the bitfield and so waits for the emit pass (the last
+//    reader of this step), beside the loss and backward stages.
+// The main stream joins the second one before step_end. With stage events (profiling)
+// everything runs in order on one stream, Adam included.
 int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream;
-    const bool side = ev == nullptr && tr->M > 0;
+    const bool pipe = ev == nullptr && tr->ctx->tune.side_sms > 0;
+    const bool side = ev == nullptr && (tr->M > 0 || pipe);
     cudaStream_t so = side ? tr->aux : s;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
@@ -176,7 +211,15 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
     if (st == TN_OK && side) {
         st = cuda_status(cudaEventRecord(tr->ev_fork, s), "fork");
         if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
-        if (st == TN_OK) st = enqueue_occupancy_query(tr, so, grid);
+        if (st == TN_OK && pipe) {
+            AdamPlacement place;
+            place.max_blocks = tr->ctx->tune.side_sms;
+            place.reserve_smem = exclusive_smem();
+            place.enable = &tr->state->adam_pending;
+            st = enqueue_adam(tr, so, &tr->state->adam_lr, place);
+            if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_adam, so), "adam done");
+        }
+        if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_query(tr, so, grid);
     }
     if (st == TN_OK) {
         if (external_rays)
@@ -197,12 +240,13 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
                            nullptr, tr->ori, tr->dir, tr->ray_t, tr->alive, tr->n_steps, tr->offsets, nullptr, tr->s_t,
                            tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
     mark(ST_EMIT);
-    if (st == TN_OK && side) {
+    if (st == TN_OK && side && tr->M > 0) {
         st = cuda_status(cudaEventRecord(tr->ev_emit, s), "emit done");
         if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_emit, 0), "emit done");
         if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid);
-        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_join, so), "join");
     }
+    if (st == TN_OK && side) st = cuda_status(cudaEventRecord(tr->ev_join, so), "join");
+    if (st == TN_OK && pipe) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_adam, 0), "adam done");
     if (st == TN_OK)
         st = tr->net.forward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
                              tr->net_rgb);
@@ -221,11 +265,9 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
     mark(ST_BACKWARD);
     // Adam, then the occupancy update: the reference trains first and refreshes the grid after
     // the step (update_occupancy_grid follows train_step, src/main.cu:157-166); the freshly
-    // written bitfield is then still in L2 for the next step's march.
-    if (st == TN_OK)
-        st = launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate,
-                         &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
-                         tr->steps);
+    // written bitfield is then still in L2 for the next step's march. Pipelined, the update is
+    // left pending for the next step.
+    if (st == TN_OK && !pipe) st = enqueue_adam(tr, s, &tr->state->lr, AdamPlacement{});
     mark(ST_ADAM);
     if (st == TN_OK && !side && tr->M > 0) st = enqueue_occupancy_query(tr, s, grid);
     mark(ST_OCC_QUERY);
@@ -233,7 +275,7 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
     mark(ST_OCCUPANCY);
     if (st == TN_OK && side) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_join, 0), "join");
     if (st == TN_OK) {
-        step_end_kernel<<<1, 1, 0, s>>>(tr->state);
+        step_end_kernel<<<1, 1, 0, s>>>(tr->state, pipe ? 1u : 0u);
         st = check_launch("step_end");
     }
     return st;
@@ -305,7 +347,7 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
                          "batch info");
         if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "plain info sync");
         if (st == TN_OK) {
-            step_end_kernel<<<1, 1, 0, s>>>(tr->state);
+            step_end_kernel<<<1, 1, 0, s>>>(tr->state, 0u);
             st = check_launch("step_end");
         }
     }
@@ -406,7 +448,7 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     }
     st = cuda_status(cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking), "stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->aux, cudaStreamNonBlocking), "aux stream");
-    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join})
+    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join, &tr->ev_adam})
         if (st == TN_OK) st = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "step events");
     if (st == TN_OK) st = tn_ctx_create(&tr->ctx);
     const uint32_t R = desc->n_rays_per_step, B = desc->batch_size;
@@ -417,6 +459,15 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     tr->chunk = std::min(B, V);
     const uint32_t occ_n = std::max(tr->M, tr->chunk);
     if (st == TN_OK) st = tn_ctx_reserve(tr->ctx, R, B);
+    // Pipelined Adam by default: the march count in 256-ray blocks, one per SM, and the other
+    // SMs for the previous step's Adam update, when that leaves at least 16 of them.
+    if (st == TN_OK && desc->path == TN_PATH_FUSED) {
+        const int side = num_sms() - (int)((R + 255) / 256);
+        if (side >= 16) {
+            tr->ctx->tune.count_rays_per_block = 256;
+            tr->ctx->tune.side_sms = (uint32_t)side;
+        }
+    }
 #define ALLOC(p, n) if (st == TN_OK) st = tr->alloc(p, (size_t)(n))
     ALLOC(tr->ori, 3 * R); ALLOC(tr->dir, 3 * R); ALLOC(tr->ray_t, R); ALLOC(tr->ray_tmax, R); ALLOC(tr->target, 4 * R);
     ALLOC(tr->bg, 3 * R); ALLOC(tr->alive, R); ALLOC(tr->n_steps, R); ALLOC(tr->offsets, R);
@@ -459,7 +510,7 @@ int tn_trainer_destroy(tn_trainer* tr) {
     if (tr->synth.waves) cudaFree(tr->synth.waves);
     if (tr->state_host) cudaFreeHost(tr->state_host);
     if (tr->ctx) tn_ctx_destroy(tr->ctx);
-    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join})
+    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join, tr->ev_adam})
         if (e) cudaEventDestroy(e);
     if (tr->aux) cudaStreamDestroy(tr->aux);
     if (tr->stream) cudaStreamDestroy(tr->stream);
@@ -495,6 +546,8 @@ int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bit
 
 int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_touched_out) {
     TN_NONNULL(tr);
+    const int fst = flush_adam(tr);  // a pending update reads the gradients rewritten here
+    if (fst != TN_OK) return fst;
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream;
     const tn_grid_desc grid = tr->grid();
@@ -613,6 +666,9 @@ int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori
 int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages) {
     TN_NONNULL(tr); TN_NONNULL(stage_ms);
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "stage timing covers the fused path");
+    // the timed step runs its own Adam in order; a pending one is applied first, untimed
+    const int fst = flush_adam(tr);
+    if (fst != TN_OK) return fst;
     cudaEvent_t ev[ST_N + 1];
     for (auto& e : ev) cudaEventCreate(&e);
     int st = enqueue_fused_step(tr, false, ev);
@@ -639,6 +695,8 @@ static void drop_graphs(tn_trainer* tr) {
 int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
     TN_NONNULL(tr);
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "tn_trainer_autotune: the fused path only");
+    const int fst = flush_adam(tr);  // the network forward below reads the parameters
+    if (fst != TN_OK) return fst;
     cudaStream_t s = tr->stream;
     const tn_trainer_desc& d = tr->d;
     const tn_grid_desc grid = tr->grid();
@@ -671,6 +729,13 @@ int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
     return st;
 }
 
+int tn_trainer_flush(tn_trainer* tr) {
+    TN_NONNULL(tr);
+    int st = flush_adam(tr);
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_flush");
+    return st;
+}
+
 int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out) {
     TN_NONNULL(tr);
     return tn_ctx_get_tuning(tr->ctx, out);
@@ -678,7 +743,8 @@ int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out) {
 
 int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t) {
     TN_NONNULL(tr);
-    int st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_set_tuning");
+    int st = flush_adam(tr);
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_set_tuning");
     if (st == TN_OK) st = tn_ctx_set_tuning(tr->ctx, t);
     if (st == TN_OK) drop_graphs(tr);
     return st;
@@ -717,6 +783,8 @@ int tn_trainer_sync_metrics(tn_trainer* tr, tn_training_metrics* metrics) {
 
 int tn_trainer_update_occupancy_grid(tn_trainer* tr, uint32_t training_step, tn_occupancy_metrics* metrics) {
     TN_NONNULL(tr);
+    const int fst = flush_adam(tr);  // the density network reads the parameters
+    if (fst != TN_OK) return fst;
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream;
     const tn_grid_desc grid = tr->grid();
@@ -772,6 +840,10 @@ int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out) {
 
 int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes) {
     TN_NONNULL(tr); TN_NONNULL(ptr);
+    // the parameters the caller may read include every step's update
+    int fst = flush_adam(tr);
+    if (fst == TN_OK) fst = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_buffer");
+    if (fst != TN_OK) return fst;
     const uint64_t R = tr->R, B = tr->B, V = tr->V, P = tr->P, L = (uint64_t)tr->d.grid.n_levels;
     void* p = nullptr;
     uint64_t n = 0;

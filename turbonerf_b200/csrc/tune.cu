@@ -144,10 +144,20 @@ int tn_autotune_march(tn_ctx* ctx, tn_stream_t stream, const tn_grid_desc* grid,
                              sample_stride, batch_info, ray_img_id, ori, dir, ray_t, alive, n_steps, offsets,
                              out_img_id, out_t, out_pos, out_dir, out_dt, out_m_norm, out_dt_norm);
     };
+    // With SMs kept aside, count blocks hold an SM each: only block sizes whose blocks all fit
+    // on the remaining SMs at once are candidates.
+    std::vector<uint32_t> cands;
+    for (uint32_t c : COUNT_CANDIDATES)
+        if (!ctx->tune.side_sms || (n_rays + c - 1) / c <= (uint32_t)num_sms() - ctx->tune.side_sms)
+            cands.push_back(c);
+    if (cands.empty()) cands.push_back(COUNT_CANDIDATES[3]);
+    int cur = -1;
+    for (size_t i = 0; i < cands.size(); ++i)
+        if (cands[i] == ctx->tune.count_rays_per_block) cur = (int)i;
     // the count modifies only `alive`, and only to clear rays without samples: calling it again
     // gives the same outputs
-    st = pick(stream, 4, index_of(COUNT_CANDIDATES, ctx->tune.count_rays_per_block),
-              [&](int c) { ctx->tune.count_rays_per_block = COUNT_CANDIDATES[c]; }, no_pre, count, count_report);
+    st = pick(stream, (int)cands.size(), cur, [&](int c) { ctx->tune.count_rays_per_block = cands[c]; }, no_pre,
+              count, count_report);
     if (st == TN_OK) st = count();  // the emit candidates read this count's block prefixes
     if (st == TN_OK)
         st = pick(stream, N_EMIT, emit_index(ctx->tune), [&](int c) { set_emit(ctx, c); }, no_pre, emit,

@@ -85,7 +85,8 @@ class Tuning(ctypes.Structure):
     """tn_tuning: launch shapes of the tunable kernels."""
     _fields_ = [("count_rays_per_block", ctypes.c_uint32), ("emit_warps_per_block", ctypes.c_uint32),
                 ("emit_rays_per_warp", ctypes.c_uint32), ("loss_rays_per_block", ctypes.c_uint32),
-                ("compact_tile", ctypes.c_uint32), ("multi_chunk_rays", ctypes.c_uint32)]
+                ("compact_tile", ctypes.c_uint32), ("multi_chunk_rays", ctypes.c_uint32),
+                ("side_sms", ctypes.c_uint32)]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
@@ -158,6 +159,7 @@ SIGNATURES = {
     "tn_autotune_compact": [_vp, _vp, _u32, _vp, _vp, _vp, _P(TuneReport)],
     "tn_trainer_autotune": [_vp, _P(TuneReport)],
     "tn_trainer_get_tuning": [_vp, _P(Tuning)],
+    "tn_trainer_flush": [_vp],
     "tn_trainer_set_tuning": [_vp, _P(Tuning)],
     "tn_rays_init_bbox": [_vp, _u32, _u32, _P(Bbox), _f32, _vp, _vp, _vp, _vp, _vp],
     "tn_march_count": [_vp, _vp, _P(GridDesc), _vp, _P(Bbox), _P(MarchDesc), _u32, _u32, _vp, _vp, _vp, _vp, _vp,

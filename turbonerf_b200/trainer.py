@@ -221,6 +221,11 @@ class Trainer:
         return {"count": reps[0].as_dict(), "emit": reps[1].as_dict(), "losses": reps[2].as_dict(),
                 "tuning": self.tuning}
 
+    def flush(self) -> None:
+        """Applies a pending Adam update (pipelined steps run each update at the start of the
+        next step) and waits for the trainer's stream."""
+        call("tn_trainer_flush", self._handle())
+
     @property
     def tuning(self) -> dict:
         t = Tuning()
