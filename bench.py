@@ -345,7 +345,7 @@ def run_ours(args):
                    "samples_last_step": result["last"]["n_samples"], "rays_last_step": result["last"]["n_rays"],
                    "touched_hash_grads": result["n_touched"], "launch_shapes": tuned["tuning"],
                    "autotuned": not args.no_autotune},
-        "e2e": {"value": round(e2e_value, 1), "unit": "samples/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": 68},
+        "e2e": {"value": round(e2e_value, 1), "unit": "samples/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": 76},
         "gpu_launches": int(result["kernels"]) * args.steps,
         "roofline": result["roofline"],
         "stages": result["stages"],

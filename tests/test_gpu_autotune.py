@@ -49,8 +49,9 @@ def _same(a, b, what, nsamp):
 
 
 def test_every_march_shape_is_bit_identical():
-    """All 4 count block sizes x 15 emit shapes against the default shape, which is itself
-    checked against the oracle (with the batch cut of training)."""
+    """All 4 count block sizes x 15 emit shapes, with and without the SM reservation of
+    side_sms, against the default shape, which is itself checked against the oracle (with the
+    batch cut of training)."""
     from turbonerf_b200 import hotpath as hp
     sc = scenes.march_scene_cascaded()
     n = sc.rays.n
@@ -67,7 +68,8 @@ def test_every_march_shape_is_bit_identical():
     assert int(base["info"][1]) == nsamp
     for cg in COUNT:
         for w, rpw in EMIT:
-            ctx.tuning = dict(count_rays_per_block=cg, emit_warps_per_block=w, emit_rays_per_warp=rpw)
+            ctx.tuning = dict(count_rays_per_block=cg, emit_warps_per_block=w, emit_rays_per_warp=rpw,
+                              side_sms=20 if (w + rpw) & 1 else 0)
             got = _march(hp, ctx, sc, batch, ss, img)
             _same(got, base, f"count {cg}, emit {w}x{rpw}", nsamp)
     assert ctx.check() == 0

@@ -399,7 +399,7 @@ __device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const Ray
         } else {
             occ = (__ldg(cg.bits + idx) >> k) & 1u;
         }
-        // DDA skip to the next cell boundary, in whole multiples of dt_min
+        // DDA skip to the next cell boundary: t_target / dt_min rounded up (to a float), times dt_min
         const float kc = __fmul_rn(cg.cell0, pow2i(k));
         const float tx = axis_dt(fx, hx, r.idx, kc);
         const float ty = axis_dt(fy, hy, r.idy, kc);
