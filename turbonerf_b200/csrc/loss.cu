@@ -21,6 +21,7 @@
 #include <thrust/reduce.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -66,52 +67,82 @@ struct CompFwd {
     uint32_t used; // samples composited (reference: loop index at the transmittance break + 1)
 };
 
+// ---- register-blocked compositor -----------------------------------------------------------
+// A ray is processed in blocks of 32 * K samples, lane l owning the K consecutive samples
+// [base + K l, base + K l + K). Each running sum along the ray is a prefix (or suffix) inside the
+// lane plus one warp scan of the 32 lane totals, so the warp scans once per 32 * K samples, not
+// once per 32: a few instructions per sample instead of one full warp scan per sample and sum.
+constexpr int CB_K = 4;
+
 // density_to_ray_rgba_forward, src/utils/training-kernels-fused.cuh:227-264, with
 // T_j = exp(-sum_{i<j} sigma_i dt_i) and alpha_j = -expm1(-sigma_j dt_j). Sample j is
 // composited while T_j >= min_t, i.e. up to and including the first sample after which
 // the transmittance drops below min_t.
+template <int K>
 __device__ CompFwd composite_forward_ray(const Samples& S, uint32_t o, uint32_t n, float min_t, int lane,
                                          float* __restrict__ t_out = nullptr, float* __restrict__ w_out = nullptr) {
-    float carry = 0.0f, t_prev = 1.0f;
+    float carry = 0.0f;  // optical depth before the current block
     float ar = 0.0f, ag = 0.0f, ab = 0.0f, aa = 0.0f;
     CompFwd out;
     out.used = n;
     out.depth = 0.0f;
     bool done = false;
-    for (uint32_t base = 0; base < n && !done; base += WARP) {
-        const uint32_t j = base + lane;
-        const bool valid = j < n;
-        float x = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
-        if (valid) {
-            const size_t s = (size_t)o + j;
-            x = act_sigma(S.act, S.density[s]) * S.dt[s];
-            cr = S.rgb[s];
-            cg = S.rgb[s + S.ss];
-            cb = S.rgb[s + 2 * (size_t)S.ss];
+    for (uint32_t base = 0; base < n && !done; base += WARP * K) {
+        const uint32_t j0 = base + (uint32_t)lane * K;
+        float x[K], cr[K], cg[K], cb[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            x[q] = cr[q] = cg[q] = cb[q] = 0.0f;
+            if (j0 + q < n) {
+                const size_t s = (size_t)o + j0 + q;
+                x[q] = act_sigma(S.act, S.density[s]) * S.dt[s];
+                cr[q] = S.rgb[s];
+                cg[q] = S.rgb[s + S.ss];
+                cb[q] = S.rgb[s + 2 * (size_t)S.ss];
+            }
         }
-        const float incl = warp_inclusive_sum(x, lane) + carry;
-        const float tn = expf(-incl);
-        const float tj = shift_up(tn, lane, t_prev);
-        const float w = tj * -expm1f(-x);
-        const unsigned term = __ballot_sync(FULL_MASK, valid && tn < min_t);
-        const int first = term ? __ffs(term) - 1 : WARP;
-        if (valid && lane <= first) {
-            ar += w * cr;
-            ag += w * cg;
-            ab += w * cb;
-            aa += w;
-            if (t_out) {
-                t_out[(size_t)o + j] = tn;  // transmittance after the sample
-                w_out[(size_t)o + j] = w;
+        float run = 0.0f, d[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            run += x[q];
+            d[q] = run;
+        }
+        const float lane_incl = warp_inclusive_sum(run, lane);
+        const float before = shift_up(lane_incl, lane, 0.0f) + carry;  // depth before the lane's first sample
+        float tprev = expf(-before), tn[K], w[K];
+        int fq = K;  // the lane's first sample after which T < min_t
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            d[q] += before;
+            tn[q] = expf(-d[q]);
+            w[q] = tprev * -expm1f(-x[q]);
+            if (fq == K && j0 + q < n && tn[q] < min_t) fq = q;
+            tprev = tn[q];
+        }
+        const unsigned term = __ballot_sync(FULL_MASK, fq < K);
+        const int fl = term ? __ffs(term) - 1 : WARP;
+        const int last_q = lane < fl ? K - 1 : (lane == fl ? fq : -1);
+        float dsel = 0.0f;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            if (q == fq) dsel = d[q];
+            if (q <= last_q && j0 + q < n) {
+                ar += w[q] * cr[q];
+                ag += w[q] * cg[q];
+                ab += w[q] * cb[q];
+                aa += w[q];
+                if (t_out) {
+                    t_out[(size_t)o + j0 + q] = tn[q];  // transmittance after the sample
+                    w_out[(size_t)o + j0 + q] = w[q];
+                }
             }
         }
         if (term) {
-            out.used = base + first + 1;
-            out.depth = __shfl_sync(FULL_MASK, incl, first);
+            out.used = base + (uint32_t)fl * K + (uint32_t)__shfl_sync(FULL_MASK, fq, fl) + 1u;
+            out.depth = __shfl_sync(FULL_MASK, dsel, fl);
             done = true;
         } else {
-            carry = __shfl_sync(FULL_MASK, incl, WARP - 1);
-            t_prev = __shfl_sync(FULL_MASK, tn, WARP - 1);
+            carry += __shfl_sync(FULL_MASK, lane_incl, WARP - 1);
         }
     }
     if (!done) out.depth = carry;
@@ -124,47 +155,81 @@ __device__ CompFwd composite_forward_ray(const Samples& S, uint32_t o, uint32_t 
 
 // Reverse-scan vector-Jacobian product of the compositor for one ray over samples
 // [0, used): dL/dsigma_j = dt_j * sum_c g_c (T_{j+1} c_j - sum_{i>j} w_i c_i)
-//                        + dt_j * g_a (T_{j+1} - sum_{i>j} w_i);   dL/dc_j = cscale * g_c * w_j.
-// The callback `emit(j, valid, dsigma_density, drgb_r, drgb_g, drgb_b, chunk_base)` consumes
-// each chunk's gradients (dsigma already multiplied by d sigma / d input).
-template <typename Emit>
-__device__ __forceinline__ void composite_vjp_chunk(const Samples& S, uint32_t o, uint32_t used, float depth,
-                                                    float gr, float gg, float gb, float ga, float cscale,
-                                                    uint32_t base, int lane, float& sx, float& sr, float& sg,
-                                                    float& sb, float& sa, Emit&& emit) {
-    const uint32_t j = base + lane;
-    const bool valid = j < used;
-    float x = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f, dtv = 0.0f, sigma = 0.0f;
-    if (valid) {
-        const size_t s = (size_t)o + j;
-        sigma = act_sigma(S.act, S.density[s]);
-        dtv = S.dt[s];
-        x = sigma * dtv;
-        cr = S.rgb[s];
-        cg = S.rgb[s + S.ss];
-        cb = S.rgb[s + 2 * (size_t)S.ss];
+//                        + dt_j * g_a (T_{j+1} - sum_{i>j} w_i);   dL/dc_j = cscale * g_c * w_j,
+// with T rebuilt from the forward's optical depth `depth` minus suffix sums of sigma dt.
+// The callback `emit(j, valid, dsigma_density, drgb_r, drgb_g, drgb_b)` consumes each sample's
+// gradients (dsigma already multiplied by d sigma / d input), blocks from the last one down.
+template <int K, typename Emit>
+__device__ __forceinline__ void composite_vjp_ray(const Samples& S, uint32_t o, uint32_t used, float depth, float gr,
+                                                  float gg, float gb, float ga, float cscale, int lane, Emit&& emit) {
+    if (used == 0) return;
+    float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;  // sums over the later blocks
+    const uint32_t span = WARP * K;
+    for (int64_t base = (int64_t)((used - 1) / span) * span; base >= 0; base -= span) {
+        const uint32_t j0 = (uint32_t)base + (uint32_t)lane * K;
+        float x[K], cr[K], cg[K], cb[K], dtv[K], sig[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            x[q] = cr[q] = cg[q] = cb[q] = dtv[q] = sig[q] = 0.0f;
+            if (j0 + q < used) {
+                const size_t s = (size_t)o + j0 + q;
+                sig[q] = act_sigma(S.act, S.density[s]);
+                dtv[q] = S.dt[s];
+                x[q] = sig[q] * dtv[q];
+                cr[q] = S.rgb[s];
+                cg[q] = S.rgb[s + S.ss];
+                cb[q] = S.rgb[s + 2 * (size_t)S.ss];
+            }
+        }
+        // suffix sums of x inside the lane, then over the later lanes and blocks
+        float xs[K], run = 0.0f;
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q) {
+            run += x[q];
+            xs[q] = run;
+        }
+        const float lx = warp_inclusive_suffix_sum(run, lane);
+        const float ax = shift_down(lx, lane, 0.0f) + sx;  // sum over the samples after the lane's block
+        float tn[K], w[K], wr[K], wg[K], wb[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const float xi = ax + xs[q];                             // sum_{i>=j} x_i
+            const float xe = ax + (q + 1 < K ? xs[q + 1] : 0.0f);    // sum_{i>j} x_i
+            const float tj = expf(-fmaxf(depth - xi, 0.0f));
+            tn[q] = expf(-fmaxf(depth - xe, 0.0f));
+            w[q] = j0 + q < used ? tj * -expm1f(-x[q]) : 0.0f;
+            wr[q] = w[q] * cr[q];
+            wg[q] = w[q] * cg[q];
+            wb[q] = w[q] * cb[q];
+        }
+        float rs[K], gs[K], bs[K], as[K], rr = 0.0f, rg = 0.0f, rb = 0.0f, ra = 0.0f;
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q) {
+            rr += wr[q]; rs[q] = rr;
+            rg += wg[q]; gs[q] = rg;
+            rb += wb[q]; bs[q] = rb;
+            ra += w[q]; as[q] = ra;
+        }
+        const float lr = warp_inclusive_suffix_sum(rr, lane), lg = warp_inclusive_suffix_sum(rg, lane);
+        const float lb = warp_inclusive_suffix_sum(rb, lane), la = warp_inclusive_suffix_sum(ra, lane);
+        const float a_r = shift_down(lr, lane, 0.0f) + sr, a_g = shift_down(lg, lane, 0.0f) + sg;
+        const float a_b = shift_down(lb, lane, 0.0f) + sb, a_a = shift_down(la, lane, 0.0f) + sa;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const bool next = q + 1 < K;
+            const float r_ex = a_r + (next ? rs[q + 1] : 0.0f), g_ex = a_g + (next ? gs[q + 1] : 0.0f);
+            const float b_ex = a_b + (next ? bs[q + 1] : 0.0f), a_ex = a_a + (next ? as[q + 1] : 0.0f);
+            const float ds = dtv[q] * (gr * (tn[q] * cr[q] - r_ex) + gg * (tn[q] * cg[q] - g_ex) +
+                                       gb * (tn[q] * cb[q] - b_ex) + ga * (tn[q] - a_ex));
+            emit(j0 + q, j0 + q < used, ds * act_dsigma(S.act, sig[q]), cscale * gr * w[q], cscale * gg * w[q],
+                 cscale * gb * w[q]);
+        }
+        sx += __shfl_sync(FULL_MASK, lx, 0);
+        sr += __shfl_sync(FULL_MASK, lr, 0);
+        sg += __shfl_sync(FULL_MASK, lg, 0);
+        sb += __shfl_sync(FULL_MASK, lb, 0);
+        sa += __shfl_sync(FULL_MASK, la, 0);
     }
-    const float xs_incl = warp_inclusive_suffix_sum(x, lane) + sx;  // sum_{i>=j} x_i
-    const float xs_excl = shift_down(xs_incl, lane, sx);             // sum_{i>j} x_i
-    const float tj = expf(-fmaxf(depth - xs_incl, 0.0f));
-    const float tn = expf(-fmaxf(depth - xs_excl, 0.0f));
-    const float w = valid ? tj * -expm1f(-x) : 0.0f;
-    const float wr = w * cr, wg = w * cg, wb = w * cb;
-    const float r_incl = warp_inclusive_suffix_sum(wr, lane) + sr;
-    const float g_incl = warp_inclusive_suffix_sum(wg, lane) + sg;
-    const float b_incl = warp_inclusive_suffix_sum(wb, lane) + sb;
-    const float a_incl = warp_inclusive_suffix_sum(w, lane) + sa;
-    const float r_ex = shift_down(r_incl, lane, sr);
-    const float g_ex = shift_down(g_incl, lane, sg);
-    const float b_ex = shift_down(b_incl, lane, sb);
-    const float a_ex = shift_down(a_incl, lane, sa);
-    const float ds = dtv * (gr * (tn * cr - r_ex) + gg * (tn * cg - g_ex) + gb * (tn * cb - b_ex) + ga * (tn - a_ex));
-    emit(j, valid, ds * act_dsigma(S.act, sigma), cscale * gr * w, cscale * gg * w, cscale * gb * w);
-    sx = __shfl_sync(FULL_MASK, xs_incl, 0);
-    sr = __shfl_sync(FULL_MASK, r_incl, 0);
-    sg = __shfl_sync(FULL_MASK, g_incl, 0);
-    sb = __shfl_sync(FULL_MASK, b_incl, 0);
-    sa = __shfl_sync(FULL_MASK, a_incl, 0);
 }
 
 __device__ __forceinline__ void zero_tail(float* __restrict__ dd, float* __restrict__ drgb, uint32_t ss, uint32_t o,
@@ -415,57 +480,353 @@ __device__ __forceinline__ uint32_t live_rays(uint32_t n_rays, const uint32_t* n
 }
 
 // ---- kernels ----------------------------------------------------------------------------
-__global__ void __launch_bounds__(LOSS_THREADS)
-composite_fwd_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
-                     const uint32_t* __restrict__ offsets, float min_t, float* __restrict__ rgba,
-                     float* __restrict__ depth, uint32_t* __restrict__ n_used, float* __restrict__ t_out,
-                     float* __restrict__ w_out) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t n_live = live_rays(n_rays, n_dev);
-    const uint32_t nw = gridDim.x * LOSS_WARPS;
-    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
-        const CompFwd c = composite_forward_ray(S, offsets[r], counts[r], min_t, lane, t_out, w_out);
-        if (lane == 0) {
-            rgba[r] = c.r; rgba[r + rs] = c.g; rgba[r + 2 * (size_t)rs] = c.b; rgba[r + 3 * (size_t)rs] = c.a;
-            if (depth) depth[r] = c.depth;
-            if (n_used) n_used[r] = c.used;
+// ---- sample tiles over several rays (the compositor's launch form) -------------------------
+// Each warp owns `rpw` consecutive rays, whose samples are one contiguous range (offsets are the
+// exclusive scan of the counts), and walks that range in tiles of 32 * K samples, lane l owning
+// the K consecutive samples [base + K l, base + K l + K). Short rays share a tile and long rays
+// span several; every running sum along a ray is a segmented sum: inside a lane, then one
+// segmented warp scan of the lane aggregates, then a carry into the next tile. The loads of a
+// tile are 32 * K consecutive samples whatever the ray lengths (16-byte vectors when the
+// batch's arrays allow: tiles then start at a multiple of 4), and the warp scans once per tile,
+// not once per ray or per 32 samples. The warp's ray table sits in shared memory; each lane
+// finds the ray of its first sample once per tile and steps to the next ray at ray ends.
+constexpr int ST_K = 4;
+
+// Last i < nr with off[i] <= s (rays without samples share their start with the next ray and
+// are passed over).
+__device__ __forceinline__ int find_ray(const uint32_t* off, int nr, uint32_t s) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const int mid = lo + step;
+        if (mid < nr && off[mid] <= s) lo = mid;
+    }
+    return lo;
+}
+
+// Inclusive segmented scans of N values over the lanes, in increasing (SUFFIX = false) or
+// decreasing (SUFFIX = true) lane order: a lane with `cut` set starts a new segment there.
+template <int N, bool SUFFIX>
+__device__ __forceinline__ void seg_scan(float (&v)[N], bool cut, int lane) {
+    unsigned f = cut ? 1u : 0u;
+#pragma unroll
+    for (int d = 1; d < WARP; d <<= 1) {
+        const unsigned fo = SUFFIX ? __shfl_down_sync(FULL_MASK, f, d) : __shfl_up_sync(FULL_MASK, f, d);
+        const bool in = SUFFIX ? lane + d < WARP : lane >= d;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const float vo = SUFFIX ? __shfl_down_sync(FULL_MASK, v[k], d) : __shfl_up_sync(FULL_MASK, v[k], d);
+            if (in && !f) v[k] += vo;
+        }
+        if (in) f |= fo;
+    }
+}
+
+// The K samples of a lane starting at s0: sigma dt and rgb (16-byte loads when VEC).
+template <int K, bool VEC>
+__device__ __forceinline__ void load_tile(const Samples& S, uint32_t s0, const bool (&in)[K], float (&sig)[K],
+                                          float (&dtv)[K], float (&cr)[K], float (&cg)[K], float (&cb)[K]) {
+    bool any_in = false;
+#pragma unroll
+    for (int q = 0; q < K; ++q) any_in = any_in || in[q];
+    if (VEC && K == 4 && !any_in) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) sig[q] = dtv[q] = cr[q] = cg[q] = cb[q] = 0.0f;
+    } else if (VEC && K == 4) {
+        // s0 is a multiple of 4 and one of its samples lies below sample_stride, itself a
+        // multiple of 4: the vector is in bounds
+        const float4 a = *reinterpret_cast<const float4*>(S.density + s0);
+        const float4 b = *reinterpret_cast<const float4*>(S.dt + s0);
+        const float4 r = *reinterpret_cast<const float4*>(S.rgb + s0);
+        const float4 g = *reinterpret_cast<const float4*>(S.rgb + S.ss + s0);
+        const float4 c = *reinterpret_cast<const float4*>(S.rgb + 2 * (size_t)S.ss + s0);
+        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w}, rv[4] = {r.x, r.y, r.z, r.w},
+                    gv[4] = {g.x, g.y, g.z, g.w}, cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            sig[q] = in[q] ? act_sigma(S.act, av[q]) : 0.0f;
+            dtv[q] = in[q] ? bv[q] : 0.0f;
+            cr[q] = in[q] ? rv[q] : 0.0f;
+            cg[q] = in[q] ? gv[q] : 0.0f;
+            cb[q] = in[q] ? cv[q] : 0.0f;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            sig[q] = dtv[q] = cr[q] = cg[q] = cb[q] = 0.0f;
+            if (in[q]) {
+                const size_t s = (size_t)s0 + q;
+                sig[q] = act_sigma(S.act, S.density[s]);
+                dtv[q] = S.dt[s];
+                cr[q] = S.rgb[s];
+                cg[q] = S.rgb[s + S.ss];
+                cb[q] = S.rgb[s + 2 * (size_t)S.ss];
+            }
         }
     }
 }
 
+// Compositor forward over the rays of each warp (semantics of composite_forward_ray).
+template <int K, bool VEC>
 __global__ void __launch_bounds__(LOSS_THREADS)
-composite_bwd_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
-                     const uint32_t* __restrict__ offsets, const float* __restrict__ depth,
-                     const uint32_t* __restrict__ n_used, const float* __restrict__ grad_rgba,
-                     float* __restrict__ dd, float* __restrict__ drgb) {
-    const int lane = threadIdx.x & 31;
+composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
+                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float min_t,
+                           float* __restrict__ rgba, float* __restrict__ depth, uint32_t* __restrict__ n_used,
+                           float* __restrict__ t_out, float* __restrict__ w_out) {
+    __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_end[LOSS_WARPS][WARP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_live = live_rays(n_rays, n_dev);
-    const uint32_t nw = gridDim.x * LOSS_WARPS;
-    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
-        const uint32_t o = offsets[r], n = counts[r];
-        const uint32_t used = min(n_used[r], n);
-        const float dep = depth[r];
-        const float gr = grad_rgba[r], gg = grad_rgba[r + rs], gb = grad_rgba[r + 2 * (size_t)rs],
-                    ga = grad_rgba[r + 3 * (size_t)rs];
-        zero_tail(dd, drgb, S.ss, o, used, n, lane);
-        float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
-        if (used == 0) continue;
-        for (int base = (int)(((used - 1) / WARP) * WARP); base >= 0; base -= WARP) {
-            composite_vjp_chunk(S, o, used, dep, gr, gg, gb, ga, 1.0f, (uint32_t)base, lane, sx, sr, sg, sb, sa,
-                                [&](uint32_t j, bool valid, float ds, float xr, float xg, float xb) {
-                                    if (!valid) return;
-                                    const size_t s = (size_t)o + j;
-                                    dd[s] = ds;
-                                    drgb[s] = xr;
-                                    drgb[s + S.ss] = xg;
-                                    drgb[s + 2 * (size_t)S.ss] = xb;
-                                });
+    const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
+    if (r0 >= n_live) return;  // whole warps leave together
+    const int nr = (int)min(rpw, n_live - r0);
+    if (lane < nr) {
+        const uint32_t o = offsets[r0 + lane], e = o + counts[r0 + lane];
+        t_off[wid][lane] = o;
+        t_end[wid][lane] = e;
+        if (e == o) {  // a ray without samples
+            const uint32_t r = r0 + lane;
+            rgba[r] = 0.0f; rgba[r + rs] = 0.0f; rgba[r + 2 * (size_t)rs] = 0.0f; rgba[r + 3 * (size_t)rs] = 0.0f;
+            if (depth) depth[r] = 0.0f;
+            if (n_used) n_used[r] = 0u;
         }
+    }
+    __syncwarp();
+    const uint32_t s_begin = t_off[wid][0], s_end = t_end[wid][nr - 1];
+    float cx = 0.0f, csum[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // running sums of the ray open at the tile start
+    for (uint32_t base = VEC ? (s_begin & ~3u) : s_begin; base < s_end; base += WARP * K) {
+        const uint32_t s0 = base + (uint32_t)lane * K;
+        bool in[K], head[K], last[K];
+        int ri[K];
+        uint32_t roff[K];
+        int cur = find_ray(t_off[wid], nr, s0 > s_begin ? s0 : s_begin);
+        uint32_t coff = t_off[wid][cur], cend = t_end[wid][cur];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t s = s0 + q;
+            in[q] = s >= s_begin && s < s_end;
+            while (in[q] && s >= cend) {  // the next ray with samples
+                ++cur;
+                coff = t_off[wid][cur];
+                cend = t_end[wid][cur];
+            }
+            ri[q] = cur;
+            roff[q] = coff;
+            head[q] = in[q] && s == coff;
+            last[q] = in[q] && s + 1 == cend;
+        }
+        float x[K], dtv[K], cr[K], cg[K], cb[K];
+        load_tile<K, VEC>(S, s0, in, x, dtv, cr, cg, cb);
+#pragma unroll
+        for (int q = 0; q < K; ++q) x[q] *= dtv[q];
+        // optical depth: the lane's open-segment aggregate, scanned, then per sample
+        bool any_head = false;
+        float agg[1] = {0.0f};
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            if (head[q]) { agg[0] = 0.0f; any_head = true; }
+            agg[0] += x[q];
+        }
+        if (lane == 0 && !any_head) agg[0] += cx;
+        seg_scan<1, false>(agg, any_head, lane);
+        float run = __shfl_up_sync(FULL_MASK, agg[0], 1);
+        if (lane == 0) run = cx;
+        float d[K], wv[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const float excl = head[q] ? 0.0f : run;
+            run = excl + x[q];
+            d[q] = run;
+            // sample j is composited while the transmittance before it is >= min_t
+            const float tb = expf(-excl), tn = expf(-run);
+            const bool comp = in[q] && (head[q] || tb >= min_t);
+            wv[q] = comp ? tb * -expm1f(-x[q]) : 0.0f;
+            if (comp && t_out) {
+                t_out[s0 + q] = tn;
+                w_out[s0 + q] = wv[q];
+            }
+            // a ray composites nothing after its terminating sample; a composited last sample that
+            // does not terminate means the ray never terminated
+            if (comp && (tn < min_t || last[q])) {
+                const uint32_t r = r0 + (uint32_t)ri[q];
+                if (depth) depth[r] = d[q];
+                if (n_used) n_used[r] = s0 + q - roff[q] + 1u;
+            }
+        }
+        // weighted colour and alpha sums per ray
+        float a4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            if (head[q]) a4[0] = a4[1] = a4[2] = a4[3] = 0.0f;
+            a4[0] += wv[q] * cr[q]; a4[1] += wv[q] * cg[q]; a4[2] += wv[q] * cb[q]; a4[3] += wv[q];
+        }
+        if (lane == 0 && !any_head) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a4[k] += csum[k];
+        }
+        seg_scan<4, false>(a4, any_head, lane);
+        float c4[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            c4[k] = __shfl_up_sync(FULL_MASK, a4[k], 1);
+            if (lane == 0) c4[k] = csum[k];
+        }
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            if (head[q]) c4[0] = c4[1] = c4[2] = c4[3] = 0.0f;
+            c4[0] += wv[q] * cr[q]; c4[1] += wv[q] * cg[q]; c4[2] += wv[q] * cb[q]; c4[3] += wv[q];
+            if (last[q]) {
+                const uint32_t r = r0 + (uint32_t)ri[q];
+                rgba[r] = c4[0]; rgba[r + rs] = c4[1]; rgba[r + 2 * (size_t)rs] = c4[2];
+                rgba[r + 3 * (size_t)rs] = c4[3];
+            }
+        }
+        // carries of the ray open at the end of the tile (lane 31 holds the tile's last samples)
+        cx = __shfl_sync(FULL_MASK, agg[0], WARP - 1);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) csum[k] = __shfl_sync(FULL_MASK, a4[k], WARP - 1);
+    }
+}
+
+// Compositor VJP over the rays of each warp (semantics of composite_vjp_ray): tiles from the end
+// of the warp's samples down; segmented suffix sums of x = sigma dt over [j, used) rebuild the
+// transmittance from each ray's forward depth, then suffix sums of w c and w. Samples of a ray
+// at or past its `used` get zero gradients.
+template <int K, bool VEC>
+__global__ void __launch_bounds__(LOSS_THREADS)
+composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
+                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                           const float* __restrict__ depth, const uint32_t* __restrict__ n_used,
+                           const float* __restrict__ grad_rgba, float* __restrict__ dd, float* __restrict__ drgb) {
+    __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_end[LOSS_WARPS][WARP], t_lim[LOSS_WARPS][WARP];
+    __shared__ float t_dep[LOSS_WARPS][WARP], t_g[LOSS_WARPS][4][WARP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
+    if (r0 >= n_live) return;
+    const int nr = (int)min(rpw, n_live - r0);
+    if (lane < nr) {
+        const uint32_t r = r0 + lane;
+        const uint32_t o = offsets[r], c = counts[r];
+        t_off[wid][lane] = o;
+        t_end[wid][lane] = o + c;
+        t_lim[wid][lane] = o + min(n_used[r], c);  // end of the composited samples
+        t_dep[wid][lane] = depth[r];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) t_g[wid][k][lane] = grad_rgba[r + k * (size_t)rs];
+    }
+    __syncwarp();
+    const uint32_t s_begin = t_off[wid][0], s_end = t_end[wid][nr - 1];
+    const uint32_t b0 = VEC ? (s_begin & ~3u) : s_begin;
+    const uint32_t span = WARP * K;
+    const uint32_t n_tiles = (s_end - b0 + span - 1) / span;
+    float cx = 0.0f, c4[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // suffix sums of the ray open at the tile end
+    for (int t = (int)n_tiles - 1; t >= 0; --t) {
+        const uint32_t s0 = b0 + (uint32_t)t * span + (uint32_t)lane * K;
+        bool in[K], valid[K], tail[K];
+        int ri[K];
+        int cur = find_ray(t_off[wid], nr, s0 > s_begin ? s0 : s_begin);
+        uint32_t cend = t_end[wid][cur], clim = t_lim[wid][cur];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t s = s0 + q;
+            in[q] = s >= s_begin && s < s_end;
+            while (in[q] && s >= cend) {
+                ++cur;
+                cend = t_end[wid][cur];
+                clim = t_lim[wid][cur];
+            }
+            ri[q] = cur;
+            valid[q] = in[q] && s < clim;
+            tail[q] = in[q] && s + 1 == cend;
+        }
+        float x[K], dtv[K], cr[K], cg[K], cb[K];
+        load_tile<K, VEC>(S, s0, valid, x, dtv, cr, cg, cb);
+        float sig[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            sig[q] = x[q];
+            x[q] *= dtv[q];
+        }
+        // suffix sums of x: the lane's aggregate is its samples up to its first ray end
+        bool any_tail = false;
+        float agg[1] = {0.0f};
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q) {
+            if (tail[q]) { agg[0] = 0.0f; any_tail = true; }
+            agg[0] += x[q];
+        }
+        if (lane == WARP - 1 && !any_tail) agg[0] += cx;
+        seg_scan<1, true>(agg, any_tail, lane);
+        float run = __shfl_down_sync(FULL_MASK, agg[0], 1);
+        if (lane == WARP - 1) run = cx;
+        float tn[K], wv[K];
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q) {
+            const float xe = tail[q] ? 0.0f : run;  // sum_{i>j} x_i within the ray
+            run = xe + x[q];                         // sum_{i>=j} x_i
+            const float dep = t_dep[wid][ri[q]];
+            const float tj = expf(-fmaxf(dep - run, 0.0f));
+            tn[q] = expf(-fmaxf(dep - xe, 0.0f));
+            wv[q] = valid[q] ? tj * -expm1f(-x[q]) : 0.0f;
+        }
+        float a4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q) {
+            if (tail[q]) a4[0] = a4[1] = a4[2] = a4[3] = 0.0f;
+            a4[0] += wv[q] * cr[q]; a4[1] += wv[q] * cg[q]; a4[2] += wv[q] * cb[q]; a4[3] += wv[q];
+        }
+        if (lane == WARP - 1 && !any_tail) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a4[k] += c4[k];
+        }
+        seg_scan<4, true>(a4, any_tail, lane);
+        float e4[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            e4[k] = __shfl_down_sync(FULL_MASK, a4[k], 1);
+            if (lane == WARP - 1) e4[k] = c4[k];
+        }
+        float o_d[K], o_r[K], o_g[K], o_b[K];
+#pragma unroll
+        for (int q = K - 1; q >= 0; --q) {
+            if (tail[q]) e4[0] = e4[1] = e4[2] = e4[3] = 0.0f;  // sums over i > j within the ray
+            const float g0 = t_g[wid][0][ri[q]], g1 = t_g[wid][1][ri[q]], g2 = t_g[wid][2][ri[q]],
+                        g3 = t_g[wid][3][ri[q]];
+            const float ds = dtv[q] * (g0 * (tn[q] * cr[q] - e4[0]) + g1 * (tn[q] * cg[q] - e4[1]) +
+                                       g2 * (tn[q] * cb[q] - e4[2]) + g3 * (tn[q] - e4[3]));
+            o_d[q] = valid[q] ? ds * act_dsigma(S.act, sig[q]) : 0.0f;
+            o_r[q] = g0 * wv[q];
+            o_g[q] = g1 * wv[q];
+            o_b[q] = g2 * wv[q];
+            e4[0] += wv[q] * cr[q]; e4[1] += wv[q] * cg[q]; e4[2] += wv[q] * cb[q]; e4[3] += wv[q];
+        }
+        bool all_in = true;
+#pragma unroll
+        for (int q = 0; q < K; ++q) all_in = all_in && in[q];
+        if (VEC && K == 4 && all_in) {
+            *reinterpret_cast<float4*>(dd + s0) = make_float4(o_d[0], o_d[1], o_d[2], o_d[3]);
+            *reinterpret_cast<float4*>(drgb + s0) = make_float4(o_r[0], o_r[1], o_r[2], o_r[3]);
+            *reinterpret_cast<float4*>(drgb + S.ss + s0) = make_float4(o_g[0], o_g[1], o_g[2], o_g[3]);
+            *reinterpret_cast<float4*>(drgb + 2 * (size_t)S.ss + s0) = make_float4(o_b[0], o_b[1], o_b[2], o_b[3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                if (!in[q]) continue;
+                const size_t s = (size_t)s0 + q;
+                dd[s] = o_d[q];
+                drgb[s] = o_r[q];
+                drgb[s + S.ss] = o_g[q];
+                drgb[s + 2 * (size_t)S.ss] = o_b[q];
+            }
+        }
+        cx = __shfl_sync(FULL_MASK, agg[0], 0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) c4[k] = __shfl_sync(FULL_MASK, a4[k], 0);
     }
 }
 
 // VJP of the compositor from the forward's stored per-sample transmittance (after the sample)
-// and weights, the alternative to recomputing them (composite_bwd_kernel): the same suffix
+// and weights, the alternative to recomputing them (composite_bwd_tiles_kernel): the same suffix
 // sums, read instead of rebuilt.
 __global__ void __launch_bounds__(LOSS_THREADS)
 composite_bwd_stored_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs,
@@ -524,7 +885,7 @@ recon_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, con
     float acc[1] = {0.0f};
     for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
         const uint32_t o = offsets[r], n = counts[r];
-        const CompFwd c = composite_forward_ray(S, o, n, min_t, lane);
+        const CompFwd c = composite_forward_ray<CB_K>(S, o, n, min_t, lane);
         const ReconGrad g = recon_loss_ray(c, target, bg, r, rs, inv_nrays);
         if (lane == 0) {
             if (ray_rgba) {
@@ -537,11 +898,8 @@ recon_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, con
             acc[0] += g.l[0] + g.l[1] + g.l[2] + g.l[3];
         }
         zero_tail(dd, drgb, S.ss, o, c.used, n, lane);
-        float sx = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
-        if (c.used == 0) continue;
-        for (int base = (int)(((c.used - 1) / WARP) * WARP); base >= 0; base -= WARP) {
-            composite_vjp_chunk(S, o, c.used, c.depth, g.gr, g.gg, g.gb, g.ga, grad_scale, (uint32_t)base, lane, sx, sr,
-                                sg, sb, sa, [&](uint32_t j, bool valid, float ds, float xr, float xg, float xb) {
+        composite_vjp_ray<CB_K>(S, o, c.used, c.depth, g.gr, g.gg, g.gb, g.ga, grad_scale, lane,
+                                [&](uint32_t j, bool valid, float ds, float xr, float xg, float xb) {
                                     if (!valid) return;
                                     const size_t s = (size_t)o + j;
                                     dd[s] = ds;
@@ -549,7 +907,6 @@ recon_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, con
                                     drgb[s + S.ss] = xg;
                                     drgb[s + 2 * (size_t)S.ss] = xb;
                                 });
-        }
     }
     if (loss_sum) block_sum_and_finish<1>(acc, partials, ticket, loss_sum, FinishScale{{inv_nrays, 0.0f}, nullptr, 0u, 0u});
 }
@@ -1383,6 +1740,29 @@ static int launch_train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_ba
     return check_launch("tn_train_losses");
 }
 
+// Rays per warp of the sample-tile compositor, from the batch's mean samples per ray
+// (sample_stride / n_rays, an upper bound): up to 4 tiles (32 * ST_K samples each) of samples per
+// warp while that leaves at least 32 warps per SM (the setup of a warp's range and its partly
+// filled first and last tiles are then paid once per 4 tiles), else 1 tile per warp.
+static uint32_t tile_rays_per_warp(const tn_ray_batch* b) {
+    const double mean = b->n_rays ? std::max(1.0, (double)b->sample_stride / (double)b->n_rays) : 1.0;
+    const double per_tile = (double)(WARP * ST_K);
+    const double fill = (double)b->sample_stride / (per_tile * num_sms() * 32.0);
+    const double tiles = std::min(4.0, std::max(1.0, std::floor(fill)));
+    return (uint32_t)std::min(32.0, std::max(1.0, std::floor(tiles * per_tile / mean)));
+}
+
+// 16-byte sample vectors: every per-sample array 16-byte aligned and the stride a multiple of 4.
+static bool tile_vec(const Samples& S, const void* a, const void* b) {
+    const uintptr_t m = (uintptr_t)S.density | (uintptr_t)S.rgb | (uintptr_t)S.dt | (uintptr_t)a | (uintptr_t)b;
+    return (m & 15u) == 0 && (S.ss & 3u) == 0;
+}
+
+static int tile_grid(uint32_t n_rays, uint32_t rpw) {
+    const uint32_t warps = (n_rays + rpw - 1) / rpw;
+    return (int)((warps + LOSS_WARPS - 1) / LOSS_WARPS);
+}
+
 static int check_batch(const tn_ray_batch* b) {
     TN_REQUIRE(b != nullptr, TN_E_NULL, "ray batch is NULL");
     TN_NONNULL(b->counts);
@@ -1407,10 +1787,15 @@ int tn_composite_fwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch,
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
-    const int grid = loss_grid((const void*)composite_fwd_kernel, batch->n_rays);
-    composite_fwd_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
-                                                            batch->counts, batch->offsets, min_transmittance, rgba,
-                                                            depth, n_used, nullptr, nullptr);
+    const uint32_t rpw = tile_rays_per_warp(batch);
+    if (tile_vec(S, nullptr, nullptr))
+        composite_fwd_tiles_kernel<ST_K, true><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
+            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
+            min_transmittance, rgba, depth, n_used, nullptr, nullptr);
+    else
+        composite_fwd_tiles_kernel<ST_K, false><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
+            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
+            min_transmittance, rgba, depth, n_used, nullptr, nullptr);
     return check_launch("tn_composite_fwd");
 }
 
@@ -1425,10 +1810,15 @@ int tn_composite_fwd_store(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* 
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
-    const int grid = loss_grid((const void*)composite_fwd_kernel, batch->n_rays);
-    composite_fwd_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
-                                                            batch->counts, batch->offsets, min_transmittance, rgba,
-                                                            nullptr, n_used, t_saved, w_saved);
+    const uint32_t rpw = tile_rays_per_warp(batch);
+    if (tile_vec(S, nullptr, nullptr))
+        composite_fwd_tiles_kernel<ST_K, true><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
+            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
+            min_transmittance, rgba, nullptr, n_used, t_saved, w_saved);
+    else
+        composite_fwd_tiles_kernel<ST_K, false><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
+            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
+            min_transmittance, rgba, nullptr, n_used, t_saved, w_saved);
     return check_launch("tn_composite_fwd_store");
 }
 
@@ -1462,10 +1852,15 @@ int tn_composite_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch,
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
-    const int grid = loss_grid((const void*)composite_bwd_kernel, batch->n_rays);
-    composite_bwd_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
-                                                            batch->counts, batch->offsets, depth, n_used, grad_rgba,
-                                                            dL_ddensity, dL_drgb);
+    const uint32_t rpw = tile_rays_per_warp(batch);
+    if (tile_vec(S, dL_ddensity, dL_drgb))
+        composite_bwd_tiles_kernel<ST_K, true><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
+            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets, depth, n_used,
+            grad_rgba, dL_ddensity, dL_drgb);
+    else
+        composite_bwd_tiles_kernel<ST_K, false><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
+            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets, depth, n_used,
+            grad_rgba, dL_ddensity, dL_drgb);
     return check_launch("tn_composite_bwd");
 }
 
