@@ -37,6 +37,22 @@ constexpr int SAVED_CHUNKS = 64;  // distortion chunk carries kept in registers 
 __device__ __forceinline__ float act_sigma(int act, float d) { return act == 0 ? d : expf(fminf(d, 12.0f) - 1.0f); }
 __device__ __forceinline__ float act_dsigma(int act, float sigma) { return act == 0 ? 1.0f : sigma; }
 
+// 1 - exp(-x) for x >= 0 (the opacity of a sample with optical depth x): below 1/4 the first
+// seven terms of its Taylor series, x (1 - x/2 (1 - x/3 (... (1 - x/7)))), whose truncation error
+// is below 2e-9 of the result; above, 1 - exp(-x), free of cancellation there.
+__device__ __forceinline__ float opacity(float x) {
+    if (x < 0.25f) {
+        float p = fmaf(-x, 1.0f / 7.0f, 1.0f);
+        p = fmaf(-x * (1.0f / 6.0f), p, 1.0f);
+        p = fmaf(-x * (1.0f / 5.0f), p, 1.0f);
+        p = fmaf(-x * (1.0f / 4.0f), p, 1.0f);
+        p = fmaf(-x * (1.0f / 3.0f), p, 1.0f);
+        p = fmaf(-x * 0.5f, p, 1.0f);
+        return x * p;
+    }
+    return 1.0f - expf(-x);
+}
+
 
 // Exclusive value from an inclusive warp scan: lane 0 gets `carry`.
 __device__ __forceinline__ float shift_up(float incl, int lane, float carry) {
@@ -522,33 +538,40 @@ __device__ __forceinline__ void seg_scan(float (&v)[N], bool cut, int lane) {
     }
 }
 
-// The K samples of a lane starting at s0: sigma dt and rgb (16-byte loads when VEC).
-template <int K, bool VEC>
+// The K samples of a lane starting at s0: sigma and dt and rgb (16-byte loads when VEC; K is then a
+// multiple of 4). Samples outside `in` read as zero.
+template <int K, bool VEC, int ACT>
 __device__ __forceinline__ void load_tile(const Samples& S, uint32_t s0, const bool (&in)[K], float (&sig)[K],
                                           float (&dtv)[K], float (&cr)[K], float (&cg)[K], float (&cb)[K]) {
-    bool any_in = false;
+    if (VEC) {
+        static_assert(!VEC || K % 4 == 0, "vector loads take 4 samples at a time");
 #pragma unroll
-    for (int q = 0; q < K; ++q) any_in = any_in || in[q];
-    if (VEC && K == 4 && !any_in) {
+        for (int v = 0; v < K / 4; ++v) {
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, r = a, g = a, c = a;
+            // sv is a multiple of 4; a vector holding an in-range sample (below sample_stride, itself
+            // a multiple of 4) ends at or before sample_stride
+            const uint32_t sv = s0 + 4u * v;
+            bool vin = false;
 #pragma unroll
-        for (int q = 0; q < K; ++q) sig[q] = dtv[q] = cr[q] = cg[q] = cb[q] = 0.0f;
-    } else if (VEC && K == 4) {
-        // s0 is a multiple of 4 and one of its samples lies below sample_stride, itself a
-        // multiple of 4: the vector is in bounds
-        const float4 a = *reinterpret_cast<const float4*>(S.density + s0);
-        const float4 b = *reinterpret_cast<const float4*>(S.dt + s0);
-        const float4 r = *reinterpret_cast<const float4*>(S.rgb + s0);
-        const float4 g = *reinterpret_cast<const float4*>(S.rgb + S.ss + s0);
-        const float4 c = *reinterpret_cast<const float4*>(S.rgb + 2 * (size_t)S.ss + s0);
-        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w}, rv[4] = {r.x, r.y, r.z, r.w},
-                    gv[4] = {g.x, g.y, g.z, g.w}, cv[4] = {c.x, c.y, c.z, c.w};
+            for (int k = 0; k < 4; ++k) vin = vin || in[4 * v + k];
+            if (vin) {
+                a = *reinterpret_cast<const float4*>(S.density + sv);
+                b = *reinterpret_cast<const float4*>(S.dt + sv);
+                r = *reinterpret_cast<const float4*>(S.rgb + sv);
+                g = *reinterpret_cast<const float4*>(S.rgb + S.ss + sv);
+                c = *reinterpret_cast<const float4*>(S.rgb + 2 * (size_t)S.ss + sv);
+            }
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w}, rv[4] = {r.x, r.y, r.z, r.w},
+                        gv[4] = {g.x, g.y, g.z, g.w}, cv[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
-        for (int q = 0; q < K; ++q) {
-            sig[q] = in[q] ? act_sigma(S.act, av[q]) : 0.0f;
-            dtv[q] = in[q] ? bv[q] : 0.0f;
-            cr[q] = in[q] ? rv[q] : 0.0f;
-            cg[q] = in[q] ? gv[q] : 0.0f;
-            cb[q] = in[q] ? cv[q] : 0.0f;
+            for (int k = 0; k < 4; ++k) {
+                const int q = 4 * v + k;
+                sig[q] = in[q] ? act_sigma(ACT, av[k]) : 0.0f;
+                dtv[q] = in[q] ? bv[k] : 0.0f;
+                cr[q] = in[q] ? rv[k] : 0.0f;
+                cg[q] = in[q] ? gv[k] : 0.0f;
+                cb[q] = in[q] ? cv[k] : 0.0f;
+            }
         }
     } else {
 #pragma unroll
@@ -556,7 +579,7 @@ __device__ __forceinline__ void load_tile(const Samples& S, uint32_t s0, const b
             sig[q] = dtv[q] = cr[q] = cg[q] = cb[q] = 0.0f;
             if (in[q]) {
                 const size_t s = (size_t)s0 + q;
-                sig[q] = act_sigma(S.act, S.density[s]);
+                sig[q] = act_sigma(ACT, S.density[s]);
                 dtv[q] = S.dt[s];
                 cr[q] = S.rgb[s];
                 cg[q] = S.rgb[s + S.ss];
@@ -566,11 +589,16 @@ __device__ __forceinline__ void load_tile(const Samples& S, uint32_t s0, const b
     }
 }
 
-// Compositor forward over the rays of each warp (semantics of composite_forward_ray).
-template <int K, bool VEC>
+// Compositor forward over the rays of each warp (density_to_ray_rgba_forward,
+// src/utils/training-kernels-fused.cuh:227-264). Termination is decided on the optical depth
+// d = sum sigma dt: sample j is composited while the depth before it is at most
+// depth_max = -ln(min_t) (transmittance >= min_t), and the first sample whose depth after it
+// exceeds depth_max is the last one composited. The weights use the transmittance as a product
+// of (1 - alpha) inside each lane from exp(-depth) at the lane's first sample.
+template <int K, bool VEC, int ACT, bool STORE>
 __global__ void __launch_bounds__(LOSS_THREADS)
 composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
-                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float min_t,
+                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float depth_max,
                            float* __restrict__ rgba, float* __restrict__ depth, uint32_t* __restrict__ n_used,
                            float* __restrict__ t_out, float* __restrict__ w_out) {
     __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_end[LOSS_WARPS][WARP];
@@ -615,7 +643,7 @@ composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
             last[q] = in[q] && s + 1 == cend;
         }
         float x[K], dtv[K], cr[K], cg[K], cb[K];
-        load_tile<K, VEC>(S, s0, in, x, dtv, cr, cg, cb);
+        load_tile<K, VEC, ACT>(S, s0, in, x, dtv, cr, cg, cb);
 #pragma unroll
         for (int q = 0; q < K; ++q) x[q] *= dtv[q];
         // optical depth: the lane's open-segment aggregate, scanned, then per sample
@@ -631,26 +659,29 @@ composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
         float run = __shfl_up_sync(FULL_MASK, agg[0], 1);
         if (lane == 0) run = cx;
         float d[K], wv[K];
+        float tb = expf(-run);  // transmittance before the lane's first sample
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             const float excl = head[q] ? 0.0f : run;
+            if (head[q]) tb = 1.0f;
             run = excl + x[q];
             d[q] = run;
-            // sample j is composited while the transmittance before it is >= min_t
-            const float tb = expf(-excl), tn = expf(-run);
-            const bool comp = in[q] && (head[q] || tb >= min_t);
-            wv[q] = comp ? tb * -expm1f(-x[q]) : 0.0f;
-            if (comp && t_out) {
+            const bool comp = in[q] && (head[q] || excl <= depth_max);
+            const float a = opacity(x[q]);
+            wv[q] = comp ? tb * a : 0.0f;
+            const float tn = fmaf(-tb, a, tb);  // transmittance after the sample
+            if (STORE && comp) {
                 t_out[s0 + q] = tn;
                 w_out[s0 + q] = wv[q];
             }
             // a ray composites nothing after its terminating sample; a composited last sample that
             // does not terminate means the ray never terminated
-            if (comp && (tn < min_t || last[q])) {
+            if (comp && (run > depth_max || last[q])) {
                 const uint32_t r = r0 + (uint32_t)ri[q];
                 if (depth) depth[r] = d[q];
                 if (n_used) n_used[r] = s0 + q - roff[q] + 1u;
             }
+            tb = tn;
         }
         // weighted colour and alpha sums per ray
         float a4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -691,7 +722,7 @@ composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
 // of the warp's samples down; segmented suffix sums of x = sigma dt over [j, used) rebuild the
 // transmittance from each ray's forward depth, then suffix sums of w c and w. Samples of a ray
 // at or past its `used` get zero gradients.
-template <int K, bool VEC>
+template <int K, bool VEC, int ACT>
 __global__ void __launch_bounds__(LOSS_THREADS)
 composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
@@ -740,7 +771,7 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
             tail[q] = in[q] && s + 1 == cend;
         }
         float x[K], dtv[K], cr[K], cg[K], cb[K];
-        load_tile<K, VEC>(S, s0, valid, x, dtv, cr, cg, cb);
+        load_tile<K, VEC, ACT>(S, s0, valid, x, dtv, cr, cg, cb);
         float sig[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) {
@@ -759,15 +790,22 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
         seg_scan<1, true>(agg, any_tail, lane);
         float run = __shfl_down_sync(FULL_MASK, agg[0], 1);
         if (lane == WARP - 1) run = cx;
-        float tn[K], wv[K];
+        // transmittance after (tn) and before (tj) each sample; inside a ray the one before sample
+        // q is the one after sample q - 1, from the same suffix sum
+        float tn[K], wv[K], xi[K], dep[K];
 #pragma unroll
         for (int q = K - 1; q >= 0; --q) {
             const float xe = tail[q] ? 0.0f : run;  // sum_{i>j} x_i within the ray
             run = xe + x[q];                         // sum_{i>=j} x_i
-            const float dep = t_dep[wid][ri[q]];
-            const float tj = expf(-fmaxf(dep - run, 0.0f));
-            tn[q] = expf(-fmaxf(dep - xe, 0.0f));
-            wv[q] = valid[q] ? tj * -expm1f(-x[q]) : 0.0f;
+            xi[q] = run;
+            dep[q] = t_dep[wid][ri[q]];
+            tn[q] = expf(-fmaxf(dep[q] - xe, 0.0f));
+        }
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const float tj = (q > 0 && ri[q] == ri[q - 1]) ? tn[q > 0 ? q - 1 : 0]
+                                                           : expf(-fmaxf(dep[q] - xi[q], 0.0f));
+            wv[q] = valid[q] ? tj * opacity(x[q]) : 0.0f;
         }
         float a4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
@@ -794,29 +832,36 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
                         g3 = t_g[wid][3][ri[q]];
             const float ds = dtv[q] * (g0 * (tn[q] * cr[q] - e4[0]) + g1 * (tn[q] * cg[q] - e4[1]) +
                                        g2 * (tn[q] * cb[q] - e4[2]) + g3 * (tn[q] - e4[3]));
-            o_d[q] = valid[q] ? ds * act_dsigma(S.act, sig[q]) : 0.0f;
+            o_d[q] = valid[q] ? ds * act_dsigma(ACT, sig[q]) : 0.0f;
             o_r[q] = g0 * wv[q];
             o_g[q] = g1 * wv[q];
             o_b[q] = g2 * wv[q];
             e4[0] += wv[q] * cr[q]; e4[1] += wv[q] * cg[q]; e4[2] += wv[q] * cb[q]; e4[3] += wv[q];
         }
-        bool all_in = true;
 #pragma unroll
-        for (int q = 0; q < K; ++q) all_in = all_in && in[q];
-        if (VEC && K == 4 && all_in) {
-            *reinterpret_cast<float4*>(dd + s0) = make_float4(o_d[0], o_d[1], o_d[2], o_d[3]);
-            *reinterpret_cast<float4*>(drgb + s0) = make_float4(o_r[0], o_r[1], o_r[2], o_r[3]);
-            *reinterpret_cast<float4*>(drgb + S.ss + s0) = make_float4(o_g[0], o_g[1], o_g[2], o_g[3]);
-            *reinterpret_cast<float4*>(drgb + 2 * (size_t)S.ss + s0) = make_float4(o_b[0], o_b[1], o_b[2], o_b[3]);
-        } else {
+        for (int v = 0; v < K / 4; ++v) {
+            bool all_in = true;
 #pragma unroll
-            for (int q = 0; q < K; ++q) {
-                if (!in[q]) continue;
-                const size_t s = (size_t)s0 + q;
-                dd[s] = o_d[q];
-                drgb[s] = o_r[q];
-                drgb[s + S.ss] = o_g[q];
-                drgb[s + 2 * (size_t)S.ss] = o_b[q];
+            for (int k = 0; k < 4; ++k) all_in = all_in && in[4 * v + k];
+            const uint32_t sv = s0 + 4u * v;
+            if (VEC && all_in) {
+                *reinterpret_cast<float4*>(dd + sv) = make_float4(o_d[4 * v], o_d[4 * v + 1], o_d[4 * v + 2], o_d[4 * v + 3]);
+                *reinterpret_cast<float4*>(drgb + sv) = make_float4(o_r[4 * v], o_r[4 * v + 1], o_r[4 * v + 2], o_r[4 * v + 3]);
+                *reinterpret_cast<float4*>(drgb + S.ss + sv) =
+                    make_float4(o_g[4 * v], o_g[4 * v + 1], o_g[4 * v + 2], o_g[4 * v + 3]);
+                *reinterpret_cast<float4*>(drgb + 2 * (size_t)S.ss + sv) =
+                    make_float4(o_b[4 * v], o_b[4 * v + 1], o_b[4 * v + 2], o_b[4 * v + 3]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int q = 4 * v + k;
+                    if (!in[q]) continue;
+                    const size_t s = (size_t)s0 + q;
+                    dd[s] = o_d[q];
+                    drgb[s] = o_r[q];
+                    drgb[s + S.ss] = o_g[q];
+                    drgb[s + 2 * (size_t)S.ss] = o_b[q];
+                }
             }
         }
         cx = __shfl_sync(FULL_MASK, agg[0], 0);
@@ -1763,6 +1808,51 @@ static int tile_grid(uint32_t n_rays, uint32_t rpw) {
     return (int)((warps + LOSS_WARPS - 1) / LOSS_WARPS);
 }
 
+// Launch of the compositor forward tiles, specialised on the vector loads, the activation and
+// whether per-sample transmittance and weights are stored. depth_max = -ln(min_transmittance).
+static void launch_composite_fwd_tiles(cudaStream_t stream, const tn_ray_batch* b, const Samples& S, float min_t,
+                                       float* rgba, float* depth, uint32_t* n_used, float* t_out, float* w_out) {
+    const uint32_t rpw = tile_rays_per_warp(b);
+    const int grid = tile_grid(b->n_rays, rpw);
+    const float depth_max = min_t > 0.0f ? -logf(min_t) : INFINITY;
+    const bool vec = tile_vec(S, t_out, w_out), store = t_out != nullptr;
+#define TN_FWD_TILES(V, A, ST)                                                                                  \
+    composite_fwd_tiles_kernel<ST_K, V, A, ST><<<grid, LOSS_THREADS, 0, stream>>>(                              \
+        S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth_max, rgba, depth, n_used,  \
+        t_out, w_out)
+    const int key = (vec ? 4 : 0) | (S.act ? 2 : 0) | (store ? 1 : 0);
+    switch (key) {
+        case 0: TN_FWD_TILES(false, 0, false); break;
+        case 1: TN_FWD_TILES(false, 0, true); break;
+        case 2: TN_FWD_TILES(false, 1, false); break;
+        case 3: TN_FWD_TILES(false, 1, true); break;
+        case 4: TN_FWD_TILES(true, 0, false); break;
+        case 5: TN_FWD_TILES(true, 0, true); break;
+        case 6: TN_FWD_TILES(true, 1, false); break;
+        default: TN_FWD_TILES(true, 1, true); break;
+    }
+#undef TN_FWD_TILES
+}
+
+static void launch_composite_bwd_tiles(cudaStream_t stream, const tn_ray_batch* b, const Samples& S,
+                                       const float* depth, const uint32_t* n_used, const float* grad_rgba, float* dd,
+                                       float* drgb) {
+    const uint32_t rpw = tile_rays_per_warp(b);
+    const int grid = tile_grid(b->n_rays, rpw);
+    const bool vec = tile_vec(S, dd, drgb);
+#define TN_BWD_TILES(V, A)                                                                                      \
+    composite_bwd_tiles_kernel<ST_K, V, A><<<grid, LOSS_THREADS, 0, stream>>>(                                  \
+        S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth, n_used, grad_rgba, dd, drgb)
+    const int key = (vec ? 2 : 0) | (S.act ? 1 : 0);
+    switch (key) {
+        case 0: TN_BWD_TILES(false, 0); break;
+        case 1: TN_BWD_TILES(false, 1); break;
+        case 2: TN_BWD_TILES(true, 0); break;
+        default: TN_BWD_TILES(true, 1); break;
+    }
+#undef TN_BWD_TILES
+}
+
 static int check_batch(const tn_ray_batch* b) {
     TN_REQUIRE(b != nullptr, TN_E_NULL, "ray batch is NULL");
     TN_NONNULL(b->counts);
@@ -1787,15 +1877,7 @@ int tn_composite_fwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch,
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
-    const uint32_t rpw = tile_rays_per_warp(batch);
-    if (tile_vec(S, nullptr, nullptr))
-        composite_fwd_tiles_kernel<ST_K, true><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
-            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
-            min_transmittance, rgba, depth, n_used, nullptr, nullptr);
-    else
-        composite_fwd_tiles_kernel<ST_K, false><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
-            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
-            min_transmittance, rgba, depth, n_used, nullptr, nullptr);
+    launch_composite_fwd_tiles(stream, batch, S, min_transmittance, rgba, depth, n_used, nullptr, nullptr);
     return check_launch("tn_composite_fwd");
 }
 
@@ -1810,15 +1892,7 @@ int tn_composite_fwd_store(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* 
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
-    const uint32_t rpw = tile_rays_per_warp(batch);
-    if (tile_vec(S, nullptr, nullptr))
-        composite_fwd_tiles_kernel<ST_K, true><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
-            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
-            min_transmittance, rgba, nullptr, n_used, t_saved, w_saved);
-    else
-        composite_fwd_tiles_kernel<ST_K, false><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
-            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets,
-            min_transmittance, rgba, nullptr, n_used, t_saved, w_saved);
+    launch_composite_fwd_tiles(stream, batch, S, min_transmittance, rgba, nullptr, n_used, t_saved, w_saved);
     return check_launch("tn_composite_fwd_store");
 }
 
@@ -1852,15 +1926,7 @@ int tn_composite_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch,
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, rgb, dt, nullptr, nullptr, nullptr, batch->sample_stride, activation};
-    const uint32_t rpw = tile_rays_per_warp(batch);
-    if (tile_vec(S, dL_ddensity, dL_drgb))
-        composite_bwd_tiles_kernel<ST_K, true><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
-            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets, depth, n_used,
-            grad_rgba, dL_ddensity, dL_drgb);
-    else
-        composite_bwd_tiles_kernel<ST_K, false><<<tile_grid(batch->n_rays, rpw), LOSS_THREADS, 0, stream>>>(
-            S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, rpw, batch->counts, batch->offsets, depth, n_used,
-            grad_rgba, dL_ddensity, dL_drgb);
+    launch_composite_bwd_tiles(stream, batch, S, depth, n_used, grad_rgba, dL_ddensity, dL_drgb);
     return check_launch("tn_composite_bwd");
 }
 
