@@ -648,6 +648,95 @@ def run_multi_scene(args):
     print(json.dumps(out), flush=True)
 
 
+def run_kernel_tour(args):
+    """Every kernel of the library, launched at representative sizes, for profiling (for instance
+    `ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum`, one pass per
+    launch): the fused and plain train steps of the train-step workload (graph replay, stage
+    timing, the full occupancy update), the compositor, distortion and fused losses on 2^22
+    samples (65,571 rays, truncated geometric counts, mean 64), the march, scan and compaction
+    entry points on 2^14 rays of the 5-cascade scene, and the batched multi-scene march of six
+    small scenes. About 1.2 GB of device memory. Prints what ran."""
+    import torch
+    from turbonerf_b200 import hotpath as hp, native, scenes
+
+    torch.cuda.set_device(0)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ran = []
+    # training steps
+    scene = _scene(0x7B0)
+    tr = _trainer(scene, "fused", 0x7B0)
+    for _ in range(3):
+        tr.train_step()
+    tr.profile_step()
+    tr.update_occupancy_grid(300)
+    tr.flush()
+    ran.append("fused train steps (eager, graph capture and replay, stage timing, full occupancy update)")
+    del tr
+    trp = _trainer(scene, "plain", 0x7B0)
+    trp.train_step()
+    ran.append("plain train step")
+    del trp
+    # compositor and losses
+    sb = scenes.make_sample_batch(0x7B5, 1 << 22, mean=64.0, max_count=1024)
+    n, ss = sb.n_rays, sb.n_samples
+    counts, offsets = d(sb.counts.view(np.int32)), d(sb.offsets.view(np.int32))
+    sig, rgb, dt, mn, dtn, t = (d(a) for a in (sb.sigma, sb.rgb, sb.dt, sb.m_norm, sb.dt_norm, sb.t))
+    tgt, bg = d(sb.target_rgba), d(sb.bg_rgb)
+    rb = hp.ray_batch(counts, offsets, n, n, ss)
+    ctx = hp.Context(n, ss)
+    g_rgba = torch.full((4 * n,), 1e-3, device="cuda")
+    fo = hp.composite_fwd(ctx, rb, sig, rgb, dt)
+    hp.composite_bwd(ctx, rb, sig, rgb, dt, fo["depth"], fo["n_used"], g_rgba)
+    st = hp.composite_fwd_store(ctx, rb, sig, rgb, dt)
+    hp.composite_bwd_stored(ctx, rb, sig, rgb, dt, st["n_used"], st["t_saved"], st["w_saved"], g_rgba)
+    hp.recon_loss_fwd_bwd(ctx, rb, sig, rgb, dt, tgt, bg, 1.0 / n)
+    hp.distortion_fwd_bwd(ctx, rb, sig, mn, dtn, 1e-3)
+    gd = torch.zeros(ss, device="cuda")
+    hp.train_losses(ctx, rb, sig, rgb, dt, mn, dtn, t, tgt, bg, gd, inv_nrays=1.0 / n, lam=1e-3)
+    hp.grad_epilogue(ss, 1.0, gd, gd, t, torch.zeros(ss, device="cuda"))
+    ran.append(f"compositor, distortion and fused losses on {ss} samples / {n} rays")
+    rbs = hp.ray_batch(counts[:4096].contiguous(), offsets[:4096].contiguous(), 4096, 4096, ss)
+    hp.plain_recon_loss(rbs, sig, rgb, dt, tgt, bg, 1.0 / 4096)
+    hp.plain_distortion(rbs, sig, mn, dtn, 1e-3)
+    hp.plain_grad_epilogue(ss, 1.0, gd, gd, t, torch.zeros(ss, device="cuda"))
+    ran.append("plain compositor and distortion on the first 4096 rays")
+    del sig, rgb, dt, mn, dtn, t, gd, fo, st
+    # march, scan, compaction
+    sc = scenes.march_scene_cascaded(seed=0x7B0, n_rays=RAYS, n_levels=5)
+    r = sc.rays
+    ori, dr = d(r.ori), d(r.dir)
+    hp.rays_init_bbox(ori, dr, RAYS, RAYS, sc.bbox, t_far=3.0e38)
+    g = hp.GridSpec(sc.grid.n_levels, sc.grid.resolution, sc.grid.base_size)
+    m = hp.MarchSpec(sc.cone_angle, sc.dt_min, sc.dt_max, 0)
+    bits = d(sc.grid.bitfield)
+    t0, tm, al = d(r.t), d(r.t_max), d(r.alive)
+    mctx = hp.Context(RAYS, BATCH)
+    ns, info = hp.march_count(mctx, g, bits, sc.bbox, m, RAYS, RAYS, ori, dr, t0, tm, al, BATCH)
+    hp.march_emit(mctx, g, bits, sc.bbox, m, 1.0 / sc.aabb_size, RAYS, RAYS, BATCH + 64, info, ori, dr, t0, al, ns)
+    hp.plain_march_count(g, bits, sc.bbox, m, RAYS, RAYS, ori, dr, t0, tm, al.clone())
+    hp.scan_offsets(mctx, ns, BATCH)
+    hp.compact_nonzero(mctx, ns)
+    hp.popcount(mctx, bits)
+    off_na, info_na = torch.zeros(RAYS, dtype=torch.int32, device="cuda"), torch.zeros(4, dtype=torch.int32, device="cuda")
+    native.call("tn_scan_offsets_noalloc", hp._stream(), RAYS, hp._ptr(ns), hp._ptr(off_na), BATCH, hp._ptr(info_na))
+    ran.append(f"box clip, march count and emit, plain march count, scans, compaction, popcount on {RAYS} rays")
+    # batched multi-scene march
+    params = scenes.multi_scene_params(seed=0x7C1, n_scenes=6, ray_lo=64, ray_hi=2048)
+    ms = scenes.make_multi_scene(params, resolution=32)
+    rows = [dict(grid=hp.GridSpec(s_.grid.n_levels, s_.grid.resolution, s_.grid.base_size), bitfield=d(s_.grid.bitfield),
+                 bbox=s_.bbox, march=hp.MarchSpec(s_.cone_angle, s_.dt_min, s_.dt_max, s_.max_steps),
+                 inv_aabb=1.0 / s_.aabb_size, ray_begin=int(b), n_rays=s_.rays.n) for s_, b in zip(ms.scenes, ms.ray_begin)]
+    table = hp.scene_table(rows)
+    mr = ms.rays
+    mo, mdr, mt, mtm, mal = d(mr.ori), d(mr.dir), d(mr.t), d(mr.t_max), d(mr.alive)
+    n_steps, _, minfo = hp.multi_march_count(mctx, table, mr.n, mo, mdr, mt, mtm, mal)
+    hp.multi_march_emit(mctx, table, mr.n, int(minfo[1].item()) + 64, mo, mdr, mt, mal, n_steps)
+    ran.append(f"multi-scene march count and emit: {len(rows)} scenes, {mr.n} rays")
+    torch.cuda.synchronize()
+    assert ctx.check() == 0 and mctx.check() == 0
+    print(json.dumps({"workload": "kernel tour", "ran": ran, "data": "synthetic"}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -658,14 +747,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="train-step", choices=["train-step", "backward-memory", "multi-scene"],
+    ap.add_argument("--workload", default="train-step", choices=["train-step", "backward-memory", "multi-scene", "kernel-tour"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "
-                         "multi-scene: the batched persistent march of 16 scenes against one launch per scene")
+                         "multi-scene: the batched persistent march of 16 scenes against one launch per scene; "
+                         "kernel-tour: every kernel once at representative sizes, for profiling")
     args = ap.parse_args()
     if args.workload == "backward-memory":
         run_backward_memory(args)
     elif args.workload == "multi-scene":
         run_multi_scene(args)
+    elif args.workload == "kernel-tour":
+        run_kernel_tour(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
