@@ -194,6 +194,54 @@ STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "net
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass, after the warm-up steps).
 NCU_TRAFFIC = {"march_count": 1_007_616, "march_emit": 1_285_376, "losses": 9_637_888, "adam": 304_766_208,
                "occupancy": 50_338_304}
+# The same for the compositor tile kernels on the 2^22-sample batch (kernel tour capture).
+NCU_TRAFFIC_COMPOSITE = {"composite_fwd_tiles": 87_174_144, "composite_bwd_tiles": 114_450_688}
+
+
+def compositor_rooflines(peak, reps=20):
+    """Roofline of the compositor's tile kernels (forward, VJP) on the compositor workload at 2^22
+    samples (truncated geometric counts, mean 64, at most 1024: 65,571 rays): the L2 (126 MB) is
+    flushed before every timed launch (a 256 MB write outside the events), each launch timed with
+    CUDA events, the mean kept. Algorithmic bytes: forward 20 B/sample + 32 B/ray, VJP 36 B/sample
+    + 24 B/ray."""
+    import torch
+    from turbonerf_b200 import hotpath as hp, scenes
+    sb = scenes.make_sample_batch(0x7B5, 1 << 22, mean=64.0, max_count=1024)
+    n, ss = sb.n_rays, sb.n_samples
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    counts, offsets = d(sb.counts.view(np.int32)), d(sb.offsets.view(np.int32))
+    sig, rgb, dt = d(sb.sigma), d(sb.rgb), d(sb.dt)
+    rb = hp.ray_batch(counts, offsets, n, n, ss)
+    ctx = hp.Context(n, ss)
+    g_rgba = torch.full((4 * n,), 1e-3, device="cuda")
+    fo = hp.composite_fwd(ctx, rb, sig, rgb, dt)
+    bo = hp.composite_bwd(ctx, rb, sig, rgb, dt, fo["depth"], fo["n_used"], g_rgba)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    kernels = {
+        "composite_fwd_tiles": (lambda: hp.composite_fwd(ctx, rb, sig, rgb, dt, out=fo), 20 * ss + 32 * n),
+        "composite_bwd_tiles": (lambda: hp.composite_bwd(ctx, rb, sig, rgb, dt, fo["depth"], fo["n_used"], g_rgba,
+                                                         out=bo), 36 * ss + 24 * n),
+    }
+    out = []
+    for name, (fn, alg) in kernels.items():
+        for _ in range(3):
+            fn()
+        total = 0.0
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        ms = total / reps
+        gbs = alg / (ms * 1e-3) / 1e9
+        out.append({"kernel": name, "workload": f"compositor, 2^22 samples over {n} rays (mean 64), L2 flushed",
+                    "bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 4),
+                    "traffic": NCU_TRAFFIC_COMPOSITE[name], "alg_bytes": int(alg), "ms": round(ms, 4)})
+    assert ctx.check() == 0
+    return out
 
 
 def run_ours(args):
@@ -270,7 +318,8 @@ def run_ours(args):
                     "traffic": NCU_TRAFFIC.get(dom), "peak_source": peak_kind}
         result = dict(value=value, ms=ms_max, samples=samples, rays=rays_used, kernels=kernels_per_step,
                       clocks=clk.summary(), stages=stages, roofline=roofline, n_touched=tr.n_touched_grads,
-                      last=dict(n_rays=m.n_rays, n_samples=m.n_samples, loss=m.loss))
+                      last=dict(n_rays=m.n_rays, n_samples=m.n_samples, loss=m.loss),
+                      rooflines=compositor_rooflines(peak))
 
     # e2e: public API with host rays (pinned) copied in and metrics read back every step
     from turbonerf_b200 import scenes
@@ -348,6 +397,7 @@ def run_ours(args):
         "e2e": {"value": round(e2e_value, 1), "unit": "samples/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": 76},
         "gpu_launches": int(result["kernels"]) * args.steps,
         "roofline": result["roofline"],
+        "rooflines": result["rooflines"],
         "stages": result["stages"],
         "clocks": result["clocks"],
         "plain": plain,

@@ -349,11 +349,15 @@ def composite_fwd(ctx, rb: RayBatchDesc, density, rgb, dt, activation=0, min_t=1
     return out
 
 
-def composite_bwd(ctx, rb: RayBatchDesc, density, rgb, dt, depth, n_used, grad_rgba, activation=0):
+def composite_bwd(ctx, rb: RayBatchDesc, density, rgb, dt, depth, n_used, grad_rgba, activation=0, out=None):
+    """Compositor VJP. Returns (dL/d density, dL/d rgb); `out` = (dd, drgb) reuses buffers."""
     dev = density.device
     ss = rb.sample_stride
-    dd = torch.zeros(ss, dtype=torch.float32, device=dev)
-    drgb = torch.zeros(3 * ss, dtype=torch.float32, device=dev)
+    if out is None:
+        dd = torch.zeros(ss, dtype=torch.float32, device=dev)
+        drgb = torch.zeros(3 * ss, dtype=torch.float32, device=dev)
+    else:
+        dd, drgb = out
     call("tn_composite_bwd", ctx.handle, _stream(), ctypes.byref(rb), activation, _ptr(density), _ptr(rgb), _ptr(dt),
          _ptr(depth), _ptr(n_used), _ptr(grad_rgba), _ptr(dd), _ptr(drgb))
     return dd, drgb
