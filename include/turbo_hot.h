@@ -446,6 +446,47 @@ typedef struct tn_network {
                    const float* pos, float* density);
 } tn_network;
 
+/* ---- renderer: inference images of one NeRF ---------------------------------------
+ * Reference Renderer::submit / perform_task (src/core/renderer.cu:172-646) for one NeRF
+ * with an identity transform, through the linear ray batch
+ * (src/rendering/ray-batch-coordinators/linear-buffer-ray-batch-coordinator.cu). */
+
+/* Pinhole camera (reference Camera, src/models/camera.cuh:34-137; lens distortion is not
+ * part of this surface). transform: camera to world, row-major 3 x 4 [R | t]. */
+typedef struct tn_camera {
+    int32_t width, height;
+    float near, far;                 /* ray origins at `near`, t_max = far - near */
+    float focal_x, focal_y;          /* pixels */
+    float principal_x, principal_y;  /* pixels */
+    float shift_x, shift_y;          /* fractions of the resolution */
+    float transform[12];
+} tn_camera;
+
+typedef struct tn_render_desc {
+    tn_grid_desc grid;
+    const uint8_t* bitfield;         /* device, as tn_march_count */
+    tn_bbox render_bbox;             /* samples outside it are skipped */
+    tn_bbox training_bbox;           /* network positions = (p - min) / (max - min) */
+    float dt_min;                    /* reference min_step_size; dt_max = 8 dt_min */
+    float cone_angle;                /* reference NeRFConstants::cone_angle */
+    float min_transmittance;         /* reference NeRFConstants::min_transmittance = 1e-4 */
+    uint32_t batch_size;             /* samples per iteration; 0 selects 1 << 20 */
+} tn_render_desc;
+
+typedef struct tn_render_stats {
+    uint32_t rays_hit;    /* pixels whose ray meets the render box */
+    uint32_t iterations;  /* march/network/composite rounds */
+    uint64_t samples;     /* samples sent to the network */
+    uint64_t steps;       /* march steps taken */
+} tn_render_stats;
+
+/* Renders camera->width x camera->height pixels into out_rgba (device, interleaved
+ * premultiplied RGBA, pixel i at out_rgba[4 i .. 4 i + 3]; pixels whose ray misses the
+ * box are 0). Queries net->forward on packed valid samples. Synchronous: it reads the live
+ * ray count back after every round, so not during stream capture. stats may be NULL. */
+int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const tn_camera* camera,
+              const tn_network* net, float* out_rgba, tn_render_stats* stats);
+
 typedef struct tn_trainer_desc {
     tn_grid_desc grid;
     tn_bbox bbox;                       /* training box; aabb size = max_x - min_x */
@@ -533,6 +574,13 @@ int tn_trainer_flush(tn_trainer* tr);
  * capture its graph again. */
 int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out);
 int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t);
+/* Renders the trainer's scene (its grid, training box, cone angle, transmittance cut and
+ * network) with tn_render (reference NeRFRenderingController::submit,
+ * src/controllers/nerf-rendering-controller.cu:50). render_bbox NULL selects the training
+ * box; min_step_size <= 0 the trainer's; batch_size 0 the renderer default (1 << 20).
+ * Applies a pending Adam update first. */
+int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,
+                      uint32_t batch_size, float* out_rgba, tn_render_stats* stats);
 /* 0/1: kernel nodes in the captured step graph (synthetic / caller rays), 2: graph nodes,
  * 3: samples processed so far, 4: rays used so far, 5: steps (3-5 synchronise). */
 int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out);

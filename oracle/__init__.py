@@ -76,6 +76,8 @@ def _declare(L):
         "orc_popcount": (ctypes.c_uint64, [i64, vp]),
         "orc_adam_step": (None, [i64, i64, i64, f64, f64, f64, f64, f64, f64, vp, vp, vp, vp, vp, vp]),
         "orc_blob_field": (None, [i64, i64, vp, f32, i32, vp, vp, vp, vp, i64]),
+        "orc_render": (i64, [vp, ctypes.POINTER(Bbox), ctypes.POINTER(Bbox), i32, i32, f32, vp, f32, f32, f64, i32,
+                             vp, vp, f32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -289,3 +291,34 @@ def blob_field(pos, stride, n, aabb_size, blobs, waves, out_stride=None, want_rg
     lib().orc_blob_field(n, stride, _p(_c(pos, np.float32)), aabb_size, len(blobs), _p(_c(blobs, np.float32)),
                          _p(_c(waves, np.float32)), _p(sig), _p(rgb), out_stride)
     return sig, rgb
+
+
+class Camera(ctypes.Structure):
+    """Same layout as the library's tn_camera: transform = camera to world, row-major 3 x 4."""
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("near", ctypes.c_float),
+                ("far", ctypes.c_float), ("focal_x", ctypes.c_float), ("focal_y", ctypes.c_float),
+                ("principal_x", ctypes.c_float), ("principal_y", ctypes.c_float), ("shift_x", ctypes.c_float),
+                ("shift_y", ctypes.c_float), ("transform", ctypes.c_float * 12)]
+
+
+def render(camera: dict, render_bbox, training_bbox, grid, dt_min, cone, min_t, blobs, waves, aabb_size):
+    """Inference render of one NeRF whose network is the blob field. camera: dict(width,
+    height, near, far, focal (fx, fy), principal (cx, cy), shift (sx, sy), transform [3][4]).
+    Returns (rgba [h][w][4] float64, ambiguous [h][w] uint8 flags, queried samples)."""
+    c = Camera()
+    c.width, c.height = int(camera["width"]), int(camera["height"])
+    c.near, c.far = float(camera["near"]), float(camera["far"])
+    c.focal_x, c.focal_y = [float(v) for v in camera["focal"]]
+    c.principal_x, c.principal_y = [float(v) for v in camera["principal"]]
+    c.shift_x, c.shift_y = [float(v) for v in camera["shift"]]
+    for k, v in enumerate(np.asarray(camera["transform"], np.float32)[:3, :4].reshape(-1)):
+        c.transform[k] = float(v)
+    n = c.width * c.height
+    out = np.zeros(4 * n)
+    amb = np.zeros(n, np.uint8)
+    rb, tb = bbox_struct(render_bbox), bbox_struct(training_bbox)
+    bits = _c(grid["bitfield"], np.uint8)
+    total = lib().orc_render(ctypes.byref(c), ctypes.byref(rb), ctypes.byref(tb), grid["n_levels"], grid["res"],
+                             grid["base"], _p(bits), dt_min, cone, min_t, len(blobs), _p(_c(blobs, np.float32)),
+                             _p(_c(waves, np.float32)), aabb_size, _p(out), _p(amb))
+    return out.reshape(c.height, c.width, 4), amb.reshape(c.height, c.width), int(total)

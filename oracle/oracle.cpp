@@ -762,28 +762,154 @@ void orc_adam_step(int64_t n, int64_t n_grid, int64_t n_mlp, double loss_scale, 
 // waves is [3][4] = (ax, ay, az, phase). Positions are normalised network inputs in
 // [0,1]^3 ([3][stride]); world = (pos - 0.5) * aabb_size. FP64.
 // ---------------------------------------------------------------------------
+static inline void blob_at(float px, float py, float pz, float aabb_size, int n_blobs, const float* blobs,
+                           const float* waves, double* sigma, double* rgb, int64_t rgb_stride) {
+    const double x = ((double)px - 0.5) * aabb_size;
+    const double y = ((double)py - 0.5) * aabb_size;
+    const double z = ((double)pz - 0.5) * aabb_size;
+    double s = 0.0;
+    for (int b = 0; b < n_blobs; ++b) {
+        const double ddx = x - blobs[5 * b], ddy = y - blobs[5 * b + 1], ddz = z - blobs[5 * b + 2];
+        const double sd = blobs[5 * b + 3];
+        s += blobs[5 * b + 4] * std::exp(-(ddx * ddx + ddy * ddy + ddz * ddz) / (2.0 * sd * sd));
+    }
+    *sigma = s;
+    if (rgb) {
+        for (int c = 0; c < 3; ++c) {
+            const double a = waves[4 * c] * x + waves[4 * c + 1] * y + waves[4 * c + 2] * z + waves[4 * c + 3];
+            rgb[c * rgb_stride] = 1.0 / (1.0 + std::exp(-std::sin(a)));
+        }
+    }
+}
+
 void orc_blob_field(int64_t n, int64_t stride, const float* pos, float aabb_size,
                     int n_blobs, const float* blobs, const float* waves,
                     double* sigma_out, double* rgb_out, int64_t out_stride) {
 #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i)
+        blob_at(pos[i], pos[i + stride], pos[i + 2 * stride], aabb_size, n_blobs, blobs, waves, sigma_out + i,
+                rgb_out ? rgb_out + i : nullptr, out_stride);
+}
+
+// ---------------------------------------------------------------------------
+// Inference render of one NeRF with the synthetic field as its network (the reference
+// Renderer::perform_task, src/core/renderer.cu:172-646, for one NeRF with an identity
+// transform), one ray at a time. Ray generation: Camera::global_ray_at_pixel_xy without
+// lens distortion (src/models/camera.cuh:94-137); box clip: prepare_for_linear_
+// raymarching_kernel (src/utils/rendering-kernels.cu:175-262); sample validity and network
+// inputs: filter_and_localize_samples_for_nerf_kernel and assign_normalized_network_
+// inputs_kernel (:336-478); compositing: accumulate_nerf_samples_kernel and
+// composite_samples_kernel (:480-618); kill_terminated_rays_kernel (:620-637).
+//
+// Positions, steps and validity in FP32 with the reference's operation order (so the
+// set of queried samples is exact); field, opacity and compositing in FP64. The reference
+// marches rays in rounds of max(batch / live rays, 1) steps and drops a ray past t_max only
+// after its round; this restatement stops at the first step past t_max, which gives the
+// same image as long as no valid sample lies beyond t_max before the ray leaves the render
+// box. Flags per pixel (ambiguous[i], OR of):
+//   1  a valid sample lies past t_max inside the render box (the image then depends on
+//      the round schedule);
+//   2  the transmittance came within 0.1% of min_transmittance (FP32 and FP64 may end
+//      the ray one sample apart);
+//   4  a sample opacity came within 0.001% of the colour cut 1e-4.
+// out_rgba: interleaved premultiplied RGBA. Returns the number of queried samples.
+// ---------------------------------------------------------------------------
+struct Camera {
+    int32_t width, height;
+    float near_, far_;
+    float focal_x, focal_y;
+    float principal_x, principal_y;
+    float shift_x, shift_y;
+    float transform[12];  // row-major 3 x 4 [R | t], camera to world
+};
+
+int64_t orc_render(const Camera* cam, const Bbox* render_bbox, const Bbox* train_bbox, int n_levels, int res,
+                   float base, const uint8_t* bits, float dt_min, float cone, double min_t, int n_blobs,
+                   const float* blobs, const float* waves, float aabb_size, double* out_rgba, uint8_t* ambiguous) {
+    const Grid g{n_levels, res, base, bits};
+    const Bbox box = *render_bbox, tb = *train_bbox;
+    const int64_t n = (int64_t)cam->width * cam->height;
+    const float dt_max = 8.0f * dt_min;
+    const float sx = tb.max_x - tb.min_x, sy = tb.max_y - tb.min_y, sz = tb.max_z - tb.min_z;
+    const float inv_size = 1.0f / sx;
+    const float offx = cam->shift_x * (float)cam->width - cam->principal_x;
+    const float offy = cam->shift_y * (float)cam->height - cam->principal_y;
+    const float* m = cam->transform;
+    int64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
     for (int64_t i = 0; i < n; ++i) {
-        const double x = ((double)pos[i] - 0.5) * aabb_size;
-        const double y = ((double)pos[i + stride] - 0.5) * aabb_size;
-        const double z = ((double)pos[i + 2 * stride] - 0.5) * aabb_size;
-        double s = 0.0;
-        for (int b = 0; b < n_blobs; ++b) {
-            const double ddx = x - blobs[5 * b], ddy = y - blobs[5 * b + 1], ddz = z - blobs[5 * b + 2];
-            const double sd = blobs[5 * b + 3];
-            s += blobs[5 * b + 4] * std::exp(-(ddx * ddx + ddy * ddy + ddz * ddz) / (2.0 * sd * sd));
-        }
-        sigma_out[i] = s;
-        if (rgb_out) {
-            for (int c = 0; c < 3; ++c) {
-                const double a = waves[4 * c] * x + waves[4 * c + 1] * y + waves[4 * c + 2] * z + waves[4 * c + 3];
-                rgb_out[i + c * out_stride] = 1.0 / (1.0 + std::exp(-std::sin(a)));
+        double* o4 = out_rgba + 4 * i;
+        o4[0] = o4[1] = o4[2] = o4[3] = 0.0;
+        ambiguous[i] = 0;
+        const uint32_t py = (uint32_t)(i / cam->width), px = (uint32_t)(i % cam->width);
+        const float vx = ((float)px + offx + 0.5f) / cam->focal_x;
+        const float vy = ((float)py + offy + 0.5f) / cam->focal_y;
+        const float vz = 1.0f;
+        const float vlen = std::sqrt(vx * vx + vy * vy + vz * vz);
+        const float gx = m[0] * vx + m[1] * vy + m[2] * vz;
+        const float gy = m[4] * vx + m[5] * vy + m[6] * vz;
+        const float gz = m[8] * vx + m[9] * vy + m[10] * vz;
+        const float gl = std::sqrt(gx * gx + gy * gy + gz * gz);
+        const float dx = gx / gl, dy = gy / gl, dz = gz / gl;
+        float ox = m[3] + cam->near_ * (vlen * dx);
+        float oy = m[7] + cam->near_ * (vlen * dy);
+        float oz = m[11] + cam->near_ * (vlen * dz);
+        const float ix = 1.0f / dx, iy = 1.0f / dy, iz = 1.0f / dz;
+        float t1x = (box.min_x - ox) * ix, t2x = (box.max_x - ox) * ix;
+        float t1y = (box.min_y - oy) * iy, t2y = (box.max_y - oy) * iy;
+        float t1z = (box.min_z - oz) * iz, t2z = (box.max_z - oz) * iz;
+        if (t1x > t2x) std::swap(t1x, t2x);
+        if (t1y > t2y) std::swap(t1y, t2y);
+        if (t1z > t2z) std::swap(t1z, t2z);
+        const float bmin = std::fmax(t1x, std::fmax(t1y, t1z)), bmax = std::fmin(t2x, std::fmin(t2y, t2z));
+        const bool volume = box.max_x > box.min_x && box.max_y > box.min_y && box.max_z > box.min_z;
+        if (!(volume && bmax >= bmin)) continue;
+        const float t0 = std::fmax(bmin, 1e-4f);
+        ox = ox + t0 * dx;
+        oy = oy + t0 * dy;
+        oz = oz + t0 * dz;
+        const float tmax = std::fmin(bmax, cam->far_ - cam->near_);
+        const float dir_len = std::sqrt(dx * dx + dy * dy + dz * dz);
+        double T = 1.0;
+        float t = 0.0f;
+        bool past = false;
+        for (int64_t guard = 0; guard < (1 << 24); ++guard) {
+            const float dt = get_dt(t, cone, dt_min, dt_max);
+            const float x = ox + t * dx, y = oy + t * dy, z = oz + t * dz;
+            if (past && !bbox_contains(box, x, y, z)) break;
+            const float dt_net = inv_size * (dir_len * dt);
+            bool valid = false;
+            float u[3] = {(x - tb.min_x) / sx, (y - tb.min_y) / sy, (z - tb.min_z) / sz};
+            if (bbox_contains(box, x, y, z)) {
+                const int k = grid_level_at(g, x, y, z, dt_net);
+                valid = is_occupied(g, k, x, y, z) && u[0] >= 0.0f && u[0] <= 1.0f && u[1] >= 0.0f &&
+                        u[1] <= 1.0f && u[2] >= 0.0f && u[2] <= 1.0f;
             }
+            if (valid && past) {
+                ambiguous[i] |= 1;
+                break;
+            }
+            if (valid) {
+                for (int c = 0; c < 3; ++c) u[c] = clampf_ref(u[c], 0.0f, 1.0f);
+                double sigma, rgb[3];
+                blob_at(u[0], u[1], u[2], aabb_size, n_blobs, blobs, waves, &sigma, rgb, 1);
+                ++total;
+                const double alpha = 1.0 - std::exp(-sigma * (double)dt_net);
+                if (std::fabs(alpha - 1e-4) <= 1e-9) ambiguous[i] |= 4;
+                const double inv_a = alpha > 1e-4 ? 1.0 / alpha : 0.0;
+                const double a = std::fmin(alpha, 1.0);
+                const double w = a * T;
+                for (int c = 0; c < 3; ++c) o4[c] += w * (rgb[c] * alpha * inv_a);
+                o4[3] += w;
+                T *= 1.0 - a;
+                if (std::fabs(T - min_t) <= 1e-3 * min_t) ambiguous[i] |= 2;
+                if (T < min_t) break;
+            }
+            t = t + dt;
+            if (t > tmax) past = true;
         }
     }
+    return total;
 }
 
 }  // extern "C"

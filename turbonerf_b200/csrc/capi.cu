@@ -94,6 +94,7 @@ int ensure_block_u32(tn_ctx* ctx, size_t n) { return ensure(ctx->block_u32, ctx-
 int ensure_block_f32(tn_ctx* ctx, size_t n) { return ensure(ctx->block_f32, ctx->block_f32_cap, n, "scratch(f32)"); }
 int ensure_mip(tn_ctx* ctx, size_t bytes) { return ensure(ctx->mip, ctx->mip_cap, bytes, "scratch(mip)"); }
 int ensure_slots(tn_ctx* ctx, size_t n) { return ensure(ctx->slots, ctx->slots_cap, n, "scratch(slots)"); }
+int ensure_render_ws(tn_ctx* ctx, size_t bytes) { return ensure(ctx->render_ws, ctx->render_ws_cap, bytes, "scratch(render)"); }
 
 int validate_grid(const tn_grid_desc* grid) {
     TN_REQUIRE(grid != nullptr, TN_E_NULL, "grid descriptor is NULL");
@@ -142,6 +143,7 @@ int tn_ctx_destroy(tn_ctx* ctx) {
     cudaFree(ctx->block_f32);
     cudaFree(ctx->mip);
     cudaFree(ctx->slots);
+    cudaFree(ctx->render_ws);
     delete ctx;
     return TN_OK;
 }

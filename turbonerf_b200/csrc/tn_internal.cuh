@@ -27,6 +27,8 @@ struct tn_ctx {
     tn_tuning tune{64, 8, 1, 4, 128, 64, 0};  // launch shapes (tn_tuning_default)
     uint32_t count_group_used = 0;      // rays per block of the last tn_march_count (its emit's grouping)
     uint32_t multi_chunk_used = 0;      // rays per chunk of the last tn_multi_march_count
+    uint8_t* render_ws = nullptr;       // ray and sample buffers of tn_render
+    size_t render_ws_cap = 0;
 };
 
 namespace tn {
@@ -52,6 +54,7 @@ int ensure_block_u32(tn_ctx* ctx, size_t n);
 int ensure_block_f32(tn_ctx* ctx, size_t n);
 int ensure_mip(tn_ctx* ctx, size_t bytes);
 int ensure_slots(tn_ctx* ctx, size_t n);
+int ensure_render_ws(tn_ctx* ctx, size_t bytes);
 bool stream_capturing(cudaStream_t s);
 int num_sms();
 

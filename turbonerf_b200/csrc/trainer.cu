@@ -736,6 +736,23 @@ int tn_trainer_flush(tn_trainer* tr) {
     return st;
 }
 
+int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,
+                      uint32_t batch_size, float* out_rgba, tn_render_stats* stats) {
+    TN_NONNULL(tr);
+    int st = flush_adam(tr);
+    if (st != TN_OK) return st;
+    tn_render_desc rd{};
+    rd.grid = tr->d.grid;
+    rd.bitfield = tr->bits;
+    rd.training_bbox = tr->d.bbox;
+    rd.render_bbox = render_bbox ? *render_bbox : tr->d.bbox;
+    rd.dt_min = min_step_size > 0.0f ? min_step_size : tr->d.min_step_size;
+    rd.cone_angle = tr->d.cone_angle;
+    rd.min_transmittance = tr->d.min_transmittance;
+    rd.batch_size = batch_size;
+    return tn_render(tr->ctx, tr->stream, &rd, camera, &tr->net, out_rgba, stats);
+}
+
 int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out) {
     TN_NONNULL(tr);
     return tn_ctx_get_tuning(tr->ctx, out);

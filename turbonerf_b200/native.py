@@ -120,6 +120,25 @@ class TrainerDesc(ctypes.Structure):
                 ("ray_jitter", ctypes.c_float)]
 
 
+class CameraC(ctypes.Structure):
+    """tn_camera: pinhole camera, transform = camera to world, row-major 3 x 4 [R | t]."""
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("near", ctypes.c_float),
+                ("far", ctypes.c_float), ("focal_x", ctypes.c_float), ("focal_y", ctypes.c_float),
+                ("principal_x", ctypes.c_float), ("principal_y", ctypes.c_float), ("shift_x", ctypes.c_float),
+                ("shift_y", ctypes.c_float), ("transform", ctypes.c_float * 12)]
+
+
+class RenderDescC(ctypes.Structure):
+    _fields_ = [("grid", GridDesc), ("bitfield", ctypes.c_void_p), ("render_bbox", Bbox),
+                ("training_bbox", Bbox), ("dt_min", ctypes.c_float), ("cone_angle", ctypes.c_float),
+                ("min_transmittance", ctypes.c_float), ("batch_size", ctypes.c_uint32)]
+
+
+class RenderStatsC(ctypes.Structure):
+    _fields_ = [("rays_hit", ctypes.c_uint32), ("iterations", ctypes.c_uint32), ("samples", ctypes.c_uint64),
+                ("steps", ctypes.c_uint64)]
+
+
 class TrainingMetricsC(ctypes.Structure):
     _fields_ = [("step", ctypes.c_uint32), ("n_rays", ctypes.c_uint32), ("n_samples", ctypes.c_uint32),
                 ("loss", ctypes.c_float)]
@@ -199,6 +218,8 @@ SIGNATURES = {
                                        _vp, _P(_u32)],
     "tn_plain_adam_step": [_vp, _u32, _u32, _u32, _f32, _f32, _f32, _f32, _f32, _f32, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_synth_field": [_vp, _u32, _vp, _u32, _vp, _f32, _u32, _vp, _vp, _vp, _vp, _u32],
+    "tn_render": [_vp, _vp, _P(RenderDescC), _P(CameraC), _vp, _vp, _P(RenderStatsC)],
+    "tn_trainer_render": [_vp, _P(CameraC), _P(Bbox), _f32, _u32, _vp, _P(RenderStatsC)],
     "tn_trainer_default_desc": [_vp],
     "tn_trainer_create": [_P(_vp), _vp, _vp],
     "tn_trainer_destroy": [_vp],

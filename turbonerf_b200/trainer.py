@@ -73,6 +73,7 @@ class SyntheticNeRF:
     bitfield: np.ndarray | None = None  # [res^3] uint8 (None: all bits set, like the reference)
     resolution: int = 128
     base_size: float = 1.0
+    render_bbox: BoundingBox | None = None  # renderer crop (reference NeRFProxy::render_bbox); None: bounding_box
 
     @classmethod
     def from_scene(cls, scene) -> "SyntheticNeRF":
