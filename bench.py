@@ -787,6 +787,81 @@ def run_kernel_tour(args):
     print(json.dumps({"workload": "kernel tour", "ran": ran, "data": "synthetic"}), flush=True)
 
 
+def _look_at(eye, target=(0.0, 0.0, 0.0)):
+    """Camera to world [3][4]: columns right, down, forward (the camera looks along +z)."""
+    eye = np.asarray(eye, np.float64)
+    f = np.asarray(target, np.float64) - eye
+    f /= np.linalg.norm(f)
+    r = np.cross(f, [0.0, 1.0, 0.0])
+    r /= np.linalg.norm(r)
+    t = np.zeros((3, 4))
+    t[:, 0], t[:, 1], t[:, 2], t[:, 3] = r, np.cross(f, r), f, eye
+    return t
+
+
+def run_render(args):
+    """Inference render (Renderer.submit) of the train-step scene: 5 cascades of 128^3 built
+    from the 8-blob field, which also stands in for the network; the camera at (0.3, 0.8, 4.0)
+    looks at the centre from inside the 16-unit training box (focal 0.7 x width). Frames of
+    800 x 800 and 1920 x 1080 at sample budgets of 2^20 (the reference default), 2^22 and 2^24
+    per round. A frame is one synchronous submit (it reads the live ray count back every
+    round), so frames are timed on the host clock around the call. The CPU oracle renders the
+    same view at 200 x 200 on all host threads; its rays/s is the CPU baseline, and its image
+    is compared with the GPU frame of the same size."""
+    import torch
+    import oracle
+    from turbonerf_b200 import scenes
+    from turbonerf_b200.renderer import Camera, CPURenderBuffer, CUDARenderBuffer, RenderRequest, Renderer
+
+    torch.cuda.set_device(0)
+    sc = _scene(0x7B0)
+    tr = _trainer(sc, "fused", 0x7B0)
+    eye = (0.3, 0.8, 4.0)
+
+    def cam(w, h):
+        return Camera((w, h), 0.1, 100.0, (0.7 * w, 0.7 * w), (w / 2, h / 2), (0.0, 0.0), _look_at(eye))
+
+    out = {"workload": "inference render of the train-step scene (5x128^3 cascades, 8-blob field as the network)",
+           "metric": "rays/s per frame (host clock around the synchronous submit)", "dtype": "f32",
+           "data": "synthetic", "frames": []}
+    buf = CUDARenderBuffer()
+    for (w, h) in ((800, 800), (1920, 1080)):
+        for bs in (1 << 20, 1 << 22, 1 << 24):
+            r = Renderer(batch_size=bs)
+            req = RenderRequest(cam(w, h), [tr], buf)
+            for _ in range(max(args.warmup, 3)):
+                r.submit(req)
+            reps = max(min(args.steps, 20), 3)
+            times = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                st = r.submit(req)
+                times.append(time.perf_counter() - t0)
+            ms = 1e3 * statistics.median(times)
+            out["frames"].append({"width": w, "height": h, "batch_size": bs, "ms_per_frame": round(ms, 3),
+                                  "rays_per_s": round(w * h / (ms / 1e3), 1),
+                                  "samples_per_s": round(st["samples"] / (ms / 1e3), 1),
+                                  "steps_per_s": round(st["steps"] / (ms / 1e3), 1), **st})
+    # CPU oracle on a 200 x 200 frame of the same view, and the GPU frame it is compared with
+    c = cam(200, 200)
+    od = dict(width=200, height=200, near=c.near, far=c.far, focal=c.focal_length, principal=c.principal_point,
+              shift=c.shift, transform=c.transform)
+    t0 = time.perf_counter()
+    ref, amb, _ = oracle.render(od, sc.bbox, sc.bbox, sc.grid.as_dict(), float(np.float32(scenes.MIN_STEP_SIZE)),
+                                1.0 / 256.0, 1e-4, sc.field.blobs, sc.field.waves, sc.aabb_size)
+    el = time.perf_counter() - t0
+    cpu = CPURenderBuffer()
+    Renderer().submit(RenderRequest(c, [tr], cpu))
+    img = cpu.get_rgba().astype(np.float64)
+    ok = amb == 0
+    err = np.abs(img - ref)[ok] / (np.abs(ref)[ok] + 1e-6 * np.abs(ref).max())
+    out["cpu_baseline"] = {"value": round(200 * 200 / el, 1), "unit": "rays/s", "cores": oracle.num_threads(),
+                           "kind": "port", "sample": f"one 200 x 200 frame of the same view on the CPU oracle, {el:.2f} s"}
+    out["parity_200x200"] = {"max_rel_err": float(err.max()), "ambiguous_pixels": int((~ok).sum())}
+    tr.teardown()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -797,10 +872,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="train-step", choices=["train-step", "backward-memory", "multi-scene", "kernel-tour"],
+    ap.add_argument("--workload", default="train-step",
+                    choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "
                          "multi-scene: the batched persistent march of 16 scenes against one launch per scene; "
-                         "kernel-tour: every kernel once at representative sizes, for profiling")
+                         "kernel-tour: every kernel once at representative sizes, for profiling; "
+                         "render: inference frames through Renderer.submit")
     args = ap.parse_args()
     if args.workload == "backward-memory":
         run_backward_memory(args)
@@ -808,6 +885,8 @@ def main():
         run_multi_scene(args)
     elif args.workload == "kernel-tour":
         run_kernel_tour(args)
+    elif args.workload == "render":
+        run_render(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

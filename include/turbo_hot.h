@@ -477,7 +477,8 @@ typedef struct tn_render_stats {
     uint32_t rays_hit;    /* pixels whose ray meets the render box */
     uint32_t iterations;  /* march/network/composite rounds */
     uint64_t samples;     /* samples sent to the network */
-    uint64_t steps;       /* march steps taken */
+    uint64_t steps;       /* march steps taken (the reference's t += dt steps) */
+    uint64_t tests;       /* steps whose sample was tested; the others crossed known-empty cells */
 } tn_render_stats;
 
 /* Renders camera->width x camera->height pixels into out_rgba (device, interleaved

@@ -894,7 +894,7 @@ int64_t orc_render(const Camera* cam, const Bbox* render_bbox, const Bbox* train
                 double sigma, rgb[3];
                 blob_at(u[0], u[1], u[2], aabb_size, n_blobs, blobs, waves, &sigma, rgb, 1);
                 ++total;
-                const double alpha = 1.0 - std::exp(-sigma * (double)dt_net);
+                const double alpha = -std::expm1(-sigma * (double)dt_net);
                 if (std::fabs(alpha - 1e-4) <= 1e-9) ambiguous[i] |= 4;
                 const double inv_a = alpha > 1e-4 ? 1.0 / alpha : 0.0;
                 const double a = std::fmin(alpha, 1.0);

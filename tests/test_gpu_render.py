@@ -31,16 +31,18 @@ def look_at(eye, target=(0.0, 0.0, 0.0)):
     return t
 
 
-def _trainer(n_levels=5, cells=0, render_bbox=None):
+def _trainer(n_levels=5, cells=0, render_bbox=None, min_transmittance=1e-4, bitfield=None):
     from turbonerf_b200.trainer import BoundingBox, SyntheticNeRF, Trainer
     sc = scenes.march_scene_cascaded(n_rays=8, n_levels=n_levels)
+    if bitfield is not None:
+        sc.grid.bitfield = bitfield
     nerf = SyntheticNeRF.from_scene(sc)
     if render_bbox is not None:
         b = BoundingBox()
         b.min_x, b.min_y, b.min_z, b.max_x, b.max_y, b.max_z = render_bbox
         nerf.render_bbox = b
     tr = Trainer(nerf, n_rays_per_step=4096, occupancy_cells_per_step=cells, occupancy_threshold=0.01,
-                 n_grid_params=16 * (1 << 15) * 2)
+                 n_grid_params=16 * (1 << 15) * 2, min_transmittance=min_transmittance)
     tr.setup_data(batch_size=1 << 16)
     return sc, tr
 
@@ -51,13 +53,13 @@ def _camera(w, h, eye, far=100.0, shift=(0.0, 0.0)):
     return Camera((w, h), 0.1, far, (f, f), (w / 2, h / 2), shift, look_at(eye))
 
 
-def _oracle_image(sc, cam, bits=None, render_bbox=None, dt_min=scenes.MIN_STEP_SIZE):
+def _oracle_image(sc, cam, bits=None, render_bbox=None, dt_min=scenes.MIN_STEP_SIZE, min_t=1e-4):
     grid = sc.grid.as_dict()
     if bits is not None:
         grid = dict(grid, bitfield=bits)
     c = dict(width=cam.resolution[0], height=cam.resolution[1], near=cam.near, far=cam.far,
              focal=cam.focal_length, principal=cam.principal_point, shift=cam.shift, transform=cam.transform)
-    return oracle.render(c, render_bbox or sc.bbox, sc.bbox, grid, float(np.float32(dt_min)), CONE, 1e-4,
+    return oracle.render(c, render_bbox or sc.bbox, sc.bbox, grid, float(np.float32(dt_min)), CONE, min_t,
                          sc.field.blobs, sc.field.waves, sc.aabb_size)
 
 
@@ -193,4 +195,27 @@ def test_render_rejects_bad_cameras():
     cam = Camera((0, 16), 0.1, 10.0, (10.0, 10.0), (8, 8), (0, 0), look_at((0, 0, 4)))
     with pytest.raises(TurboError, match="empty image"):
         _submit(tr, cam)
+    tr.teardown()
+
+
+@pytest.mark.parametrize("density", [0.002, 0.03, 0.3])
+def test_render_sample_set_is_exact_on_random_grids(density):
+    """With no early termination (min_transmittance 0) every ray collects all of its valid
+    samples, so the number sent to the network must equal the oracle's step-by-step count
+    exactly: a sample lost or added by the empty-space skipping changes it. Random bitfields
+    put occupied cells at every level next to empty ones, and the views include cameras inside
+    several cascade levels."""
+    rng = np.random.default_rng(int(density * 1e4))
+    R = 128
+    bits = np.zeros(R ** 3, np.uint8)
+    for k in range(5):
+        bits |= ((rng.random(R ** 3) < density).astype(np.uint8) << np.uint8(k))
+    sc, tr = _trainer(min_transmittance=0.0, bitfield=bits)
+    for eye in ((0.3, 0.8, 4.0), (0.05, -0.2, 0.3), (-1.7, 0.9, 1.2), (6.0, -5.0, 7.5), (12.0, 3.0, -9.0)):
+        cam = _camera(48, 40, eye)
+        img, stats = _submit(tr, cam, batch_size=1 << 16)
+        ref, amb, n_ref = _oracle_image(sc, cam, min_t=0.0)
+        assert stats["samples"] == n_ref, (eye, stats, n_ref)
+        assert stats["tests"] <= stats["steps"]
+        _compare(img, ref, amb, f"random grid {density} eye {eye}")
     tr.teardown()

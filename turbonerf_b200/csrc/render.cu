@@ -98,45 +98,202 @@ __global__ void render_rays_kernel(uint32_t n, tn_camera cam, tn_bbox box, float
     hit[i] = 1u;
 }
 
-// One sample of a ray at t: whether the network is queried there (filter_and_localize_samples_for_
-// nerf_kernel and assign_normalized_network_inputs_kernel, rendering-kernels.cu:336-478, identity
-// transform) and its network inputs.
-struct RenderSample {
-    bool valid;
-    float ux, uy, uz;  // unit-cube position, clamped to [0, 1]
-    float dt_net;      // step in units of the training box size
-};
-
-__device__ __forceinline__ RenderSample render_sample(const RenderArgs& A, const RayMarch& r, float t, float dt,
-                                                      float dir_len) {
-    RenderSample o;
-    float x, y, z;
-    ray_point(r, t, x, y, z);
-    o.dt_net = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, dt));
-    const float ux = __fdiv_rn(__fadd_rn(x, -A.train_bbox.min_x), A.train_size_x);
-    const float uy = __fdiv_rn(__fadd_rn(y, -A.train_bbox.min_y), A.train_size_y);
-    const float uz = __fdiv_rn(__fadd_rn(z, -A.train_bbox.min_z), A.train_size_z);
-    o.valid = false;
-    if (bbox_contains(A.render_bbox, x, y, z)) {
-        const int k = grid_level_at(A.g, x, y, z, o.dt_net);
-        o.valid = ((A.g.bits[voxel_morton(A.g, k, x, y, z)] >> k) & 1u) && ux >= 0.0f && ux <= 1.0f &&
-                  uy >= 0.0f && uy <= 1.0f && uz >= 0.0f && uz <= 1.0f;
+// Coarse occupancy: mip[m] is the OR of the 64 bitfield bytes of the 4 x 4 x 4 block of cells
+// with Morton index m (cells [64 m, 64 m + 64)), so bit k of mip[idx >> 6] is clear when the
+// whole block of cell idx is empty at level k.
+__global__ void render_mip_kernel(uint32_t n_blocks, const uint4* __restrict__ bits, uint8_t* __restrict__ mip) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_blocks) return;
+    uint32_t v = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const uint4 u = __ldg(bits + 4 * (size_t)m + q);
+        v |= u.x | u.y | u.z | u.w;
     }
-    o.ux = clamp_ref(ux, 0.0f, 1.0f);
-    o.uy = clamp_ref(uy, 0.0f, 1.0f);
-    o.uz = clamp_ref(uz, 0.0f, 1.0f);
-    return o;
+    mip[m] = (uint8_t)((v | (v >> 8) | (v >> 16) | (v >> 24)) & 0xFFu);
 }
 
-// count (EMIT = false: counts[j]) or emit (EMIT = true: packed network inputs at offsets[j], and
-// the ray's t advanced) the valid samples of the next `steps` steps of each live ray
-template <bool EMIT>
-__global__ void render_march_kernel(RenderArgs A, uint32_t n, uint32_t n_live, uint32_t steps,
-                                    const uint32_t* __restrict__ live, const float* __restrict__ ori,
-                                    const float* __restrict__ dir, float* __restrict__ ray_t,
-                                    uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                                    uint32_t cap, float* __restrict__ s_pos, float* __restrict__ s_dir,
-                                    float* __restrict__ s_dt, uint32_t* flags) {
+// World coordinate of the cell boundary with index c (scaled coordinate f = c) at level size ls:
+// f = (x / ls + 0.5) R  <=>  x = (c / R - 0.5) ls. The skip margin covers its rounding.
+__device__ __forceinline__ float cell_boundary(uint32_t c, float inv_res, float ls) {
+    return (float)c * inv_res * ls - 0.5f * ls;
+}
+
+// The t window in which the sample position o + t d, computed in FP32, lies inside [lo, hi]
+// along one axis with a margin on both faces: the faces are pulled in by far more than the
+// rounding of the position (o + t d), of these expressions and of the cell coordinate
+// (x / ls + 0.5) R, so a step with t in the window gives a cell coordinate strictly inside the
+// box. A zero (or below 2^-128) direction leaves the coordinate in place: the window is then
+// everything or nothing.
+__device__ __forceinline__ void axis_window(float o, float d, float inv_d, float lo, float hi, float ls, float& t_in,
+                                            float& t_out) {
+    const float e_lo = 4e-6f * (fabsf(lo) + fabsf(o) + ls), e_hi = 4e-6f * (fabsf(hi) + fabsf(o) + ls);
+    const float a = lo + e_lo, b = hi - e_hi;
+    if (!(fabsf(inv_d) < INFINITY)) {
+        // |d| below 2^-128 (or zero): the coordinate moves by less than the margin at any finite t
+        const bool inside = o >= a && o <= b;
+        t_in = inside ? -INFINITY : INFINITY;
+        t_out = inside ? INFINITY : -INFINITY;
+    } else if (d > 0.0f) {
+        t_in = (a - o) * inv_d;
+        t_out = (b - o) * inv_d;
+    } else if (d < 0.0f) {
+        t_in = (b - o) * inv_d;
+        t_out = (a - o) * inv_d;
+    } else {
+        const bool inside = o >= a && o <= b;
+        t_in = inside ? -INFINITY : INFINITY;
+        t_out = inside ? INFINITY : -INFINITY;
+    }
+}
+
+// One round of one ray: from its t, the steps t += get_dt(t) of the reference's march
+// (march_rays_and_generate_global_sample_points_kernel, rendering-kernels.cu:264-334), each sample
+// tested as filter_and_localize_samples_for_nerf_kernel and assign_normalized_network_inputs_kernel
+// do (:336-478, identity transform): inside the render box, occupied at the level that
+// get_grid_level_at picks from the position and the step scaled to the training box, and inside
+// the training box in unit coordinates. The t of each valid sample goes to slots[c * stride]; the
+// round ends after `quota` valid samples or once t has passed t_max (*done).
+//
+// Empty space: when a sample's cell is empty, the position's cell (or, when the coarse mip says
+// so, its whole 4 x 4 x 4 block) at that level k is empty, and the following steps are taken with
+// the same FP32 recurrence but without tests while their positions lie inside that box with a
+// margin on every face (axis_window). Each of them would read an empty cell at level k, since the
+// level choice max(position term, step term) stays k:
+//  * inside the box the position lies inside level k's extent, so the position term is <= k;
+//  * aligned blocks (R >= 16) and cells (R >= 4) lie wholly inside or wholly outside the extent of
+//    level k - 1; outside it, the position term is >= k (the margin keeps the position clear of
+//    the boundary); inside it, the step term must already be >= k at the current step;
+//  * the step term only grows along the ray, and is checked to stay <= k at the largest step
+//    (dt_max) unless k is the coarsest level.
+// The set of valid samples is therefore exactly the step-by-step one.
+struct WalkResult {
+    uint32_t count;
+    bool done;
+    uint32_t steps, tests;
+};
+
+__device__ WalkResult render_walk(const RenderArgs& A, const RayMarch& r, float dir_len, float& t_io, float tmax,
+                                  uint32_t quota, float* __restrict__ slots, uint32_t stride,
+                                  const uint8_t* __restrict__ mip, uint32_t max_iters, uint32_t* flags) {
+    const GridView& g = A.g;
+    const float dtn_max = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, A.dt_max));
+    const bool cells_ok = g.res >= 4, blocks_ok = g.res >= 16 && mip != nullptr;
+    float t = t_io;
+    uint32_t c = 0, iters = 0, tests = 0;
+    bool done = false;
+    while (c < quota) {
+        if (t > tmax) {
+            done = true;
+            break;
+        }
+        if (++iters > max_iters) {
+            raise_flag(flags, ERR_GUARD);
+            done = true;
+            break;
+        }
+        const float dt = get_dt(t, A.cone, A.dt_min, A.dt_max);
+        float x, y, z;
+        ray_point(r, t, x, y, z);
+        ++tests;
+        if (bbox_contains(A.render_bbox, x, y, z)) {
+            const float dt_net = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, dt));
+            const int k = grid_level_at(g, x, y, z, dt_net);
+            const float s = g.inv_ls[k];
+            const float fx = __fmul_rn(__fadd_rn(__fmul_rn(x, s), 0.5f), g.res_f);
+            const float fy = __fmul_rn(__fadd_rn(__fmul_rn(y, s), 0.5f), g.res_f);
+            const float fz = __fmul_rn(__fadd_rn(__fmul_rn(z, s), 0.5f), g.res_f);
+            const uint32_t cx = cell_coord(x, s, g.res_f, g.res), cy = cell_coord(y, s, g.res_f, g.res),
+                           cz = cell_coord(z, s, g.res_f, g.res);
+            const uint32_t idx = morton3d(cx, cy, cz);
+            if ((__ldg(g.bits + idx) >> k) & 1u) {
+                const float ux = __fdiv_rn(__fadd_rn(x, -A.train_bbox.min_x), A.train_size_x);
+                const float uy = __fdiv_rn(__fadd_rn(y, -A.train_bbox.min_y), A.train_size_y);
+                const float uz = __fdiv_rn(__fadd_rn(z, -A.train_bbox.min_z), A.train_size_z);
+                if (ux >= 0.0f && ux <= 1.0f && uy >= 0.0f && uy <= 1.0f && uz >= 0.0f && uz <= 1.0f) {
+                    slots[(size_t)c * stride] = t;
+                    ++c;
+                }
+            } else if (cells_ok && fx >= 0.0f && fx < g.res_f && fy >= 0.0f && fy < g.res_f && fz >= 0.0f &&
+                       fz < g.res_f && (k == g.n_levels - 1 || dtn_max < g.cell[k])) {
+                // the empty box: the block when the mip says it is empty, else the cell
+                const int sh = (blocks_ok && !((__ldg(mip + (idx >> 6)) >> k) & 1u)) ? 2 : 0;
+                const uint32_t lx = (cx >> sh) << sh, ly = (cy >> sh) << sh, lz = (cz >> sh) << sh;
+                const uint32_t w = 1u << sh, q1 = (uint32_t)g.res >> 2, q3 = 3u * q1;
+                const bool inner = lx >= q1 && lx + w <= q3 && ly >= q1 && ly + w <= q3 && lz >= q1 && lz + w <= q3;
+                t = __fadd_rn(t, dt);
+                if (!inner || k == 0 || !(g.cell[k - 1] > dt_net)) {
+                    const float ls = g.ls[k];
+                    float ix0, ix1, iy0, iy1, iz0, iz1;
+                    axis_window(r.ox, r.dx, r.idx, cell_boundary(lx, g.inv_res, ls),
+                                cell_boundary(lx + w, g.inv_res, ls), ls, ix0, ix1);
+                    axis_window(r.oy, r.dy, r.idy, cell_boundary(ly, g.inv_res, ls),
+                                cell_boundary(ly + w, g.inv_res, ls), ls, iy0, iy1);
+                    axis_window(r.oz, r.dz, r.idz, cell_boundary(lz, g.inv_res, ls),
+                                cell_boundary(lz + w, g.inv_res, ls), ls, iz0, iz1);
+                    const float t_in = fmaxf(ix0, fmaxf(iy0, iz0));
+                    const float t_out = fminf(fminf(ix1, fminf(iy1, iz1)), tmax);
+                    if (t >= t_in) {
+                        while (t <= t_out && iters < max_iters) {
+                            t = __fadd_rn(t, get_dt(t, A.cone, A.dt_min, A.dt_max));
+                            ++iters;
+                        }
+                    }
+                }
+                continue;
+            }
+        }
+        t = __fadd_rn(t, dt);
+    }
+    t_io = t;
+    return {c, done, iters, tests};
+}
+
+// One round of every live ray: counts[j] valid samples with their t in slots[c * n_live + j],
+// the ray's t advanced; keep[j] = 0 once the ray has passed t_max.
+__global__ void render_walk_kernel(RenderArgs A, uint32_t n, uint32_t n_live, uint32_t quota,
+                                   const uint32_t* __restrict__ live, const float* __restrict__ ori,
+                                   const float* __restrict__ dir, float* __restrict__ ray_t,
+                                   const float* __restrict__ ray_tmax, const uint8_t* __restrict__ mip,
+                                   uint32_t max_iters, uint32_t* __restrict__ counts, float* __restrict__ slots,
+                                   uint32_t* __restrict__ keep, unsigned long long* __restrict__ totals,
+                                   uint32_t* flags) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t steps = 0, tests = 0;
+    if (j < n_live) {
+        const uint32_t i = live[j];
+        RayMarch r;
+        r.ox = ori[i]; r.oy = ori[i + n]; r.oz = ori[i + 2 * (size_t)n];
+        r.dx = dir[i]; r.dy = dir[i + n]; r.dz = dir[i + 2 * (size_t)n];
+        r.idx = __fdiv_rn(1.0f, r.dx);
+        r.idy = __fdiv_rn(1.0f, r.dy);
+        r.idz = __fdiv_rn(1.0f, r.dz);
+        const float dir_len =
+            __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dy, r.dy)), __fmul_rn(r.dz, r.dz)));
+        float t = ray_t[i];
+        const WalkResult w = render_walk(A, r, dir_len, t, ray_tmax[i], quota, slots + j, n_live, mip, max_iters, flags);
+        ray_t[i] = t;
+        counts[j] = w.count;
+        keep[j] = w.done ? 0u : 1u;
+        steps = w.steps;
+        tests = w.tests;
+    }
+    // steps and tests of the round (statistics)
+    const unsigned long long ws = warp_sum((unsigned long long)steps), wt = warp_sum((unsigned long long)tests);
+    if ((threadIdx.x & 31u) == 0 && (ws | wt)) {
+        atomicAdd(totals, ws);
+        atomicAdd(totals + 1, wt);
+    }
+}
+
+// Network inputs of the round's samples, packed at offsets[j]: unit-cube position clamped to
+// [0, 1], direction 0.5 d + 0.5, and the step in units of the training box size
+// (assign_normalized_network_inputs_kernel, rendering-kernels.cu:404-478).
+__global__ void render_expand_kernel(RenderArgs A, uint32_t n, uint32_t n_live, const uint32_t* __restrict__ live,
+                                     const float* __restrict__ ori, const float* __restrict__ dir,
+                                     const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                                     const float* __restrict__ slots, uint32_t cap, float* __restrict__ s_pos,
+                                     float* __restrict__ s_dir, float* __restrict__ s_dt, uint32_t* flags) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_live) return;
     const uint32_t i = live[j];
@@ -146,39 +303,33 @@ __global__ void render_march_kernel(RenderArgs A, uint32_t n, uint32_t n_live, u
     const float dir_len =
         __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dy, r.dy)), __fmul_rn(r.dz, r.dz)));
     const float nx = __fmaf_rn(0.5f, r.dx, 0.5f), ny = __fmaf_rn(0.5f, r.dy, 0.5f), nz = __fmaf_rn(0.5f, r.dz, 0.5f);
-    float t = ray_t[i];
-    uint32_t c = 0, o = EMIT ? offsets[j] : 0u;
-    for (uint32_t s = 0; s < steps; ++s) {
-        const float dt = get_dt(t, A.cone, A.dt_min, A.dt_max);
-        const RenderSample smp = render_sample(A, r, t, dt, dir_len);
-        if (smp.valid) {
-            if (EMIT) {
-                if (o < cap) {
-                    s_pos[o] = smp.ux; s_pos[o + cap] = smp.uy; s_pos[o + 2 * (size_t)cap] = smp.uz;
-                    s_dir[o] = nx; s_dir[o + cap] = ny; s_dir[o + 2 * (size_t)cap] = nz;
-                    s_dt[o] = smp.dt_net;
-                } else {
-                    raise_flag(flags, ERR_CAPACITY);
-                }
-                ++o;
-            }
-            ++c;
-        }
-        t = __fadd_rn(t, dt);
+    const uint32_t c = counts[j], o = offsets[j];
+    if (o + c > cap) {
+        raise_flag(flags, ERR_CAPACITY);
+        return;
     }
-    if (EMIT) ray_t[i] = t;
-    else counts[j] = c;
+    for (uint32_t q = 0; q < c; ++q) {
+        const float t = slots[(size_t)q * n_live + j];
+        const float dt = get_dt(t, A.cone, A.dt_min, A.dt_max);
+        float x, y, z;
+        ray_point(r, t, x, y, z);
+        const uint32_t s = o + q;
+        s_pos[s] = clamp_ref(__fdiv_rn(__fadd_rn(x, -A.train_bbox.min_x), A.train_size_x), 0.0f, 1.0f);
+        s_pos[s + cap] = clamp_ref(__fdiv_rn(__fadd_rn(y, -A.train_bbox.min_y), A.train_size_y), 0.0f, 1.0f);
+        s_pos[s + 2 * (size_t)cap] = clamp_ref(__fdiv_rn(__fadd_rn(z, -A.train_bbox.min_z), A.train_size_z), 0.0f, 1.0f);
+        s_dir[s] = nx; s_dir[s + cap] = ny; s_dir[s + 2 * (size_t)cap] = nz;
+        s_dt[s] = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, dt));
+    }
 }
 
 // composite_samples_kernel (rendering-kernels.cu:530-618) after accumulate_nerf_samples_kernel
-// (:480-528) for one NeRF: each live ray composites its samples of this iteration in order.
-// keep[j] = 1 while the ray stays live: transmittance not below min_transmittance and t not past
-// t_max (kill_terminated_rays_kernel, :620-637).
+// (:480-528) for one NeRF: each live ray composites its samples of this round in order. keep[j]
+// (set by the walk while t has not passed t_max, kill_terminated_rays_kernel :620-637) is cleared
+// when the transmittance falls below min_transmittance.
 __global__ void render_composite_kernel(RenderArgs A, uint32_t n_live, const uint32_t* __restrict__ live,
                                         const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
                                         uint32_t cap, const float* __restrict__ density, const float* __restrict__ rgb,
-                                        const float* __restrict__ s_dt, const float* __restrict__ ray_t,
-                                        const float* __restrict__ ray_tmax, float* __restrict__ trans,
+                                        const float* __restrict__ s_dt, float* __restrict__ trans,
                                         float* __restrict__ out, uint32_t* __restrict__ keep) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_live) return;
@@ -213,7 +364,7 @@ __global__ void render_composite_kernel(RenderArgs A, uint32_t n_live, const uin
     float4 v = *px;
     v.x += orr; v.y += og; v.z += ob; v.w += oa;
     *px = v;
-    keep[j] = (alive && !(ray_t[i] > ray_tmax[i])) ? 1u : 0u;
+    if (!alive) keep[j] = 0u;
 }
 
 // next live list: the rays whose keep flag is set, in list order
@@ -272,10 +423,14 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
     A.act = net->activation;
 
     // workspace: rays [o 3 | d 3 | t | t_max | T] x n floats; pixel lists [live | live2 | counts |
-    // offsets | keep | idx] x n u32; counters (16 u32); samples [pos 3 | dir 3 | dt | density | rgb 3]
-    // x cap floats
-    const size_t ray_words = (size_t)9 * n, list_words = (size_t)6 * n, smp_words = (size_t)11 * cap;
-    st = ensure_render_ws(ctx, (ray_words + list_words + 16 + smp_words) * 4);
+    // offsets | keep | idx] x n u32; counters (16 u32); coarse mip (R^3 / 64 bytes, rounded to
+    // 16 u32); samples [slots | pos 3 | dir 3 | dt | density | rgb 3] x cap floats
+    const uint32_t res = (uint32_t)desc->grid.resolution;
+    const uint32_t mip_blocks = res >= 16 ? res * res * res / 64 : 0u;
+    const size_t ray_words = ((size_t)9 * n + 3) & ~(size_t)3, list_words = ((size_t)6 * n + 3) & ~(size_t)3;
+    const size_t mip_words = ((size_t)mip_blocks + 63) / 64 * 16;
+    const size_t smp_words = (size_t)12 * cap;
+    st = ensure_render_ws(ctx, (ray_words + list_words + 16 + mip_words + smp_words) * 4);
     if (st != TN_OK) return st;
     float* rays = reinterpret_cast<float*>(ctx->render_ws);
     float *ori = rays, *dir = rays + 3 * (size_t)n, *ray_t = rays + 6 * (size_t)n, *ray_tmax = rays + 7 * (size_t)n,
@@ -284,15 +439,26 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
     uint32_t *live = u32, *live2 = u32 + n, *counts = u32 + 2 * (size_t)n, *offsets = u32 + 3 * (size_t)n,
              *keep = u32 + 4 * (size_t)n;
     int32_t* idx = reinterpret_cast<int32_t*>(u32 + 5 * (size_t)n);
-    uint32_t* counters = u32 + list_words;  // [0] live rays, [1..4] batch info, [5] kept rays
+    // [0] live rays, [1..4] batch info, [5] kept rays, [8..11] steps and tests (two u64)
+    uint32_t* counters = u32 + list_words;
+    unsigned long long* totals = reinterpret_cast<unsigned long long*>(counters + 8);
     uint32_t* info = counters + 1;
-    float* smp = reinterpret_cast<float*>(counters + 16);
-    float *s_pos = smp, *s_dir = smp + 3 * (size_t)cap, *s_dt = smp + 6 * (size_t)cap,
-          *s_density = smp + 7 * (size_t)cap, *s_rgb = smp + 8 * (size_t)cap;
+    uint8_t* mip = mip_blocks ? reinterpret_cast<uint8_t*>(counters + 16) : nullptr;
+    float* smp = reinterpret_cast<float*>(counters + 16 + mip_words);
+    float *slots = smp, *s_pos = smp + (size_t)cap, *s_dir = smp + 4 * (size_t)cap, *s_dt = smp + 7 * (size_t)cap,
+          *s_density = smp + 8 * (size_t)cap, *s_rgb = smp + 9 * (size_t)cap;
+    TN_REQUIRE(!mip_blocks || ((uintptr_t)desc->bitfield & 15u) == 0, TN_E_INVALID,
+               "tn_render: bitfield must be 16-byte aligned");
+    const uint32_t max_iters = 1u << 24;  // steps of one ray in one round
 
     tn_render_stats S{};
     st = cuda_status(cudaMemsetAsync(out_rgba, 0, (size_t)n * 16, stream), "tn_render(clear)");
     if (st == TN_OK) st = cuda_status(cudaMemsetAsync(counters, 0, 64, stream), "tn_render(counters)");
+    if (st == TN_OK && mip_blocks) {
+        render_mip_kernel<<<(mip_blocks + 255) / 256, 256, 0, stream>>>(
+            mip_blocks, reinterpret_cast<const uint4*>(desc->bitfield), mip);
+        st = check_launch("tn_render(mip)");
+    }
     if (st == TN_OK) {
         render_rays_kernel<<<(n + 255) / 256, 256, 0, stream>>>(n, *camera, desc->render_bbox, ori, dir, ray_t,
                                                                 ray_tmax, trans, keep);
@@ -305,23 +471,25 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
         st = cuda_status(cudaMemcpyAsync(&n_live, counters, 4, cudaMemcpyDeviceToHost, stream), "tn_render(hits)");
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(stream), "tn_render(sync)");
     S.rays_hit = n_live;
-    const uint32_t max_iters = 1u << 20;
-    while (st == TN_OK && n_live > 0 && S.iterations < max_iters) {
-        const uint32_t steps = std::max(batch / n_live, 1u);  // renderer.cu:301
+    const uint32_t max_rounds = 1u << 20;
+    while (st == TN_OK && n_live > 0 && S.iterations < max_rounds) {
+        // each live ray collects up to `quota` valid samples this round (the reference's round is
+        // max(batch / live rays, 1) steps, renderer.cu:301)
+        const uint32_t quota = std::max(batch / n_live, 1u);
         const int grid = (int)((n_live + 255) / 256);
-        render_march_kernel<false><<<grid, 256, 0, stream>>>(A, n, n_live, steps, live, ori, dir, ray_t, counts,
-                                                              nullptr, cap, nullptr, nullptr, nullptr, ctx->flags);
-        st = check_launch("tn_render(count)");
+        render_walk_kernel<<<grid, 256, 0, stream>>>(A, n, n_live, quota, live, ori, dir, ray_t, ray_tmax, mip,
+                                                     max_iters, counts, slots, keep, totals, ctx->flags);
+        st = check_launch("tn_render(walk)");
         if (st == TN_OK) st = tn_scan_offsets(ctx, stream, n_live, counts, offsets, 0xffffffffu, info);
         if (st == TN_OK) {
-            render_march_kernel<true><<<grid, 256, 0, stream>>>(A, n, n_live, steps, live, ori, dir, ray_t, counts,
-                                                                 offsets, cap, s_pos, s_dir, s_dt, ctx->flags);
-            st = check_launch("tn_render(emit)");
+            render_expand_kernel<<<grid, 256, 0, stream>>>(A, n, n_live, live, ori, dir, counts, offsets, slots, cap,
+                                                           s_pos, s_dir, s_dt, ctx->flags);
+            st = check_launch("tn_render(expand)");
         }
         if (st == TN_OK) st = net->forward(net->user, stream, cap, info + 1, cap, s_pos, s_dir, s_density, s_rgb);
         if (st == TN_OK) {
             render_composite_kernel<<<grid, 256, 0, stream>>>(A, n_live, live, counts, offsets, cap, s_density, s_rgb,
-                                                              s_dt, ray_t, ray_tmax, trans, out_rgba, keep);
+                                                              s_dt, trans, out_rgba, keep);
             st = check_launch("tn_render(composite)");
         }
         if (st == TN_OK) st = tn_compact_nonzero(ctx, stream, n_live, keep, idx, counters + 5);
@@ -336,15 +504,22 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
         if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(stream), "tn_render(sync)");
         if (st != TN_OK) break;
         S.samples += host[1];
-        S.steps += (uint64_t)steps * n_live;
         ++S.iterations;
         n_live = host[4];
         std::swap(live, live2);
     }
-    if (st == TN_OK && n_live > 0) st = fail(TN_E_DEVICE, "tn_render: rays still live after %u iterations", max_iters);
+    if (st == TN_OK && n_live > 0) st = fail(TN_E_DEVICE, "tn_render: rays still live after %u rounds", max_rounds);
+    if (st == TN_OK) {
+        unsigned long long tot[2] = {0, 0};
+        st = cuda_status(cudaMemcpyAsync(tot, totals, sizeof(tot), cudaMemcpyDeviceToHost, stream), "tn_render(stats)");
+        if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(stream), "tn_render(sync)");
+        S.steps = tot[0];
+        S.tests = tot[1];
+    }
     uint32_t flags = 0;
     if (st == TN_OK) st = tn_ctx_check(ctx, stream, &flags);
     if (st == TN_OK && (flags & TN_FLAG_CAPACITY)) st = fail(TN_E_CAPACITY, "tn_render: sample capacity exceeded");
+    if (st == TN_OK && (flags & TN_FLAG_GUARD)) st = fail(TN_E_DEVICE, "tn_render: a ray took over %u steps in a round", max_iters);
     if (stats) *stats = S;
     return st;
 }

@@ -136,7 +136,7 @@ class RenderDescC(ctypes.Structure):
 
 class RenderStatsC(ctypes.Structure):
     _fields_ = [("rays_hit", ctypes.c_uint32), ("iterations", ctypes.c_uint32), ("samples", ctypes.c_uint64),
-                ("steps", ctypes.c_uint64)]
+                ("steps", ctypes.c_uint64), ("tests", ctypes.c_uint64)]
 
 
 class TrainingMetricsC(ctypes.Structure):

@@ -230,7 +230,7 @@ class Renderer:
              int(self.batch_size), ctypes.c_void_p(dev.data_ptr()), ctypes.byref(stats))
         out._finish(dev)
         request.stats = {"rays_hit": int(stats.rays_hit), "iterations": int(stats.iterations),
-                         "samples": int(stats.samples), "steps": int(stats.steps)}
+                         "samples": int(stats.samples), "steps": int(stats.steps), "tests": int(stats.tests)}
         if request.on_progress:
             request.on_progress(1.0)
         if request.on_complete:

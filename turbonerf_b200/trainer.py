@@ -91,7 +91,7 @@ class Trainer:
                  n_rays_per_step: int = 1 << 14, occupancy_cells_per_step: int = 0,
                  distortion_lambda: float = 0.01, occupancy_threshold: float = 0.01 * MIN_STEP_SIZE,
                  n_grid_params: int = 16 * (1 << 19) * 2, n_mlp_params: int = 7168, beta2: float = 0.999,
-                 max_steps_per_ray: int = 0, seed: int = 0x7B0):
+                 max_steps_per_ray: int = 0, seed: int = 0x7B0, min_transmittance: float = 1e-4):
         if path not in ("fused", "plain"):
             raise ValueError("path must be 'fused' or 'plain'")
         self.nerf = nerf
@@ -106,6 +106,7 @@ class Trainer:
         self.beta2 = beta2
         self.max_steps_per_ray = max_steps_per_ray
         self.seed = seed
+        self.min_transmittance = min_transmittance  # NeRFConstants::min_transmittance
         # reference training settings (nerf-training-controller.h:75-78)
         self.alpha_selection_threshold = 1.0
         self.alpha_selection_probability = 1.0
@@ -130,6 +131,7 @@ class Trainer:
         d.n_rays_per_step = int(self.n_rays_per_step)
         d.min_step_size = float(self.min_step_size)
         d.max_steps_per_ray = int(self.max_steps_per_ray)
+        d.min_transmittance = float(self.min_transmittance)
         d.use_distortion_loss = int(bool(self.use_distortion_loss))
         d.distortion_lambda = float(self.distortion_lambda)
         d.occupancy_threshold = float(self.occupancy_threshold)
