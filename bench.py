@@ -825,8 +825,10 @@ def run_render(args):
            "metric": "rays/s per frame (host clock around the synchronous submit)", "dtype": "f32",
            "data": "synthetic", "frames": []}
     buf = CUDARenderBuffer()
-    for (w, h) in ((800, 800), (1920, 1080)):
-        for bs in (1 << 20, 1 << 22, 1 << 24):
+    sizes = [tuple(int(v) for v in wh.split("x")) for wh in args.render_sizes.split(",")]
+    batches = [int(v) for v in args.render_batches.split(",")]
+    for (w, h) in sizes:
+        for bs in batches:
             r = Renderer(batch_size=bs)
             req = RenderRequest(cam(w, h), [tr], buf)
             for _ in range(max(args.warmup, 3)):
@@ -842,6 +844,10 @@ def run_render(args):
                                   "rays_per_s": round(w * h / (ms / 1e3), 1),
                                   "samples_per_s": round(st["samples"] / (ms / 1e3), 1),
                                   "steps_per_s": round(st["steps"] / (ms / 1e3), 1), **st})
+    if args.no_cpu:
+        tr.teardown()
+        print(json.dumps(out), flush=True)
+        return
     # CPU oracle on a 200 x 200 frame of the same view, and the GPU frame it is compared with
     c = cam(200, 200)
     od = dict(width=200, height=200, near=c.near, far=c.far, focal=c.focal_length, principal=c.principal_point,
@@ -872,6 +878,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--render-sizes", default="800x800,1920x1080", help="render workload: frame sizes WxH")
+    ap.add_argument("--render-batches", default="1048576,4194304,16777216",
+                    help="render workload: sample budgets per round")
     ap.add_argument("--workload", default="train-step",
                     choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "

@@ -23,6 +23,8 @@
 // Output: premultiplied RGBA per pixel, interleaved (pixel i at out[4 i .. 4 i + 3]), the layout
 // the reference copies into its render target (copy_packed_rgba_linear_buffer_kernel).
 #include <algorithm>
+#include <cmath>
+#include <cstring>
 
 #include "tn_internal.cuh"
 
@@ -36,7 +38,27 @@ struct RenderArgs {
     float cone, dt_min, dt_max;
     float min_t;
     int act;
+    // level choice from float bit patterns (valid when level k's half extent and cell size are
+    // level 0's times 2^k exactly, checked on the host): see render_level
+    int fast_level;
+    int half0_bits, cell0_bits;
 };
+
+// get_grid_level_at (occupancy-grid.cuh:232-248): the finest level whose extent holds the point
+// (max |coordinate| m < half extent) and whose cell is larger than the step, else the coarsest.
+// Both conditions turn true at some level and stay true above it. For positive floats the order
+// of values is the order of bit patterns and level j's constants are level 0's patterns plus
+// j << 23, so m < half0 2^j <=> j > (bits(m) - bits(half0)) >> 23 (an arithmetic shift is the
+// floor), likewise for the step; the level is the larger first level, clamped to the grid.
+__device__ __forceinline__ int render_level(const RenderArgs& A, float x, float y, float z, float dt) {
+    if (A.fast_level) {
+        const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));
+        const int jp = (__float_as_int(m) - A.half0_bits) >> 23;
+        const int jd = (__float_as_int(dt) - A.cell0_bits) >> 23;
+        return min(max(max(jp, jd) + 1, 0), A.g.n_levels - 1);
+    }
+    return grid_level_at(A.g, x, y, z, dt);
+}
 
 // sigma of a network density output (TN_ACT_DENSITY: density_to_sigma,
 // common-network-kernels.cuh:7-10) and the opacity 1 - exp(-sigma dt) of one step
@@ -175,7 +197,8 @@ struct WalkResult {
 
 __device__ WalkResult render_walk(const RenderArgs& A, const RayMarch& r, float dir_len, float& t_io, float tmax,
                                   uint32_t quota, float* __restrict__ slots, uint32_t stride,
-                                  const uint8_t* __restrict__ mip, uint32_t max_iters, uint32_t* flags) {
+                                  const uint8_t* __restrict__ mip, const uint32_t* __restrict__ spread,
+                                  uint32_t max_iters, uint32_t* flags) {
     const GridView& g = A.g;
     const float dtn_max = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, A.dt_max));
     const bool cells_ok = g.res >= 4, blocks_ok = g.res >= 16 && mip != nullptr;
@@ -198,15 +221,19 @@ __device__ WalkResult render_walk(const RenderArgs& A, const RayMarch& r, float 
         ++tests;
         if (bbox_contains(A.render_bbox, x, y, z)) {
             const float dt_net = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, dt));
-            const int k = grid_level_at(g, x, y, z, dt_net);
+            const int k = render_level(A, x, y, z, dt_net);
             const float s = g.inv_ls[k];
             const float fx = __fmul_rn(__fadd_rn(__fmul_rn(x, s), 0.5f), g.res_f);
             const float fy = __fmul_rn(__fadd_rn(__fmul_rn(y, s), 0.5f), g.res_f);
             const float fz = __fmul_rn(__fadd_rn(__fmul_rn(z, s), 0.5f), g.res_f);
-            const uint32_t cx = cell_coord(x, s, g.res_f, g.res), cy = cell_coord(y, s, g.res_f, g.res),
-                           cz = cell_coord(z, s, g.res_f, g.res);
-            const uint32_t idx = morton3d(cx, cy, cz);
-            if ((__ldg(g.bits + idx) >> k) & 1u) {
+            // cell coordinates of get_voxel_morton_index, clamped to the grid (cell_coord)
+            const uint32_t rm1 = (uint32_t)g.res - 1u;
+            const uint32_t cx = min(__float2uint_rz(fx), rm1), cy = min(__float2uint_rz(fy), rm1),
+                           cz = min(__float2uint_rz(fz), rm1);
+            const uint32_t idx = spread[cx] | spread[g.res + cy] | spread[2 * g.res + cz];
+            // the coarse mip first: an empty block needs no read of the bitfield
+            const bool block_on = !blocks_ok || ((__ldg(mip + (idx >> 6)) >> k) & 1u);
+            if (block_on && ((__ldg(g.bits + idx) >> k) & 1u)) {
                 const float ux = __fdiv_rn(__fadd_rn(x, -A.train_bbox.min_x), A.train_size_x);
                 const float uy = __fdiv_rn(__fadd_rn(y, -A.train_bbox.min_y), A.train_size_y);
                 const float uz = __fdiv_rn(__fadd_rn(z, -A.train_bbox.min_z), A.train_size_z);
@@ -217,7 +244,7 @@ __device__ WalkResult render_walk(const RenderArgs& A, const RayMarch& r, float 
             } else if (cells_ok && fx >= 0.0f && fx < g.res_f && fy >= 0.0f && fy < g.res_f && fz >= 0.0f &&
                        fz < g.res_f && (k == g.n_levels - 1 || dtn_max < g.cell[k])) {
                 // the empty box: the block when the mip says it is empty, else the cell
-                const int sh = (blocks_ok && !((__ldg(mip + (idx >> 6)) >> k) & 1u)) ? 2 : 0;
+                const int sh = block_on ? 0 : 2;
                 const uint32_t lx = (cx >> sh) << sh, ly = (cy >> sh) << sh, lz = (cz >> sh) << sh;
                 const uint32_t w = 1u << sh, q1 = (uint32_t)g.res >> 2, q3 = 3u * q1;
                 const bool inner = lx >= q1 && lx + w <= q3 && ly >= q1 && ly + w <= q3 && lz >= q1 && lz + w <= q3;
@@ -258,6 +285,16 @@ __global__ void render_walk_kernel(RenderArgs A, uint32_t n, uint32_t n_live, ui
                                    uint32_t max_iters, uint32_t* __restrict__ counts, float* __restrict__ slots,
                                    uint32_t* __restrict__ keep, unsigned long long* __restrict__ totals,
                                    uint32_t* flags) {
+    // Morton spread tables (get_voxel_morton_index), one per axis, pre-shifted: 3 R words
+    extern __shared__ uint32_t spread[];
+    const uint32_t R = (uint32_t)A.g.res;
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        const uint32_t v = part1by2(c);
+        spread[c] = v;
+        spread[R + c] = v << 1;
+        spread[2 * R + c] = v << 2;
+    }
+    __syncthreads();
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t steps = 0, tests = 0;
     if (j < n_live) {
@@ -271,7 +308,8 @@ __global__ void render_walk_kernel(RenderArgs A, uint32_t n, uint32_t n_live, ui
         const float dir_len =
             __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dy, r.dy)), __fmul_rn(r.dz, r.dz)));
         float t = ray_t[i];
-        const WalkResult w = render_walk(A, r, dir_len, t, ray_tmax[i], quota, slots + j, n_live, mip, max_iters, flags);
+        const WalkResult w =
+            render_walk(A, r, dir_len, t, ray_tmax[i], quota, slots + j, n_live, mip, spread, max_iters, flags);
         ray_t[i] = t;
         counts[j] = w.count;
         keep[j] = w.done ? 0u : 1u;
@@ -286,39 +324,73 @@ __global__ void render_walk_kernel(RenderArgs A, uint32_t n, uint32_t n_live, ui
     }
 }
 
+// A warp owns 32 consecutive live rays, whose samples are one contiguous range of the packed
+// batch (the offsets are the exclusive scan of the counts in live order): ray_of_sample finds the
+// lane whose range holds sample s, the largest r with off[r] <= s, by binary search over the
+// warp's offsets in shared memory (lanes past the last live ray hold UINT32_MAX).
+constexpr int RW_WARPS = 8;  // warps per block of the expand and composite kernels
+
+__device__ __forceinline__ int ray_of_sample(const uint32_t* off, uint32_t s) {
+    int r = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1)
+        if (off[r + step] <= s) r += step;
+    return r;
+}
+
 // Network inputs of the round's samples, packed at offsets[j]: unit-cube position clamped to
 // [0, 1], direction 0.5 d + 0.5, and the step in units of the training box size
-// (assign_normalized_network_inputs_kernel, rendering-kernels.cu:404-478).
-__global__ void render_expand_kernel(RenderArgs A, uint32_t n, uint32_t n_live, const uint32_t* __restrict__ live,
-                                     const float* __restrict__ ori, const float* __restrict__ dir,
-                                     const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                                     const float* __restrict__ slots, uint32_t cap, float* __restrict__ s_pos,
-                                     float* __restrict__ s_dir, float* __restrict__ s_dt, uint32_t* flags) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n_live) return;
-    const uint32_t i = live[j];
-    RayMarch r;
-    r.ox = ori[i]; r.oy = ori[i + n]; r.oz = ori[i + 2 * (size_t)n];
-    r.dx = dir[i]; r.dy = dir[i + n]; r.dz = dir[i + 2 * (size_t)n];
-    const float dir_len =
-        __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dy, r.dy)), __fmul_rn(r.dz, r.dz)));
-    const float nx = __fmaf_rn(0.5f, r.dx, 0.5f), ny = __fmaf_rn(0.5f, r.dy, 0.5f), nz = __fmaf_rn(0.5f, r.dz, 0.5f);
-    const uint32_t c = counts[j], o = offsets[j];
-    if (o + c > cap) {
-        raise_flag(flags, ERR_CAPACITY);
+// (assign_normalized_network_inputs_kernel, rendering-kernels.cu:404-478). One thread per
+// sample of the warp's range, so consecutive lanes write consecutive samples.
+__global__ void __launch_bounds__(32 * RW_WARPS)
+render_expand_kernel(RenderArgs A, uint32_t n, uint32_t n_live, const uint32_t* __restrict__ live,
+                     const float* __restrict__ ori, const float* __restrict__ dir, const uint32_t* __restrict__ counts,
+                     const uint32_t* __restrict__ offsets, const float* __restrict__ slots, uint32_t cap,
+                     float* __restrict__ s_pos, float* __restrict__ s_dir, float* __restrict__ s_dt, uint32_t* flags) {
+    __shared__ uint32_t sh_off[RW_WARPS][32];
+    __shared__ float sh_ray[RW_WARPS][7][32];  // o 3 | d 3 | |d|
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t j0 = (blockIdx.x * RW_WARPS + w) * 32u;
+    if (j0 >= n_live) return;  // the whole warp leaves
+    const uint32_t j = j0 + lane;
+    uint32_t off = 0xFFFFFFFFu, end = 0;
+    if (j < n_live) {
+        const uint32_t i = live[j];
+        off = offsets[j];
+        end = off + counts[j];
+        const float dx = dir[i], dy = dir[i + n], dz = dir[i + 2 * (size_t)n];
+        sh_ray[w][0][lane] = ori[i];
+        sh_ray[w][1][lane] = ori[i + n];
+        sh_ray[w][2][lane] = ori[i + 2 * (size_t)n];
+        sh_ray[w][3][lane] = dx;
+        sh_ray[w][4][lane] = dy;
+        sh_ray[w][5][lane] = dz;
+        sh_ray[w][6][lane] = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+    }
+    sh_off[w][lane] = off;
+    const uint32_t last = min(31u, n_live - 1u - j0);
+    const uint32_t base = __shfl_sync(FULL_MASK, off, 0), stop = __shfl_sync(FULL_MASK, end, last);
+    __syncwarp();
+    if (stop > cap) {
+        if (lane == 0) raise_flag(flags, ERR_CAPACITY);
         return;
     }
-    for (uint32_t q = 0; q < c; ++q) {
-        const float t = slots[(size_t)q * n_live + j];
+    for (uint32_t s = base + lane; s < stop; s += 32) {
+        const int r = ray_of_sample(sh_off[w], s);
+        const float t = slots[(size_t)(s - sh_off[w][r]) * n_live + j0 + r];
+        RayMarch ray;
+        ray.ox = sh_ray[w][0][r]; ray.oy = sh_ray[w][1][r]; ray.oz = sh_ray[w][2][r];
+        ray.dx = sh_ray[w][3][r]; ray.dy = sh_ray[w][4][r]; ray.dz = sh_ray[w][5][r];
         const float dt = get_dt(t, A.cone, A.dt_min, A.dt_max);
         float x, y, z;
-        ray_point(r, t, x, y, z);
-        const uint32_t s = o + q;
+        ray_point(ray, t, x, y, z);
         s_pos[s] = clamp_ref(__fdiv_rn(__fadd_rn(x, -A.train_bbox.min_x), A.train_size_x), 0.0f, 1.0f);
         s_pos[s + cap] = clamp_ref(__fdiv_rn(__fadd_rn(y, -A.train_bbox.min_y), A.train_size_y), 0.0f, 1.0f);
         s_pos[s + 2 * (size_t)cap] = clamp_ref(__fdiv_rn(__fadd_rn(z, -A.train_bbox.min_z), A.train_size_z), 0.0f, 1.0f);
-        s_dir[s] = nx; s_dir[s + cap] = ny; s_dir[s + 2 * (size_t)cap] = nz;
-        s_dt[s] = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, dt));
+        s_dir[s] = __fmaf_rn(0.5f, ray.dx, 0.5f);
+        s_dir[s + cap] = __fmaf_rn(0.5f, ray.dy, 0.5f);
+        s_dir[s + 2 * (size_t)cap] = __fmaf_rn(0.5f, ray.dz, 0.5f);
+        s_dt[s] = __fmul_rn(A.inv_train_size, __fmul_rn(sh_ray[w][6][r], dt));
     }
 }
 
@@ -326,39 +398,66 @@ __global__ void render_expand_kernel(RenderArgs A, uint32_t n, uint32_t n_live, 
 // (:480-528) for one NeRF: each live ray composites its samples of this round in order. keep[j]
 // (set by the walk while t has not passed t_max, kill_terminated_rays_kernel :620-637) is cleared
 // when the transmittance falls below min_transmittance.
-__global__ void render_composite_kernel(RenderArgs A, uint32_t n_live, const uint32_t* __restrict__ live,
-                                        const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                                        uint32_t cap, const float* __restrict__ density, const float* __restrict__ rgb,
-                                        const float* __restrict__ s_dt, float* __restrict__ trans,
-                                        float* __restrict__ out, uint32_t* __restrict__ keep) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n_live) return;
-    const uint32_t i = live[j];
-    float T = trans[i];
+// The warp walks its sample range in chunks of RC_CHUNK: all lanes load a chunk with coalesced
+// reads and compute each sample's opacity, then each lane composites its own ray's samples of the
+// chunk in order from shared memory.
+constexpr int RC_CHUNK = 128;
+
+__global__ void __launch_bounds__(32 * RW_WARPS)
+render_composite_kernel(RenderArgs A, uint32_t n_live, const uint32_t* __restrict__ live,
+                        const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, uint32_t cap,
+                        const float* __restrict__ density, const float* __restrict__ rgb,
+                        const float* __restrict__ s_dt, float* __restrict__ trans, float* __restrict__ out,
+                        uint32_t* __restrict__ keep) {
+    __shared__ float sh[RW_WARPS][4][RC_CHUNK];  // alpha | r | g | b
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t j0 = (blockIdx.x * RW_WARPS + w) * 32u;
+    if (j0 >= n_live) return;  // the whole warp leaves
+    const uint32_t j = j0 + lane;
+    const bool has = j < n_live;
+    uint32_t i = 0, off = 0, end = 0;
+    float T = 1.0f;
+    if (has) {
+        i = live[j];
+        off = offsets[j];
+        end = min(off + counts[j], cap);
+        T = trans[i];
+    }
+    const uint32_t last = min(31u, n_live - 1u - j0);
+    const uint32_t base = __shfl_sync(FULL_MASK, off, 0), stop = min(__shfl_sync(FULL_MASK, end, last), cap);
     float orr = 0.0f, og = 0.0f, ob = 0.0f, oa = 0.0f;
     bool alive = true;
-    const uint32_t o = offsets[j];
-    const uint32_t c = o < cap ? min(counts[j], cap - o) : 0u;
-    for (uint32_t k = 0; k < c; ++k) {
-        const uint32_t s = o + k;
-        const float alpha = render_alpha(__fmul_rn(render_sigma(A.act, density[s]), s_dt[s]));
-        // one NeRF's sample colour: (c alpha) / alpha, zero when alpha <= 1e-4
-        const float inv_a = alpha > 0.0001f ? __fdiv_rn(1.0f, alpha) : 0.0f;
-        const float cr = __fmul_rn(__fmul_rn(rgb[s], alpha), inv_a);
-        const float cg = __fmul_rn(__fmul_rn(rgb[s + cap], alpha), inv_a);
-        const float cb = __fmul_rn(__fmul_rn(rgb[s + 2 * (size_t)cap], alpha), inv_a);
-        const float a = fminf(alpha, 1.0f);
-        const float w = __fmul_rn(a, T);
-        orr = __fadd_rn(orr, __fmul_rn(w, cr));
-        og = __fadd_rn(og, __fmul_rn(w, cg));
-        ob = __fadd_rn(ob, __fmul_rn(w, cb));
-        oa = __fadd_rn(oa, w);
-        T = __fmul_rn(T, __fadd_rn(1.0f, -a));
-        if (T < A.min_t) {
-            alive = false;
-            break;
+    for (uint32_t c0 = base; c0 < stop; c0 += RC_CHUNK) {
+        const uint32_t cn = min((uint32_t)RC_CHUNK, stop - c0);
+        for (uint32_t q = lane; q < cn; q += 32) {
+            const uint32_t s = c0 + q;
+            sh[w][0][q] = render_alpha(__fmul_rn(render_sigma(A.act, density[s]), s_dt[s]));
+            sh[w][1][q] = rgb[s];
+            sh[w][2][q] = rgb[s + cap];
+            sh[w][3][q] = rgb[s + 2 * (size_t)cap];
         }
+        __syncwarp();
+        const uint32_t lo = max(off, c0), hi = min(end, c0 + cn);
+        for (uint32_t s = lo; alive && s < hi; ++s) {
+            const uint32_t q = s - c0;
+            const float alpha = sh[w][0][q];
+            // one NeRF's sample colour: (c alpha) / alpha, zero when alpha <= 1e-4
+            const float inv_a = alpha > 0.0001f ? __fdiv_rn(1.0f, alpha) : 0.0f;
+            const float cr = __fmul_rn(__fmul_rn(sh[w][1][q], alpha), inv_a);
+            const float cg = __fmul_rn(__fmul_rn(sh[w][2][q], alpha), inv_a);
+            const float cb = __fmul_rn(__fmul_rn(sh[w][3][q], alpha), inv_a);
+            const float a = fminf(alpha, 1.0f);
+            const float wt = __fmul_rn(a, T);
+            orr = __fadd_rn(orr, __fmul_rn(wt, cr));
+            og = __fadd_rn(og, __fmul_rn(wt, cg));
+            ob = __fadd_rn(ob, __fmul_rn(wt, cb));
+            oa = __fadd_rn(oa, wt);
+            T = __fmul_rn(T, __fadd_rn(1.0f, -a));
+            if (T < A.min_t) alive = false;
+        }
+        __syncwarp();
     }
+    if (!has) return;
     trans[i] = T;
     float4* px = reinterpret_cast<float4*>(out) + i;
     float4 v = *px;
@@ -421,6 +520,17 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
     A.dt_max = 8.0f * desc->dt_min;  // renderer.cu:305
     A.min_t = desc->min_transmittance;
     A.act = net->activation;
+    {
+        // the bit-pattern level choice needs every level's constants to be level 0's times 2^k
+        auto bits_of = [](float f) { int b; memcpy(&b, &f, 4); return b; };
+        A.half0_bits = bits_of(A.g.half[0]);
+        A.cell0_bits = bits_of(A.g.cell[0]);
+        bool ok = std::isnormal(A.g.half[0]) && std::isnormal(A.g.cell[0]) && A.g.half[0] > 0.0f && A.g.cell[0] > 0.0f;
+        for (int k = 0; k < A.g.n_levels; ++k)
+            ok = ok && bits_of(A.g.half[k]) == A.half0_bits + (k << 23) && bits_of(A.g.cell[k]) == A.cell0_bits + (k << 23);
+        A.fast_level = ok ? 1 : 0;
+    }
+    const size_t spread_bytes = (size_t)3 * desc->grid.resolution * sizeof(uint32_t);  // <= 12 KiB (R <= 1024)
 
     // workspace: rays [o 3 | d 3 | t | t_max | T] x n floats; pixel lists [live | live2 | counts |
     // offsets | keep | idx] x n u32; counters (16 u32); coarse mip (R^3 / 64 bytes, rounded to
@@ -477,8 +587,9 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
         // max(batch / live rays, 1) steps, renderer.cu:301)
         const uint32_t quota = std::max(batch / n_live, 1u);
         const int grid = (int)((n_live + 255) / 256);
-        render_walk_kernel<<<grid, 256, 0, stream>>>(A, n, n_live, quota, live, ori, dir, ray_t, ray_tmax, mip,
-                                                     max_iters, counts, slots, keep, totals, ctx->flags);
+        render_walk_kernel<<<grid, 256, spread_bytes, stream>>>(A, n, n_live, quota, live, ori, dir, ray_t, ray_tmax,
+                                                                mip, max_iters, counts, slots, keep, totals,
+                                                                ctx->flags);
         st = check_launch("tn_render(walk)");
         if (st == TN_OK) st = tn_scan_offsets(ctx, stream, n_live, counts, offsets, 0xffffffffu, info);
         if (st == TN_OK) {
