@@ -803,8 +803,8 @@ def run_render(args):
     """Inference render (Renderer.submit) of the train-step scene: 5 cascades of 128^3 built
     from the 8-blob field, which also stands in for the network; the camera at (0.3, 0.8, 4.0)
     looks at the centre from inside the 16-unit training box (focal 0.7 x width). Frames of
-    800 x 800 and 1920 x 1080 at sample budgets of 2^20 (the reference default), 2^22 and 2^24
-    per round. A frame is one synchronous submit (it reads the live ray count back every
+    800 x 800 and 1920 x 1080 (--render-sizes) at sample budgets per round (--render-batches) of
+    the library default (0), 2^20 (the reference default), 2^22 and 2^24. A frame is one synchronous submit (it reads the live ray count back every
     round), so frames are timed on the host clock around the call. The CPU oracle renders the
     same view at 200 x 200 on all host threads; its rays/s is the CPU baseline, and its image
     is compared with the GPU frame of the same size."""
@@ -879,8 +879,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--render-sizes", default="800x800,1920x1080", help="render workload: frame sizes WxH")
-    ap.add_argument("--render-batches", default="1048576,4194304,16777216",
-                    help="render workload: sample budgets per round")
+    ap.add_argument("--render-batches", default="0,1048576,4194304,16777216",
+                    help="render workload: sample budgets per round (0: the library default)")
     ap.add_argument("--workload", default="train-step",
                     choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "

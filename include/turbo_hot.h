@@ -470,7 +470,7 @@ typedef struct tn_render_desc {
     float dt_min;                    /* reference min_step_size; dt_max = 8 dt_min */
     float cone_angle;                /* reference NeRFConstants::cone_angle */
     float min_transmittance;         /* reference NeRFConstants::min_transmittance = 1e-4 */
-    uint32_t batch_size;             /* samples per iteration; 0 selects 1 << 20 */
+    uint32_t batch_size;             /* samples per round; 0 selects 8 per pixel within [2^20, 2^25] */
 } tn_render_desc;
 
 typedef struct tn_render_stats {
@@ -578,7 +578,7 @@ int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t);
 /* Renders the trainer's scene (its grid, training box, cone angle, transmittance cut and
  * network) with tn_render (reference NeRFRenderingController::submit,
  * src/controllers/nerf-rendering-controller.cu:50). render_bbox NULL selects the training
- * box; min_step_size <= 0 the trainer's; batch_size 0 the renderer default (1 << 20).
+ * box; min_step_size <= 0 the trainer's; batch_size 0 the tn_render default.
  * Applies a pending Adam update first. */
 int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,
                       uint32_t batch_size, float* out_rgba, tn_render_stats* stats);

@@ -93,7 +93,7 @@ def test_camera_and_png_without_gpu(tmp_path):
     cam = Camera((8, 4), 0.1, 10.0, (8, 8), (4, 2), (0.5, 0.0), np.eye(4))
     c = cam.c_struct()
     assert (c.width, c.height, c.shift_x) == (8, 4, 0.5) and list(c.transform)[:4] == [1.0, 0.0, 0.0, 0.0]
-    assert Renderer().batch_size == 1 << 20 and Renderer(batch_size=4096).batch_size == 4096
+    assert Renderer().batch_size == 0 and Renderer(batch_size=4096).batch_size == 4096
     assert Renderer(pattern=RenderPattern.HexagonalGrid).pattern == RenderPattern.HexagonalGrid
     assert int(RenderFlags.Preview | RenderFlags.Final) == 3
     buf = CPURenderBuffer()

@@ -261,6 +261,17 @@ __device__ WalkResult render_walk(const RenderArgs& A, const RayMarch& r, float 
                     const float t_in = fmaxf(ix0, fmaxf(iy0, iz0));
                     const float t_out = fminf(fminf(ix1, fminf(iy1, iz1)), tmax);
                     if (t >= t_in) {
+                        // once t cone has reached dt_max every later step is dt_max (t only grows):
+                        // four steps per window test; t is monotone, so the fourth decides
+                        if (__fmul_rn(t, A.cone) >= A.dt_max) {
+                            while (iters + 4u <= max_iters) {
+                                const float t4 = __fadd_rn(
+                                    __fadd_rn(__fadd_rn(__fadd_rn(t, A.dt_max), A.dt_max), A.dt_max), A.dt_max);
+                                if (!(t4 <= t_out)) break;
+                                t = t4;
+                                iters += 4u;
+                            }
+                        }
                         while (t <= t_out && iters < max_iters) {
                             t = __fadd_rn(t, get_dt(t, A.cone, A.dt_min, A.dt_max));
                             ++iters;
@@ -429,30 +440,30 @@ render_composite_kernel(RenderArgs A, uint32_t n_live, const uint32_t* __restric
     bool alive = true;
     for (uint32_t c0 = base; c0 < stop; c0 += RC_CHUNK) {
         const uint32_t cn = min((uint32_t)RC_CHUNK, stop - c0);
+        // per sample, in parallel: a = min(alpha, 1) and the colour of one NeRF's sample, the
+        // network colour where alpha > 1e-4 and zero below (the reference's (c alpha) / alpha,
+        // with the product and quotient, which cancel to within two roundings, left out)
         for (uint32_t q = lane; q < cn; q += 32) {
             const uint32_t s = c0 + q;
-            sh[w][0][q] = render_alpha(__fmul_rn(render_sigma(A.act, density[s]), s_dt[s]));
-            sh[w][1][q] = rgb[s];
-            sh[w][2][q] = rgb[s + cap];
-            sh[w][3][q] = rgb[s + 2 * (size_t)cap];
+            const float alpha = render_alpha(__fmul_rn(render_sigma(A.act, density[s]), s_dt[s]));
+            const bool lit = alpha > 0.0001f;
+            sh[w][0][q] = fminf(alpha, 1.0f);
+            sh[w][1][q] = lit ? rgb[s] : 0.0f;
+            sh[w][2][q] = lit ? rgb[s + cap] : 0.0f;
+            sh[w][3][q] = lit ? rgb[s + 2 * (size_t)cap] : 0.0f;
         }
         __syncwarp();
+        // per ray, in order: the transmittance chain
         const uint32_t lo = max(off, c0), hi = min(end, c0 + cn);
         for (uint32_t s = lo; alive && s < hi; ++s) {
             const uint32_t q = s - c0;
-            const float alpha = sh[w][0][q];
-            // one NeRF's sample colour: (c alpha) / alpha, zero when alpha <= 1e-4
-            const float inv_a = alpha > 0.0001f ? __fdiv_rn(1.0f, alpha) : 0.0f;
-            const float cr = __fmul_rn(__fmul_rn(sh[w][1][q], alpha), inv_a);
-            const float cg = __fmul_rn(__fmul_rn(sh[w][2][q], alpha), inv_a);
-            const float cb = __fmul_rn(__fmul_rn(sh[w][3][q], alpha), inv_a);
-            const float a = fminf(alpha, 1.0f);
-            const float wt = __fmul_rn(a, T);
-            orr = __fadd_rn(orr, __fmul_rn(wt, cr));
-            og = __fadd_rn(og, __fmul_rn(wt, cg));
-            ob = __fadd_rn(ob, __fmul_rn(wt, cb));
-            oa = __fadd_rn(oa, wt);
-            T = __fmul_rn(T, __fadd_rn(1.0f, -a));
+            const float a = sh[w][0][q];
+            const float wt = a * T;
+            orr = fmaf(wt, sh[w][1][q], orr);
+            og = fmaf(wt, sh[w][2][q], og);
+            ob = fmaf(wt, sh[w][3][q], ob);
+            oa += wt;
+            T = T * (1.0f - a);
             if (T < A.min_t) alive = false;
         }
         __syncwarp();
@@ -499,7 +510,10 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
     const uint64_t n64 = (uint64_t)camera->width * (uint64_t)camera->height;
     TN_REQUIRE(n64 <= (1u << 26), TN_E_CAPACITY, "tn_render: %llu pixels exceed 2^26", (unsigned long long)n64);
     const uint32_t n = (uint32_t)n64;
-    const uint32_t batch = desc->batch_size ? desc->batch_size : (1u << 20);  // renderer default batch
+    // 0: a budget from the image size, 8 samples per pixel within [2^20, 2^25] (the reference fixes
+    // 1 << 20 and leaves deriving it from the GPU as a to-do, nerf-rendering-controller.cu:20-23)
+    const uint32_t batch = desc->batch_size ? desc->batch_size
+                                            : (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8 * n64, 1u << 20), 1u << 25);
     TN_REQUIRE(batch <= (1u << 28), TN_E_CAPACITY, "tn_render: batch_size %u exceeds 2^28", batch);
     // live rays x steps never exceeds max(batch, live rays)
     const uint32_t cap = std::max(batch, n);

@@ -200,11 +200,13 @@ class RenderRequest:
 
 class Renderer:
     """Rendering controller (reference NeRFRenderingController, src/controllers/
-    nerf-rendering-controller.cu:16-80): batch_size 0 selects 1 << 20 samples per round."""
+    nerf-rendering-controller.cu:16-80). batch_size is the sample budget of one round (the
+    reference's 1 << 20 when asked for); 0 lets the library pick 8 samples per pixel within
+    [2^20, 2^25]. The image does not depend on it."""
 
     def __init__(self, pattern: RenderPattern = RenderPattern.LinearChunks, batch_size: int = 0):
         self.pattern = RenderPattern(pattern)
-        self.batch_size = int(batch_size) if batch_size else 1 << 20
+        self.batch_size = int(batch_size)  # 0: the library picks the budget from the image size
         self.min_step_size = MIN_STEP_SIZE
 
     def submit(self, request: RenderRequest) -> dict:
