@@ -9,8 +9,9 @@ lr 1e-2) over 16 x 2^19 x 2 hash-grid + 7168 MLP parameters with fixed sparse sy
 gradients -> occupancy EMA (decay 0.95, threshold 0.01, 2^16 random cells re-sampled).
 
 Prints ONE JSON line. `value` = samples/s of the fused, CUDA-graph-captured step with
-inputs resident in HBM; `e2e` = the same through Trainer.train_step_rays() with host rays
-copied in and the metrics read back every step; `plain` = the one-kernel-per-stage path.
+inputs resident in HBM; `e2e` = the same through Trainer.train_step_rays_pipelined() with each
+step's host rays copied in and its metrics copied back and read by the host (one step later, the
+last one inside the timed region); `plain` = the one-kernel-per-stage path.
 `--impl reference` times the CPU restatement of the reference (the oracle) instead.
 """
 from __future__ import annotations
@@ -339,13 +340,17 @@ def run_ours(args):
     s0 = tr.stat(3)
     e0.record(stream)
     wall0 = time.perf_counter()
+    # each call enqueues its step (rays in, state out) and reads the previous step's metrics;
+    # the last step's metrics are read inside the timed region
     for i in range(args.steps):
-        tr.train_step_rays(*host[i % n_batches])
+        tr.train_step_rays_pipelined(*host[i % n_batches])
+    last_m = tr.sync_metrics()
     e1.record(stream)
     e1.synchronize()
     wall = time.perf_counter() - wall0
     e_ms = e0.elapsed_time(e1)
     e_samples = tr.stat(3) - s0
+    assert last_m.step == tr.stat(5)
     te = torch.tensor([max(e_ms, wall * 1e3)], device=dev)
     ts = torch.tensor([float(e_samples)], device=dev)
     if world > 1:

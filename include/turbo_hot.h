@@ -555,6 +555,16 @@ int tn_trainer_train_step(tn_trainer* tr, tn_training_metrics* metrics);
  * (training-batch-kernels.cuh:82-187); the box clip runs on the device. */
 int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori, const float* dir,
                                const float* target_rgba, const float* bg_rgb, tn_training_metrics* metrics);
+/* The same step as tn_trainer_train_step_rays, pipelined for a training loop that feeds rays
+ * from the host: the call enqueues this step (ray copies in, the step, a copy of its state and
+ * error word out) and returns the metrics of the previous pipelined step in *previous, waiting
+ * for that step only, so the GPU always has the next step queued. previous->step = 0 on the
+ * first pipelined call (after a synchronous read: tn_trainer_sync_metrics returns the last
+ * step's metrics). A previous step's device error is reported by this call's status. The host
+ * arrays of a step must stay unchanged until the call after it returns. Fused path only. */
+int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const float* ori, const float* dir,
+                                         const float* target_rgba, const float* bg_rgb,
+                                         tn_training_metrics* previous);
 /* Runs one fused step eagerly with events between its stages and writes the stage times
  * (ms): rays, march count, march emit, network forward, losses, network backward,
  * Adam, occupancy query (cell sampling and the density network), occupancy update. */

@@ -143,3 +143,40 @@ def test_train_step_rays_host_input():
     assert m1.n_samples > 0 and m2.step == 2
     assert_bitwise(_h(tr.buffer(17)), r.ori, "uploaded origins")
     tr.teardown()
+
+
+def test_pipelined_caller_ray_steps_match_synchronous_steps():
+    """train_step_rays_pipelined returns each step's metrics one call later and leaves the
+    trainer in the state that the synchronous calls leave: the same metrics step by step and
+    the same weights, moments and grid bit for bit."""
+    import torch
+    rng = np.random.default_rng(5)
+    batches = []
+    for _ in range(3):
+        r = scenes.sphere_rays(rng, R)
+        tgt = np.concatenate([rng.uniform(0, 1, 3 * R), np.ones(R)]).astype(np.float32)
+        bg = rng.uniform(0, 1, 3 * R).astype(np.float32)
+        batches.append([torch.from_numpy(a).pin_memory() for a in (r.ori, r.dir, tgt, bg)])
+    steps = 6
+    _, a = _make()
+    sync = [a.train_step_rays(*batches[i % 3]) for i in range(steps)]
+    _, b = _make()
+    piped = []
+    for i in range(steps):
+        m = b.train_step_rays_pipelined(*batches[i % 3])
+        assert (m is None) == (i == 0)
+        if m is not None:
+            piped.append(m)
+    piped.append(b.sync_metrics())
+    assert [m.step for m in piped] == list(range(1, steps + 1))
+    for ms, mp in zip(sync, piped):
+        assert (ms.step, ms.n_rays, ms.n_samples) == (mp.step, mp.n_rays, mp.n_samples)
+        assert np.float32(ms.loss) == np.float32(mp.loss)
+    for idx, name in ((0, "weights"), (2, "first moments"), (3, "second moments"), (5, "grid density")):
+        assert_bitwise(_h(a.buffer(idx)), _h(b.buffer(idx)), name)
+    assert_bitwise(_h(a.buffer(6, np.uint8)), _h(b.buffer(6, np.uint8)), "bitfield")
+    # a synchronous read in between starts a new pipeline
+    assert b.train_step_rays_pipelined(*batches[0]) is None
+    assert b.sync_metrics().step == steps + 1
+    a.teardown()
+    b.teardown()

@@ -117,6 +117,12 @@ struct tn_trainer {
     // step state
     StepState* state = nullptr;
     StepState* state_host = nullptr;  // pinned
+    // pipelined caller-ray steps: each step's state and error word copied to pinned slots
+    // (alternating), read by the host one call later
+    StepState* ring_state = nullptr;  // pinned [2]
+    uint32_t* ring_flags = nullptr;   // pinned [2]
+    cudaEvent_t ev_ring[2] = {nullptr, nullptr};
+    uint64_t ring_calls = 0;          // pipelined calls since the last synchronous read
     cudaGraph_t graph[2] = {nullptr, nullptr};           // [synthetic rays, caller rays]
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     uint32_t graph_kernels[2] = {0, 0};
@@ -364,6 +370,19 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
     return st;
 }
 
+// Metrics of a step from its state and its error word, as read back to the host.
+int metrics_from(tn_trainer* tr, const StepState& h, uint32_t flags, tn_training_metrics* out) {
+    if (flags & TN_FLAG_NO_RAYS) return fail(TN_E_NO_RAYS, "No rays were generated for this training batch");
+    if (flags & TN_FLAG_NO_SAMPLES) return fail(TN_E_NO_SAMPLES, "No samples were generated for this training batch");
+    if (flags) return fail(TN_E_DEVICE, "device error flags 0x%x", flags);
+    tr->last.step = h.step_count;
+    tr->last.n_rays = h.batch_info[0];
+    tr->last.n_samples = h.batch_info[1];
+    tr->last.loss = h.loss_sums[0] + h.loss_sums[1];
+    if (out) *out = tr->last;
+    return TN_OK;
+}
+
 int read_state(tn_trainer* tr, tn_training_metrics* out) {
     int st = cuda_status(cudaMemcpyAsync(tr->state_host, tr->state, sizeof(StepState), cudaMemcpyDeviceToHost, tr->stream),
                          "state read");
@@ -372,16 +391,8 @@ int read_state(tn_trainer* tr, tn_training_metrics* out) {
     uint32_t flags = 0;
     st = tn_ctx_check(tr->ctx, tr->stream, &flags);
     if (st != TN_OK) return st;
-    if (flags & TN_FLAG_NO_RAYS) return fail(TN_E_NO_RAYS, "No rays were generated for this training batch");
-    if (flags & TN_FLAG_NO_SAMPLES) return fail(TN_E_NO_SAMPLES, "No samples were generated for this training batch");
-    if (flags) return fail(TN_E_DEVICE, "device error flags 0x%x", flags);
-    const StepState& h = *tr->state_host;
-    tr->last.step = h.step_count;
-    tr->last.n_rays = h.batch_info[0];
-    tr->last.n_samples = h.batch_info[1];
-    tr->last.loss = h.loss_sums[0] + h.loss_sums[1];
-    if (out) *out = tr->last;
-    return TN_OK;
+    tr->ring_calls = 0;  // every earlier step is complete; its error word is in `flags`
+    return metrics_from(tr, *tr->state_host, flags, out);
 }
 
 }  // namespace
@@ -448,7 +459,7 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     }
     st = cuda_status(cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking), "stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->aux, cudaStreamNonBlocking), "aux stream");
-    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join, &tr->ev_adam})
+    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join, &tr->ev_adam, &tr->ev_ring[0], &tr->ev_ring[1]})
         if (st == TN_OK) st = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "step events");
     if (st == TN_OK) st = tn_ctx_create(&tr->ctx);
     const uint32_t R = desc->n_rays_per_step, B = desc->batch_size;
@@ -486,6 +497,8 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     ALLOC(tr->state, 1);
 #undef ALLOC
     if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->state_host, sizeof(StepState)), "pinned state");
+    if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->ring_state, 2 * sizeof(StepState)), "pinned state ring");
+    if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->ring_flags, 2 * sizeof(uint32_t)), "pinned flag ring");
     // reference initial grid: every bit set, densities zero (occupancy-grid.cuh:81-85)
     if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->bits, 0xFF, V, tr->stream), "bitfield init");
     if (st == TN_OK) st = launch_synth_params(tr->stream, P, desc->n_grid_params, desc->seed, tr->w);
@@ -509,8 +522,10 @@ int tn_trainer_destroy(tn_trainer* tr) {
     if (tr->synth.blobs) cudaFree(tr->synth.blobs);
     if (tr->synth.waves) cudaFree(tr->synth.waves);
     if (tr->state_host) cudaFreeHost(tr->state_host);
+    if (tr->ring_state) cudaFreeHost(tr->ring_state);
+    if (tr->ring_flags) cudaFreeHost(tr->ring_flags);
     if (tr->ctx) tn_ctx_destroy(tr->ctx);
-    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join, tr->ev_adam})
+    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join, tr->ev_adam, tr->ev_ring[0], tr->ev_ring[1]})
         if (e) cudaEventDestroy(e);
     if (tr->aux) cudaStreamDestroy(tr->aux);
     if (tr->stream) cudaStreamDestroy(tr->stream);
@@ -661,6 +676,37 @@ int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori
     if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(tr->bg, row, bg_rgb, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
     if (st != TN_OK) return st;
     return train_step_impl(tr, true, metrics);
+}
+
+int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const float* ori, const float* dir,
+                                         const float* target_rgba, const float* bg_rgb,
+                                         tn_training_metrics* previous) {
+    TN_NONNULL(tr); TN_NONNULL(previous);
+    TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "pipelined steps run on the fused path");
+    int st = tn_trainer_train_step_rays(tr, n_rays, ori, dir, target_rgba, bg_rgb, nullptr);
+    if (st != TN_OK) return st;
+    cudaStream_t s = tr->stream;
+    const int slot = (int)(tr->ring_calls & 1u);
+    // this step's state and error word to its slot, the error word cleared for the next step
+    st = cuda_status(cudaMemcpyAsync(&tr->ring_state[slot], tr->state, sizeof(StepState), cudaMemcpyDeviceToHost, s),
+                     "state to ring");
+    if (st == TN_OK)
+        st = cuda_status(cudaMemcpyAsync(&tr->ring_flags[slot], tr->ctx->flags, sizeof(uint32_t),
+                                         cudaMemcpyDeviceToHost, s), "flags to ring");
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->ctx->flags, 0, sizeof(uint32_t), s), "flags clear");
+    if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_ring[slot], s), "ring event");
+    if (st != TN_OK) return st;
+    const bool has_prev = tr->ring_calls > 0;
+    ++tr->ring_calls;
+    if (!has_prev) {
+        *previous = tn_training_metrics{};  // step 0: no earlier pipelined step
+        return TN_OK;
+    }
+    // the previous step: wait for it only (this step stays queued behind it)
+    const int prev = slot ^ 1;
+    st = cuda_status(cudaEventSynchronize(tr->ev_ring[prev]), "previous step");
+    if (st != TN_OK) return st;
+    return metrics_from(tr, tr->ring_state[prev], tr->ring_flags[prev], previous);
 }
 
 int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages) {

@@ -228,6 +228,7 @@ SIGNATURES = {
     "tn_trainer_init_synthetic_gradients": [_vp, _f32, _P(_u32)],
     "tn_trainer_train_step": [_vp, _vp],
     "tn_trainer_train_step_rays": [_vp, _u32, _vp, _vp, _vp, _vp, _vp],
+    "tn_trainer_train_step_rays_pipelined": [_vp, _u32, _vp, _vp, _vp, _vp, _vp],
     "tn_trainer_profile_step": [_vp, _vp, _u32, _P(_u32)],
     "tn_trainer_stat": [_vp, _i32, _P(_u64)],
     "tn_trainer_update_occupancy_grid": [_vp, _u32, _vp],

@@ -191,6 +191,16 @@ class Trainer:
         call("tn_trainer_train_step_rays", self._handle(), self.n_rays_per_step, *arrs, ctypes.byref(m))
         return TrainingMetrics(m.step, m.loss, m.n_rays, m.n_samples)
 
+    def train_step_rays_pipelined(self, ori, dir_, target_rgba, bg_rgb) -> TrainingMetrics | None:
+        """The same step as train_step_rays for a loop that feeds rays from the host: enqueues
+        this step and returns the metrics of the previous pipelined step (None on the first
+        call), waiting for that step only. The host arrays must stay unchanged until the next
+        call returns; sync_metrics() returns the last step's metrics."""
+        m = TrainingMetricsC()
+        arrs = [self._host_ptr(a) for a in (ori, dir_, target_rgba, bg_rgb)]
+        call("tn_trainer_train_step_rays_pipelined", self._handle(), self.n_rays_per_step, *arrs, ctypes.byref(m))
+        return None if m.step == 0 else TrainingMetrics(m.step, m.loss, m.n_rays, m.n_samples)
+
     @staticmethod
     def _host_ptr(a):
         try:
