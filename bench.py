@@ -256,17 +256,14 @@ def run_ours(args):
     else:
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
-    seed = 0x7B0 + 7919 * rank
+    from turbonerf_b200.replicas import barrier, job_throughput, replica_seed
+    seed = replica_seed(0x7B0, rank)
 
     scene = _scene(0x7B0)
     tr = _trainer(scene, "fused", seed)
     stream = torch.cuda.ExternalStream(tr.stream_handle())
     # launch shapes of the march and the loss kernel, chosen on this trainer's own batch
     tuned = tr.autotune() if not args.no_autotune else {"tuning": tr.tuning}
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
 
     for _ in range(max(args.warmup, 3)):
         tr.train_step_async()
@@ -288,13 +285,7 @@ def run_ours(args):
     samples = tr.stat(3) - s0
     rays_used = last.n_rays
     kernels_per_step = tr.stat(0)
-    t = torch.tensor([ms], device=dev)
-    tot = torch.tensor([float(samples)], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    ms_max = float(t.item())
-    value = float(tot.item()) / (ms_max / 1e3)
+    value, ms_max, _ = job_throughput(ms, samples, dev)
 
     # per-stage timing (eager step with events between stages), averaged
     prof = []
@@ -351,12 +342,7 @@ def run_ours(args):
     e_ms = e0.elapsed_time(e1)
     e_samples = tr.stat(3) - s0
     assert last_m.step == tr.stat(5)
-    te = torch.tensor([max(e_ms, wall * 1e3)], device=dev)
-    ts = torch.tensor([float(e_samples)], device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
-    e2e_value = float(ts.item()) / (float(te.item()) / 1e3)
+    e2e_value, _, _ = job_throughput(max(e_ms, wall * 1e3), e_samples, dev)
     tr.teardown()
 
     # plain path (reference launch structure) on the same workload
