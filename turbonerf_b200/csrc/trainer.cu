@@ -123,6 +123,11 @@ struct tn_trainer {
     uint32_t* ring_flags = nullptr;   // pinned [2]
     cudaEvent_t ev_ring[2] = {nullptr, nullptr};
     uint64_t ring_calls = 0;          // pipelined calls since the last synchronous read
+    // pipelined steps copy their host rays into a staging buffer on a copy stream, beside the
+    // previous step; the step stream takes them from there with one device copy
+    cudaStream_t h2d = nullptr;
+    float* stage[2] = {nullptr, nullptr};
+    cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_consumed[2] = {nullptr, nullptr};
     cudaGraph_t graph[2] = {nullptr, nullptr};           // [synthetic rays, caller rays]
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     uint32_t graph_kernels[2] = {0, 0};
@@ -459,7 +464,9 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     }
     st = cuda_status(cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking), "stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->aux, cudaStreamNonBlocking), "aux stream");
-    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join, &tr->ev_adam, &tr->ev_ring[0], &tr->ev_ring[1]})
+    if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->h2d, cudaStreamNonBlocking), "copy stream");
+    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join, &tr->ev_adam, &tr->ev_ring[0], &tr->ev_ring[1],
+                           &tr->ev_staged[0], &tr->ev_staged[1], &tr->ev_consumed[0], &tr->ev_consumed[1]})
         if (st == TN_OK) st = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "step events");
     if (st == TN_OK) st = tn_ctx_create(&tr->ctx);
     const uint32_t R = desc->n_rays_per_step, B = desc->batch_size;
@@ -480,8 +487,17 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
         }
     }
 #define ALLOC(p, n) if (st == TN_OK) st = tr->alloc(p, (size_t)(n))
-    ALLOC(tr->ori, 3 * R); ALLOC(tr->dir, 3 * R); ALLOC(tr->ray_t, R); ALLOC(tr->ray_tmax, R); ALLOC(tr->target, 4 * R);
-    ALLOC(tr->bg, 3 * R); ALLOC(tr->alive, R); ALLOC(tr->n_steps, R); ALLOC(tr->offsets, R);
+    // the step's input rays in one allocation, [ori 3R | dir 3R | target 4R | bg 3R], so that a
+    // pipelined step takes them from its staging buffer in one copy
+    ALLOC(tr->ori, 13 * (size_t)R);
+    if (st == TN_OK) {
+        tr->dir = tr->ori + 3 * (size_t)R;
+        tr->target = tr->ori + 6 * (size_t)R;
+        tr->bg = tr->ori + 10 * (size_t)R;
+    }
+    ALLOC(tr->stage[0], 13 * (size_t)R); ALLOC(tr->stage[1], 13 * (size_t)R);
+    ALLOC(tr->ray_t, R); ALLOC(tr->ray_tmax, R);
+    ALLOC(tr->alive, R); ALLOC(tr->n_steps, R); ALLOC(tr->offsets, R);
     ALLOC(tr->s_t, B); ALLOC(tr->s_pos, 3 * B); ALLOC(tr->s_dir, 3 * B); ALLOC(tr->s_dt, B); ALLOC(tr->s_mnorm, B);
     ALLOC(tr->s_dtnorm, B); ALLOC(tr->net_density, B); ALLOC(tr->net_rgb, 3 * B); ALLOC(tr->grad_density, B);
     ALLOC(tr->dl_drgb, 3 * B);
@@ -525,8 +541,11 @@ int tn_trainer_destroy(tn_trainer* tr) {
     if (tr->ring_state) cudaFreeHost(tr->ring_state);
     if (tr->ring_flags) cudaFreeHost(tr->ring_flags);
     if (tr->ctx) tn_ctx_destroy(tr->ctx);
-    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join, tr->ev_adam, tr->ev_ring[0], tr->ev_ring[1]})
+    if (tr->h2d) cudaStreamSynchronize(tr->h2d);
+    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join, tr->ev_adam, tr->ev_ring[0], tr->ev_ring[1],
+                          tr->ev_staged[0], tr->ev_staged[1], tr->ev_consumed[0], tr->ev_consumed[1]})
         if (e) cudaEventDestroy(e);
+    if (tr->h2d) cudaStreamDestroy(tr->h2d);
     if (tr->aux) cudaStreamDestroy(tr->aux);
     if (tr->stream) cudaStreamDestroy(tr->stream);
     delete tr;
@@ -682,11 +701,29 @@ int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const 
                                          const float* target_rgba, const float* bg_rgb,
                                          tn_training_metrics* previous) {
     TN_NONNULL(tr); TN_NONNULL(previous);
+    TN_NONNULL(ori); TN_NONNULL(dir); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "pipelined steps run on the fused path");
-    int st = tn_trainer_train_step_rays(tr, n_rays, ori, dir, target_rgba, bg_rgb, nullptr);
-    if (st != TN_OK) return st;
+    TN_REQUIRE(n_rays == tr->R, TN_E_INVALID, "tn_trainer_train_step_rays_pipelined: n_rays must equal n_rays_per_step (%u)",
+               tr->R);
     cudaStream_t s = tr->stream;
     const int slot = (int)(tr->ring_calls & 1u);
+    // host rays to this slot's staging buffer on the copy stream, once the step two calls back has
+    // taken the slot's previous contents; the step stream waits for the copy and takes the rays
+    const size_t R = n_rays;
+    float* stg = tr->stage[slot];
+    int st = cuda_status(cudaStreamWaitEvent(tr->h2d, tr->ev_consumed[slot], 0), "staging free");
+    const float* src[4] = {ori, dir, target_rgba, bg_rgb};
+    const size_t at[4] = {0, 3 * R, 6 * R, 10 * R}, len[4] = {3 * R, 3 * R, 4 * R, 3 * R};
+    for (int k = 0; k < 4 && st == TN_OK; ++k)
+        st = cuda_status(cudaMemcpyAsync(stg + at[k], src[k], len[k] * sizeof(float), cudaMemcpyHostToDevice, tr->h2d),
+                         "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_staged[slot], tr->h2d), "staged");
+    if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_staged[slot], 0), "wait staged");
+    if (st == TN_OK)
+        st = cuda_status(cudaMemcpyAsync(tr->ori, stg, 13 * R * sizeof(float), cudaMemcpyDeviceToDevice, s), "rays D2D");
+    if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_consumed[slot], s), "consumed");
+    if (st == TN_OK) st = train_step_impl(tr, true, nullptr);
+    if (st != TN_OK) return st;
     // this step's state and error word to its slot, the error word cleared for the next step
     st = cuda_status(cudaMemcpyAsync(&tr->ring_state[slot], tr->state, sizeof(StepState), cudaMemcpyDeviceToHost, s),
                      "state to ring");
