@@ -16,8 +16,8 @@ from turbonerf_b200 import scenes
 pytestmark = pytest.mark.gpu
 
 
-def _batch(n_samples, mean, seed=0x7B1):
-    return scenes.make_sample_batch(seed, n_samples, mean=mean)
+def _batch(n_samples, mean, seed=0x7B1, max_count=1024):
+    return scenes.make_sample_batch(seed, n_samples, mean=mean, max_count=max_count)
 
 
 def _rb(sb, counts_t, offsets_t):
@@ -103,10 +103,14 @@ def test_recon_loss_fused_and_plain(act):
     assert ctx.check() == 0
 
 
-@pytest.mark.parametrize("mean,n_samples", [(48, 1 << 18), (2, 2048), (1024, 1 << 16)])
-def test_distortion_fused_and_plain(mean, n_samples):
+@pytest.mark.parametrize("mean,n_samples,max_count", [
+    (48, 1 << 18, 1024), (2, 2048, 1024), (1024, 1 << 16, 1024),
+    (64, 1 << 22, 1024),     # the compositor workload: several rays per warp, vector loads
+    (6000, 1 << 17, 20000),  # rays beyond 64 tiles of 128 samples (tile carries replayed)
+])
+def test_distortion_fused_and_plain(mean, n_samples, max_count):
     from turbonerf_b200 import hotpath as hp
-    sb = _batch(n_samples, mean, seed=0x7B3)
+    sb = _batch(n_samples, mean, seed=0x7B3, max_count=max_count)
     n, ss = sb.n_rays, sb.n_samples
     lam = 1e-3
     ctx = hp.Context()

@@ -32,7 +32,7 @@ namespace tn {
 
 constexpr int LOSS_WARPS = 8;
 constexpr int LOSS_THREADS = LOSS_WARPS * WARP;
-constexpr int SAVED_CHUNKS = 64;  // distortion chunk carries kept in registers (2 per lane)
+constexpr int SAVED_TILES = 64;  // distortion tile carries kept in lane registers (2 per lane)
 
 __device__ __forceinline__ float act_sigma(int act, float d) { return act == 0 ? d : expf(fminf(d, 12.0f) - 1.0f); }
 __device__ __forceinline__ float act_dsigma(int act, float sigma) { return act == 0 ? 1.0f : sigma; }
@@ -309,123 +309,6 @@ __device__ __forceinline__ ReconGrad recon_loss_ray(const CompFwd& c, const floa
 // which is the reference's gradient (:188-223) written without cancelling sums (m is
 // non-decreasing along a ray, so every increment m_i - m_{i-1} is >= 0).
 struct DistCarry { float x, w, a, m; };
-
-struct DistChunk {
-    float dtn, w, t_next, dm, a, sigma;
-    bool valid;
-};
-
-__device__ __forceinline__ DistChunk dist_chunk_forward(const Samples& S, uint32_t o, uint32_t n, uint32_t base,
-                                                        int lane, const DistCarry& c, DistCarry& next) {
-    DistChunk d;
-    const uint32_t j = base + lane;
-    d.valid = j < n;
-    float x = 0.0f, m = c.m;
-    d.dtn = 0.0f; d.sigma = 0.0f;
-    if (d.valid) {
-        const size_t s = (size_t)o + j;
-        d.sigma = act_sigma(S.act, S.density[s]);
-        d.dtn = S.dt_norm[s];
-        m = S.m_norm[s];
-        x = d.sigma * d.dtn;
-    }
-    const float x_incl = warp_inclusive_sum(x, lane) + c.x;
-    const float x_excl = shift_up(x_incl, lane, c.x);
-    const float em = expm1f(-x);
-    const float tj = expf(-x_excl);
-    d.w = d.valid ? tj * -em : 0.0f;
-    d.t_next = tj * (1.0f + em);  // T_j (1 - alpha_j)
-    const float w_incl = warp_inclusive_sum(d.w, lane) + c.w;
-    const float w_excl = shift_up(w_incl, lane, c.w);
-    const float m_prev = shift_up(m, lane, c.m);
-    d.dm = d.valid ? fmaxf(m - m_prev, 0.0f) : 0.0f;
-    d.a = warp_inclusive_sum(d.dm * w_excl, lane) + c.a;  // A_j
-    next.x = __shfl_sync(FULL_MASK, x_incl, WARP - 1);
-    next.w = __shfl_sync(FULL_MASK, w_incl, WARP - 1);
-    next.a = __shfl_sync(FULL_MASK, d.a, WARP - 1);
-    next.m = __shfl_sync(FULL_MASK, m, WARP - 1);
-    return d;
-}
-
-// Chunk carries of the distortion forward, distributed over lanes: chunk c lives in lane
-// (c % 32), slot c / 32 (two slots).
-struct DistCarryStore {
-    DistCarry s0, s1;
-    __device__ __forceinline__ void put(uint32_t c, int lane, const DistCarry& v) {
-        if ((uint32_t)lane == (c & 31u)) {
-            if (c < 32u) s0 = v; else if (c < 64u) s1 = v;
-        }
-    }
-    __device__ __forceinline__ DistCarry get(uint32_t c) const {
-        const int src = (int)(c & 31u);
-        const DistCarry& s = c < 32u ? s0 : s1;
-        DistCarry v;
-        v.x = __shfl_sync(FULL_MASK, s.x, src);
-        v.w = __shfl_sync(FULL_MASK, s.w, src);
-        v.a = __shfl_sync(FULL_MASK, s.a, src);
-        v.m = __shfl_sync(FULL_MASK, s.m, src);
-        return v;
-    }
-};
-
-struct DistFwd { float loss, k; };
-
-__device__ __forceinline__ DistCarry dist_first_carry(const Samples& S, uint32_t o, uint32_t n) {
-    // m_{-1} := m_0 so that the first increment is zero
-    DistCarry c{0.0f, 0.0f, 0.0f, 0.0f};
-    if (n) c.m = S.m_norm[o];
-    return c;
-}
-
-__device__ __forceinline__ DistFwd dist_forward_ray(const Samples& S, uint32_t o, uint32_t n, float lambda, int lane,
-                                                    DistCarryStore& store) {
-    DistCarry c = dist_first_carry(S, o, n);
-    float uni = 0.0f, cross = 0.0f;
-    uint32_t ci = 0;
-    for (uint32_t base = 0; base < n; base += WARP, ++ci) {
-        store.put(ci, lane, c);
-        DistCarry nx;
-        const DistChunk d = dist_chunk_forward(S, o, n, base, lane, c, nx);
-        uni += d.dtn * d.w * d.w;
-        cross += d.w * d.a;
-        c = nx;
-    }
-    uni = warp_sum(uni);
-    cross = warp_sum(cross);
-    DistFwd f;
-    f.k = n ? lambda / (float)n : 0.0f;
-    f.loss = f.k * ((1.0f / 3.0f) * uni + 2.0f * cross);
-    return f;
-}
-
-// Carry at the start of chunk `ci` (>= SAVED_CHUNKS): replay the forward from the last
-// saved chunk.
-__device__ DistCarry dist_replay_carry(const Samples& S, uint32_t o, uint32_t n, uint32_t ci, int lane,
-                                       const DistCarryStore& store) {
-    DistCarry c = store.get(SAVED_CHUNKS - 1);
-    for (uint32_t k = SAVED_CHUNKS - 1; k < ci; ++k) {
-        DistCarry nx;
-        (void)dist_chunk_forward(S, o, n, k * WARP, lane, c, nx);
-        c = nx;
-    }
-    return c;
-}
-
-// Reverse carries: W_{>=}, B (as the suffix sum of the increments' terms), sum g w.
-struct DistSuffix { float w, f, gw; };
-
-__device__ __forceinline__ float dist_chunk_backward(const DistChunk& d, float k, int lane, DistSuffix& suf) {
-    const float w_ge = warp_inclusive_suffix_sum(d.w, lane) + suf.w;       // W_{>=j}
-    const float f_incl = warp_inclusive_suffix_sum(d.dm * w_ge, lane) + suf.f;
-    const float b = shift_down(f_incl, lane, suf.f);                       // B_j
-    const float g = k * ((2.0f / 3.0f) * d.dtn * d.w + 2.0f * (d.a + b));   // dL/dw_j
-    const float gw_incl = warp_inclusive_suffix_sum(g * d.w, lane) + suf.gw;
-    const float gw_excl = shift_down(gw_incl, lane, suf.gw);               // sum_{l>j} g_l w_l
-    suf.w = __shfl_sync(FULL_MASK, w_ge, 0);
-    suf.f = __shfl_sync(FULL_MASK, f_incl, 0);
-    suf.gw = __shfl_sync(FULL_MASK, gw_incl, 0);
-    return d.valid ? d.dtn * (g * d.t_next - gw_excl) : 0.0f;
-}
 
 // ---- block-level deterministic sums (per-block partials, last block adds them) ---------
 // out[k] = scale[k] * (block-summed v[k]), additionally divided by the live ray count
@@ -870,6 +753,324 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
     }
 }
 
+// ---- distortion loss over sample tiles ------------------------------------------------------
+// The distortion loss forward and backward (mipNeRF360_distortion_loss_forward_kernel /
+// _backward_kernel, training-kernels-fused.cuh:13-224, with the sums A, B above) in the tile
+// form of the compositor: a warp owns `rpw` consecutive rays and walks their samples in tiles of
+// 32 * K, lane l owning K consecutive samples. Forward, tiles in increasing order: per sample the
+// optical depth before it, the weight w = T (1 - e^-x), the weight sum before it W_<, the
+// increment dm of m and A = sum dm W_<, each a segmented scan of the lane aggregates with a
+// carry into the next tile; the per-ray loss k (sum dtn w^2 / 3 + 2 sum w A), k = lambda / n,
+// is a segmented sum closed at the ray's last sample. The carry at each tile's start (x, w, a, m
+// of the ray open there) is kept, two tiles per lane, for the backward. Backward, tiles in
+// decreasing order: the tile's forward quantities rebuilt from its carry, then the segmented
+// suffix sums W_>=, F = sum dm W_>= (B = F of the next sample) and sum g w over later samples,
+// with g = k ((2/3) dtn w + 2 (A + B)) and dL/dsigma = dtn (g T_{j+1} - sum_{l>j} g_l w_l).
+// Tiles past the kept ones replay the forward from the last kept carry.
+
+struct DistTile {
+    float sig[ST_K], dtn[ST_K], w[ST_K], tn[ST_K], dm[ST_K], a[ST_K];
+};
+
+// Forward quantities of one tile from the carry `c` of the ray open at its start; `next` is the
+// carry at its end.
+template <bool VEC, int ACT>
+__device__ __forceinline__ void dist_tile_forward(const Samples& S, uint32_t s0, const bool (&in)[ST_K],
+                                                  const bool (&head)[ST_K], int lane, const DistCarry& c,
+                                                  DistCarry& next, DistTile& d) {
+    constexpr int K = ST_K;
+    float m[K];
+    if (VEC) {
+        bool vin = false;
+#pragma unroll
+        for (int q = 0; q < K; ++q) vin = vin || in[q];
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, e = a;
+        if (vin) {  // s0 is a multiple of 4 and the vector ends at or before the sample stride
+            a = *reinterpret_cast<const float4*>(S.density + s0);
+            b = *reinterpret_cast<const float4*>(S.dt_norm + s0);
+            e = *reinterpret_cast<const float4*>(S.m_norm + s0);
+        }
+        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w}, ev[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            d.sig[q] = in[q] ? act_sigma(ACT, av[q]) : 0.0f;
+            d.dtn[q] = in[q] ? bv[q] : 0.0f;
+            m[q] = in[q] ? ev[q] : 0.0f;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            d.sig[q] = d.dtn[q] = m[q] = 0.0f;
+            if (in[q]) {
+                d.sig[q] = act_sigma(ACT, S.density[s0 + q]);
+                d.dtn[q] = S.dt_norm[s0 + q];
+                m[q] = S.m_norm[s0 + q];
+            }
+        }
+    }
+    bool any_head = false;
+#pragma unroll
+    for (int q = 0; q < K; ++q) any_head = any_head || head[q];
+    // optical depth before each sample, weights, transmittance after each sample
+    float x[K];
+    float agg[1] = {0.0f};
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        x[q] = d.sig[q] * d.dtn[q];
+        if (head[q]) agg[0] = 0.0f;
+        agg[0] += x[q];
+    }
+    if (lane == 0 && !any_head) agg[0] += c.x;
+    seg_scan<1, false>(agg, any_head, lane);
+    float run = shift_up(agg[0], lane, c.x);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const float excl = head[q] ? 0.0f : run;
+        run = excl + x[q];
+        const float tj = expf(-excl), em = expm1f(-x[q]);
+        d.w[q] = in[q] ? tj * -em : 0.0f;
+        d.tn[q] = tj * expf(-x[q]);  // not tj (1 + em): that cancels once e^-x is small
+    }
+    next.x = __shfl_sync(FULL_MASK, agg[0], WARP - 1);
+    // weight sums before each sample
+    float wex[K];
+    agg[0] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        if (head[q]) agg[0] = 0.0f;
+        agg[0] += d.w[q];
+    }
+    if (lane == 0 && !any_head) agg[0] += c.w;
+    seg_scan<1, false>(agg, any_head, lane);
+    run = shift_up(agg[0], lane, c.w);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        wex[q] = head[q] ? 0.0f : run;
+        run = wex[q] + d.w[q];
+    }
+    next.w = __shfl_sync(FULL_MASK, agg[0], WARP - 1);
+    // increments of m (the first sample of a ray has none) and A = sum dm W_<
+    const float m_before = shift_up(m[K - 1], lane, c.m);
+    agg[0] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const float mp = head[q] ? m[q] : (q ? m[q - 1] : m_before);
+        d.dm[q] = in[q] ? fmaxf(m[q] - mp, 0.0f) : 0.0f;
+        if (head[q]) agg[0] = 0.0f;
+        agg[0] += d.dm[q] * wex[q];
+    }
+    if (lane == 0 && !any_head) agg[0] += c.a;
+    seg_scan<1, false>(agg, any_head, lane);
+    run = shift_up(agg[0], lane, c.a);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        run = (head[q] ? 0.0f : run) + d.dm[q] * wex[q];
+        d.a[q] = run;
+    }
+    next.a = __shfl_sync(FULL_MASK, agg[0], WARP - 1);
+    next.m = __shfl_sync(FULL_MASK, m[K - 1], WARP - 1);
+}
+
+// Sample flags of a tile: in range, first / last sample of its ray, and the ray's index in the
+// warp's table.
+__device__ __forceinline__ void tile_flags(const uint32_t* t_off, const uint32_t* t_end, int nr, uint32_t s_begin,
+                                           uint32_t s_end, uint32_t s0, bool (&in)[ST_K], bool (&head)[ST_K],
+                                           bool (&last)[ST_K], int (&ri)[ST_K]) {
+    int cur = find_ray(t_off, nr, s0 > s_begin ? s0 : s_begin);
+    uint32_t coff = t_off[cur], cend = t_end[cur];
+#pragma unroll
+    for (int q = 0; q < ST_K; ++q) {
+        const uint32_t s = s0 + q;
+        in[q] = s >= s_begin && s < s_end;
+        while (in[q] && s >= cend) {  // the next ray with samples
+            ++cur;
+            coff = t_off[cur];
+            cend = t_end[cur];
+        }
+        ri[q] = cur;
+        head[q] = in[q] && s == coff;
+        last[q] = in[q] && s + 1 == cend;
+    }
+}
+
+template <bool VEC, int ACT>
+__global__ void __launch_bounds__(LOSS_THREADS)
+distortion_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rpw,
+                        const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float lambda,
+                        const float* __restrict__ grad_ray, float* __restrict__ ray_loss, float* loss_sum,
+                        float* __restrict__ dd, float* partials, uint32_t* ticket) {
+    constexpr int K = ST_K;
+    __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_end[LOSS_WARPS][WARP];
+    __shared__ float t_k[LOSS_WARPS][WARP], t_gs[LOSS_WARPS][WARP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
+    float acc[1] = {0.0f};
+    if (r0 < n_live) {  // whole warps; every thread reaches the block sum below
+        const int nr = (int)min(rpw, n_live - r0);
+        if (lane < nr) {
+            const uint32_t r = r0 + lane, o = offsets[r], n = counts[r];
+            t_off[wid][lane] = o;
+            t_end[wid][lane] = o + n;
+            t_k[wid][lane] = n ? lambda / (float)n : 0.0f;
+            t_gs[wid][lane] = grad_ray ? grad_ray[r] : 1.0f;
+            if (n == 0 && ray_loss) ray_loss[r] = 0.0f;
+        }
+        __syncwarp();
+        const uint32_t s_begin = t_off[wid][0], s_end = t_end[wid][nr - 1];
+        const uint32_t b0 = VEC ? (s_begin & ~3u) : s_begin;
+        const uint32_t span = WARP * K;
+        const uint32_t n_tiles = s_end > b0 ? (s_end - b0 + span - 1) / span : 0u;
+        // forward: carries kept for the backward (tile t in lane t % 32, slot t / 32)
+        DistCarry keep0{0.0f, 0.0f, 0.0f, 0.0f}, keep1 = keep0;
+        DistCarry c{0.0f, 0.0f, 0.0f, 0.0f};
+        float cl[2] = {0.0f, 0.0f};  // running loss sums (sum dtn w^2, sum w A) of the open ray
+        for (uint32_t t = 0; t < n_tiles; ++t) {
+            if ((uint32_t)lane == (t & 31u)) {
+                if (t < 32u) keep0 = c; else if (t < 64u) keep1 = c;
+            }
+            const uint32_t s0 = b0 + t * span + (uint32_t)lane * K;
+            bool in[K], head[K], last[K];
+            int ri[K];
+            tile_flags(t_off[wid], t_end[wid], nr, s_begin, s_end, s0, in, head, last, ri);
+            DistTile d;
+            DistCarry nx;
+            dist_tile_forward<VEC, ACT>(S, s0, in, head, lane, c, nx, d);
+            bool any_head = false;
+            float l2[2] = {0.0f, 0.0f};
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                if (head[q]) { l2[0] = l2[1] = 0.0f; any_head = true; }
+                l2[0] += d.dtn[q] * d.w[q] * d.w[q];
+                l2[1] += d.w[q] * d.a[q];
+            }
+            if (lane == 0 && !any_head) { l2[0] += cl[0]; l2[1] += cl[1]; }
+            seg_scan<2, false>(l2, any_head, lane);
+            float e2[2] = {shift_up(l2[0], lane, cl[0]), shift_up(l2[1], lane, cl[1])};
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                if (head[q]) e2[0] = e2[1] = 0.0f;
+                e2[0] += d.dtn[q] * d.w[q] * d.w[q];
+                e2[1] += d.w[q] * d.a[q];
+                if (last[q]) {
+                    const float loss = t_k[wid][ri[q]] * ((1.0f / 3.0f) * e2[0] + 2.0f * e2[1]);
+                    if (ray_loss) ray_loss[r0 + (uint32_t)ri[q]] = loss;
+                    acc[0] += loss;
+                }
+            }
+            cl[0] = __shfl_sync(FULL_MASK, l2[0], WARP - 1);
+            cl[1] = __shfl_sync(FULL_MASK, l2[1], WARP - 1);
+            c = nx;
+        }
+        if (dd) {
+            // backward: tiles from the last; suffix carries of the ray open at each tile's end
+            float sw = 0.0f, sf = 0.0f, sg = 0.0f;
+            for (int t = (int)n_tiles - 1; t >= 0; --t) {
+                DistCarry ct;
+                if (t < SAVED_TILES) {
+                    const DistCarry& kc = t < 32 ? keep0 : keep1;
+                    const int src = t & 31;
+                    ct.x = __shfl_sync(FULL_MASK, kc.x, src);
+                    ct.w = __shfl_sync(FULL_MASK, kc.w, src);
+                    ct.a = __shfl_sync(FULL_MASK, kc.a, src);
+                    ct.m = __shfl_sync(FULL_MASK, kc.m, src);
+                } else {  // replay the forward from the last kept carry
+                    const int src = (SAVED_TILES - 1) & 31;
+                    ct.x = __shfl_sync(FULL_MASK, keep1.x, src);
+                    ct.w = __shfl_sync(FULL_MASK, keep1.w, src);
+                    ct.a = __shfl_sync(FULL_MASK, keep1.a, src);
+                    ct.m = __shfl_sync(FULL_MASK, keep1.m, src);
+                    for (int u = SAVED_TILES - 1; u < t; ++u) {
+                        const uint32_t su = b0 + (uint32_t)u * span + (uint32_t)lane * K;
+                        bool in[K], head[K], last[K];
+                        int ri[K];
+                        tile_flags(t_off[wid], t_end[wid], nr, s_begin, s_end, su, in, head, last, ri);
+                        DistTile du;
+                        DistCarry nx;
+                        dist_tile_forward<VEC, ACT>(S, su, in, head, lane, ct, nx, du);
+                        ct = nx;
+                    }
+                }
+                const uint32_t s0 = b0 + (uint32_t)t * span + (uint32_t)lane * K;
+                bool in[K], head[K], last[K];
+                int ri[K];
+                tile_flags(t_off[wid], t_end[wid], nr, s_begin, s_end, s0, in, head, last, ri);
+                DistTile d;
+                DistCarry nx;
+                dist_tile_forward<VEC, ACT>(S, s0, in, head, lane, ct, nx, d);
+                bool any_tail = false;
+#pragma unroll
+                for (int q = 0; q < K; ++q) any_tail = any_tail || last[q];
+                // W_>= (inclusive suffix of w)
+                float agg[1] = {0.0f};
+#pragma unroll
+                for (int q = K - 1; q >= 0; --q) {
+                    if (last[q]) agg[0] = 0.0f;
+                    agg[0] += d.w[q];
+                }
+                if (lane == WARP - 1 && !any_tail) agg[0] += sw;
+                seg_scan<1, true>(agg, any_tail, lane);
+                float run = shift_down(agg[0], lane, sw);
+                float wge[K];
+#pragma unroll
+                for (int q = K - 1; q >= 0; --q) {
+                    wge[q] = (last[q] ? 0.0f : run) + d.w[q];
+                    run = wge[q];
+                }
+                sw = __shfl_sync(FULL_MASK, agg[0], 0);
+                // B = sum over later samples of dm W_>=
+                agg[0] = 0.0f;
+#pragma unroll
+                for (int q = K - 1; q >= 0; --q) {
+                    if (last[q]) agg[0] = 0.0f;
+                    agg[0] += d.dm[q] * wge[q];
+                }
+                if (lane == WARP - 1 && !any_tail) agg[0] += sf;
+                seg_scan<1, true>(agg, any_tail, lane);
+                run = shift_down(agg[0], lane, sf);
+                float g[K];
+#pragma unroll
+                for (int q = K - 1; q >= 0; --q) {
+                    const float b = last[q] ? 0.0f : run;
+                    g[q] = t_k[wid][ri[q]] * ((2.0f / 3.0f) * d.dtn[q] * d.w[q] + 2.0f * (d.a[q] + b));
+                    run = b + d.dm[q] * wge[q];
+                }
+                sf = __shfl_sync(FULL_MASK, agg[0], 0);
+                // sum over later samples of g w, and the gradient
+                agg[0] = 0.0f;
+#pragma unroll
+                for (int q = K - 1; q >= 0; --q) {
+                    if (last[q]) agg[0] = 0.0f;
+                    agg[0] += g[q] * d.w[q];
+                }
+                if (lane == WARP - 1 && !any_tail) agg[0] += sg;
+                seg_scan<1, true>(agg, any_tail, lane);
+                run = shift_down(agg[0], lane, sg);
+                float o[K];
+#pragma unroll
+                for (int q = K - 1; q >= 0; --q) {
+                    const float later = last[q] ? 0.0f : run;
+                    o[q] = in[q] ? t_gs[wid][ri[q]] * d.dtn[q] * (g[q] * d.tn[q] - later) * act_dsigma(ACT, d.sig[q])
+                                 : 0.0f;
+                    run = later + g[q] * d.w[q];
+                }
+                sg = __shfl_sync(FULL_MASK, agg[0], 0);
+                bool all_in = true;
+#pragma unroll
+                for (int q = 0; q < K; ++q) all_in = all_in && in[q];
+                if (VEC && all_in) {
+                    *reinterpret_cast<float4*>(dd + s0) = make_float4(o[0], o[1], o[2], o[3]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < K; ++q)
+                        if (in[q]) dd[s0 + q] = o[q];
+                }
+            }
+        }
+    }
+    if (loss_sum) block_sum_and_finish<1>(acc, partials, ticket, loss_sum, FinishScale{{1.0f, 0.0f}, n_dev, n_rays, 1u});
+}
+
 // VJP of the compositor from the forward's stored per-sample transmittance (after the sample)
 // and weights, the alternative to recomputing them (composite_bwd_tiles_kernel): the same suffix
 // sums, read instead of rebuilt.
@@ -954,39 +1155,6 @@ recon_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, con
                                 });
     }
     if (loss_sum) block_sum_and_finish<1>(acc, partials, ticket, loss_sum, FinishScale{{inv_nrays, 0.0f}, nullptr, 0u, 0u});
-}
-
-__global__ void __launch_bounds__(LOSS_THREADS)
-distortion_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, const uint32_t* __restrict__ counts,
-                  const uint32_t* __restrict__ offsets, float lambda, const float* __restrict__ grad_ray,
-                  float* __restrict__ ray_loss, float* loss_sum, float* __restrict__ dd, float* partials,
-                  uint32_t* ticket) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t n_live = live_rays(n_rays, n_dev);
-    const uint32_t nw = gridDim.x * LOSS_WARPS;
-    float acc[1] = {0.0f};
-    for (uint32_t r = blockIdx.x * LOSS_WARPS + (threadIdx.x >> 5); r < n_live; r += nw) {
-        const uint32_t o = offsets[r], n = counts[r];
-        DistCarryStore store;
-        const DistFwd f = dist_forward_ray(S, o, n, lambda, lane, store);
-        if (lane == 0) {
-            if (ray_loss) ray_loss[r] = f.loss;
-            acc[0] += f.loss;
-        }
-        if (!dd || n == 0) continue;
-        const float gscale = grad_ray ? grad_ray[r] : 1.0f;
-        DistSuffix suf{0.0f, 0.0f, 0.0f};
-        const uint32_t nch = (n + WARP - 1) / WARP;
-        for (int ci = (int)nch - 1; ci >= 0; --ci) {
-            const DistCarry c = ci < SAVED_CHUNKS ? store.get((uint32_t)ci)
-                                                  : dist_replay_carry(S, o, n, (uint32_t)ci, lane, store);
-            DistCarry nx;
-            const DistChunk d = dist_chunk_forward(S, o, n, (uint32_t)ci * WARP, lane, c, nx);
-            const float g = dist_chunk_backward(d, f.k, lane, suf);
-            if (d.valid) dd[(size_t)o + (uint32_t)ci * WARP + lane] = gscale * g * act_dsigma(S.act, d.sigma);
-        }
-    }
-    if (loss_sum) block_sum_and_finish<1>(acc, partials, ticket, loss_sum, FinishScale{{1.0f, 0.0f}, n_dev, n_rays, 1u});
 }
 
 // ---- register-blocked rays -----------------------------------------------------------------
@@ -1962,12 +2130,23 @@ int tn_distortion_fwd_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* b
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, nullptr, nullptr, m_norm, dt_norm, nullptr, batch->sample_stride, activation};
-    const int grid = loss_grid((const void*)distortion_kernel, batch->n_rays);
+    const uint32_t rpw = tile_rays_per_warp(batch);
+    const int grid = tile_grid(batch->n_rays, rpw);
     st = ensure_block_f32(ctx, (size_t)grid * 2);
     if (st != TN_OK) return st;
-    distortion_kernel<<<grid, LOSS_THREADS, 0, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->counts,
-                                                         batch->offsets, lambda, grad_ray, ray_loss, loss_sum,
-                                                         dL_ddensity, ctx->block_f32, ctx->tickets + TICKET_DIST);
+    const uintptr_t al = (uintptr_t)density | (uintptr_t)m_norm | (uintptr_t)dt_norm | (uintptr_t)dL_ddensity;
+    const bool vec = (al & 15u) == 0 && (batch->sample_stride & 3u) == 0;
+#define TN_DIST_TILES(V, A)                                                                                     \
+    distortion_tiles_kernel<V, A><<<grid, LOSS_THREADS, 0, stream>>>(                                           \
+        S, batch->n_rays, batch->n_rays_dev, rpw, batch->counts, batch->offsets, lambda, grad_ray, ray_loss,     \
+        loss_sum, dL_ddensity, ctx->block_f32, ctx->tickets + TICKET_DIST)
+    switch ((vec ? 2 : 0) | (activation ? 1 : 0)) {
+        case 0: TN_DIST_TILES(false, 0); break;
+        case 1: TN_DIST_TILES(false, 1); break;
+        case 2: TN_DIST_TILES(true, 0); break;
+        default: TN_DIST_TILES(true, 1); break;
+    }
+#undef TN_DIST_TILES
     return check_launch("tn_distortion_fwd_bwd");
 }
 
