@@ -1371,7 +1371,7 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
                 const float em = expm1f(-x);
                 const float tj = expf(-(q ? p[q - 1] : before));
                 wd[q] = j0 + q < n ? tj * -em : 0.0f;
-                tnext[q] = tj * (1.0f + em);  // T_j (1 - alpha_j)
+                tnext[q] = expf(-p[q]);  // T_{j+1}; T_j (1 + em) cancels once e^-x is small
             }
         }
         {
@@ -1477,7 +1477,7 @@ __device__ __forceinline__ void sc_dist_forward(const float (&sig)[K], const flo
         const float em = expm1f(-sig[q] * dtn[q]);
         const float tj = expf(-(q ? p[q - 1] : before));
         wd[q] = j0 + q < n ? tj * -em : 0.0f;
-        tnext[q] = tj * (1.0f + em);
+        tnext[q] = expf(-p[q]);  // T_{j+1}; T_j (1 + em) cancels once e^-x is small
     }
     float W[K];
 #pragma unroll
