@@ -404,7 +404,8 @@ __device__ __forceinline__ int find_ray(const uint32_t* off, int nr, uint32_t s)
 }
 
 // Inclusive segmented scans of N values over the lanes, in increasing (SUFFIX = false) or
-// decreasing (SUFFIX = true) lane order: a lane with `cut` set starts a new segment there.
+// decreasing (SUFFIX = true) lane order: a lane with `cut` set starts a new segment there. The
+// segment flags travel with the values, so their shuffles overlap.
 template <int N, bool SUFFIX>
 __device__ __forceinline__ void seg_scan(float (&v)[N], bool cut, int lane) {
     unsigned f = cut ? 1u : 0u;
@@ -418,6 +419,39 @@ __device__ __forceinline__ void seg_scan(float (&v)[N], bool cut, int lane) {
             if (in && !f) v[k] += vo;
         }
         if (in) f |= fo;
+    }
+}
+
+// The same scans in two parts, for many scans over one set of segments (several of them
+// chained, so the flags cannot travel with every one). seg_plan records, per level of the scan (bit l for distance 2^l),
+// whether this lane adds the value from the lane that far below (above, SUFFIX): it does when
+// that lane exists and no segment start lies in between. seg_scan_plan runs a scan of N values
+// from the plan.
+template <bool SUFFIX>
+__device__ __forceinline__ uint32_t seg_plan(bool cut, int lane) {
+    unsigned f = cut ? 1u : 0u;
+    uint32_t plan = 0;
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+        const int d = 1 << l;
+        const unsigned fo = SUFFIX ? __shfl_down_sync(FULL_MASK, f, d) : __shfl_up_sync(FULL_MASK, f, d);
+        const bool in = SUFFIX ? lane + d < WARP : lane >= d;
+        if (in && !f) plan |= 1u << l;
+        if (in) f |= fo;
+    }
+    return plan;
+}
+
+template <int N, bool SUFFIX>
+__device__ __forceinline__ void seg_scan_plan(float (&v)[N], uint32_t plan) {
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+        const int d = 1 << l;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const float vo = SUFFIX ? __shfl_down_sync(FULL_MASK, v[k], d) : __shfl_up_sync(FULL_MASK, v[k], d);
+            if ((plan >> l) & 1u) v[k] += vo;
+        }
     }
 }
 
@@ -776,8 +810,8 @@ struct DistTile {
 // carry at its end.
 template <bool VEC, int ACT>
 __device__ __forceinline__ void dist_tile_forward(const Samples& S, uint32_t s0, const bool (&in)[ST_K],
-                                                  const bool (&head)[ST_K], int lane, const DistCarry& c,
-                                                  DistCarry& next, DistTile& d) {
+                                                  const bool (&head)[ST_K], bool any_head, uint32_t plan, int lane,
+                                                  const DistCarry& c, DistCarry& next, DistTile& d) {
     constexpr int K = ST_K;
     float m[K];
     if (VEC) {
@@ -808,9 +842,6 @@ __device__ __forceinline__ void dist_tile_forward(const Samples& S, uint32_t s0,
             }
         }
     }
-    bool any_head = false;
-#pragma unroll
-    for (int q = 0; q < K; ++q) any_head = any_head || head[q];
     // optical depth before each sample, weights, transmittance after each sample
     float x[K];
     float agg[1] = {0.0f};
@@ -821,15 +852,19 @@ __device__ __forceinline__ void dist_tile_forward(const Samples& S, uint32_t s0,
         agg[0] += x[q];
     }
     if (lane == 0 && !any_head) agg[0] += c.x;
-    seg_scan<1, false>(agg, any_head, lane);
+    seg_scan_plan<1, false>(agg, plan);
     float run = shift_up(agg[0], lane, c.x);
+    // T before the lane's first sample; inside a ray the transmittance before a sample is the one
+    // after the previous sample, the same exp of the same depth. After a sample it is exp(-depth),
+    // not T (1 - alpha), which cancels once e^-x is small.
+    float tj = expf(-run);
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-        const float excl = head[q] ? 0.0f : run;
-        run = excl + x[q];
-        const float tj = expf(-excl), em = expm1f(-x[q]);
-        d.w[q] = in[q] ? tj * -em : 0.0f;
-        d.tn[q] = tj * expf(-x[q]);  // not tj (1 + em): that cancels once e^-x is small
+        if (head[q]) { run = 0.0f; tj = 1.0f; }
+        run += x[q];
+        d.w[q] = in[q] ? tj * opacity(x[q]) : 0.0f;
+        d.tn[q] = expf(-run);
+        tj = d.tn[q];
     }
     next.x = __shfl_sync(FULL_MASK, agg[0], WARP - 1);
     // weight sums before each sample
@@ -841,7 +876,7 @@ __device__ __forceinline__ void dist_tile_forward(const Samples& S, uint32_t s0,
         agg[0] += d.w[q];
     }
     if (lane == 0 && !any_head) agg[0] += c.w;
-    seg_scan<1, false>(agg, any_head, lane);
+    seg_scan_plan<1, false>(agg, plan);
     run = shift_up(agg[0], lane, c.w);
 #pragma unroll
     for (int q = 0; q < K; ++q) {
@@ -860,7 +895,7 @@ __device__ __forceinline__ void dist_tile_forward(const Samples& S, uint32_t s0,
         agg[0] += d.dm[q] * wex[q];
     }
     if (lane == 0 && !any_head) agg[0] += c.a;
-    seg_scan<1, false>(agg, any_head, lane);
+    seg_scan_plan<1, false>(agg, plan);
     run = shift_up(agg[0], lane, c.a);
 #pragma unroll
     for (int q = 0; q < K; ++q) {
@@ -933,19 +968,22 @@ distortion_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint3
             bool in[K], head[K], last[K];
             int ri[K];
             tile_flags(t_off[wid], t_end[wid], nr, s_begin, s_end, s0, in, head, last, ri);
+            bool any_head = false;
+#pragma unroll
+            for (int q = 0; q < K; ++q) any_head = any_head || head[q];
+            const uint32_t plan = seg_plan<false>(any_head, lane);
             DistTile d;
             DistCarry nx;
-            dist_tile_forward<VEC, ACT>(S, s0, in, head, lane, c, nx, d);
-            bool any_head = false;
+            dist_tile_forward<VEC, ACT>(S, s0, in, head, any_head, plan, lane, c, nx, d);
             float l2[2] = {0.0f, 0.0f};
 #pragma unroll
             for (int q = 0; q < K; ++q) {
-                if (head[q]) { l2[0] = l2[1] = 0.0f; any_head = true; }
+                if (head[q]) l2[0] = l2[1] = 0.0f;
                 l2[0] += d.dtn[q] * d.w[q] * d.w[q];
                 l2[1] += d.w[q] * d.a[q];
             }
             if (lane == 0 && !any_head) { l2[0] += cl[0]; l2[1] += cl[1]; }
-            seg_scan<2, false>(l2, any_head, lane);
+            seg_scan_plan<2, false>(l2, plan);
             float e2[2] = {shift_up(l2[0], lane, cl[0]), shift_up(l2[1], lane, cl[1])};
 #pragma unroll
             for (int q = 0; q < K; ++q) {
@@ -985,9 +1023,13 @@ distortion_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint3
                         bool in[K], head[K], last[K];
                         int ri[K];
                         tile_flags(t_off[wid], t_end[wid], nr, s_begin, s_end, su, in, head, last, ri);
+                        bool any_head = false;
+#pragma unroll
+                        for (int q = 0; q < K; ++q) any_head = any_head || head[q];
                         DistTile du;
                         DistCarry nx;
-                        dist_tile_forward<VEC, ACT>(S, su, in, head, lane, ct, nx, du);
+                        dist_tile_forward<VEC, ACT>(S, su, in, head, any_head, seg_plan<false>(any_head, lane), lane,
+                                                    ct, nx, du);
                         ct = nx;
                     }
                 }
@@ -995,12 +1037,17 @@ distortion_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint3
                 bool in[K], head[K], last[K];
                 int ri[K];
                 tile_flags(t_off[wid], t_end[wid], nr, s_begin, s_end, s0, in, head, last, ri);
+                bool any_head = false, any_tail = false;
+#pragma unroll
+                for (int q = 0; q < K; ++q) {
+                    any_head = any_head || head[q];
+                    any_tail = any_tail || last[q];
+                }
                 DistTile d;
                 DistCarry nx;
-                dist_tile_forward<VEC, ACT>(S, s0, in, head, lane, ct, nx, d);
-                bool any_tail = false;
-#pragma unroll
-                for (int q = 0; q < K; ++q) any_tail = any_tail || last[q];
+                dist_tile_forward<VEC, ACT>(S, s0, in, head, any_head, seg_plan<false>(any_head, lane), lane, ct, nx,
+                                            d);
+                const uint32_t splan = seg_plan<true>(any_tail, lane);
                 // W_>= (inclusive suffix of w)
                 float agg[1] = {0.0f};
 #pragma unroll
@@ -1009,7 +1056,7 @@ distortion_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint3
                     agg[0] += d.w[q];
                 }
                 if (lane == WARP - 1 && !any_tail) agg[0] += sw;
-                seg_scan<1, true>(agg, any_tail, lane);
+                seg_scan_plan<1, true>(agg, splan);
                 float run = shift_down(agg[0], lane, sw);
                 float wge[K];
 #pragma unroll
@@ -1026,7 +1073,7 @@ distortion_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint3
                     agg[0] += d.dm[q] * wge[q];
                 }
                 if (lane == WARP - 1 && !any_tail) agg[0] += sf;
-                seg_scan<1, true>(agg, any_tail, lane);
+                seg_scan_plan<1, true>(agg, splan);
                 run = shift_down(agg[0], lane, sf);
                 float g[K];
 #pragma unroll
@@ -1044,7 +1091,7 @@ distortion_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint3
                     agg[0] += g[q] * d.w[q];
                 }
                 if (lane == WARP - 1 && !any_tail) agg[0] += sg;
-                seg_scan<1, true>(agg, any_tail, lane);
+                seg_scan_plan<1, true>(agg, splan);
                 run = shift_down(agg[0], lane, sg);
                 float o[K];
 #pragma unroll
