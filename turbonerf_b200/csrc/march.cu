@@ -168,6 +168,42 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
     return before + inc - v;
 }
 
+// Exclusive scan of the nb per-block totals in block_agg by the one block that runs it, ITEMS
+// consecutive totals per thread and one block scan per blockDim.x * ITEMS totals (the totals are
+// read with independent loads). visit(b, prefix) receives each block's 64-bit prefix, in order of
+// b within a thread; the return value is the 64-bit sum. Within one pass the sums are 32-bit, as
+// block_exclusive_scan's are.
+template <int BLOCK, int ITEMS, typename Visit>
+__device__ __forceinline__ unsigned long long scan_block_totals(uint32_t nb, const uint32_t* block_agg, Visit visit) {
+    __shared__ unsigned long long carry_s;
+    if (threadIdx.x == 0) carry_s = 0ull;
+    __syncthreads();
+    const uint32_t per_pass = blockDim.x * ITEMS;
+    for (uint32_t base = 0; base < nb; base += per_pass) {
+        const uint32_t b0 = base + threadIdx.x * ITEMS;
+        uint32_t v[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) v[j] = b0 + j < nb ? *((volatile const uint32_t*)(block_agg + b0 + j)) : 0u;
+        uint32_t sum = 0;
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t t = v[j];
+            v[j] = sum;
+            sum += t;
+        }
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<BLOCK>(sum, &tot);
+        const unsigned long long c = carry_s;
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j)
+            if (b0 + j < nb) visit(b0 + j, c + ex + v[j]);
+        __syncthreads();
+        if (threadIdx.x == 0) carry_s = c + tot;
+        __syncthreads();
+    }
+    return carry_s;
+}
+
 // Last-block epilogue of the count pass: exclusive scan of the block totals into
 // block_prefix, then the reference batch cut (src/core/trainer.cu:133-183):
 // L = last ray index whose offset < batch_size; n_rays = L; n_samples = offset[L].
@@ -176,34 +212,22 @@ template <int BLOCK = MARCH_BLOCK>
 __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t* __restrict__ counts,
                                     uint32_t* block_agg, uint32_t* block_prefix, uint32_t batch_size,
                                     uint32_t* batch_info, uint32_t* flags) {
-    __shared__ unsigned long long carry_s;
     __shared__ int last_block_s;
     __shared__ int last_ray_s;
-    if (threadIdx.x == 0) { carry_s = 0ull; last_block_s = -1; last_ray_s = -1; }
-    __syncthreads();
+    if (threadIdx.x == 0) { last_block_s = -1; last_ray_s = -1; }
     const uint32_t bs = blockDim.x;
     const uint32_t nb_live = (n_live + bs - 1) / bs;
-    for (uint32_t base = 0; base < nb; base += bs) {
-        const uint32_t b = base + threadIdx.x;
-        const uint32_t v = b < nb ? *((volatile uint32_t*)(block_agg + b)) : 0u;
-        uint32_t tot;
-        const uint32_t ex = block_exclusive_scan<BLOCK>(v, &tot);
-        const unsigned long long pre = carry_s + ex;
-        if (b < nb) {
-            block_prefix[b] = pre > 0xffffffffull ? 0xffffffffu : (uint32_t)pre;
-            if (pre > 0xffffffffull) raise_flag(flags, ERR_CAPACITY);
-            if (b < nb_live && pre < batch_size) atomicMax(&last_block_s, (int)b);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) carry_s += tot;
-        __syncthreads();
-    }
+    const unsigned long long carry = scan_block_totals<BLOCK, 4>(nb, block_agg, [&](uint32_t b, unsigned long long pre) {
+        block_prefix[b] = pre > 0xffffffffull ? 0xffffffffu : (uint32_t)pre;
+        if (pre > 0xffffffffull) raise_flag(flags, ERR_CAPACITY);
+        if (b < nb_live && pre < batch_size) atomicMax(&last_block_s, (int)b);
+    });
     const int lb = last_block_s;
     uint32_t n_rays_cut = 0, n_samples = 0;
     if (batch_size == 0xffffffffu) {
         // no cut (render / inference use): every live ray is kept
         if (threadIdx.x == 0) {
-            const unsigned long long total = carry_s;
+            const unsigned long long total = carry;
             batch_info[0] = n_live;
             batch_info[1] = total > 0xffffffffull ? 0xffffffffu : (uint32_t)total;
             batch_info[2] = batch_info[1];
@@ -230,7 +254,7 @@ __device__ void scan_blocks_and_cut(uint32_t nb, uint32_t n_live, const uint32_t
     __syncthreads();
     if (threadIdx.x == 0) {
         if (last_ray_s < 0) { batch_info[0] = 0; batch_info[1] = 0; }
-        const unsigned long long total = carry_s;
+        const unsigned long long total = carry;
         batch_info[2] = total > 0xffffffffull ? 0xffffffffu : (uint32_t)total;
         const uint32_t nr = last_ray_s < 0 ? 0u : (uint32_t)last_ray_s;
         if (nr == 0) raise_flag(flags, ERR_NO_RAYS);
@@ -939,21 +963,10 @@ compact_count_kernel(uint32_t n, const uint32_t* __restrict__ values, uint32_t* 
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    __shared__ uint32_t carry_s;
-    if (threadIdx.x == 0) carry_s = 0u;
-    __syncthreads();
-    for (uint32_t base = 0; base < gridDim.x; base += BLOCK) {
-        const uint32_t b = base + threadIdx.x;
-        const uint32_t v = b < gridDim.x ? *((volatile uint32_t*)(block_agg + b)) : 0u;
-        uint32_t tot;
-        const uint32_t ex = block_exclusive_scan<BLOCK>(v, &tot);
-        if (b < gridDim.x) block_prefix[b] = carry_s + ex;
-        __syncthreads();
-        if (threadIdx.x == 0) carry_s += tot;
-        __syncthreads();
-    }
+    const unsigned long long total = scan_block_totals<BLOCK, 4>(
+        gridDim.x, block_agg, [&](uint32_t b, unsigned long long pre) { block_prefix[b] = (uint32_t)pre; });
     if (threadIdx.x == 0) {
-        *count_dev = carry_s;
+        *count_dev = (uint32_t)total;
         *ticket = 0u;
     }
 }
