@@ -122,7 +122,8 @@ __global__ void render_rays_kernel(uint32_t n, tn_camera cam, tn_bbox box, float
 
 // Coarse occupancy: mip[m] is the OR of the 64 bitfield bytes of the 4 x 4 x 4 block of cells
 // with Morton index m (cells [64 m, 64 m + 64)), so bit k of mip[idx >> 6] is clear when the
-// whole block of cell idx is empty at level k.
+// whole block of cell idx is empty at level k. The same kernel over mip gives the 16 x 16 x 16
+// blocks: bit k of mip2[idx >> 12].
 __global__ void render_mip_kernel(uint32_t n_blocks, const uint4* __restrict__ bits, uint8_t* __restrict__ mip) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= n_blocks) return;
@@ -177,13 +178,14 @@ __device__ __forceinline__ void axis_window(float o, float d, float inv_d, float
 // the training box in unit coordinates. The t of each valid sample goes to slots[c * stride]; the
 // round ends after `quota` valid samples or once t has passed t_max (*done).
 //
-// Empty space: when a sample's cell is empty, the position's cell (or, when the coarse mip says
-// so, its whole 4 x 4 x 4 block) at that level k is empty, and the following steps are taken with
+// Empty space: when a sample's cell is empty, the position's cell (or, when the coarse mips say
+// so, its whole 4 x 4 x 4 or 16 x 16 x 16 block) at that level k is empty, and the following steps are taken with
 // the same FP32 recurrence but without tests while their positions lie inside that box with a
 // margin on every face (axis_window). Each of them would read an empty cell at level k, since the
 // level choice max(position term, step term) stays k:
 //  * inside the box the position lies inside level k's extent, so the position term is <= k;
-//  * aligned blocks (R >= 16) and cells (R >= 4) lie wholly inside or wholly outside the extent of
+//  * aligned blocks of 16^3 (R >= 64) and 4^3 (R >= 16) cells and single cells (R >= 4) lie wholly
+//    inside or wholly outside the extent of
 //    level k - 1; outside it, the position term is >= k (the margin keeps the position clear of
 //    the boundary); inside it, the step term must already be >= k at the current step;
 //  * the step term only grows along the ray, and is checked to stay <= k at the largest step
@@ -197,11 +199,12 @@ struct WalkResult {
 
 __device__ WalkResult render_walk(const RenderArgs& A, const RayMarch& r, float dir_len, float& t_io, float tmax,
                                   uint32_t quota, float* __restrict__ slots, uint32_t stride,
-                                  const uint8_t* __restrict__ mip, const uint32_t* __restrict__ spread,
-                                  uint32_t max_iters, uint32_t* flags) {
+                                  const uint8_t* __restrict__ mip, const uint8_t* __restrict__ mip2,
+                                  const uint32_t* __restrict__ spread, uint32_t max_iters, uint32_t* flags) {
     const GridView& g = A.g;
     const float dtn_max = __fmul_rn(A.inv_train_size, __fmul_rn(dir_len, A.dt_max));
     const bool cells_ok = g.res >= 4, blocks_ok = g.res >= 16 && mip != nullptr;
+    const bool supers_ok = g.res >= 64 && mip2 != nullptr;
     float t = t_io;
     uint32_t c = 0, iters = 0, tests = 0;
     bool done = false;
@@ -243,8 +246,8 @@ __device__ WalkResult render_walk(const RenderArgs& A, const RayMarch& r, float 
                 }
             } else if (cells_ok && fx >= 0.0f && fx < g.res_f && fy >= 0.0f && fy < g.res_f && fz >= 0.0f &&
                        fz < g.res_f && (k == g.n_levels - 1 || dtn_max < g.cell[k])) {
-                // the empty box: the block when the mip says it is empty, else the cell
-                const int sh = block_on ? 0 : 2;
+                // the empty box: the 16^3 or 4^3 block when the mips say it is empty, else the cell
+                const int sh = block_on ? 0 : ((supers_ok && !((__ldg(mip2 + (idx >> 12)) >> k) & 1u)) ? 4 : 2);
                 const uint32_t lx = (cx >> sh) << sh, ly = (cy >> sh) << sh, lz = (cz >> sh) << sh;
                 const uint32_t w = 1u << sh, q1 = (uint32_t)g.res >> 2, q3 = 3u * q1;
                 const bool inner = lx >= q1 && lx + w <= q3 && ly >= q1 && ly + w <= q3 && lz >= q1 && lz + w <= q3;
@@ -293,7 +296,7 @@ __global__ void render_walk_kernel(RenderArgs A, uint32_t n, uint32_t n_live, ui
                                    const uint32_t* __restrict__ live, const float* __restrict__ ori,
                                    const float* __restrict__ dir, float* __restrict__ ray_t,
                                    const float* __restrict__ ray_tmax, const uint8_t* __restrict__ mip,
-                                   uint32_t max_iters, uint32_t* __restrict__ counts, float* __restrict__ slots,
+                                   const uint8_t* __restrict__ mip2, uint32_t max_iters, uint32_t* __restrict__ counts, float* __restrict__ slots,
                                    uint32_t* __restrict__ keep, unsigned long long* __restrict__ totals,
                                    uint32_t* flags) {
     // Morton spread tables (get_voxel_morton_index), one per axis, pre-shifted: 3 R words
@@ -320,7 +323,7 @@ __global__ void render_walk_kernel(RenderArgs A, uint32_t n, uint32_t n_live, ui
             __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dy, r.dy)), __fmul_rn(r.dz, r.dz)));
         float t = ray_t[i];
         const WalkResult w =
-            render_walk(A, r, dir_len, t, ray_tmax[i], quota, slots + j, n_live, mip, spread, max_iters, flags);
+            render_walk(A, r, dir_len, t, ray_tmax[i], quota, slots + j, n_live, mip, mip2, spread, max_iters, flags);
         ray_t[i] = t;
         counts[j] = w.count;
         keep[j] = w.done ? 0u : 1u;
@@ -547,12 +550,15 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
     const size_t spread_bytes = (size_t)3 * desc->grid.resolution * sizeof(uint32_t);  // <= 12 KiB (R <= 1024)
 
     // workspace: rays [o 3 | d 3 | t | t_max | T] x n floats; pixel lists [live | live2 | counts |
-    // offsets | keep | idx] x n u32; counters (16 u32); coarse mip (R^3 / 64 bytes, rounded to
-    // 16 u32); samples [slots | pos 3 | dir 3 | dt | density | rgb 3] x cap floats
+    // offsets | keep | idx] x n u32; counters (16 u32); coarse mips (R^3 / 64 bytes for 4^3 blocks
+    // and R^3 / 4096 for 16^3 blocks, each rounded up to 64 bytes); samples [slots | pos 3 | dir 3 |
+    // dt | density | rgb 3] x cap floats
     const uint32_t res = (uint32_t)desc->grid.resolution;
     const uint32_t mip_blocks = res >= 16 ? res * res * res / 64 : 0u;
+    const uint32_t mip2_blocks = res >= 64 ? mip_blocks / 64 : 0u;
     const size_t ray_words = ((size_t)9 * n + 3) & ~(size_t)3, list_words = ((size_t)6 * n + 3) & ~(size_t)3;
-    const size_t mip_words = ((size_t)mip_blocks + 63) / 64 * 16;
+    const size_t mip1_words = ((size_t)mip_blocks + 63) / 64 * 16;
+    const size_t mip_words = mip1_words + ((size_t)mip2_blocks + 63) / 64 * 16;
     const size_t smp_words = (size_t)12 * cap;
     st = ensure_render_ws(ctx, (ray_words + list_words + 16 + mip_words + smp_words) * 4);
     if (st != TN_OK) return st;
@@ -568,6 +574,7 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
     unsigned long long* totals = reinterpret_cast<unsigned long long*>(counters + 8);
     uint32_t* info = counters + 1;
     uint8_t* mip = mip_blocks ? reinterpret_cast<uint8_t*>(counters + 16) : nullptr;
+    uint8_t* mip2 = mip2_blocks ? reinterpret_cast<uint8_t*>(counters + 16 + mip1_words) : nullptr;
     float* smp = reinterpret_cast<float*>(counters + 16 + mip_words);
     float *slots = smp, *s_pos = smp + (size_t)cap, *s_dir = smp + 4 * (size_t)cap, *s_dt = smp + 7 * (size_t)cap,
           *s_density = smp + 8 * (size_t)cap, *s_rgb = smp + 9 * (size_t)cap;
@@ -582,6 +589,11 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
         render_mip_kernel<<<(mip_blocks + 255) / 256, 256, 0, stream>>>(
             mip_blocks, reinterpret_cast<const uint4*>(desc->bitfield), mip);
         st = check_launch("tn_render(mip)");
+    }
+    if (st == TN_OK && mip2_blocks) {  // the same OR, of the 64 4^3 blocks of each 16^3 block
+        render_mip_kernel<<<(mip2_blocks + 255) / 256, 256, 0, stream>>>(
+            mip2_blocks, reinterpret_cast<const uint4*>(mip), mip2);
+        st = check_launch("tn_render(mip2)");
     }
     if (st == TN_OK) {
         render_rays_kernel<<<(n + 255) / 256, 256, 0, stream>>>(n, *camera, desc->render_bbox, ori, dir, ray_t,
@@ -602,7 +614,7 @@ int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const
         const uint32_t quota = std::max(batch / n_live, 1u);
         const int grid = (int)((n_live + 255) / 256);
         render_walk_kernel<<<grid, 256, spread_bytes, stream>>>(A, n, n_live, quota, live, ori, dir, ray_t, ray_tmax,
-                                                                mip, max_iters, counts, slots, keep, totals,
+                                                                mip, mip2, max_iters, counts, slots, keep, totals,
                                                                 ctx->flags);
         st = check_launch("tn_render(walk)");
         if (st == TN_OK) st = tn_scan_offsets(ctx, stream, n_live, counts, offsets, 0xffffffffu, info);
