@@ -183,7 +183,9 @@ class RenderModifiers:
 class RenderRequest:
     """What to render: `camera`, `nerfs` (one Trainer after setup_data, whose device state
     holds the NeRF), `output` (a RenderTarget; resized to the camera's resolution), and the
-    reference's flags and callbacks (on_complete(), on_progress(fraction), on_cancel())."""
+    reference's flags and callbacks. A submit renders the whole image synchronously, so
+    on_progress(1.0) and on_complete() are called once at its end; flags (preview or final)
+    do not change the image, and on_cancel() is never called (there is nothing to cancel)."""
 
     def __init__(self, camera: Camera, nerfs, output: RenderTarget, modifiers: RenderModifiers | None = None,
                  flags: RenderFlags = RenderFlags.Final, on_complete=None, on_progress=None, on_cancel=None):
