@@ -69,9 +69,33 @@ def occupancy_fixture():
                 out_bitfield=nb, n_occupied=np.uint32(nocc))
 
 
+def render_camera():
+    """Camera of the render fixture: 24 x 16 pixels from (0.4, 0.9, 3.5) toward the centre."""
+    eye = np.array([0.4, 0.9, 3.5])
+    fwd = -eye / np.linalg.norm(eye)
+    right = np.cross(fwd, [0.0, 1.0, 0.0])
+    right /= np.linalg.norm(right)
+    xf = np.stack([right, np.cross(fwd, right), fwd, eye], axis=1).astype(np.float32)
+    return dict(width=24, height=16, near=0.1, far=50.0, focal=(17.0, 17.0), principal=(12.0, 8.0),
+                shift=(0.0, 0.0), transform=xf)
+
+
+def render_fixture():
+    rng = np.random.default_rng(0x63)
+    fld = scenes.make_blob_field(rng, 8)
+    grid = scenes.build_grid(fld, n_levels=2, base_size=2.0, resolution=32)
+    bbox = (-2.0, -2.0, -2.0, 2.0, 2.0, 2.0)
+    cam = render_camera()
+    rgba, amb, n = oracle.render(cam, bbox, bbox, grid.as_dict(), float(np.float32(scenes.MIN_STEP_SIZE)),
+                                 1.0 / 256.0, 1e-4, fld.blobs, fld.waves, 4.0)
+    return dict(bitfield=grid.bitfield, blobs=fld.blobs, waves=fld.waves,
+                n_levels=np.int32(2), res=np.int32(32), base=np.float32(2.0), bbox=np.float32(bbox),
+                transform=cam["transform"], rgba=rgba, ambiguous=amb, n_samples=np.int64(n))
+
+
 def main():
     for name, fn in (("march_small", march_fixture), ("loss_small", loss_fixture),
-                     ("occupancy_small", occupancy_fixture)):
+                     ("occupancy_small", occupancy_fixture), ("render_small", render_fixture)):
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **fn())
         print(path, os.path.getsize(path))

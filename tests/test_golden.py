@@ -36,3 +36,10 @@ def test_occupancy_fixture_reproduces():
     for k in ("out_density", "out_bitfield", "n_occupied"):
         _same(new[k], fx[k], k)
     assert oracle.popcount(fx["out_bitfield"]) == int(fx["n_occupied"])
+
+
+def test_render_fixture_reproduces():
+    fx, new = _load("render_small"), make_golden.render_fixture()
+    for k in ("rgba", "ambiguous", "n_samples", "bitfield"):
+        _same(new[k], fx[k], k)
+    assert int(fx["n_samples"]) > 0 and not fx["ambiguous"].any()

@@ -73,3 +73,28 @@ def test_occupancy_matches_golden():
     assert_bitwise(host(d), fx["out_density"].ravel(), "density")
     assert_bitwise(host(b), fx["out_bitfield"], "bitfield")
     assert int(host(nocc)[0]) == int(fx["n_occupied"])
+
+
+def test_render_matches_golden():
+    """Renderer.submit on the fixture's scene (2 cascades of 32^3, base 2, its blob field as the
+    network) against the oracle's image, within the composite tolerance."""
+    from tests.golden.make_golden import render_camera
+    from turbonerf_b200.renderer import Camera, CPURenderBuffer, Renderer, RenderRequest
+    from turbonerf_b200.trainer import BoundingBox, SyntheticNeRF, Trainer
+    fx = _load("render_small")
+    b = BoundingBox(4.0)
+    nerf = SyntheticNeRF(b, int(fx["n_levels"]), fx["blobs"], fx["waves"], None, fx["bitfield"],
+                         int(fx["res"]), float(fx["base"]))
+    tr = Trainer(nerf, n_rays_per_step=4096, n_grid_params=16 * (1 << 15) * 2)
+    tr.setup_data(batch_size=1 << 16)
+    c = render_camera()
+    cam = Camera((c["width"], c["height"]), c["near"], c["far"], c["focal"], c["principal"], c["shift"],
+                 fx["transform"])
+    buf = CPURenderBuffer()
+    Renderer().submit(RenderRequest(cam, [tr], buf))
+    img = buf.get_rgba()
+    ref = fx["rgba"]
+    for ch in range(4):
+        assert_close(img[..., ch].ravel(), ref[..., ch].ravel(), 1e-5, f"rendered channel {ch}")
+    assert np.all(img[ref[..., 3] == 0] == 0)
+    tr.teardown()
