@@ -2000,16 +2000,28 @@ static int launch_train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_ba
     return check_launch("tn_train_losses");
 }
 
-// Rays per warp of the sample-tile compositor, from the batch's mean samples per ray
+// Rays per warp of the sample-tile kernels, from the batch's mean samples per ray
 // (sample_stride / n_rays, an upper bound): up to 4 tiles (32 * ST_K samples each) of samples per
 // warp while that leaves at least 32 warps per SM (the setup of a warp's range and its partly
-// filled first and last tiles are then paid once per 4 tiles), else 1 tile per warp.
-static uint32_t tile_rays_per_warp(const tn_ray_batch* b) {
+// filled first and last tiles are then paid once per 4 tiles), else 1 tile per warp; more when
+// the grid would otherwise take more than one wave of resident warps.
+static uint32_t tile_rays_per_warp(const tn_ray_batch* b, const void* kernel, uint32_t max_tiles = 0) {
     const double mean = b->n_rays ? std::max(1.0, (double)b->sample_stride / (double)b->n_rays) : 1.0;
     const double per_tile = (double)(WARP * ST_K);
     const double fill = (double)b->sample_stride / (per_tile * num_sms() * 32.0);
     const double tiles = std::min(4.0, std::max(1.0, std::floor(fill)));
-    return (uint32_t)std::min(32.0, std::max(1.0, std::floor(tiles * per_tile / mean)));
+    uint32_t rpw = (uint32_t)std::min(32.0, std::max(1.0, std::floor(tiles * per_tile / mean)));
+    // when the grid would take more than one wave of resident warps, enough rays per warp (at most
+    // 32) that it takes one: no partly filled last wave
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, LOSS_THREADS, 0) == cudaSuccess && per_sm > 0) {
+        const uint64_t resident = (uint64_t)num_sms() * (uint64_t)per_sm * LOSS_WARPS;
+        const uint64_t warps = (b->n_rays + rpw - 1) / rpw;
+        if (warps > resident) rpw = (uint32_t)std::min<uint64_t>(32, (b->n_rays + resident - 1) / resident);
+    }
+    // a kernel that keeps per-tile state for max_tiles tiles: rays of about that many tiles a warp
+    if (max_tiles) rpw = std::min(rpw, (uint32_t)std::max(1.0, std::floor(max_tiles * per_tile / mean)));
+    return rpw;
 }
 
 // 16-byte sample vectors: every per-sample array 16-byte aligned and the stride a multiple of 4.
@@ -2027,10 +2039,11 @@ static int tile_grid(uint32_t n_rays, uint32_t rpw) {
 // whether per-sample transmittance and weights are stored. depth_max = -ln(min_transmittance).
 static void launch_composite_fwd_tiles(cudaStream_t stream, const tn_ray_batch* b, const Samples& S, float min_t,
                                        float* rgba, float* depth, uint32_t* n_used, float* t_out, float* w_out) {
-    const uint32_t rpw = tile_rays_per_warp(b);
-    const int grid = tile_grid(b->n_rays, rpw);
     const float depth_max = min_t > 0.0f ? -logf(min_t) : INFINITY;
     const bool vec = tile_vec(S, t_out, w_out), store = t_out != nullptr;
+    const uint32_t rpw = tile_rays_per_warp(
+        b, vec ? (const void*)composite_fwd_tiles_kernel<ST_K, true, 0, false> : (const void*)composite_fwd_tiles_kernel<ST_K, false, 0, false>);
+    const int grid = tile_grid(b->n_rays, rpw);
 #define TN_FWD_TILES(V, A, ST)                                                                                  \
     composite_fwd_tiles_kernel<ST_K, V, A, ST><<<grid, LOSS_THREADS, 0, stream>>>(                              \
         S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth_max, rgba, depth, n_used,  \
@@ -2052,9 +2065,10 @@ static void launch_composite_fwd_tiles(cudaStream_t stream, const tn_ray_batch* 
 static void launch_composite_bwd_tiles(cudaStream_t stream, const tn_ray_batch* b, const Samples& S,
                                        const float* depth, const uint32_t* n_used, const float* grad_rgba, float* dd,
                                        float* drgb) {
-    const uint32_t rpw = tile_rays_per_warp(b);
-    const int grid = tile_grid(b->n_rays, rpw);
     const bool vec = tile_vec(S, dd, drgb);
+    const uint32_t rpw = tile_rays_per_warp(
+        b, vec ? (const void*)composite_bwd_tiles_kernel<ST_K, true, 0> : (const void*)composite_bwd_tiles_kernel<ST_K, false, 0>);
+    const int grid = tile_grid(b->n_rays, rpw);
 #define TN_BWD_TILES(V, A)                                                                                      \
     composite_bwd_tiles_kernel<ST_K, V, A><<<grid, LOSS_THREADS, 0, stream>>>(                                  \
         S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth, n_used, grad_rgba, dd, drgb)
@@ -2177,12 +2191,14 @@ int tn_distortion_fwd_bwd(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* b
     TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
     if (batch->n_rays == 0) return TN_OK;
     Samples S{density, nullptr, nullptr, m_norm, dt_norm, nullptr, batch->sample_stride, activation};
-    const uint32_t rpw = tile_rays_per_warp(batch);
+    const uintptr_t al = (uintptr_t)density | (uintptr_t)m_norm | (uintptr_t)dt_norm | (uintptr_t)dL_ddensity;
+    const bool vec = (al & 15u) == 0 && (batch->sample_stride & 3u) == 0;
+    const uint32_t rpw = tile_rays_per_warp(
+        batch, vec ? (const void*)distortion_tiles_kernel<true, 0> : (const void*)distortion_tiles_kernel<false, 0>,
+        SAVED_TILES / 2);
     const int grid = tile_grid(batch->n_rays, rpw);
     st = ensure_block_f32(ctx, (size_t)grid * 2);
     if (st != TN_OK) return st;
-    const uintptr_t al = (uintptr_t)density | (uintptr_t)m_norm | (uintptr_t)dt_norm | (uintptr_t)dL_ddensity;
-    const bool vec = (al & 15u) == 0 && (batch->sample_stride & 3u) == 0;
 #define TN_DIST_TILES(V, A)                                                                                     \
     distortion_tiles_kernel<V, A><<<grid, LOSS_THREADS, 0, stream>>>(                                           \
         S, batch->n_rays, batch->n_rays_dev, rpw, batch->counts, batch->offsets, lambda, grad_ray, ray_loss,     \
