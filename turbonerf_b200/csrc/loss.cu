@@ -506,6 +506,22 @@ __device__ __forceinline__ void load_tile(const Samples& S, uint32_t s0, const b
     }
 }
 
+// L2 prefetch of one tile of samples [s, s + 32 K) of the five sample arrays (density, dt and the
+// three rgb planes), one 128-byte line per lane for the first 5 * 32 K / 32 lanes: the next tile's
+// loads then find their lines in L2 instead of DRAM. Lines past the arrays' end are not touched.
+template <int K>
+__device__ __forceinline__ void prefetch_tile(const Samples& S, uint32_t s, int lane) {
+    constexpr int LINES = WARP * K / 32;  // 128-byte lines of one array per tile
+    if (lane < 5 * LINES) {
+        const int arr = lane / LINES, line = lane % LINES;
+        const uint32_t at = s + (uint32_t)line * 32u;
+        if (at < S.ss) {
+            const float* base = arr == 0 ? S.density : arr == 1 ? S.dt : S.rgb + (size_t)(arr - 2) * S.ss;
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(base + at));
+        }
+    }
+}
+
 // Compositor forward over the rays of each warp (density_to_ray_rgba_forward,
 // src/utils/training-kernels-fused.cuh:227-264). Termination is decided on the optical depth
 // d = sum sigma dt: sample j is composited while the depth before it is at most
@@ -539,6 +555,7 @@ composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
     const uint32_t s_begin = t_off[wid][0], s_end = t_end[wid][nr - 1];
     float cx = 0.0f, csum[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // running sums of the ray open at the tile start
     for (uint32_t base = VEC ? (s_begin & ~3u) : s_begin; base < s_end; base += WARP * K) {
+        if (base + WARP * K < s_end) prefetch_tile<K>(S, base + WARP * K, lane);
         const uint32_t s0 = base + (uint32_t)lane * K;
         bool in[K], head[K], last[K];
         int ri[K];
@@ -669,6 +686,7 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
     const uint32_t n_tiles = (s_end - b0 + span - 1) / span;
     float cx = 0.0f, c4[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // suffix sums of the ray open at the tile end
     for (int t = (int)n_tiles - 1; t >= 0; --t) {
+        if (t > 0) prefetch_tile<K>(S, b0 + (uint32_t)(t - 1) * span, lane);
         const uint32_t s0 = b0 + (uint32_t)t * span + (uint32_t)lane * K;
         bool in[K], valid[K], tail[K];
         int ri[K];
