@@ -488,6 +488,22 @@ typedef struct tn_render_stats {
 int tn_render(tn_ctx* ctx, tn_stream_t stream, const tn_render_desc* desc, const tn_camera* camera,
               const tn_network* net, float* out_rgba, tn_render_stats* stats);
 
+/* ---- training rays from posed images ------------------------------------------------
+ * Reference initialize_training_rays_and_pixels_kernel + deactivate_rays_with_alpha_threshold_kernel
+ * (src/utils/training-batch-kernels.cuh:82-208) as called by Trainer::generate_next_training_batch
+ * (src/core/trainer.cu:40-100). Ray i belongs to image (uint32)(i / (n_rays / n_images)), at pixel
+ * position p = width * height * random[i] (x = fmod(p, width), y = p / width) of that image's
+ * camera (device array of tn_camera, no lens distortion); it is clipped to bbox (t = max(0,
+ * t_min + 1e-5), t_max = min(far - near, box exit); alive = 0 when it misses or t_max < t); its
+ * target is the RGBA8 texel min(floor(p), w h - 1) of images [n_images][height][width][4] (device)
+ * over 255. With alpha_threshold < 1 and alpha_probability < 1, a ray whose target alpha is below
+ * the threshold is dropped when random[ray_stride + i] > alpha_probability. Outputs [c][ray_stride];
+ * img_id may be NULL. */
+int tn_dataset_rays(tn_stream_t stream, uint32_t n_rays, uint32_t ray_stride, uint32_t n_images, int32_t width,
+                    int32_t height, const tn_camera* cameras, const uint8_t* images, const tn_bbox* bbox,
+                    const float* random, float alpha_threshold, float alpha_probability, float* pix_rgba,
+                    uint32_t* img_id, float* ori, float* dir, float* ray_t, float* ray_t_max, uint8_t* alive);
+
 typedef struct tn_trainer_desc {
     tn_grid_desc grid;
     tn_bbox bbox;                       /* training box; aabb size = max_x - min_x */
@@ -592,6 +608,18 @@ int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t);
  * Applies a pending Adam update first. */
 int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,
                       uint32_t batch_size, float* out_rgba, tn_render_stats* stats);
+/* Trains on rays from posed images instead of the built-in synthetic rays (the reference trains
+ * on its Dataset, src/core/trainer.cu:40-100): n_images cameras and RGBA8 images
+ * [n_images][height][width][4], host arrays, copied to the device. Every step draws its pixel
+ * positions, alpha-selection draws and background colours from the trainer's seed and step
+ * (tn_dataset_rays). The next step captures its graph again. */
+int tn_trainer_set_dataset(tn_trainer* tr, uint32_t n_images, int32_t width, int32_t height, const tn_camera* cameras,
+                           const uint8_t* images);
+/* The training controller's alpha selection (reference NeRFTrainingController::
+ * alpha_selection_threshold / alpha_selection_probability, nerf-training-controller.h:75-76):
+ * while both are below 1, dataset rays whose target alpha is below the threshold are kept with
+ * the given probability. Defaults 1, 1 (off). */
+int tn_trainer_set_alpha_selection(tn_trainer* tr, float threshold, float probability);
 /* 0/1: kernel nodes in the captured step graph (synthetic / caller rays), 2: graph nodes,
  * 3: samples processed so far, 4: rays used so far, 5: steps (3-5 synchronise). */
 int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out);
@@ -607,7 +635,8 @@ int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out);
  * density, 6 bitfield, 7 sample t, 8 sample pos, 9 sample dt, 10 ray offsets,
  * 11 ray n_steps, 12 batch_info[4], 13 network density, 14 network rgb,
  * 15 grad density, 16 dL/drgb, 17 ray origins, 18 ray directions, 19 ray t,
- * 20 ray t_max, 21 ray alive, 22 target rgba, 23 background rgb, 24 m_norm, 25 dt_norm. */
+ * 20 ray t_max, 21 ray alive, 22 target rgba, 23 background rgb, 24 m_norm, 25 dt_norm,
+ * 26 the dataset rays' draws [2][n_rays] (pixel, alpha selection; NULL without a dataset). */
 int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes);
 
 #ifdef __cplusplus

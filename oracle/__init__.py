@@ -78,6 +78,8 @@ def _declare(L):
         "orc_blob_field": (None, [i64, i64, vp, f32, i32, vp, vp, vp, vp, i64]),
         "orc_render": (i64, [vp, ctypes.POINTER(Bbox), ctypes.POINTER(Bbox), i32, i32, f32, vp, f32, f32, f64, i32,
                              vp, vp, f32, vp, vp]),
+        "orc_dataset_rays": (i64, [i64, i64, i64, i32, i32, vp, vp, ctypes.POINTER(Bbox), vp, f32, f32, vp, vp, vp,
+                                   vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -322,3 +324,34 @@ def render(camera: dict, render_bbox, training_bbox, grid, dt_min, cone, min_t, 
                              grid["base"], _p(bits), dt_min, cone, min_t, len(blobs), _p(_c(blobs, np.float32)),
                              _p(_c(waves, np.float32)), aabb_size, _p(out), _p(amb))
     return out.reshape(c.height, c.width, 4), amb.reshape(c.height, c.width), int(total)
+
+
+def camera_struct(camera: dict) -> "Camera":
+    c = Camera()
+    c.width, c.height = int(camera["width"]), int(camera["height"])
+    c.near, c.far = float(camera["near"]), float(camera["far"])
+    c.focal_x, c.focal_y = [float(v) for v in camera["focal"]]
+    c.principal_x, c.principal_y = [float(v) for v in camera["principal"]]
+    c.shift_x, c.shift_y = [float(v) for v in camera["shift"]]
+    for k, v in enumerate(np.asarray(camera["transform"], np.float32)[:3, :4].reshape(-1)):
+        c.transform[k] = float(v)
+    return c
+
+
+def dataset_rays(n_rays, cameras, images, bbox, random, alpha_threshold=1.0, alpha_probability=1.0):
+    """Training rays from posed RGBA8 images [n][h][w][4]; random: [2][n_rays] draws. Returns a
+    dict of the outputs ([c][n_rays] arrays; a dead ray's values other than alive are unspecified)
+    and the live count."""
+    images = _c(images, np.uint8)
+    n_img, h, w = images.shape[:3]
+    cams = (Camera * n_img)(*[camera_struct(c) for c in cameras])
+    rs = n_rays
+    out = dict(pix_rgba=np.zeros(4 * rs, np.float32), img_id=np.zeros(rs, np.uint32), ori=np.zeros(3 * rs, np.float32),
+               dir=np.zeros(3 * rs, np.float32), t=np.zeros(rs, np.float32), t_max=np.zeros(rs, np.float32),
+               alive=np.zeros(rs, np.uint8))
+    b = bbox_struct(bbox)
+    live = lib().orc_dataset_rays(n_rays, rs, n_img, w, h, cams, _p(images), ctypes.byref(b),
+                                  _p(_c(random, np.float32)), alpha_threshold, alpha_probability, _p(out["pix_rgba"]),
+                                  _p(out["img_id"]), _p(out["ori"]), _p(out["dir"]), _p(out["t"]), _p(out["t_max"]),
+                                  _p(out["alive"]))
+    return out, int(live)

@@ -823,6 +823,28 @@ struct Camera {
     float transform[12];  // row-major 3 x 4 [R | t], camera to world
 };
 
+// Camera::global_ray_at_pixel_xy, src/models/camera.cuh:94-137, without lens distortion.
+static inline void pinhole_ray(const Camera& cam, float x, float y, float& ox, float& oy, float& oz, float& dx,
+                               float& dy, float& dz) {
+    const float offx = cam.shift_x * (float)cam.width - cam.principal_x;
+    const float offy = cam.shift_y * (float)cam.height - cam.principal_y;
+    const float* m = cam.transform;
+    const float vx = (x + offx + 0.5f) / cam.focal_x;
+    const float vy = (y + offy + 0.5f) / cam.focal_y;
+    const float vz = 1.0f;
+    const float vlen = std::sqrt(vx * vx + vy * vy + vz * vz);
+    const float gx = m[0] * vx + m[1] * vy + m[2] * vz;
+    const float gy = m[4] * vx + m[5] * vy + m[6] * vz;
+    const float gz = m[8] * vx + m[9] * vy + m[10] * vz;
+    const float gl = std::sqrt(gx * gx + gy * gy + gz * gz);
+    dx = gx / gl;
+    dy = gy / gl;
+    dz = gz / gl;
+    ox = m[3] + cam.near_ * (vlen * dx);
+    oy = m[7] + cam.near_ * (vlen * dy);
+    oz = m[11] + cam.near_ * (vlen * dz);
+}
+
 int64_t orc_render(const Camera* cam, const Bbox* render_bbox, const Bbox* train_bbox, int n_levels, int res,
                    float base, const uint8_t* bits, float dt_min, float cone, double min_t, int n_blobs,
                    const float* blobs, const float* waves, float aabb_size, double* out_rgba, uint8_t* ambiguous) {
@@ -832,9 +854,6 @@ int64_t orc_render(const Camera* cam, const Bbox* render_bbox, const Bbox* train
     const float dt_max = 8.0f * dt_min;
     const float sx = tb.max_x - tb.min_x, sy = tb.max_y - tb.min_y, sz = tb.max_z - tb.min_z;
     const float inv_size = 1.0f / sx;
-    const float offx = cam->shift_x * (float)cam->width - cam->principal_x;
-    const float offy = cam->shift_y * (float)cam->height - cam->principal_y;
-    const float* m = cam->transform;
     int64_t total = 0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
     for (int64_t i = 0; i < n; ++i) {
@@ -842,18 +861,8 @@ int64_t orc_render(const Camera* cam, const Bbox* render_bbox, const Bbox* train
         o4[0] = o4[1] = o4[2] = o4[3] = 0.0;
         ambiguous[i] = 0;
         const uint32_t py = (uint32_t)(i / cam->width), px = (uint32_t)(i % cam->width);
-        const float vx = ((float)px + offx + 0.5f) / cam->focal_x;
-        const float vy = ((float)py + offy + 0.5f) / cam->focal_y;
-        const float vz = 1.0f;
-        const float vlen = std::sqrt(vx * vx + vy * vy + vz * vz);
-        const float gx = m[0] * vx + m[1] * vy + m[2] * vz;
-        const float gy = m[4] * vx + m[5] * vy + m[6] * vz;
-        const float gz = m[8] * vx + m[9] * vy + m[10] * vz;
-        const float gl = std::sqrt(gx * gx + gy * gy + gz * gz);
-        const float dx = gx / gl, dy = gy / gl, dz = gz / gl;
-        float ox = m[3] + cam->near_ * (vlen * dx);
-        float oy = m[7] + cam->near_ * (vlen * dy);
-        float oz = m[11] + cam->near_ * (vlen * dz);
+        float ox, oy, oz, dx, dy, dz;
+        pinhole_ray(*cam, (float)px, (float)py, ox, oy, oz, dx, dy, dz);
         const float ix = 1.0f / dx, iy = 1.0f / dy, iz = 1.0f / dz;
         float t1x = (box.min_x - ox) * ix, t2x = (box.max_x - ox) * ix;
         float t1y = (box.min_y - oy) * iy, t2y = (box.max_y - oy) * iy;
@@ -910,6 +919,61 @@ int64_t orc_render(const Camera* cam, const Bbox* render_bbox, const Bbox* train
         }
     }
     return total;
+}
+
+// ---------------------------------------------------------------------------
+// Training rays from posed RGBA8 images: initialize_training_rays_and_pixels_kernel and
+// deactivate_rays_with_alpha_threshold_kernel, src/utils/training-batch-kernels.cuh:82-208, with
+// n_rays_per_image = n_rays / n_images (src/core/trainer.cu:60). random: [2][rs] (pixel draw,
+// alpha-selection draw). Outputs [c][rs]; a ray that misses the box keeps alive = 0 and its other
+// outputs are unspecified (the reference leaves them untouched). Returns the number of live rays.
+// ---------------------------------------------------------------------------
+int64_t orc_dataset_rays(int64_t n_rays, int64_t rs, int64_t n_images, int width, int height, const Camera* cameras,
+                         const uint8_t* images, const Bbox* bbox, const float* random, float alpha_threshold,
+                         float alpha_probability, float* pix_rgba, uint32_t* img_id, float* ori, float* dir,
+                         float* ray_t, float* ray_t_max, uint8_t* alive) {
+    const uint32_t n_pixels = (uint32_t)width * (uint32_t)height;
+    const float rays_per_image = (float)n_rays / (float)n_images;
+    const bool selection = alpha_threshold < 1.0f && alpha_probability < 1.0f;
+    const Bbox b = *bbox;
+    int64_t live = 0;
+#pragma omp parallel for schedule(static) reduction(+ : live)
+    for (int64_t i = 0; i < n_rays; ++i) {
+        alive[i] = 0;
+        const uint32_t image = std::min((uint32_t)((float)i / rays_per_image), (uint32_t)n_images - 1u);
+        const float p = (float)n_pixels * random[i];
+        const float w = (float)width;
+        const float x = std::fmod(p, w), y = p / w;
+        float ox, oy, oz, dx, dy, dz;
+        pinhole_ray(cameras[image], x, y, ox, oy, oz, dx, dy, dz);
+        const float ix = 1.0f / dx, iy = 1.0f / dy, iz = 1.0f / dz;
+        float t1x = (b.min_x - ox) * ix, t2x = (b.max_x - ox) * ix;
+        float t1y = (b.min_y - oy) * iy, t2y = (b.max_y - oy) * iy;
+        float t1z = (b.min_z - oz) * iz, t2z = (b.max_z - oz) * iz;
+        if (t1x > t2x) std::swap(t1x, t2x);
+        if (t1y > t2y) std::swap(t1y, t2y);
+        if (t1z > t2z) std::swap(t1z, t2z);
+        const float tmin = std::fmax(t1x, std::fmax(t1y, t1z)), tmax = std::fmin(t2x, std::fmin(t2y, t2z));
+        if (!(tmax >= tmin)) continue;
+        const Camera& cam = cameras[image];
+        const float t_max = std::fmin(cam.far_ - cam.near_, tmax);
+        const float t = std::fmax(0.0f, tmin + 1e-5f);
+        if (t_max < t) continue;
+        const size_t k = std::min((size_t)p, (size_t)n_pixels - 1);
+        const uint8_t* px = images + 4 * ((size_t)n_pixels * image + k);
+        const float rgba[4] = {(float)px[0] / 255.0f, (float)px[1] / 255.0f, (float)px[2] / 255.0f,
+                               (float)px[3] / 255.0f};
+        for (int c = 0; c < 4; ++c) pix_rgba[i + c * rs] = rgba[c];
+        ori[i] = ox; ori[i + rs] = oy; ori[i + 2 * rs] = oz;
+        dir[i] = dx; dir[i + rs] = dy; dir[i + 2 * rs] = dz;
+        ray_t[i] = t;
+        ray_t_max[i] = t_max;
+        img_id[i] = image;
+        if (selection && rgba[3] < alpha_threshold && random[i + rs] > alpha_probability) continue;
+        alive[i] = 1;
+        ++live;
+    }
+    return live;
 }
 
 }  // extern "C"

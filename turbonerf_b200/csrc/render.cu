@@ -79,21 +79,8 @@ __global__ void render_rays_kernel(uint32_t n, tn_camera cam, tn_bbox box, float
     if (i >= n) return;
     const uint32_t w = (uint32_t)cam.width;
     const uint32_t py = i / w, px = i - py * w;
-    const float offx = __fadd_rn(__fmul_rn(cam.shift_x, (float)cam.width), -cam.principal_x);
-    const float offy = __fadd_rn(__fmul_rn(cam.shift_y, (float)cam.height), -cam.principal_y);
-    const float vx = __fdiv_rn(__fadd_rn(__fadd_rn((float)px, offx), 0.5f), cam.focal_x);
-    const float vy = __fdiv_rn(__fadd_rn(__fadd_rn((float)py, offy), 0.5f), cam.focal_y);
-    const float vz = 1.0f;
-    const float vlen = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
-    const float* m = cam.transform;  // row-major 3 x 4: rotation | translation
-    const float gx = __fadd_rn(__fadd_rn(__fmul_rn(m[0], vx), __fmul_rn(m[1], vy)), __fmul_rn(m[2], vz));
-    const float gy = __fadd_rn(__fadd_rn(__fmul_rn(m[4], vx), __fmul_rn(m[5], vy)), __fmul_rn(m[6], vz));
-    const float gz = __fadd_rn(__fadd_rn(__fmul_rn(m[8], vx), __fmul_rn(m[9], vy)), __fmul_rn(m[10], vz));
-    const float gl = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), __fmul_rn(gz, gz)));
-    const float dx = __fdiv_rn(gx, gl), dy = __fdiv_rn(gy, gl), dz = __fdiv_rn(gz, gl);
-    float ox = __fadd_rn(m[3], __fmul_rn(cam.near, __fmul_rn(vlen, dx)));
-    float oy = __fadd_rn(m[7], __fmul_rn(cam.near, __fmul_rn(vlen, dy)));
-    float oz = __fadd_rn(m[11], __fmul_rn(cam.near, __fmul_rn(vlen, dz)));
+    float ox, oy, oz, dx, dy, dz;
+    pinhole_ray(cam, (float)px, (float)py, ox, oy, oz, dx, dy, dz);
     // BoundingBox::get_ray_t_intersections, bounding-box.cuh:27-51
     const float ix = __fdiv_rn(1.0f, dx), iy = __fdiv_rn(1.0f, dy), iz = __fdiv_rn(1.0f, dz);
     float t1x = __fmul_rn(__fadd_rn(box.min_x, -ox), ix), t2x = __fmul_rn(__fadd_rn(box.max_x, -ox), ix);

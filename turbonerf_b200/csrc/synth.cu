@@ -61,22 +61,6 @@ int tn_synth_field(tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32
 // ---- counter-based random numbers (synthetic inputs only) ---------------------------------
 namespace tn {
 
-// 32-bit integer hash (PCG output permutation over a mixed counter)
-__host__ __device__ __forceinline__ uint32_t hash_u32(uint32_t v) {
-    uint32_t s = v * 747796405u + 2891336453u;
-    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
-    return (w >> 22u) ^ w;
-}
-
-__host__ __device__ __forceinline__ uint32_t rng_u32(uint32_t seed, uint32_t stream, uint32_t i, uint32_t k) {
-    return hash_u32(hash_u32(hash_u32(seed ^ 0x9E3779B9u) + stream * 0x85EBCA6Bu) ^ (i * 0xC2B2AE35u + k * 0x27D4EB2Fu));
-}
-
-// uniform in [0, 1)
-__device__ __forceinline__ float rng_uniform(uint32_t seed, uint32_t stream, uint32_t i, uint32_t k) {
-    return (float)(rng_u32(seed, stream, i, k) >> 8) * (1.0f / 16777216.0f);
-}
-
 __device__ __forceinline__ float rng_normal(uint32_t seed, uint32_t stream, uint32_t i, uint32_t k) {
     const float u1 = fmaxf(rng_uniform(seed, stream, i, 2 * k), 1e-7f);
     const float u2 = rng_uniform(seed, stream, i, 2 * k + 1);

@@ -149,6 +149,49 @@ __device__ __forceinline__ void ray_point(const RayMarch& r, float t, float& x, 
     z = __fadd_rn(r.oz, __fmul_rn(t, r.dz));
 }
 
+// Camera::global_ray_at_pixel_xy (src/models/camera.cuh:94-137) without lens distortion: the ray
+// through pixel position (x, y) of a pinhole camera (transform: camera to world, row-major 3 x 4),
+// origin on the near plane, unit direction, in FP32 with the reference's operation order.
+__device__ __forceinline__ void pinhole_ray(const tn_camera& cam, float x, float y, float& ox, float& oy, float& oz,
+                                            float& dx, float& dy, float& dz) {
+    const float offx = __fadd_rn(__fmul_rn(cam.shift_x, (float)cam.width), -cam.principal_x);
+    const float offy = __fadd_rn(__fmul_rn(cam.shift_y, (float)cam.height), -cam.principal_y);
+    const float vx = __fdiv_rn(__fadd_rn(__fadd_rn(x, offx), 0.5f), cam.focal_x);
+    const float vy = __fdiv_rn(__fadd_rn(__fadd_rn(y, offy), 0.5f), cam.focal_y);
+    const float vz = 1.0f;
+    const float vlen = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+    const float* m = cam.transform;
+    const float gx = __fadd_rn(__fadd_rn(__fmul_rn(m[0], vx), __fmul_rn(m[1], vy)), __fmul_rn(m[2], vz));
+    const float gy = __fadd_rn(__fadd_rn(__fmul_rn(m[4], vx), __fmul_rn(m[5], vy)), __fmul_rn(m[6], vz));
+    const float gz = __fadd_rn(__fadd_rn(__fmul_rn(m[8], vx), __fmul_rn(m[9], vy)), __fmul_rn(m[10], vz));
+    const float gl = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), __fmul_rn(gz, gz)));
+    dx = __fdiv_rn(gx, gl);
+    dy = __fdiv_rn(gy, gl);
+    dz = __fdiv_rn(gz, gl);
+    ox = __fadd_rn(m[3], __fmul_rn(cam.near, __fmul_rn(vlen, dx)));
+    oy = __fadd_rn(m[7], __fmul_rn(cam.near, __fmul_rn(vlen, dy)));
+    oz = __fadd_rn(m[11], __fmul_rn(cam.near, __fmul_rn(vlen, dz)));
+}
+
+// ------------------------------------------------------------------------------------
+// Counter-based random numbers (synthetic inputs and the trainer's own draws)
+// ------------------------------------------------------------------------------------
+// 32-bit integer hash (PCG output permutation over a mixed counter)
+__host__ __device__ __forceinline__ uint32_t hash_u32(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+
+__host__ __device__ __forceinline__ uint32_t rng_u32(uint32_t seed, uint32_t stream, uint32_t i, uint32_t k) {
+    return hash_u32(hash_u32(hash_u32(seed ^ 0x9E3779B9u) + stream * 0x85EBCA6Bu) ^ (i * 0xC2B2AE35u + k * 0x27D4EB2Fu));
+}
+
+// uniform in [0, 1)
+__device__ __forceinline__ float rng_uniform(uint32_t seed, uint32_t stream, uint32_t i, uint32_t k) {
+    return (float)(rng_u32(seed, stream, i, k) >> 8) * (1.0f / 16777216.0f);
+}
+
 // ------------------------------------------------------------------------------------
 // Warp scans
 // ------------------------------------------------------------------------------------

@@ -132,6 +132,13 @@ int launch_synth_hash_grads(cudaStream_t stream, uint32_t n, const uint32_t* n_d
                             int n_levels, uint32_t log2_table, int n_features, float base_res, float per_level_scale,
                             uint32_t seed, float std, float* grads);
 int launch_synth_params(cudaStream_t stream, uint32_t n, uint32_t n_grid, uint32_t seed, float* w);
+int check_dataset(uint32_t n_images, int32_t width, int32_t height);
+int launch_dataset_rays(cudaStream_t stream, uint32_t n_rays, uint32_t rs, uint32_t n_images, int32_t width,
+                        int32_t height, const tn_camera* cameras, const uint8_t* images, const tn_bbox& bbox,
+                        const float* random, float alpha_threshold, float alpha_probability, float* pix_rgba,
+                        uint32_t* img_id, float* ori, float* dir, float* ray_t, float* ray_tmax, uint8_t* alive);
+int launch_dataset_draws(cudaStream_t stream, uint32_t n, uint32_t rs, uint32_t seed, const uint32_t* step_dev,
+                         float* random, float* bg);
 
 }  // namespace tn
 

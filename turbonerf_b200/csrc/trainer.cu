@@ -127,6 +127,13 @@ struct tn_trainer {
     // previous step; the step stream takes them from there with one device copy
     cudaStream_t h2d = nullptr;
     float* stage[2] = {nullptr, nullptr};
+    // a dataset of posed images as the ray source (tn_trainer_set_dataset)
+    tn_camera* ds_cameras = nullptr;
+    uint8_t* ds_images = nullptr;
+    float* ds_random = nullptr;  // [2][R]: pixel and alpha-selection draws of the step
+    uint32_t ds_n = 0;
+    int32_t ds_w = 0, ds_h = 0;
+    float alpha_threshold = 1.0f, alpha_probability = 1.0f;
     cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_consumed[2] = {nullptr, nullptr};
     cudaGraph_t graph[2] = {nullptr, nullptr};           // [synthetic rays, caller rays]
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
@@ -158,6 +165,22 @@ namespace {
 
 // Stage boundaries of one fused step (for per-stage timing with events).
 enum Stage : int { ST_RAYS = 0, ST_COUNT, ST_EMIT, ST_FORWARD, ST_LOSSES, ST_BACKWARD, ST_ADAM, ST_OCC_QUERY, ST_OCCUPANCY, ST_N };
+
+// The step's rays when the caller supplies none: from the dataset when one is set, else the
+// built-in synthetic rays.
+static int enqueue_own_rays(tn_trainer* tr, cudaStream_t s) {
+    const tn_trainer_desc& d = tr->d;
+    if (tr->ds_n) {
+        int st = launch_dataset_draws(s, tr->R, tr->R, d.seed, &tr->state->cur_step, tr->ds_random, tr->bg);
+        if (st == TN_OK)
+            st = launch_dataset_rays(s, tr->R, tr->R, tr->ds_n, tr->ds_w, tr->ds_h, tr->ds_cameras, tr->ds_images,
+                                     d.bbox, tr->ds_random, tr->alpha_threshold, tr->alpha_probability, tr->target,
+                                     nullptr, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax, tr->alive);
+        return st;
+    }
+    return launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
+                             3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+}
 
 // Occupancy query of one step: random cells, their sample points, the density network.
 static int enqueue_occupancy_query(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid) {
@@ -237,8 +260,7 @@ int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
             st = tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax,
                                    tr->alive);
         else
-            st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
-                                   3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+            st = enqueue_own_rays(tr, s);
     }
     mark(ST_RAYS);
     uint32_t* info = tr->state->batch_info;
@@ -306,8 +328,7 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
             st = tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax,
                                    tr->alive);
         else
-            st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
-                                   3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+            st = enqueue_own_rays(tr, s);
     }
     if (st == TN_OK)
         st = tn_plain_march_count(s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, tr->ori, tr->dir, tr->ray_t,
@@ -589,8 +610,7 @@ int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_t
     // one batch of samples from the current grid (rays of step 0)
     int st = cuda_status(cudaMemsetAsync(tr->state, 0, sizeof(StepState), s), "state clear");
     if (st == TN_OK)
-        st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
-                               3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+        st = enqueue_own_rays(tr, s);
     uint32_t* info = tr->state->batch_info;
     if (st == TN_OK)
         st = tn_march_count(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, tr->ori, tr->dir,
@@ -775,6 +795,48 @@ static void drop_graphs(tn_trainer* tr) {
     }
 }
 
+int tn_trainer_set_dataset(tn_trainer* tr, uint32_t n_images, int32_t width, int32_t height, const tn_camera* cameras,
+                           const uint8_t* images) {
+    TN_NONNULL(tr); TN_NONNULL(cameras); TN_NONNULL(images);
+    int st = check_dataset(n_images, width, height);
+    if (st != TN_OK) return st;
+    st = flush_adam(tr);
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_set_dataset");
+    if (st != TN_OK) return st;
+    const size_t texels = (size_t)n_images * (size_t)width * (size_t)height;
+    tn_camera* cams = nullptr;
+    uint8_t* imgs = nullptr;
+    st = tr->alloc(cams, n_images);
+    if (st == TN_OK) st = tr->alloc(imgs, 4 * texels);
+    if (st == TN_OK && !tr->ds_random) st = tr->alloc(tr->ds_random, 2 * (size_t)tr->R);
+    if (st == TN_OK)
+        st = cuda_status(cudaMemcpyAsync(cams, cameras, n_images * sizeof(tn_camera), cudaMemcpyHostToDevice, tr->stream),
+                         "dataset cameras");
+    if (st == TN_OK)
+        st = cuda_status(cudaMemcpyAsync(imgs, images, 4 * texels, cudaMemcpyHostToDevice, tr->stream), "dataset images");
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "dataset upload");
+    if (st != TN_OK) return st;
+    tr->ds_cameras = cams;
+    tr->ds_images = imgs;
+    tr->ds_n = n_images;
+    tr->ds_w = width;
+    tr->ds_h = height;
+    drop_graphs(tr);  // the next step captures the dataset rays
+    return TN_OK;
+}
+
+int tn_trainer_set_alpha_selection(tn_trainer* tr, float threshold, float probability) {
+    TN_NONNULL(tr);
+    TN_REQUIRE(threshold == threshold && probability == probability, TN_E_INVALID, "alpha selection: NaN");
+    if (threshold == tr->alpha_threshold && probability == tr->alpha_probability) return TN_OK;
+    const int st = flush_adam(tr);
+    if (st != TN_OK) return st;
+    tr->alpha_threshold = threshold;
+    tr->alpha_probability = probability;
+    drop_graphs(tr);  // kernel parameters of the captured step
+    return cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_set_alpha_selection");
+}
+
 int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
     TN_NONNULL(tr);
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "tn_trainer_autotune: the fused path only");
@@ -787,8 +849,7 @@ int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
     int st = cuda_status(cudaStreamSynchronize(s), "tn_trainer_autotune");
     // before the first step the ray buffers are empty: generate the first step's rays
     if (st == TN_OK && tr->fused_steps_enqueued == 0)
-        st = launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
-                               3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+        st = enqueue_own_rays(tr, s);
     uint32_t* info = tr->state->batch_info;
     tn_tune_report rep[3] = {};
     if (st == TN_OK)
@@ -974,6 +1035,7 @@ int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes) {
         case 23: p = tr->bg; n = 12 * R; break;
         case 24: p = tr->s_mnorm; n = 4 * B; break;
         case 25: p = tr->s_dtnorm; n = 4 * B; break;
+        case 26: p = tr->ds_random; n = tr->ds_random ? 8 * R : 0; break;
         default: return fail(TN_E_INVALID, "unknown trainer buffer %d", which);
     }
     *ptr = p;

@@ -220,6 +220,10 @@ SIGNATURES = {
     "tn_synth_field": [_vp, _u32, _vp, _u32, _vp, _f32, _u32, _vp, _vp, _vp, _vp, _u32],
     "tn_render": [_vp, _vp, _P(RenderDescC), _P(CameraC), _vp, _vp, _P(RenderStatsC)],
     "tn_trainer_render": [_vp, _P(CameraC), _P(Bbox), _f32, _u32, _vp, _P(RenderStatsC)],
+    "tn_dataset_rays": [_vp, _u32, _u32, _u32, _i32, _i32, _vp, _vp, _P(Bbox), _vp, _f32, _f32, _vp, _vp, _vp, _vp,
+                        _vp, _vp, _vp],
+    "tn_trainer_set_dataset": [_vp, _u32, _i32, _i32, _vp, _vp],
+    "tn_trainer_set_alpha_selection": [_vp, _f32, _f32],
     "tn_trainer_default_desc": [_vp],
     "tn_trainer_create": [_P(_vp), _vp, _vp],
     "tn_trainer_destroy": [_vp],

@@ -61,6 +61,23 @@ class OccupancyGridMetrics:
     n_total: int
 
 
+class Dataset:
+    """Posed images to train on (the reference's Dataset, src/models/dataset.h, loaded here from
+    arrays instead of a transforms.json): `cameras`, one renderer.Camera per image, all of the
+    images' resolution, and `images`, uint8 RGBA [n_images][height][width][4]."""
+
+    def __init__(self, cameras, images):
+        self.cameras = list(cameras)
+        self.images = np.ascontiguousarray(images, dtype=np.uint8)
+        if self.images.ndim != 4 or self.images.shape[3] != 4:
+            raise ValueError("images must be [n_images][height][width][4] RGBA8")
+        if len(self.cameras) != self.images.shape[0]:
+            raise ValueError("one camera per image")
+        h, w = self.images.shape[1:3]
+        if any(c.resolution != (w, h) for c in self.cameras):
+            raise ValueError("every camera must have the images' resolution")
+
+
 @dataclass
 class SyntheticNeRF:
     """What the trainer trains on: the cascaded occupancy grid (base size 1 = the reference's
@@ -74,6 +91,7 @@ class SyntheticNeRF:
     resolution: int = 128
     base_size: float = 1.0
     render_bbox: BoundingBox | None = None  # renderer crop (reference NeRFProxy::render_bbox); None: bounding_box
+    dataset: Dataset | None = None  # posed images to train on; None: the built-in synthetic rays
 
     @classmethod
     def from_scene(cls, scene) -> "SyntheticNeRF":
@@ -119,7 +137,8 @@ class Trainer:
     def setup_data(self, batch_size: int = 2 << 21, synthetic_grad_std: float = 1e-3) -> None:
         """Allocates every buffer, uploads the grid and the synthetic field, and seeds the
         parameter gradients (reference setup_data, nerf-training-controller.cu:27-85)."""
-        if self.alpha_selection_threshold < 1.0 and self.alpha_selection_probability < 1.0:
+        if (self.alpha_selection_threshold < 1.0 and self.alpha_selection_probability < 1.0
+                and self.nerf.dataset is None):
             raise NotImplementedError("alpha selection acts on image alpha; the synthetic ray source has none")
         self.teardown()
         d = TrainerDesc()
@@ -145,6 +164,7 @@ class Trainer:
         h = ctypes.c_void_p()
         call("tn_trainer_create", ctypes.byref(h), ctypes.byref(d), None)
         self._h = h
+        self._alpha_applied = None
         blobs = np.ascontiguousarray(n.blobs, np.float32)
         waves = np.ascontiguousarray(n.waves, np.float32)
         call("tn_trainer_set_synthetic_field", h, blobs.shape[0], blobs.ctypes.data_as(ctypes.c_void_p),
@@ -153,6 +173,12 @@ class Trainer:
         bits = None if n.bitfield is None else np.ascontiguousarray(n.bitfield, np.uint8)
         call("tn_trainer_set_grid", h, dens.ctypes.data_as(ctypes.c_void_p) if dens is not None else None,
              bits.ctypes.data_as(ctypes.c_void_p) if bits is not None else None)
+        if n.dataset is not None:
+            cams = (native.CameraC * len(n.dataset.cameras))(*[c.c_struct() for c in n.dataset.cameras])
+            im = n.dataset.images
+            call("tn_trainer_set_dataset", h, im.shape[0], im.shape[2], im.shape[1], cams,
+                 im.ctypes.data_as(ctypes.c_void_p))
+            self._apply_alpha_selection()
         touched = ctypes.c_uint32(0)
         call("tn_trainer_init_synthetic_gradients", h, float(synthetic_grad_std), ctypes.byref(touched))
         self.n_touched_grads = touched.value
@@ -173,14 +199,26 @@ class Trainer:
             raise RuntimeError("call setup_data() first")
         return self._h
 
+    def _apply_alpha_selection(self) -> None:
+        """Hands the alpha-selection attributes to the controller when they changed (they act on
+        dataset rays; the reference reads them on every step)."""
+        cur = (float(self.alpha_selection_threshold), float(self.alpha_selection_probability))
+        if self._h is not None and getattr(self, "_alpha_applied", None) != cur:
+            if cur[0] < 1.0 and cur[1] < 1.0 and self.nerf.dataset is None:
+                raise NotImplementedError("alpha selection acts on image alpha; the synthetic ray source has none")
+            call("tn_trainer_set_alpha_selection", self._h, cur[0], cur[1])
+            self._alpha_applied = cur
+
     # -- steps ---------------------------------------------------------------------------
     def train_step(self) -> TrainingMetrics:
+        self._apply_alpha_selection()
         m = TrainingMetricsC()
         call("tn_trainer_train_step", self._handle(), ctypes.byref(m))
         return TrainingMetrics(m.step, m.loss, m.n_rays, m.n_samples)
 
     def train_step_async(self) -> None:
         """Enqueues one step without waiting (fused path: a graph replay)."""
+        self._apply_alpha_selection()
         call("tn_trainer_train_step", self._handle(), None)
 
     def train_step_rays(self, ori, dir_, target_rgba, bg_rgb) -> TrainingMetrics:
