@@ -620,6 +620,29 @@ int tn_trainer_set_dataset(tn_trainer* tr, uint32_t n_images, int32_t width, int
  * while both are below 1, dataset rays whose target alpha is below the threshold are kept with
  * the given probability. Defaults 1, 1 (off). */
 int tn_trainer_set_alpha_selection(tn_trainer* tr, float threshold, float probability);
+/* .turbo snapshots (reference FileManager::save / load, src/services/file-manager.cuh:18-198):
+ * the reference's 300-byte header, the fp32 parameters ([hash grid | MLP]: n_density_params
+ * carries the hash-grid count, n_color_params the MLP count) and the occupancy bitfield, which
+ * the reference's loader reads; then a resume block of this library (Adam moments and step
+ * counts, grid densities, the trainer's step counters) that the reference's loader ignores.
+ * Save applies a pending Adam update first and synchronises. Load restores into a trainer
+ * created with the same parameter counts, grid and box: everything the file holds, so a file
+ * with the resume block continues training exactly; a reference file (no resume block) sets
+ * the parameters and the bitfield and leaves the rest. */
+typedef struct tn_turbo_info {
+    uint64_t n_params;
+    uint64_t file_bytes;
+    uint32_t n_occ_grid_bits;
+    uint32_t aabb_scale;
+    uint32_t has_resume;
+    uint32_t step_count;
+    uint32_t n_levels, resolution;
+    char dataset_path[256];
+} tn_turbo_info;
+int tn_trainer_save(tn_trainer* tr, const char* path, const char* dataset_path);
+int tn_trainer_load(tn_trainer* tr, const char* path);
+/* Reads a .turbo file's header and resume block (no GPU work). */
+int tn_turbo_file_info(const char* path, tn_turbo_info* out);
 /* 0/1: kernel nodes in the captured step graph (synthetic / caller rays), 2: graph nodes,
  * 3: samples processed so far, 4: rays used so far, 5: steps (3-5 synchronise). */
 int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out);

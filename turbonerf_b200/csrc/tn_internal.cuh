@@ -133,6 +133,32 @@ int launch_synth_hash_grads(cudaStream_t stream, uint32_t n, const uint32_t* n_d
                             uint32_t seed, float std, float* grads);
 int launch_synth_params(cudaStream_t stream, uint32_t n, uint32_t n_grid, uint32_t seed, float* w);
 int check_dataset(uint32_t n_images, int32_t width, int32_t height);
+
+// .turbo snapshot (snapshot.cu): the reference's header and sections (FileManager::save,
+// src/services/file-manager.cuh:18-120), then this library's resume block.
+struct TurboHeader {
+    char project_name[16];  // "TurboNeRF"
+    char dataset_path[256];
+    uint32_t version;       // 0
+    uint32_t n_color_params;
+    uint32_t n_density_params;
+    uint32_t n_appearance_embedding_params;
+    uint32_t n_occ_grid_bits;
+    uint32_t aabb_scale;
+    uint32_t n_appearances;
+};
+static_assert(sizeof(TurboHeader) == 300, "the reference's NeRFFileData layout");
+
+struct TurboResume {
+    char magic[8];  // "TNRESUME"
+    uint32_t version;
+    uint32_t n_levels, resolution;
+    uint32_t n_grid_params, n_mlp_params;
+    uint32_t step_count;
+    uint64_t samples_total, rays_total;
+};
+
+int read_turbo_file(const char* path, TurboHeader* header, TurboResume* resume, bool* has_resume, uint64_t* size);
 int launch_dataset_rays(cudaStream_t stream, uint32_t n_rays, uint32_t rs, uint32_t n_images, int32_t width,
                         int32_t height, const tn_camera* cameras, const uint8_t* images, const tn_bbox& bbox,
                         const float* random, float alpha_threshold, float alpha_probability, float* pix_rgba,

@@ -18,6 +18,8 @@
 // replayed without any host synchronisation.
 // Plain path: the reference's launch structure (thrust scans, blocking device->host reads of
 // the sample count and the losses, separate memsets and epilogue kernels, dense Adam).
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -878,6 +880,136 @@ int tn_trainer_flush(tn_trainer* tr) {
     int st = flush_adam(tr);
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_flush");
     return st;
+}
+
+namespace {
+
+// The AABB scale of the reference's header: the edge of the training box (a whole number there).
+uint32_t turbo_aabb_scale(const tn_trainer* tr) { return (uint32_t)std::lround(tr->aabb); }
+
+struct FileCloser {
+    FILE* f;
+    ~FileCloser() { if (f) std::fclose(f); }
+};
+
+}  // namespace
+
+int tn_trainer_save(tn_trainer* tr, const char* path, const char* dataset_path) {
+    TN_NONNULL(tr); TN_NONNULL(path);
+    int st = flush_adam(tr);
+    if (st != TN_OK) return st;
+    const size_t P = tr->P, V = tr->V, LV = (size_t)tr->d.grid.n_levels * V;
+    std::vector<float> w(P), m(P), v(P), density(LV);
+    std::vector<uint32_t> steps(P);
+    std::vector<uint8_t> bits(V);
+    cudaStream_t s = tr->stream;
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        if (st == TN_OK) st = cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "save read");
+    };
+    d2h(w.data(), tr->w, P * 4); d2h(m.data(), tr->m, P * 4); d2h(v.data(), tr->v, P * 4);
+    d2h(steps.data(), tr->steps, P * 4); d2h(density.data(), tr->density, LV * 4); d2h(bits.data(), tr->bits, V);
+    d2h(tr->state_host, tr->state, sizeof(StepState));
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "save sync");
+    if (st != TN_OK) return st;
+    const StepState& h = *tr->state_host;
+    TurboHeader hd{};
+    std::strncpy(hd.project_name, "TurboNeRF", sizeof(hd.project_name));
+    if (dataset_path) std::strncpy(hd.dataset_path, dataset_path, sizeof(hd.dataset_path) - 1);
+    hd.version = 0;
+    hd.n_color_params = tr->d.n_mlp_params;
+    hd.n_density_params = tr->d.n_grid_params;
+    hd.n_appearance_embedding_params = 0;
+    hd.n_occ_grid_bits = (uint32_t)V;
+    hd.aabb_scale = turbo_aabb_scale(tr);
+    hd.n_appearances = 0;
+    TurboResume r{};
+    std::memcpy(r.magic, "TNRESUME", 8);
+    r.version = 1;
+    r.n_levels = (uint32_t)tr->d.grid.n_levels;
+    r.resolution = (uint32_t)tr->d.grid.resolution;
+    r.n_grid_params = tr->d.n_grid_params;
+    r.n_mlp_params = tr->d.n_mlp_params;
+    r.step_count = h.step_count;
+    r.samples_total = h.samples_total;
+    r.rays_total = h.rays_total;
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) return fail(TN_E_INVALID, "cannot create %s", path);
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, fc.f) == 1 && std::fwrite(w.data(), 4, P, fc.f) == P &&
+              std::fwrite(bits.data(), 1, V, fc.f) == V && std::fwrite(&r, sizeof(r), 1, fc.f) == 1 &&
+              std::fwrite(m.data(), 4, P, fc.f) == P && std::fwrite(v.data(), 4, P, fc.f) == P &&
+              std::fwrite(steps.data(), 4, P, fc.f) == P && std::fwrite(density.data(), 4, LV, fc.f) == LV;
+    ok = std::fclose(fc.f) == 0 && ok;
+    fc.f = nullptr;
+    return ok ? TN_OK : fail(TN_E_INVALID, "writing %s failed", path);
+}
+
+int tn_trainer_load(tn_trainer* tr, const char* path) {
+    TN_NONNULL(tr); TN_NONNULL(path);
+    TurboHeader hd;
+    TurboResume r;
+    bool has = false;
+    uint64_t size = 0;
+    int st = read_turbo_file(path, &hd, &r, &has, &size);
+    if (st != TN_OK) return st;
+    const size_t P = tr->P, V = tr->V, LV = (size_t)tr->d.grid.n_levels * V;
+    TN_REQUIRE(hd.n_density_params == tr->d.n_grid_params && hd.n_color_params == tr->d.n_mlp_params &&
+                   hd.n_appearance_embedding_params == 0,
+               TN_E_INVALID, "%s holds %u + %u + %u parameters; the trainer has %u (hash grid) + %u (MLP)", path,
+               hd.n_density_params, hd.n_color_params, hd.n_appearance_embedding_params, tr->d.n_grid_params,
+               tr->d.n_mlp_params);
+    TN_REQUIRE(hd.n_occ_grid_bits == V, TN_E_INVALID, "%s holds a %u-byte bitfield; the trainer's grid has %zu cells",
+               path, hd.n_occ_grid_bits, V);
+    TN_REQUIRE(hd.aabb_scale == turbo_aabb_scale(tr), TN_E_INVALID, "%s: AABB scale %u, the trainer's box is %u",
+               path, hd.aabb_scale, turbo_aabb_scale(tr));
+    if (has) {
+        TN_REQUIRE(r.n_levels == (uint32_t)tr->d.grid.n_levels && r.resolution == (uint32_t)tr->d.grid.resolution &&
+                       r.n_grid_params == tr->d.n_grid_params && r.n_mlp_params == tr->d.n_mlp_params,
+                   TN_E_INVALID, "%s: resume block of a %u-level %u^3 grid; the trainer has %d levels of %d^3", path,
+                   r.n_levels, r.resolution, tr->d.grid.n_levels, tr->d.grid.resolution);
+        const uint64_t need = sizeof(TurboHeader) + 4ull * P + V + sizeof(TurboResume) + 12ull * P + 4ull * LV;
+        TN_REQUIRE(size >= need, TN_E_INVALID, "%s: resume block truncated (%llu bytes of %llu)", path,
+                   (unsigned long long)size, (unsigned long long)need);
+    }
+    std::vector<float> w(P), m, v, density;
+    std::vector<uint32_t> steps;
+    std::vector<uint8_t> bits(V);
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return fail(TN_E_INVALID, "cannot open %s", path);
+    bool ok = std::fseek(fc.f, (long)sizeof(TurboHeader), SEEK_SET) == 0 && std::fread(w.data(), 4, P, fc.f) == P &&
+              std::fread(bits.data(), 1, V, fc.f) == V;
+    if (ok && has) {
+        m.resize(P); v.resize(P); steps.resize(P); density.resize(LV);
+        ok = std::fseek(fc.f, (long)sizeof(TurboResume), SEEK_CUR) == 0 && std::fread(m.data(), 4, P, fc.f) == P &&
+             std::fread(v.data(), 4, P, fc.f) == P && std::fread(steps.data(), 4, P, fc.f) == P &&
+             std::fread(density.data(), 4, LV, fc.f) == LV;
+    }
+    if (!ok) return fail(TN_E_INVALID, "reading %s failed", path);
+    // a pending Adam update belongs to the replaced state: dropped, not applied
+    cudaStream_t s = tr->stream;
+    st = cuda_status(cudaStreamSynchronize(s), "load sync");
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        if (st == TN_OK) st = cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "load write");
+    };
+    h2d(tr->w, w.data(), P * 4);
+    h2d(tr->bits, bits.data(), V);
+    StepState& h = *tr->state_host;
+    h = StepState{};
+    if (has) {
+        h2d(tr->m, m.data(), P * 4); h2d(tr->v, v.data(), P * 4); h2d(tr->steps, steps.data(), P * 4);
+        h2d(tr->density, density.data(), LV * 4);
+        h.step_count = r.step_count;
+        h.samples_total = r.samples_total;
+        h.rays_total = r.rays_total;
+        h.cur_step = r.step_count ? r.step_count - 1u : 0u;
+    }
+    h2d(tr->state, &h, sizeof(StepState));
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "load sync");
+    if (st != TN_OK) return st;
+    tr->host_step = h.step_count;
+    tr->last = tn_training_metrics{};
+    tr->last.step = h.step_count;
+    tr->ring_calls = 0;
+    return TN_OK;
 }
 
 int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,

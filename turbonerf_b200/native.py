@@ -120,6 +120,13 @@ class TrainerDesc(ctypes.Structure):
                 ("ray_jitter", ctypes.c_float)]
 
 
+class TurboInfoC(ctypes.Structure):
+    """tn_turbo_info: a .turbo file's header and resume block."""
+    _fields_ = [("n_params", ctypes.c_uint64), ("file_bytes", ctypes.c_uint64), ("n_occ_grid_bits", ctypes.c_uint32),
+                ("aabb_scale", ctypes.c_uint32), ("has_resume", ctypes.c_uint32), ("step_count", ctypes.c_uint32),
+                ("n_levels", ctypes.c_uint32), ("resolution", ctypes.c_uint32), ("dataset_path", ctypes.c_char * 256)]
+
+
 class CameraC(ctypes.Structure):
     """tn_camera: pinhole camera, transform = camera to world, row-major 3 x 4 [R | t]."""
     _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("near", ctypes.c_float),
@@ -224,6 +231,9 @@ SIGNATURES = {
                         _vp, _vp, _vp],
     "tn_trainer_set_dataset": [_vp, _u32, _i32, _i32, _vp, _vp],
     "tn_trainer_set_alpha_selection": [_vp, _f32, _f32],
+    "tn_trainer_save": [_vp, ctypes.c_char_p, ctypes.c_char_p],
+    "tn_trainer_load": [_vp, ctypes.c_char_p],
+    "tn_turbo_file_info": [ctypes.c_char_p, _P(TurboInfoC)],
     "tn_trainer_default_desc": [_vp],
     "tn_trainer_create": [_P(_vp), _vp, _vp],
     "tn_trainer_destroy": [_vp],

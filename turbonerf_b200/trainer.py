@@ -322,3 +322,32 @@ class Trainer:
                                         "version": 3}
 
         return torch.as_tensor(_View(), device="cuda")
+
+
+class FileManager:
+    """`.turbo` snapshots, named like the reference's `FileManager` (python_bindings.cu:647-662,
+    src/services/file-manager.cuh:34-198). The reference saves a NeRF proxy; here the trained
+    state lives in the `Trainer`, so that is what `save` and `load` take. The file holds the
+    reference's header, fp32 parameters ([hash grid | MLP]) and occupancy bitfield, then a resume
+    block (Adam moments and step counts, grid densities, step counters) that the reference's
+    loader does not read. `load` needs a trainer set up with the same parameter counts, grid and
+    box; after it, training continues from the saved step exactly."""
+
+    @staticmethod
+    def save(trainer: Trainer, path: str, dataset_path: str | None = None) -> None:
+        if dataset_path is None:
+            dataset_path = getattr(trainer.nerf.dataset, "file_path", None) or ""
+        call("tn_trainer_save", trainer._handle(), str(path).encode(), str(dataset_path).encode())
+
+    @staticmethod
+    def load(trainer: Trainer, path: str) -> None:
+        call("tn_trainer_load", trainer._handle(), str(path).encode())
+
+    @staticmethod
+    def info(path: str) -> dict:
+        """The header and resume block of a .turbo file (no GPU work)."""
+        i = native.TurboInfoC()
+        call("tn_turbo_file_info", str(path).encode(), ctypes.byref(i))
+        return {"n_params": i.n_params, "file_bytes": i.file_bytes, "n_occ_grid_bits": i.n_occ_grid_bits,
+                "aabb_scale": i.aabb_scale, "has_resume": bool(i.has_resume), "step_count": i.step_count,
+                "n_levels": i.n_levels, "resolution": i.resolution, "dataset_path": i.dataset_path.decode()}
