@@ -95,3 +95,47 @@ def test_load_rejects_another_layout(tmp_path):
         FileManager.load(b, f)
     a.teardown()
     b.teardown()
+
+
+def test_resumed_dataset_run_draws_the_same_rays(tmp_path):
+    """The dataset rays of a step are drawn from the seed and the step index, so a trainer that
+    resumes from a snapshot takes the same rays as the one that kept going."""
+    from tests.test_gpu_dataset import _trainer as dataset_trainer
+    _, _, a = dataset_trainer()
+    for _ in range(2):
+        a.train_step()
+    f = str(tmp_path / "ds.turbo")
+    FileManager.save(a, f)
+    _, _, b = dataset_trainer()
+    FileManager.load(b, f)
+    ma, mb = a.train_step(), b.train_step()
+    assert (ma.step, ma.n_rays, ma.n_samples) == (mb.step, mb.n_rays, mb.n_samples) and ma.step == 3
+    for k, dt in ((17, np.float32), (18, np.float32), (22, np.float32), (26, np.float32), (21, np.uint8)):
+        assert_bitwise(b.buffer(k, dt).cpu().numpy(), a.buffer(k, dt).cpu().numpy(), f"ray buffer {k}")
+    sa, sb = _state(a), _state(b)
+    for k in STATE:
+        assert_bitwise(sb[k], sa[k], f"buffer {k} after the resumed step")
+    a.teardown()
+    b.teardown()
+
+
+def test_loaded_trainer_renders_the_same_frame(tmp_path):
+    from tests.test_gpu_render import _camera
+    from turbonerf_b200.renderer import CPURenderBuffer, Renderer, RenderPattern, RenderRequest
+    a = _trainer()
+    for _ in range(2):
+        a.train_step()
+    f = str(tmp_path / "run.turbo")
+    FileManager.save(a, f)
+    b = _trainer()
+    FileManager.load(b, f)
+    cam = _camera(64, 48, (0.3, 0.8, 4.0))
+    imgs = []
+    for tr in (a, b):
+        out = CPURenderBuffer()
+        Renderer(RenderPattern.LinearChunks).submit(RenderRequest(cam, [tr], out))
+        imgs.append(out.get_rgba())
+    assert imgs[0][..., 3].max() > 0
+    assert_bitwise(imgs[1], imgs[0], "rendered frame")
+    a.teardown()
+    b.teardown()
