@@ -199,10 +199,28 @@ NCU_TRAFFIC = {"march_count": 1_007_616, "march_emit": 1_285_376, "losses": 9_63
 NCU_TRAFFIC_COMPOSITE = {"composite_fwd_tiles": 87_174_144, "composite_bwd_tiles": 114_450_688}
 
 
+class L2Flush:
+    """Flushes the L2 (126 MB) between timed launches, outside the timed region: a 256 MB write,
+    then a 256 MB read of a second buffer. The read evicts the dirty lines of the write, so the
+    timed launch does not pay for writing them back (as under ncu, whose cache control leaves
+    clean caches); its DRAM traffic is its own."""
+
+    def __init__(self):
+        import torch
+        self.w = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+        self.r = torch.ones(64 << 20, dtype=torch.float32, device="cuda")
+        self.s = torch.empty((), dtype=torch.float32, device="cuda")
+
+    def __call__(self):
+        import torch
+        self.w.fill_(1.0)
+        torch.sum(self.r, dim=0, out=self.s)
+
+
 def compositor_rooflines(peak, reps=20):
     """Roofline of the compositor's tile kernels (forward, VJP) on the compositor workload at 2^22
     samples (truncated geometric counts, mean 64, at most 1024: 65,571 rays): the L2 (126 MB) is
-    flushed before every timed launch (a 256 MB write outside the events), each launch timed with
+    flushed before every timed launch (L2Flush, outside the events), each launch timed with
     CUDA events, the mean kept. Algorithmic bytes: forward 20 B/sample + 32 B/ray, VJP 36 B/sample
     + 24 B/ray."""
     import torch
@@ -217,7 +235,7 @@ def compositor_rooflines(peak, reps=20):
     g_rgba = torch.full((4 * n,), 1e-3, device="cuda")
     fo = hp.composite_fwd(ctx, rb, sig, rgb, dt)
     bo = hp.composite_bwd(ctx, rb, sig, rgb, dt, fo["depth"], fo["n_used"], g_rgba)
-    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    flush = L2Flush()
     kernels = {
         "composite_fwd_tiles": (lambda: hp.composite_fwd(ctx, rb, sig, rgb, dt, out=fo), 20 * ss + 32 * n),
         "composite_bwd_tiles": (lambda: hp.composite_bwd(ctx, rb, sig, rgb, dt, fo["depth"], fo["n_used"], g_rgba,
@@ -229,7 +247,7 @@ def compositor_rooflines(peak, reps=20):
             fn()
         total = 0.0
         for _ in range(reps):
-            flush.fill_(1.0)
+            flush()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             fn()
@@ -859,6 +877,127 @@ def run_render(args):
     print(json.dumps(out), flush=True)
 
 
+def run_dataset_rays(args):
+    """Training rays from posed images (tn_dataset_rays; reference
+    initialize_training_rays_and_pixels_kernel + deactivate_rays_with_alpha_threshold_kernel):
+    100 synthetic 800 x 800 RGBA8 images (256 MB on the device, larger than L2; 40% of texels
+    transparent) seen by cameras on a radius-4 sphere around the 16-unit training box, 2^20 rays
+    per launch, with alpha selection off and on (threshold 0.5, probability 0.25). Each launch is
+    timed with CUDA events after an L2 flush (L2Flush). Algorithmic bytes: 65 per ray (two draws and one
+    texel read; RGBA, image id, origin, direction, t, t_max and alive written). The CPU oracle
+    runs the same 2^20 rays; its output is compared with the GPU's bit for bit. Last, the
+    train step on dataset rays (the train-step workload with the images as the ray source)."""
+    import ctypes
+    import torch
+    import oracle
+    from turbonerf_b200.native import Bbox, CameraC, call
+    from turbonerf_b200.renderer import Camera
+    from turbonerf_b200.trainer import Dataset, SyntheticNeRF, Trainer
+
+    torch.cuda.set_device(0)
+    n_img, w, h, n = 100, 800, 800, 1 << 20
+    rng = np.random.default_rng(0x7B0)
+    cams = []
+    for _ in range(n_img):
+        e = rng.normal(size=3)
+        cams.append(Camera((w, h), 0.1, 100.0, (1111.0, 1111.0), (w / 2, h / 2), (0.0, 0.0),
+                           _look_at(tuple(4.0 * e / np.linalg.norm(e)))))
+    imgs = rng.integers(0, 256, (n_img, h, w, 4), dtype=np.uint8)
+    imgs[..., 3] = np.where(rng.random((n_img, h, w)) < 0.4, rng.integers(0, 40, (n_img, h, w)), 255)
+    half = 8.0
+    bbox = (-half, -half, -half, half, half, half)
+    cam_arr = (CameraC * n_img)(*[c.c_struct() for c in cams])
+    cam_dev = torch.frombuffer(bytearray(bytes(cam_arr)), dtype=torch.uint8).cuda()
+    img_dev = torch.from_numpy(imgs).cuda()
+    rnd = torch.rand((2, n), device="cuda", generator=torch.Generator("cuda").manual_seed(0x7B0))
+    f32 = lambda k: torch.empty(k, device="cuda")  # noqa: E731
+    outs = dict(pix_rgba=f32(4 * n), img_id=torch.empty(n, dtype=torch.int32, device="cuda"), ori=f32(3 * n),
+                dir=f32(3 * n), t=f32(n), t_max=f32(n), alive=torch.empty(n, dtype=torch.uint8, device="cuda"))
+    b = Bbox(*bbox)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    stream = torch.cuda.current_stream()
+    flush = L2Flush()
+    peak, peak_src = _peaks()
+    alg = 65 * n
+
+    def launch(thr, prob, k=n):
+        call("tn_dataset_rays", ctypes.c_void_p(stream.cuda_stream), k, n, n_img, w, h, p(cam_dev), p(img_dev),
+             ctypes.byref(b), p(rnd), thr, prob, p(outs["pix_rgba"]), p(outs["img_id"]), p(outs["ori"]),
+             p(outs["dir"]), p(outs["t"]), p(outs["t_max"]), p(outs["alive"]))
+
+    res = {"workload": "training rays from 100 posed 800x800 RGBA8 images, 2^20 rays per launch, L2 flushed",
+           "metric": "rays/s", "dtype": "f32", "data": "synthetic", "launches": []}
+    reps = max(min(args.steps, 50), 5)
+    for thr, prob in ((1.0, 1.0), (0.5, 0.25)):
+        for _ in range(max(args.warmup, 3)):
+            launch(thr, prob)
+        ms = []
+        for _ in range(reps):
+            flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            launch(thr, prob)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        m = statistics.mean(ms)
+        live = int(outs["alive"].sum().item())
+        res["launches"].append({"alpha_threshold": thr, "alpha_probability": prob, "ms": round(m, 4),
+                                "rays_per_s": round(n / (m / 1e3), 1), "live_rays": live,
+                                "roofline": {"bound": "hbm", "achieved": round(alg / (m / 1e3) / 1e9, 1),
+                                             "peak": peak, "unit": "GB/s",
+                                             "frac": round(alg / (m / 1e3) / 1e9 / peak, 4),
+                                             "alg_bytes": alg, "peak_source": peak_src}})
+    # parity and the CPU baseline: the oracle on the same 2^20 rays as the last launch
+    torch.cuda.synchronize()
+    od = [dict(width=w, height=h, near=c.near, far=c.far, focal=c.focal_length, principal=c.principal_point,
+               shift=c.shift, transform=c.transform) for c in cams]
+    r_host = rnd.cpu().numpy()
+    t0 = time.perf_counter()
+    ref, live = oracle.dataset_rays(n, od, imgs, bbox, r_host, 0.5, 0.25)
+    el = time.perf_counter() - t0
+    got = {key: v.cpu().numpy() for key, v in outs.items()}
+    alive = got["alive"].astype(bool)
+    bad = int(np.count_nonzero(alive != ref["alive"].astype(bool)))
+    for key in ("ori", "dir", "pix_rgba", "t", "t_max"):
+        comps = got[key].size // n
+        g = got[key].reshape(comps, n)[:, alive]
+        r = np.asarray(ref[key], np.float32).reshape(comps, n)[:, alive]
+        bad += int(np.count_nonzero(g.view(np.uint32) != r.view(np.uint32)))
+    res["parity_2e20"] = {"mismatched_values": bad, "live_rays": int(live)}
+    res["cpu_baseline"] = {"value": round(n / el, 1), "unit": "rays/s", "cores": oracle.num_threads(), "kind": "port",
+                           "sample": f"the same 2^20 rays on the CPU oracle, {el:.3f} s"}
+    del flush, img_dev
+    # the train step with the images as its ray source (2^14 rays on 100 smaller images)
+    sc = _scene(0x7B0)
+    nerf = SyntheticNeRF.from_scene(sc)
+    nerf.dataset = Dataset(cams[:20], imgs[:20])
+    tr = Trainer(nerf, path="fused", n_rays_per_step=RAYS, occupancy_cells_per_step=OCC_CELLS,
+                 distortion_lambda=LAMBDA, occupancy_threshold=THRESHOLD, n_grid_params=N_GRID, n_mlp_params=N_MLP,
+                 beta2=0.99, seed=0x7B0)
+    tr.use_distortion_loss = True
+    tr.setup_data(batch_size=BATCH, synthetic_grad_std=1e-3)
+    for _ in range(max(args.warmup, 3)):
+        tr.train_step_async()
+    torch.cuda.synchronize()
+    steps = max(min(args.steps, 100), 5)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s = torch.cuda.ExternalStream(tr.stream_handle())
+    e0.record(s)
+    for _ in range(steps):
+        tr.train_step_async()
+    e1.record(s)
+    e1.synchronize()
+    m = tr.sync_metrics()
+    ms = e0.elapsed_time(e1) / steps
+    res["train_step_on_dataset_rays"] = {"ms_per_step": round(ms, 4), "samples_last_step": m.n_samples,
+                                         "rays_last_step": m.n_rays,
+                                         "samples_per_s": round(m.n_samples / (ms / 1e3), 1),
+                                         "images": "20 of the 800x800 images"}
+    tr.teardown()
+    print(json.dumps(res), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -873,11 +1012,12 @@ def main():
     ap.add_argument("--render-batches", default="0,1048576,4194304,16777216",
                     help="render workload: sample budgets per round (0: the library default)")
     ap.add_argument("--workload", default="train-step",
-                    choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render"],
+                    choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render", "dataset-rays"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "
                          "multi-scene: the batched persistent march of 16 scenes against one launch per scene; "
                          "kernel-tour: every kernel once at representative sizes, for profiling; "
-                         "render: inference frames through Renderer.submit")
+                         "render: inference frames through Renderer.submit; "
+                         "dataset-rays: training rays from posed images")
     args = ap.parse_args()
     if args.workload == "backward-memory":
         run_backward_memory(args)
@@ -887,6 +1027,8 @@ def main():
         run_kernel_tour(args)
     elif args.workload == "render":
         run_render(args)
+    elif args.workload == "dataset-rays":
+        run_dataset_rays(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
