@@ -998,6 +998,109 @@ def run_dataset_rays(args):
     print(json.dumps(res), flush=True)
 
 
+def run_configs(args):
+    """GPU and CPU oracle side by side on the smaller configurations, samples/s each:
+    * forward march + composite: 1 cascade of 128^3 over [-1.5, 1.5]^3, 8 blobs, 4096 rays from
+      a radius-4 sphere, fixed dt = sqrt(3)/1024, at most 1024 steps; march count, emit (no
+      batch cut), the blob field as the network, compositor forward;
+    * compositor + distortion: 2^18 samples (truncated geometric counts, mean 48), compositor
+      forward and backward with the fused distortion forward/backward (lambda 1e-3);
+    * large-batch backward: the same on 2^22 samples (mean 64, at most 1024).
+    GPU: CUDA events around the chain, L2 flushed before each repetition (L2Flush), mean.
+    CPU: the oracle's restatement of the same stages on all host threads."""
+    import torch
+    import oracle
+    from turbonerf_b200 import hotpath as hp, scenes
+
+    torch.cuda.set_device(0)
+    oracle.build()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    flush = L2Flush()
+    reps = max(min(args.steps, 20), 3)
+
+    def gpu_time(fn, before=None):
+        for _ in range(max(args.warmup, 3)):
+            if before:
+                before()
+            fn()
+        total = 0.0
+        for _ in range(reps):
+            if before:
+                before()
+            flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / reps / 1e3
+
+    out = {"workload": "march + composite (1 cascade, 4096 rays); compositor + distortion at 2^18 and 2^22 samples",
+           "metric": "samples/s", "dtype": "f32", "data": "synthetic", "cores": oracle.num_threads(), "configs": []}
+    # forward march + composite
+    sc = scenes.march_scene_single(seed=0x7B0)
+    r = sc.rays
+    n, B = r.n, 1 << 22
+    ss = B + 64
+    g = hp.GridSpec(sc.grid.n_levels, sc.grid.resolution, sc.grid.base_size)
+    m = hp.MarchSpec(sc.cone_angle, sc.dt_min, sc.dt_max, sc.max_steps)
+    bits, ori, dr, t0, tm, al0 = d(sc.grid.bitfield), d(r.ori), d(r.dir), d(r.t), d(r.t_max), d(r.alive)
+    al = al0.clone()
+    blobs, waves = d(sc.field.blobs), d(sc.field.waves)
+    mctx = hp.Context(n, B)
+    state = {}
+
+    def chain0():
+        ns, info = hp.march_count(mctx, g, bits, sc.bbox, m, n, n, ori, dr, t0, tm, al, 0xFFFFFFFF)
+        off, smp = hp.march_emit(mctx, g, bits, sc.bbox, m, 1.0 / sc.aabb_size, n, n, ss, info, ori, dr, t0, al, ns)
+        sig, rgb = hp.synth_field(smp["pos"], ss, ss, sc.aabb_size, blobs, waves, n_dev=info[1:])
+        rb = hp.ray_batch(ns, off, n, n, ss)
+        state["fo"] = hp.composite_fwd(mctx, rb, sig, rgb, smp["dt"])
+        state["info"] = info
+
+    sec = gpu_time(chain0, before=lambda: al.copy_(al0))
+    n_samp = int(state["info"][1].item())
+    rd, gd = r.as_dict(), sc.grid.as_dict()
+    md = dict(bbox=sc.bbox, cone=sc.cone_angle, dt_min=sc.dt_min, dt_max=sc.dt_max, max_steps=sc.max_steps)
+    c0 = time.perf_counter()
+    n_steps, alive, _ = oracle.march_count(rd, gd, md)
+    ns_cpu = int(n_steps.astype(np.int64).sum())
+    offsets = np.concatenate([[0], np.cumsum(n_steps.astype(np.int64))[:-1]]).astype(np.uint32)
+    sst = ns_cpu + 64
+    smp = oracle.march_emit(rd, gd, md, offsets, n_steps, alive, n, sst, 1.0 / sc.aabb_size)
+    sig_c, rgb_c = oracle.blob_field(smp["pos"], sst, ns_cpu, sc.aabb_size, sc.field.blobs, sc.field.waves,
+                                     out_stride=sst)
+    oracle.composite_fwd(n_steps, offsets, sig_c.astype(np.float32), rgb_c.astype(np.float32), smp["dt"], n, sst)
+    el = time.perf_counter() - c0
+    out["configs"].append({"config": "forward march + composite, 1 x 128^3, 4096 rays", "samples": n_samp,
+                           "samples_cpu": int(ns_cpu), "gpu_ms": round(sec * 1e3, 4),
+                           "gpu_samples_per_s": round(n_samp / sec, 1), "cpu_s": round(el, 3),
+                           "cpu_samples_per_s": round(ns_cpu / el, 1)})
+    del mctx
+    # compositor + distortion, forward and backward
+    for label, seed, total, mean in (("compositor + distortion fwd/bwd, 2^18 samples", 0x7B1, 1 << 18, 48.0),
+                                     ("large-batch backward, 2^22 samples", 0x7B5, 1 << 22, 64.0)):
+        sb = scenes.make_sample_batch(seed, total, mean=mean, max_count=1024)
+        nr, ns = sb.n_rays, sb.n_samples
+        counts, offs = d(sb.counts.view(np.int32)), d(sb.offsets.view(np.int32))
+        sig, rgb, dt, mn, dtn = (d(a) for a in (sb.sigma, sb.rgb, sb.dt, sb.m_norm, sb.dt_norm))
+        rb = hp.ray_batch(counts, offs, nr, nr, ns)
+        ctx = hp.Context(nr, ns)
+        g_rgba = torch.full((4 * nr,), 1e-3, device="cuda")
+        sec = gpu_time(lambda: hp.backward_recompute(ctx, rb, sig, rgb, dt, mn, dtn, g_rgba, 1e-3))
+        c0 = time.perf_counter()
+        oracle.composite_fwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, nr, ns)
+        oracle.composite_vjp(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, np.full(4 * nr, 1e-3), nr, ns)
+        oracle.distortion_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.m_norm, sb.dt_norm, 1e-3, ns)
+        el = time.perf_counter() - c0
+        out["configs"].append({"config": label, "samples": ns, "rays": nr, "gpu_ms": round(sec * 1e3, 4),
+                               "gpu_samples_per_s": round(ns / sec, 1), "cpu_s": round(el, 3),
+                               "cpu_samples_per_s": round(ns / el, 1)})
+        del ctx
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1012,12 +1115,13 @@ def main():
     ap.add_argument("--render-batches", default="0,1048576,4194304,16777216",
                     help="render workload: sample budgets per round (0: the library default)")
     ap.add_argument("--workload", default="train-step",
-                    choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render", "dataset-rays"],
+                    choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render", "dataset-rays", "configs"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "
                          "multi-scene: the batched persistent march of 16 scenes against one launch per scene; "
                          "kernel-tour: every kernel once at representative sizes, for profiling; "
                          "render: inference frames through Renderer.submit; "
-                         "dataset-rays: training rays from posed images")
+                         "dataset-rays: training rays from posed images; "
+                         "configs: GPU and CPU oracle on the smaller configurations")
     args = ap.parse_args()
     if args.workload == "backward-memory":
         run_backward_memory(args)
@@ -1029,6 +1133,8 @@ def main():
         run_render(args)
     elif args.workload == "dataset-rays":
         run_dataset_rays(args)
+    elif args.workload == "configs":
+        run_configs(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
