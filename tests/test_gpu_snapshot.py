@@ -139,3 +139,24 @@ def test_loaded_trainer_renders_the_same_frame(tmp_path):
     assert_bitwise(imgs[1], imgs[0], "rendered frame")
     a.teardown()
     b.teardown()
+
+
+def test_save_and_load_report_bad_paths_and_truncated_resume_blocks(tmp_path):
+    a = _trainer()
+    a.train_step()
+    with pytest.raises(native.TurboError, match="cannot create"):
+        FileManager.save(a, str(tmp_path / "missing-dir" / "run.turbo"))
+    with pytest.raises(native.TurboError, match="cannot open"):
+        FileManager.load(a, str(tmp_path / "missing.turbo"))
+    f = str(tmp_path / "run.turbo")
+    FileManager.save(a, f)
+    cut = str(tmp_path / "cut.turbo")
+    with open(f, "rb") as src, open(cut, "wb") as dst:
+        dst.write(src.read()[:-4])  # the densities end one float short
+    before = _state(a)
+    with pytest.raises(native.TurboError, match="truncated"):
+        FileManager.load(a, cut)
+    after = _state(a)
+    for k in STATE:
+        assert_bitwise(after[k], before[k], f"buffer {k} untouched by a rejected load")
+    a.teardown()
