@@ -777,7 +777,8 @@ def run_kernel_tour(args):
     hp.compact_nonzero(mctx, ns)
     hp.popcount(mctx, bits)
     off_na, info_na = torch.zeros(RAYS, dtype=torch.int32, device="cuda"), torch.zeros(4, dtype=torch.int32, device="cuda")
-    native.call("tn_scan_offsets_noalloc", hp._stream(), RAYS, hp._ptr(ns), hp._ptr(off_na), BATCH, hp._ptr(info_na))
+    native.call("tn_scan_offsets_noalloc", hp._stream(), RAYS, hp._ptr(ns), hp._ptr(off_na), BATCH, hp._ptr(info_na),
+                hp._ptr(info_na[3:]))
     ran.append(f"box clip, march count and emit, plain march count, scans, compaction, popcount on {RAYS} rays")
     # batched multi-scene march
     params = scenes.multi_scene_params(seed=0x7C1, n_scenes=6, ray_lo=64, ray_hi=2048)

@@ -248,14 +248,26 @@ int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t*
  * for callers that cannot allocate device memory and hold no tn_ctx: for instance a plugin
  * whose host application owns every device allocation, or a loop that must not pay the
  * device synchronisation of cudaMalloc. No counterpart in the reference (which has no such
- * callers). Its scratch is a fixed array inside the library image, held by every device that
- * loads the library until exit. Limit: n <= TN_SCAN_NOALLOC_MAX_COUNTS; larger n returns
- * TN_E_CAPACITY. The first call on a device looks up the array's device address, so make
- * that first call before any stream capture. All calls share the array: calls that overlap
- * on the GPU race and must be serialised. */
+ * callers). Its scratch is a fixed array inside the library image (128.25 KiB), held by every
+ * device that loads the library until exit.
+ *
+ * Limit: n <= TN_SCAN_NOALLOC_MAX_COUNTS; larger n returns TN_E_CAPACITY at once.
+ *
+ * Errors found on the device: with no tn_ctx there is no tn_ctx_check, so the call stores its
+ * device-side error bits (TN_FLAG_* above; 0 when the call succeeded) into *error_word, a
+ * caller-owned device word written by a plain store at the end of the call (it needs no
+ * clearing). They are TN_FLAG_NO_RAYS and TN_FLAG_NO_SAMPLES (the reference's two runtime
+ * errors of the batch cut; batch_info then holds n_rays = n_samples = 0) and TN_FLAG_CAPACITY
+ * (the total of the counts passed 2^32: offsets past that point are wrong). error_word may be
+ * NULL; batch_info[0] == 0 or batch_info[1] == 0 then remain the only signs of an empty cut.
+ *
+ * The first call on a device (and the first after a cudaDeviceReset) looks up the array's
+ * device address, so make that first call before any stream capture. All calls share the
+ * array and keep the last call's contents: calls that overlap on the GPU race and must be
+ * serialised. */
 #define TN_SCAN_NOALLOC_MAX_COUNTS (1u << 21)
 int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,
-                            uint32_t batch_size, uint32_t* batch_info);
+                            uint32_t batch_size, uint32_t* batch_info, uint32_t* error_word);
 
 /* Ascending list of the indices i < n with values[i] != 0 (reference
  * generate_nonzero_compaction_indices, src/utils/stream-compaction.cuh:120-139);
@@ -597,6 +609,13 @@ int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports);
  * tn_trainer_train_step the last step's update is pending. tn_trainer_buffer, the full
  * occupancy update and stage timing apply it first. */
 int tn_trainer_flush(tn_trainer* tr);
+/* Clears the training data (reference NeRFTrainingController::reset_training,
+ * src/controllers/nerf-training-controller.cu:108-120, bound at
+ * src/api/python_bindings.cu:453-457): parameters re-drawn from the seed, Adam moments and
+ * per-parameter step counts zero, every occupancy bit set and densities zero
+ * (occupancy-grid.cuh:81-85), step counter and metrics zero. A pending Adam update is dropped.
+ * Buffers, launch shapes, the dataset and the network are kept. Synchronous. */
+int tn_trainer_reset(tn_trainer* tr);
 /* Launch shapes of the trainer's context; setting them (validated) makes the next step
  * capture its graph again. */
 int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out);

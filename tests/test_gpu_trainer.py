@@ -180,3 +180,26 @@ def test_pipelined_caller_ray_steps_match_synchronous_steps():
     assert b.sync_metrics().step == steps + 1
     a.teardown()
     b.teardown()
+
+
+def test_reset_training_starts_over():
+    """reset_training (reference NeRFTrainingController::reset_training) returns the trainer to
+    the state setup_data left: after a reset, three steps give the same metrics and the same
+    weights, moments, step counts and grid, bit for bit, as three steps of a fresh trainer."""
+    _, a = _make()
+    for _ in range(3):
+        a.train_step()
+    a.update_occupancy_grid(3)
+    a.reset_training()
+    ma = [a.train_step() for _ in range(3)]
+    _, b = _make()
+    mb = [b.train_step() for _ in range(3)]
+    for x, y in zip(ma, mb):
+        assert (x.step, x.n_rays, x.n_samples) == (y.step, y.n_rays, y.n_samples)
+        assert np.float32(x.loss) == np.float32(y.loss)
+    for idx, name in ((0, "weights"), (2, "first moments"), (3, "second moments"), (5, "grid density")):
+        assert_bitwise(_h(a.buffer(idx)), _h(b.buffer(idx)), name)
+    assert_bitwise(_h(a.buffer(4), np.uint32), _h(b.buffer(4), np.uint32), "param steps")
+    assert_bitwise(_h(a.buffer(6, np.uint8)), _h(b.buffer(6, np.uint8)), "bitfield")
+    a.teardown()
+    b.teardown()

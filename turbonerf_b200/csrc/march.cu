@@ -286,16 +286,23 @@ __device__ __forceinline__ bool block_total_and_ticket(uint32_t cnt, uint32_t* b
     return is_last;
 }
 
-// Pass 1: per-block totals; the last block scans them and applies the batch cut.
+// Pass 1: per-block totals; the last block scans them and applies the batch cut. Every error
+// bit of the call is raised by that last block; when flags_out is given, the block also stores
+// the final error word there (a plain store, so the caller's word needs no clearing).
 __global__ void __launch_bounds__(MARCH_BLOCK)
 scan_count_kernel(uint32_t n, const uint32_t* __restrict__ counts, uint32_t batch_size, uint32_t* batch_info,
-                  uint32_t* block_agg, uint32_t* block_prefix, uint32_t* ticket, uint32_t* flags) {
+                  uint32_t* block_agg, uint32_t* block_prefix, uint32_t* ticket, uint32_t* flags,
+                  uint32_t* flags_out) {
     const uint32_t i = blockIdx.x * MARCH_BLOCK + threadIdx.x;
     const uint32_t cnt = i < n ? counts[i] : 0u;
     if (!block_total_and_ticket<MARCH_BLOCK>(cnt, block_agg, ticket)) return;
     __threadfence();
     scan_blocks_and_cut<MARCH_BLOCK>(gridDim.x, n, counts, block_agg, block_prefix, batch_size, batch_info, flags);
-    if (threadIdx.x == 0) *ticket = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *ticket = 0u;
+        if (flags_out) *flags_out = atomicOr(flags, 0u);
+    }
 }
 
 // Pass 2: offsets = block scan + the block's prefix.
@@ -1416,7 +1423,8 @@ int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t*
     int st = ensure_block_u32(ctx, 2 * (size_t)nb);
     if (st != TN_OK) return st;
     scan_count_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, batch_size, batch_info, ctx->block_u32,
-                                                      ctx->block_u32 + nb, ctx->tickets + TICKET_SCAN, ctx->flags);
+                                                      ctx->block_u32 + nb, ctx->tickets + TICKET_SCAN, ctx->flags,
+                                                      nullptr);
     st = check_launch("tn_scan_offsets(count)");
     if (st != TN_OK) return st;
     scan_offsets_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, ctx->block_u32 + nb, offsets);
@@ -1431,32 +1439,66 @@ int tn_scan_offsets(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t*
 // error word) is a fixed array in device memory that lives in the library image itself and is
 // held by every device that loads the library until the process exits.
 //
-// Limit: at most TN_SCAN_NOALLOC_MAX_COUNTS counts per call (2 x 16,384 block entries =
-// 128 KiB of scratch). Every call uses the same array, so two calls that overlap on the GPU
-// (different streams, or different host threads on one device) race on it; serialise them.
+// Limit: at most TN_SCAN_NOALLOC_MAX_COUNTS counts per call (2 x 16,384 block entries plus 64
+// words: 128.25 KiB of scratch). Every call uses the same array, so two calls that overlap on
+// the GPU (different streams, or different host threads on one device) race on it; serialise
+// them.
 constexpr uint32_t NOALLOC_MAX_BLOCKS = TN_SCAN_NOALLOC_MAX_COUNTS / MARCH_BLOCK;
 constexpr uint32_t NOALLOC_WORDS = 2 * NOALLOC_MAX_BLOCKS + 64;  // [agg | prefix | ticket, flags, ...]
 static __device__ __align__(256) uint32_t g_scan_noalloc_scratch[NOALLOC_WORDS];
 
-// The array's name is a host-side stand-in in host code, not a device address: the device
-// address is looked up once per device (with that device current) and cached here.
-static uint32_t* g_scan_noalloc_ptr[64] = {};
+// In host code the array's name is a host-side stand-in, not a device address. The device
+// address is looked up with cudaGetSymbolAddress once per device, with that device current,
+// and cached together with the CUDA context it belongs to: after a cudaDeviceReset the device
+// gets a new primary context, the library's module is loaded again, and the address is looked
+// up again instead of reusing a stale one. The context is read through the driver entry point
+// (the runtime is linked statically and the library does not link libcuda).
+typedef int (*CtxGetCurrentFn)(void**);
+struct NoallocSlot {
+    void* ctx;
+    uint32_t* ptr;
+};
+static NoallocSlot g_scan_noalloc_slot[64] = {};
 static std::mutex g_scan_noalloc_mutex;
+
+static int current_context(void** ctx) {
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        int st = cuda_status(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q),
+                             "tn_scan_offsets_noalloc: cudaGetDriverEntryPoint");
+        if (st != TN_OK) return st;
+        TN_REQUIRE(q == cudaDriverEntryPointSuccess && f != nullptr, TN_E_CUDA,
+                   "tn_scan_offsets_noalloc: cuCtxGetCurrent not found");
+        fn = reinterpret_cast<CtxGetCurrentFn>(f);
+    }
+    TN_REQUIRE(fn(ctx) == 0, TN_E_CUDA, "tn_scan_offsets_noalloc: cuCtxGetCurrent failed");
+    return TN_OK;
+}
 
 static int scan_noalloc_scratch(uint32_t** out) {
     int dev = 0;
     int st = cuda_status(cudaGetDevice(&dev), "tn_scan_offsets_noalloc: cudaGetDevice");
     if (st != TN_OK) return st;
     TN_REQUIRE(dev >= 0 && dev < 64, TN_E_INVALID, "tn_scan_offsets_noalloc: device %d out of range", dev);
+    void* ctx = nullptr;
+    st = current_context(&ctx);
+    if (st != TN_OK) return st;
     std::lock_guard<std::mutex> lock(g_scan_noalloc_mutex);
-    if (!g_scan_noalloc_ptr[dev]) {
+    NoallocSlot& slot = g_scan_noalloc_slot[dev];
+    if (!slot.ptr || !ctx || slot.ctx != ctx) {
         void* p = nullptr;
+        // the lookup also makes the runtime's primary context current when none was
         st = cuda_status(cudaGetSymbolAddress(&p, g_scan_noalloc_scratch),
                          "tn_scan_offsets_noalloc: cudaGetSymbolAddress");
         if (st != TN_OK) return st;
-        g_scan_noalloc_ptr[dev] = static_cast<uint32_t*>(p);
+        st = current_context(&ctx);
+        if (st != TN_OK) return st;
+        slot.ptr = static_cast<uint32_t*>(p);
+        slot.ctx = ctx;
     }
-    *out = g_scan_noalloc_ptr[dev];
+    *out = slot.ptr;
     return TN_OK;
 }
 
@@ -1479,7 +1521,7 @@ int tn_compact_nonzero(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32
 }
 
 int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* counts, uint32_t* offsets,
-                            uint32_t batch_size, uint32_t* batch_info) {
+                            uint32_t batch_size, uint32_t* batch_info, uint32_t* error_word) {
     TN_NONNULL(counts); TN_NONNULL(offsets); TN_NONNULL(batch_info);
     TN_REQUIRE(n > 0, TN_E_NO_RAYS, "tn_scan_offsets_noalloc: n = 0");
     TN_REQUIRE(n <= TN_SCAN_NOALLOC_MAX_COUNTS, TN_E_CAPACITY,
@@ -1497,7 +1539,7 @@ int tn_scan_offsets_noalloc(tn_stream_t stream, uint32_t n, const uint32_t* coun
     if (st != TN_OK) return st;
     const uint32_t nb = (n + MARCH_BLOCK - 1) / MARCH_BLOCK;
     scan_count_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, batch_size, batch_info, block_agg, block_prefix, ticket,
-                                                      flags);
+                                                      flags, error_word);
     st = check_launch("tn_scan_offsets_noalloc(count)");
     if (st != TN_OK) return st;
     scan_offsets_kernel<<<nb, MARCH_BLOCK, 0, stream>>>(n, counts, block_prefix, offsets);

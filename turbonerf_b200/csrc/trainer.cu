@@ -1012,6 +1012,40 @@ int tn_trainer_load(tn_trainer* tr, const char* path) {
     return TN_OK;
 }
 
+// NeRFTrainingController::reset_training (src/controllers/nerf-training-controller.cu:108-120):
+// the reference frees the network's training data, the occupancy grid, the parameters and the
+// workspace, then runs setup_data again, which re-creates them as at the start of training
+// (parameters from the fixed seed, fresh optimizer state, every grid bit set, densities zero,
+// training_step = 0). Here the buffers are kept and rewritten to that state; the captured step
+// graphs stay valid, since they only hold the buffers' addresses. A pending Adam update belongs
+// to the discarded run and is dropped. The gradient source of the built-in stand-in network
+// (its fixed synthetic gradients) is the network's, not the trainer's, and is kept.
+int tn_trainer_reset(tn_trainer* tr) {
+    TN_NONNULL(tr);
+    cudaStream_t s = tr->stream;
+    int st = cuda_status(cudaStreamSynchronize(tr->h2d), "reset sync");
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->aux), "reset sync");
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "reset sync");
+    const size_t P = tr->P, V = tr->V, LV = (size_t)tr->d.grid.n_levels * V;
+    auto clear = [&](void* p, int value, size_t bytes) {
+        if (st == TN_OK) st = cuda_status(cudaMemsetAsync(p, value, bytes, s), "reset clear");
+    };
+    clear(tr->bits, 0xFF, V);  // occupancy-grid.cuh:81-85
+    clear(tr->density, 0, LV * 4);
+    clear(tr->m, 0, P * 4);
+    clear(tr->v, 0, P * 4);
+    clear(tr->steps, 0, P * 4);
+    clear(tr->state, 0, sizeof(StepState));
+    clear(tr->ctx->flags, 0, sizeof(uint32_t));
+    if (st == TN_OK) st = launch_synth_params(s, (uint32_t)P, tr->d.n_grid_params, tr->d.seed, tr->w);
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "reset sync");
+    if (st != TN_OK) return st;
+    tr->host_step = 0;
+    tr->last = tn_training_metrics{};
+    tr->ring_calls = 0;
+    return TN_OK;
+}
+
 int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,
                       uint32_t batch_size, float* out_rgba, tn_render_stats* stats) {
     TN_NONNULL(tr);

@@ -186,6 +186,7 @@ SIGNATURES = {
     "tn_trainer_autotune": [_vp, _P(TuneReport)],
     "tn_trainer_get_tuning": [_vp, _P(Tuning)],
     "tn_trainer_flush": [_vp],
+    "tn_trainer_reset": [_vp],
     "tn_trainer_set_tuning": [_vp, _P(Tuning)],
     "tn_rays_init_bbox": [_vp, _u32, _u32, _P(Bbox), _f32, _vp, _vp, _vp, _vp, _vp],
     "tn_march_count": [_vp, _vp, _P(GridDesc), _vp, _P(Bbox), _P(MarchDesc), _u32, _u32, _vp, _vp, _vp, _vp, _vp,
@@ -196,7 +197,7 @@ SIGNATURES = {
     "tn_multi_march_count": [_vp, _vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_multi_march_emit": [_vp, _vp, _u32, _vp, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                             _vp, _vp, _vp],
-    "tn_scan_offsets_noalloc": [_vp, _u32, _vp, _vp, _u32, _vp],
+    "tn_scan_offsets_noalloc": [_vp, _u32, _vp, _vp, _u32, _vp, _vp],
     "tn_compact_nonzero": [_vp, _vp, _u32, _vp, _vp, _vp],
     "tn_composite_fwd": [_vp, _vp, _P(RayBatchDesc), _i32, _f32, _vp, _vp, _vp, _vp, _vp, _vp],
     "tn_composite_bwd": [_vp, _vp, _P(RayBatchDesc), _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -169,10 +169,7 @@ class Trainer:
         waves = np.ascontiguousarray(n.waves, np.float32)
         call("tn_trainer_set_synthetic_field", h, blobs.shape[0], blobs.ctypes.data_as(ctypes.c_void_p),
              waves.ctypes.data_as(ctypes.c_void_p))
-        dens = None if n.density is None else np.ascontiguousarray(n.density, np.float32)
-        bits = None if n.bitfield is None else np.ascontiguousarray(n.bitfield, np.uint8)
-        call("tn_trainer_set_grid", h, dens.ctypes.data_as(ctypes.c_void_p) if dens is not None else None,
-             bits.ctypes.data_as(ctypes.c_void_p) if bits is not None else None)
+        self._upload_grid()
         if n.dataset is not None:
             cams = (native.CameraC * len(n.dataset.cameras))(*[c.c_struct() for c in n.dataset.cameras])
             im = n.dataset.images
@@ -182,6 +179,23 @@ class Trainer:
         touched = ctypes.c_uint32(0)
         call("tn_trainer_init_synthetic_gradients", h, float(synthetic_grad_std), ctypes.byref(touched))
         self.n_touched_grads = touched.value
+
+    def _upload_grid(self) -> None:
+        """The NeRF's initial occupancy grid (densities and/or bitfield), when it has one."""
+        n = self.nerf
+        dens = None if n.density is None else np.ascontiguousarray(n.density, np.float32)
+        bits = None if n.bitfield is None else np.ascontiguousarray(n.bitfield, np.uint8)
+        call("tn_trainer_set_grid", self._handle(), dens.ctypes.data_as(ctypes.c_void_p) if dens is not None else None,
+             bits.ctypes.data_as(ctypes.c_void_p) if bits is not None else None)
+
+    def reset_training(self) -> None:
+        """Clears the training data and starts over (reference reset_training,
+        nerf-training-controller.cu:108-120, which frees the training buffers and runs
+        setup_data again): parameters re-drawn from the seed, Adam moments and per-parameter
+        steps zero, the step counter zero, the occupancy grid re-initialised and the NeRF's
+        initial grid uploaded again, as setup_data does. Buffers and launch shapes are kept."""
+        call("tn_trainer_reset", self._handle())
+        self._upload_grid()
 
     def teardown(self) -> None:
         if self._h is not None:
