@@ -12,7 +12,9 @@ Prints ONE JSON line. `value` = samples/s of the fused, CUDA-graph-captured step
 inputs resident in HBM; `e2e` = the same through Trainer.train_step_rays_pipelined() with each
 step's host rays copied in and its metrics copied back and read by the host (one step later, the
 last one inside the timed region); `plain` = the one-kernel-per-stage path.
-`--impl reference` times the CPU restatement of the reference (the oracle) instead.
+`--impl reference` times the reference's own kernels compiled on the host cores (oracle/_ref,
+OpenMP) on the same workload instead, or the oracle's restatement where that library is not
+built.
 """
 from __future__ import annotations
 
@@ -472,10 +474,81 @@ class CpuStep:
         return nsamp
 
 
-def cpu_baseline(seconds=12.0):
+class RefCpuStep(CpuStep):
+    """The same train step through the reference's own kernels compiled on the host
+    (oracle/_ref: TurboNeRF's kernel sources, unchanged, with OpenMP over its CUDA threads):
+    march count and emit, fused reconstruction loss forward/backward, distortion loss forward
+    and backward, the gradient merge, the occupancy decay and threshold, the popcount and
+    Adam. Between them, as in the reference's host code: the exclusive scan and batch cut (the
+    reference: thrust), the stand-in network (the blob field), and the occupancy max-update of
+    the sampled cells (the reference's kernel for it cannot be compiled on the host: its
+    update_sigma_at returns nothing from a float function)."""
+
+    def __init__(self, seed=0x7B0):
+        super().__init__(seed)
+        from oracle import ref
+        self.r = ref
+        self.w32 = self.adam["w"].astype(np.float32)
+        P = self.w32.size
+        self.m32, self.v32, self.s32 = np.zeros(P, np.float32), np.zeros(P, np.float32), np.zeros(P, np.uint32)
+        self.w_copy = np.zeros(P, np.float32)
+
+    def step(self):
+        from turbonerf_b200 import scenes
+        o, r, sc = self.o, self.r, self.sc
+        rays = scenes.rays_init_bbox(scenes.sphere_rays(self.rng, RAYS), sc.bbox)
+        rd = rays.as_dict()
+        grid = dict(n_levels=5, res=128, base=1.0, bitfield=self.bits)
+        march = dict(bbox=np.float32(sc.bbox), cone=sc.cone_angle, dt_min=sc.dt_min, dt_max=sc.dt_max)
+        ns, alive = r.march_count(rd, grid, march)
+        st, off, nr, nsamp = o.scan_cut(ns, BATCH)
+        em = r.march_emit(rd, grid, march, off, ns, alive, nr, BATCH, 1.0 / sc.aabb_size)
+        sig, rgb = o.blob_field(em["pos"], BATCH, BATCH, sc.aabb_size, sc.field.blobs, sc.field.waves)
+        dens = (np.log(np.maximum(sig, 1e-30)) + 1.0).astype(np.float32)  # network density of that sigma
+        tgt = np.zeros(4 * BATCH, np.float32)
+        tgt[:3 * BATCH] = self.rng.uniform(0, 1, 3 * BATCH).astype(np.float32)
+        tgt[3 * BATCH:3 * BATCH + nr] = 1.0
+        bg = self.rng.uniform(0, 1, 3 * BATCH).astype(np.float32)
+        counts = ns[:nr]
+        rec = r.fused_reconstruction(counts, off[:nr], dens, rgb.astype(np.float32), em["dt"], tgt, bg, nr, BATCH)
+        _, ddist = r.distortion(counts, off[:nr], dens, em["m_norm"], em["dt_norm"], BATCH)
+        r.grad_merge(nsamp, 1.0, rec["dL_ddensity"], ddist, em["t"], np.zeros(BATCH, np.float32))
+        # occupancy: decay (reference) -> sampled cells' max-update -> threshold (reference)
+        lv = self.rng.integers(0, 5, OCC_CELLS).astype(np.int32)
+        cells = self.rng.integers(0, 128 ** 3, OCC_CELLS).astype(np.uint32)
+        r3 = self.rng.random(3 * OCC_CELLS).astype(np.float32)
+        pos = o.occupancy_sample_points(lv, cells, r3, OCC_CELLS, 128, 1.0, 1.0 / sc.aabb_size, OCC_CELLS)
+        vals, _ = o.blob_field(pos, OCC_CELLS, OCC_CELLS, sc.aabb_size, sc.field.blobs, sc.field.waves, want_rgb=False)
+        d = np.ascontiguousarray(self.density, np.float32).ravel()
+        r.occupancy_decay(d, 5, 128, 0.95)
+        rs = self.rng.random(OCC_CELLS)
+        sel = np.ones(OCC_CELLS, bool) if self.k < 256 else (rs < 0.25) | (
+            (rs <= 0.5) & ((self.bits[cells] >> lv) & 1).astype(bool))
+        idx = lv[sel].astype(np.int64) * 128 ** 3 + cells[sel]
+        np.maximum.at(d, idx, vals[sel].astype(np.float32))
+        self.density = d
+        r.occupancy_bits(d, self.bits, 5, 128, THRESHOLD)
+        r.popcount(self.bits)
+        lr = 1e-2 / (1.0 + 3.3e-5 * self.k)
+        r.adam_step(self.w32, self.grad, self.m32, self.v32, self.s32, N_GRID, N_MLP, lr, inplace=True,
+                    weights_copy=self.w_copy)
+        self.k += 1
+        return nsamp
+
+
+def _cpu_step():
+    """The reference's own kernels on the host when they are built (kind "reference"), else the
+    oracle's restatement (kind "port")."""
     import oracle
     oracle.build()
-    cs = CpuStep()
+    from oracle import ref
+    if ref.available():
+        return RefCpuStep(), "reference", ref.num_threads()
+    return CpuStep(), "port", oracle.num_threads()
+
+
+def cpu_baseline(seconds=12.0):
+    cs, kind, cores = _cpu_step()
     cs.step()  # warm-up (first touch of the buffers)
     t0 = time.perf_counter()
     samples, steps = 0, 0
@@ -485,17 +558,16 @@ def cpu_baseline(seconds=12.0):
         if time.perf_counter() - t0 >= seconds:
             break
     el = time.perf_counter() - t0
-    return {"value": round(samples / el, 1), "unit": "samples/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"{steps} full train steps of the same workload on the CPU oracle (OpenMP), {el:.1f} s"}
+    what = "the reference's kernels compiled on the host" if kind == "reference" else "the CPU oracle"
+    return {"value": round(samples / el, 1), "unit": "samples/s", "cores": cores, "kind": kind,
+            "sample": f"{steps} full train steps of the same workload on {what} (OpenMP), {el:.1f} s"}
 
 
 def run_reference(args):
     rank, world, _ = _env_rank()
     if rank != 0:
         return
-    import oracle
-    oracle.build()
-    cs = CpuStep()
+    cs, kind, cores = _cpu_step()
     for _ in range(max(args.warmup, 1)):
         cs.step()
     t0 = time.perf_counter()
@@ -505,15 +577,16 @@ def run_reference(args):
         samples += cs.step()
     el = time.perf_counter() - t0
     v = samples / el
-    cores = oracle.num_threads()
+    what = "the reference's kernels compiled on the host" if kind == "reference" else "the CPU oracle"
     line = {
         "metric": METRIC, "value": round(v, 1), "unit": "samples/s", "n_gpus": world, "steps": k,
         "warmup": args.warmup, "ms_per_step": round(el / k * 1e3, 2), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic", "impl": "reference",
+        "vs_baseline": None, "dtype": "f32" if kind == "reference" else "f64/f32", "data": "synthetic",
+        "impl": "reference",
         "config": {"workload": WORKLOAD, "batch_size_samples": BATCH, "rays_per_step": RAYS, "cascades": 5,
                    "parallelism": "cpu"},
-        "cpu_baseline": {"value": round(v, 1), "unit": "samples/s", "cores": cores, "kind": "port",
-                         "sample": f"{k} full train steps on the CPU oracle (OpenMP, {cores} threads)"},
+        "cpu_baseline": {"value": round(v, 1), "unit": "samples/s", "cores": cores, "kind": kind,
+                         "sample": f"{k} full train steps on {what} (OpenMP, {cores} threads)"},
         "e2e": {"value": round(v, 1), "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -3,8 +3,9 @@
 The oracle restates the reference kernels of TurboNeRF's training hot path on the CPU
 (FP32 with the reference's operation order for integer outputs, FP64 for float
 outputs). Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
-this module, and only as the checker or the timed CPU baseline. Parity is UNPINNED:
-the reference ships no tests or golden vectors and cannot be built here.
+this module, and only as the checker or the timed CPU baseline. The reference ships no tests
+or golden vectors; the restatement is pinned to the reference's own kernels compiled on the
+host (oracle/ref.py, oracle/_ref) through the fixtures under tests/golden/ref_*.npz.
 
 All arrays are numpy arrays in the reference's structure-of-arrays layout
 (component c of item i at buf[c * stride + i]).
@@ -64,10 +65,11 @@ def _declare(L):
                                   vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
         "orc_compact_nonzero": (i64, [i64, vp, vp]),
         "orc_recon_fwd_bwd": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, vp, vp, f64, f64, f64, f64,
-                                     vp, vp, vp, vp, vp, vp]),
+                                     vp, vp, vp, vp, vp, vp, vp]),
         "orc_recon_loss_rgb": (f64, [i64, i64, i64, vp, vp, i32, vp, vp, vp, vp, vp, f64, f64, vp]),
-        "orc_composite_fwd": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, f64, vp, vp]),
-        "orc_composite_vjp": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, f64, vp, vp, vp]),
+        "orc_composite_fwd": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, f64, vp, vp, vp]),
+        "orc_composite_vjp": (None, [i64, i64, i64, vp, vp, i32, vp, vp, vp, f64, vp, vp, vp, vp]),
+        "orc_cut_branches": (i64, [i64, vp, vp, i32, vp, vp, f64, f64, i32, vp, vp]),
         "orc_distortion_fwd_bwd": (None, [i64, vp, vp, i32, vp, vp, vp, f64, vp, vp, vp]),
         "orc_distortion_loss_sum": (f64, [i64, vp, vp, i32, vp, vp, vp, f64]),
         "orc_grad_epilogue": (None, [i64, f64, vp, vp, vp, vp]),
@@ -180,7 +182,9 @@ def compact_nonzero(values):
 
 
 def recon_fwd_bwd(counts, offsets, density, rgb, dt, target_rgba, bg_rgb, ray_stride, sample_stride,
-                  act=0, inv_nrays=None, grad_scale=1.0, min_t=1e-4, amb_eps=1e-4):
+                  act=0, inv_nrays=None, grad_scale=1.0, min_t=1e-4, amb_eps=1e-4, fixed_used=None):
+    """fixed_used (per ray, optional): composite exactly that many samples instead of stopping
+    at the transmittance cut (to evaluate the other side of a cut that rounding decides)."""
     n = len(counts)
     if inv_nrays is None:
         inv_nrays = 1.0 / max(n, 1)
@@ -193,7 +197,8 @@ def recon_fwd_bwd(counts, offsets, density, rgb, dt, target_rgba, bg_rgb, ray_st
     lib().orc_recon_fwd_bwd(n, ray_stride, sample_stride, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
                             _p(_c(density, np.float32)), _p(_c(rgb, np.float32)), _p(_c(dt, np.float32)),
                             _p(_c(target_rgba, np.float32)), _p(_c(bg_rgb, np.float32)), inv_nrays, grad_scale,
-                            min_t, amb_eps, _p(ray_rgba), _p(loss), _p(dd), _p(drgb), _p(used), _p(amb))
+                            min_t, amb_eps, _p(ray_rgba), _p(loss), _p(dd), _p(drgb), _p(used), _p(amb),
+                            _p(_c(fixed_used, np.uint32) if fixed_used is not None else None))
     return dict(ray_rgba=ray_rgba, loss=loss, dL_ddensity=dd, dL_drgb=drgb, n_used=used, ambiguous=amb)
 
 
@@ -209,24 +214,40 @@ def recon_loss_rgb(counts, offsets, density, rgb, dt, target_rgba, bg_rgb, ray_s
                                     _p(_c(bg_rgb, np.float64)), inv_nrays, min_t, _p(fu))
 
 
-def composite_fwd(counts, offsets, density, rgb, dt, ray_stride, sample_stride, act=0, min_t=1e-4):
+def composite_fwd(counts, offsets, density, rgb, dt, ray_stride, sample_stride, act=0, min_t=1e-4,
+                  fixed_used=None):
     n = len(counts)
     rgba = np.zeros(4 * ray_stride)
     used = np.zeros(n, np.uint32)
     lib().orc_composite_fwd(n, ray_stride, sample_stride, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
                             _p(_c(density, np.float32)), _p(_c(rgb, np.float32)), _p(_c(dt, np.float32)), min_t,
-                            _p(rgba), _p(used))
+                            _p(rgba), _p(used), _p(_c(fixed_used, np.uint32) if fixed_used is not None else None))
     return rgba, used
 
 
-def composite_vjp(counts, offsets, density, rgb, dt, grad_rgba, ray_stride, sample_stride, act=0, min_t=1e-4):
+def composite_vjp(counts, offsets, density, rgb, dt, grad_rgba, ray_stride, sample_stride, act=0, min_t=1e-4,
+                  fixed_used=None):
     n = len(counts)
     dd = np.zeros(sample_stride)
     drgb = np.zeros(3 * sample_stride)
     lib().orc_composite_vjp(n, ray_stride, sample_stride, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
                             _p(_c(density, np.float32)), _p(_c(rgb, np.float32)), _p(_c(dt, np.float32)), min_t,
-                            _p(_c(grad_rgba, np.float64)), _p(dd), _p(drgb))
+                            _p(_c(grad_rgba, np.float64)), _p(dd), _p(drgb),
+                            _p(_c(fixed_used, np.uint32) if fixed_used is not None else None))
     return dd, drgb
+
+
+def cut_branches(counts, offsets, density, dt, act=0, min_t=1e-4, band=1e-4, max_alt=8):
+    """Per ray, the sample counts at which an FP32 compositor may legitimately stop (the FP64
+    cut and every count whose transmittance after it is within `band` of min_t, up to the
+    first sample clearly below). Returns (n_alt [n], alt [n, max_alt], overflow)."""
+    n = len(counts)
+    n_alt = np.zeros(n, np.uint32)
+    alt = np.zeros((n, max_alt), np.uint32)
+    over = lib().orc_cut_branches(n, _p(_c(counts, np.uint32)), _p(_c(offsets, np.uint32)), act,
+                                  _p(_c(density, np.float32)), _p(_c(dt, np.float32)), min_t, band, max_alt,
+                                  _p(n_alt), _p(alt))
+    return n_alt, alt, int(over)
 
 
 def distortion_fwd_bwd(counts, offsets, density, m_norm, dt_norm, lam, n_samples, act=0, grad_ray=None):

@@ -370,7 +370,7 @@ void orc_recon_fwd_bwd(int64_t n_rays, int64_t ray_stride, int64_t sample_stride
                        const float* target_rgba, const float* bg_rgb,
                        double inv_nrays, double grad_scale, double min_t, double amb_eps,
                        double* ray_rgba, double* loss, double* dL_ddensity, double* dL_drgb,
-                       uint32_t* n_used, uint8_t* ambiguous) {
+                       uint32_t* n_used, uint8_t* ambiguous, const uint32_t* fixed_used) {
     const int64_t rs = ray_stride, ss = sample_stride;
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < n_rays; ++i) {
@@ -395,7 +395,7 @@ void orc_recon_fwd_bwd(int64_t n_rays, int64_t ray_stride, int64_t sample_stride
             trans *= (1.0 - alpha);
             ++used;
             if (std::fabs(trans - min_t) <= amb_eps * min_t) amb = 1;
-            if (trans < min_t) break;
+            if (fixed_used ? used >= fixed_used[i] : trans < min_t) break;
         }
         n_used[i] = used;
         ambiguous[i] = amb;
@@ -476,10 +476,50 @@ double orc_recon_loss_rgb(int64_t n_rays, int64_t ray_stride, int64_t sample_str
 // sample, with the same transmittance cut as density_to_ray_rgba_forward
 // (src/utils/training-kernels-fused.cuh:227-264).
 // ---------------------------------------------------------------------------
+// Sample counts at which an FP32 compositor may legitimately stop a ray. The reference breaks
+// after the first sample whose transmittance falls below min_t
+// (src/utils/training-kernels-fused.cuh:255, 337). A transmittance within a relative `band` of
+// min_t is decided by rounding: FP32 and FP64 may take different sides of it. So a ray may stop
+// after any sample whose transmittance lies inside the band, and at the latest after the first
+// sample clearly below it (or after its last sample). For each ray this lists those counts
+// (the FP64 cut among them; at most max_alt values, ascending; `overflow` counts the rays that
+// had more).
+int64_t orc_cut_branches(int64_t n_rays, const uint32_t* counts, const uint32_t* offsets, int act,
+                         const float* density, const float* dt, double min_t, double band, int max_alt,
+                         uint32_t* n_alt, uint32_t* alt) {
+    int64_t overflow = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : overflow)
+    for (int64_t i = 0; i < n_rays; ++i) {
+        const uint32_t n = counts[i];
+        const int64_t o = offsets[i];
+        uint32_t k = 0;
+        bool over = false;
+        auto add = [&](uint32_t u) {
+            if (k > 0 && alt[i * max_alt + k - 1] == u) return;
+            if ((int)k < max_alt) alt[i * max_alt + k++] = u;
+            else over = true;
+        };
+        double trans = 1.0;
+        uint32_t used = 0;
+        bool stopped = false;
+        for (uint32_t j = 0; j < n && !stopped; ++j) {
+            const double sigma = act_sigma(act, density[o + j]);
+            trans *= std::exp(-sigma * (double)dt[o + j]);
+            ++used;
+            if (std::fabs(trans - min_t) <= band * min_t) add(used);
+            if (trans < min_t * (1.0 - band)) { add(used); stopped = true; }
+        }
+        if (!stopped) add(used);
+        n_alt[i] = k;
+        overflow += over ? 1 : 0;
+    }
+    return overflow;
+}
+
 void orc_composite_fwd(int64_t n_rays, int64_t ray_stride, int64_t sample_stride,
                        const uint32_t* counts, const uint32_t* offsets, int act,
                        const float* density, const float* rgb, const float* dt, double min_t,
-                       double* ray_rgba, uint32_t* n_used) {
+                       double* ray_rgba, uint32_t* n_used, const uint32_t* fixed_used) {
     const int64_t rs = ray_stride, ss = sample_stride;
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < n_rays; ++i) {
@@ -494,7 +534,7 @@ void orc_composite_fwd(int64_t n_rays, int64_t ray_stride, int64_t sample_stride
             r += w * rgb[o + j]; g += w * rgb[o + j + ss]; bb += w * rgb[o + j + 2 * ss]; a += w;
             trans *= (1.0 - alpha);
             ++used;
-            if (trans < min_t) break;
+            if (fixed_used ? used >= fixed_used[i] : trans < min_t) break;
         }
         ray_rgba[i] = r; ray_rgba[i + rs] = g; ray_rgba[i + 2 * rs] = bb; ray_rgba[i + 3 * rs] = a;
         if (n_used) n_used[i] = used;
@@ -504,7 +544,7 @@ void orc_composite_fwd(int64_t n_rays, int64_t ray_stride, int64_t sample_stride
 void orc_composite_vjp(int64_t n_rays, int64_t ray_stride, int64_t sample_stride,
                        const uint32_t* counts, const uint32_t* offsets, int act,
                        const float* density, const float* rgb, const float* dt, double min_t,
-                       const double* grad_rgba, double* dL_ddensity, double* dL_drgb) {
+                       const double* grad_rgba, double* dL_ddensity, double* dL_drgb, const uint32_t* fixed_used) {
     const int64_t rs = ray_stride, ss = sample_stride;
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < n_rays; ++i) {
@@ -521,7 +561,7 @@ void orc_composite_vjp(int64_t n_rays, int64_t ray_stride, int64_t sample_stride
             trans *= (1.0 - alpha);
             T[j + 1] = trans;
             ++used;
-            if (trans < min_t) break;
+            if (fixed_used ? used >= fixed_used[i] : trans < min_t) break;
         }
         const double gr = grad_rgba[i], gg = grad_rgba[i + rs], gb = grad_rgba[i + 2 * rs], ga = grad_rgba[i + 3 * rs];
         double sr = 0, sg = 0, sb = 0, sa = 0;   // suffix sums over j > current

@@ -8,3 +8,12 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a) and the built libturbo_hot.so")
+
+
+def pytest_terminal_summary(terminalreporter):
+    from tests.helpers import ELEM_FLOOR, ELEMENTWISE_REPORT
+    if not ELEMENTWISE_REPORT:
+        return
+    terminalreporter.write_sep("-", f"element-wise gradient errors (entries >= {ELEM_FLOOR:g} of the largest)")
+    for what, n, worst in ELEMENTWISE_REPORT:
+        terminalreporter.write_line(f"{what:60s} {n:10d} entries  worst rel err {worst:.3e}")

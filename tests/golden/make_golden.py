@@ -1,9 +1,10 @@
 """Writes the small golden fixtures under tests/golden/ from the CPU oracle.
 
-The reference ships no golden vectors and cannot be built here, so these fixtures are the
-oracle's own outputs on seeded inputs. They pin the oracle against regressions
-(tests/test_golden.py) and give the GPU tests a fixed expected answer
-(tests/test_gpu_golden.py). Regenerate with: python tests/golden/make_golden.py
+The reference ships no golden vectors, so these fixtures are the oracle's own outputs on
+seeded inputs (the fixtures written from the reference's own kernels are ref_*.npz, made by
+make_ref_golden.py). They pin the oracle against regressions (tests/test_golden.py) and give
+the GPU tests a fixed expected answer (tests/test_gpu_golden.py). Regenerate with:
+python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -41,14 +42,24 @@ def march_fixture():
 
 
 def loss_fixture():
+    """Reconstruction and distortion losses on a seeded batch. Where a ray's transmittance lies
+    within rounding of the cut, the reference may stop it at more than one sample; br_* hold
+    the outputs at every legitimate set of cuts (branch 0 is the FP64 cut of every ray)."""
     sb = scenes.make_sample_batch(0x61, 3000, mean=20)
     n, ss = sb.n_rays, sb.n_samples
     rec = oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss)
     dl, dd = oracle.distortion_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.m_norm, sb.dt_norm, 1e-3, ss)
+    n_alt, alt, _ = oracle.cut_branches(sb.counts, sb.offsets, sb.sigma, sb.dt, band=1e-4)
+    br = []
+    for b in range(int(n_alt.max())):
+        fu = alt[np.arange(n), np.minimum(b, n_alt.astype(np.int64) - 1)]
+        br.append(oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n,
+                                       ss, fixed_used=fu))
     return dict(counts=sb.counts, offsets=sb.offsets, sigma=sb.sigma, rgb=sb.rgb, dt=sb.dt, m_norm=sb.m_norm,
                 dt_norm=sb.dt_norm, target=sb.target_rgba, bg=sb.bg_rgb, ray_rgba=rec["ray_rgba"], loss=rec["loss"],
                 dL_ddensity=rec["dL_ddensity"], dL_drgb=rec["dL_drgb"], n_used=rec["n_used"],
-                ambiguous=rec["ambiguous"], dist_loss=dl, dist_dd=dd)
+                ambiguous=rec["ambiguous"], dist_loss=dl, dist_dd=dd, n_alt=n_alt, alt=alt,
+                **{"br_" + k: np.stack([r[k] for r in br]) for k in ("ray_rgba", "loss", "dL_ddensity", "dL_drgb")})
 
 
 def occupancy_fixture():

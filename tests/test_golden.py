@@ -27,8 +27,11 @@ def test_march_fixture_reproduces():
 
 def test_loss_fixture_reproduces():
     fx, new = _load("loss_small"), make_golden.loss_fixture()
-    for k in ("ray_rgba", "loss", "dL_ddensity", "dL_drgb", "n_used", "dist_loss", "dist_dd"):
+    for k in ("ray_rgba", "loss", "dL_ddensity", "dL_drgb", "n_used", "dist_loss", "dist_dd", "n_alt", "alt",
+              "br_ray_rgba", "br_loss", "br_dL_ddensity", "br_dL_drgb"):
         _same(new[k], fx[k], k)
+    # branch 0 is the FP64 cut of every ray; the fixture holds rays that rounding decides
+    assert np.array_equal(fx["br_dL_ddensity"][0], fx["dL_ddensity"])
 
 
 def test_occupancy_fixture_reproduces():

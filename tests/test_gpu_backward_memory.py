@@ -5,7 +5,8 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import RTOL_GRAD, assert_norm_close, dev, expand_rays, host, i32
+from tests.helpers import (CUT_BAND, RTOL_GRAD, assert_norm_close, assert_per_ray_norm_close, branch_cuts, dev,
+                           host, i32, pick_branches, record_elementwise)
 from turbonerf_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -22,12 +23,21 @@ def test_backward_variants_match_oracle(variant):
     rb = hp.ray_batch(i32(sb.counts), i32(sb.offsets), n, n, ss)
     fn = hp.backward_recompute if variant == "recompute" else hp.backward_store
     dd, drgb, ddist = fn(ctx, rb, dev(sb.sigma), dev(sb.rgb), dev(sb.dt), dev(sb.m_norm), dev(sb.dt_norm), dev(g), lam)
-    ref_dd, ref_drgb = oracle.composite_vjp(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, g.astype(np.float64), n, ss)
     _, ref_dist = oracle.distortion_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.m_norm, sb.dt_norm, lam, ss)
-    rec = oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss,
-                               amb_eps=1e-5)
-    sm = expand_rays(rec["ambiguous"] == 0, sb.counts, sb.offsets, ss)
-    assert_norm_close(host(dd), ref_dd, RTOL_GRAD, f"compositor dL/dsigma ({variant})", mask=sm)
-    assert_norm_close(host(drgb), ref_drgb, RTOL_GRAD, f"dL/drgb ({variant})", mask=np.tile(sm, 3))
+    # the VJP at every legitimate set of transmittance cuts, assembled ray by ray from the closest
+    n_alt, alt, over = oracle.cut_branches(sb.counts, sb.offsets, sb.sigma, sb.dt, band=CUT_BAND)
+    assert over == 0
+    branches = []
+    for fu in branch_cuts(n_alt, alt):
+        a, b = oracle.composite_vjp(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, g.astype(np.float64), n, ss,
+                                    fixed_used=fu)
+        branches.append(dict(dd=a, drgb=b))
+    gpu = dict(dd=host(dd), drgb=host(drgb))
+    ref, _ = pick_branches(gpu, branches, sb.counts, sb.offsets, sample_keys=("dd", "drgb"), sample_stride=ss)
+    assert_norm_close(gpu["dd"], ref["dd"], RTOL_GRAD, f"compositor dL/dsigma ({variant})")
+    assert_per_ray_norm_close(gpu["dd"], ref["dd"], sb.counts, sb.offsets, RTOL_GRAD,
+                              f"compositor dL/dsigma per ray ({variant})")
+    assert_norm_close(gpu["drgb"], ref["drgb"], RTOL_GRAD, f"dL/drgb ({variant})")
+    record_elementwise(gpu["dd"], ref["dd"], f"backward {variant} compositor dL/dsigma")
     assert_norm_close(host(ddist), ref_dist, RTOL_GRAD, f"distortion dL/dsigma ({variant})")
     assert ctx.check() == 0

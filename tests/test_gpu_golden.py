@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from tests.helpers import RTOL_GRAD, assert_bitwise, assert_close, assert_norm_close, dev, expand_rays, host, i32
+from tests.helpers import RTOL_GRAD, assert_bitwise, assert_close, assert_norm_close, dev, host, i32, pick_branches
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -50,13 +50,16 @@ def test_losses_match_golden():
     rb = hp.ray_batch(i32(fx["counts"]), i32(fx["offsets"]), n, n, ss)
     out = hp.recon_loss_fwd_bwd(ctx, rb, dev(fx["sigma"]), dev(fx["rgb"]), dev(fx["dt"]), dev(fx["target"]),
                                 dev(fx["bg"]), inv_nrays=1.0 / n)
-    ok = fx["ambiguous"] == 0
+    # every ray against the fixture's branch closest to it (rays whose cut rounding decides carry
+    # one branch per legitimate cut)
+    gpu = {k: host(out[k]) for k in ("ray_rgba", "loss", "dL_ddensity", "dL_drgb")}
+    branches = [{k: fx["br_" + k][b] for k in gpu} for b in range(fx["br_ray_rgba"].shape[0])]
+    ref, _ = pick_branches(gpu, branches, fx["counts"], fx["offsets"], ray_keys=("ray_rgba", "loss"),
+                           sample_keys=("dL_ddensity", "dL_drgb"), ray_stride=n, sample_stride=ss)
     for c in range(4):
-        assert_close(host(out["ray_rgba"])[c * n:(c + 1) * n], fx["ray_rgba"][c * n:(c + 1) * n], 1e-5, "rgba",
-                     mask=ok)
-    sm = expand_rays(ok, fx["counts"], fx["offsets"], ss)
-    assert_norm_close(host(out["dL_ddensity"]), fx["dL_ddensity"], RTOL_GRAD, "dL/ddensity", mask=sm)
-    assert_norm_close(host(out["dL_drgb"]), fx["dL_drgb"], RTOL_GRAD, "dL/drgb", mask=np.tile(sm, 3))
+        assert_close(gpu["ray_rgba"][c * n:(c + 1) * n], ref["ray_rgba"][c * n:(c + 1) * n], 1e-5, "rgba")
+    assert_norm_close(gpu["dL_ddensity"], ref["dL_ddensity"], RTOL_GRAD, "dL/ddensity")
+    assert_norm_close(gpu["dL_drgb"], ref["dL_drgb"], RTOL_GRAD, "dL/drgb")
     d = hp.distortion_fwd_bwd(ctx, rb, dev(fx["sigma"]), dev(fx["m_norm"]), dev(fx["dt_norm"]), 1e-3)
     assert_norm_close(host(d["ray_loss"]), fx["dist_loss"], 1e-4, "distortion loss")
     assert_norm_close(host(d["dL_ddensity"]), fx["dist_dd"], RTOL_GRAD, "distortion gradient")

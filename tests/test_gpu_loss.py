@@ -9,8 +9,9 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import (RTOL_COMPOSITE, RTOL_GRAD, assert_bitwise, assert_close, assert_norm_close, assert_per_ray_norm_close,
-                           dev, expand_rays, host, i32)
+from tests.helpers import (CUT_BAND, RTOL_COMPOSITE, RTOL_GRAD, assert_bitwise, assert_close, assert_legal_cut,
+                           assert_norm_close, assert_per_ray_norm_close, branch_cuts, dev, host, i32, pick_branches,
+                           record_elementwise)
 from turbonerf_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -41,37 +42,52 @@ def test_composite_forward_and_vjp(mean, n_samples):
     rb = _rb(sb, counts, offsets)
     sig, rgb, dt = dev(sb.sigma), dev(sb.rgb), dev(sb.dt)
     out = hp.composite_fwd(ctx, rb, sig, rgb, dt)
-    ref_rgba, ref_used = oracle.composite_fwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, n, ss)
-    # rays whose transmittance check sits at the threshold within FP32 rounding may cut one
-    # sample apart; they are identified by the oracle and checked separately
-    rec = oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss,
-                               amb_eps=1e-5)
-    ok = rec["ambiguous"] == 0
-    assert ok.mean() > 0.97
-    _rgb_ok(ref_rgba, host(out["rgba"]), n, ok)
+    # every ray stops where the reference may stop it: at the FP64 cut, or, where the
+    # transmittance lies within rounding of the threshold, at one of the other legitimate counts
     used = host(out["n_used"]).view(np.uint32)
-    assert np.array_equal(used[ok], ref_used[ok])
+    n_alt, alt, over = oracle.cut_branches(sb.counts, sb.offsets, sb.sigma, sb.dt, band=CUT_BAND)
+    assert over == 0
+    assert_legal_cut(used, n_alt, alt)
+    # then every ray, the ones whose cut rounding decides included, against the oracle at that cut
+    ref_rgba, _ = oracle.composite_fwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, n, ss, fixed_used=used)
+    _rgb_ok(ref_rgba, host(out["rgba"]), n, None)
     g = np.random.default_rng(1).normal(size=4 * n)
     dd, drgb = hp.composite_bwd(ctx, rb, sig, rgb, dt, out["depth"], out["n_used"], dev(g.astype(np.float32)))
     ref_dd, ref_drgb = oracle.composite_vjp(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt,
-                                            g.astype(np.float32).astype(np.float64), n, ss)
-    sm = expand_rays(ok, sb.counts, sb.offsets, ss)
-    assert_per_ray_norm_close(host(dd), ref_dd, sb.counts, sb.offsets, RTOL_GRAD, "dL/dsigma", ray_mask=ok)
+                                            g.astype(np.float32).astype(np.float64), n, ss, fixed_used=used)
+    assert_per_ray_norm_close(host(dd), ref_dd, sb.counts, sb.offsets, RTOL_GRAD, "dL/dsigma")
     for c in range(3):
         assert_per_ray_norm_close(host(drgb)[c * ss:(c + 1) * ss], ref_drgb[c * ss:(c + 1) * ss], sb.counts, sb.offsets,
-                                  RTOL_GRAD, f"dL/drgb[{c}]", ray_mask=ok)
-    assert_norm_close(host(dd), ref_dd, RTOL_GRAD, "dL/dsigma (batch)", mask=sm)
+                                  RTOL_GRAD, f"dL/drgb[{c}]")
+    assert_norm_close(host(dd), ref_dd, RTOL_GRAD, "dL/dsigma (batch)")
+    record_elementwise(host(dd), ref_dd, f"composite VJP dL/dsigma, mean {mean}")
+    record_elementwise(host(drgb), ref_drgb, f"composite VJP dL/drgb, mean {mean}")
     # the store-instead-of-recompute variant: same composite, same VJP
     st = hp.composite_fwd_store(ctx, rb, sig, rgb, dt)
     assert_bitwise(host(st["n_used"]).view(np.uint32), used, "n_used (store variant)")
-    _rgb_ok(ref_rgba, host(st["rgba"]), n, ok)
+    _rgb_ok(ref_rgba, host(st["rgba"]), n, None)
     dd2, drgb2 = hp.composite_bwd_stored(ctx, rb, sig, rgb, dt, st["n_used"], st["t_saved"], st["w_saved"],
                                          dev(g.astype(np.float32)))
-    assert_per_ray_norm_close(host(dd2), ref_dd, sb.counts, sb.offsets, RTOL_GRAD, "dL/dsigma (stored)", ray_mask=ok)
+    assert_per_ray_norm_close(host(dd2), ref_dd, sb.counts, sb.offsets, RTOL_GRAD, "dL/dsigma (stored)")
     for c in range(3):
         assert_per_ray_norm_close(host(drgb2)[c * ss:(c + 1) * ss], ref_drgb[c * ss:(c + 1) * ss], sb.counts,
-                                  sb.offsets, RTOL_GRAD, f"dL/drgb[{c}] (stored)", ray_mask=ok)
+                                  sb.offsets, RTOL_GRAD, f"dL/drgb[{c}] (stored)")
     assert ctx.check() == 0
+
+
+def _recon_reference(sb, dens, act, gpu, grad_scale=1.0):
+    """The oracle's reconstruction fwd/bwd at every legitimate set of cuts, assembled ray by
+    ray from the branch closest to the GPU's outputs (gpu: dict of host arrays)."""
+    n, ss = sb.n_rays, sb.n_samples
+    n_alt, alt, over = oracle.cut_branches(sb.counts, sb.offsets, dens, sb.dt, act=act, band=CUT_BAND)
+    assert over == 0
+    recs = [oracle.recon_fwd_bwd(sb.counts, sb.offsets, dens, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss,
+                                 act=act, grad_scale=grad_scale, fixed_used=fu) for fu in branch_cuts(n_alt, alt)]
+    keys = [k for k in ("ray_rgba", "loss") if k in gpu]
+    skeys = [k for k in ("dL_ddensity", "dL_drgb") if k in gpu]
+    ref, _ = pick_branches(gpu, recs, sb.counts, sb.offsets, ray_keys=keys, sample_keys=skeys, ray_stride=n,
+                           sample_stride=ss)
+    return ref, recs, n_alt
 
 
 @pytest.mark.parametrize("act", [0, 1])
@@ -85,21 +101,23 @@ def test_recon_loss_fused_and_plain(act):
     rb = _rb(sb, counts, offsets)
     args = (dev(dens), dev(sb.rgb), dev(sb.dt), dev(sb.target_rgba), dev(sb.bg_rgb))
     out = hp.recon_loss_fwd_bwd(ctx, rb, *args, inv_nrays=1.0 / n, grad_scale=1.0, activation=act)
-    ref = oracle.recon_fwd_bwd(sb.counts, sb.offsets, dens, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss, act=act)
-    ok = ref["ambiguous"] == 0
-    _rgb_ok(ref["ray_rgba"], host(out["ray_rgba"]), n, ok)
+    gpu = {k: host(out[k]) for k in ("ray_rgba", "loss", "dL_ddensity", "dL_drgb")}
+    ref, _, n_alt = _recon_reference(sb, dens, act, gpu)
+    _rgb_ok(ref["ray_rgba"], gpu["ray_rgba"], n, None)
     for c in range(4):
-        assert_norm_close(host(out["loss"])[c * n:(c + 1) * n], ref["loss"][c * n:(c + 1) * n], 1e-4, f"loss[{c}]",
-                          mask=ok)
+        assert_norm_close(gpu["loss"][c * n:(c + 1) * n], ref["loss"][c * n:(c + 1) * n], 1e-4, f"loss[{c}]")
     ref_sum = ref["loss"][:4 * n].sum() / n
     assert abs(float(host(out["loss_sum"])[0]) - ref_sum) <= 1e-5 * abs(ref_sum)
-    sm = expand_rays(ok, sb.counts, sb.offsets, ss)
-    assert_norm_close(host(out["dL_ddensity"]), ref["dL_ddensity"], RTOL_GRAD, "dL/ddensity", mask=sm)
-    assert_norm_close(host(out["dL_drgb"]), ref["dL_drgb"], RTOL_GRAD, "dL/drgb", mask=np.tile(sm, 3))
+    assert_norm_close(gpu["dL_ddensity"], ref["dL_ddensity"], RTOL_GRAD, "dL/ddensity")
+    assert_norm_close(gpu["dL_drgb"], ref["dL_drgb"], RTOL_GRAD, "dL/drgb")
+    assert_per_ray_norm_close(gpu["dL_ddensity"], ref["dL_ddensity"], sb.counts, sb.offsets, RTOL_GRAD,
+                              "dL/ddensity per ray", floor=1e-3)
+    record_elementwise(gpu["dL_ddensity"], ref["dL_ddensity"], f"reconstruction dL/ddensity, act {act}")
     # the plain path (reference structure, one thread per ray, FP32 suffix subtraction)
     loss, dd, drgb, lsum = hp.plain_recon_loss(rb, *args, inv_nrays=1.0 / n, grad_scale=1.0, activation=act)
+    ref_p, _, _ = _recon_reference(sb, dens, act, {"dL_ddensity": host(dd)})
     assert abs(lsum - ref_sum) <= 1e-4 * abs(ref_sum)
-    assert_norm_close(host(dd), ref["dL_ddensity"], 1e-3, "plain dL/ddensity", mask=sm)
+    assert_norm_close(host(dd), ref_p["dL_ddensity"], 1e-3, "plain dL/ddensity")
     assert ctx.check() == 0
 
 
@@ -154,15 +172,23 @@ def test_train_losses_fused_matches_oracle_chain(mean, max_count, n_samples, sig
     gd, drgb, sums = hp.train_losses(ctx, rb, dev(sb.sigma), dev(sb.rgb), dev(sb.dt), dev(sb.m_norm), dev(sb.dt_norm),
                                      dev(t_world), dev(sb.target_rgba), dev(sb.bg_rgb), gd, inv_nrays=1.0 / n,
                                      grad_scale=scale, lam=lam, ray_rgba=ray_rgba)
-    rec = oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss,
-                               grad_scale=scale)
     dl, ddist = oracle.distortion_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.m_norm, sb.dt_norm, lam, ss)
-    ref_g = oracle.grad_epilogue(ss, scale, rec["dL_ddensity"], ddist, t_world, grad_in.astype(np.float64))
-    ok = rec["ambiguous"] == 0
-    sm = expand_rays(ok, sb.counts, sb.offsets, ss)
-    assert_norm_close(host(gd), ref_g, RTOL_GRAD, "merged density gradient", mask=sm)
-    assert_norm_close(host(drgb), rec["dL_drgb"], RTOL_GRAD, "dL/drgb", mask=np.tile(sm, 3))
-    _rgb_ok(rec["ray_rgba"], host(ray_rgba), n, ok)
+    # the merged gradient of every legitimate set of cuts (the distortion loss has no cut)
+    n_alt, alt, over = oracle.cut_branches(sb.counts, sb.offsets, sb.sigma, sb.dt, band=CUT_BAND)
+    assert over == 0
+    branches = []
+    for fu in branch_cuts(n_alt, alt):
+        r = oracle.recon_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.rgb, sb.dt, sb.target_rgba, sb.bg_rgb, n, ss,
+                                 grad_scale=scale, fixed_used=fu)
+        r["g"] = oracle.grad_epilogue(ss, scale, r["dL_ddensity"], ddist, t_world, grad_in.astype(np.float64))
+        branches.append(r)
+    gpu = dict(g=host(gd), dL_drgb=host(drgb), ray_rgba=host(ray_rgba))
+    rec, _ = pick_branches(gpu, branches, sb.counts, sb.offsets, ray_keys=("ray_rgba",), sample_keys=("g", "dL_drgb"),
+                           ray_stride=n, sample_stride=ss, carry_ray_keys=("loss",))
+    assert_norm_close(gpu["g"], rec["g"], RTOL_GRAD, "merged density gradient")
+    assert_norm_close(gpu["dL_drgb"], rec["dL_drgb"], RTOL_GRAD, "dL/drgb")
+    record_elementwise(gpu["g"], rec["g"], f"train losses merged gradient, mean {mean}, sigma x{sigma_scale:g}")
+    _rgb_ok(rec["ray_rgba"], gpu["ray_rgba"], n, None)
     s = host(sums)
     assert abs(s[0] - rec["loss"][:4 * n].sum() / n) <= 1e-5 * abs(rec["loss"][:4 * n].sum() / n)
     assert abs(s[1] - dl.mean()) <= 1e-5 * abs(dl.mean())

@@ -5,7 +5,8 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import RTOL_GRAD, assert_bitwise, assert_norm_close, expand_rays
+from tests.helpers import (CUT_BAND, RTOL_GRAD, assert_bitwise, assert_norm_close, branch_cuts, pick_branches,
+                           record_elementwise)
 from turbonerf_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -59,13 +60,21 @@ def test_fused_step_matches_oracle_stage_by_stage():
     bg = _h(tr.buffer(23))
     tgt_c = np.concatenate([tgt[c * R:c * R + nr] for c in range(4)])
     bg_c = np.concatenate([bg[c * R:c * R + nr] for c in range(3)])
-    rec = oracle.recon_fwd_bwd(ns[:nr], off[:nr], sig, rgb, em["dt"], tgt_c, bg_c, nr, B)
     dl, ddist = oracle.distortion_fwd_bwd(ns[:nr], off[:nr], sig, em["m_norm"], em["dt_norm"], 1e-3, B)
-    ref_g = oracle.grad_epilogue(nsamp, 1.0, rec["dL_ddensity"][:nsamp], ddist[:nsamp], em["t"][:nsamp],
-                                 np.zeros(nsamp))
-    ok = rec["ambiguous"] == 0
-    sm = expand_rays(ok, ns[:nr], off[:nr], nsamp)
-    assert_norm_close(_h(tr.buffer(15))[:nsamp], ref_g, RTOL_GRAD, "merged density gradient", mask=sm)
+    # every legitimate set of transmittance cuts, the closest ray by ray
+    n_alt, alt, over = oracle.cut_branches(ns[:nr], off[:nr], sig, em["dt"], band=CUT_BAND)
+    assert over == 0
+    branches = []
+    for fu in branch_cuts(n_alt, alt):
+        r = oracle.recon_fwd_bwd(ns[:nr], off[:nr], sig, rgb, em["dt"], tgt_c, bg_c, nr, B, fixed_used=fu)
+        r["g"] = oracle.grad_epilogue(nsamp, 1.0, r["dL_ddensity"][:nsamp], ddist[:nsamp], em["t"][:nsamp],
+                                      np.zeros(nsamp))
+        branches.append(r)
+    gpu = dict(g=_h(tr.buffer(15))[:nsamp])
+    rec, _ = pick_branches(gpu, branches, ns[:nr], off[:nr], sample_keys=("g",), sample_stride=nsamp,
+                           carry_ray_keys=("loss",), ray_stride=nr)
+    assert_norm_close(gpu["g"], rec["g"], RTOL_GRAD, "merged density gradient")
+    record_elementwise(gpu["g"], rec["g"], "train step merged density gradient (4096 rays)")
     ref_loss = rec["loss"][:4 * nr].sum() / nr + dl.mean()
     assert abs(m.loss - ref_loss) <= 1e-5 * abs(ref_loss)
     # Adam on the fixed synthetic gradients
