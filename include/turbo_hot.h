@@ -575,7 +575,13 @@ int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bit
 int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_touched_out);
 /* One training step (reference NeRFTrainingController::train_step,
  * nerf-training-controller.cu:185-212). With metrics == NULL the fused path only enqueues
- * (no host synchronisation); otherwise the call waits and fills the metrics. */
+ * (no host synchronisation); otherwise the call waits and fills the metrics.
+ * With tn_tuning side_sms > 0 (the default when at least 16 SMs remain beside a march of
+ * 256-ray blocks) the fused path counts ahead: the step's tail (emit, network, losses, Adam,
+ * occupancy update) runs beside the next step's rays and march count, which start once the
+ * occupancy update has rewritten the grid; results are those of the in-order step, bit for
+ * bit. A head counted ahead is dropped when the grid, the ray source or the launch shapes
+ * change. */
 int tn_trainer_train_step(tn_trainer* tr, tn_training_metrics* metrics);
 /* The same step on rays supplied by the caller in host memory (pinned for asynchronous
  * copies): ori/dir [3][n_rays], target_rgba [4][n_rays], bg_rgb [3][n_rays]; n_rays must
@@ -584,12 +590,13 @@ int tn_trainer_train_step(tn_trainer* tr, tn_training_metrics* metrics);
 int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori, const float* dir,
                                const float* target_rgba, const float* bg_rgb, tn_training_metrics* metrics);
 /* The same step as tn_trainer_train_step_rays, pipelined for a training loop that feeds rays
- * from the host: the call enqueues this step (ray copies in, the step, a copy of its state and
- * error word out) and returns the metrics of the previous pipelined step in *previous, waiting
- * for that step only, so the GPU always has the next step queued. previous->step = 0 on the
- * first pipelined call (after a synchronous read: tn_trainer_sync_metrics returns the last
- * step's metrics). A previous step's device error is reported by this call's status. The host
- * arrays of a step must stay unchanged until the call after it returns. Fused path only. */
+ * from the host: the call copies this step's rays in and enqueues the tail of the previous
+ * pipelined step beside this step's rays and march count (its head), then returns the
+ * previous step's metrics in *previous, waiting for that step's tail only, so the GPU always
+ * has work queued. previous->step = 0 on the first pipelined call (after a synchronous read:
+ * tn_trainer_sync_metrics runs the last step's tail and returns its metrics). A previous step's
+ * device error is reported by this call's status. The host arrays of a step must stay
+ * unchanged until the call after it returns. Fused path only. */
 int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const float* ori, const float* dir,
                                          const float* target_rgba, const float* bg_rgb,
                                          tn_training_metrics* previous);
@@ -603,17 +610,15 @@ int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages
  * captures its graph again with the chosen shapes. reports[3] (may be NULL): count, emit,
  * losses. Synchronous. */
 int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports);
-/* Applies a pending Adam update and waits for the trainer's stream. With tn_tuning side_sms
- * > 0 (the default when at least 16 SMs remain beside a march of 256-ray blocks) each step's
- * Adam update runs at the start of the next step beside its march, so after
- * tn_trainer_train_step the last step's update is pending. tn_trainer_buffer, the full
- * occupancy update and stage timing apply it first. */
+/* Runs the tail of a pipelined caller-ray step still pending (tn_trainer_train_step_rays_pipelined
+ * leaves it to the next call) and waits for the trainer's stream. tn_trainer_buffer, the
+ * snapshot, render and metric calls do the same first. */
 int tn_trainer_flush(tn_trainer* tr);
 /* Clears the training data (reference NeRFTrainingController::reset_training,
  * src/controllers/nerf-training-controller.cu:108-120, bound at
  * src/api/python_bindings.cu:453-457): parameters re-drawn from the seed, Adam moments and
  * per-parameter step counts zero, every occupancy bit set and densities zero
- * (occupancy-grid.cuh:81-85), step counter and metrics zero. A pending Adam update is dropped.
+ * (occupancy-grid.cuh:81-85), step counter and metrics zero.
  * Buffers, launch shapes, the dataset and the network are kept. Synchronous. */
 int tn_trainer_reset(tn_trainer* tr);
 /* Launch shapes of the trainer's context; setting them (validated) makes the next step
@@ -624,7 +629,7 @@ int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t);
  * network) with tn_render (reference NeRFRenderingController::submit,
  * src/controllers/nerf-rendering-controller.cu:50). render_bbox NULL selects the training
  * box; min_step_size <= 0 the trainer's; batch_size 0 the tn_render default.
- * Applies a pending Adam update first. */
+ * A pending caller-ray step completes first. */
 int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,
                       uint32_t batch_size, float* out_rgba, tn_render_stats* stats);
 /* Trains on rays from posed images instead of the built-in synthetic rays (the reference trains
@@ -644,7 +649,7 @@ int tn_trainer_set_alpha_selection(tn_trainer* tr, float threshold, float probab
  * carries the hash-grid count, n_color_params the MLP count) and the occupancy bitfield, which
  * the reference's loader reads; then a resume block of this library (Adam moments and step
  * counts, grid densities, the trainer's step counters) that the reference's loader ignores.
- * Save applies a pending Adam update first and synchronises. Load restores into a trainer
+ * Save completes a pending caller-ray step first and synchronises. Load restores into a trainer
  * created with the same parameter counts, grid and box: everything the file holds, so a file
  * with the resume block continues training exactly; a reference file (no resume block) sets
  * the parameters and the bitfield and leaves the rest. */
@@ -678,7 +683,9 @@ int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out);
  * 11 ray n_steps, 12 batch_info[4], 13 network density, 14 network rgb,
  * 15 grad density, 16 dL/drgb, 17 ray origins, 18 ray directions, 19 ray t,
  * 20 ray t_max, 21 ray alive, 22 target rgba, 23 background rgb, 24 m_norm, 25 dt_norm,
- * 26 the dataset rays' draws [2][n_rays] (pixel, alpha selection; NULL without a dataset). */
+ * 26 the dataset rays' draws [2][n_rays] (pixel, alpha selection; NULL without a dataset),
+ * the last step's occupancy update inputs (occupancy_cells_per_step entries each): 27 levels,
+ * 28 Morton cells, 29 network density values, 30 selection draws. */
 int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes);
 
 #ifdef __cplusplus

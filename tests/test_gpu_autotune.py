@@ -264,12 +264,13 @@ def test_trainer_autotune_trains_identically():
         assert_bitwise(host(a.buffer(k, dt)), host(b.buffer(k, dt)), what)
 
 
-def test_pipelined_adam_matches_in_order_adam():
-    """The default trainer runs each step's Adam update at the start of the next step, beside
-    its march, on SMs the march leaves free. Against a trainer that runs Adam in order at the
-    end of each step (side_sms = 0): identical metrics every step, and after the pending update
-    is applied (buffer access flushes it) bit-identical parameters, moments, step counters,
-    grid densities and bitfield. A second flush applies nothing more."""
+def test_count_ahead_matches_in_order_steps():
+    """The default trainer runs each step's tail (emit, network, losses, Adam, occupancy update)
+    beside the next step's head (its rays and march count, started once the occupancy update has
+    rewritten the grid). Against a trainer that runs every step in order (side_sms = 0): identical
+    metrics every step and bit-identical rays, counts, parameters, moments, step counters, grid
+    densities and bitfield, also after buffer reads between steps (which leave the head computed
+    ahead in place), after a grid change (which drops it) and with the launch shapes changed."""
     from turbonerf_b200.trainer import SyntheticNeRF, Trainer
     sc = scenes.march_scene_cascaded(n_rays=8, n_levels=5)
 
@@ -281,21 +282,43 @@ def test_pipelined_adam_matches_in_order_adam():
         tr.setup_data(batch_size=1 << 16)
         return tr
 
+    def same(a, b, tag):
+        for k, what in ((0, "weights"), (2, "first moments"), (3, "second moments"), (4, "param steps"),
+                        (5, "grid density"), (6, "bitfield"), (11, "n_steps"), (10, "offsets"), (17, "origins")):
+            dt = np.uint8 if k == 6 else (np.uint32 if k in (4, 10, 11) else np.float32)
+            assert_bitwise(host(a.buffer(k, dt)), host(b.buffer(k, dt)), f"{what} {tag}")
+
     a, b = make(), make()
-    assert a.tuning["side_sms"] > 0, "the trainer pipelines Adam by default"
+    assert a.tuning["side_sms"] > 0, "the trainer counts ahead by default"
     b.tuning = dict(side_sms=0)
-    for _ in range(5):  # eager first step, then graph capture and replays
+    for i in range(6):  # eager first runs, then graph capture and replays of both ray sets
         ma, mb = a.train_step(), b.train_step()
         assert (ma.step, ma.n_rays, ma.n_samples) == (mb.step, mb.n_rays, mb.n_samples)
         assert ma.loss == mb.loss
-    for k, what in ((0, "weights"), (2, "first moments"), (3, "second moments"), (4, "param steps"),
-                    (5, "grid density"), (6, "bitfield")):
-        dt = np.uint8 if k == 6 else (np.uint32 if k == 4 else np.float32)
-        assert_bitwise(host(a.buffer(k, dt)), host(b.buffer(k, dt)), what)
-    w1 = host(a.buffer(0)).copy()
-    a.flush()
-    assert_bitwise(host(a.buffer(0)), w1, "weights after a second flush")
-    # training goes on after a flush: the next step's graph skips the update already applied
-    ma, mb = a.train_step(), b.train_step()
-    assert ma.loss == mb.loss
-    assert_bitwise(host(a.buffer(0)), host(b.buffer(0)), "weights one step after the flush")
+        if i == 2:
+            same(a, b, "mid-run")
+    same(a, b, "after six steps")
+    # a grid change drops the head computed ahead from the old grid
+    bits = host(a.buffer(6, np.uint8)).copy()
+    bits[::7] = 0
+    for t in (a, b):
+        call_set_grid(t, bits)
+    for _ in range(3):
+        ma, mb = a.train_step(), b.train_step()
+        assert (ma.step, ma.n_rays, ma.n_samples, ma.loss) == (mb.step, mb.n_rays, mb.n_samples, mb.loss)
+    same(a, b, "after a grid change")
+    # asynchronous steps, then the metrics
+    for _ in range(3):
+        a.train_step_async()
+        b.train_step_async()
+    ma, mb = a.sync_metrics(), b.sync_metrics()
+    assert (ma.step, ma.loss) == (mb.step, mb.loss)
+    same(a, b, "after asynchronous steps")
+    a.teardown()
+    b.teardown()
+
+
+def call_set_grid(tr, bits):
+    import ctypes
+    from turbonerf_b200 import native
+    native.call("tn_trainer_set_grid", tr._handle(), None, bits.ctypes.data_as(ctypes.c_void_p))

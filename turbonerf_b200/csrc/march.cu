@@ -437,13 +437,14 @@ __device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const Ray
         const float tz = axis_dt(fz, hz, r.idz, kc);
         const float t_target = fmaxf(a.dt_min, fminf(fminf(tx, ty), tz));
         const float t_skip = __fadd_rn(t, __fmul_rn(div_ru_pos(t_target, a.dt_min, a.inv_dt_min), a.dt_min));
-        if (occ) {
-            if (n < slot_cap) slots[n] = t;
-            t = __fadd_rn(t, dt);
-            if (++n >= max_steps) break;
-        } else {
-            t = t_skip;
-        }
+        // branch-free step: the slot store runs every iteration (a skip's t is overwritten by the
+        // next occupied step, and the emit pass reads only the first n slots), so the select of
+        // the successor carries no branch
+        if (n < slot_cap) slots[n] = t;
+        const float t_occ = __fadd_rn(t, dt);
+        t = occ ? t_occ : t_skip;
+        n += occ ? 1u : 0u;
+        if (n >= max_steps) break;
     }
     return n;
 }

@@ -5,12 +5,21 @@
 // reconstruction + distortion losses with the gradient merge -> network backward ->
 // [occupancy re-sampling of random cells] -> Adam.
 //
-// Pipelined Adam (tn_tuning side_sms > 0, the trainer's default when the SMs allow it): a
-// step's Adam update is left pending and runs at the start of the next step on a second stream,
-// on side_sms SMs, beside that step's march (which holds the other SMs: see exclusive_smem);
-// the next network forward waits for it. The march reads no parameters, so every step computes
-// what the reference computes. A pending update is applied by tn_trainer_flush and before the
-// trainer's buffers are handed out, the full occupancy update and stage timing.
+// Count-ahead schedule (tn_tuning side_sms > 0, the trainer's default when the SMs allow it):
+// a step is split into its head (the rays and the march count with the batch cut) and its tail
+// (emit, network forward, losses, network backward, Adam, and the step's occupancy update).
+// The march count is bound by the latency of its longest ray (a dependent chain of a few
+// hundred steps), not by bandwidth, and fills only part of the GPU; so each step's tail runs
+// beside the next step's head: the next step's rays and count start as soon as this step's
+// occupancy update has rewritten the bitfield (the count must see the updated grid, as in the
+// reference's order), on count_rays_per_block-ray blocks that each hold an SM alone (see
+// exclusive_smem), while Adam runs on the other side_sms SMs. The two steps in flight use two
+// sets of ray buffers and two march contexts (slots, per-block scan totals, error word). Every
+// step computes what the in-order schedule computes, bit for bit: the head of step N+1 reads
+// only its own rays and the grid after step N's update, and the tail of step N reads only its
+// own set. A head computed ahead for the trainer's own rays is dropped when anything it read
+// changes (grid, dataset, launch shapes, a load or reset); a head of caller rays (the
+// pipelined caller-ray call) is completed by its tail before the trainer's state is read.
 //
 // Fused path: every stage is one of the library's fused kernels; every step-dependent
 // scalar (step index, learning rate, occupancy selection policy, ray and sample counts)
@@ -18,9 +27,11 @@
 // replayed without any host synchronisation.
 // Plain path: the reference's launch structure (thrust scans, blocking device->host reads of
 // the sample count and the losses, separate memsets and epilogue kernels, dense Adam).
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "tn_internal.cuh"
@@ -30,23 +41,26 @@ namespace tn {
 struct StepState {
     unsigned long long samples_total;  // samples processed by all steps so far
     unsigned long long rays_total;     // rays used by all steps so far
-    uint32_t step_count;   // completed steps
+    uint32_t step_count;   // started steps; also the key of the next step's rays
     uint32_t cur_step;     // index of the running step
     float lr;              // decayed learning rate of the running step
     uint32_t sample_all;   // occupancy selection policy: 1 while cur_step < 256
-    uint32_t batch_info[4];
+    uint32_t batch_info[4];  // batch cut of the last completed step
     uint32_t n_occupied;
     float loss_sums[2];
-    float adam_lr;          // learning rate of the step whose Adam update is pending
-    uint32_t adam_pending;  // 1 while the last step's Adam update has not run
-    uint32_t pad;
+    uint32_t err;          // error bits of the completed steps not yet read (TN_FLAG_*)
+    uint32_t pad[3];
 };
 
-__global__ void step_end_kernel(StepState* s, uint32_t adam_left_pending) {
-    s->samples_total += s->batch_info[1];
-    s->rays_total += s->batch_info[0];
-    s->adam_lr = s->lr;
-    s->adam_pending = adam_left_pending;
+// End of a step's tail: its batch cut becomes the state's, the totals grow, and the error bits
+// of the step's march context move into the state (the context's word is left clear for the
+// head that will use it next).
+__global__ void step_end_kernel(StepState* s, const uint32_t* __restrict__ info, uint32_t* ctx_flags) {
+    for (int k = 0; k < 4; ++k) s->batch_info[k] = info[k];
+    s->samples_total += info[1];
+    s->rays_total += info[0];
+    s->err |= *ctx_flags;
+    *ctx_flags = 0u;
 }
 
 __global__ void step_begin_kernel(StepState* s, float base_lr, float lr_decay) {
@@ -84,19 +98,39 @@ static int synth_density(void* user, tn_stream_t stream, uint32_t n, const uint3
 
 using namespace tn;
 
+// One set of per-step ray buffers with the march context that counted them: two steps are in
+// flight at once in the count-ahead schedule (the tail of one, the head of the next).
+struct RaySet {
+    float *ori = nullptr, *dir = nullptr, *target = nullptr, *bg = nullptr;  // one allocation, [3|3|4|3][R]
+    float *ray_t = nullptr, *ray_tmax = nullptr;
+    uint8_t* alive = nullptr;
+    uint32_t *n_steps = nullptr, *offsets = nullptr;
+    uint32_t* info = nullptr;      // device batch_info[4] of this set's count
+    float* ds_random = nullptr;    // [2][R] dataset draws of this set's rays (with a dataset)
+    tn_ctx* ctx = nullptr;
+};
+
+// Step graphs: in-order step (head + tail of one step), tail of this step + head of the next,
+// head alone, tail alone; per ray source (own, caller) and per ray set of the tail.
+enum StepKind : int { K_HT = 0, K_TH = 1, K_H = 2, K_T = 3, K_KINDS = 4 };
+
 struct tn_trainer {
     tn_trainer_desc d{};
     tn_network net{};
     SynthNet synth;
     cudaStream_t stream = nullptr;
-    // second stream of the captured step: occupancy query and update beside the training chain
-    cudaStream_t aux = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_emit = nullptr, ev_join = nullptr, ev_adam = nullptr;
-    tn_ctx* ctx = nullptr;
+    // the occupancy query and update beside the training chain, and the next step's head
+    cudaStream_t aux = nullptr, cstream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_emit = nullptr, ev_occ = nullptr, ev_head = nullptr;
+    RaySet set[2];
+    int cur = 0;               // set of the last completed step (the aliases below point into it)
+    bool spec_own = false;     // set cur ^ 1 holds the head of the next step, computed from own rays
+    bool pending_ext = false;  // set cur ^ 1 holds the head of a requested caller-ray step, tail not run
+    tn_ctx* ctx = nullptr;     // set[cur].ctx
     std::vector<void*> allocs;
     uint32_t R = 0, B = 0, V = 0, P = 0, M = 0, chunk = 0;
     float aabb = 1.0f;
-    // rays
+    // rays of the last completed step (aliases of set[cur])
     float *ori, *dir, *ray_t, *ray_tmax, *target, *bg;
     uint8_t* alive;
     uint32_t *n_steps, *offsets;
@@ -122,8 +156,7 @@ struct tn_trainer {
     // pipelined caller-ray steps: each step's state and error word copied to pinned slots
     // (alternating), read by the host one call later
     StepState* ring_state = nullptr;  // pinned [2]
-    uint32_t* ring_flags = nullptr;   // pinned [2]
-    cudaEvent_t ev_ring[2] = {nullptr, nullptr};
+    volatile uint32_t* ring_flag = nullptr;  // pinned [2]: step count of the state in the slot
     uint64_t ring_calls = 0;          // pipelined calls since the last synchronous read
     // pipelined steps copy their host rays into a staging buffer on a copy stream, beside the
     // previous step; the step stream takes them from there with one device copy
@@ -132,18 +165,28 @@ struct tn_trainer {
     // a dataset of posed images as the ray source (tn_trainer_set_dataset)
     tn_camera* ds_cameras = nullptr;
     uint8_t* ds_images = nullptr;
-    float* ds_random = nullptr;  // [2][R]: pixel and alpha-selection draws of the step
     uint32_t ds_n = 0;
     int32_t ds_w = 0, ds_h = 0;
     float alpha_threshold = 1.0f, alpha_probability = 1.0f;
     cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_consumed[2] = {nullptr, nullptr};
-    cudaGraph_t graph[2] = {nullptr, nullptr};           // [synthetic rays, caller rays]
-    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
-    uint32_t graph_kernels[2] = {0, 0};
-    uint32_t graph_nodes[2] = {0, 0};
+    // [kind][ray source: own, caller][ray set of the tail, or of the head for K_H]
+    cudaGraph_t graph[K_KINDS][2][2] = {};
+    cudaGraphExec_t graph_exec[K_KINDS][2][2] = {};
+    bool warm[K_KINDS][2][2] = {};        // ran once eagerly (lazy resources initialised)
+    uint32_t graph_kernels[K_KINDS][2] = {};  // kernels captured in one graph of each kind and ray source
+    uint32_t graph_nodes[K_KINDS][2] = {};
     uint32_t fused_steps_enqueued = 0;
     uint32_t host_step = 0;
     tn_training_metrics last{};
+
+    void select(int p) {
+        cur = p;
+        RaySet& q = set[p];
+        ori = q.ori; dir = q.dir; target = q.target; bg = q.bg;
+        ray_t = q.ray_t; ray_tmax = q.ray_tmax; alive = q.alive; n_steps = q.n_steps; offsets = q.offsets;
+        ctx = q.ctx;
+    }
+    bool lookahead() const { return d.path == TN_PATH_FUSED && ctx->tune.side_sms > 0; }
 
     template <typename T>
     int alloc(T*& p, size_t n) {
@@ -168,20 +211,22 @@ namespace {
 // Stage boundaries of one fused step (for per-stage timing with events).
 enum Stage : int { ST_RAYS = 0, ST_COUNT, ST_EMIT, ST_FORWARD, ST_LOSSES, ST_BACKWARD, ST_ADAM, ST_OCC_QUERY, ST_OCCUPANCY, ST_N };
 
-// The step's rays when the caller supplies none: from the dataset when one is set, else the
-// built-in synthetic rays.
-static int enqueue_own_rays(tn_trainer* tr, cudaStream_t s) {
+// The rays of the step keyed by the state's step_count (the index the next step_begin gives
+// the step) when the caller supplies none: from the dataset when one is set, else the built-in
+// synthetic rays. Written into set q.
+static int enqueue_own_rays(tn_trainer* tr, cudaStream_t s, RaySet& q) {
     const tn_trainer_desc& d = tr->d;
+    const uint32_t* key = &tr->state->step_count;
     if (tr->ds_n) {
-        int st = launch_dataset_draws(s, tr->R, tr->R, d.seed, &tr->state->cur_step, tr->ds_random, tr->bg);
+        int st = launch_dataset_draws(s, tr->R, tr->R, d.seed, key, q.ds_random, q.bg);
         if (st == TN_OK)
             st = launch_dataset_rays(s, tr->R, tr->R, tr->ds_n, tr->ds_w, tr->ds_h, tr->ds_cameras, tr->ds_images,
-                                     d.bbox, tr->ds_random, tr->alpha_threshold, tr->alpha_probability, tr->target,
-                                     nullptr, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax, tr->alive);
+                                     d.bbox, q.ds_random, tr->alpha_threshold, tr->alpha_probability, q.target,
+                                     nullptr, q.ori, q.dir, q.ray_t, q.ray_tmax, q.alive);
         return st;
     }
-    return launch_synth_rays(s, tr->R, tr->R, d.seed, &tr->state->cur_step, d.ray_radius, d.ray_jitter, d.bbox,
-                             3.0e38f, tr->ori, tr->dir, tr->target, tr->bg, tr->ray_t, tr->ray_tmax, tr->alive);
+    return launch_synth_rays(s, tr->R, tr->R, d.seed, key, d.ray_radius, d.ray_jitter, d.bbox, 3.0e38f, q.ori, q.dir,
+                             q.target, q.bg, q.ray_t, q.ray_tmax, q.alive);
 }
 
 // Occupancy query of one step: random cells, their sample points, the density network.
@@ -197,122 +242,250 @@ static int enqueue_occupancy_query(tn_trainer* tr, cudaStream_t s, const tn_grid
 }
 
 // Occupancy update of one step: decay + max-update of the queried cells, bitfield rebuild.
-static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid) {
+static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, tn_ctx* ctx) {
     const tn_trainer_desc& d = tr->d;
-    return launch_occupancy_update(tr->ctx, s, &grid, tr->density, tr->bits, tr->M, tr->occ_levels, tr->occ_cells,
+    return launch_occupancy_update(ctx, s, &grid, tr->density, tr->bits, tr->M, tr->occ_levels, tr->occ_cells,
                                    tr->occ_values, tr->occ_rsel, tr->net.activation, 0, &tr->state->sample_all,
                                    nullptr, d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied);
 }
 
-// The Adam update of the step whose gradients sit in tr->g. With a placement of the side SMs it
-// runs only while a pending update is flagged (the previous step's, at the start of the next).
-static int enqueue_adam(tn_trainer* tr, cudaStream_t s, const float* lr_dev, const AdamPlacement& place) {
+// Head of a step: its rays (own, or the caller's already in set q, clipped to the box) and the
+// march count with the batch cut into set q's buffers and context.
+static int enqueue_head(tn_trainer* tr, cudaStream_t s, bool external, RaySet& q) {
     const tn_trainer_desc& d = tr->d;
-    return launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate, lr_dev,
-                       d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v, tr->steps, place);
-}
-
-// Applies a pending Adam update (pipelined steps leave the last step's update pending).
-static int flush_adam(tn_trainer* tr) {
-    if (tr->d.path != TN_PATH_FUSED) return TN_OK;
-    AdamPlacement place;
-    place.enable = &tr->state->adam_pending;
-    int st = enqueue_adam(tr, tr->stream, &tr->state->adam_lr, place);
+    const tn_grid_desc grid = tr->grid();
+    const tn_march_desc march = tr->march();
+    int st = external ? tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, q.ori, q.dir, q.ray_t, q.ray_tmax, q.alive)
+                      : enqueue_own_rays(tr, s, q);
     if (st == TN_OK)
-        st = cuda_status(cudaMemsetAsync(&tr->state->adam_pending, 0, sizeof(uint32_t), tr->stream), "flush");
+        st = tn_march_count(q.ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, q.ori, q.dir,
+                            q.ray_t, q.ray_tmax, q.alive, q.n_steps, tr->B, q.info);
     return st;
 }
 
-// One fused step. Without stage events, work runs on a second stream beside the training chain:
-//  * pipelined (side_sms > 0): first the previous step's pending Adam update on side_sms SMs,
-//    beside this step's rays and march (the network forward waits for it);
-//  * the occupancy query (cell sampling and the density network; after that Adam update, since
-//    the network reads the parameters), beside the march;
-//  * the occupancy update, which rewrites the bitfield and so waits for the emit pass (the last
-//    reader of this step), beside the loss and backward stages.
-// The main stream joins the second one before step_end. With stage events (profiling)
-// everything runs in order on one stream, Adam included.
-int enqueue_fused_step(tn_trainer* tr, bool external_rays, cudaEvent_t* ev) {
+// Tail of the step whose head is in set p: step_begin, emit, network forward, the fused losses,
+// network backward, Adam and, on the second stream, the step's occupancy query and update. With
+// next != nullptr the head of the following step (rays from next_external / own rays) runs on
+// the third stream into set *next once the occupancy update has rewritten the bitfield, and Adam
+// keeps to side_sms SMs beside it. ring >= 0 copies the finished step's state into that pinned
+// slot (and clears the state's error bits) before the head is joined.
+static int enqueue_tail(tn_trainer* tr, RaySet& p, RaySet* next, bool next_external, int ring) {
     const tn_trainer_desc& d = tr->d;
-    cudaStream_t s = tr->stream;
-    const bool pipe = ev == nullptr && tr->ctx->tune.side_sms > 0;
-    const bool side = ev == nullptr && (tr->M > 0 || pipe);
-    cudaStream_t so = side ? tr->aux : s;
+    cudaStream_t s = tr->stream, so = tr->aux, cs = tr->cstream;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
-    auto mark = [&](int k) { if (ev) cudaEventRecord(ev[k + 1], s); };
-    if (ev) cudaEventRecord(ev[0], s);
+    const bool occ = tr->M > 0;
     step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
     int st = check_launch("step_begin");
-    if (st == TN_OK && side) {
+    if (st == TN_OK && (occ || next)) {
         st = cuda_status(cudaEventRecord(tr->ev_fork, s), "fork");
-        if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
-        if (st == TN_OK && pipe) {
-            AdamPlacement place;
-            place.max_blocks = tr->ctx->tune.side_sms;
-            place.reserve_smem = exclusive_smem();
-            place.enable = &tr->state->adam_pending;
-            st = enqueue_adam(tr, so, &tr->state->adam_lr, place);
-            if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_adam, so), "adam done");
-        }
-        if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_query(tr, so, grid);
+        if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
+        if (st == TN_OK && occ) st = enqueue_occupancy_query(tr, so, grid);
     }
-    if (st == TN_OK) {
-        if (external_rays)
-            st = tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax,
-                                   tr->alive);
-        else
-            st = enqueue_own_rays(tr, s);
-    }
-    mark(ST_RAYS);
-    uint32_t* info = tr->state->batch_info;
+    uint32_t* info = p.info;
     if (st == TN_OK)
-        st = tn_march_count(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, tr->ori, tr->dir,
-                            tr->ray_t, tr->ray_tmax, tr->alive, tr->n_steps, tr->B, info);
-    mark(ST_COUNT);
-    if (st == TN_OK)
-        st = tn_march_emit(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B, info,
-                           nullptr, tr->ori, tr->dir, tr->ray_t, tr->alive, tr->n_steps, tr->offsets, nullptr, tr->s_t,
-                           tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
-    mark(ST_EMIT);
-    if (st == TN_OK && side && tr->M > 0) {
+        st = tn_march_emit(p.ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B, info,
+                           nullptr, p.ori, p.dir, p.ray_t, p.alive, p.n_steps, p.offsets, nullptr, tr->s_t, tr->s_pos,
+                           tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
+    // the occupancy update rewrites the bitfield, which the emit pass may still read
+    if (st == TN_OK && occ) {
         st = cuda_status(cudaEventRecord(tr->ev_emit, s), "emit done");
         if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_emit, 0), "emit done");
-        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid);
+        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid, p.ctx);
+        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_occ, so), "occupancy done");
     }
-    if (st == TN_OK && side) st = cuda_status(cudaEventRecord(tr->ev_join, so), "join");
-    if (st == TN_OK && pipe) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_adam, 0), "adam done");
+    // the next step's head reads the updated grid
+    if (st == TN_OK && next) {
+        st = cuda_status(cudaStreamWaitEvent(cs, occ ? tr->ev_occ : tr->ev_fork, 0), "head start");
+        if (st == TN_OK) st = enqueue_head(tr, cs, next_external, *next);
+        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_head, cs), "head done");
+    }
     if (st == TN_OK)
         st = tr->net.forward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
                              tr->net_rgb);
-    mark(ST_FORWARD);
     if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->grad_density, 0, (size_t)tr->B * 4, s), "grad memset");
-    tn_ray_batch rb{tr->R, tr->R, tr->B, 0, tr->n_steps, tr->offsets, info};
+    tn_ray_batch rb{tr->R, tr->R, tr->B, 0, p.n_steps, p.offsets, info};
     if (st == TN_OK)
-        st = tn_train_losses(tr->ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, info, d.loss_scale,
+        st = tn_train_losses(p.ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, info, d.loss_scale,
                              d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb,
-                             tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, tr->target, tr->bg, nullptr,
-                             tr->grad_density, tr->dl_drgb, tr->state->loss_sums);
-    mark(ST_LOSSES);
+                             tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, p.target, p.bg, nullptr, tr->grad_density,
+                             tr->dl_drgb, tr->state->loss_sums);
     if (st == TN_OK && tr->net.backward)
         st = tr->net.backward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->grad_density,
                               tr->dl_drgb, tr->g);
-    mark(ST_BACKWARD);
-    // Adam, then the occupancy update: the reference trains first and refreshes the grid after
-    // the step (update_occupancy_grid follows train_step, src/main.cu:157-166); the freshly
-    // written bitfield is then still in L2 for the next step's march. Pipelined, the update is
-    // left pending for the next step.
-    if (st == TN_OK && !pipe) st = enqueue_adam(tr, s, &tr->state->lr, AdamPlacement{});
-    mark(ST_ADAM);
-    if (st == TN_OK && !side && tr->M > 0) st = enqueue_occupancy_query(tr, s, grid);
-    mark(ST_OCC_QUERY);
-    if (st == TN_OK && !side && tr->M > 0) st = enqueue_occupancy_update(tr, s, grid);
-    mark(ST_OCCUPANCY);
-    if (st == TN_OK && side) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_join, 0), "join");
     if (st == TN_OK) {
-        step_end_kernel<<<1, 1, 0, s>>>(tr->state, pipe ? 1u : 0u);
+        AdamPlacement place;
+        if (next && p.ctx->tune.side_sms) {
+            place.max_blocks = p.ctx->tune.side_sms;
+            place.reserve_smem = exclusive_smem();
+        }
+        st = launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate,
+                         &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
+                         tr->steps, place);
+    }
+    if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_occ, 0), "occupancy joined");
+    if (st == TN_OK) {
+        step_end_kernel<<<1, 1, 0, s>>>(tr->state, info, p.ctx->flags);
         st = check_launch("step_end");
     }
+    // The finished step's state to the pinned ring slot, then its step count to the slot's pinned
+    // flag word: the copies run in stream order, so once the host sees the flag the state has
+    // landed. The host polls the flag (tn_trainer_train_step_rays_pipelined) while the next
+    // step's head may still be marching.
+    if (st == TN_OK && ring >= 0) {
+        st = cuda_status(cudaMemcpyAsync(&tr->ring_state[ring], tr->state, sizeof(StepState), cudaMemcpyDeviceToHost,
+                                         s), "state to ring");
+        if (st == TN_OK)
+            st = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(&tr->ring_flag[ring]), &tr->state->step_count, sizeof(uint32_t),
+                                             cudaMemcpyDeviceToHost, s), "ring flag");
+        if (st == TN_OK) st = cuda_status(cudaMemsetAsync(&tr->state->err, 0, sizeof(uint32_t), s), "err clear");
+    }
+    if (st == TN_OK && next) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_head, 0), "head joined");
+    return st;
+}
+
+// One fused step in order on the trainer's stream with events between its stages (stage
+// timing): head and tail of the step in set p, nothing beside it.
+static int enqueue_profiled_step(tn_trainer* tr, RaySet& p, cudaEvent_t* ev) {
+    const tn_trainer_desc& d = tr->d;
+    cudaStream_t s = tr->stream;
+    const tn_grid_desc grid = tr->grid();
+    const tn_march_desc march = tr->march();
+    cudaEventRecord(ev[0], s);
+    int st = enqueue_own_rays(tr, s, p);
+    cudaEventRecord(ev[ST_RAYS + 1], s);
+    if (st == TN_OK)
+        st = tn_march_count(p.ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, p.ori, p.dir,
+                            p.ray_t, p.ray_tmax, p.alive, p.n_steps, tr->B, p.info);
+    cudaEventRecord(ev[ST_COUNT + 1], s);
+    if (st == TN_OK) {
+        step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
+        st = check_launch("step_begin");
+    }
+    if (st == TN_OK)
+        st = tn_march_emit(p.ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B, p.info,
+                           nullptr, p.ori, p.dir, p.ray_t, p.alive, p.n_steps, p.offsets, nullptr, tr->s_t, tr->s_pos,
+                           tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
+    cudaEventRecord(ev[ST_EMIT + 1], s);
+    if (st == TN_OK)
+        st = tr->net.forward(tr->net.user, s, tr->B, p.info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
+                             tr->net_rgb);
+    cudaEventRecord(ev[ST_FORWARD + 1], s);
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->grad_density, 0, (size_t)tr->B * 4, s), "grad memset");
+    tn_ray_batch rb{tr->R, tr->R, tr->B, 0, p.n_steps, p.offsets, p.info};
+    if (st == TN_OK)
+        st = tn_train_losses(p.ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, p.info, d.loss_scale,
+                             d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb,
+                             tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, p.target, p.bg, nullptr, tr->grad_density,
+                             tr->dl_drgb, tr->state->loss_sums);
+    cudaEventRecord(ev[ST_LOSSES + 1], s);
+    if (st == TN_OK && tr->net.backward)
+        st = tr->net.backward(tr->net.user, s, tr->B, p.info + 1, tr->B, tr->s_pos, tr->s_dir, tr->grad_density,
+                              tr->dl_drgb, tr->g);
+    cudaEventRecord(ev[ST_BACKWARD + 1], s);
+    if (st == TN_OK)
+        st = launch_adam(s, false, tr->P, d.n_grid_params, d.n_mlp_params, d.loss_scale, d.learning_rate,
+                         &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
+                         tr->steps, AdamPlacement{});
+    cudaEventRecord(ev[ST_ADAM + 1], s);
+    if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_query(tr, s, grid);
+    cudaEventRecord(ev[ST_OCC_QUERY + 1], s);
+    if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_update(tr, s, grid, p.ctx);
+    cudaEventRecord(ev[ST_OCCUPANCY + 1], s);
+    if (st == TN_OK) {
+        step_end_kernel<<<1, 1, 0, s>>>(tr->state, p.info, p.ctx->flags);
+        st = check_launch("step_end");
+    }
+    return st;
+}
+
+// Enqueues one kind of step (ray source: own or caller rays) with set p as the set of its
+// tail (K_HT, K_TH, K_T) or of its head (K_H). The first run of each variant is eager (it also
+// initialises every lazily created resource); later runs replay a graph captured once.
+static int enqueue_kind(tn_trainer* tr, int kind, bool external, int p, int ring) {
+    const int src = external ? 1 : 0;
+    auto body = [&]() -> int {
+        RaySet& a = tr->set[p];
+        RaySet& b = tr->set[p ^ 1];
+        switch (kind) {
+            case K_HT: {
+                int st = enqueue_head(tr, tr->stream, external, a);
+                return st == TN_OK ? enqueue_tail(tr, a, nullptr, false, ring) : st;
+            }
+            case K_TH: return enqueue_tail(tr, a, &b, external, ring);
+            case K_H: return enqueue_head(tr, tr->stream, external, a);
+            default: return enqueue_tail(tr, a, nullptr, false, ring);
+        }
+    };
+    // a ring copy is baked into a graph: the pipelined caller-ray steps copy into slot p
+    if (!tr->d.use_cuda_graph || !tr->warm[kind][src][p] || (ring >= 0 && ring != p)) {
+        tr->warm[kind][src][p] = true;
+        return body();
+    }
+    cudaGraphExec_t& ex = tr->graph_exec[kind][src][p];
+    if (!ex) {
+        int st = cuda_status(cudaStreamBeginCapture(tr->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        if (st != TN_OK) return st;
+        const int est = body();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(tr->stream, &g);
+        if (est != TN_OK) {
+            if (g) cudaGraphDestroy(g);
+            return est;
+        }
+        st = cuda_status(e, "end capture");
+        if (st == TN_OK) st = cuda_status(cudaGraphInstantiate(&ex, g, 0), "instantiate");
+        if (st != TN_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        tr->graph[kind][src][p] = g;
+        size_t n_nodes = 0;
+        cudaGraphGetNodes(g, nullptr, &n_nodes);
+        std::vector<cudaGraphNode_t> nodes(n_nodes);
+        cudaGraphGetNodes(g, nodes.data(), &n_nodes);
+        uint32_t kernels = 0;
+        for (auto nd : nodes) {
+            cudaGraphNodeType t;
+            cudaGraphNodeGetType(nd, &t);
+            kernels += t == cudaGraphNodeTypeKernel;
+        }
+        tr->graph_kernels[kind][src] = kernels;
+        tr->graph_nodes[kind][src] = (uint32_t)n_nodes;
+    }
+    return cuda_status(cudaGraphLaunch(ex, tr->stream), "graph launch");
+}
+
+// Drops a head computed ahead from own rays (what it read is about to change, or the next
+// step takes caller rays): its work is done by the time the stream is idle, and the error bits
+// it raised belong to no step.
+static int drop_spec(tn_trainer* tr) {
+    if (!tr->spec_own) return TN_OK;
+    tr->spec_own = false;
+    int st = cuda_status(cudaStreamSynchronize(tr->stream), "drop head");
+    if (st == TN_OK)
+        st = cuda_status(cudaMemsetAsync(tr->set[tr->cur ^ 1].ctx->flags, 0, sizeof(uint32_t), tr->stream),
+                         "drop head flags");
+    return st;
+}
+
+// Runs the tail of a requested caller-ray step whose head is in set cur ^ 1.
+static int finish_pending(tn_trainer* tr) {
+    if (!tr->pending_ext) return TN_OK;
+    tr->pending_ext = false;
+    const int q = tr->cur ^ 1;
+    int st = enqueue_kind(tr, K_T, true, q, -1);
+    if (st != TN_OK) return st;
+    tr->select(q);
+    ++tr->fused_steps_enqueued;
+    return TN_OK;
+}
+
+// Brings the trainer to a step boundary with nothing in flight ahead of it: a requested step is
+// completed; a head computed ahead is kept (keep_spec) or dropped.
+static int settle(tn_trainer* tr, bool keep_spec = false) {
+    int st = finish_pending(tr);
+    if (st == TN_OK && !keep_spec) st = drop_spec(tr);
     return st;
 }
 
@@ -323,14 +496,14 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
     const tn_march_desc march = tr->march();
     const uint32_t k = tr->host_step;
     const float lr = d.learning_rate / (1.0f + d.learning_rate_decay * (float)k);
-    step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
-    int st = check_launch("step_begin");
+    // the step's rays (own rays keyed by the step's index, the state's step_count before
+    // step_begin), then step_begin
+    int st = external_rays ? tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t,
+                                               tr->ray_tmax, tr->alive)
+                           : enqueue_own_rays(tr, s, tr->set[tr->cur]);
     if (st == TN_OK) {
-        if (external_rays)
-            st = tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, tr->ori, tr->dir, tr->ray_t, tr->ray_tmax,
-                                   tr->alive);
-        else
-            st = enqueue_own_rays(tr, s);
+        step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
+        st = check_launch("step_begin");
     }
     if (st == TN_OK)
         st = tn_plain_march_count(s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, tr->ori, tr->dir, tr->ray_t,
@@ -376,12 +549,12 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
                                                 d.occupancy_decay, d.occupancy_threshold, tr->count_scratch, &nocc);
     }
     if (st == TN_OK) {
-        uint32_t info[2] = {nr, ns};
-        st = cuda_status(cudaMemcpyAsync(tr->state->batch_info, info, sizeof(info), cudaMemcpyHostToDevice, s),
+        uint32_t info[4] = {nr, ns, 0, 0};
+        st = cuda_status(cudaMemcpyAsync(tr->set[tr->cur].info, info, sizeof(info), cudaMemcpyHostToDevice, s),
                          "batch info");
         if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "plain info sync");
         if (st == TN_OK) {
-            step_end_kernel<<<1, 1, 0, s>>>(tr->state, 0u);
+            step_end_kernel<<<1, 1, 0, s>>>(tr->state, tr->set[tr->cur].info, tr->ctx->flags);
             st = check_launch("step_end");
         }
     }
@@ -398,8 +571,9 @@ int run_plain_step(tn_trainer* tr, bool external_rays, tn_training_metrics* out)
     return st;
 }
 
-// Metrics of a step from its state and its error word, as read back to the host.
-int metrics_from(tn_trainer* tr, const StepState& h, uint32_t flags, tn_training_metrics* out) {
+// Metrics of a step from its state (with its error bits), as read back to the host.
+int metrics_from(tn_trainer* tr, const StepState& h, tn_training_metrics* out) {
+    const uint32_t flags = h.err;
     if (flags & TN_FLAG_NO_RAYS) return fail(TN_E_NO_RAYS, "No rays were generated for this training batch");
     if (flags & TN_FLAG_NO_SAMPLES) return fail(TN_E_NO_SAMPLES, "No samples were generated for this training batch");
     if (flags) return fail(TN_E_DEVICE, "device error flags 0x%x", flags);
@@ -411,16 +585,16 @@ int metrics_from(tn_trainer* tr, const StepState& h, uint32_t flags, tn_training
     return TN_OK;
 }
 
+// Waits for the trainer's stream and reads the state of the last completed step; its error bits
+// (every step's since the last read) are cleared.
 int read_state(tn_trainer* tr, tn_training_metrics* out) {
     int st = cuda_status(cudaMemcpyAsync(tr->state_host, tr->state, sizeof(StepState), cudaMemcpyDeviceToHost, tr->stream),
                          "state read");
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(&tr->state->err, 0, sizeof(uint32_t), tr->stream), "err clear");
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "state sync");
     if (st != TN_OK) return st;
-    uint32_t flags = 0;
-    st = tn_ctx_check(tr->ctx, tr->stream, &flags);
-    if (st != TN_OK) return st;
-    tr->ring_calls = 0;  // every earlier step is complete; its error word is in `flags`
-    return metrics_from(tr, *tr->state_host, flags, out);
+    tr->ring_calls = 0;  // every earlier step is complete; its error bits were in the state
+    return metrics_from(tr, *tr->state_host, out);
 }
 
 }  // namespace
@@ -487,11 +661,12 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     }
     st = cuda_status(cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking), "stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->aux, cudaStreamNonBlocking), "aux stream");
+    if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->cstream, cudaStreamNonBlocking), "head stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->h2d, cudaStreamNonBlocking), "copy stream");
-    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_join, &tr->ev_adam, &tr->ev_ring[0], &tr->ev_ring[1],
+    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_occ, &tr->ev_head,
                            &tr->ev_staged[0], &tr->ev_staged[1], &tr->ev_consumed[0], &tr->ev_consumed[1]})
         if (st == TN_OK) st = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "step events");
-    if (st == TN_OK) st = tn_ctx_create(&tr->ctx);
+    for (int k = 0; k < 2 && st == TN_OK; ++k) st = tn_ctx_create(&tr->set[k].ctx);
     const uint32_t R = desc->n_rays_per_step, B = desc->batch_size;
     const uint32_t res = (uint32_t)desc->grid.resolution;
     const uint32_t V = res * res * res, L = (uint32_t)desc->grid.n_levels;
@@ -499,28 +674,34 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     tr->R = R; tr->B = B; tr->V = V; tr->P = P; tr->M = desc->occupancy_cells_per_step;
     tr->chunk = std::min(B, V);
     const uint32_t occ_n = std::max(tr->M, tr->chunk);
-    if (st == TN_OK) st = tn_ctx_reserve(tr->ctx, R, B);
-    // Pipelined Adam by default: the march count in 256-ray blocks, one per SM, and the other
-    // SMs for the previous step's Adam update, when that leaves at least 16 of them.
+    for (int k = 0; k < 2 && st == TN_OK; ++k) st = tn_ctx_reserve(tr->set[k].ctx, R, B);
+    // Count-ahead by default: the march count in 256-ray blocks, one per SM, and the other SMs
+    // for Adam beside it, when that leaves at least 16 of them.
     if (st == TN_OK && desc->path == TN_PATH_FUSED) {
         const int side = num_sms() - (int)((R + 255) / 256);
         if (side >= 16) {
-            tr->ctx->tune.count_rays_per_block = 256;
-            tr->ctx->tune.side_sms = (uint32_t)side;
+            for (int k = 0; k < 2; ++k) {
+                tr->set[k].ctx->tune.count_rays_per_block = 256;
+                tr->set[k].ctx->tune.side_sms = (uint32_t)side;
+            }
         }
     }
 #define ALLOC(p, n) if (st == TN_OK) st = tr->alloc(p, (size_t)(n))
-    // the step's input rays in one allocation, [ori 3R | dir 3R | target 4R | bg 3R], so that a
+    // each set's input rays in one allocation, [ori 3R | dir 3R | target 4R | bg 3R], so that a
     // pipelined step takes them from its staging buffer in one copy
-    ALLOC(tr->ori, 13 * (size_t)R);
-    if (st == TN_OK) {
-        tr->dir = tr->ori + 3 * (size_t)R;
-        tr->target = tr->ori + 6 * (size_t)R;
-        tr->bg = tr->ori + 10 * (size_t)R;
+    for (int k = 0; k < 2; ++k) {
+        RaySet& q = tr->set[k];
+        ALLOC(q.ori, 13 * (size_t)R);
+        if (st == TN_OK) {
+            q.dir = q.ori + 3 * (size_t)R;
+            q.target = q.ori + 6 * (size_t)R;
+            q.bg = q.ori + 10 * (size_t)R;
+        }
+        ALLOC(q.ray_t, R); ALLOC(q.ray_tmax, R);
+        ALLOC(q.alive, R); ALLOC(q.n_steps, R); ALLOC(q.offsets, R); ALLOC(q.info, 4);
     }
+    if (st == TN_OK) tr->select(0);
     ALLOC(tr->stage[0], 13 * (size_t)R); ALLOC(tr->stage[1], 13 * (size_t)R);
-    ALLOC(tr->ray_t, R); ALLOC(tr->ray_tmax, R);
-    ALLOC(tr->alive, R); ALLOC(tr->n_steps, R); ALLOC(tr->offsets, R);
     ALLOC(tr->s_t, B); ALLOC(tr->s_pos, 3 * B); ALLOC(tr->s_dir, 3 * B); ALLOC(tr->s_dt, B); ALLOC(tr->s_mnorm, B);
     ALLOC(tr->s_dtnorm, B); ALLOC(tr->net_density, B); ALLOC(tr->net_rgb, 3 * B); ALLOC(tr->grad_density, B);
     ALLOC(tr->dl_drgb, 3 * B);
@@ -537,7 +718,11 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
 #undef ALLOC
     if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->state_host, sizeof(StepState)), "pinned state");
     if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->ring_state, 2 * sizeof(StepState)), "pinned state ring");
-    if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->ring_flags, 2 * sizeof(uint32_t)), "pinned flag ring");
+    if (st == TN_OK) {
+        uint32_t* f = nullptr;
+        st = cuda_status(cudaMallocHost(&f, 2 * sizeof(uint32_t)), "pinned ring flags");
+        tr->ring_flag = f;
+    }
     // reference initial grid: every bit set, densities zero (occupancy-grid.cuh:81-85)
     if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->bits, 0xFF, V, tr->stream), "bitfield init");
     if (st == TN_OK) st = launch_synth_params(tr->stream, P, desc->n_grid_params, desc->seed, tr->w);
@@ -550,26 +735,27 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     return TN_OK;
 }
 
+static void drop_graphs(tn_trainer* tr);
+
 int tn_trainer_destroy(tn_trainer* tr) {
     if (!tr) return TN_OK;
     if (tr->stream) cudaStreamSynchronize(tr->stream);
-    for (int i = 0; i < 2; ++i) {
-        if (tr->graph_exec[i]) cudaGraphExecDestroy(tr->graph_exec[i]);
-        if (tr->graph[i]) cudaGraphDestroy(tr->graph[i]);
-    }
+    drop_graphs(tr);
     for (void* p : tr->allocs) cudaFree(p);
     if (tr->synth.blobs) cudaFree(tr->synth.blobs);
     if (tr->synth.waves) cudaFree(tr->synth.waves);
     if (tr->state_host) cudaFreeHost(tr->state_host);
     if (tr->ring_state) cudaFreeHost(tr->ring_state);
-    if (tr->ring_flags) cudaFreeHost(tr->ring_flags);
-    if (tr->ctx) tn_ctx_destroy(tr->ctx);
+    if (tr->ring_flag) cudaFreeHost(const_cast<uint32_t*>(tr->ring_flag));
+    for (int k = 0; k < 2; ++k)
+        if (tr->set[k].ctx) tn_ctx_destroy(tr->set[k].ctx);
     if (tr->h2d) cudaStreamSynchronize(tr->h2d);
-    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_join, tr->ev_adam, tr->ev_ring[0], tr->ev_ring[1],
+    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_occ, tr->ev_head,
                           tr->ev_staged[0], tr->ev_staged[1], tr->ev_consumed[0], tr->ev_consumed[1]})
         if (e) cudaEventDestroy(e);
     if (tr->h2d) cudaStreamDestroy(tr->h2d);
     if (tr->aux) cudaStreamDestroy(tr->aux);
+    if (tr->cstream) cudaStreamDestroy(tr->cstream);
     if (tr->stream) cudaStreamDestroy(tr->stream);
     delete tr;
     return TN_OK;
@@ -578,8 +764,11 @@ int tn_trainer_destroy(tn_trainer* tr) {
 int tn_trainer_set_synthetic_field(tn_trainer* tr, uint32_t n_blobs, const float* blobs, const float* waves) {
     TN_NONNULL(tr); TN_NONNULL(blobs); TN_NONNULL(waves);
     TN_REQUIRE(n_blobs >= 1 && n_blobs <= 256, TN_E_INVALID, "n_blobs %u outside 1..256", n_blobs);
-    TN_REQUIRE(tr->graph_exec[0] == nullptr && tr->graph_exec[1] == nullptr, TN_E_STATE,
-               "the field must be set before the first captured step");
+    bool captured = false;
+    for (auto& k : tr->graph_exec)
+        for (auto& r : k)
+            for (auto& e : r) captured = captured || e != nullptr;
+    TN_REQUIRE(!captured, TN_E_STATE, "the field must be set before the first captured step");
     if (tr->synth.blobs) cudaFree(tr->synth.blobs);
     if (tr->synth.waves) cudaFree(tr->synth.waves);
     tr->synth.blobs = tr->synth.waves = nullptr;
@@ -594,7 +783,7 @@ int tn_trainer_set_synthetic_field(tn_trainer* tr, uint32_t n_blobs, const float
 int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bitfield) {
     TN_NONNULL(tr);
     const size_t L = (size_t)tr->d.grid.n_levels;
-    int st = TN_OK;
+    int st = settle(tr);  // a head computed ahead read the old grid
     if (density) st = cuda_status(cudaMemcpyAsync(tr->density, density, L * tr->V * sizeof(float), cudaMemcpyHostToDevice, tr->stream), "density copy");
     if (st == TN_OK && bitfield) st = cuda_status(cudaMemcpyAsync(tr->bits, bitfield, tr->V, cudaMemcpyHostToDevice, tr->stream), "bits copy");
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "set_grid sync");
@@ -603,7 +792,7 @@ int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bit
 
 int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_touched_out) {
     TN_NONNULL(tr);
-    const int fst = flush_adam(tr);  // a pending update reads the gradients rewritten here
+    const int fst = settle(tr);
     if (fst != TN_OK) return fst;
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream;
@@ -612,8 +801,8 @@ int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_t
     // one batch of samples from the current grid (rays of step 0)
     int st = cuda_status(cudaMemsetAsync(tr->state, 0, sizeof(StepState), s), "state clear");
     if (st == TN_OK)
-        st = enqueue_own_rays(tr, s);
-    uint32_t* info = tr->state->batch_info;
+        st = enqueue_own_rays(tr, s, tr->set[tr->cur]);
+    uint32_t* info = tr->set[tr->cur].info;
     if (st == TN_OK)
         st = tn_march_count(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, tr->ori, tr->dir,
                             tr->ray_t, tr->ray_tmax, tr->alive, tr->n_steps, tr->B, info);
@@ -656,48 +845,32 @@ int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_t
     return st;
 }
 
-static int train_step_impl(tn_trainer* tr, bool external, tn_training_metrics* metrics) {
-    if (tr->d.path == TN_PATH_PLAIN) return run_plain_step(tr, external, metrics);
-    int st = TN_OK;
-    const int gi = external ? 1 : 0;
-    // The first step runs eagerly (it also warms up every lazily initialised resource);
-    // later steps replay a graph captured once per ray source.
-    if (tr->d.use_cuda_graph && tr->fused_steps_enqueued >= 1) {
-        if (!tr->graph_exec[gi]) {
-            st = cuda_status(cudaStreamBeginCapture(tr->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            if (st == TN_OK) {
-                const int est = enqueue_fused_step(tr, external, nullptr);
-                cudaGraph_t g = nullptr;
-                const cudaError_t e = cudaStreamEndCapture(tr->stream, &g);
-                if (est != TN_OK) { if (g) cudaGraphDestroy(g); return est; }
-                st = cuda_status(e, "end capture");
-                if (st == TN_OK) tr->graph[gi] = g;
-            }
-            if (st == TN_OK) st = cuda_status(cudaGraphInstantiate(&tr->graph_exec[gi], tr->graph[gi], 0), "instantiate");
-            if (st == TN_OK) {
-                size_t n_nodes = 0;
-                cudaGraphGetNodes(tr->graph[gi], nullptr, &n_nodes);
-                std::vector<cudaGraphNode_t> nodes(n_nodes);
-                cudaGraphGetNodes(tr->graph[gi], nodes.data(), &n_nodes);
-                uint32_t kernels = 0;
-                for (auto nd : nodes) {
-                    cudaGraphNodeType t;
-                    cudaGraphNodeGetType(nd, &t);
-                    kernels += t == cudaGraphNodeTypeKernel;
-                }
-                tr->graph_kernels[gi] = kernels;
-                tr->graph_nodes[gi] = (uint32_t)n_nodes;
-            }
-            if (st != TN_OK) return st;
-        }
-        st = cuda_status(cudaGraphLaunch(tr->graph_exec[gi], tr->stream), "graph launch");
+// One fused step. Own rays with the count-ahead schedule: the head of this step was computed
+// ahead by the previous step (or runs first here), and this step's tail runs beside the next
+// step's head. Otherwise (caller rays, already copied into set cur ^ 1, or side_sms = 0) the
+// head and the tail of the step run in order.
+static int fused_step(tn_trainer* tr, bool external, tn_training_metrics* metrics) {
+    int st = finish_pending(tr);
+    if (st != TN_OK) return st;
+    const int q = tr->cur ^ 1;
+    if (!external && tr->lookahead()) {
+        if (!tr->spec_own) st = enqueue_kind(tr, K_H, false, q, -1);
+        if (st == TN_OK) st = enqueue_kind(tr, K_TH, false, q, -1);
+        tr->spec_own = st == TN_OK;
     } else {
-        st = enqueue_fused_step(tr, external, nullptr);
+        st = drop_spec(tr);
+        if (st == TN_OK) st = enqueue_kind(tr, K_HT, external, q, -1);
     }
     if (st != TN_OK) return st;
+    tr->select(q);
     ++tr->fused_steps_enqueued;
     if (metrics) return read_state(tr, metrics);
     return TN_OK;
+}
+
+static int train_step_impl(tn_trainer* tr, bool external, tn_training_metrics* metrics) {
+    if (tr->d.path == TN_PATH_PLAIN) return run_plain_step(tr, external, metrics);
+    return fused_step(tr, external, metrics);
 }
 
 int tn_trainer_train_step(tn_trainer* tr, tn_training_metrics* metrics) {
@@ -709,12 +882,16 @@ int tn_trainer_train_step_rays(tn_trainer* tr, uint32_t n_rays, const float* ori
                                const float* target_rgba, const float* bg_rgb, tn_training_metrics* metrics) {
     TN_NONNULL(tr); TN_NONNULL(ori); TN_NONNULL(dir); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
     TN_REQUIRE(n_rays == tr->R, TN_E_INVALID, "tn_trainer_train_step_rays: n_rays must equal n_rays_per_step (%u)", tr->R);
+    int st = settle(tr);
+    if (st != TN_OK) return st;
+    // the plain path steps in the current set; the fused path takes the step's head into the other
+    RaySet& q = tr->set[tr->d.path == TN_PATH_PLAIN ? tr->cur : tr->cur ^ 1];
     cudaStream_t s = tr->stream;
     const size_t row = (size_t)n_rays * sizeof(float);
-    int st = cuda_status(cudaMemcpy2DAsync(tr->ori, row, ori, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
-    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(tr->dir, row, dir, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
-    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(tr->target, row, target_rgba, row, row, 4, cudaMemcpyHostToDevice, s), "rays H2D");
-    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(tr->bg, row, bg_rgb, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
+    st = cuda_status(cudaMemcpy2DAsync(q.ori, row, ori, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(q.dir, row, dir, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(q.target, row, target_rgba, row, row, 4, cudaMemcpyHostToDevice, s), "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaMemcpy2DAsync(q.bg, row, bg_rgb, row, row, 3, cudaMemcpyHostToDevice, s), "rays H2D");
     if (st != TN_OK) return st;
     return train_step_impl(tr, true, metrics);
 }
@@ -727,13 +904,15 @@ int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const 
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "pipelined steps run on the fused path");
     TN_REQUIRE(n_rays == tr->R, TN_E_INVALID, "tn_trainer_train_step_rays_pipelined: n_rays must equal n_rays_per_step (%u)",
                tr->R);
+    int st = drop_spec(tr);
+    if (st != TN_OK) return st;
     cudaStream_t s = tr->stream;
     const int slot = (int)(tr->ring_calls & 1u);
-    // host rays to this slot's staging buffer on the copy stream, once the step two calls back has
+    // host rays to this slot's staging buffer on the copy stream, once the call two back has
     // taken the slot's previous contents; the step stream waits for the copy and takes the rays
     const size_t R = n_rays;
     float* stg = tr->stage[slot];
-    int st = cuda_status(cudaStreamWaitEvent(tr->h2d, tr->ev_consumed[slot], 0), "staging free");
+    st = cuda_status(cudaStreamWaitEvent(tr->h2d, tr->ev_consumed[slot], 0), "staging free");
     const float* src[4] = {ori, dir, target_rgba, bg_rgb};
     const size_t at[4] = {0, 3 * R, 6 * R, 10 * R}, len[4] = {3 * R, 3 * R, 4 * R, 3 * R};
     for (int k = 0; k < 4 && st == TN_OK; ++k)
@@ -741,60 +920,77 @@ int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const 
                          "rays H2D");
     if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_staged[slot], tr->h2d), "staged");
     if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_staged[slot], 0), "wait staged");
+    // The new step's head goes into the set that no step in flight uses: with a step pending,
+    // the set of the last completed step (the pending step's tail runs on the other one).
+    const bool has_prev = tr->pending_ext;
+    const int p = tr->cur ^ 1;
+    RaySet& dst = tr->set[has_prev ? tr->cur : p];
     if (st == TN_OK)
-        st = cuda_status(cudaMemcpyAsync(tr->ori, stg, 13 * R * sizeof(float), cudaMemcpyDeviceToDevice, s), "rays D2D");
+        st = cuda_status(cudaMemcpyAsync(dst.ori, stg, 13 * R * sizeof(float), cudaMemcpyDeviceToDevice, s), "rays D2D");
     if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_consumed[slot], s), "consumed");
-    if (st == TN_OK) st = train_step_impl(tr, true, nullptr);
     if (st != TN_OK) return st;
-    // this step's state and error word to its slot, the error word cleared for the next step
-    st = cuda_status(cudaMemcpyAsync(&tr->ring_state[slot], tr->state, sizeof(StepState), cudaMemcpyDeviceToHost, s),
-                     "state to ring");
-    if (st == TN_OK)
-        st = cuda_status(cudaMemcpyAsync(&tr->ring_flags[slot], tr->ctx->flags, sizeof(uint32_t),
-                                         cudaMemcpyDeviceToHost, s), "flags to ring");
-    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->ctx->flags, 0, sizeof(uint32_t), s), "flags clear");
-    if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_ring[slot], s), "ring event");
-    if (st != TN_OK) return st;
-    const bool has_prev = tr->ring_calls > 0;
     ++tr->ring_calls;
     if (!has_prev) {
-        *previous = tn_training_metrics{};  // step 0: no earlier pipelined step
+        // first call: the step's head only; its tail runs beside the next call's head
+        st = enqueue_kind(tr, K_H, true, p, -1);
+        if (st != TN_OK) return st;
+        tr->pending_ext = true;
+        *previous = tn_training_metrics{};
         return TN_OK;
     }
-    // the previous step: wait for it only (this step stays queued behind it)
-    const int prev = slot ^ 1;
-    st = cuda_status(cudaEventSynchronize(tr->ev_ring[prev]), "previous step");
+    // the pending step's tail beside this step's head; its state is copied to ring slot p
+    constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+    tr->ring_flag[p] = kEmpty;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    st = enqueue_kind(tr, K_TH, true, p, p);
     if (st != TN_OK) return st;
-    return metrics_from(tr, tr->ring_state[prev], tr->ring_flags[prev], previous);
+    tr->select(p);
+    ++tr->fused_steps_enqueued;
+    // wait for the pending step only (this step's head may still be marching): the slot's flag,
+    // or the end of everything queued, whichever comes first; a failed stream ends the wait
+    while (tr->ring_flag[p] == kEmpty) {
+        const cudaError_t q = cudaStreamQuery(s);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) return cuda_status(q, "previous step");
+        std::this_thread::yield();
+    }
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    if (tr->ring_flag[p] == kEmpty) return fail(TN_E_CUDA, "previous step: its state never arrived");
+    return metrics_from(tr, tr->ring_state[p], previous);
 }
 
 int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages) {
     TN_NONNULL(tr); TN_NONNULL(stage_ms);
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "stage timing covers the fused path");
-    // the timed step runs its own Adam in order; a pending one is applied first, untimed
-    const int fst = flush_adam(tr);
+    // the timed step runs alone and in order
+    const int fst = settle(tr);
     if (fst != TN_OK) return fst;
+    const int q = tr->cur ^ 1;
     cudaEvent_t ev[ST_N + 1];
     for (auto& e : ev) cudaEventCreate(&e);
-    int st = enqueue_fused_step(tr, false, ev);
+    int st = enqueue_profiled_step(tr, tr->set[q], ev);
     if (st == TN_OK) st = cuda_status(cudaEventSynchronize(ev[ST_N]), "profile sync");
     const uint32_t n = std::min<uint32_t>(max_stages, ST_N);
     for (uint32_t k = 0; k < n && st == TN_OK; ++k) cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
     for (auto& e : ev) cudaEventDestroy(e);
+    if (st == TN_OK) tr->select(q);
     ++tr->fused_steps_enqueued;
     if (n_stages) *n_stages = n;
     return st;
 }
 
-// Releases the captured step graphs; the next step captures them again (after a change of
-// launch shapes).
+// Releases the captured step graphs; the next steps run eagerly once and capture them again
+// (after a change of launch shapes, ray source or alpha selection).
 static void drop_graphs(tn_trainer* tr) {
-    for (int i = 0; i < 2; ++i) {
-        if (tr->graph_exec[i]) cudaGraphExecDestroy(tr->graph_exec[i]);
-        if (tr->graph[i]) cudaGraphDestroy(tr->graph[i]);
-        tr->graph_exec[i] = nullptr;
-        tr->graph[i] = nullptr;
-    }
+    for (int k = 0; k < K_KINDS; ++k)
+        for (int r = 0; r < 2; ++r)
+            for (int p = 0; p < 2; ++p) {
+                if (tr->graph_exec[k][r][p]) cudaGraphExecDestroy(tr->graph_exec[k][r][p]);
+                if (tr->graph[k][r][p]) cudaGraphDestroy(tr->graph[k][r][p]);
+                tr->graph_exec[k][r][p] = nullptr;
+                tr->graph[k][r][p] = nullptr;
+                tr->warm[k][r][p] = false;
+            }
 }
 
 int tn_trainer_set_dataset(tn_trainer* tr, uint32_t n_images, int32_t width, int32_t height, const tn_camera* cameras,
@@ -802,7 +998,7 @@ int tn_trainer_set_dataset(tn_trainer* tr, uint32_t n_images, int32_t width, int
     TN_NONNULL(tr); TN_NONNULL(cameras); TN_NONNULL(images);
     int st = check_dataset(n_images, width, height);
     if (st != TN_OK) return st;
-    st = flush_adam(tr);
+    st = settle(tr);  // a head computed ahead took the old ray source
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_set_dataset");
     if (st != TN_OK) return st;
     const size_t texels = (size_t)n_images * (size_t)width * (size_t)height;
@@ -810,7 +1006,8 @@ int tn_trainer_set_dataset(tn_trainer* tr, uint32_t n_images, int32_t width, int
     uint8_t* imgs = nullptr;
     st = tr->alloc(cams, n_images);
     if (st == TN_OK) st = tr->alloc(imgs, 4 * texels);
-    if (st == TN_OK && !tr->ds_random) st = tr->alloc(tr->ds_random, 2 * (size_t)tr->R);
+    for (int k = 0; k < 2; ++k)
+        if (st == TN_OK && !tr->set[k].ds_random) st = tr->alloc(tr->set[k].ds_random, 2 * (size_t)tr->R);
     if (st == TN_OK)
         st = cuda_status(cudaMemcpyAsync(cams, cameras, n_images * sizeof(tn_camera), cudaMemcpyHostToDevice, tr->stream),
                          "dataset cameras");
@@ -831,7 +1028,7 @@ int tn_trainer_set_alpha_selection(tn_trainer* tr, float threshold, float probab
     TN_NONNULL(tr);
     TN_REQUIRE(threshold == threshold && probability == probability, TN_E_INVALID, "alpha selection: NaN");
     if (threshold == tr->alpha_threshold && probability == tr->alpha_probability) return TN_OK;
-    const int st = flush_adam(tr);
+    const int st = settle(tr);  // a head computed ahead selected its rays with the old values
     if (st != TN_OK) return st;
     tr->alpha_threshold = threshold;
     tr->alpha_probability = probability;
@@ -842,7 +1039,7 @@ int tn_trainer_set_alpha_selection(tn_trainer* tr, float threshold, float probab
 int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
     TN_NONNULL(tr);
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "tn_trainer_autotune: the fused path only");
-    const int fst = flush_adam(tr);  // the network forward below reads the parameters
+    const int fst = settle(tr);  // the tuners rewrite the march context's scratch
     if (fst != TN_OK) return fst;
     cudaStream_t s = tr->stream;
     const tn_trainer_desc& d = tr->d;
@@ -851,8 +1048,8 @@ int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
     int st = cuda_status(cudaStreamSynchronize(s), "tn_trainer_autotune");
     // before the first step the ray buffers are empty: generate the first step's rays
     if (st == TN_OK && tr->fused_steps_enqueued == 0)
-        st = enqueue_own_rays(tr, s);
-    uint32_t* info = tr->state->batch_info;
+        st = enqueue_own_rays(tr, s, tr->set[tr->cur]);
+    uint32_t* info = tr->set[tr->cur].info;
     tn_tune_report rep[3] = {};
     if (st == TN_OK)
         st = tn_autotune_march(tr->ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, nullptr,
@@ -869,6 +1066,8 @@ int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
                                 d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb,
                                 tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, tr->target, tr->bg, nullptr,
                                 tr->grad_density, tr->dl_drgb, tr->state->loss_sums, &rep[2]);
+    // both march contexts take the chosen shapes
+    if (st == TN_OK) st = tn_ctx_set_tuning(tr->set[tr->cur ^ 1].ctx, &tr->ctx->tune);
     drop_graphs(tr);  // the captured step graphs hold the previous shapes
     if (reports)
         for (int k = 0; k < 3; ++k) reports[k] = rep[k];
@@ -877,7 +1076,7 @@ int tn_trainer_autotune(tn_trainer* tr, tn_tune_report* reports) {
 
 int tn_trainer_flush(tn_trainer* tr) {
     TN_NONNULL(tr);
-    int st = flush_adam(tr);
+    int st = settle(tr, true);
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_flush");
     return st;
 }
@@ -896,7 +1095,7 @@ struct FileCloser {
 
 int tn_trainer_save(tn_trainer* tr, const char* path, const char* dataset_path) {
     TN_NONNULL(tr); TN_NONNULL(path);
-    int st = flush_adam(tr);
+    int st = settle(tr, true);
     if (st != TN_OK) return st;
     const size_t P = tr->P, V = tr->V, LV = (size_t)tr->d.grid.n_levels * V;
     std::vector<float> w(P), m(P), v(P), density(LV);
@@ -984,9 +1183,10 @@ int tn_trainer_load(tn_trainer* tr, const char* path) {
              std::fread(density.data(), 4, LV, fc.f) == LV;
     }
     if (!ok) return fail(TN_E_INVALID, "reading %s failed", path);
-    // a pending Adam update belongs to the replaced state: dropped, not applied
+    // a requested step completes on the old state; a head computed ahead read the old grid
+    st = settle(tr);
     cudaStream_t s = tr->stream;
-    st = cuda_status(cudaStreamSynchronize(s), "load sync");
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "load sync");
     auto h2d = [&](void* dst, const void* src, size_t bytes) {
         if (st == TN_OK) st = cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "load write");
     };
@@ -1017,13 +1217,15 @@ int tn_trainer_load(tn_trainer* tr, const char* path) {
 // workspace, then runs setup_data again, which re-creates them as at the start of training
 // (parameters from the fixed seed, fresh optimizer state, every grid bit set, densities zero,
 // training_step = 0). Here the buffers are kept and rewritten to that state; the captured step
-// graphs stay valid, since they only hold the buffers' addresses. A pending Adam update belongs
-// to the discarded run and is dropped. The gradient source of the built-in stand-in network
-// (its fixed synthetic gradients) is the network's, not the trainer's, and is kept.
+// graphs stay valid, since they only hold the buffers' addresses. A pending caller-ray step
+// completes first and a head counted ahead is dropped. The gradient source of the built-in
+// stand-in network (its fixed synthetic gradients) is the network's, not the trainer's, and is
+// kept.
 int tn_trainer_reset(tn_trainer* tr) {
     TN_NONNULL(tr);
     cudaStream_t s = tr->stream;
-    int st = cuda_status(cudaStreamSynchronize(tr->h2d), "reset sync");
+    int st = settle(tr);
+    if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->h2d), "reset sync");
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->aux), "reset sync");
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "reset sync");
     const size_t P = tr->P, V = tr->V, LV = (size_t)tr->d.grid.n_levels * V;
@@ -1036,7 +1238,7 @@ int tn_trainer_reset(tn_trainer* tr) {
     clear(tr->v, 0, P * 4);
     clear(tr->steps, 0, P * 4);
     clear(tr->state, 0, sizeof(StepState));
-    clear(tr->ctx->flags, 0, sizeof(uint32_t));
+    for (int k = 0; k < 2; ++k) clear(tr->set[k].ctx->flags, 0, sizeof(uint32_t));
     if (st == TN_OK) st = launch_synth_params(s, (uint32_t)P, tr->d.n_grid_params, tr->d.seed, tr->w);
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(s), "reset sync");
     if (st != TN_OK) return st;
@@ -1049,7 +1251,7 @@ int tn_trainer_reset(tn_trainer* tr) {
 int tn_trainer_render(tn_trainer* tr, const tn_camera* camera, const tn_bbox* render_bbox, float min_step_size,
                       uint32_t batch_size, float* out_rgba, tn_render_stats* stats) {
     TN_NONNULL(tr);
-    int st = flush_adam(tr);
+    int st = settle(tr, true);
     if (st != TN_OK) return st;
     tn_render_desc rd{};
     rd.grid = tr->d.grid;
@@ -1070,9 +1272,9 @@ int tn_trainer_get_tuning(tn_trainer* tr, tn_tuning* out) {
 
 int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t) {
     TN_NONNULL(tr);
-    int st = flush_adam(tr);
+    int st = settle(tr);  // a head computed ahead ran with the old shapes
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_set_tuning");
-    if (st == TN_OK) st = tn_ctx_set_tuning(tr->ctx, t);
+    for (int k = 0; k < 2 && st == TN_OK; ++k) st = tn_ctx_set_tuning(tr->set[k].ctx, t);
     if (st == TN_OK) drop_graphs(tr);
     return st;
 }
@@ -1080,13 +1282,17 @@ int tn_trainer_set_tuning(tn_trainer* tr, const tn_tuning* t) {
 int tn_trainer_stat(tn_trainer* tr, int which, uint64_t* out) {
     TN_NONNULL(tr); TN_NONNULL(out);
     switch (which) {
-        case 0: *out = tr->graph_kernels[0]; return TN_OK;
-        case 1: *out = tr->graph_kernels[1]; return TN_OK;
-        case 2: *out = tr->graph_nodes[0]; return TN_OK;
+        // the step graph of own rays (tail beside the next head, or the in-order step) and of
+        // caller rays (the pipelined or the synchronous call)
+        case 0: *out = tr->graph_kernels[tr->lookahead() ? K_TH : K_HT][0]; return TN_OK;
+        case 1: *out = tr->graph_kernels[K_TH][1] ? tr->graph_kernels[K_TH][1] : tr->graph_kernels[K_HT][1]; return TN_OK;
+        case 2: *out = tr->graph_nodes[tr->lookahead() ? K_TH : K_HT][0]; return TN_OK;
         case 3:
         case 4:
         case 5: {
-            int st = cuda_status(cudaMemcpyAsync(tr->state_host, tr->state, sizeof(StepState), cudaMemcpyDeviceToHost,
+            int st = settle(tr, true);  // a requested step counts once its tail has run
+            if (st == TN_OK)
+                st = cuda_status(cudaMemcpyAsync(tr->state_host, tr->state, sizeof(StepState), cudaMemcpyDeviceToHost,
                                                  tr->stream), "stat");
             if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "stat sync");
             if (st != TN_OK) return st;
@@ -1105,12 +1311,13 @@ int tn_trainer_sync_metrics(tn_trainer* tr, tn_training_metrics* metrics) {
         if (metrics) *metrics = tr->last;
         return st;
     }
-    return read_state(tr, metrics);
+    const int st = settle(tr, true);  // a requested caller-ray step runs its tail first
+    return st == TN_OK ? read_state(tr, metrics) : st;
 }
 
 int tn_trainer_update_occupancy_grid(tn_trainer* tr, uint32_t training_step, tn_occupancy_metrics* metrics) {
     TN_NONNULL(tr);
-    const int fst = flush_adam(tr);  // the density network reads the parameters
+    const int fst = settle(tr);  // a head computed ahead read the grid this rewrites
     if (fst != TN_OK) return fst;
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream;
@@ -1167,8 +1374,8 @@ int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out) {
 
 int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes) {
     TN_NONNULL(tr); TN_NONNULL(ptr);
-    // the parameters the caller may read include every step's update
-    int fst = flush_adam(tr);
+    // the state the caller reads includes every requested step
+    int fst = settle(tr, true);
     if (fst == TN_OK) fst = cuda_status(cudaStreamSynchronize(tr->stream), "tn_trainer_buffer");
     if (fst != TN_OK) return fst;
     const uint64_t R = tr->R, B = tr->B, V = tr->V, P = tr->P, L = (uint64_t)tr->d.grid.n_levels;
@@ -1201,7 +1408,11 @@ int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes) {
         case 23: p = tr->bg; n = 12 * R; break;
         case 24: p = tr->s_mnorm; n = 4 * B; break;
         case 25: p = tr->s_dtnorm; n = 4 * B; break;
-        case 26: p = tr->ds_random; n = tr->ds_random ? 8 * R : 0; break;
+        case 26: p = tr->set[tr->cur].ds_random; n = p ? 8 * R : 0; break;
+        case 27: p = tr->occ_levels; n = 4ull * tr->M; break;
+        case 28: p = tr->occ_cells; n = 4ull * tr->M; break;
+        case 29: p = tr->occ_values; n = 4ull * tr->M; break;
+        case 30: p = tr->occ_rsel; n = 4ull * tr->M; break;
         default: return fail(TN_E_INVALID, "unknown trainer buffer %d", which);
     }
     *ptr = p;

@@ -287,8 +287,8 @@ class Trainer:
                 "tuning": self.tuning}
 
     def flush(self) -> None:
-        """Applies a pending Adam update (pipelined steps run each update at the start of the
-        next step) and waits for the trainer's stream."""
+        """Completes a requested caller-ray step (the pipelined call leaves the last step's tail
+        to run beside the next call's march) and waits for the trainer's stream."""
         call("tn_trainer_flush", self._handle())
 
     @property
