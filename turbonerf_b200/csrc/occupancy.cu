@@ -264,7 +264,7 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
                             uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
                             const float* values, const float* rand_select, int activation, int sample_all,
                             const uint32_t* sample_all_dev, const uint32_t* n_dev, float decay, float threshold,
-                            uint32_t* n_occupied_dev) {
+                            uint32_t* n_occupied_dev, uint8_t* bitfield_out) {
     TN_NONNULL(ctx);
     int st = validate_grid(grid);
     if (st != TN_OK) return st;
@@ -273,7 +273,9 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
         TN_NONNULL(levels); TN_NONNULL(cells); TN_NONNULL(values);
         if (!sample_all || sample_all_dev) TN_NONNULL(rand_select);
     }
-    TN_REQUIRE(((uintptr_t)density & 15u) == 0 && ((uintptr_t)bitfield & 3u) == 0, TN_E_INVALID,
+    // the selection rule reads `bitfield`; the rebuilt bits go to bitfield_out (default: in place)
+    if (!bitfield_out) bitfield_out = bitfield;
+    TN_REQUIRE(((uintptr_t)density & 15u) == 0 && ((uintptr_t)bitfield_out & 3u) == 0, TN_E_INVALID,
                "tn_occupancy_update: density must be 16-byte and bitfield 4-byte aligned");
     const uint32_t volume = (uint32_t)grid->resolution * grid->resolution * grid->resolution;
     if (n_occupied_dev) {
@@ -289,8 +291,8 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
         if (st != TN_OK) return st;
     }
     const uint32_t v4 = volume / 4;
-    occ_sweep_kernel<<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield, decay, threshold,
-                                                           n_occupied_dev);
+    occ_sweep_kernel<<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out, decay,
+                                                           threshold, n_occupied_dev);
     return check_launch("tn_occupancy_update(sweep)");
 }
 

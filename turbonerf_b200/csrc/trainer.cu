@@ -107,6 +107,10 @@ struct RaySet {
     uint32_t *n_steps = nullptr, *offsets = nullptr;
     uint32_t* info = nullptr;      // device batch_info[4] of this set's count
     float* ds_random = nullptr;    // [2][R] dataset draws of this set's rays (with a dataset)
+    // the occupancy query of this set's step: random cells, their points, the network's values
+    int32_t* occ_levels = nullptr;
+    uint32_t* occ_cells = nullptr;
+    float *occ_rand3 = nullptr, *occ_rsel = nullptr, *occ_pos = nullptr, *occ_values = nullptr;
     tn_ctx* ctx = nullptr;
 };
 
@@ -140,10 +144,14 @@ struct tn_trainer {
     // plain-path scratch
     float *loss4, *dl_rec, *dl_dist, *ray5, *sample2, *ray_loss;
     uint8_t* count_scratch;
-    // grid
+    // grid: densities, and the bitfield of the last completed step (an alias of bits_buf). With
+    // an occupancy update in every step the bitfield is double-buffered, so that a step's update
+    // can rebuild it while the step's emit pass still reads the one its count used: the step in
+    // set s reads bits_buf[s ^ 1] and writes bits_buf[s].
     float* density;
     uint8_t* bits;
-    // occupancy re-sampling
+    uint8_t* bits_buf[2] = {nullptr, nullptr};
+    // occupancy re-sampling of the last completed step (aliases of set[cur])
     int32_t* occ_levels;
     uint32_t* occ_cells;
     float *occ_rand3, *occ_rsel, *occ_pos, *occ_values;
@@ -184,8 +192,14 @@ struct tn_trainer {
         RaySet& q = set[p];
         ori = q.ori; dir = q.dir; target = q.target; bg = q.bg;
         ray_t = q.ray_t; ray_tmax = q.ray_tmax; alive = q.alive; n_steps = q.n_steps; offsets = q.offsets;
+        occ_levels = q.occ_levels; occ_cells = q.occ_cells; occ_rand3 = q.occ_rand3; occ_rsel = q.occ_rsel;
+        occ_pos = q.occ_pos; occ_values = q.occ_values;
         ctx = q.ctx;
+        bits = bits_buf[M > 0 ? p : 0];
     }
+    // the bitfield the step in set s marches on, and the one its occupancy update writes
+    uint8_t* head_bits(int s) const { return bits_buf[M > 0 ? s ^ 1 : 0]; }
+    uint8_t* tail_bits(int s) const { return bits_buf[M > 0 ? s : 0]; }
     bool lookahead() const { return d.path == TN_PATH_FUSED && ctx->tune.side_sms > 0; }
 
     template <typename T>
@@ -229,77 +243,80 @@ static int enqueue_own_rays(tn_trainer* tr, cudaStream_t s, RaySet& q) {
                              q.target, q.bg, q.ray_t, q.ray_tmax, q.alive);
 }
 
-// Occupancy query of one step: random cells, their sample points, the density network.
-static int enqueue_occupancy_query(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid) {
+// Occupancy query of one step (the step keyed by *key): random cells, their sample points, the
+// density network, into set q's query buffers.
+static int enqueue_occupancy_query(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, RaySet& q,
+                                   const uint32_t* key) {
     const tn_trainer_desc& d = tr->d;
-    int st = launch_synth_cells(s, tr->M, d.seed, &tr->state->cur_step, grid.n_levels, tr->V, tr->occ_levels,
-                                tr->occ_cells, tr->occ_rand3, tr->M, tr->occ_rsel);
+    int st = launch_synth_cells(s, tr->M, d.seed, key, grid.n_levels, tr->V, q.occ_levels, q.occ_cells, q.occ_rand3,
+                                tr->M, q.occ_rsel);
     if (st == TN_OK)
-        st = tn_occupancy_sample_points(s, &grid, tr->M, tr->occ_levels, tr->occ_cells, tr->occ_rand3, tr->M,
-                                        1.0f / tr->aabb, tr->occ_pos, tr->M);
-    if (st == TN_OK) st = tr->net.density(tr->net.user, s, tr->M, nullptr, tr->M, tr->occ_pos, tr->occ_values);
+        st = tn_occupancy_sample_points(s, &grid, tr->M, q.occ_levels, q.occ_cells, q.occ_rand3, tr->M,
+                                        1.0f / tr->aabb, q.occ_pos, tr->M);
+    if (st == TN_OK) st = tr->net.density(tr->net.user, s, tr->M, nullptr, tr->M, q.occ_pos, q.occ_values);
     return st;
 }
 
-// Occupancy update of one step: decay + max-update of the queried cells, bitfield rebuild.
-static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, tn_ctx* ctx) {
+// Occupancy update of the step in set pi: decay + max-update of the queried cells (the selection
+// rule reads the bitfield the step marched on), bitfield rebuild into the step's output bitfield.
+static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, int pi) {
     const tn_trainer_desc& d = tr->d;
-    return launch_occupancy_update(ctx, s, &grid, tr->density, tr->bits, tr->M, tr->occ_levels, tr->occ_cells,
-                                   tr->occ_values, tr->occ_rsel, tr->net.activation, 0, &tr->state->sample_all,
-                                   nullptr, d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied);
+    RaySet& p = tr->set[pi];
+    return launch_occupancy_update(p.ctx, s, &grid, tr->density, tr->head_bits(pi), tr->M, p.occ_levels, p.occ_cells,
+                                   p.occ_values, p.occ_rsel, tr->net.activation, 0, &tr->state->sample_all, nullptr,
+                                   d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied,
+                                   tr->tail_bits(pi));
 }
 
 // Head of a step: its rays (own, or the caller's already in set q, clipped to the box) and the
 // march count with the batch cut into set q's buffers and context.
-static int enqueue_head(tn_trainer* tr, cudaStream_t s, bool external, RaySet& q) {
+static int enqueue_head(tn_trainer* tr, cudaStream_t s, bool external, int qi) {
     const tn_trainer_desc& d = tr->d;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
+    RaySet& q = tr->set[qi];
     int st = external ? tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, q.ori, q.dir, q.ray_t, q.ray_tmax, q.alive)
                       : enqueue_own_rays(tr, s, q);
     if (st == TN_OK)
-        st = tn_march_count(q.ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, q.ori, q.dir,
+        st = tn_march_count(q.ctx, s, &grid, tr->head_bits(qi), &d.bbox, &march, tr->R, tr->R, nullptr, q.ori, q.dir,
                             q.ray_t, q.ray_tmax, q.alive, q.n_steps, tr->B, q.info);
     return st;
 }
 
-// Tail of the step whose head is in set p: step_begin, emit, network forward, the fused losses,
-// network backward, Adam and, on the second stream, the step's occupancy query and update. With
-// next != nullptr the head of the following step (rays from next_external / own rays) runs on
-// the third stream into set *next once the occupancy update has rewritten the bitfield, and Adam
-// keeps to side_sms SMs beside it. ring >= 0 copies the finished step's state into that pinned
-// slot (and clears the state's error bits) before the head is joined.
-static int enqueue_tail(tn_trainer* tr, RaySet& p, RaySet* next, bool next_external, int ring) {
+// Tail of the step whose head is in set pi: step_begin, emit, network forward, the fused losses,
+// network backward and Adam; on the second stream the step's occupancy update (from the query
+// made with its head), which rebuilds the step's output bitfield while the emit pass still reads
+// the one the count used. With next >= 0 the head of the following step (rays from
+// next_external / own rays) runs on the third stream into set next once the occupancy update is
+// done, Adam keeps to side_sms SMs beside it, and the following step's occupancy query runs
+// after Adam (the density network reads the updated parameters). ring >= 0 copies the finished
+// step's state into that pinned slot before the head is joined.
+static int enqueue_tail(tn_trainer* tr, int pi, int next, bool next_external, int ring) {
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream, so = tr->aux, cs = tr->cstream;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
     const bool occ = tr->M > 0;
+    RaySet& p = tr->set[pi];
     step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
     int st = check_launch("step_begin");
-    if (st == TN_OK && (occ || next)) {
-        st = cuda_status(cudaEventRecord(tr->ev_fork, s), "fork");
-        if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
-        if (st == TN_OK && occ) st = enqueue_occupancy_query(tr, so, grid);
+    if (st == TN_OK && (occ || next >= 0)) st = cuda_status(cudaEventRecord(tr->ev_fork, s), "fork");
+    if (st == TN_OK && occ) {
+        st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
+        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid, pi);
+        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_occ, so), "occupancy done");
+    }
+    // the next step's head reads the rebuilt grid
+    if (st == TN_OK && next >= 0) {
+        st = cuda_status(cudaStreamWaitEvent(cs, occ ? tr->ev_occ : tr->ev_fork, 0), "head start");
+        if (st == TN_OK) st = enqueue_head(tr, cs, next_external, next);
+        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_head, cs), "head done");
     }
     uint32_t* info = p.info;
     if (st == TN_OK)
-        st = tn_march_emit(p.ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B, info,
-                           nullptr, p.ori, p.dir, p.ray_t, p.alive, p.n_steps, p.offsets, nullptr, tr->s_t, tr->s_pos,
-                           tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
-    // the occupancy update rewrites the bitfield, which the emit pass may still read
-    if (st == TN_OK && occ) {
-        st = cuda_status(cudaEventRecord(tr->ev_emit, s), "emit done");
-        if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(so, tr->ev_emit, 0), "emit done");
-        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid, p.ctx);
-        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_occ, so), "occupancy done");
-    }
-    // the next step's head reads the updated grid
-    if (st == TN_OK && next) {
-        st = cuda_status(cudaStreamWaitEvent(cs, occ ? tr->ev_occ : tr->ev_fork, 0), "head start");
-        if (st == TN_OK) st = enqueue_head(tr, cs, next_external, *next);
-        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_head, cs), "head done");
-    }
+        st = tn_march_emit(p.ctx, s, &grid, tr->head_bits(pi), &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B,
+                           info, nullptr, p.ori, p.dir, p.ray_t, p.alive, p.n_steps, p.offsets, nullptr, tr->s_t,
+                           tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
     if (st == TN_OK)
         st = tr->net.forward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
                              tr->net_rgb);
@@ -315,7 +332,7 @@ static int enqueue_tail(tn_trainer* tr, RaySet& p, RaySet* next, bool next_exter
                               tr->dl_drgb, tr->g);
     if (st == TN_OK) {
         AdamPlacement place;
-        if (next && p.ctx->tune.side_sms) {
+        if (next >= 0 && p.ctx->tune.side_sms) {
             place.max_blocks = p.ctx->tune.side_sms;
             place.reserve_smem = exclusive_smem();
         }
@@ -324,6 +341,8 @@ static int enqueue_tail(tn_trainer* tr, RaySet& p, RaySet* next, bool next_exter
                          tr->steps, place);
     }
     if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_occ, 0), "occupancy joined");
+    // the following step's occupancy query, keyed by its index (step_count after this step_begin)
+    if (st == TN_OK && occ && next >= 0) st = enqueue_occupancy_query(tr, s, grid, tr->set[next], &tr->state->step_count);
     if (st == TN_OK) {
         step_end_kernel<<<1, 1, 0, s>>>(tr->state, info, p.ctx->flags);
         st = check_launch("step_end");
@@ -336,26 +355,27 @@ static int enqueue_tail(tn_trainer* tr, RaySet& p, RaySet* next, bool next_exter
         st = cuda_status(cudaMemcpyAsync(&tr->ring_state[ring], tr->state, sizeof(StepState), cudaMemcpyDeviceToHost,
                                          s), "state to ring");
         if (st == TN_OK)
-            st = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(&tr->ring_flag[ring]), &tr->state->step_count, sizeof(uint32_t),
-                                             cudaMemcpyDeviceToHost, s), "ring flag");
+            st = cuda_status(cudaMemcpyAsync(const_cast<uint32_t*>(&tr->ring_flag[ring]), &tr->state->step_count,
+                                             sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "ring flag");
         if (st == TN_OK) st = cuda_status(cudaMemsetAsync(&tr->state->err, 0, sizeof(uint32_t), s), "err clear");
     }
-    if (st == TN_OK && next) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_head, 0), "head joined");
+    if (st == TN_OK && next >= 0) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_head, 0), "head joined");
     return st;
 }
 
 // One fused step in order on the trainer's stream with events between its stages (stage
-// timing): head and tail of the step in set p, nothing beside it.
-static int enqueue_profiled_step(tn_trainer* tr, RaySet& p, cudaEvent_t* ev) {
+// timing): head and tail of the step in set pi, nothing beside it.
+static int enqueue_profiled_step(tn_trainer* tr, int pi, cudaEvent_t* ev) {
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
+    RaySet& p = tr->set[pi];
     cudaEventRecord(ev[0], s);
     int st = enqueue_own_rays(tr, s, p);
     cudaEventRecord(ev[ST_RAYS + 1], s);
     if (st == TN_OK)
-        st = tn_march_count(p.ctx, s, &grid, tr->bits, &d.bbox, &march, tr->R, tr->R, nullptr, p.ori, p.dir,
+        st = tn_march_count(p.ctx, s, &grid, tr->head_bits(pi), &d.bbox, &march, tr->R, tr->R, nullptr, p.ori, p.dir,
                             p.ray_t, p.ray_tmax, p.alive, p.n_steps, tr->B, p.info);
     cudaEventRecord(ev[ST_COUNT + 1], s);
     if (st == TN_OK) {
@@ -363,9 +383,9 @@ static int enqueue_profiled_step(tn_trainer* tr, RaySet& p, cudaEvent_t* ev) {
         st = check_launch("step_begin");
     }
     if (st == TN_OK)
-        st = tn_march_emit(p.ctx, s, &grid, tr->bits, &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B, p.info,
-                           nullptr, p.ori, p.dir, p.ray_t, p.alive, p.n_steps, p.offsets, nullptr, tr->s_t, tr->s_pos,
-                           tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
+        st = tn_march_emit(p.ctx, s, &grid, tr->head_bits(pi), &d.bbox, &march, 1.0f / tr->aabb, tr->R, tr->R, tr->B,
+                           p.info, nullptr, p.ori, p.dir, p.ray_t, p.alive, p.n_steps, p.offsets, nullptr, tr->s_t,
+                           tr->s_pos, tr->s_dir, tr->s_dt, tr->s_mnorm, tr->s_dtnorm);
     cudaEventRecord(ev[ST_EMIT + 1], s);
     if (st == TN_OK)
         st = tr->net.forward(tr->net.user, s, tr->B, p.info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
@@ -388,9 +408,9 @@ static int enqueue_profiled_step(tn_trainer* tr, RaySet& p, cudaEvent_t* ev) {
                          &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
                          tr->steps, AdamPlacement{});
     cudaEventRecord(ev[ST_ADAM + 1], s);
-    if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_query(tr, s, grid);
+    if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_query(tr, s, grid, p, &tr->state->cur_step);
     cudaEventRecord(ev[ST_OCC_QUERY + 1], s);
-    if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_update(tr, s, grid, p.ctx);
+    if (st == TN_OK && tr->M > 0) st = enqueue_occupancy_update(tr, s, grid, pi);
     cudaEventRecord(ev[ST_OCCUPANCY + 1], s);
     if (st == TN_OK) {
         step_end_kernel<<<1, 1, 0, s>>>(tr->state, p.info, p.ctx->flags);
@@ -404,17 +424,24 @@ static int enqueue_profiled_step(tn_trainer* tr, RaySet& p, cudaEvent_t* ev) {
 // initialises every lazily created resource); later runs replay a graph captured once.
 static int enqueue_kind(tn_trainer* tr, int kind, bool external, int p, int ring) {
     const int src = external ? 1 : 0;
+    // a head without a tail before it also makes its step's occupancy query (a tail runs the
+    // next step's query after its Adam update); before its step_begin, the step's key is
+    // step_count
+    auto head_alone = [&]() -> int {
+        int st = enqueue_head(tr, tr->stream, external, p);
+        if (st == TN_OK && tr->M > 0)
+            st = enqueue_occupancy_query(tr, tr->stream, tr->grid(), tr->set[p], &tr->state->step_count);
+        return st;
+    };
     auto body = [&]() -> int {
-        RaySet& a = tr->set[p];
-        RaySet& b = tr->set[p ^ 1];
         switch (kind) {
             case K_HT: {
-                int st = enqueue_head(tr, tr->stream, external, a);
-                return st == TN_OK ? enqueue_tail(tr, a, nullptr, false, ring) : st;
+                const int st = head_alone();
+                return st == TN_OK ? enqueue_tail(tr, p, -1, false, ring) : st;
             }
-            case K_TH: return enqueue_tail(tr, a, &b, external, ring);
-            case K_H: return enqueue_head(tr, tr->stream, external, a);
-            default: return enqueue_tail(tr, a, nullptr, false, ring);
+            case K_TH: return enqueue_tail(tr, p, p ^ 1, external, ring);
+            case K_H: return head_alone();
+            default: return enqueue_tail(tr, p, -1, false, ring);
         }
     };
     // a ring copy is baked into a graph: the pipelined caller-ray steps copy into slot p
@@ -700,7 +727,6 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
         ALLOC(q.ray_t, R); ALLOC(q.ray_tmax, R);
         ALLOC(q.alive, R); ALLOC(q.n_steps, R); ALLOC(q.offsets, R); ALLOC(q.info, 4);
     }
-    if (st == TN_OK) tr->select(0);
     ALLOC(tr->stage[0], 13 * (size_t)R); ALLOC(tr->stage[1], 13 * (size_t)R);
     ALLOC(tr->s_t, B); ALLOC(tr->s_pos, 3 * B); ALLOC(tr->s_dir, 3 * B); ALLOC(tr->s_dt, B); ALLOC(tr->s_mnorm, B);
     ALLOC(tr->s_dtnorm, B); ALLOC(tr->net_density, B); ALLOC(tr->net_rgb, 3 * B); ALLOC(tr->grad_density, B);
@@ -710,12 +736,21 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
         ALLOC(tr->sample2, 2 * B); ALLOC(tr->ray_loss, R);
     }
     ALLOC(tr->count_scratch, V / 4);
-    ALLOC(tr->density, (size_t)L * V); ALLOC(tr->bits, V);
-    ALLOC(tr->occ_levels, occ_n); ALLOC(tr->occ_cells, occ_n); ALLOC(tr->occ_rand3, 3 * (size_t)occ_n);
-    ALLOC(tr->occ_rsel, occ_n); ALLOC(tr->occ_pos, 3 * (size_t)occ_n); ALLOC(tr->occ_values, occ_n);
+    ALLOC(tr->density, (size_t)L * V); ALLOC(tr->bits_buf[0], V);
+    if (tr->M > 0) {
+        ALLOC(tr->bits_buf[1], V);
+    } else {
+        tr->bits_buf[1] = tr->bits_buf[0];
+    }
+    for (int k = 0; k < 2; ++k) {
+        RaySet& q = tr->set[k];
+        ALLOC(q.occ_levels, occ_n); ALLOC(q.occ_cells, occ_n); ALLOC(q.occ_rand3, 3 * (size_t)occ_n);
+        ALLOC(q.occ_rsel, occ_n); ALLOC(q.occ_pos, 3 * (size_t)occ_n); ALLOC(q.occ_values, occ_n);
+    }
     ALLOC(tr->w, P); ALLOC(tr->g, P); ALLOC(tr->m, P); ALLOC(tr->v, P); ALLOC(tr->steps, P);
     ALLOC(tr->state, 1);
 #undef ALLOC
+    if (st == TN_OK) tr->select(0);
     if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->state_host, sizeof(StepState)), "pinned state");
     if (st == TN_OK) st = cuda_status(cudaMallocHost(&tr->ring_state, 2 * sizeof(StepState)), "pinned state ring");
     if (st == TN_OK) {
@@ -724,7 +759,8 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
         tr->ring_flag = f;
     }
     // reference initial grid: every bit set, densities zero (occupancy-grid.cuh:81-85)
-    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->bits, 0xFF, V, tr->stream), "bitfield init");
+    for (int k = 0; k < 2 && st == TN_OK; ++k)
+        st = cuda_status(cudaMemsetAsync(tr->bits_buf[k], 0xFF, V, tr->stream), "bitfield init");
     if (st == TN_OK) st = launch_synth_params(tr->stream, P, desc->n_grid_params, desc->seed, tr->w);
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "trainer init");
     if (st != TN_OK) {
@@ -968,7 +1004,7 @@ int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages
     const int q = tr->cur ^ 1;
     cudaEvent_t ev[ST_N + 1];
     for (auto& e : ev) cudaEventCreate(&e);
-    int st = enqueue_profiled_step(tr, tr->set[q], ev);
+    int st = enqueue_profiled_step(tr, q, ev);
     if (st == TN_OK) st = cuda_status(cudaEventSynchronize(ev[ST_N]), "profile sync");
     const uint32_t n = std::min<uint32_t>(max_stages, ST_N);
     for (uint32_t k = 0; k < n && st == TN_OK; ++k) cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
