@@ -394,13 +394,51 @@ __device__ __forceinline__ uint32_t cell_of(float f, uint32_t res_m1) { return m
 // reference computes the same expression in both, occupancy-grid.cuh:155-159 and :268-272).
 //  * t_lim = min(the float below t_max, t_stop) merges `t < t_max` with the tail cut: past
 //    t_stop the ray stays outside every occupied cell, so the loop ends with the same count.
-//  * max_steps is UINT32_MAX when unlimited.
+//  * the box test (`if (!bbox.contains(p)) break`, training-batch-kernels.cuh:263-265) is made
+//    once at the first step and folded into t_lim for the others (box_exit_t below).
+//  * LIMIT: max_steps (otherwise unlimited) ends the ray after that many occupied steps.
 //  * spread holds three Morton spread tables, pre-shifted for x, y and z.
 //  * slots record the t of the first slot_cap occupied steps for the emit pass.
-template <int NL, bool MIP>
-__device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const RayMarch& r, float t_lim,
-                              uint32_t max_steps, uint32_t* flags, const uint8_t* __restrict__ mip,
-                              const uint32_t* __restrict__ spread, float* __restrict__ slots, uint32_t slot_cap) {
+// Order-preserving map of the non-NaN floats to unsigned integers (a < b <=> key(a) < key(b)).
+__device__ __forceinline__ uint32_t float_key(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+// The last t >= t0 at which the march's point o + t d (computed fl(o + fl(t d)), as ray_point
+// does) still lies on the inner side of the box face the ray leaves through along one axis.
+// Both roundings are monotone, so the coordinate is monotone in t and the face test holds on a
+// prefix of the floats from t0; the end of the prefix is found by bisection over the float
+// order (at most 32 halvings). The caller has checked the test at t0. d == 0: never leaves.
+__device__ float axis_exit_t(float o, float d, float lo, float hi, float t0) {
+    if (d == 0.0f) return INFINITY;
+    uint32_t a = float_key(t0), b = float_key(INFINITY);  // inside at a, outside at b (o + inf d = +-inf)
+    while (b - a > 1u) {
+        const uint32_t m = a + ((b - a) >> 1);
+        const float x = __fadd_rn(o, __fmul_rn(key_float(m), d));
+        if (d > 0.0f ? x <= hi : x >= lo) a = m;
+        else b = m;
+    }
+    return key_float(a);
+}
+
+// The last t of the loop's steps (from t0 on) whose point the reference's box test accepts,
+// given that it accepts the point at t0: along every axis the face test facing the ray's
+// origin keeps holding once it holds (the coordinate moves away from that face), so the test
+// fails first at the earliest exit over the three axes.
+__device__ __forceinline__ float box_exit_t(const tn_bbox& b, const RayMarch& r, float t0) {
+    return fminf(axis_exit_t(r.ox, r.dx, b.min_x, b.max_x, t0),
+                 fminf(axis_exit_t(r.oy, r.dy, b.min_y, b.max_y, t0), axis_exit_t(r.oz, r.dz, b.min_z, b.max_z, t0)));
+}
+
+template <int NL, bool MIP, bool LIMIT>
+__device__ uint32_t count_ray_loop(const MarchArgs& a, const CountGrid& cg, const RayMarch& r, float t_lim,
+                                   uint32_t max_steps, uint32_t* flags, const uint8_t* __restrict__ mip,
+                                   const uint32_t* __restrict__ spread, float* __restrict__ slots,
+                                   uint32_t slot_cap) {
     const float hx = __fmul_rn(0.5f, copysignf(1.0f, r.dx));
     const float hy = __fmul_rn(0.5f, copysignf(1.0f, r.dy));
     const float hz = __fmul_rn(0.5f, copysignf(1.0f, r.dz));
@@ -412,7 +450,6 @@ __device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const Ray
         if (++iters > a.max_iters) { raise_flag(flags, ERR_GUARD); break; }
         float x, y, z;
         ray_point(r, t, x, y, z);
-        if (!bbox_contains(a.bbox, x, y, z)) break;
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
         const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));
         const int k = count_level<NL>(m, dt, cg.half0_bits, cg.cell0_bits, cg.n_levels);
@@ -444,9 +481,23 @@ __device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const Ray
         const float t_occ = __fadd_rn(t, dt);
         t = occ ? t_occ : t_skip;
         n += occ ? 1u : 0u;
-        if (n >= max_steps) break;
+        if (LIMIT && n >= max_steps) break;
     }
     return n;
+}
+
+template <int NL, bool MIP>
+__device__ uint32_t count_ray(const MarchArgs& a, const CountGrid& cg, const RayMarch& r, float t_lim,
+                              uint32_t max_steps, uint32_t* flags, const uint8_t* __restrict__ mip,
+                              const uint32_t* __restrict__ spread, float* __restrict__ slots, uint32_t slot_cap) {
+    if (!(r.t <= t_lim)) return 0;  // no step (a NaN limit included)
+    float x, y, z;
+    ray_point(r, r.t, x, y, z);
+    if (!bbox_contains(a.bbox, x, y, z)) return 0;  // the first step leaves the box
+    t_lim = fminf(t_lim, box_exit_t(a.bbox, r, r.t));
+    return max_steps == 0xffffffffu
+               ? count_ray_loop<NL, MIP, false>(a, cg, r, t_lim, max_steps, flags, mip, spread, slots, slot_cap)
+               : count_ray_loop<NL, MIP, true>(a, cg, r, t_lim, max_steps, flags, mip, spread, slots, slot_cap);
 }
 
 // World-space box that holds every occupied cell of every level: per level, the box of its

@@ -82,7 +82,11 @@ __global__ void occ_scatter_kernel(uint32_t n, uint32_t volume, int n_levels, fl
 __device__ __forceinline__ float settle(float v, float decay) { return signbit(v) ? -v : v * decay; }
 
 // Issues every level's 16-byte load of the thread's four cells before using any of them, so
-// each thread keeps n_levels loads in flight.
+// each thread keeps n_levels loads in flight. WRITE_DENSITY stores the settled densities;
+// WRITE_BITS rebuilds the bitfield (and counts its set bits). The one-pass update does both; the
+// split update runs a bits-only pass first (what the next march waits for) and the density
+// write-back after it, beside the march.
+template <bool WRITE_DENSITY, bool WRITE_BITS>
 __global__ void __launch_bounds__(256)
 occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, uint8_t* __restrict__ bits,
                  float decay, float threshold, uint32_t* __restrict__ n_occupied) {
@@ -93,7 +97,7 @@ occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, ui
         float4 v[MAX_LEVELS];
 #pragma unroll
         for (int k = 0; k < MAX_LEVELS; ++k)
-            if (k < n_levels) v[k] = __ldcs(d4 + (size_t)k * volume4 + i);
+            if (k < n_levels) v[k] = WRITE_DENSITY ? __ldcs(d4 + (size_t)k * volume4 + i) : d4[(size_t)k * volume4 + i];
         uint32_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
 #pragma unroll
         for (int k = 0; k < MAX_LEVELS; ++k) {
@@ -103,7 +107,7 @@ occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, ui
                 x.y = settle(x.y, decay);
                 x.z = settle(x.z, decay);
                 x.w = settle(x.w, decay);
-                __stcs(d4 + (size_t)k * volume4 + i, x);
+                if (WRITE_DENSITY) __stcs(d4 + (size_t)k * volume4 + i, x);
                 b0 |= (uint32_t)(x.x > threshold) << k;
                 b1 |= (uint32_t)(x.y > threshold) << k;
                 b2 |= (uint32_t)(x.z > threshold) << k;
@@ -111,10 +115,10 @@ occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, ui
             }
         }
         const uint32_t packed = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
-        reinterpret_cast<uint32_t*>(bits)[i] = packed;
+        if (WRITE_BITS) reinterpret_cast<uint32_t*>(bits)[i] = packed;
         cnt = __popc(packed);
     }
-    if (n_occupied) {
+    if (WRITE_BITS && n_occupied) {
         cnt = warp_sum(cnt);
         __shared__ uint32_t ws[8];
         if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = cnt;
@@ -219,8 +223,8 @@ int launch_occupancy_sweep(cudaStream_t stream, const tn_grid_desc* grid, float*
         if (st != TN_OK) return st;
     }
     const uint32_t v4 = volume / 4;
-    occ_sweep_kernel<<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield, decay, threshold,
-                                                           n_occupied_dev);
+    occ_sweep_kernel<true, true><<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield, decay,
+                                                                       threshold, n_occupied_dev);
     return check_launch("occupancy sweep");
 }
 
@@ -264,7 +268,10 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
                             uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
                             const float* values, const float* rand_select, int activation, int sample_all,
                             const uint32_t* sample_all_dev, const uint32_t* n_dev, float decay, float threshold,
-                            uint32_t* n_occupied_dev, uint8_t* bitfield_out) {
+                            uint32_t* n_occupied_dev, uint8_t* bitfield_out, cudaEvent_t bits_done) {
+    // bits_done: split update; the event is recorded once the bitfield is rebuilt, before the
+    // settled densities are written back
+    const bool split = bits_done != nullptr;
     TN_NONNULL(ctx);
     int st = validate_grid(grid);
     if (st != TN_OK) return st;
@@ -291,9 +298,20 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
         if (st != TN_OK) return st;
     }
     const uint32_t v4 = volume / 4;
-    occ_sweep_kernel<<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out, decay,
-                                                           threshold, n_occupied_dev);
-    return check_launch("tn_occupancy_update(sweep)");
+    if (!split) {
+        occ_sweep_kernel<true, true><<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out,
+                                                                           decay, threshold, n_occupied_dev);
+        return check_launch("tn_occupancy_update(sweep)");
+    }
+    occ_sweep_kernel<false, true><<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out,
+                                                                        decay, threshold, n_occupied_dev);
+    st = check_launch("tn_occupancy_update(bits)");
+    if (st != TN_OK || !bits_done) return st;
+    st = cuda_status(cudaEventRecord(bits_done, stream), "occupancy bits done");
+    if (st != TN_OK) return st;
+    occ_sweep_kernel<true, false><<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out,
+                                                                        decay, threshold, nullptr);
+    return check_launch("tn_occupancy_update(densities)");
 }
 
 }  // namespace tn

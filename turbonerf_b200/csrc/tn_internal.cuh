@@ -108,7 +108,8 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
                             uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
                             const float* values, const float* rand_select, int activation, int sample_all,
                             const uint32_t* sample_all_dev, const uint32_t* n_dev, float decay, float threshold,
-                            uint32_t* n_occupied_dev, uint8_t* bitfield_out = nullptr);
+                            uint32_t* n_occupied_dev, uint8_t* bitfield_out = nullptr,
+                            cudaEvent_t bits_done = nullptr);
 int launch_occupancy_scatter(cudaStream_t stream, const tn_grid_desc* grid, float* density, const uint8_t* bitfield,
                              uint32_t n_updates, const int32_t* levels, const uint32_t* cells, const float* values,
                              const float* rand_select, int activation, int sample_all, float decay);

@@ -125,7 +125,7 @@ struct tn_trainer {
     cudaStream_t stream = nullptr;
     // the occupancy query and update beside the training chain, and the next step's head
     cudaStream_t aux = nullptr, cstream = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_emit = nullptr, ev_occ = nullptr, ev_head = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_emit = nullptr, ev_occ = nullptr, ev_occ_all = nullptr, ev_head = nullptr;
     RaySet set[2];
     int cur = 0;               // set of the last completed step (the aliases below point into it)
     bool spec_own = false;     // set cur ^ 1 holds the head of the next step, computed from own rays
@@ -259,28 +259,39 @@ static int enqueue_occupancy_query(tn_trainer* tr, cudaStream_t s, const tn_grid
 
 // Occupancy update of the step in set pi: decay + max-update of the queried cells (the selection
 // rule reads the bitfield the step marched on), bitfield rebuild into the step's output bitfield.
-static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, int pi) {
+// With bits_done the rebuild runs first and records the event, and the decayed densities are
+// written back after it (the next step's march waits only for the bits).
+static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, int pi,
+                                    cudaEvent_t bits_done = nullptr) {
     const tn_trainer_desc& d = tr->d;
     RaySet& p = tr->set[pi];
     return launch_occupancy_update(p.ctx, s, &grid, tr->density, tr->head_bits(pi), tr->M, p.occ_levels, p.occ_cells,
                                    p.occ_values, p.occ_rsel, tr->net.activation, 0, &tr->state->sample_all, nullptr,
                                    d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied,
-                                   tr->tail_bits(pi));
+                                   tr->tail_bits(pi), bits_done);
 }
 
 // Head of a step: its rays (own, or the caller's already in set q, clipped to the box) and the
 // march count with the batch cut into set q's buffers and context.
-static int enqueue_head(tn_trainer* tr, cudaStream_t s, bool external, int qi) {
+static int enqueue_head_rays(tn_trainer* tr, cudaStream_t s, bool external, int qi) {
+    const tn_trainer_desc& d = tr->d;
+    RaySet& q = tr->set[qi];
+    return external ? tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, q.ori, q.dir, q.ray_t, q.ray_tmax, q.alive)
+                    : enqueue_own_rays(tr, s, q);
+}
+
+static int enqueue_head_count(tn_trainer* tr, cudaStream_t s, int qi) {
     const tn_trainer_desc& d = tr->d;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
     RaySet& q = tr->set[qi];
-    int st = external ? tn_rays_init_bbox(s, tr->R, tr->R, &d.bbox, 3.0e38f, q.ori, q.dir, q.ray_t, q.ray_tmax, q.alive)
-                      : enqueue_own_rays(tr, s, q);
-    if (st == TN_OK)
-        st = tn_march_count(q.ctx, s, &grid, tr->head_bits(qi), &d.bbox, &march, tr->R, tr->R, nullptr, q.ori, q.dir,
-                            q.ray_t, q.ray_tmax, q.alive, q.n_steps, tr->B, q.info);
-    return st;
+    return tn_march_count(q.ctx, s, &grid, tr->head_bits(qi), &d.bbox, &march, tr->R, tr->R, nullptr, q.ori, q.dir,
+                          q.ray_t, q.ray_tmax, q.alive, q.n_steps, tr->B, q.info);
+}
+
+static int enqueue_head(tn_trainer* tr, cudaStream_t s, bool external, int qi) {
+    int st = enqueue_head_rays(tr, s, external, qi);
+    return st == TN_OK ? enqueue_head_count(tr, s, qi) : st;
 }
 
 // Tail of the step whose head is in set pi: step_begin, emit, network forward, the fused losses,
@@ -301,15 +312,18 @@ static int enqueue_tail(tn_trainer* tr, int pi, int next, bool next_external, in
     step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
     int st = check_launch("step_begin");
     if (st == TN_OK && (occ || next >= 0)) st = cuda_status(cudaEventRecord(tr->ev_fork, s), "fork");
+    // the occupancy update; beside a next head, split: ev_occ once the bitfield is rebuilt
     if (st == TN_OK && occ) {
         st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
-        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid, pi);
-        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_occ, so), "occupancy done");
+        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid, pi, next >= 0 ? tr->ev_occ : nullptr);
+        if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_occ_all, so), "occupancy done");
     }
-    // the next step's head reads the rebuilt grid
+    // the next step's head: its rays at once, its march count on the rebuilt grid
     if (st == TN_OK && next >= 0) {
-        st = cuda_status(cudaStreamWaitEvent(cs, occ ? tr->ev_occ : tr->ev_fork, 0), "head start");
-        if (st == TN_OK) st = enqueue_head(tr, cs, next_external, next);
+        st = cuda_status(cudaStreamWaitEvent(cs, tr->ev_fork, 0), "head start");
+        if (st == TN_OK) st = enqueue_head_rays(tr, cs, next_external, next);
+        if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(cs, tr->ev_occ, 0), "grid rebuilt");
+        if (st == TN_OK) st = enqueue_head_count(tr, cs, next);
         if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_head, cs), "head done");
     }
     uint32_t* info = p.info;
@@ -340,7 +354,7 @@ static int enqueue_tail(tn_trainer* tr, int pi, int next, bool next_external, in
                          &tr->state->lr, d.beta1, d.beta2, d.epsilon, d.l2_reg, tr->w, nullptr, tr->g, tr->m, tr->v,
                          tr->steps, place);
     }
-    if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_occ, 0), "occupancy joined");
+    if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_occ_all, 0), "occupancy joined");
     // the following step's occupancy query, keyed by its index (step_count after this step_begin)
     if (st == TN_OK && occ && next >= 0) st = enqueue_occupancy_query(tr, s, grid, tr->set[next], &tr->state->step_count);
     if (st == TN_OK) {
@@ -690,7 +704,7 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->aux, cudaStreamNonBlocking), "aux stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->cstream, cudaStreamNonBlocking), "head stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->h2d, cudaStreamNonBlocking), "copy stream");
-    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_occ, &tr->ev_head,
+    for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_occ, &tr->ev_occ_all, &tr->ev_head,
                            &tr->ev_staged[0], &tr->ev_staged[1], &tr->ev_consumed[0], &tr->ev_consumed[1]})
         if (st == TN_OK) st = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "step events");
     for (int k = 0; k < 2 && st == TN_OK; ++k) st = tn_ctx_create(&tr->set[k].ctx);
@@ -786,7 +800,7 @@ int tn_trainer_destroy(tn_trainer* tr) {
     for (int k = 0; k < 2; ++k)
         if (tr->set[k].ctx) tn_ctx_destroy(tr->set[k].ctx);
     if (tr->h2d) cudaStreamSynchronize(tr->h2d);
-    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_occ, tr->ev_head,
+    for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_occ, tr->ev_occ_all, tr->ev_head,
                           tr->ev_staged[0], tr->ev_staged[1], tr->ev_consumed[0], tr->ev_consumed[1]})
         if (e) cudaEventDestroy(e);
     if (tr->h2d) cudaStreamDestroy(tr->h2d);
