@@ -166,17 +166,16 @@ struct tn_trainer {
     StepState* ring_state = nullptr;  // pinned [2]
     volatile uint32_t* ring_flag = nullptr;  // pinned [2]: step count of the state in the slot
     uint64_t ring_calls = 0;          // pipelined calls since the last synchronous read
-    // pipelined steps copy their host rays into a staging buffer on a copy stream, beside the
-    // previous step; the step stream takes them from there with one device copy
+    // pipelined steps copy their host rays into the idle ray set on a copy stream, beside the
+    // step in flight
     cudaStream_t h2d = nullptr;
-    float* stage[2] = {nullptr, nullptr};
     // a dataset of posed images as the ray source (tn_trainer_set_dataset)
     tn_camera* ds_cameras = nullptr;
     uint8_t* ds_images = nullptr;
     uint32_t ds_n = 0;
     int32_t ds_w = 0, ds_h = 0;
     float alpha_threshold = 1.0f, alpha_probability = 1.0f;
-    cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_consumed[2] = {nullptr, nullptr};
+    cudaEvent_t ev_staged[2] = {nullptr, nullptr};
     // [kind][ray source: own, caller][ray set of the tail, or of the head for K_H]
     cudaGraph_t graph[K_KINDS][2][2] = {};
     cudaGraphExec_t graph_exec[K_KINDS][2][2] = {};
@@ -705,7 +704,7 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->cstream, cudaStreamNonBlocking), "head stream");
     if (st == TN_OK) st = cuda_status(cudaStreamCreateWithFlags(&tr->h2d, cudaStreamNonBlocking), "copy stream");
     for (cudaEvent_t* e : {&tr->ev_fork, &tr->ev_emit, &tr->ev_occ, &tr->ev_occ_all, &tr->ev_head,
-                           &tr->ev_staged[0], &tr->ev_staged[1], &tr->ev_consumed[0], &tr->ev_consumed[1]})
+                           &tr->ev_staged[0], &tr->ev_staged[1]})
         if (st == TN_OK) st = cuda_status(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "step events");
     for (int k = 0; k < 2 && st == TN_OK; ++k) st = tn_ctx_create(&tr->set[k].ctx);
     const uint32_t R = desc->n_rays_per_step, B = desc->batch_size;
@@ -728,8 +727,7 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
         }
     }
 #define ALLOC(p, n) if (st == TN_OK) st = tr->alloc(p, (size_t)(n))
-    // each set's input rays in one allocation, [ori 3R | dir 3R | target 4R | bg 3R], so that a
-    // pipelined step takes them from its staging buffer in one copy
+    // each set's input rays in one allocation, [ori 3R | dir 3R | target 4R | bg 3R]
     for (int k = 0; k < 2; ++k) {
         RaySet& q = tr->set[k];
         ALLOC(q.ori, 13 * (size_t)R);
@@ -741,7 +739,6 @@ int tn_trainer_create(tn_trainer** out, const tn_trainer_desc* desc, const tn_ne
         ALLOC(q.ray_t, R); ALLOC(q.ray_tmax, R);
         ALLOC(q.alive, R); ALLOC(q.n_steps, R); ALLOC(q.offsets, R); ALLOC(q.info, 4);
     }
-    ALLOC(tr->stage[0], 13 * (size_t)R); ALLOC(tr->stage[1], 13 * (size_t)R);
     ALLOC(tr->s_t, B); ALLOC(tr->s_pos, 3 * B); ALLOC(tr->s_dir, 3 * B); ALLOC(tr->s_dt, B); ALLOC(tr->s_mnorm, B);
     ALLOC(tr->s_dtnorm, B); ALLOC(tr->net_density, B); ALLOC(tr->net_rgb, 3 * B); ALLOC(tr->grad_density, B);
     ALLOC(tr->dl_drgb, 3 * B);
@@ -801,7 +798,7 @@ int tn_trainer_destroy(tn_trainer* tr) {
         if (tr->set[k].ctx) tn_ctx_destroy(tr->set[k].ctx);
     if (tr->h2d) cudaStreamSynchronize(tr->h2d);
     for (cudaEvent_t e : {tr->ev_fork, tr->ev_emit, tr->ev_occ, tr->ev_occ_all, tr->ev_head,
-                          tr->ev_staged[0], tr->ev_staged[1], tr->ev_consumed[0], tr->ev_consumed[1]})
+                          tr->ev_staged[0], tr->ev_staged[1]})
         if (e) cudaEventDestroy(e);
     if (tr->h2d) cudaStreamDestroy(tr->h2d);
     if (tr->aux) cudaStreamDestroy(tr->aux);
@@ -957,27 +954,24 @@ int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const 
     int st = drop_spec(tr);
     if (st != TN_OK) return st;
     cudaStream_t s = tr->stream;
-    const int slot = (int)(tr->ring_calls & 1u);
-    // host rays to this slot's staging buffer on the copy stream, once the call two back has
-    // taken the slot's previous contents; the step stream waits for the copy and takes the rays
-    const size_t R = n_rays;
-    float* stg = tr->stage[slot];
-    st = cuda_status(cudaStreamWaitEvent(tr->h2d, tr->ev_consumed[slot], 0), "staging free");
-    const float* src[4] = {ori, dir, target_rgba, bg_rgb};
-    const size_t at[4] = {0, 3 * R, 6 * R, 10 * R}, len[4] = {3 * R, 3 * R, 4 * R, 3 * R};
-    for (int k = 0; k < 4 && st == TN_OK; ++k)
-        st = cuda_status(cudaMemcpyAsync(stg + at[k], src[k], len[k] * sizeof(float), cudaMemcpyHostToDevice, tr->h2d),
-                         "rays H2D");
-    if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_staged[slot], tr->h2d), "staged");
-    if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_staged[slot], 0), "wait staged");
     // The new step's head goes into the set that no step in flight uses: with a step pending,
-    // the set of the last completed step (the pending step's tail runs on the other one).
+    // the set of the last completed step (the pending step's tail runs on the other one, and
+    // the previous call waited for the step before it). The host rays are copied straight into
+    // it on the copy stream, beside whatever the step stream is still running; the step waits
+    // for the copy.
     const bool has_prev = tr->pending_ext;
     const int p = tr->cur ^ 1;
     RaySet& dst = tr->set[has_prev ? tr->cur : p];
-    if (st == TN_OK)
-        st = cuda_status(cudaMemcpyAsync(dst.ori, stg, 13 * R * sizeof(float), cudaMemcpyDeviceToDevice, s), "rays D2D");
-    if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_consumed[slot], s), "consumed");
+    const int slot = (int)(tr->ring_calls & 1u);
+    const size_t R = n_rays;
+    const float* src[4] = {ori, dir, target_rgba, bg_rgb};
+    float* to[4] = {dst.ori, dst.dir, dst.target, dst.bg};
+    const size_t len[4] = {3 * R, 3 * R, 4 * R, 3 * R};
+    for (int k = 0; k < 4 && st == TN_OK; ++k)
+        st = cuda_status(cudaMemcpyAsync(to[k], src[k], len[k] * sizeof(float), cudaMemcpyHostToDevice, tr->h2d),
+                         "rays H2D");
+    if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_staged[slot], tr->h2d), "staged");
+    if (st == TN_OK) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_staged[slot], 0), "wait staged");
     if (st != TN_OK) return st;
     ++tr->ring_calls;
     if (!has_prev) {
@@ -997,12 +991,14 @@ int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const 
     tr->select(p);
     ++tr->fused_steps_enqueued;
     // wait for the pending step only (this step's head may still be marching): the slot's flag,
-    // or the end of everything queued, whichever comes first; a failed stream ends the wait
+    // or the end of everything queued, whichever comes first; a failed stream ends the wait. The
+    // flag is read many times between two queries of the stream.
     while (tr->ring_flag[p] == kEmpty) {
+        for (int spin = 0; spin < 256 && tr->ring_flag[p] == kEmpty; ++spin) std::this_thread::yield();
+        if (tr->ring_flag[p] != kEmpty) break;
         const cudaError_t q = cudaStreamQuery(s);
         if (q == cudaSuccess) break;
         if (q != cudaErrorNotReady) return cuda_status(q, "previous step");
-        std::this_thread::yield();
     }
     std::atomic_thread_fence(std::memory_order_seq_cst);
     if (tr->ring_flag[p] == kEmpty) return fail(TN_E_CUDA, "previous step: its state never arrived");
