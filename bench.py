@@ -393,6 +393,12 @@ def run_ours(args):
         return
 
     cpu = None if args.no_cpu else cpu_baseline(seconds=args.cpu_seconds)
+    others = None
+    if world == 1 and not args.no_configs:
+        try:
+            others = other_configs(args)
+        except Exception as e:  # a side measurement never takes the headline line with it
+            others = {"error": f"{type(e).__name__}: {e}"}
     bi = RAYS * 4 * (3 + 3 + 4 + 3)
     line = {
         "metric": METRIC, "value": round(result["value"], 1), "unit": "samples/s", "n_gpus": world,
@@ -414,6 +420,7 @@ def run_ours(args):
         "plain": plain,
         "speedup_vs_plain": round(result["value"] / plain["value"], 2) if plain else None,
         "cpu_baseline": cpu,
+        "other_configs": others,
     }
     print(json.dumps(line), flush=True)
 
@@ -592,7 +599,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_backward_memory(args):
+def backward_memory_result(args):
     """Backward memory study: 2^22 samples over about 2^16 rays (truncated geometric counts,
     mean 64, at most 1024; sigma and rgb as in the compositor workload), compositor + distortion
     loss forward and backward, two ways:
@@ -650,7 +657,11 @@ def run_backward_memory(args):
             "n_samples": ss, "n_rays": n, "dtype": "f32", "data": "synthetic",
             "store_minus_recompute_bytes": result["store"]["extra_device_bytes"] -
                                            result["recompute"]["extra_device_bytes"], **result}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_backward_memory(args):
+    print(json.dumps(backward_memory_result(args)), flush=True)
 
 
 def _multi_scene_gpu(params, resolution=128, threshold=THRESHOLD):
@@ -683,7 +694,7 @@ def _multi_scene_gpu(params, resolution=128, threshold=THRESHOLD):
     return ms, table
 
 
-def run_multi_scene(args):
+def multi_scene_result(args, labels=("as_drawn", "scaled_2e19_samples")):
     """Batched multi-scene march: 16 scenes, each its own blob field (8-32 blobs), 1-5 cascades
     of 128^3 and an AABB of size 0.5-16, ray counts log-uniform in 2^10..2^16, rays from a
     sphere of radius 4A/3 toward the centre (cone stepping 1/256). Times the march count +
@@ -701,6 +712,8 @@ def run_multi_scene(args):
     out = {"workload": "batched multi-scene march count + emit: 16 scenes, 8-32 blobs, 1-5 cascades of 128^3, "
                        "AABB 0.5-16, rays log-uniform 2^10..2^16", "dtype": "f32", "data": "synthetic"}
     for label, scale in (("as_drawn", None), ("scaled_2e19_samples", 1 << 19)):
+        if label not in labels:
+            continue
         ps = [dict(p) for p in params]
         if scale is not None:
             f = scale / max(out["as_drawn"]["n_samples"], 1)
@@ -777,7 +790,11 @@ def run_multi_scene(args):
         assert ctx.check() == 0 and ctx_s.check() == 0
         res["persistent_speedup"] = round(res["per_scene"]["ms"] / res["persistent"]["ms"], 3)
         out[label] = res
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_multi_scene(args):
+    print(json.dumps(multi_scene_result(args)), flush=True)
 
 
 def run_kernel_tour(args):
@@ -1072,7 +1089,7 @@ def run_dataset_rays(args):
     print(json.dumps(res), flush=True)
 
 
-def run_configs(args):
+def configs_result(args):
     """GPU and CPU oracle side by side on the smaller configurations, samples/s each:
     * forward march + composite: 1 cascade of 128^3 over [-1.5, 1.5]^3, 8 blobs, 4096 rays from
       a radius-4 sphere, fixed dt = sqrt(3)/1024, at most 1024 steps; march count, emit (no
@@ -1172,7 +1189,39 @@ def run_configs(args):
                                "gpu_samples_per_s": round(ns / sec, 1), "cpu_s": round(el, 3),
                                "cpu_samples_per_s": round(ns / el, 1)})
         del ctx
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_configs(args):
+    print(json.dumps(configs_result(args)), flush=True)
+
+
+def other_configs(args):
+    """The smaller configurations beside the train step, for the default bench line: GPU and
+    CPU-oracle samples/s of the forward march + composite (1 cascade, 4096 rays) and of the
+    compositor + distortion forward/backward at 2^18 samples; the batched multi-scene march
+    (16 scenes, 128^3, 2^10..2^16 rays a scene), persistent launch against one launch per scene;
+    the device memory of the recompute and store backwards at 2^22 samples."""
+    import torch
+    cfg = configs_result(args)
+    rows = {c["config"]: c for c in cfg["configs"]}
+    out = {"cores": cfg["cores"]}
+    for key, label in (("march_composite_4096_rays", "forward march + composite, 1 x 128^3, 4096 rays"),
+                       ("compositor_distortion_2e18", "compositor + distortion fwd/bwd, 2^18 samples")):
+        c = rows[label]
+        out[key] = {"gpu_samples_per_s": c["gpu_samples_per_s"], "cpu_samples_per_s": c["cpu_samples_per_s"],
+                    "samples": c["samples"], "gpu_ms": c["gpu_ms"]}
+    torch.cuda.empty_cache()
+    ms = multi_scene_result(args, labels=("as_drawn",))["as_drawn"]
+    out["multi_scene_16"] = {"n_rays": ms["n_rays"], "n_samples": ms["n_samples"],
+                             "persistent_ms": ms["persistent"]["ms"], "per_scene_ms": ms["per_scene"]["ms"],
+                             "persistent_speedup": ms["persistent_speedup"]}
+    torch.cuda.empty_cache()
+    bm = backward_memory_result(args)
+    out["backward_memory_2e22"] = {v: {"extra_device_bytes": bm[v]["extra_device_bytes"], "ms": bm[v]["ms"]}
+                                   for v in ("recompute", "store")}
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -1183,6 +1232,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="leave the smaller configurations out of the line")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--render-sizes", default="800x800,1920x1080", help="render workload: frame sizes WxH")

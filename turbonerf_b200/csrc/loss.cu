@@ -1578,28 +1578,55 @@ __device__ __forceinline__ void sc_load_dist(const Samples& S, uint32_t o, uint3
     }
 }
 
+// A ray of more than RB_MAX samples: the same three passes as the blocked path (compositor
+// forward to the cut, distortion forward, reversed backward with the merge), each over chunks
+// of RB_MAX samples that are staged through the warp's buffer `sm` with cp.async, with the
+// chunk's outputs written back through the buffer in coalesced rows.
 __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r, uint32_t o, uint32_t n, int lane,
                                                    float min_t, float inv_nrays, float grad_scale, float lambda,
                                                    const float* __restrict__ target, const float* __restrict__ bg,
                                                    uint32_t rs, float* __restrict__ ray_rgba,
                                                    float* __restrict__ grad_density, float* __restrict__ drgb,
-                                                   float& acc_rec, float& acc_dist) {
+                                                   float& acc_rec, float& acc_dist, float* sm) {
     constexpr int K = RB_SPL;
     const size_t ss = S.ss;
     const uint32_t nch = (n + RB_MAX - 1) / RB_MAX;
+    const uint32_t l0 = (uint32_t)lane * K;  // the lane's first sample inside a chunk
+    float* const b_sig = sm + SA_SIG * RB_SKEW;
+    float* const b_dt = sm + SA_DT * RB_SKEW;
+    float* const b_r = sm + SA_R * RB_SKEW;
+    float* const b_g = sm + SA_G * RB_SKEW;
+    float* const b_b = sm + SA_B * RB_SKEW;
+    float* const b_dtn = sm + SA_DTN * RB_SKEW;
+    float* const b_m = sm + SA_M * RB_SKEW;
+    float* const b_t = sm + SA_T * RB_SKEW;
+    float* const b_gd = sm + SA_GD * RB_SKEW;
+    // Each pass stages a chunk's inputs into the warp's buffer (one round trip to memory) and
+    // reads them from there; the chunk's samples are [c0, c0 + len).
+    auto chunk_len = [&](uint32_t c) { return min(RB_MAX, n - c * RB_MAX); };
+    auto stage_done = [&]() { cp_async_wait_all(); __syncwarp(); };
     // ---- compositor forward over the chunks up to the transmittance cut
     float cx = 0.0f, tin = 1.0f;
     float ar = 0.0f, ag = 0.0f, ab = 0.0f, aa = 0.0f;
     uint32_t used = n;
     float depth = 0.0f;
     for (uint32_t c = 0; c < nch; ++c) {
-        const uint32_t j0 = c * RB_MAX + (uint32_t)lane * K;
+        const size_t c0 = (size_t)o + (size_t)c * RB_MAX;
+        const uint32_t len = chunk_len(c);
+        __syncwarp();  // the previous chunk's reads of the buffer are done
+        stage_segment(b_sig, S.density, c0, len, lane);
+        stage_segment(b_dt, S.dt, c0, len, lane);
+        stage_segment(b_r, S.rgb, c0, len, lane);
+        stage_segment(b_g, S.rgb + ss, c0, len, lane);
+        stage_segment(b_b, S.rgb + 2 * ss, c0, len, lane);
+        stage_done();
+        const uint32_t j0 = c * RB_MAX + l0;
         float x[K], p[K], T[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) {
-            const bool valid = j0 + q < n;
-            const size_t s = (size_t)o + j0 + q;
-            x[q] = valid ? act_sigma(S.act, S.density[s]) * S.dt[s] : 0.0f;
+            const bool valid = l0 + q < len;
+            const uint32_t k = skew(l0 + q);
+            x[q] = valid ? act_sigma(S.act, b_sig[k]) * b_dt[k] : 0.0f;
             p[q] = x[q];
         }
         blk_prefix(p, lane, cx);
@@ -1622,9 +1649,9 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
         for (int q = 0; q < K; ++q) {
             const uint32_t j = j0 + q;
             if (j < cut) {
-                const size_t s = (size_t)o + j;
+                const uint32_t k = skew(l0 + q);
                 const float w = (q ? T[q - 1] : t_lane) * -expm1f(-x[q]);
-                ar += w * S.rgb[s]; ag += w * S.rgb[s + ss]; ab += w * S.rgb[s + 2 * ss]; aa += w;
+                ar += w * b_r[k]; ag += w * b_g[k]; ab += w * b_b[k]; aa += w;
             }
         }
         if (term) { used = cut; break; }
@@ -1644,6 +1671,27 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
         }
         acc_rec += g.l[0] + g.l[1] + g.l[2] + g.l[3];
     }
+    // distortion inputs of chunk c from the buffer (staged by the caller of this lambda)
+    auto dist_from_buffer = [&](uint32_t len, float (&sig)[K], float (&dtn)[K], float (&mm)[K]) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const bool valid = l0 + q < len;
+            const uint32_t k = skew(l0 + q);
+            sig[q] = valid ? act_sigma(S.act, b_sig[k]) : 0.0f;
+            dtn[q] = valid ? b_dtn[k] : 0.0f;
+            mm[q] = valid ? b_m[k] : 0.0f;
+        }
+    };
+    auto stage_dist = [&](uint32_t c) {
+        const size_t c0 = (size_t)o + (size_t)c * RB_MAX;
+        const uint32_t len = chunk_len(c);
+        __syncwarp();
+        stage_segment(b_sig, S.density, c0, len, lane);
+        stage_segment(b_dtn, S.dt_norm, c0, len, lane);
+        stage_segment(b_m, S.m_norm, c0, len, lane);
+        stage_done();
+        return len;
+    };
     // ---- distortion forward over all chunks, keeping each chunk's starting carry
     ScStore store;
     store.s = ScCarry{0.0f, 0.0f, 0.0f, 0.0f};
@@ -1653,9 +1701,9 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
         float uni = 0.0f, cross = 0.0f;
         for (uint32_t ci = 0; ci < nch; ++ci) {
             store.put(ci, lane, c);
-            const uint32_t j0 = ci * RB_MAX + (uint32_t)lane * K;
+            const uint32_t j0 = ci * RB_MAX + l0;
             float sig[K], dtn[K], mm[K], wd[K], tnext[K], dm[K], A[K];
-            sc_load_dist(S, o, j0, n, sig, dtn, mm);
+            dist_from_buffer(stage_dist(ci), sig, dtn, mm);
             ScCarry nx;
             sc_dist_forward(sig, dtn, mm, j0, n, lane, c, wd, tnext, dm, A, nx, uni, cross);
             c = nx;
@@ -1669,28 +1717,59 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
     float sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;  // compositor: sums of w c, w after the chunk
     float sw = 0.0f, sf = 0.0f, sgw = 0.0f;           // distortion suffix sums after the chunk
     for (int ci = (int)nch - 1; ci >= 0; --ci) {
-        const uint32_t j0 = (uint32_t)ci * RB_MAX + (uint32_t)lane * K;
+        const uint32_t j0 = (uint32_t)ci * RB_MAX + l0;
+        const size_t c0 = (size_t)o + (size_t)ci * RB_MAX;
+        const uint32_t len = chunk_len((uint32_t)ci);
+        // chunks beyond 31 replay the distortion forward from chunk 31 (reads straight from memory)
+        ScCarry dc = store.get((uint32_t)ci);
+        if (lambda > 0.0f) {
+            for (uint32_t k = 31u; k < (uint32_t)ci; ++k) {
+                float sig[K], dtn[K], mm[K], wd[K], tnext[K], dm[K], A[K];
+                const uint32_t jk = k * RB_MAX + l0;
+                sc_load_dist(S, o, jk, n, sig, dtn, mm);
+                ScCarry nx;
+                float u0 = 0.0f, c0_ = 0.0f;
+                sc_dist_forward(sig, dtn, mm, jk, n, lane, dc, wd, tnext, dm, A, nx, u0, c0_);
+                dc = nx;
+            }
+        }
+        __syncwarp();
+        stage_segment(b_sig, S.density, c0, len, lane);
+        stage_segment(b_dt, S.dt, c0, len, lane);
+        stage_segment(b_r, S.rgb, c0, len, lane);
+        stage_segment(b_g, S.rgb + ss, c0, len, lane);
+        stage_segment(b_b, S.rgb + 2 * ss, c0, len, lane);
+        if (lambda > 0.0f) {
+            stage_segment(b_dtn, S.dt_norm, c0, len, lane);
+            stage_segment(b_m, S.m_norm, c0, len, lane);
+        }
+        if (S.t) stage_segment(b_t, S.t, c0, len, lane);
+        stage_segment(b_gd, grad_density, c0, len, lane);
+        stage_done();
         float ds[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) ds[q] = 0.0f;
+        float w[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) w[q] = 0.0f;
         if ((uint32_t)ci * RB_MAX < used) {
             float sig[K], dt[K], cr[K], cg[K], cb[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) {
                 const bool valid = j0 + q < used;
-                const size_t s = (size_t)o + j0 + q;
-                sig[q] = valid ? act_sigma(S.act, S.density[s]) : 0.0f;
-                dt[q] = valid ? S.dt[s] : 0.0f;
-                cr[q] = valid ? S.rgb[s] : 0.0f;
-                cg[q] = valid ? S.rgb[s + ss] : 0.0f;
-                cb[q] = valid ? S.rgb[s + 2 * ss] : 0.0f;
+                const uint32_t k = skew(l0 + q);
+                sig[q] = valid ? act_sigma(S.act, b_sig[k]) : 0.0f;
+                dt[q] = valid ? b_dt[k] : 0.0f;
+                cr[q] = valid ? b_r[k] : 0.0f;
+                cg[q] = valid ? b_g[k] : 0.0f;
+                cb[q] = valid ? b_b[k] : 0.0f;
             }
             // T before / after sample j from the optical depth and the suffix sums of x
             float xs[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) xs[q] = sig[q] * dt[q];
             const float xs_after = blk_suffix(xs, lane, sx);
-            float w[K], ta[K], vr[K], vg[K], vb[K], va[K];
+            float ta[K], vr[K], vg[K], vb[K], va[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) {
                 const float xs_ex = q < K - 1 ? xs[q + 1] : xs_after;
@@ -1713,39 +1792,13 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
             sx = __shfl_sync(FULL_MASK, xs[0], 0);
             sr = __shfl_sync(FULL_MASK, vr[0], 0); sg = __shfl_sync(FULL_MASK, vg[0], 0);
             sb = __shfl_sync(FULL_MASK, vb[0], 0); sa = __shfl_sync(FULL_MASK, va[0], 0);
-#pragma unroll
-            for (int q = 0; q < K; ++q) {
-                if (j0 + q < n) {
-                    const size_t s = (size_t)o + j0 + q;
-                    drgb[s] = grad_scale * g.gr * w[q];
-                    drgb[s + ss] = grad_scale * g.gg * w[q];
-                    drgb[s + 2 * ss] = grad_scale * g.gb * w[q];
-                }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < K; ++q) {
-                if (j0 + q < n) {
-                    const size_t s = (size_t)o + j0 + q;
-                    drgb[s] = 0.0f; drgb[s + ss] = 0.0f; drgb[s + 2 * ss] = 0.0f;
-                }
-            }
         }
         if (lambda > 0.0f) {
-            ScCarry c = store.get((uint32_t)ci);
             float sig[K], dtn[K], mm[K], wd[K], tnext[K], dm[K], A[K];
-            for (uint32_t k = 31u; k < (uint32_t)ci; ++k) {  // chunks beyond 31: replay from chunk 31
-                const uint32_t jk = k * RB_MAX + (uint32_t)lane * K;
-                sc_load_dist(S, o, jk, n, sig, dtn, mm);
-                ScCarry nx;
-                float u0 = 0.0f, c0 = 0.0f;
-                sc_dist_forward(sig, dtn, mm, jk, n, lane, c, wd, tnext, dm, A, nx, u0, c0);
-                c = nx;
-            }
-            sc_load_dist(S, o, j0, n, sig, dtn, mm);
+            dist_from_buffer(len, sig, dtn, mm);
             ScCarry nx;
-            float u0 = 0.0f, c0 = 0.0f;
-            sc_dist_forward(sig, dtn, mm, j0, n, lane, c, wd, tnext, dm, A, nx, u0, c0);
+            float u0 = 0.0f, c0_ = 0.0f;
+            sc_dist_forward(sig, dtn, mm, j0, n, lane, dc, wd, tnext, dm, A, nx, u0, c0_);
             float Wge[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) Wge[q] = wd[q];
@@ -1771,16 +1824,25 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
             sf = __shfl_sync(FULL_MASK, f[0], 0);
             sgw = __shfl_sync(FULL_MASK, gw[0], 0);
         }
+        // outputs through the buffer: dL/drgb (zero past the cut) and the merged density gradient
+        __syncwarp();  // every lane has read the chunk's inputs
 #pragma unroll
         for (int q = 0; q < K; ++q) {
-            const uint32_t j = j0 + q;
-            if (j < n) {
-                const size_t s = (size_t)o + j;
-                float gd = grad_density[s] + ds[q];
-                if (S.t) { const float tt = S.t[s]; if (tt < 1.0f) gd *= tt * tt; }
-                grad_density[s] = gd;
+            if (l0 + q < len) {
+                const uint32_t k = skew(l0 + q);
+                b_r[k] = grad_scale * g.gr * w[q];
+                b_g[k] = grad_scale * g.gg * w[q];
+                b_b[k] = grad_scale * g.gb * w[q];
+                float gd = b_gd[k] + ds[q];
+                if (S.t) { const float tt = b_t[k]; if (tt < 1.0f) gd *= tt * tt; }
+                b_gd[k] = gd;
             }
         }
+        __syncwarp();
+        store_segment(grad_density, b_gd, c0, len, lane);
+        store_segment(drgb, b_r, c0, len, lane);
+        store_segment(drgb + ss, b_g, c0, len, lane);
+        store_segment(drgb + 2 * ss, b_b, c0, len, lane);
     }
 }
 
@@ -1811,7 +1873,7 @@ train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t 
                                      grad_density, drgb, acc[0], acc[1], stage + (size_t)wid * SA_N * RB_SKEW);
         else
             train_losses_ray_long(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
-                                  grad_density, drgb, acc[0], acc[1]);
+                                  grad_density, drgb, acc[0], acc[1], stage + (size_t)wid * SA_N * RB_SKEW);
     }
     if (loss_sums) {
         acc[0] *= inv_nrays;

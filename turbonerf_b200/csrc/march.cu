@@ -446,8 +446,11 @@ __device__ uint32_t count_ray_loop(const MarchArgs& a, const CountGrid& cg, cons
     const uint32_t res = 1u << cg.res_shift;
     uint32_t n = 0, iters = 0;
     float t = r.t;
-    while (t <= t_lim) {
-        if (++iters > a.max_iters) { raise_flag(flags, ERR_GUARD); break; }
+    // the iteration guard is part of the loop condition (no branch with a side effect in the
+    // body, which stays one straight block); the flag is raised after the loop
+    const uint32_t max_iters = a.max_iters;
+    while ((t <= t_lim) & (iters < max_iters)) {
+        ++iters;
         float x, y, z;
         ray_point(r, t, x, y, z);
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
@@ -483,6 +486,7 @@ __device__ uint32_t count_ray_loop(const MarchArgs& a, const CountGrid& cg, cons
         n += occ ? 1u : 0u;
         if (LIMIT && n >= max_steps) break;
     }
+    if (iters >= max_iters && t <= t_lim && !(LIMIT && n >= max_steps)) raise_flag(flags, ERR_GUARD);
     return n;
 }
 
