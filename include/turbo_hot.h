@@ -449,7 +449,8 @@ typedef struct tn_network {
     int activation; /* TN_ACT_SIGMA or TN_ACT_DENSITY: what `forward` writes into density */
     int (*forward)(void* user, tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t stride,
                    const float* pos, const float* dir, float* density, float* rgb);
-    /* dL/d density (merged, scaled) and dL/d rgb -> parameter gradients; may be NULL */
+    /* dL/d density (merged, scaled) and dL/d rgb -> parameter gradients; may be NULL. Both
+     * hold the n_dev live samples; entries past them are unspecified. */
     int (*backward)(void* user, tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32_t stride,
                     const float* pos, const float* dir, const float* dL_ddensity, const float* dL_drgb,
                     float* param_grads);

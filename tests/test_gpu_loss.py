@@ -148,15 +148,19 @@ def test_distortion_fused_and_plain(mean, n_samples, max_count):
     assert ctx.check() == 0
 
 
-@pytest.mark.parametrize("mean,max_count,n_samples,sigma_scale", [
-    (48, 1024, 1 << 18, 1.0),      # the training mix: most rays in registers, a few long ones
-    (700, 1024, 1 << 16, 1.0),     # rays of 2-4 super-chunks, cut early by the transmittance
-    (700, 1024, 1 << 16, 1e-3),    # long composites that cross super-chunks
-    (6000, 9000, 1 << 16, 1e-4),   # rays beyond 32 super-chunks (distortion carries replayed)
+@pytest.mark.parametrize("mean,max_count,n_samples,sigma_scale,shift", [
+    (48, 1024, 1 << 18, 1.0, 0),      # the training mix: most rays in registers, a few long ones
+    (48, 1024, 1 << 18, 1.0, 1),      # the same with sigma 4 bytes off 16-byte alignment: scalar staging
+    (178, 256, 1 << 18, 1.0, 0),      # the train step's mix: rays up to 256 samples at any offset mod 4
+    (700, 1024, 1 << 16, 1.0, 0),     # rays of 2-4 super-chunks, cut early by the transmittance
+    (700, 1024, 1 << 16, 1e-3, 0),    # long composites that cross super-chunks
+    (6000, 9000, 1 << 16, 1e-4, 0),   # rays beyond 32 super-chunks (distortion carries replayed)
 ])
-def test_train_losses_fused_matches_oracle_chain(mean, max_count, n_samples, sigma_scale):
+def test_train_losses_fused_matches_oracle_chain(mean, max_count, n_samples, sigma_scale, shift):
     """One kernel = reconstruction fwd/bwd + distortion fwd/bwd + gradient merge with
-    distance scaling, against the oracle's separate stages."""
+    distance scaling, against the oracle's separate stages. With every sample array 16-byte
+    aligned (shift 0) the kernel stages whole 16-byte groups; a shifted sigma array takes the
+    sample-by-sample staging."""
     from turbonerf_b200 import hotpath as hp
     sb = scenes.make_sample_batch(0x7B4, n_samples, mean=mean, max_count=max_count)
     sb.sigma = (sb.sigma * np.float32(sigma_scale)).astype(np.float32)
@@ -169,7 +173,8 @@ def test_train_losses_fused_matches_oracle_chain(mean, max_count, n_samples, sig
     rb = _rb(sb, counts, offsets)
     gd = dev(grad_in.copy())
     ray_rgba = dev(np.zeros(4 * n, np.float32))
-    gd, drgb, sums = hp.train_losses(ctx, rb, dev(sb.sigma), dev(sb.rgb), dev(sb.dt), dev(sb.m_norm), dev(sb.dt_norm),
+    sig_d = dev(np.concatenate([np.zeros(shift, np.float32), sb.sigma]))[shift:]
+    gd, drgb, sums = hp.train_losses(ctx, rb, sig_d, dev(sb.rgb), dev(sb.dt), dev(sb.m_norm), dev(sb.dt_norm),
                                      dev(t_world), dev(sb.target_rgba), dev(sb.bg_rgb), gd, inv_nrays=1.0 / n,
                                      grad_scale=scale, lam=lam, ray_rgba=ray_rgba)
     dl, ddist = oracle.distortion_fwd_bwd(sb.counts, sb.offsets, sb.sigma, sb.m_norm, sb.dt_norm, lam, ss)

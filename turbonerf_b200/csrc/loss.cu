@@ -1257,18 +1257,29 @@ __device__ __forceinline__ float blk_suffix(float (&v)[K], int lane, float carry
 }
 
 // ---- shared-memory staging of one ray's samples ----------------------------------------
-// Each input array of the ray is copied with cp.async (coalesced, one sample per lane per
-// step) into a per-warp buffer, all of them before a single wait, so the ray pays one memory
-// latency. Sample j sits at j + j/32: lane l then reads its consecutive samples 8l..8l+7
-// without bank conflicts. Results go back through the same buffers with coalesced stores.
-constexpr int RB_SKEW = RB_MAX + RB_MAX / WARP;
+// Each input array of the ray is copied with cp.async into a per-warp buffer, all of them before
+// a single wait, so the ray pays one memory latency; results go back through the same buffers
+// with coalesced stores. A buffer array holds RB_PITCH floats. Rays of at most RB_MAX samples use
+// the slot layout: slot i at i + 4 (i / 32), so that every 16-byte group of slots (4c .. 4c + 3)
+// stays whole and aligned, and lane l reads its slots 8l .. 8l + 7 as two 16-byte loads without
+// bank conflicts (8 consecutive lanes cover the 32 banks). With 16-byte staging the ray's first
+// sample sits in slot o mod 4 (o its first sample in the batch), so that the copies are whole
+// aligned groups. The chunks of longer rays use the layout j + j / 32 (one sample per lane
+// per copy).
+constexpr int RB_PITCH = RB_MAX + RB_MAX / WARP * 4;
 enum StageArray : int { SA_SIG = 0, SA_DT, SA_R, SA_G, SA_B, SA_DTN, SA_M, SA_T, SA_GD, SA_N };
-constexpr size_t TL_STAGE_BYTES = (size_t)SA_N * RB_SKEW * sizeof(float);  // one warp's staging buffer
+constexpr size_t TL_STAGE_BYTES = (size_t)SA_N * RB_PITCH * sizeof(float);  // one warp's staging buffer
 
 __device__ __forceinline__ uint32_t skew(uint32_t j) { return j + (j >> 5); }
+__device__ __forceinline__ uint32_t slot4(uint32_t i) { return i + ((i >> 5) << 2); }
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
@@ -1283,60 +1294,141 @@ __device__ __forceinline__ void store_segment(float* __restrict__ dst, const flo
     for (uint32_t j = (uint32_t)lane; j < n; j += WARP) dst[o + j] = buf[skew(j)];
 }
 
-// One ray of the fused training losses (the same quantities as the chunked path below, with
-// the compositor's transmittance and weights kept from its forward instead of recomputed):
+// Samples [o, o + n) of src into the slots from e: with VEC the whole 16-byte groups of
+// [o - e, o + n) (e = o mod 4; src 16-byte aligned), else one sample per copy (e = 0).
+template <bool VEC>
+__device__ __forceinline__ void stage_slots(float* buf, const float* __restrict__ src, uint32_t o, uint32_t e,
+                                            uint32_t n, int lane) {
+    if (VEC) {
+        const uint32_t groups = (e + n + 3u) >> 2;
+        const float* base = src + (o - e);
+        for (uint32_t c = (uint32_t)lane; c < groups; c += WARP) cp_async16(buf + slot4(4u * c), base + 4u * c);
+    } else {
+        for (uint32_t j = (uint32_t)lane; j < n; j += WARP) cp_async4(buf + slot4(j), src + o + j);
+    }
+}
+
+// Slots [e, e + n) back to dst[o, o + n): whole 16-byte groups in one store, the ray's partial
+// first and last groups sample by sample (their other samples belong to neighbouring rays).
+template <bool VEC>
+__device__ __forceinline__ void store_slots(float* __restrict__ dst, const float* buf, uint32_t o, uint32_t e,
+                                            uint32_t n, int lane) {
+    if (VEC) {
+        const uint32_t groups = (e + n + 3u) >> 2, end = e + n;
+        float* base = dst + (o - e);
+        for (uint32_t c = (uint32_t)lane; c < groups; c += WARP) {
+            const uint32_t i = 4u * c;
+            const float4 v = *reinterpret_cast<const float4*>(buf + slot4(i));
+            if (i >= e && i + 4u <= end) {
+                *reinterpret_cast<float4*>(base + i) = v;
+            } else {
+                if (i >= e && i < end) base[i] = v.x;
+                if (i + 1u >= e && i + 1u < end) base[i + 1u] = v.y;
+                if (i + 2u >= e && i + 2u < end) base[i + 2u] = v.z;
+                if (i + 3u >= e && i + 3u < end) base[i + 3u] = v.w;
+            }
+        }
+    } else {
+        for (uint32_t j = (uint32_t)lane; j < n; j += WARP) dst[o + j] = buf[slot4(j)];
+    }
+}
+
+// The lane's K slots K lane .. K lane + K - 1 (K a multiple of 4).
+template <int K>
+__device__ __forceinline__ void read_slots(const float* buf, int lane, float (&v)[K]) {
+    const float4* p = reinterpret_cast<const float4*>(buf + slot4((uint32_t)(K * lane)));
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c) {
+        const float4 a = p[c];
+        v[4 * c] = a.x; v[4 * c + 1] = a.y; v[4 * c + 2] = a.z; v[4 * c + 3] = a.w;
+    }
+}
+template <int K>
+__device__ __forceinline__ void write_slots(float* buf, int lane, const float (&v)[K]) {
+    float4* p = reinterpret_cast<float4*>(buf + slot4((uint32_t)(K * lane)));
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c) p[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+}
+
+// e^-x for the transmittances and opacities of the fused loss kernel: the fast intrinsic, whose
+// relative error at the optical depths that matter here (x below about 20) is a few 1e-6.
+__device__ __forceinline__ float exp_neg(float x) { return __expf(-x); }
+
+// opacity(x) without a branch (both forms evaluated, one selected), from exp_neg.
+__device__ __forceinline__ float opacity_nb(float x) {
+    float p = fmaf(-x, 1.0f / 7.0f, 1.0f);
+    p = fmaf(-x * (1.0f / 6.0f), p, 1.0f);
+    p = fmaf(-x * (1.0f / 5.0f), p, 1.0f);
+    p = fmaf(-x * (1.0f / 4.0f), p, 1.0f);
+    p = fmaf(-x * (1.0f / 3.0f), p, 1.0f);
+    p = fmaf(-x * 0.5f, p, 1.0f);
+    const float big = 1.0f - exp_neg(x);
+    return x < 0.25f ? x * p : big;
+}
+
+// One ray of at most 32 K samples (32 K - o mod 4 with VEC) of the fused training losses, in
+// the slot layout, with the compositor's transmittance and weights kept from its forward:
 // compositor forward (training-kernels-fused.cuh:227-264), reconstruction loss (:434-477),
 // compositor VJP (:269-341), distortion forward/backward in the non-cancelling form above, and
 // the gradient merge with the distance scaling (nerf-network.cu:734-758). `sm` is the warp's
-// staging buffer, SA_N arrays of RB_SKEW floats.
+// staging buffer, SA_N arrays of RB_PITCH floats. Lane l owns the slots K l .. K l + K - 1,
+// sample j = slot - e; slots outside the ray read as zero (their staged values belong to other
+// rays). `accumulate`: the merged gradient is added to grad_density (else written over it).
+template <bool VEC, int K>
 __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint32_t r, uint32_t o, uint32_t n,
                                                          int lane, float min_t, float inv_nrays, float grad_scale,
                                                          float lambda, const float* __restrict__ target,
                                                          const float* __restrict__ bg, uint32_t rs,
                                                          float* __restrict__ ray_rgba,
                                                          float* __restrict__ grad_density, float* __restrict__ drgb,
-                                                         float& acc_rec, float& acc_dist, float* sm) {
-    constexpr int K = RB_SPL;
-    const uint32_t j0 = (uint32_t)lane * K;
+                                                         float& acc_rec, float& acc_dist, float* sm, bool accumulate) {
+    static_assert(K % 4 == 0 && K <= RB_SPL, "slots are read in 16-byte groups");
+    const uint32_t e = VEC ? (o & 3u) : 0u;
+    const uint32_t j0 = (uint32_t)lane * K - e;  // sample of the lane's first slot (wraps below the ray)
     const size_t ss = S.ss;
-    float* const b_sig = sm + SA_SIG * RB_SKEW;
-    float* const b_dt = sm + SA_DT * RB_SKEW;
-    float* const b_r = sm + SA_R * RB_SKEW;
-    float* const b_g = sm + SA_G * RB_SKEW;
-    float* const b_b = sm + SA_B * RB_SKEW;
-    float* const b_dtn = sm + SA_DTN * RB_SKEW;
-    float* const b_m = sm + SA_M * RB_SKEW;
-    float* const b_t = sm + SA_T * RB_SKEW;
-    float* const b_gd = sm + SA_GD * RB_SKEW;
+    float* const b_sig = sm + SA_SIG * RB_PITCH;
+    float* const b_dt = sm + SA_DT * RB_PITCH;
+    float* const b_r = sm + SA_R * RB_PITCH;
+    float* const b_g = sm + SA_G * RB_PITCH;
+    float* const b_b = sm + SA_B * RB_PITCH;
+    float* const b_dtn = sm + SA_DTN * RB_PITCH;
+    float* const b_m = sm + SA_M * RB_PITCH;
+    float* const b_t = sm + SA_T * RB_PITCH;
+    float* const b_gd = sm + SA_GD * RB_PITCH;
     // every input of the ray in flight at once; the per-ray inputs of the loss meanwhile
     __syncwarp();  // the previous ray's write-back reads of the buffers are done
-    stage_segment(b_sig, S.density, o, n, lane);
-    stage_segment(b_dt, S.dt, o, n, lane);
-    stage_segment(b_r, S.rgb, o, n, lane);
-    stage_segment(b_g, S.rgb + ss, o, n, lane);
-    stage_segment(b_b, S.rgb + 2 * ss, o, n, lane);
+    stage_slots<VEC>(b_sig, S.density, o, e, n, lane);
+    stage_slots<VEC>(b_dt, S.dt, o, e, n, lane);
+    stage_slots<VEC>(b_r, S.rgb, o, e, n, lane);
+    stage_slots<VEC>(b_g, S.rgb + ss, o, e, n, lane);
+    stage_slots<VEC>(b_b, S.rgb + 2 * ss, o, e, n, lane);
     if (lambda > 0.0f) {
-        stage_segment(b_dtn, S.dt_norm, o, n, lane);
-        stage_segment(b_m, S.m_norm, o, n, lane);
+        stage_slots<VEC>(b_dtn, S.dt_norm, o, e, n, lane);
+        stage_slots<VEC>(b_m, S.m_norm, o, e, n, lane);
     }
-    if (S.t) stage_segment(b_t, S.t, o, n, lane);
-    stage_segment(b_gd, grad_density, o, n, lane);
+    if (S.t) stage_slots<VEC>(b_t, S.t, o, e, n, lane);
+    if (accumulate) stage_slots<VEC>(b_gd, grad_density, o, e, n, lane);
     const float gt_r = target[r], gt_g = target[r + rs], gt_b = target[r + 2 * (size_t)rs];
     const float gt_a = target[r + 3 * (size_t)rs];
     const float bg_r = bg[r], bg_g = bg[r + rs], bg_b = bg[r + 2 * (size_t)rs];
     cp_async_wait_all();
     __syncwarp();
+    bool valid[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) valid[q] = j0 + q < n;
     float sig[K], dt[K], cr[K], cg[K], cb[K];
+    read_slots(b_sig, lane, sig);
+    read_slots(b_dt, lane, dt);
+    read_slots(b_r, lane, cr);
+    read_slots(b_g, lane, cg);
+    read_slots(b_b, lane, cb);
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-        const uint32_t j = j0 + q;
-        const bool valid = j < n;
-        const uint32_t k = skew(j);
-        sig[q] = valid ? act_sigma(S.act, b_sig[k]) : 0.0f;
-        dt[q] = valid ? b_dt[k] : 0.0f;
-        cr[q] = valid ? b_r[k] : 0.0f;
-        cg[q] = valid ? b_g[k] : 0.0f;
-        cb[q] = valid ? b_b[k] : 0.0f;
+        sig[q] = valid[q] ? act_sigma(S.act, sig[q]) : 0.0f;
+        dt[q] = valid[q] ? dt[q] : 0.0f;
+        cr[q] = valid[q] ? cr[q] : 0.0f;
+        cg[q] = valid[q] ? cg[q] : 0.0f;
+        cb[q] = valid[q] ? cb[q] : 0.0f;
     }
     // ---- compositor forward: T after each sample, weights, the transmittance cut
     float T[K], w[K];
@@ -1348,20 +1440,19 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
         for (int q = 0; q < K; ++q) p[q] = sig[q] * dt[q];
         blk_prefix(p, lane);
 #pragma unroll
-        for (int q = 0; q < K; ++q) T[q] = expf(-p[q]);
+        for (int q = 0; q < K; ++q) T[q] = exp_neg(p[q]);
         const float t_in = shift_up(T[K - 1], lane, 1.0f);
         int first_q = K;
         float cut_depth = 0.0f;
 #pragma unroll
         for (int q = K - 1; q >= 0; --q) {
-            const float x = sig[q] * dt[q];
-            w[q] = (q ? T[q - 1] : t_in) * -expm1f(-x);
-            if (j0 + q < n && T[q] < min_t) { first_q = q; cut_depth = p[q]; }
+            w[q] = (q ? T[q - 1] : t_in) * opacity_nb(sig[q] * dt[q]);
+            if (valid[q] && T[q] < min_t) { first_q = q; cut_depth = p[q]; }
         }
         const unsigned term = __ballot_sync(FULL_MASK, first_q < K);
         if (term) {
             const int fl = __ffs(term) - 1;
-            used = (uint32_t)fl * K + (uint32_t)__shfl_sync(FULL_MASK, first_q, fl) + 1u;
+            used = (uint32_t)fl * K + (uint32_t)__shfl_sync(FULL_MASK, first_q, fl) + 1u - e;
             depth = __shfl_sync(FULL_MASK, cut_depth, fl);
         } else {
             depth = __shfl_sync(FULL_MASK, p[K - 1], WARP - 1);
@@ -1370,7 +1461,7 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
     float ar = 0.0f, ag = 0.0f, ab = 0.0f, aa = 0.0f;
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-        if (j0 + q >= used) w[q] = 0.0f;
+        w[q] = j0 + q < used ? w[q] : 0.0f;
         ar += w[q] * cr[q];
         ag += w[q] * cg[q];
         ab += w[q] * cb[q];
@@ -1400,57 +1491,54 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
             su[q] = w[q] * cu[q];
         }
         const float su_after = blk_suffix(su, lane);
+        float dr[K], dg[K], db[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) {
-            const uint32_t j = j0 + q;
             const float u_ex = q < K - 1 ? su[q + 1] : su_after;
             const float d = dt[q] * (T[q] * cu[q] - u_ex);
-            ds[q] = j < used ? grad_scale * d * act_dsigma(S.act, sig[q]) : 0.0f;
-            if (j < n) {
-                const uint32_t k = skew(j);
-                b_r[k] = grad_scale * g.gr * w[q];
-                b_g[k] = grad_scale * g.gg * w[q];
-                b_b[k] = grad_scale * g.gb * w[q];
-            }
+            ds[q] = j0 + q < used ? grad_scale * d * act_dsigma(S.act, sig[q]) : 0.0f;
+            dr[q] = grad_scale * g.gr * w[q];
+            dg[q] = grad_scale * g.gg * w[q];
+            db[q] = grad_scale * g.gb * w[q];
         }
+        write_slots(b_r, lane, dr);
+        write_slots(b_g, lane, dg);
+        write_slots(b_b, lane, db);
     }
     // ---- distortion forward and backward (all n samples, no transmittance cut)
     if (lambda > 0.0f) {
         float dtn[K], mm[K];
+        read_slots(b_dtn, lane, dtn);
+        read_slots(b_m, lane, mm);
 #pragma unroll
         for (int q = 0; q < K; ++q) {
-            const uint32_t j = j0 + q;
-            const bool valid = j < n;
-            dtn[q] = valid ? b_dtn[skew(j)] : 0.0f;
-            mm[q] = valid ? b_m[skew(j)] : 0.0f;
+            dtn[q] = valid[q] ? dtn[q] : 0.0f;
+            mm[q] = valid[q] ? mm[q] : 0.0f;
         }
         float wd[K], tnext[K], dm[K], A[K];
         {
             float p[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) p[q] = sig[q] * dtn[q];
-            const float before = blk_prefix(p, lane);
+            blk_prefix(p, lane);
 #pragma unroll
-            for (int q = 0; q < K; ++q) {
-                const float x = sig[q] * dtn[q];
-                const float em = expm1f(-x);
-                const float tj = expf(-(q ? p[q - 1] : before));
-                wd[q] = j0 + q < n ? tj * -em : 0.0f;
-                tnext[q] = expf(-p[q]);  // T_{j+1}; T_j (1 + em) cancels once e^-x is small
-            }
+            for (int q = 0; q < K; ++q) tnext[q] = exp_neg(p[q]);  // T_{j+1}
+            const float t_in = shift_up(tnext[K - 1], lane, 1.0f);
+#pragma unroll
+            for (int q = 0; q < K; ++q)
+                wd[q] = valid[q] ? (q ? tnext[q - 1] : t_in) * opacity_nb(sig[q] * dtn[q]) : 0.0f;
         }
         {
             float W[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) W[q] = wd[q];
             const float w_before = blk_prefix(W, lane);
-            // m of the previous sample; the first sample's predecessor is itself (zero increment)
+            // m of the previous sample; the first sample has no increment
             const float m_in = __shfl_up_sync(FULL_MASK, mm[K - 1], 1);
-            const float m0 = __shfl_sync(FULL_MASK, mm[0], 0);
 #pragma unroll
             for (int q = 0; q < K; ++q) {
-                const float m_prev = q ? mm[q - 1] : (lane ? m_in : m0);
-                dm[q] = j0 + q < n ? fmaxf(mm[q] - m_prev, 0.0f) : 0.0f;
+                const float m_prev = q ? mm[q - 1] : m_in;
+                dm[q] = valid[q] && j0 + q != 0u ? fmaxf(mm[q] - m_prev, 0.0f) : 0.0f;
                 A[q] = dm[q] * (q ? W[q - 1] : w_before);
             }
             blk_prefix(A, lane);
@@ -1481,25 +1569,33 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             const float gw_ex = q < K - 1 ? gw[q + 1] : gw_after;
-            if (j0 + q < n) ds[q] += grad_scale * dtn[q] * (gq[q] * tnext[q] - gw_ex) * act_dsigma(S.act, sig[q]);
+            const float dd = grad_scale * dtn[q] * (gq[q] * tnext[q] - gw_ex) * act_dsigma(S.act, sig[q]);
+            ds[q] += valid[q] ? dd : 0.0f;
         }
     }
     // ---- gradient merge: copy_gradients_kernel<1,true> twice + apply_gradient_distance_scaling_kernel
+    {
+        float gd[K], tt[K];
+        if (accumulate) {
+            read_slots(b_gd, lane, gd);
+        } else {
 #pragma unroll
-    for (int q = 0; q < K; ++q) {
-        const uint32_t j = j0 + q;
-        if (j < n) {
-            const uint32_t k = skew(j);
-            float gd = b_gd[k] + ds[q];
-            if (S.t) { const float tt = b_t[k]; if (tt < 1.0f) gd *= tt * tt; }
-            b_gd[k] = gd;
+            for (int q = 0; q < K; ++q) gd[q] = 0.0f;
         }
+        if (S.t) read_slots(b_t, lane, tt);
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            float v = gd[q] + ds[q];
+            if (S.t) v = tt[q] < 1.0f ? v * (tt[q] * tt[q]) : v;
+            gd[q] = v;
+        }
+        write_slots(b_gd, lane, gd);
     }
     __syncwarp();
-    store_segment(grad_density, b_gd, o, n, lane);
-    store_segment(drgb, b_r, o, n, lane);
-    store_segment(drgb + ss, b_g, o, n, lane);
-    store_segment(drgb + 2 * ss, b_b, o, n, lane);
+    store_slots<VEC>(grad_density, b_gd, o, e, n, lane);
+    store_slots<VEC>(drgb, b_r, o, e, n, lane);
+    store_slots<VEC>(drgb + ss, b_g, o, e, n, lane);
+    store_slots<VEC>(drgb + 2 * ss, b_b, o, e, n, lane);
 }
 
 // Rays longer than RB_MAX: the same computation over super-chunks of RB_MAX samples in the
@@ -1587,20 +1683,21 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
                                                    const float* __restrict__ target, const float* __restrict__ bg,
                                                    uint32_t rs, float* __restrict__ ray_rgba,
                                                    float* __restrict__ grad_density, float* __restrict__ drgb,
-                                                   float& acc_rec, float& acc_dist, float* sm) {
+                                                   float& acc_rec, float& acc_dist, float* sm,
+                                                   bool accumulate) {
     constexpr int K = RB_SPL;
     const size_t ss = S.ss;
     const uint32_t nch = (n + RB_MAX - 1) / RB_MAX;
     const uint32_t l0 = (uint32_t)lane * K;  // the lane's first sample inside a chunk
-    float* const b_sig = sm + SA_SIG * RB_SKEW;
-    float* const b_dt = sm + SA_DT * RB_SKEW;
-    float* const b_r = sm + SA_R * RB_SKEW;
-    float* const b_g = sm + SA_G * RB_SKEW;
-    float* const b_b = sm + SA_B * RB_SKEW;
-    float* const b_dtn = sm + SA_DTN * RB_SKEW;
-    float* const b_m = sm + SA_M * RB_SKEW;
-    float* const b_t = sm + SA_T * RB_SKEW;
-    float* const b_gd = sm + SA_GD * RB_SKEW;
+    float* const b_sig = sm + SA_SIG * RB_PITCH;
+    float* const b_dt = sm + SA_DT * RB_PITCH;
+    float* const b_r = sm + SA_R * RB_PITCH;
+    float* const b_g = sm + SA_G * RB_PITCH;
+    float* const b_b = sm + SA_B * RB_PITCH;
+    float* const b_dtn = sm + SA_DTN * RB_PITCH;
+    float* const b_m = sm + SA_M * RB_PITCH;
+    float* const b_t = sm + SA_T * RB_PITCH;
+    float* const b_gd = sm + SA_GD * RB_PITCH;
     // Each pass stages a chunk's inputs into the warp's buffer (one round trip to memory) and
     // reads them from there; the chunk's samples are [c0, c0 + len).
     auto chunk_len = [&](uint32_t c) { return min(RB_MAX, n - c * RB_MAX); };
@@ -1744,7 +1841,7 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
             stage_segment(b_m, S.m_norm, c0, len, lane);
         }
         if (S.t) stage_segment(b_t, S.t, c0, len, lane);
-        stage_segment(b_gd, grad_density, c0, len, lane);
+        if (accumulate) stage_segment(b_gd, grad_density, c0, len, lane);
         stage_done();
         float ds[K];
 #pragma unroll
@@ -1833,7 +1930,7 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
                 b_r[k] = grad_scale * g.gr * w[q];
                 b_g[k] = grad_scale * g.gg * w[q];
                 b_b[k] = grad_scale * g.gb * w[q];
-                float gd = b_gd[k] + ds[q];
+                float gd = (accumulate ? b_gd[k] : 0.0f) + ds[q];
                 if (S.t) { const float tt = b_t[k]; if (tt < 1.0f) gd *= tt * tt; }
                 b_gd[k] = gd;
             }
@@ -1847,17 +1944,18 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
 }
 
 // Reconstruction + distortion forward/backward + gradient merge, one warp per ray with its own
-// staging buffer (dynamic shared memory, 9.3 KB a warp); W warps a block (tn_tuning
+// staging buffer (dynamic shared memory, 10.1 KB a warp); W warps a block (tn_tuning
 // loss_rays_per_block: 2, 4 or 8) and 16 / W blocks an SM (128 registers a thread) keep 16 rays
-// in flight per SM.
-template <int W>
+// in flight per SM. VEC: 16-byte staging (every sample array 16-byte aligned, stride a multiple
+// of 4).
+template <int W, bool VEC>
 __global__ void __launch_bounds__(W * WARP, 16 / W)
 train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
                     const uint32_t* __restrict__ offsets, float min_t, float inv_nrays_host,
                     const uint32_t* __restrict__ inv_from, float grad_scale, float lambda,
                     const float* __restrict__ target, const float* __restrict__ bg, float* __restrict__ ray_rgba,
                     float* __restrict__ grad_density, float* __restrict__ drgb, float* loss_sums, float* partials,
-                    uint32_t* ticket) {
+                    uint32_t* ticket, bool accumulate) {
     extern __shared__ __align__(16) float stage[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_live = live_rays(n_rays, n_dev);
@@ -1866,14 +1964,16 @@ train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t 
     const uint32_t nw = gridDim.x * W;
     const float lam = lambda > 0.0f ? lambda : 0.0f;
     float acc[2] = {0.0f, 0.0f};
+    float* const sm = stage + (size_t)wid * SA_N * RB_PITCH;
     for (uint32_t r = blockIdx.x * W + wid; r < n_live; r += nw) {
         const uint32_t o = offsets[r], n = counts[r];
-        if (n <= RB_MAX)
-            train_losses_ray_blocked(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
-                                     grad_density, drgb, acc[0], acc[1], stage + (size_t)wid * SA_N * RB_SKEW);
+        const uint32_t span = n + (VEC ? (o & 3u) : 0u);  // slots the ray takes
+        if (span <= RB_MAX)
+            train_losses_ray_blocked<VEC, RB_SPL>(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs,
+                                                  ray_rgba, grad_density, drgb, acc[0], acc[1], sm, accumulate);
         else
             train_losses_ray_long(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
-                                  grad_density, drgb, acc[0], acc[1], stage + (size_t)wid * SA_N * RB_SKEW);
+                                  grad_density, drgb, acc[0], acc[1], sm, accumulate);
     }
     if (loss_sums) {
         acc[0] *= inv_nrays;
@@ -2059,25 +2159,40 @@ static int loss_grid(const void* kernel, uint32_t n_rays, int threads = LOSS_THR
     return (int)max(1u, min(want, cap));
 }
 
+template <int W, bool VEC>
+static int launch_train_losses_v(tn_ctx* ctx, cudaStream_t stream, const tn_ray_batch* batch, const Samples& S,
+                                 float min_t, float inv_nrays, const uint32_t* inv_from, float grad_scale,
+                                 float lambda, const float* target, const float* bg, float* ray_rgba,
+                                 float* grad_density, float* drgb, float* loss_sums, bool accumulate) {
+    const size_t smem = W * TL_STAGE_BYTES;
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        cudaFuncSetAttribute(train_losses_kernel<W, VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
+    const int grid = loss_grid((const void*)train_losses_kernel<W, VEC>, batch->n_rays, W * WARP, smem);
+    int st = ensure_block_f32(ctx, (size_t)grid * 2);
+    if (st != TN_OK) return st;
+    train_losses_kernel<W, VEC><<<grid, W * WARP, smem, stream>>>(
+        S, batch->n_rays, batch->n_rays_dev, batch->ray_stride, batch->counts, batch->offsets, min_t, inv_nrays,
+        inv_from, grad_scale, lambda, target, bg, ray_rgba, grad_density, drgb, loss_sums, ctx->block_f32,
+        ctx->tickets + TICKET_TRAIN, accumulate);
+    return check_launch("tn_train_losses");
+}
+
+// 16-byte staging when every per-sample array the kernel reads or writes is 16-byte aligned and
+// the sample stride is a multiple of 4 (then no 16-byte group of a ray reaches past the arrays).
 template <int W>
 static int launch_train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_batch* batch, const Samples& S,
                                float min_t, float inv_nrays, const uint32_t* inv_from, float grad_scale, float lambda,
                                const float* target, const float* bg, float* ray_rgba, float* grad_density,
-                               float* drgb, float* loss_sums) {
-    const size_t smem = W * TL_STAGE_BYTES;
-    static std::once_flag once;
-    std::call_once(once, [&] {
-        cudaFuncSetAttribute(train_losses_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    });
-    const int grid = loss_grid((const void*)train_losses_kernel<W>, batch->n_rays, W * WARP, smem);
-    int st = ensure_block_f32(ctx, (size_t)grid * 2);
-    if (st != TN_OK) return st;
-    train_losses_kernel<W><<<grid, W * WARP, smem, stream>>>(S, batch->n_rays, batch->n_rays_dev, batch->ray_stride,
-                                                              batch->counts, batch->offsets, min_t, inv_nrays,
-                                                              inv_from, grad_scale, lambda, target, bg, ray_rgba,
-                                                              grad_density, drgb, loss_sums, ctx->block_f32,
-                                                              ctx->tickets + TICKET_TRAIN);
-    return check_launch("tn_train_losses");
+                               float* drgb, float* loss_sums, bool accumulate) {
+    const uintptr_t m = (uintptr_t)S.density | (uintptr_t)S.rgb | (uintptr_t)S.dt | (uintptr_t)S.m_norm |
+                        (uintptr_t)S.dt_norm | (uintptr_t)S.t | (uintptr_t)grad_density | (uintptr_t)drgb;
+    if ((m & 15u) == 0 && (S.ss & 3u) == 0)
+        return launch_train_losses_v<W, true>(ctx, stream, batch, S, min_t, inv_nrays, inv_from, grad_scale, lambda,
+                                              target, bg, ray_rgba, grad_density, drgb, loss_sums, accumulate);
+    return launch_train_losses_v<W, false>(ctx, stream, batch, S, min_t, inv_nrays, inv_from, grad_scale, lambda,
+                                           target, bg, ray_rgba, grad_density, drgb, loss_sums, accumulate);
 }
 
 // Rays per warp of the sample-tile kernels, from the batch's mean samples per ray
@@ -2168,6 +2283,35 @@ static int check_batch(const tn_ray_batch* b) {
     TN_NONNULL(b->offsets);
     TN_REQUIRE(b->ray_stride >= b->n_rays, TN_E_INVALID, "ray_stride %u < n_rays %u", b->ray_stride, b->n_rays);
     return TN_OK;
+}
+
+// tn_train_losses, and the trainer's form that writes the merged gradient over grad_density
+// instead of adding to it (accumulate false: no zeroing pass before it).
+int train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_batch* batch, int activation, float min_transmittance,
+                 float inv_nrays, const uint32_t* inv_nrays_from_dev, float grad_scale, float lambda,
+                 const float* density, const float* rgb, const float* dt, const float* m_norm, const float* dt_norm,
+                 const float* t, const float* target_rgba, const float* bg_rgb, float* ray_rgba, float* grad_density,
+                 float* dL_drgb, float* loss_sums, bool accumulate) {
+    TN_NONNULL(ctx);
+    int st = check_batch(batch);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
+    TN_NONNULL(grad_density); TN_NONNULL(dL_drgb);
+    if (lambda > 0.0f) { TN_NONNULL(m_norm); TN_NONNULL(dt_norm); }
+    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
+    if (batch->n_rays == 0) return TN_OK;
+    Samples S{density, rgb, dt, m_norm, dt_norm, t, batch->sample_stride, activation};
+    switch (ctx->tune.loss_rays_per_block) {
+        case 2: return launch_train_losses<2>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
+                                              grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density,
+                                              dL_drgb, loss_sums, accumulate);
+        case 8: return launch_train_losses<8>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
+                                              grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density,
+                                              dL_drgb, loss_sums, accumulate);
+        default: return launch_train_losses<4>(ctx, stream, batch, S, min_transmittance, inv_nrays,
+                                               inv_nrays_from_dev, grad_scale, lambda, target_rgba, bg_rgb, ray_rgba,
+                                               grad_density, dL_drgb, loss_sums, accumulate);
+    }
 }
 
 }  // namespace tn
@@ -2307,27 +2451,9 @@ int tn_train_losses(tn_ctx* ctx, tn_stream_t stream, const tn_ray_batch* batch, 
                     float lambda, const float* density, const float* rgb, const float* dt, const float* m_norm,
                     const float* dt_norm, const float* t, const float* target_rgba, const float* bg_rgb,
                     float* ray_rgba, float* grad_density, float* dL_drgb, float* loss_sums) {
-    TN_NONNULL(ctx);
-    int st = check_batch(batch);
-    if (st != TN_OK) return st;
-    TN_NONNULL(density); TN_NONNULL(rgb); TN_NONNULL(dt); TN_NONNULL(target_rgba); TN_NONNULL(bg_rgb);
-    TN_NONNULL(grad_density); TN_NONNULL(dL_drgb);
-    if (lambda > 0.0f) { TN_NONNULL(m_norm); TN_NONNULL(dt_norm); }
-    TN_REQUIRE(activation == TN_ACT_SIGMA || activation == TN_ACT_DENSITY, TN_E_INVALID, "unknown activation %d", activation);
-    if (batch->n_rays == 0) return TN_OK;
-    Samples S{density, rgb, dt, m_norm, dt_norm, t, batch->sample_stride, activation};
-    switch (ctx->tune.loss_rays_per_block) {
-        case 2: st = launch_train_losses<2>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
-                                            grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density, dL_drgb,
-                                            loss_sums); break;
-        case 8: st = launch_train_losses<8>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
-                                            grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density, dL_drgb,
-                                            loss_sums); break;
-        default: st = launch_train_losses<4>(ctx, stream, batch, S, min_transmittance, inv_nrays, inv_nrays_from_dev,
-                                             grad_scale, lambda, target_rgba, bg_rgb, ray_rgba, grad_density, dL_drgb,
-                                             loss_sums); break;
-    }
-    return st;
+    return tn::train_losses(ctx, stream, batch, activation, min_transmittance, inv_nrays, inv_nrays_from_dev,
+                            grad_scale, lambda, density, rgb, dt, m_norm, dt_norm, t, target_rgba, bg_rgb, ray_rgba,
+                            grad_density, dL_drgb, loss_sums, true);
 }
 
 // fused_reconstruction_loss_forward_backward launch structure (src/core/nerf-network.cu:547-602):

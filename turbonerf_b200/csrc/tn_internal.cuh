@@ -104,6 +104,12 @@ int launch_adam(cudaStream_t stream, bool plain, uint32_t n, uint32_t n_grid, ui
                 float lr, const float* lr_dev, float beta1, float beta2, float epsilon, float l2_reg, float* weights,
                 float* weights_copy, const float* gradients, float* first_moments, float* second_moments,
                 uint32_t* param_steps, const AdamPlacement& place = AdamPlacement{});
+// tn_train_losses; accumulate false writes the merged density gradient over grad_density.
+int train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_batch* batch, int activation, float min_transmittance,
+                 float inv_nrays, const uint32_t* inv_nrays_from_dev, float grad_scale, float lambda,
+                 const float* density, const float* rgb, const float* dt, const float* m_norm, const float* dt_norm,
+                 const float* t, const float* target_rgba, const float* bg_rgb, float* ray_rgba, float* grad_density,
+                 float* dL_drgb, float* loss_sums, bool accumulate);
 int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc* grid, float* density,
                             uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
                             const float* values, const float* rand_select, int activation, int sample_all,

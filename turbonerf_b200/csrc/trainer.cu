@@ -28,9 +28,12 @@
 // Plain path: the reference's launch structure (thrust scans, blocking device->host reads of
 // the sample count and the losses, separate memsets and epilogue kernels, dense Adam).
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <condition_variable>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -333,13 +336,13 @@ static int enqueue_tail(tn_trainer* tr, int pi, int next, bool next_external, in
     if (st == TN_OK)
         st = tr->net.forward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
                              tr->net_rgb);
-    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->grad_density, 0, (size_t)tr->B * 4, s), "grad memset");
+    // the merged density gradient is written over grad_density (no zeroing pass)
     tn_ray_batch rb{tr->R, tr->R, tr->B, 0, p.n_steps, p.offsets, info};
     if (st == TN_OK)
-        st = tn_train_losses(p.ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, info, d.loss_scale,
-                             d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb,
-                             tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, p.target, p.bg, nullptr, tr->grad_density,
-                             tr->dl_drgb, tr->state->loss_sums);
+        st = train_losses(p.ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, info, d.loss_scale,
+                          d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb, tr->s_dt,
+                          tr->s_mnorm, tr->s_dtnorm, tr->s_t, p.target, p.bg, nullptr, tr->grad_density, tr->dl_drgb,
+                          tr->state->loss_sums, false);
     if (st == TN_OK && tr->net.backward)
         st = tr->net.backward(tr->net.user, s, tr->B, info + 1, tr->B, tr->s_pos, tr->s_dir, tr->grad_density,
                               tr->dl_drgb, tr->g);
@@ -404,13 +407,12 @@ static int enqueue_profiled_step(tn_trainer* tr, int pi, cudaEvent_t* ev) {
         st = tr->net.forward(tr->net.user, s, tr->B, p.info + 1, tr->B, tr->s_pos, tr->s_dir, tr->net_density,
                              tr->net_rgb);
     cudaEventRecord(ev[ST_FORWARD + 1], s);
-    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(tr->grad_density, 0, (size_t)tr->B * 4, s), "grad memset");
     tn_ray_batch rb{tr->R, tr->R, tr->B, 0, p.n_steps, p.offsets, p.info};
     if (st == TN_OK)
-        st = tn_train_losses(p.ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, p.info, d.loss_scale,
-                             d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb,
-                             tr->s_dt, tr->s_mnorm, tr->s_dtnorm, tr->s_t, p.target, p.bg, nullptr, tr->grad_density,
-                             tr->dl_drgb, tr->state->loss_sums);
+        st = train_losses(p.ctx, s, &rb, tr->net.activation, d.min_transmittance, 0.0f, p.info, d.loss_scale,
+                          d.use_distortion_loss ? d.distortion_lambda : 0.0f, tr->net_density, tr->net_rgb, tr->s_dt,
+                          tr->s_mnorm, tr->s_dtnorm, tr->s_t, p.target, p.bg, nullptr, tr->grad_density, tr->dl_drgb,
+                          tr->state->loss_sums, false);
     cudaEventRecord(ev[ST_LOSSES + 1], s);
     if (st == TN_OK && tr->net.backward)
         st = tr->net.backward(tr->net.user, s, tr->B, p.info + 1, tr->B, tr->s_pos, tr->s_dir, tr->grad_density,
@@ -1005,6 +1007,26 @@ int tn_trainer_train_step_rays_pipelined(tn_trainer* tr, uint32_t n_rays, const 
     return metrics_from(tr, tr->ring_state[p], previous);
 }
 
+// Holds a stream until the host has enqueued everything behind it (at most a second), so that
+// the stages after it run back to back, as in the captured step, without gaps for host launches.
+struct StreamGate {
+    std::mutex mu;
+    std::condition_variable cv;
+    bool open = false;
+    static void CUDART_CB wait(void* self) {
+        auto* g = static_cast<StreamGate*>(self);
+        std::unique_lock<std::mutex> lock(g->mu);
+        g->cv.wait_for(lock, std::chrono::seconds(1), [g] { return g->open; });
+    }
+    void release() {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            open = true;
+        }
+        cv.notify_all();
+    }
+};
+
 int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages, uint32_t* n_stages) {
     TN_NONNULL(tr); TN_NONNULL(stage_ms);
     TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "stage timing covers the fused path");
@@ -1014,8 +1036,12 @@ int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages
     const int q = tr->cur ^ 1;
     cudaEvent_t ev[ST_N + 1];
     for (auto& e : ev) cudaEventCreate(&e);
-    int st = enqueue_profiled_step(tr, q, ev);
+    StreamGate gate;
+    int st = cuda_status(cudaLaunchHostFunc(tr->stream, StreamGate::wait, &gate), "profile gate");
+    if (st == TN_OK) st = enqueue_profiled_step(tr, q, ev);
+    gate.release();
     if (st == TN_OK) st = cuda_status(cudaEventSynchronize(ev[ST_N]), "profile sync");
+    else cudaStreamSynchronize(tr->stream);  // the gate must not outlive this frame
     const uint32_t n = std::min<uint32_t>(max_stages, ST_N);
     for (uint32_t k = 0; k < n && st == TN_OK; ++k) cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
     for (auto& e : ev) cudaEventDestroy(e);
