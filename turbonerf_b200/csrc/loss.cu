@@ -37,22 +37,21 @@ constexpr int SAVED_TILES = 64;  // distortion tile carries kept in lane registe
 __device__ __forceinline__ float act_sigma(int act, float d) { return act == 0 ? d : expf(fminf(d, 12.0f) - 1.0f); }
 __device__ __forceinline__ float act_dsigma(int act, float sigma) { return act == 0 ? 1.0f : sigma; }
 
-// 1 - exp(-x) for x >= 0 (the opacity of a sample with optical depth x): below 1/4 the first
-// seven terms of its Taylor series, x (1 - x/2 (1 - x/3 (... (1 - x/7)))), whose truncation error
-// is below 2e-9 of the result; above, 1 - exp(-x), free of cancellation there.
+// 1 - exp(-x) for x >= 0 (the opacity of a sample with optical depth x), without a branch: below
+// 1/4, x times the first eight terms of (1 - e^-x)/x = sum_k (-x)^k / (k+1)! in Horner form (the
+// truncation is below 5e-11 of the result); above, 1 - e^-x from the fast exponential, free of
+// cancellation there (its relative error is a few 1e-7). Both are evaluated and one selected.
 __device__ __forceinline__ float opacity(float x) {
-    if (x < 0.25f) {
-        float p = fmaf(-x, 1.0f / 7.0f, 1.0f);
-        p = fmaf(-x * (1.0f / 6.0f), p, 1.0f);
-        p = fmaf(-x * (1.0f / 5.0f), p, 1.0f);
-        p = fmaf(-x * (1.0f / 4.0f), p, 1.0f);
-        p = fmaf(-x * (1.0f / 3.0f), p, 1.0f);
-        p = fmaf(-x * 0.5f, p, 1.0f);
-        return x * p;
-    }
-    return 1.0f - expf(-x);
+    float p = fmaf(x, -1.0f / 40320.0f, 1.0f / 5040.0f);
+    p = fmaf(p, x, -1.0f / 720.0f);
+    p = fmaf(p, x, 1.0f / 120.0f);
+    p = fmaf(p, x, -1.0f / 24.0f);
+    p = fmaf(p, x, 1.0f / 6.0f);
+    p = fmaf(p, x, -0.5f);
+    p = fmaf(p, x, 1.0f);
+    const float big = 1.0f - __expf(-x);
+    return x < 0.25f ? x * p : big;
 }
-
 
 // Exclusive value from an inclusive warp scan: lane 0 gets `carry`.
 __device__ __forceinline__ float shift_up(float incl, int lane, float carry) {
@@ -390,6 +389,8 @@ __device__ __forceinline__ uint32_t live_rays(uint32_t n_rays, const uint32_t* n
 // not once per ray or per 32 samples. The warp's ray table sits in shared memory; each lane
 // finds the ray of its first sample once per tile and steps to the next ray at ray ends.
 constexpr int ST_K = 4;
+constexpr int CT_K = 8;  // samples a lane of the compositor forward tiles
+constexpr int CV_K = 4;  // samples a lane of the compositor VJP tiles
 
 // Last i < nr with off[i] <= s (rays without samples share their start with the next ray and
 // are passed over).
@@ -512,8 +513,9 @@ __device__ __forceinline__ void load_tile(const Samples& S, uint32_t s0, const b
 template <int K>
 __device__ __forceinline__ void prefetch_tile(const Samples& S, uint32_t s, int lane) {
     constexpr int LINES = WARP * K / 32;  // 128-byte lines of one array per tile
-    if (lane < 5 * LINES) {
-        const int arr = lane / LINES, line = lane % LINES;
+#pragma unroll
+    for (int i = lane; i < 5 * LINES; i += WARP) {
+        const int arr = i / LINES, line = i % LINES;
         const uint32_t at = s + (uint32_t)line * 32u;
         if (at < S.ss) {
             const float* base = arr == 0 ? S.density : arr == 1 ? S.dt : S.rgb + (size_t)(arr - 2) * S.ss;
@@ -522,188 +524,262 @@ __device__ __forceinline__ void prefetch_tile(const Samples& S, uint32_t s, int 
     }
 }
 
+// Head bits of one tile of 32 K samples [base, base + 32 K] (one word more for the sample after
+// the tile): bit d is set when a non-empty ray of the warp starts at base + d, or when the warp's
+// samples end there. `off` is the lane's ray start (lanes at or past `nne` hold none). Returns, for
+// lane l, the K + 1 bits from sample base + K l.
+template <int K>
+__device__ __forceinline__ uint32_t tile_head_bits(uint32_t* words, uint32_t base, uint32_t off, int nne,
+                                                   uint32_t s_end, int lane) {
+    if (lane <= K) words[lane] = 0u;
+    __syncwarp();
+    const uint32_t d = off - base;  // wraps for rays that started before the tile
+    if (lane < nne && d <= (uint32_t)(WARP * K)) atomicOr(&words[d >> 5], 1u << (d & 31));
+    const uint32_t e = s_end - base;
+    if (lane == 0 && e <= (uint32_t)(WARP * K)) atomicOr(&words[e >> 5], 1u << (e & 31));
+    __syncwarp();
+    const uint32_t p0 = (uint32_t)lane * K;
+    return __funnelshift_r(words[p0 >> 5], words[(p0 >> 5) + 1], p0 & 31);
+}
+
+// Ordinal (among the warp's non-empty rays, starts `off` ascending) of the ray holding sample s:
+// the last k < nne with off[k] <= s, or -1 before the first start (the part of a warp's first
+// 16-byte group that precedes its rays).
+__device__ __forceinline__ int ray_ordinal(const uint32_t* off, int nne, uint32_t s) {
+    if (off[0] > s) return -1;
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const int mid = lo + step;
+        if (mid < nne && off[mid] <= s) lo = mid;
+    }
+    return lo;
+}
+
 // Compositor forward over the rays of each warp (density_to_ray_rgba_forward,
 // src/utils/training-kernels-fused.cuh:227-264). Termination is decided on the optical depth
 // d = sum sigma dt: sample j is composited while the depth before it is at most
 // depth_max = -ln(min_t) (transmittance >= min_t), and the first sample whose depth after it
 // exceeds depth_max is the last one composited. The weights use the transmittance as a product
 // of (1 - alpha) inside each lane from exp(-depth) at the lane's first sample.
+// Ray boundaries come from the tile's head bits (one word per 32 samples, built once per tile):
+// a lane tests bits instead of searching the ray table per sample, and one segment plan serves
+// the optical-depth scan and the colour scan. The alpha of a ray is 1 - exp(-d) at its
+// terminating sample (the sum of its weights, without rounding accumulated over the samples),
+// stored with the depth and the sample count there; its colour sums are stored at its last sample
+// (the ray open at the lane's start, after the colour scan).
+// One group of the forward tiles: rays [r0, r0 + nr) (consecutive samples), walked in tiles of
+// 32 K samples. t_off, t_rid and t_head are the warp's tables.
 template <int K, bool VEC, int ACT, bool STORE>
-__global__ void __launch_bounds__(LOSS_THREADS)
-composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
-                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float depth_max,
-                           float* __restrict__ rgba, float* __restrict__ depth, uint32_t* __restrict__ n_used,
-                           float* __restrict__ t_out, float* __restrict__ w_out) {
-    __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_end[LOSS_WARPS][WARP];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint32_t n_live = live_rays(n_rays, n_dev);
-    const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
-    if (r0 >= n_live) return;  // whole warps leave together
-    const int nr = (int)min(rpw, n_live - r0);
+__device__ __forceinline__ void composite_fwd_group(const Samples& S, uint32_t r0, int nr, uint32_t rs,
+                                                    const uint32_t* __restrict__ counts,
+                                                    const uint32_t* __restrict__ offsets, float depth_max,
+                                                    float* __restrict__ rgba, float* __restrict__ depth,
+                                                    uint32_t* __restrict__ n_used, float* __restrict__ t_out,
+                                                    float* __restrict__ w_out, uint32_t* t_off, uint32_t* t_rid,
+                                                    uint32_t* t_head, int lane) {
+    uint32_t o = 0, c = 0;
     if (lane < nr) {
-        const uint32_t o = offsets[r0 + lane], e = o + counts[r0 + lane];
-        t_off[wid][lane] = o;
-        t_end[wid][lane] = e;
-        if (e == o) {  // a ray without samples
+        o = offsets[r0 + lane];
+        c = counts[r0 + lane];
+        if (c == 0) {  // a ray without samples
             const uint32_t r = r0 + lane;
             rgba[r] = 0.0f; rgba[r + rs] = 0.0f; rgba[r + 2 * (size_t)rs] = 0.0f; rgba[r + 3 * (size_t)rs] = 0.0f;
             if (depth) depth[r] = 0.0f;
             if (n_used) n_used[r] = 0u;
         }
     }
+    const unsigned ne = __ballot_sync(FULL_MASK, c > 0u);
+    if (ne == 0u) return;
+    if (c > 0u) {
+        const int k = __popc(ne & ((1u << lane) - 1u));
+        t_off[k] = o;
+        t_rid[k] = r0 + (uint32_t)lane;
+    }
+    const int nne = __popc(ne);
+    const uint32_t s_begin = __shfl_sync(FULL_MASK, o, __ffs(ne) - 1);
+    const uint32_t s_end = __shfl_sync(FULL_MASK, o + c, 31 - __clz(ne));
     __syncwarp();
-    const uint32_t s_begin = t_off[wid][0], s_end = t_end[wid][nr - 1];
-    float cx = 0.0f, csum[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // running sums of the ray open at the tile start
+    const uint32_t my_off = lane < nne ? t_off[lane] : 0u;
+    float cx = 0.0f, c3[3] = {0.0f, 0.0f, 0.0f};  // depth and colour sums of the ray open at the tile start
     for (uint32_t base = VEC ? (s_begin & ~3u) : s_begin; base < s_end; base += WARP * K) {
         if (base + WARP * K < s_end) prefetch_tile<K>(S, base + WARP * K, lane);
+        const uint32_t win = tile_head_bits<K>(t_head, base, my_off, nne, s_end, lane);
+        constexpr uint32_t LANE_BITS = (1u << K) - 1u;
+        const uint32_t hm = win & LANE_BITS, lm = (win >> 1) & LANE_BITS;  // ray starts; ray ends
         const uint32_t s0 = base + (uint32_t)lane * K;
-        bool in[K], head[K], last[K];
-        int ri[K];
-        uint32_t roff[K];
-        int cur = find_ray(t_off[wid], nr, s0 > s_begin ? s0 : s_begin);
-        uint32_t coff = t_off[wid][cur], cend = t_end[wid][cur];
+        const uint32_t lo = s_begin > s0 ? min(s_begin - s0, (uint32_t)K) : 0u;
+        const uint32_t hi = s_end > s0 ? min(s_end - s0, (uint32_t)K) : 0u;
+        const uint32_t im = ((1u << hi) - 1u) & ~((1u << lo) - 1u);  // samples inside [s_begin, s_end)
+        bool in[K];
 #pragma unroll
-        for (int q = 0; q < K; ++q) {
-            const uint32_t s = s0 + q;
-            in[q] = s >= s_begin && s < s_end;
-            while (in[q] && s >= cend) {  // the next ray with samples
-                ++cur;
-                coff = t_off[wid][cur];
-                cend = t_end[wid][cur];
-            }
-            ri[q] = cur;
-            roff[q] = coff;
-            head[q] = in[q] && s == coff;
-            last[q] = in[q] && s + 1 == cend;
-        }
+        for (int q = 0; q < K; ++q) in[q] = (im >> q) & 1u;
         float x[K], dtv[K], cr[K], cg[K], cb[K];
         load_tile<K, VEC, ACT>(S, s0, in, x, dtv, cr, cg, cb);
 #pragma unroll
         for (int q = 0; q < K; ++q) x[q] *= dtv[q];
-        // optical depth: the lane's open-segment aggregate, scanned, then per sample
-        bool any_head = false;
-        float agg[1] = {0.0f};
+        // optical depth: the lane's aggregate from its last ray start, one segmented scan
+        const bool cut = hm != 0u;
+        const uint32_t plan = seg_plan<false>(cut, lane);
+        float agg[1];
+        {
+            float a = 0.0f;
 #pragma unroll
-        for (int q = 0; q < K; ++q) {
-            if (head[q]) { agg[0] = 0.0f; any_head = true; }
-            agg[0] += x[q];
+            for (int q = 0; q < K; ++q) a = ((hm >> q) & 1u) ? x[q] : a + x[q];
+            agg[0] = (lane == 0 && !cut) ? a + cx : a;
         }
-        if (lane == 0 && !any_head) agg[0] += cx;
-        seg_scan<1, false>(agg, any_head, lane);
+        seg_scan_plan<1, false>(agg, plan);
         float run = __shfl_up_sync(FULL_MASK, agg[0], 1);
         if (lane == 0) run = cx;
-        float d[K], wv[K];
-        float tb = expf(-run);  // transmittance before the lane's first sample
+        const int k0 = ray_ordinal(t_off, nne, s0);  // the ray open at the lane's first sample
+        float tb = __expf(-run);  // transmittance before the lane's first sample
+        float a3[3] = {0.0f, 0.0f, 0.0f};
+        float f3[3] = {0.0f, 0.0f, 0.0f};
+        bool first_end = false;  // the ray open at the lane's start ends in the lane
 #pragma unroll
         for (int q = 0; q < K; ++q) {
-            const float excl = head[q] ? 0.0f : run;
-            if (head[q]) tb = 1.0f;
+            const bool h = (hm >> q) & 1u;
+            const float excl = h ? 0.0f : run;
+            tb = h ? 1.0f : tb;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) a3[k] = h ? 0.0f : a3[k];
             run = excl + x[q];
-            d[q] = run;
-            const bool comp = in[q] && (head[q] || excl <= depth_max);
-            const float a = opacity(x[q]);
-            wv[q] = comp ? tb * a : 0.0f;
-            const float tn = fmaf(-tb, a, tb);  // transmittance after the sample
+            const bool comp = in[q] && excl <= depth_max;
+            const float al = opacity(x[q]);
+            const float w = comp ? tb * al : 0.0f;
+            const float tn = fmaf(-tb, al, tb);  // transmittance after the sample
             if (STORE && comp) {
                 t_out[s0 + q] = tn;
-                w_out[s0 + q] = wv[q];
+                w_out[s0 + q] = w;
             }
-            // a ray composites nothing after its terminating sample; a composited last sample that
-            // does not terminate means the ray never terminated
-            if (comp && (run > depth_max || last[q])) {
-                const uint32_t r = r0 + (uint32_t)ri[q];
-                if (depth) depth[r] = d[q];
-                if (n_used) n_used[r] = s0 + q - roff[q] + 1u;
+            a3[0] = fmaf(w, cr[q], a3[0]);
+            a3[1] = fmaf(w, cg[q], a3[1]);
+            a3[2] = fmaf(w, cb[q], a3[2]);
+            const bool last = in[q] && ((lm >> q) & 1u);
+            const bool term = comp && (run > depth_max || last);  // the ray's terminating sample
+            if (term || last) {  // in-range samples: at or after the warp's first ray start
+                const int k = k0 + __popc(hm & ((2u << q) - 2u));
+                const uint32_t r = t_rid[k];
+                if (term) {  // depth, samples used, alpha
+                    if (depth) depth[r] = run;
+                    if (n_used) n_used[r] = s0 + q - t_off[k] + 1u;
+                    rgba[r + 3 * (size_t)rs] = -expm1f(-run);
+                }
+                if (last) {
+                    if ((hm & ((2u << q) - 1u)) == 0u) {
+                        first_end = true;  // the ray began in an earlier lane: completed after the colour scan
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) f3[c] = a3[c];
+                    } else {
+                        rgba[r] = a3[0]; rgba[r + rs] = a3[1]; rgba[r + 2 * (size_t)rs] = a3[2];
+                    }
+                }
             }
             tb = tn;
         }
-        // weighted colour and alpha sums per ray
-        float a4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        // colour sums of the ray open at each lane's end, over the lanes
+        if (lane == 0 && !cut) {
 #pragma unroll
-        for (int q = 0; q < K; ++q) {
-            if (head[q]) a4[0] = a4[1] = a4[2] = a4[3] = 0.0f;
-            a4[0] += wv[q] * cr[q]; a4[1] += wv[q] * cg[q]; a4[2] += wv[q] * cb[q]; a4[3] += wv[q];
+            for (int k = 0; k < 3; ++k) a3[k] += c3[k];
         }
-        if (lane == 0 && !any_head) {
+        seg_scan_plan<3, false>(a3, plan);
+        float e3[3];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) a4[k] += csum[k];
+        for (int k = 0; k < 3; ++k) {
+            e3[k] = __shfl_up_sync(FULL_MASK, a3[k], 1);
+            if (lane == 0) e3[k] = c3[k];
         }
-        seg_scan<4, false>(a4, any_head, lane);
-        float c4[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            c4[k] = __shfl_up_sync(FULL_MASK, a4[k], 1);
-            if (lane == 0) c4[k] = csum[k];
-        }
-#pragma unroll
-        for (int q = 0; q < K; ++q) {
-            if (head[q]) c4[0] = c4[1] = c4[2] = c4[3] = 0.0f;
-            c4[0] += wv[q] * cr[q]; c4[1] += wv[q] * cg[q]; c4[2] += wv[q] * cb[q]; c4[3] += wv[q];
-            if (last[q]) {
-                const uint32_t r = r0 + (uint32_t)ri[q];
-                rgba[r] = c4[0]; rgba[r + rs] = c4[1]; rgba[r + 2 * (size_t)rs] = c4[2];
-                rgba[r + 3 * (size_t)rs] = c4[3];
-            }
+        if (first_end) {
+            const uint32_t r = t_rid[k0];
+            rgba[r] = e3[0] + f3[0]; rgba[r + rs] = e3[1] + f3[1]; rgba[r + 2 * (size_t)rs] = e3[2] + f3[2];
         }
         // carries of the ray open at the end of the tile (lane 31 holds the tile's last samples)
         cx = __shfl_sync(FULL_MASK, agg[0], WARP - 1);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) csum[k] = __shfl_sync(FULL_MASK, a4[k], WARP - 1);
+        for (int k = 0; k < 3; ++k) c3[k] = __shfl_sync(FULL_MASK, a3[k], WARP - 1);
+        __syncwarp();  // every lane has read the tile's head words
     }
 }
 
-// Compositor VJP over the rays of each warp (semantics of composite_vjp_ray): tiles from the end
-// of the warp's samples down; segmented suffix sums of x = sigma dt over [j, used) rebuild the
-// transmittance from each ray's forward depth, then suffix sums of w c and w. Samples of a ray
-// at or past its `used` get zero gradients.
-template <int K, bool VEC, int ACT>
+template <int K, bool VEC, int ACT, bool STORE>
 __global__ void __launch_bounds__(LOSS_THREADS)
-composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
-                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                           const float* __restrict__ depth, const uint32_t* __restrict__ n_used,
-                           const float* __restrict__ grad_rgba, float* __restrict__ dd, float* __restrict__ drgb) {
-    __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_end[LOSS_WARPS][WARP], t_lim[LOSS_WARPS][WARP];
-    __shared__ float t_dep[LOSS_WARPS][WARP], t_g[LOSS_WARPS][4][WARP];
+composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
+                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float depth_max,
+                           float* __restrict__ rgba, float* __restrict__ depth, uint32_t* __restrict__ n_used,
+                           float* __restrict__ t_out, float* __restrict__ w_out) {
+    static_assert(K % 4 == 0 && K <= 16, "16-byte groups, at most 16 samples a lane");
+    __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_rid[LOSS_WARPS][WARP], t_head[LOSS_WARPS][K + 1];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_live = live_rays(n_rays, n_dev);
     const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
-    if (r0 >= n_live) return;
-    const int nr = (int)min(rpw, n_live - r0);
+    if (r0 >= n_live) return;  // whole warps leave together
+    composite_fwd_group<K, VEC, ACT, STORE>(S, r0, (int)min(rpw, n_live - r0), rs, counts, offsets, depth_max, rgba,
+                                            depth, n_used, t_out, w_out, t_off[wid], t_rid[wid], t_head[wid], lane);
+}
+
+// Compositor VJP over the rays of each warp (semantics of composite_vjp_ray): tiles from the end
+// of the warp's samples down. With the ray's upstream gradient g = (gr, gg, gb, ga) and
+// u_j = gr r_j + gg g_j + gb b_j + ga, dL/dsigma_j = dt_j (T_{j+1} u_j - sum_{i>j} w_i u_i) over the
+// composited samples: one segmented suffix sum of w u. The transmittance at each lane's first
+// sample comes from the ray's forward depth minus the segmented suffix sum of x = sigma dt (one
+// exponential a lane); inside the lane it is the product of (1 - alpha), restarted at ray starts.
+// Samples of a ray at or past its `used` get zero gradients.
+// One group of the VJP tiles: rays [r0, r0 + nr), tiles from the last. t_off, t_lim, t_dep, t_g
+// and t_head are the warp's tables.
+template <int K, bool VEC, int ACT>
+__device__ __forceinline__ void composite_bwd_group(const Samples& S, uint32_t r0, int nr, uint32_t rs,
+                                                    const uint32_t* __restrict__ counts,
+                                                    const uint32_t* __restrict__ offsets,
+                                                    const float* __restrict__ depth,
+                                                    const uint32_t* __restrict__ n_used,
+                                                    const float* __restrict__ grad_rgba, float* __restrict__ dd,
+                                                    float* __restrict__ drgb, uint32_t* t_off, uint32_t* t_lim,
+                                                    float* t_dep, float4* t_g, uint32_t* t_head, int lane) {
+    uint32_t o = 0, c = 0;
     if (lane < nr) {
-        const uint32_t r = r0 + lane;
-        const uint32_t o = offsets[r], c = counts[r];
-        t_off[wid][lane] = o;
-        t_end[wid][lane] = o + c;
-        t_lim[wid][lane] = o + min(n_used[r], c);  // end of the composited samples
-        t_dep[wid][lane] = depth[r];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) t_g[wid][k][lane] = grad_rgba[r + k * (size_t)rs];
+        o = offsets[r0 + lane];
+        c = counts[r0 + lane];
     }
+    const unsigned ne = __ballot_sync(FULL_MASK, c > 0u);
+    if (ne == 0u) return;
+    if (c > 0u) {
+        const uint32_t r = r0 + (uint32_t)lane;
+        const int k = __popc(ne & ((1u << lane) - 1u));
+        t_off[k] = o;
+        t_lim[k] = o + min(n_used[r], c);  // end of the composited samples
+        t_dep[k] = depth[r];
+        t_g[k] = make_float4(grad_rgba[r], grad_rgba[r + rs], grad_rgba[r + 2 * (size_t)rs],
+                                  grad_rgba[r + 3 * (size_t)rs]);
+    }
+    const int nne = __popc(ne);
+    const uint32_t s_begin = __shfl_sync(FULL_MASK, o, __ffs(ne) - 1);
+    const uint32_t s_end = __shfl_sync(FULL_MASK, o + c, 31 - __clz(ne));
     __syncwarp();
-    const uint32_t s_begin = t_off[wid][0], s_end = t_end[wid][nr - 1];
+    const uint32_t my_off = lane < nne ? t_off[lane] : 0u;
     const uint32_t b0 = VEC ? (s_begin & ~3u) : s_begin;
     const uint32_t span = WARP * K;
     const uint32_t n_tiles = (s_end - b0 + span - 1) / span;
-    float cx = 0.0f, c4[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // suffix sums of the ray open at the tile end
+    float cx = 0.0f, cu = 0.0f;  // suffix sums of x and w u of the ray open at the tile end
     for (int t = (int)n_tiles - 1; t >= 0; --t) {
-        if (t > 0) prefetch_tile<K>(S, b0 + (uint32_t)(t - 1) * span, lane);
-        const uint32_t s0 = b0 + (uint32_t)t * span + (uint32_t)lane * K;
-        bool in[K], valid[K], tail[K];
-        int ri[K];
-        int cur = find_ray(t_off[wid], nr, s0 > s_begin ? s0 : s_begin);
-        uint32_t cend = t_end[wid][cur], clim = t_lim[wid][cur];
+        const uint32_t base = b0 + (uint32_t)t * span;
+        if (t > 0) prefetch_tile<K>(S, base - span, lane);
+        const uint32_t win = tile_head_bits<K>(t_head, base, my_off, nne, s_end, lane);
+        constexpr uint32_t LANE_BITS = (1u << K) - 1u;
+        const uint32_t hm = win & LANE_BITS, lm = (win >> 1) & LANE_BITS;  // ray starts; ray ends
+        const uint32_t s0 = base + (uint32_t)lane * K;
+        const uint32_t lo = s_begin > s0 ? min(s_begin - s0, (uint32_t)K) : 0u;
+        const uint32_t hi = s_end > s0 ? min(s_end - s0, (uint32_t)K) : 0u;
+        const uint32_t im = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+        const int k0 = ray_ordinal(t_off, nne, s0);
+        bool in[K], valid[K];
+        float4 g[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) {
-            const uint32_t s = s0 + q;
-            in[q] = s >= s_begin && s < s_end;
-            while (in[q] && s >= cend) {
-                ++cur;
-                cend = t_end[wid][cur];
-                clim = t_lim[wid][cur];
-            }
-            ri[q] = cur;
-            valid[q] = in[q] && s < clim;
-            tail[q] = in[q] && s + 1 == cend;
+            in[q] = (im >> q) & 1u;
+            // -1 only for samples before the warp's first start, which are outside the range
+            const int k = max(k0 + __popc(hm & ((2u << q) - 2u)), 0);
+            valid[q] = in[q] && s0 + q < t_lim[k];
+            g[q] = t_g[k];
         }
         float x[K], dtv[K], cr[K], cg[K], cb[K];
         load_tile<K, VEC, ACT>(S, s0, valid, x, dtv, cr, cg, cb);
@@ -714,70 +790,55 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
             x[q] *= dtv[q];
         }
         // suffix sums of x: the lane's aggregate is its samples up to its first ray end
-        bool any_tail = false;
-        float agg[1] = {0.0f};
+        const bool cut = lm != 0u;
+        const uint32_t plan = seg_plan<true>(cut, lane);
+        float vx[1];
+        {
+            float a = 0.0f;
 #pragma unroll
-        for (int q = K - 1; q >= 0; --q) {
-            if (tail[q]) { agg[0] = 0.0f; any_tail = true; }
-            agg[0] += x[q];
+            for (int q = K - 1; q >= 0; --q) a = ((lm >> q) & 1u) ? x[q] : a + x[q];
+            vx[0] = (lane == WARP - 1 && !cut) ? a + cx : a;
         }
-        if (lane == WARP - 1 && !any_tail) agg[0] += cx;
-        seg_scan<1, true>(agg, any_tail, lane);
-        float run = __shfl_down_sync(FULL_MASK, agg[0], 1);
-        if (lane == WARP - 1) run = cx;
-        // transmittance after (tn) and before (tj) each sample; inside a ray the one before sample
-        // q is the one after sample q - 1, from the same suffix sum
-        float tn[K], wv[K], xi[K], dep[K];
+        seg_scan_plan<1, true>(vx, plan);
+        // transmittance before and after each sample, weights, u and w u
+        float tn[K], w[K], u[K], wu[K];
+        {
+            float T = __expf(-fmaxf(t_dep[max(k0, 0)] - vx[0], 0.0f));
 #pragma unroll
-        for (int q = K - 1; q >= 0; --q) {
-            const float xe = tail[q] ? 0.0f : run;  // sum_{i>j} x_i within the ray
-            run = xe + x[q];                         // sum_{i>=j} x_i
-            xi[q] = run;
-            dep[q] = t_dep[wid][ri[q]];
-            tn[q] = expf(-fmaxf(dep[q] - xe, 0.0f));
+            for (int q = 0; q < K; ++q) {
+                T = ((hm >> q) & 1u) ? 1.0f : T;
+                const float al = opacity(x[q]);
+                w[q] = valid[q] ? T * al : 0.0f;
+                tn[q] = fmaf(-T, al, T);
+                u[q] = fmaf(g[q].x, cr[q], fmaf(g[q].y, cg[q], fmaf(g[q].z, cb[q], g[q].w)));
+                wu[q] = w[q] * u[q];
+                T = tn[q];
+            }
         }
+        float vu[1];
+        {
+            float a = 0.0f;
 #pragma unroll
-        for (int q = 0; q < K; ++q) {
-            const float tj = (q > 0 && ri[q] == ri[q - 1]) ? tn[q > 0 ? q - 1 : 0]
-                                                           : expf(-fmaxf(dep[q] - xi[q], 0.0f));
-            wv[q] = valid[q] ? tj * opacity(x[q]) : 0.0f;
+            for (int q = K - 1; q >= 0; --q) a = ((lm >> q) & 1u) ? wu[q] : a + wu[q];
+            vu[0] = (lane == WARP - 1 && !cut) ? a + cu : a;
         }
-        float a4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int q = K - 1; q >= 0; --q) {
-            if (tail[q]) a4[0] = a4[1] = a4[2] = a4[3] = 0.0f;
-            a4[0] += wv[q] * cr[q]; a4[1] += wv[q] * cg[q]; a4[2] += wv[q] * cb[q]; a4[3] += wv[q];
-        }
-        if (lane == WARP - 1 && !any_tail) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a4[k] += c4[k];
-        }
-        seg_scan<4, true>(a4, any_tail, lane);
-        float e4[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            e4[k] = __shfl_down_sync(FULL_MASK, a4[k], 1);
-            if (lane == WARP - 1) e4[k] = c4[k];
-        }
+        seg_scan_plan<1, true>(vu, plan);
+        float e = __shfl_down_sync(FULL_MASK, vu[0], 1);  // sum of w u after the lane, ray open at its end
+        if (lane == WARP - 1) e = cu;
         float o_d[K], o_r[K], o_g[K], o_b[K];
 #pragma unroll
         for (int q = K - 1; q >= 0; --q) {
-            if (tail[q]) e4[0] = e4[1] = e4[2] = e4[3] = 0.0f;  // sums over i > j within the ray
-            const float g0 = t_g[wid][0][ri[q]], g1 = t_g[wid][1][ri[q]], g2 = t_g[wid][2][ri[q]],
-                        g3 = t_g[wid][3][ri[q]];
-            const float ds = dtv[q] * (g0 * (tn[q] * cr[q] - e4[0]) + g1 * (tn[q] * cg[q] - e4[1]) +
-                                       g2 * (tn[q] * cb[q] - e4[2]) + g3 * (tn[q] - e4[3]));
+            e = ((lm >> q) & 1u) ? 0.0f : e;  // sums over i > j within the ray
+            const float ds = dtv[q] * (tn[q] * u[q] - e);
             o_d[q] = valid[q] ? ds * act_dsigma(ACT, sig[q]) : 0.0f;
-            o_r[q] = g0 * wv[q];
-            o_g[q] = g1 * wv[q];
-            o_b[q] = g2 * wv[q];
-            e4[0] += wv[q] * cr[q]; e4[1] += wv[q] * cg[q]; e4[2] += wv[q] * cb[q]; e4[3] += wv[q];
+            o_r[q] = g[q].x * w[q];
+            o_g[q] = g[q].y * w[q];
+            o_b[q] = g[q].z * w[q];
+            e += wu[q];
         }
 #pragma unroll
         for (int v = 0; v < K / 4; ++v) {
-            bool all_in = true;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) all_in = all_in && in[4 * v + k];
+            const bool all_in = ((im >> (4 * v)) & 15u) == 15u;
             const uint32_t sv = s0 + 4u * v;
             if (VEC && all_in) {
                 *reinterpret_cast<float4*>(dd + sv) = make_float4(o_d[4 * v], o_d[4 * v + 1], o_d[4 * v + 2], o_d[4 * v + 3]);
@@ -799,10 +860,28 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
                 }
             }
         }
-        cx = __shfl_sync(FULL_MASK, agg[0], 0);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) c4[k] = __shfl_sync(FULL_MASK, a4[k], 0);
+        cx = __shfl_sync(FULL_MASK, vx[0], 0);
+        cu = __shfl_sync(FULL_MASK, vu[0], 0);
+        __syncwarp();  // every lane has read the tile's head words
     }
+}
+
+template <int K, bool VEC, int ACT>
+__global__ void __launch_bounds__(LOSS_THREADS)
+composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
+                           const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                           const float* __restrict__ depth, const uint32_t* __restrict__ n_used,
+                           const float* __restrict__ grad_rgba, float* __restrict__ dd, float* __restrict__ drgb) {
+    static_assert(K % 4 == 0 && K <= 16, "16-byte groups, at most 16 samples a lane");
+    __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_lim[LOSS_WARPS][WARP], t_head[LOSS_WARPS][K + 1];
+    __shared__ float t_dep[LOSS_WARPS][WARP];
+    __shared__ float4 t_g[LOSS_WARPS][WARP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t n_live = live_rays(n_rays, n_dev);
+    const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
+    if (r0 >= n_live) return;
+    composite_bwd_group<K, VEC, ACT>(S, r0, (int)min(rpw, n_live - r0), rs, counts, offsets, depth, n_used, grad_rgba,
+                                     dd, drgb, t_off[wid], t_lim[wid], t_dep[wid], t_g[wid], t_head[wid], lane);
 }
 
 // ---- distortion loss over sample tiles ------------------------------------------------------
@@ -1354,17 +1433,6 @@ __device__ __forceinline__ void write_slots(float* buf, int lane, const float (&
 // relative error at the optical depths that matter here (x below about 20) is a few 1e-6.
 __device__ __forceinline__ float exp_neg(float x) { return __expf(-x); }
 
-// opacity(x) without a branch (both forms evaluated, one selected), from exp_neg.
-__device__ __forceinline__ float opacity_nb(float x) {
-    float p = fmaf(-x, 1.0f / 7.0f, 1.0f);
-    p = fmaf(-x * (1.0f / 6.0f), p, 1.0f);
-    p = fmaf(-x * (1.0f / 5.0f), p, 1.0f);
-    p = fmaf(-x * (1.0f / 4.0f), p, 1.0f);
-    p = fmaf(-x * (1.0f / 3.0f), p, 1.0f);
-    p = fmaf(-x * 0.5f, p, 1.0f);
-    const float big = 1.0f - exp_neg(x);
-    return x < 0.25f ? x * p : big;
-}
 
 // One ray of at most 32 K samples (32 K - o mod 4 with VEC) of the fused training losses, in
 // the slot layout, with the compositor's transmittance and weights kept from its forward:
@@ -1446,7 +1514,7 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
         float cut_depth = 0.0f;
 #pragma unroll
         for (int q = K - 1; q >= 0; --q) {
-            w[q] = (q ? T[q - 1] : t_in) * opacity_nb(sig[q] * dt[q]);
+            w[q] = (q ? T[q - 1] : t_in) * opacity(sig[q] * dt[q]);
             if (valid[q] && T[q] < min_t) { first_q = q; cut_depth = p[q]; }
         }
         const unsigned term = __ballot_sync(FULL_MASK, first_q < K);
@@ -1526,7 +1594,7 @@ __device__ __forceinline__ void train_losses_ray_blocked(const Samples& S, uint3
             const float t_in = shift_up(tnext[K - 1], lane, 1.0f);
 #pragma unroll
             for (int q = 0; q < K; ++q)
-                wd[q] = valid[q] ? (q ? tnext[q - 1] : t_in) * opacity_nb(sig[q] * dtn[q]) : 0.0f;
+                wd[q] = valid[q] ? (q ? tnext[q - 1] : t_in) * opacity(sig[q] * dtn[q]) : 0.0f;
         }
         {
             float W[K];
@@ -2200,9 +2268,10 @@ static int launch_train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_ba
 // warp while that leaves at least 32 warps per SM (the setup of a warp's range and its partly
 // filled first and last tiles are then paid once per 4 tiles), else 1 tile per warp; more when
 // the grid would otherwise take more than one wave of resident warps.
-static uint32_t tile_rays_per_warp(const tn_ray_batch* b, const void* kernel, uint32_t max_tiles = 0) {
+static uint32_t tile_rays_per_warp(const tn_ray_batch* b, const void* kernel, uint32_t max_tiles = 0,
+                                   int k = ST_K) {
     const double mean = b->n_rays ? std::max(1.0, (double)b->sample_stride / (double)b->n_rays) : 1.0;
-    const double per_tile = (double)(WARP * ST_K);
+    const double per_tile = (double)(WARP * k);
     const double fill = (double)b->sample_stride / (per_tile * num_sms() * 32.0);
     const double tiles = std::min(4.0, std::max(1.0, std::floor(fill)));
     uint32_t rpw = (uint32_t)std::min(32.0, std::max(1.0, std::floor(tiles * per_tile / mean)));
@@ -2232,15 +2301,16 @@ static int tile_grid(uint32_t n_rays, uint32_t rpw) {
 
 // Launch of the compositor forward tiles, specialised on the vector loads, the activation and
 // whether per-sample transmittance and weights are stored. depth_max = -ln(min_transmittance).
-static void launch_composite_fwd_tiles(cudaStream_t stream, const tn_ray_batch* b, const Samples& S, float min_t,
-                                       float* rgba, float* depth, uint32_t* n_used, float* t_out, float* w_out) {
+static void launch_composite_fwd_tiles(cudaStream_t stream, const tn_ray_batch* b, const Samples& S,
+                                       float min_t, float* rgba, float* depth, uint32_t* n_used, float* t_out,
+                                       float* w_out) {
     const float depth_max = min_t > 0.0f ? -logf(min_t) : INFINITY;
     const bool vec = tile_vec(S, t_out, w_out), store = t_out != nullptr;
     const uint32_t rpw = tile_rays_per_warp(
-        b, vec ? (const void*)composite_fwd_tiles_kernel<ST_K, true, 0, false> : (const void*)composite_fwd_tiles_kernel<ST_K, false, 0, false>);
+        b, vec ? (const void*)composite_fwd_tiles_kernel<CT_K, true, 0, false> : (const void*)composite_fwd_tiles_kernel<CT_K, false, 0, false>, 0, CT_K);
     const int grid = tile_grid(b->n_rays, rpw);
 #define TN_FWD_TILES(V, A, ST)                                                                                  \
-    composite_fwd_tiles_kernel<ST_K, V, A, ST><<<grid, LOSS_THREADS, 0, stream>>>(                              \
+    composite_fwd_tiles_kernel<CT_K, V, A, ST><<<grid, LOSS_THREADS, 0, stream>>>(                              \
         S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth_max, rgba, depth, n_used,  \
         t_out, w_out)
     const int key = (vec ? 4 : 0) | (S.act ? 2 : 0) | (store ? 1 : 0);
@@ -2262,11 +2332,12 @@ static void launch_composite_bwd_tiles(cudaStream_t stream, const tn_ray_batch* 
                                        float* drgb) {
     const bool vec = tile_vec(S, dd, drgb);
     const uint32_t rpw = tile_rays_per_warp(
-        b, vec ? (const void*)composite_bwd_tiles_kernel<ST_K, true, 0> : (const void*)composite_bwd_tiles_kernel<ST_K, false, 0>);
+        b, vec ? (const void*)composite_bwd_tiles_kernel<CV_K, true, 0> : (const void*)composite_bwd_tiles_kernel<CV_K, false, 0>, 0, CV_K);
     const int grid = tile_grid(b->n_rays, rpw);
 #define TN_BWD_TILES(V, A)                                                                                      \
-    composite_bwd_tiles_kernel<ST_K, V, A><<<grid, LOSS_THREADS, 0, stream>>>(                                  \
-        S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth, n_used, grad_rgba, dd, drgb)
+    composite_bwd_tiles_kernel<CV_K, V, A><<<grid, LOSS_THREADS, 0, stream>>>(                                  \
+        S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth, n_used, grad_rgba, dd,    \
+        drgb)
     const int key = (vec ? 2 : 0) | (S.act ? 1 : 0);
     switch (key) {
         case 0: TN_BWD_TILES(false, 0); break;
