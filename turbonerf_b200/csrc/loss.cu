@@ -344,12 +344,25 @@ __device__ void block_sum_and_finish(float (&v)[NV], float* partials, uint32_t* 
     __syncthreads();
     if (!is_last) return;
     __threadfence();
+    // every block's partials, four blocks a thread at a time: independent loads from L2 (the
+    // other blocks' stores are there; this block never cached them), then the adds
     float acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0.0f;
-    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    constexpr int U = 4;
+    for (uint32_t b0 = threadIdx.x; b0 < gridDim.x; b0 += U * blockDim.x) {
+        float x[U][NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) acc[k] += *((volatile float*)(partials + (size_t)b * NV + k));
+        for (int u = 0; u < U; ++u) {
+            const uint32_t b = b0 + (uint32_t)u * blockDim.x;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) x[u][k] = b < gridDim.x ? __ldcg(partials + (size_t)b * NV + k) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) acc[k] += x[u][k];
+        }
     }
     __syncthreads();
 #pragma unroll
@@ -702,7 +715,7 @@ __device__ __forceinline__ void composite_fwd_group(const Samples& S, uint32_t r
 }
 
 template <int K, bool VEC, int ACT, bool STORE>
-__global__ void __launch_bounds__(LOSS_THREADS)
+__global__ void __launch_bounds__(LOSS_THREADS, 3)
 composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float depth_max,
                            float* __restrict__ rgba, float* __restrict__ depth, uint32_t* __restrict__ n_used,
