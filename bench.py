@@ -197,8 +197,9 @@ STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "net
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass, after the warm-up steps).
 NCU_TRAFFIC = {"march_count": 1_007_616, "march_emit": 1_285_376, "losses": 9_637_888, "adam": 304_766_208,
                "occupancy": 50_338_304}
-# The same for the compositor tile kernels on the 2^22-sample batch (kernel tour capture).
-NCU_TRAFFIC_COMPOSITE = {"composite_fwd_tiles": 87_174_144, "composite_bwd_tiles": 114_450_688}
+# The same for the compositor tile kernels on the 2^22-sample batch (the `--workload compositor`
+# capture: DRAM read + write of the first forward and the first VJP launch).
+NCU_TRAFFIC_COMPOSITE = {"composite_fwd_tiles": 87_864_576, "composite_bwd_tiles": 117_784_064}
 
 
 class L2Flush:
@@ -797,6 +798,56 @@ def run_multi_scene(args):
     print(json.dumps(multi_scene_result(args)), flush=True)
 
 
+def run_compositor(args):
+    """The compositor tile kernels alone on the compositor workload (the `rooflines` object of the
+    default line): 2^22 samples over 65,571 rays, L2 flushed before every timed launch."""
+    import torch
+    torch.cuda.set_device(0)
+    peak, kind = _peaks()
+    print(json.dumps({"workload": "compositor tiles, 2^22 samples", "peak_source": kind,
+                      "rooflines": compositor_rooflines(peak, reps=max(args.steps // 5, 5))}), flush=True)
+
+
+def run_losses(args):
+    """The fused train-step loss kernel alone (tn_train_losses: reconstruction + distortion forward
+    and backward + gradient merge, lambda 1e-3) on two batches of 2^18 samples shaped like the train
+    step's: late in training (truncated geometric counts, mean 120, at most 240: every ray in the
+    one-pass path) and early (mean 178, at most 290: some rays past 256 samples take the chunked
+    path). CUDA events around 20 back-to-back launches, median of 5."""
+    import torch
+    from turbonerf_b200 import hotpath as hp, scenes
+    torch.cuda.set_device(0)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    out = {"workload": "fused train-step losses, 2^18 samples", "batches": []}
+    for label, mean, mx in (("late", 120.0, 240), ("early", 178.0, 290)):
+        sb = scenes.make_sample_batch(0x7B4, 1 << 18, mean=mean, max_count=mx)
+        n, ss = sb.n_rays, sb.n_samples
+        ctx = hp.Context()
+        rb = hp.ray_batch(d(sb.counts.view(np.int32)), d(sb.offsets.view(np.int32)), n, n, ss)
+        ins = [d(a) for a in (sb.sigma, sb.rgb, sb.dt, sb.m_norm, sb.dt_norm, sb.t, sb.target_rgba, sb.bg_rgb)]
+        gd, drgb, sums = torch.zeros(ss, device="cuda"), torch.zeros(3 * ss, device="cuda"), torch.zeros(2, device="cuda")
+
+        def launch():
+            hp.train_losses(ctx, rb, *ins, gd, inv_nrays=1.0 / n, lam=1e-3, dL_drgb=drgb, loss_sums=sums)
+
+        for _ in range(max(args.warmup, 3)):
+            launch()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(20):
+                launch()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e3 / 20)
+        assert ctx.check() == 0
+        out["batches"].append({"batch": label, "rays": n, "samples": ss, "max_count": int(sb.counts.max()),
+                               "rays_over_256": int((sb.counts > 256).sum()), "us": round(float(np.median(ts)), 2)})
+    print(json.dumps(out), flush=True)
+
+
 def run_kernel_tour(args):
     """Every kernel of the library, launched at representative sizes, for profiling (for instance
     `ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum`, one pass per
@@ -1239,13 +1290,15 @@ def main():
     ap.add_argument("--render-batches", default="0,1048576,4194304,16777216",
                     help="render workload: sample budgets per round (0: the library default)")
     ap.add_argument("--workload", default="train-step",
-                    choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render", "dataset-rays", "configs"],
+                    choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render", "dataset-rays", "configs",
+                             "compositor", "losses"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "
                          "multi-scene: the batched persistent march of 16 scenes against one launch per scene; "
                          "kernel-tour: every kernel once at representative sizes, for profiling; "
                          "render: inference frames through Renderer.submit; "
                          "dataset-rays: training rays from posed images; "
-                         "configs: GPU and CPU oracle on the smaller configurations")
+                         "configs: GPU and CPU oracle on the smaller configurations; "
+                         "compositor: the compositor tile kernels alone; losses: the fused loss kernel alone")
     args = ap.parse_args()
     if args.workload == "backward-memory":
         run_backward_memory(args)
@@ -1259,6 +1312,10 @@ def main():
         run_dataset_rays(args)
     elif args.workload == "configs":
         run_configs(args)
+    elif args.workload == "compositor":
+        run_compositor(args)
+    elif args.workload == "losses":
+        run_losses(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
