@@ -695,6 +695,63 @@ def _multi_scene_gpu(params, resolution=128, threshold=THRESHOLD):
     return ms, table
 
 
+def _multi_scene_losses(args, ctx, ctx_s, table_in, R, ss, n_steps, offsets, samples):
+    """The fused losses (tn_train_losses, lambda 1e-3, distance scaling) over the packed samples of
+    every scene: one launch over all rays (its grid is every resident warp, each taking rays of all
+    scenes in turn) against one launch per scene, each captured in a CUDA graph and replayed. The
+    network outputs are seeded stand-ins (sigma = exp(N(0, 2)) clipped to 1e4, rgb U[0, 1]);
+    targets and backgrounds U[0, 1]."""
+    import torch
+    from turbonerf_b200 import hotpath as hp
+    rng = np.random.default_rng(0x7C5)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    sig = d(np.clip(np.exp(rng.normal(0.0, 2.0, ss)), 0.0, 1e4).astype(np.float32))
+    rgb = d(rng.uniform(0.0, 1.0, 3 * ss).astype(np.float32))
+    tgt = d(rng.uniform(0.0, 1.0, 4 * R).astype(np.float32))
+    bg = d(rng.uniform(0.0, 1.0, 3 * R).astype(np.float32))
+    gd = torch.zeros(ss, device="cuda")
+    drgb = torch.zeros(3 * ss, device="cuda")
+    sums = torch.zeros(2 * (len(table_in) + 1), device="cuda")
+    fields = (samples["dt"], samples["m_norm"], samples["dt_norm"], samples["t"])
+    rb_all = hp.ray_batch(n_steps, offsets, R, R, ss)
+    rbs = [hp.ray_batch(n_steps[ti["ray_begin"]:], offsets[ti["ray_begin"]:], ti["n_rays"], R, ss) for ti in table_in]
+
+    def one_launch():
+        hp.train_losses(ctx, rb_all, sig, rgb, *fields, tgt, bg, gd, inv_nrays=1.0 / R, lam=1e-3, dL_drgb=drgb,
+                        loss_sums=sums[:2])
+
+    def one_per_scene():
+        for k, (ti, rb) in enumerate(zip(table_in, rbs)):
+            b = ti["ray_begin"]
+            hp.train_losses(ctx_s, rb, sig, rgb, *fields, tgt[b:], bg[b:], gd, inv_nrays=1.0 / ti["n_rays"],
+                            lam=1e-3, dL_drgb=drgb, loss_sums=sums[2 * k + 2:2 * k + 4])
+
+    out = {"n_rays": R, "n_samples": ss - 64}
+    for name, fn in (("one_launch", one_launch), ("per_scene", one_per_scene)):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        for _ in range(3):
+            g.replay()
+        reps = max(args.steps, 10)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            g.replay()
+        e1.record()
+        e1.synchronize()
+        ms_ = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": round(ms_, 4), "samples_per_s": round((ss - 64) / (ms_ / 1e3), 1)}
+        del g
+    assert ctx.check() == 0 and ctx_s.check() == 0
+    out["one_launch_speedup"] = round(out["per_scene"]["ms"] / out["one_launch"]["ms"], 3)
+    return out
+
+
 def multi_scene_result(args, labels=("as_drawn", "scaled_2e19_samples")):
     """Batched multi-scene march: 16 scenes, each its own blob field (8-32 blobs), 1-5 cascades
     of 128^3 and an AABB of size 0.5-16, ray counts log-uniform in 2^10..2^16, rays from a
@@ -703,8 +760,10 @@ def multi_scene_result(args, labels=("as_drawn", "scaled_2e19_samples")):
       * persistent: one work-stealing count launch and one emit launch for all scenes;
       * per-scene: tn_march_count + tn_march_emit once per scene.
     A second workload scales every scene's ray count by one factor so that the batch holds
-    about 2^19 samples. Per-scene counts and samples of the persistent launch are checked
-    bit-exact against the oracle by tests/test_gpu_multi_scene.py."""
+    about 2^19 samples. Each workload then times the fused losses over the packed samples of all
+    scenes, one launch against one per scene (_multi_scene_losses). Per-scene counts and samples of
+    the persistent launch, and the losses over all scenes, are checked against the oracle by
+    tests/test_gpu_multi_scene.py."""
     import torch
     from turbonerf_b200 import hotpath as hp, scenes
 
@@ -790,6 +849,7 @@ def multi_scene_result(args, labels=("as_drawn", "scaled_2e19_samples")):
             del g
         assert ctx.check() == 0 and ctx_s.check() == 0
         res["persistent_speedup"] = round(res["per_scene"]["ms"] / res["persistent"]["ms"], 3)
+        res["losses"] = _multi_scene_losses(args, ctx, ctx_s, table_in, R, ss, n_steps, offsets, samples)
         out[label] = res
     return out
 
@@ -1266,7 +1326,10 @@ def other_configs(args):
     ms = multi_scene_result(args, labels=("as_drawn",))["as_drawn"]
     out["multi_scene_16"] = {"n_rays": ms["n_rays"], "n_samples": ms["n_samples"],
                              "persistent_ms": ms["persistent"]["ms"], "per_scene_ms": ms["per_scene"]["ms"],
-                             "persistent_speedup": ms["persistent_speedup"]}
+                             "persistent_speedup": ms["persistent_speedup"],
+                             "losses_one_launch_ms": ms["losses"]["one_launch"]["ms"],
+                             "losses_per_scene_ms": ms["losses"]["per_scene"]["ms"],
+                             "losses_one_launch_speedup": ms["losses"]["one_launch_speedup"]}
     torch.cuda.empty_cache()
     bm = backward_memory_result(args)
     out["backward_memory_2e22"] = {v: {"extra_device_bytes": bm[v]["extra_device_bytes"], "ms": bm[v]["ms"]}

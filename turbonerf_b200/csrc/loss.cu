@@ -2028,7 +2028,8 @@ __device__ __noinline__ void train_losses_ray_long(const Samples& S, uint32_t r,
 // staging buffer (dynamic shared memory, 10.1 KB a warp); W warps a block (tn_tuning
 // loss_rays_per_block: 2, 4 or 8) and 16 / W blocks an SM (128 registers a thread) keep 16 rays
 // in flight per SM. VEC: 16-byte staging (every sample array 16-byte aligned, stride a multiple
-// of 4).
+// of 4). The grid is every resident warp (or fewer), each taking rays in turn: a batch of many
+// waves (the rays of several scenes) is one persistent launch.
 template <int W, bool VEC>
 __global__ void __launch_bounds__(W * WARP, 16 / W)
 train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, const uint32_t* __restrict__ counts,
@@ -2042,11 +2043,10 @@ train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t 
     const uint32_t n_live = live_rays(n_rays, n_dev);
     float inv_nrays = inv_nrays_host;
     if (inv_from) { const uint32_t nn = *inv_from; inv_nrays = nn ? 1.0f / (float)nn : 0.0f; }
-    const uint32_t nw = gridDim.x * W;
     const float lam = lambda > 0.0f ? lambda : 0.0f;
     float acc[2] = {0.0f, 0.0f};
     float* const sm = stage + (size_t)wid * SA_N * RB_PITCH;
-    for (uint32_t r = blockIdx.x * W + wid; r < n_live; r += nw) {
+    auto one_ray = [&](uint32_t r) {
         const uint32_t o = offsets[r], n = counts[r];
         const uint32_t span = n + (VEC ? (o & 3u) : 0u);  // slots the ray takes
         if (span <= RB_MAX)
@@ -2055,7 +2055,8 @@ train_losses_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t 
         else
             train_losses_ray_long(S, r, o, n, lane, min_t, inv_nrays, grad_scale, lam, target, bg, rs, ray_rgba,
                                   grad_density, drgb, acc[0], acc[1], sm, accumulate);
-    }
+    };
+    for (uint32_t r = blockIdx.x * W + wid; r < n_live; r += gridDim.x * W) one_ray(r);
     if (loss_sums) {
         acc[0] *= inv_nrays;
         block_sum_and_finish<2>(acc, partials, ticket, loss_sums, FinishScale{{1.0f, 1.0f}, n_dev, n_rays, 2u});
