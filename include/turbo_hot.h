@@ -431,6 +431,40 @@ int tn_synth_field(tn_stream_t stream, uint32_t n, const uint32_t* n_dev, uint32
                    float aabb_size, uint32_t n_blobs, const float* blobs, const float* waves, float* sigma,
                    float* rgb, uint32_t out_stride);
 
+/* ---- hash-grid encoding (the tiny-cuda-nn boundary) ---------------------------------
+ * The multiresolution hash encoding that the reference builds as tcnn's HashGrid
+ * (src/core/nerf-network.cu:27-124: 16 levels of 2 features, 2^19 entries a level, base
+ * resolution 16, per-level scale b = exp((ln 2048 aabb - ln 16) / 15), linear interpolation) and
+ * runs forward (:431-545) and backward (:668-768). Level l has resolution
+ * N_l = floor(base_resolution * per_level_scale^l); a normalised position x in [0,1]^3 takes the
+ * trilinear interpolation of the 2 features of its cell's 8 corner vertices; a level whose
+ * (N_l + 1)^3 vertices fit in its 2^log2_hashmap_size entries indexes them directly, the others
+ * by the spatial hash (x * 1 ^ y * 2654435761 ^ z * 805459861) mod 2^log2_hashmap_size.
+ * Parameters [level][2^log2_hashmap_size][2]; features [2 n_levels][stride]. */
+typedef struct tn_hashgrid_desc {
+    uint32_t n_levels;          /* 1..16 */
+    uint32_t log2_hashmap_size; /* entries a level = 2^log2_hashmap_size, 4..24 */
+    float base_resolution;      /* N_min >= 1 */
+    float per_level_scale;      /* b >= 1 */
+} tn_hashgrid_desc;
+/* Parameter counts: hash entries (n_levels 2^log2 2 floats) and the linear heads the trainer's
+ * hash-grid network adds (density and rgb from the 2 n_levels features: 4 (2 n_levels + 1)). */
+int tn_hashgrid_n_params(const tn_hashgrid_desc* desc, uint64_t* n_hash, uint32_t* n_head);
+/* Resolution of one level and whether it indexes its vertices directly (dense = 1). */
+int tn_hashgrid_level_resolution(const tn_hashgrid_desc* desc, uint32_t level, uint32_t* resolution, int* dense);
+/* features[2l + f][i] for the n (n_dev: live count, optional) positions pos[3][stride]. */
+int tn_hashgrid_encode(tn_stream_t stream, const tn_hashgrid_desc* desc, uint32_t n, const uint32_t* n_dev,
+                       uint32_t stride, const float* pos, const float* params, float* features);
+/* grads += d features / d params^T dL_dfeatures (atomic adds). With touched_bits (caller-zeroed,
+ * n_levels 2^log2 bits), touched_list and touched_count (zero on entry): every entry a live
+ * sample touches is listed once as l 2^log2 + index, in no particular order; its bit stays set. */
+int tn_hashgrid_backward(tn_stream_t stream, const tn_hashgrid_desc* desc, uint32_t n, const uint32_t* n_dev,
+                         uint32_t stride, const float* pos, const float* dL_dfeatures, float* grads,
+                         uint32_t* touched_bits, uint32_t* touched_list, uint32_t* touched_count);
+/* Zeroes the listed entries' gradients (both features) and bitmap words, then the count. */
+int tn_hashgrid_clear_touched(tn_stream_t stream, const uint32_t* touched_list, const uint32_t* touched_count,
+                              uint32_t max_entries, float* grads, uint32_t* touched_bits);
+
 /* ---- trainer: the controller surface ----------------------------------------------
  * Mirrors the reference's NeRFTrainingController / Trainer (src/controllers/
  * nerf-training-controller.h:23-89, src/core/trainer.cuh:21-70): setup, train_step(),
@@ -574,6 +608,13 @@ int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bit
  * one step's samples touch (and on every MLP weight), zero elsewhere; the built-in
  * network then leaves it unchanged, so every step feeds Adam the same sparse gradients. */
 int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_touched_out);
+/* Makes the hash-grid encoding with linear density and colour heads the trainer's network (in
+ * place of the synthetic producer): its parameters are the trainer's (hash entries in the grid
+ * section, which must hold them exactly; the heads at the start of the MLP section), its
+ * backward writes real gradients (the heads' over their parameters, the hash entries' by atomic
+ * adds after clearing the entries the previous step touched), and Adam skips the untouched
+ * hash entries as in the reference. Fused path only. */
+int tn_trainer_use_hashgrid(tn_trainer* tr, const tn_hashgrid_desc* desc);
 /* One training step (reference NeRFTrainingController::train_step,
  * nerf-training-controller.cu:185-212). With metrics == NULL the fused path only enqueues
  * (no host synchronisation); otherwise the call waits and fills the metrics.
@@ -686,7 +727,8 @@ int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out);
  * 20 ray t_max, 21 ray alive, 22 target rgba, 23 background rgb, 24 m_norm, 25 dt_norm,
  * 26 the dataset rays' draws [2][n_rays] (pixel, alpha selection; NULL without a dataset),
  * the last step's occupancy update inputs (occupancy_cells_per_step entries each): 27 levels,
- * 28 Morton cells, 29 network density values, 30 selection draws. */
+ * 28 Morton cells, 29 network density values, 30 selection draws; with the hash-grid network:
+ * 31 the entries its last backward touched, 32 their count (uint32). */
 int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes);
 
 #ifdef __cplusplus

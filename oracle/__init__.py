@@ -53,6 +53,10 @@ def _declare(L):
                                    ctypes.c_float, ctypes.c_double, ctypes.c_void_p)
     sig = {
         "orc_morton3d": (u32, [u32, u32, u32]),
+        "orc_hashgrid_encode": (None, [i32, i32, vp, vp, i64, i64, i64, vp, vp, vp]),
+        "orc_hashgrid_backward": (None, [i32, i32, vp, vp, i64, i64, i64, vp, vp, vp, vp]),
+        "orc_hash_heads_forward": (None, [i32, i64, i64, vp, vp, vp, vp, i64]),
+        "orc_hash_heads_backward": (None, [i32, i64, i64, vp, vp, vp, vp, vp, vp]),
         "orc_morton3d_invert": (u32, [u32]),
         "orc_fdiv_ru": (f32, [f32, f32]),
         "orc_num_threads": (i32, []),
@@ -376,3 +380,60 @@ def dataset_rays(n_rays, cameras, images, bbox, random, alpha_threshold=1.0, alp
                                   _p(out["img_id"]), _p(out["ori"]), _p(out["dir"]), _p(out["t"]), _p(out["t_max"]),
                                   _p(out["alive"]))
     return out, int(live)
+
+
+# ---- hash-grid encoding and linear heads --------------------------------------------------
+def hashgrid_levels(n_levels, log2_t, base_resolution, per_level_scale):
+    """Per-level resolution floor(N_min b^l) (double precision, from N_min and b as the FP32 values
+    the library's descriptor holds) and whether the level indexes its (res + 1)^3 vertices
+    directly."""
+    import math
+    base, b = float(np.float32(base_resolution)), float(np.float32(per_level_scale))
+    res = np.array([math.floor(base * math.pow(b, l)) for l in range(n_levels)], np.uint32)
+    dense = np.array([1 if (int(r) + 1) ** 3 <= (1 << log2_t) else 0 for r in res], np.int32)
+    return res, dense
+
+
+def hashgrid_encode(levels, log2_t, pos, params, n, pstride=None, stride=None):
+    """Features [2 L][stride] (float32, the library's operation order) of n positions [3][pstride]."""
+    res, dense = levels
+    pstride = pstride or n
+    stride = stride or n
+    feat = np.zeros(2 * len(res) * stride, np.float32)
+    lib().orc_hashgrid_encode(len(res), log2_t, _p(_c(res, np.uint32)), _p(_c(dense, np.int32)), n, pstride, stride,
+                              _p(_c(pos, np.float32)), _p(_c(params, np.float32)), _p(feat))
+    return feat
+
+
+def hashgrid_backward(levels, log2_t, pos, dfeat, n, pstride=None, stride=None):
+    """(grads [L][2^log2_t][2] float64, touched [L 2^log2_t] uint8) of dL/dfeatures [2 L][stride]."""
+    res, dense = levels
+    pstride = pstride or n
+    stride = stride or n
+    L = len(res)
+    grads = np.zeros(L * (1 << log2_t) * 2)
+    touched = np.zeros(L * (1 << log2_t), np.uint8)
+    lib().orc_hashgrid_backward(L, log2_t, _p(_c(res, np.uint32)), _p(_c(dense, np.int32)), n, pstride, stride,
+                                _p(_c(pos, np.float32)), _p(_c(dfeat, np.float64)), _p(grads), _p(touched))
+    return grads, touched
+
+
+def hash_heads_forward(nf, feat, head, n, stride=None, ostride=None):
+    """(density [n] float64, rgb [3][ostride] float64) of the linear heads [4][nf + 1]."""
+    stride = stride or n
+    ostride = ostride or n
+    density = np.zeros(n)
+    rgb = np.zeros(3 * ostride)
+    lib().orc_hash_heads_forward(nf, n, stride, _p(_c(feat, np.float32)), _p(_c(head, np.float32)), _p(density),
+                                 _p(rgb), ostride)
+    return density, rgb
+
+
+def hash_heads_backward(nf, feat, head, dL_ddensity, dL_drgb, n, stride=None):
+    """(dfeat [nf][stride] float64, dhead [4][nf + 1] float64)."""
+    stride = stride or n
+    dfeat = np.zeros(nf * stride)
+    dhead = np.zeros(4 * (nf + 1))
+    lib().orc_hash_heads_backward(nf, n, stride, _p(_c(feat, np.float32)), _p(_c(head, np.float32)),
+                                  _p(_c(dL_ddensity, np.float64)), _p(_c(dL_drgb, np.float64)), _p(dfeat), _p(dhead))
+    return dfeat, dhead

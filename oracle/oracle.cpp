@@ -1016,4 +1016,129 @@ int64_t orc_dataset_rays(int64_t n_rays, int64_t rs, int64_t n_images, int width
     return live;
 }
 
+
+// ---- hash-grid encoding and the linear heads (the tiny-cuda-nn boundary) -------------------
+// tcnn's HashGrid is not in the reference tree (the submodule is empty); this is the published
+// multiresolution hash encoding (Mueller et al. 2022, section 3) with the reference's settings
+// (src/core/nerf-network.cu:27-124): level l of resolution res[l] maps x in [0,1] to the cell
+// floor(x res) (clamped to [0, res - 1]) and f = x res - cell; the 8 corners' weights are
+// ((w_x w_y) w_z) with w = f or 1 - f (bit 0: x + 1, bit 1: y + 1, bit 2: z + 1); a level whose
+// (res + 1)^3 vertices fit in its 2^log2_t entries indexes them directly (x + (res + 1) (y +
+// (res + 1) z)), the others by (x * 1) ^ (y * 2654435761) ^ (z * 805459861) mod 2^log2_t. The
+// forward is FP32 in the same operation order as the library (features bit for bit), with the
+// corners' products summed by fused multiply-adds in corner order; the backward is FP64.
+static inline uint32_t orc_hg_index(uint32_t res, int dense, int log2_t, uint32_t x, uint32_t y, uint32_t z) {
+    if (dense) {
+        const uint32_t r = res + 1u;
+        return x + r * (y + r * z);
+    }
+    return ((x * 1u) ^ (y * 2654435761u) ^ (z * 805459861u)) & ((1u << log2_t) - 1u);
+}
+
+static inline void orc_hg_corners(uint32_t res, int dense, int log2_t, float px, float py, float pz,
+                                  uint32_t idx[8], float w[8]) {
+    const float p[3] = {px, py, pz};
+    uint32_t i[3];
+    float f[3], g[3];
+    for (int d = 0; d < 3; ++d) {
+        const float s = p[d] * (float)res;
+        const float fl = std::fmin(std::fmax(std::floor(s), 0.0f), (float)(res - 1u));
+        i[d] = (uint32_t)fl;
+        f[d] = s - fl;
+        g[d] = 1.0f - f[d];
+    }
+    for (int k = 0; k < 8; ++k) {
+        const int bx = k & 1, by = (k >> 1) & 1, bz = (k >> 2) & 1;
+        idx[k] = orc_hg_index(res, dense, log2_t, i[0] + bx, i[1] + by, i[2] + bz);
+        const float wxy = (bx ? f[0] : g[0]) * (by ? f[1] : g[1]);
+        w[k] = wxy * (bz ? f[2] : g[2]);
+    }
+}
+
+// feat[2 l + c][stride] for n positions pos[3][pstride]; params [L][2^log2_t][2].
+void orc_hashgrid_encode(int n_levels, int log2_t, const uint32_t* res, const int* dense, int64_t n, int64_t pstride,
+                         int64_t stride, const float* pos, const float* params, float* feat) {
+    const size_t T = (size_t)1 << log2_t;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < n; ++s) {
+        for (int l = 0; l < n_levels; ++l) {
+            uint32_t idx[8];
+            float w[8];
+            orc_hg_corners(res[l], dense[l], log2_t, pos[s], pos[s + pstride], pos[s + 2 * pstride], idx, w);
+            const float* P = params + (size_t)l * T * 2;
+            float a0 = 0.0f, a1 = 0.0f;
+            for (int k = 0; k < 8; ++k) {
+                a0 = std::fmaf(w[k], P[2 * (size_t)idx[k]], a0);
+                a1 = std::fmaf(w[k], P[2 * (size_t)idx[k] + 1], a1);
+            }
+            feat[(size_t)(2 * l) * stride + s] = a0;
+            feat[(size_t)(2 * l + 1) * stride + s] = a1;
+        }
+    }
+}
+
+// grads[l][entry][c] += w_k dfeat[2 l + c][s] over every live sample and corner (FP64, serial);
+// touched[l 2^log2_t + entry] = 1 for every entry a sample touches.
+void orc_hashgrid_backward(int n_levels, int log2_t, const uint32_t* res, const int* dense, int64_t n,
+                           int64_t pstride, int64_t stride, const float* pos, const double* dfeat, double* grads,
+                           uint8_t* touched) {
+    const size_t T = (size_t)1 << log2_t;
+    for (int64_t s = 0; s < n; ++s) {
+        for (int l = 0; l < n_levels; ++l) {
+            uint32_t idx[8];
+            float w[8];
+            orc_hg_corners(res[l], dense[l], log2_t, pos[s], pos[s + pstride], pos[s + 2 * pstride], idx, w);
+            const double g0 = dfeat[(size_t)(2 * l) * stride + s], g1 = dfeat[(size_t)(2 * l + 1) * stride + s];
+            for (int k = 0; k < 8; ++k) {
+                const size_t e = (size_t)l * T + idx[k];
+                grads[2 * e] += (double)w[k] * g0;
+                grads[2 * e + 1] += (double)w[k] * g1;
+                if (touched) touched[e] = 1;
+            }
+        }
+    }
+}
+
+// Linear heads (FP64): z_o = b_o + W_o . f over nf features ([nf][stride]); head parameters
+// [4][nf + 1] (weights, then the bias): density = z_0, rgb_c = sigmoid(z_{c+1}).
+void orc_hash_heads_forward(int nf, int64_t n, int64_t stride, const float* feat, const float* head, double* density,
+                            double* rgb, int64_t ostride) {
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < n; ++s) {
+        for (int o = 0; o < 4; ++o) {
+            double z = head[o * (nf + 1) + nf];
+            for (int j = 0; j < nf; ++j) z += (double)head[o * (nf + 1) + j] * (double)feat[(size_t)j * stride + s];
+            if (o == 0) density[s] = z;
+            else if (rgb) rgb[(size_t)(o - 1) * ostride + s] = 1.0 / (1.0 + std::exp(-z));
+        }
+    }
+}
+
+// The heads' backward (FP64): dfeat[nf][stride] and the head parameters' gradients [4][nf + 1]
+// (summed over the n samples) from dL/d density and dL/d rgb ([3][stride]).
+void orc_hash_heads_backward(int nf, int64_t n, int64_t stride, const float* feat, const float* head,
+                             const double* dL_ddensity, const double* dL_drgb, double* dfeat, double* dhead) {
+    for (int k = 0; k < 4 * (nf + 1); ++k) dhead[k] = 0.0;
+    for (int64_t s = 0; s < n; ++s) {
+        double dz[4];
+        dz[0] = dL_ddensity[s];
+        for (int c = 0; c < 3; ++c) {
+            double z = head[(c + 1) * (nf + 1) + nf];
+            for (int j = 0; j < nf; ++j)
+                z += (double)head[(c + 1) * (nf + 1) + j] * (double)feat[(size_t)j * stride + s];
+            const double y = 1.0 / (1.0 + std::exp(-z));
+            dz[c + 1] = dL_drgb[(size_t)c * stride + s] * y * (1.0 - y);
+        }
+        for (int j = 0; j < nf; ++j) {
+            double g = 0.0;
+            for (int o = 0; o < 4; ++o) g += dz[o] * (double)head[o * (nf + 1) + j];
+            dfeat[(size_t)j * stride + s] = g;
+        }
+        for (int o = 0; o < 4; ++o) {
+            for (int j = 0; j < nf; ++j) dhead[o * (nf + 1) + j] += dz[o] * (double)feat[(size_t)j * stride + s];
+            dhead[o * (nf + 1) + nf] += dz[o];
+        }
+    }
+}
+
 }  // extern "C"

@@ -104,6 +104,13 @@ int launch_adam(cudaStream_t stream, bool plain, uint32_t n, uint32_t n_grid, ui
                 float lr, const float* lr_dev, float beta1, float beta2, float epsilon, float l2_reg, float* weights,
                 float* weights_copy, const float* gradients, float* first_moments, float* second_moments,
                 uint32_t* param_steps, const AdamPlacement& place = AdamPlacement{});
+// The hash-grid network (hashgrid.cu) over params [hash entries | heads], for batches of up to
+// cap samples and density queries of up to qcap; *handle owns its buffers.
+int hashnet_create(const tn_hashgrid_desc* desc, const float* params, uint32_t cap, uint32_t qcap, tn_network* out,
+                   void** handle);
+void hashnet_destroy(void* handle);
+// Device count (and *list) of the entries the network's last backward touched.
+const uint32_t* hashnet_touched(void* handle, const uint32_t** list);
 // tn_train_losses; accumulate false writes the merged density gradient over grad_density.
 int train_losses(tn_ctx* ctx, cudaStream_t stream, const tn_ray_batch* batch, int activation, float min_transmittance,
                  float inv_nrays, const uint32_t* inv_nrays_from_dev, float grad_scale, float lambda,

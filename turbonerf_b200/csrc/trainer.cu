@@ -125,6 +125,7 @@ struct tn_trainer {
     tn_trainer_desc d{};
     tn_network net{};
     SynthNet synth;
+    void* hashnet = nullptr;  // the built-in hash-grid network, when it is the trainer's network
     cudaStream_t stream = nullptr;
     // the occupancy query and update beside the training chain, and the next step's head
     cudaStream_t aux = nullptr, cstream = nullptr;
@@ -790,6 +791,7 @@ int tn_trainer_destroy(tn_trainer* tr) {
     if (!tr) return TN_OK;
     if (tr->stream) cudaStreamSynchronize(tr->stream);
     drop_graphs(tr);
+    if (tr->hashnet) hashnet_destroy(tr->hashnet);
     for (void* p : tr->allocs) cudaFree(p);
     if (tr->synth.blobs) cudaFree(tr->synth.blobs);
     if (tr->synth.waves) cudaFree(tr->synth.waves);
@@ -837,6 +839,31 @@ int tn_trainer_set_grid(tn_trainer* tr, const float* density, const uint8_t* bit
     if (st == TN_OK && bitfield) st = cuda_status(cudaMemcpyAsync(tr->bits, bitfield, tr->V, cudaMemcpyHostToDevice, tr->stream), "bits copy");
     if (st == TN_OK) st = cuda_status(cudaStreamSynchronize(tr->stream), "set_grid sync");
     return st;
+}
+
+int tn_trainer_use_hashgrid(tn_trainer* tr, const tn_hashgrid_desc* desc) {
+    TN_NONNULL(tr);
+    TN_REQUIRE(tr->d.path == TN_PATH_FUSED, TN_E_STATE, "the hash-grid network runs on the fused path");
+    uint64_t n_hash = 0;
+    uint32_t n_head = 0;
+    int st = tn_hashgrid_n_params(desc, &n_hash, &n_head);
+    if (st != TN_OK) return st;
+    TN_REQUIRE(n_hash == tr->d.n_grid_params, TN_E_INVALID,
+               "hash-grid entries take %llu parameters, the trainer's grid section %u",
+               (unsigned long long)n_hash, tr->d.n_grid_params);
+    TN_REQUIRE(n_head <= tr->d.n_mlp_params, TN_E_INVALID, "the heads take %u parameters, the trainer's MLP section %u",
+               n_head, tr->d.n_mlp_params);
+    st = settle(tr);
+    if (st != TN_OK) return st;
+    tn_network net{};
+    void* handle = nullptr;
+    st = hashnet_create(desc, tr->w, tr->B, std::max(tr->M, 1u), &net, &handle);
+    if (st != TN_OK) return st;
+    if (tr->hashnet) hashnet_destroy(tr->hashnet);
+    tr->hashnet = handle;
+    tr->net = net;
+    drop_graphs(tr);  // the captured graphs hold the previous network's launches
+    return cuda_status(cudaMemsetAsync(tr->g, 0, (size_t)tr->P * 4, tr->stream), "hash-grid: gradients");
 }
 
 int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_touched_out) {
@@ -1485,6 +1512,19 @@ int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes) {
         case 28: p = tr->occ_cells; n = 4ull * tr->M; break;
         case 29: p = tr->occ_values; n = 4ull * tr->M; break;
         case 30: p = tr->occ_rsel; n = 4ull * tr->M; break;
+        case 31: {  // the hash-grid network's touched-entry list and its count
+            const uint32_t* list = nullptr;
+            const uint32_t* count = tr->hashnet ? hashnet_touched(tr->hashnet, &list) : nullptr;
+            p = const_cast<uint32_t*>(list);
+            n = list ? 4ull * (tr->d.n_grid_params / 2) : 0;
+            (void)count;
+            break;
+        }
+        case 32: {
+            p = tr->hashnet ? const_cast<uint32_t*>(hashnet_touched(tr->hashnet, nullptr)) : nullptr;
+            n = p ? 4 : 0;
+            break;
+        }
         default: return fail(TN_E_INVALID, "unknown trainer buffer %d", which);
     }
     *ptr = p;

@@ -568,3 +568,70 @@ def backward_store(ctx, rb: RayBatchDesc, density, rgb, dt, m_norm, dt_norm, gra
                                     activation=activation)
     _, ddist, _ = plain_distortion(rb, density, m_norm, dt_norm, lam, activation=activation)
     return dd, drgb, ddist
+
+
+# ---- hash-grid encoding (the tiny-cuda-nn boundary) ----------------------------------------
+@dataclass
+class HashgridSpec:
+    """Multiresolution hash encoding: level l of resolution floor(base_resolution *
+    per_level_scale^l), 2 features a level, 2^log2_hashmap_size entries a level."""
+    n_levels: int = 16
+    log2_hashmap_size: int = 19
+    base_resolution: float = 16.0
+    per_level_scale: float = 2.0
+
+    @classmethod
+    def reference(cls, aabb_scale: float = 1.0, log2_hashmap_size: int = 19) -> "HashgridSpec":
+        """The reference's density encoding (src/core/nerf-network.cu:87-106): 16 levels from 16 to
+        2048 * aabb_scale."""
+        import math
+        n_max = 2048.0 * max(1.0, float(aabb_scale))
+        return cls(16, log2_hashmap_size, 16.0, math.exp((math.log(n_max) - math.log(16.0)) / 15.0))
+
+    def desc(self):
+        return native.HashgridDesc(self.n_levels, self.log2_hashmap_size, float(self.base_resolution),
+                                   float(self.per_level_scale))
+
+    @property
+    def n_features(self) -> int:
+        return 2 * self.n_levels
+
+    def n_params(self):
+        """(hash entries' floats, the linear heads' floats)."""
+        nh, nm = ctypes.c_uint64(0), ctypes.c_uint32(0)
+        call("tn_hashgrid_n_params", ctypes.byref(self.desc()), ctypes.byref(nh), ctypes.byref(nm))
+        return nh.value, nm.value
+
+    def level(self, l: int):
+        """(resolution, dense) of level l as the library computes them."""
+        r, d = ctypes.c_uint32(0), ctypes.c_int(0)
+        call("tn_hashgrid_level_resolution", ctypes.byref(self.desc()), l, ctypes.byref(r), ctypes.byref(d))
+        return r.value, bool(d.value)
+
+
+def hashgrid_encode(spec: HashgridSpec, pos, params, n, stride, n_dev=None, out=None):
+    """Features [2 L][stride] (float32) of n positions pos[3][stride] in [0, 1]."""
+    if out is None:
+        out = torch.zeros(spec.n_features * stride, dtype=torch.float32, device=pos.device)
+    call("tn_hashgrid_encode", _stream(), ctypes.byref(spec.desc()), n, _ptr(n_dev), stride, _ptr(pos), _ptr(params),
+         _ptr(out))
+    return out
+
+
+def hashgrid_backward(spec: HashgridSpec, pos, dfeat, grads, n, stride, n_dev=None, touched=True):
+    """grads += the encoding's transpose applied to dfeat [2 L][stride]. With touched: returns
+    (bits, list, count) of the entries the n samples touched (fresh buffers)."""
+    bits = lst = count = None
+    if touched:
+        entries = spec.n_levels << spec.log2_hashmap_size
+        bits = torch.zeros((entries + 31) // 32, dtype=torch.int32, device=pos.device)
+        lst = torch.zeros(entries, dtype=torch.int32, device=pos.device)
+        count = torch.zeros(1, dtype=torch.int32, device=pos.device)
+    call("tn_hashgrid_backward", _stream(), ctypes.byref(spec.desc()), n, _ptr(n_dev), stride, _ptr(pos), _ptr(dfeat),
+         _ptr(grads), _ptr(bits), _ptr(lst), _ptr(count))
+    return bits, lst, count
+
+
+def hashgrid_clear_touched(lst, count, grads, bits, max_entries=None):
+    call("tn_hashgrid_clear_touched", _stream(), _ptr(lst), _ptr(count),
+         int(max_entries if max_entries is not None else lst.numel()), _ptr(grads), _ptr(bits))

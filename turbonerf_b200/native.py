@@ -64,6 +64,11 @@ class GridDesc(ctypes.Structure):
                 ("reserved", ctypes.c_int32)]
 
 
+class HashgridDesc(ctypes.Structure):
+    _fields_ = [("n_levels", ctypes.c_uint32), ("log2_hashmap_size", ctypes.c_uint32),
+                ("base_resolution", ctypes.c_float), ("per_level_scale", ctypes.c_float)]
+
+
 class MarchDesc(ctypes.Structure):
     _fields_ = [("cone_angle", ctypes.c_float), ("dt_min", ctypes.c_float), ("dt_max", ctypes.c_float),
                 ("max_steps", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32)]
@@ -241,6 +246,12 @@ SIGNATURES = {
     "tn_trainer_set_synthetic_field": [_vp, _u32, _vp, _vp],
     "tn_trainer_set_grid": [_vp, _vp, _vp],
     "tn_trainer_init_synthetic_gradients": [_vp, _f32, _P(_u32)],
+    "tn_trainer_use_hashgrid": [_vp, _vp],
+    "tn_hashgrid_n_params": [_vp, _P(_u64), _P(_u32)],
+    "tn_hashgrid_level_resolution": [_vp, _u32, _P(_u32), _P(_i32)],
+    "tn_hashgrid_encode": [_vp, _vp, _u32, _vp, _u32, _vp, _vp, _vp],
+    "tn_hashgrid_backward": [_vp, _vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp],
+    "tn_hashgrid_clear_touched": [_vp, _vp, _vp, _u32, _vp, _vp],
     "tn_trainer_train_step": [_vp, _vp],
     "tn_trainer_train_step_rays": [_vp, _u32, _vp, _vp, _vp, _vp, _vp],
     "tn_trainer_train_step_rays_pipelined": [_vp, _u32, _vp, _vp, _vp, _vp, _vp],

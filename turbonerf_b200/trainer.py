@@ -180,6 +180,19 @@ class Trainer:
         call("tn_trainer_init_synthetic_gradients", h, float(synthetic_grad_std), ctypes.byref(touched))
         self.n_touched_grads = touched.value
 
+    def use_hashgrid(self, spec=None) -> None:
+        """Trains the multiresolution hash encoding with linear density and colour heads as the
+        network (in place of the synthetic producer): real parameter gradients each step, the
+        hash entries a step touches listed (trainer buffers 31 and 32). The trainer's grid section
+        must hold the encoding's entries exactly (n_grid_params = 2 n_levels 2^log2_hashmap_size)
+        and its MLP section the heads. spec: a hotpath.HashgridSpec (default: the reference's
+        encoding for this NeRF's box size)."""
+        from .hotpath import HashgridSpec
+        if spec is None:
+            spec = HashgridSpec.reference(self.nerf.bounding_box.size())
+        call("tn_trainer_use_hashgrid", self._handle(), ctypes.byref(spec.desc()))
+        self.hashgrid = spec
+
     def _upload_grid(self) -> None:
         """The NeRF's initial occupancy grid (densities and/or bitfield), when it has one."""
         n = self.nerf
