@@ -908,6 +908,96 @@ def run_losses(args):
     print(json.dumps(out), flush=True)
 
 
+def hashgrid_result(args):
+    """The hash-grid encoding of the reference (16 levels of 2 features, 2^19 entries a level,
+    resolutions 16..2048 x 16 for the train step's 16-unit box) on 2^18 uniform positions: the
+    encode and the backward (with the touched-entry list) alone, CUDA events over 20 launches after
+    warm-up (the 64 MB table stays in L2 between launches); then the full train step of the
+    train-step workload with the hash-grid network (and its linear heads) as the trainer's network
+    instead of the synthetic stand-in: real gradients, Adam over the entries they touch, CUDA graph,
+    count-ahead schedule."""
+    import torch
+    from turbonerf_b200 import hotpath as hp
+    from turbonerf_b200.replicas import replica_seed
+    torch.cuda.set_device(0)
+    spec = hp.HashgridSpec.reference(16.0)
+    n_hash, n_head = spec.n_params()
+    rng = np.random.default_rng(0x7C6)
+    n = 1 << 18
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    pos = d(rng.uniform(0.0, 1.0, 3 * n).astype(np.float32))
+    params = d(rng.uniform(-1e-4, 1e-4, n_hash).astype(np.float32))
+    feat = torch.zeros(spec.n_features * n, device="cuda")
+    dfeat = d(rng.normal(0.0, 1e-3, spec.n_features * n).astype(np.float32))
+    grads = torch.zeros(n_hash, device="cuda")
+    entries = spec.n_levels << spec.log2_hashmap_size
+    bits = torch.zeros((entries + 31) // 32, dtype=torch.int32, device="cuda")
+    lst = torch.zeros(entries, dtype=torch.int32, device="cuda")
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = {"workload": "hash-grid encoding, 16 levels x 2^19 x 2, 2^18 positions", "n": n}
+
+    def timed(fn, before=None):
+        for _ in range(3):
+            if before:
+                before()
+            fn()
+        ts = []
+        for _ in range(20):
+            if before:
+                before()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    ms = timed(lambda: hp.hashgrid_encode(spec, pos, params, n, n, out=feat))
+    out["encode"] = {"ms": round(ms, 4), "samples_per_s": round(n / (ms / 1e3), 1)}
+
+    def backward():
+        import ctypes
+        from turbonerf_b200.native import call
+        from turbonerf_b200.hotpath import _ptr, _stream
+        call("tn_hashgrid_backward", _stream(), ctypes.byref(spec.desc()), n, None, n, _ptr(pos), _ptr(dfeat),
+             _ptr(grads), _ptr(bits), _ptr(lst), _ptr(count))
+
+    ms = timed(backward, before=lambda: hp.hashgrid_clear_touched(lst, count, grads, bits))
+    out["backward"] = {"ms": round(ms, 4), "samples_per_s": round(n / (ms / 1e3), 1),
+                       "touched_entries": int(count.item())}
+    # the train step with the hash-grid network
+    scene = _scene(0x7B0)
+    tr = _trainer(scene, "fused", replica_seed(0x7B0, 0))
+    tr.use_hashgrid(spec)
+    tr.autotune()
+    steps = max(args.steps // 2, 10)
+    for _ in range(max(args.warmup, 3)):
+        tr.train_step_async()
+    m0 = tr.sync_metrics()
+    stream = torch.cuda.ExternalStream(tr.stream_handle())
+    s0 = tr.stat(3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        tr.train_step_async()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    m = tr.sync_metrics()
+    samples = tr.stat(3) - s0
+    out["train_step"] = {"ms_per_step": round(ms / steps, 4), "samples_per_s": round(samples / (ms / 1e3), 1),
+                         "steps": steps, "loss_first": round(float(m0.loss), 6), "loss_last": round(float(m.loss), 6),
+                         "touched_entries_last_step": int(tr.buffer(32, np.uint32)[0].item())}
+    tr.teardown()
+    return out
+
+
+def run_hashgrid(args):
+    print(json.dumps(hashgrid_result(args)), flush=True)
+
+
 def run_kernel_tour(args):
     """Every kernel of the library, launched at representative sizes, for profiling (for instance
     `ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum`, one pass per
@@ -1311,8 +1401,10 @@ def other_configs(args):
     """The smaller configurations beside the train step, for the default bench line: GPU and
     CPU-oracle samples/s of the forward march + composite (1 cascade, 4096 rays) and of the
     compositor + distortion forward/backward at 2^18 samples; the batched multi-scene march
-    (16 scenes, 128^3, 2^10..2^16 rays a scene), persistent launch against one launch per scene;
-    the device memory of the recompute and store backwards at 2^22 samples."""
+    (16 scenes, 128^3, 2^10..2^16 rays a scene), persistent launch against one launch per scene,
+    and its fused losses in one launch against one per scene; the train step with the hash-grid
+    network instead of the synthetic stand-in; the device memory of the recompute and store
+    backwards at 2^22 samples."""
     import torch
     cfg = configs_result(args)
     rows = {c["config"]: c for c in cfg["configs"]}
@@ -1330,6 +1422,11 @@ def other_configs(args):
                              "losses_one_launch_ms": ms["losses"]["one_launch"]["ms"],
                              "losses_per_scene_ms": ms["losses"]["per_scene"]["ms"],
                              "losses_one_launch_speedup": ms["losses"]["one_launch_speedup"]}
+    torch.cuda.empty_cache()
+    hg = hashgrid_result(args)
+    out["hashgrid_network_step"] = {"samples_per_s": hg["train_step"]["samples_per_s"],
+                                    "ms_per_step": hg["train_step"]["ms_per_step"],
+                                    "encode_ms_2e18": hg["encode"]["ms"], "backward_ms_2e18": hg["backward"]["ms"]}
     torch.cuda.empty_cache()
     bm = backward_memory_result(args)
     out["backward_memory_2e22"] = {v: {"extra_device_bytes": bm[v]["extra_device_bytes"], "ms": bm[v]["ms"]}
@@ -1354,14 +1451,15 @@ def main():
                     help="render workload: sample budgets per round (0: the library default)")
     ap.add_argument("--workload", default="train-step",
                     choices=["train-step", "backward-memory", "multi-scene", "kernel-tour", "render", "dataset-rays", "configs",
-                             "compositor", "losses"],
+                             "compositor", "losses", "hashgrid"],
                     help="backward-memory: the recompute-vs-store study of the compositor and distortion backward; "
                          "multi-scene: the batched persistent march of 16 scenes against one launch per scene; "
                          "kernel-tour: every kernel once at representative sizes, for profiling; "
                          "render: inference frames through Renderer.submit; "
                          "dataset-rays: training rays from posed images; "
                          "configs: GPU and CPU oracle on the smaller configurations; "
-                         "compositor: the compositor tile kernels alone; losses: the fused loss kernel alone")
+                         "compositor: the compositor tile kernels alone; losses: the fused loss kernel alone; "
+                         "hashgrid: the hash-grid encoding and the train step with it as the network")
     args = ap.parse_args()
     if args.workload == "backward-memory":
         run_backward_memory(args)
@@ -1379,6 +1477,8 @@ def main():
         run_compositor(args)
     elif args.workload == "losses":
         run_losses(args)
+    elif args.workload == "hashgrid":
+        run_hashgrid(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

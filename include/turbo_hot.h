@@ -612,8 +612,8 @@ int tn_trainer_init_synthetic_gradients(tn_trainer* tr, float std, uint32_t* n_t
  * place of the synthetic producer): its parameters are the trainer's (hash entries in the grid
  * section, which must hold them exactly; the heads at the start of the MLP section), its
  * backward writes real gradients (the heads' over their parameters, the hash entries' by atomic
- * adds after clearing the entries the previous step touched), and Adam skips the untouched
- * hash entries as in the reference. Fused path only. */
+ * adds into a cleared gradient section) and lists the hash entries with a nonzero gradient; Adam
+ * skips the others as in the reference. Fused path only. */
 int tn_trainer_use_hashgrid(tn_trainer* tr, const tn_hashgrid_desc* desc);
 /* One training step (reference NeRFTrainingController::train_step,
  * nerf-training-controller.cu:185-212). With metrics == NULL the fused path only enqueues
@@ -728,7 +728,8 @@ int tn_trainer_stream(tn_trainer* tr, tn_stream_t* out);
  * 26 the dataset rays' draws [2][n_rays] (pixel, alpha selection; NULL without a dataset),
  * the last step's occupancy update inputs (occupancy_cells_per_step entries each): 27 levels,
  * 28 Morton cells, 29 network density values, 30 selection draws; with the hash-grid network:
- * 31 the entries its last backward touched, 32 their count (uint32). */
+ * 31 the hash entries with a nonzero gradient after the last step (l 2^log2 + index, in no
+ * particular order; the entries Adam updates), 32 their count (uint32). */
 int tn_trainer_buffer(tn_trainer* tr, int which, void** ptr, uint64_t* bytes);
 
 #ifdef __cplusplus

@@ -132,26 +132,84 @@ hg_encode_kernel(HashLevels H, uint32_t n, const uint32_t* __restrict__ n_dev, u
 }
 
 // One thread per (sample, level): w_c * dL/dfeature into the corners' entries; each entry a live
-// sample touches is listed once (bitmap word atomically or-ed; the thread that set the bit
-// appends the entry l T + idx).
-__global__ void __launch_bounds__(256)
+// sample touches is listed once (the thread whose atomic or set the entry's bit appends l T + idx).
+// Contention is cut three ways: a bit already set is seen with a plain read and skips its atomic;
+// the warp's new entries take one counter atomic for the warp; and on levels of resolution up to
+// HG_SHARE_RES, where neighbouring samples (consecutive along a ray) share corners, the lanes of a
+// warp with the same entry add their contributions in shared memory and one of them makes the
+// atomic add.
+constexpr int HG_BWD_THREADS = 256;
+constexpr uint32_t HG_SHARE_RES = 8192;
+__global__ void __launch_bounds__(HG_BWD_THREADS)
 hg_backward_kernel(HashLevels H, uint32_t n, const uint32_t* __restrict__ n_dev, uint32_t pstride, uint32_t stride,
                    const float* __restrict__ pos, const float* __restrict__ dfeat, float2* __restrict__ grads,
                    uint32_t* __restrict__ bits, uint32_t* __restrict__ list, uint32_t* __restrict__ count) {
+    __shared__ float2 share[HG_BWD_THREADS];
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     const int l = blockIdx.y;
-    if (s >= live_count(n, n_dev)) return;
+    const int lane = threadIdx.x & 31;
+    const bool live = s < live_count(n, n_dev);
+    const unsigned active = __ballot_sync(FULL_MASK, live);  // the warp's lanes that continue together
+    if (!live) return;
     HashCorners c;
     hg_corners(H, l, pos[s], pos[s + pstride], pos[s + 2 * (size_t)pstride], c);
     const float g0 = dfeat[(size_t)(HG_F * l) * stride + s], g1 = dfeat[(size_t)(HG_F * l + 1) * stride + s];
     const uint32_t base = (uint32_t)l << H.log2_t;
+    const bool share_level = H.res[l] <= HG_SHARE_RES;  // the same for the whole block
+    // the gradient adds of all 8 corners (reductions without a result: nothing waits for them)
+    bool lead[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        atomicAdd(grads + base + c.idx[k], make_float2(__fmul_rn(c.w[k], g0), __fmul_rn(c.w[k], g1)));
-        if (bits) {
-            const uint32_t e = base + c.idx[k], bit = 1u << (e & 31u);
-            if (!(atomicOr(bits + (e >> 5), bit) & bit)) list[atomicAdd(count, 1u)] = e;
+        float2 v = make_float2(__fmul_rn(c.w[k], g0), __fmul_rn(c.w[k], g1));
+        lead[k] = true;
+        if (share_level) {
+            const unsigned peers = __match_any_sync(active, c.idx[k]);
+            share[threadIdx.x] = v;
+            __syncwarp(active);
+            lead[k] = lane == __ffs(peers) - 1;
+            if (lead[k]) {
+                for (unsigned rest = peers & (peers - 1u); rest; rest &= rest - 1u) {
+                    const float2 o = share[(threadIdx.x & ~31u) + (uint32_t)(__ffs(rest) - 1)];
+                    v.x += o.x;
+                    v.y += o.y;
+                }
+            }
+            __syncwarp(active);
         }
+        if (lead[k]) atomicAdd(grads + base + c.idx[k], v);
+    }
+    if (!bits) return;
+    // touched entries: every corner's bitmap word read at once, then the atomic ors of the bits
+    // still clear, then one counter atomic for the warp's new entries of all 8 corners
+    uint32_t e[8], word[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        e[k] = base + c.idx[k];
+        word[k] = lead[k] ? bits[e[k] >> 5] : ~0u;
+    }
+    bool fresh[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t bit = 1u << (e[k] & 31u);
+        fresh[k] = !(word[k] & bit) && !(atomicOr(bits + (e[k] >> 5), bit) & bit);
+    }
+    unsigned news[8];
+    uint32_t total = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        news[k] = __ballot_sync(active, fresh[k]);
+        total += (uint32_t)__popc(news[k]);
+    }
+    if (total == 0) return;
+    const int first = __ffs(active) - 1;
+    uint32_t at = 0;
+    if (lane == first) at = atomicAdd(count, total);
+    at = __shfl_sync(active, at, first);
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (fresh[k]) list[at + (uint32_t)__popc(news[k] & below)] = e[k];
+        at += (uint32_t)__popc(news[k]);
     }
 }
 
@@ -165,6 +223,49 @@ __global__ void hg_clear_kernel(const uint32_t* __restrict__ list, const uint32_
         grads[e] = make_float2(0.0f, 0.0f);
         if (bits) bits[e >> 5] = 0u;
     }
+}
+
+// Entries with a nonzero gradient (either feature), listed in no particular order: each thread
+// takes 8 consecutive entries (four 16-byte loads), a block ranks its nonzero entries with a scan of
+// the warps' counts and takes their places with one counter atomic.
+constexpr int HG_NZ_THREADS = 256;
+__global__ void __launch_bounds__(HG_NZ_THREADS)
+hg_nonzero_kernel(uint32_t n_entries, const float4* __restrict__ grads, uint32_t* __restrict__ list,
+                  uint32_t* __restrict__ count) {
+    __shared__ uint32_t warp_n[HG_NZ_THREADS / WARP];
+    __shared__ uint32_t block_at;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t e0 = (blockIdx.x * HG_NZ_THREADS + threadIdx.x) * 8u;
+    uint32_t mask = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (e0 + 2u * q < n_entries) {  // n_entries is even: the pair's second entry exists too
+            const float4 v = grads[e0 / 2u + q];
+            if (v.x != 0.0f || v.y != 0.0f) mask |= 1u << (2 * q);
+            if (v.z != 0.0f || v.w != 0.0f) mask |= 1u << (2 * q + 1);
+        }
+    }
+    const uint32_t mine = (uint32_t)__popc(mask);
+    uint32_t incl = mine;
+#pragma unroll
+    for (int d = 1; d < WARP; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(FULL_MASK, incl, d);
+        if (lane >= d) incl += o;
+    }
+    if (lane == WARP - 1) warp_n[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < HG_NZ_THREADS / WARP; ++w) {
+            const uint32_t c = warp_n[w];
+            warp_n[w] = t;
+            t += c;
+        }
+        block_at = t ? atomicAdd(count, t) : 0u;
+    }
+    __syncthreads();
+    uint32_t at = block_at + warp_n[wid] + incl - mine;
+    for (uint32_t m = mask; m; m &= m - 1u) list[at++] = e0 + (uint32_t)(__ffs(m) - 1);
 }
 
 // ---- linear heads (the stand-in for tcnn's density and colour MLPs) ------------------------
@@ -283,8 +384,8 @@ int hashgrid_backward(cudaStream_t stream, const tn_hashgrid_desc* desc, uint32_
     HashLevels H;
     int st = hash_levels(desc, H);
     if (st != TN_OK || n == 0) return st;
-    const dim3 grid((n + 255) / 256, H.n_levels);
-    hg_backward_kernel<<<grid, 256, 0, stream>>>(H, n, n_dev, pstride, stride, pos, dL_dfeatures,
+    const dim3 grid((n + HG_BWD_THREADS - 1) / HG_BWD_THREADS, H.n_levels);
+    hg_backward_kernel<<<grid, HG_BWD_THREADS, 0, stream>>>(H, n, n_dev, pstride, stride, pos, dL_dfeatures,
                                                  reinterpret_cast<float2*>(grads), touched_bits, touched_list,
                                                  touched_count);
     return check_launch("tn_hashgrid_backward");
@@ -311,13 +412,12 @@ struct HashNet {
     float* dfeat = nullptr;      // [2L][cap]
     float* qfeat = nullptr;      // [2L][qcap] features of density queries
     float* partials = nullptr;   // [blocks][HG_HEAD_SLOTS]
-    uint32_t* bits = nullptr;    // [L T / 32]
     uint32_t* list = nullptr;    // [L T]
     uint32_t* count = nullptr;   // [1]
     uint32_t cap = 0, qcap = 0;
     ~HashNet() {
         cudaFree(feat); cudaFree(dfeat); cudaFree(qfeat); cudaFree(partials);
-        cudaFree(bits); cudaFree(list); cudaFree(count);
+        cudaFree(list); cudaFree(count);
     }
 };
 
@@ -353,8 +453,11 @@ static int hashnet_backward(void* user, tn_stream_t stream, uint32_t n, const ui
                             float* param_grads) {
     auto* h = static_cast<HashNet*>(user);
     cudaStream_t s = (cudaStream_t)stream;
-    // the previous step's hash gradients (Adam has read them) and touched marks
-    int st = hashgrid_clear_touched(s, h->list, h->count, (uint32_t)(h->n_hash / HG_F), param_grads, h->bits);
+    // the previous step's hash gradients (Adam has read them): a step touches most entries of the
+    // fine levels, so one whole-array clear writes less than the entries' scattered sectors would
+    const uint64_t entries = h->n_hash / HG_F;
+    int st = cuda_status(cudaMemsetAsync(param_grads, 0, h->n_hash * sizeof(float), s), "hash-grid gradients");
+    if (st == TN_OK) st = cuda_status(cudaMemsetAsync(h->count, 0, sizeof(uint32_t), s), "hash-grid count");
     if (st != TN_OK || n == 0) return st;
     const uint32_t blocks = (n + HG_HEAD_THREADS - 1) / HG_HEAD_THREADS;
     hg_heads_backward_kernel<<<blocks, HG_HEAD_THREADS, 0, s>>>(h->n_features, n, n_dev, stride, h->feat,
@@ -365,8 +468,14 @@ static int hashnet_backward(void* user, tn_stream_t stream, uint32_t n, const ui
     hg_heads_grad_finish_kernel<<<2, 128, 0, s>>>(h->n_features, blocks, h->partials, param_grads + h->n_hash);
     st = check_launch("hash-grid heads gradients");
     if (st != TN_OK) return st;
-    return hashgrid_backward(s, &h->desc, n, n_dev, stride, h->cap, pos, h->dfeat, param_grads, h->bits, h->list,
-                             h->count);
+    st = hashgrid_backward(s, &h->desc, n, n_dev, stride, h->cap, pos, h->dfeat, param_grads, nullptr, nullptr,
+                           nullptr);
+    if (st != TN_OK) return st;
+    // the entries Adam will update: those with a nonzero gradient
+    const uint32_t nz_blocks = (uint32_t)((entries + 8ull * HG_NZ_THREADS - 1) / (8ull * HG_NZ_THREADS));
+    hg_nonzero_kernel<<<nz_blocks, HG_NZ_THREADS, 0, s>>>((uint32_t)entries, reinterpret_cast<const float4*>(param_grads),
+                                                          h->list, h->count);
+    return check_launch("hash-grid nonzero entries");
 }
 
 // A network over the parameters `params` ([hash entries | heads]) for batches of up to `cap`
@@ -392,10 +501,8 @@ int hashnet_create(const tn_hashgrid_desc* desc, const float* params, uint32_t c
     if (st == TN_OK)
         st = cuda_status(cudaMalloc(&h->partials, (size_t)std::max(blocks, 1u) * HG_HEAD_SLOTS * sizeof(float)),
                          "hash-grid partials");
-    if (st == TN_OK) st = cuda_status(cudaMalloc(&h->bits, (size_t)(entries + 31) / 32 * sizeof(uint32_t)), "hash-grid bits");
     if (st == TN_OK) st = cuda_status(cudaMalloc(&h->list, (size_t)entries * sizeof(uint32_t)), "hash-grid list");
     if (st == TN_OK) st = cuda_status(cudaMalloc(&h->count, sizeof(uint32_t)), "hash-grid count");
-    if (st == TN_OK) st = cuda_status(cudaMemset(h->bits, 0, (size_t)(entries + 31) / 32 * sizeof(uint32_t)), "hash-grid bits");
     if (st == TN_OK) st = cuda_status(cudaMemset(h->count, 0, sizeof(uint32_t)), "hash-grid count");
     if (st != TN_OK) {
         delete h;
@@ -412,7 +519,8 @@ int hashnet_create(const tn_hashgrid_desc* desc, const float* params, uint32_t c
 
 void hashnet_destroy(void* handle) { delete static_cast<HashNet*>(handle); }
 
-// Entries touched by the last backward (device count, for inspection and tests).
+// Entries with a nonzero gradient after the last backward (device count, and *list: the
+// entries, in no particular order), for inspection and tests.
 const uint32_t* hashnet_touched(void* handle, const uint32_t** list) {
     auto* h = static_cast<HashNet*>(handle);
     if (list) *list = h->list;
