@@ -224,7 +224,8 @@ def compositor_rooflines(peak, reps=20):
     """Roofline of the compositor's tile kernels (forward, VJP) on the compositor workload at 2^22
     samples (truncated geometric counts, mean 64, at most 1024: 65,571 rays): the L2 (126 MB) is
     flushed before every timed launch (L2Flush, outside the events), each launch timed with
-    CUDA events, the mean kept. Algorithmic bytes: forward 20 B/sample + 32 B/ray, VJP 36 B/sample
+    CUDA events, the median kept (a launch that meets another tenant's work on the shared GPU
+    does not move it). Algorithmic bytes: forward 20 B/sample + 32 B/ray, VJP 36 B/sample
     + 24 B/ray."""
     import torch
     from turbonerf_b200 import hotpath as hp, scenes
@@ -248,7 +249,7 @@ def compositor_rooflines(peak, reps=20):
     for name, (fn, alg) in kernels.items():
         for _ in range(3):
             fn()
-        total = 0.0
+        times = []
         for _ in range(reps):
             flush()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -256,8 +257,8 @@ def compositor_rooflines(peak, reps=20):
             fn()
             e1.record()
             e1.synchronize()
-            total += e0.elapsed_time(e1)
-        ms = total / reps
+            times.append(e0.elapsed_time(e1))
+        ms = float(np.median(times))
         gbs = alg / (ms * 1e-3) / 1e9
         out.append({"kernel": name, "workload": f"compositor, 2^22 samples over {n} rays (mean 64), L2 flushed",
                     "bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 4),

@@ -880,7 +880,7 @@ __device__ __forceinline__ void composite_bwd_group(const Samples& S, uint32_t r
 }
 
 template <int K, bool VEC, int ACT>
-__global__ void __launch_bounds__(LOSS_THREADS)
+__global__ void __launch_bounds__(LOSS_THREADS, 4)
 composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
                            const float* __restrict__ depth, const uint32_t* __restrict__ n_used,
