@@ -912,8 +912,9 @@ def run_losses(args):
 def hashgrid_result(args):
     """The hash-grid encoding of the reference (16 levels of 2 features, 2^19 entries a level,
     resolutions 16..2048 x 16 for the train step's 16-unit box) on 2^18 uniform positions: the
-    encode and the backward (with the touched-entry list) alone, CUDA events over 20 launches after
-    warm-up (the 64 MB table stays in L2 between launches); then the full train step of the
+    encode and the backward (with the touched-entry list, and without it) alone, CUDA events, median
+    of 20 launches after warm-up (the 64 MB table stays in L2 between launches); then the full
+    train step of the
     train-step workload with the hash-grid network (and its linear heads) as the trainer's network
     instead of the synthetic stand-in: real gradients, Adam over the entries they touch, CUDA graph,
     count-ahead schedule."""
@@ -967,6 +968,8 @@ def hashgrid_result(args):
     ms = timed(backward, before=lambda: hp.hashgrid_clear_touched(lst, count, grads, bits))
     out["backward"] = {"ms": round(ms, 4), "samples_per_s": round(n / (ms / 1e3), 1),
                        "touched_entries": int(count.item())}
+    ms = timed(lambda: hp.hashgrid_backward(spec, pos, dfeat, grads, n, n, touched=False))
+    out["backward_without_list"] = {"ms": round(ms, 4), "samples_per_s": round(n / (ms / 1e3), 1)}
     # the train step with the hash-grid network
     scene = _scene(0x7B0)
     tr = _trainer(scene, "fused", replica_seed(0x7B0, 0))
@@ -1427,7 +1430,8 @@ def other_configs(args):
     hg = hashgrid_result(args)
     out["hashgrid_network_step"] = {"samples_per_s": hg["train_step"]["samples_per_s"],
                                     "ms_per_step": hg["train_step"]["ms_per_step"],
-                                    "encode_ms_2e18": hg["encode"]["ms"], "backward_ms_2e18": hg["backward"]["ms"]}
+                                    "encode_ms_2e18": hg["encode"]["ms"], "backward_ms_2e18": hg["backward"]["ms"],
+                                    "backward_without_list_ms_2e18": hg["backward_without_list"]["ms"]}
     torch.cuda.empty_cache()
     bm = backward_memory_result(args)
     out["backward_memory_2e22"] = {v: {"extra_device_bytes": bm[v]["extra_device_bytes"], "ms": bm[v]["ms"]}
