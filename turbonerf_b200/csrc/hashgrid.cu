@@ -303,7 +303,8 @@ hg_heads_backward_kernel(uint32_t nf, uint32_t n, const uint32_t* __restrict__ n
                          const float* __restrict__ feat, const float* __restrict__ head,
                          const float* __restrict__ dL_ddensity, const float* __restrict__ dL_drgb,
                          float* __restrict__ dfeat, float* __restrict__ partials) {
-    __shared__ float red[HG_HEAD_THREADS / WARP][HG_HEAD_SLOTS];
+    __shared__ float rows[HG_HEAD_THREADS * (HG_MAX_FEAT + 1)];
+    __shared__ float runs[HG_HEAD_THREADS];
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const bool live = s < live_count(n, n_dev);
@@ -336,37 +337,57 @@ hg_heads_backward_kernel(uint32_t nf, uint32_t n, const uint32_t* __restrict__ n
             }
         }
     }
+    // the block's sums of dz_o f_j and dz_o, one head at a time: each thread's 33 values to a shared
+    // row; 7 groups of threads sum each column over a run of rows; 33 threads add the runs (the
+    // order is fixed)
+    constexpr int NC = HG_MAX_FEAT + 1;
+    constexpr int NG = HG_HEAD_THREADS / NC, RPG = (HG_HEAD_THREADS + NG - 1) / NG;
 #pragma unroll
     for (int o = 0; o < 4; ++o) {
 #pragma unroll
-        for (int j = 0; j <= HG_MAX_FEAT; ++j) {
-            const float v = warp_sum(j < HG_MAX_FEAT ? dz[o] * f[j] : dz[o]);
-            if (lane == 0) red[wid][o * (HG_MAX_FEAT + 1) + j] = v;
+        for (int j = 0; j < NC; ++j) rows[threadIdx.x * NC + j] = j < HG_MAX_FEAT ? dz[o] * f[j] : dz[o];
+        __syncthreads();
+        if (threadIdx.x < NG * NC) {
+            const int c = threadIdx.x % NC, g = threadIdx.x / NC;
+            float v = 0.0f;
+            for (int t = g * RPG; t < min((g + 1) * RPG, HG_HEAD_THREADS); ++t) v += rows[t * NC + c];
+            runs[g * NC + c] = v;
         }
+        __syncthreads();
+        if (threadIdx.x < NC) {
+            float v = 0.0f;
+            for (int g = 0; g < NG; ++g) v += runs[g * NC + threadIdx.x];
+            partials[(size_t)blockIdx.x * HG_HEAD_SLOTS + o * NC + threadIdx.x] = v;
+        }
+        __syncthreads();
     }
+    (void)lane;
+    (void)wid;
+}
+
+// The heads' gradients (head o, weight j < nf at o (nf + 1) + j, bias at o (nf + 1) + nf): one
+// block a parameter sums the blocks' partials, each thread a strided run of them, then a fixed tree
+// over the threads (deterministic).
+constexpr int HG_FINISH_THREADS = 256;
+__global__ void __launch_bounds__(HG_FINISH_THREADS)
+hg_heads_grad_finish_kernel(uint32_t nf, uint32_t n_blocks, const float* __restrict__ partials,
+                            float* __restrict__ grads) {
+    __shared__ float warp_s[HG_FINISH_THREADS / WARP];
+    const uint32_t k = blockIdx.x;
+    const uint32_t o = k / (nf + 1), j = k % (nf + 1);
+    const uint32_t slot = o * (HG_MAX_FEAT + 1) + (j < nf ? j : (uint32_t)HG_MAX_FEAT);
+    float v = 0.0f;
+    for (uint32_t b = threadIdx.x; b < n_blocks; b += HG_FINISH_THREADS) v += partials[(size_t)b * HG_HEAD_SLOTS + slot];
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) warp_s[threadIdx.x >> 5] = v;
     __syncthreads();
-    for (int k = threadIdx.x; k < HG_HEAD_SLOTS; k += blockDim.x) {
-        float v = 0.0f;
-        for (int w = 0; w < HG_HEAD_THREADS / WARP; ++w) v += red[w][k];
-        partials[(size_t)blockIdx.x * HG_HEAD_SLOTS + k] = v;
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < HG_FINISH_THREADS / WARP; ++w) t += warp_s[w];
+        grads[k] = t;
     }
 }
 
-// The heads' gradients (head o, weight j < nf at o (nf + 1) + j, bias at o (nf + 1) + nf): the sum
-// of the blocks' partials, in block order.
-__global__ void hg_heads_grad_finish_kernel(uint32_t nf, uint32_t n_blocks, const float* __restrict__ partials,
-                                            float* __restrict__ grads) {
-    const uint32_t np = 4 * (nf + 1);
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
-        const uint32_t o = k / (nf + 1), j = k % (nf + 1);
-        const uint32_t slot = o * (HG_MAX_FEAT + 1) + (j < nf ? j : (uint32_t)HG_MAX_FEAT);
-        float v = 0.0f;
-        for (uint32_t b = 0; b < n_blocks; ++b) v += partials[(size_t)b * HG_HEAD_SLOTS + slot];
-        grads[k] = v;
-    }
-}
-
-// positions [3][pstride], features [2L][stride]
 int hashgrid_encode(cudaStream_t stream, const tn_hashgrid_desc* desc, uint32_t n, const uint32_t* n_dev,
                     uint32_t pstride, uint32_t stride, const float* pos, const float* params, float* features) {
     HashLevels H;
@@ -465,7 +486,9 @@ static int hashnet_backward(void* user, tn_stream_t stream, uint32_t n, const ui
                                                                 h->partials);
     st = check_launch("hash-grid heads backward");
     if (st != TN_OK) return st;
-    hg_heads_grad_finish_kernel<<<2, 128, 0, s>>>(h->n_features, blocks, h->partials, param_grads + h->n_hash);
+    hg_heads_grad_finish_kernel<<<4 * (h->n_features + 1), HG_FINISH_THREADS, 0, s>>>(h->n_features, blocks,
+                                                                                      h->partials,
+                                                                                      param_grads + h->n_hash);
     st = check_launch("hash-grid heads gradients");
     if (st != TN_OK) return st;
     st = hashgrid_backward(s, &h->desc, n, n_dev, stride, h->cap, pos, h->dfeat, param_grads, nullptr, nullptr,
