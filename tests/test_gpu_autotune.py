@@ -266,8 +266,8 @@ def test_trainer_autotune_trains_identically():
 
 def test_count_ahead_matches_in_order_steps():
     """The default trainer runs each step's tail (emit, network, losses, Adam, occupancy update)
-    beside the next step's head (its rays and march count, started once the occupancy update has
-    rewritten the grid). Against a trainer that runs every step in order (side_sms = 0): identical
+    beside the next step's head (its rays and march count on the bitfield the tail before it
+    computed ahead of the occupancy update). Against a trainer that runs every step in order (side_sms = 0): identical
     metrics every step and bit-identical rays, counts, parameters, moments, step counters, grid
     densities and bitfield, also after buffer reads between steps (which leave the head computed
     ahead in place), after a grid change (which drops it) and with the launch shapes changed."""
@@ -314,6 +314,37 @@ def test_count_ahead_matches_in_order_steps():
     ma, mb = a.sync_metrics(), b.sync_metrics()
     assert (ma.step, ma.loss) == (mb.step, mb.loss)
     same(a, b, "after asynchronous steps")
+    a.teardown()
+    b.teardown()
+
+
+def test_count_ahead_matches_in_order_steps_across_the_selection_change():
+    """The tail with a next step also computes the bitfield that the next step's occupancy update
+    will write (the decayed grid against the threshold, then the queried cells it raises), so
+    that the head after that step marches without waiting for the update. Selection changes
+    at step 256 from every queried cell to the random rule that reads the bitfield; across it,
+    the count-ahead trainer stays bit-identical to the in-order one (grid densities, bitfield,
+    parameters, march counts) and gives the same metrics every step."""
+    from turbonerf_b200.trainer import SyntheticNeRF, Trainer
+    sc = scenes.march_scene_cascaded(n_rays=8, n_levels=5)
+
+    def make():
+        tr = Trainer(SyntheticNeRF.from_scene(sc), n_rays_per_step=2048, occupancy_cells_per_step=8192,
+                     distortion_lambda=1e-3, occupancy_threshold=0.01, n_grid_params=16 * (1 << 14) * 2,
+                     n_mlp_params=7168, beta2=0.99, seed=0x5E1)
+        tr.setup_data(batch_size=1 << 15)
+        return tr
+
+    a, b = make(), make()
+    assert a.tuning["side_sms"] > 0
+    b.tuning = dict(side_sms=0)
+    for i in range(262):
+        ma, mb = a.train_step(), b.train_step()
+        assert (ma.step, ma.n_rays, ma.n_samples, ma.loss) == (mb.step, mb.n_rays, mb.n_samples, mb.loss), i
+        if i in (254, 255, 256, 257, 261):
+            for k, what in ((0, "weights"), (5, "grid density"), (6, "bitfield"), (11, "n_steps")):
+                dt = np.uint8 if k == 6 else (np.uint32 if k == 11 else np.float32)
+                assert_bitwise(host(a.buffer(k, dt)), host(b.buffer(k, dt)), f"{what} after step {i}")
     a.teardown()
     b.teardown()
 

@@ -126,3 +126,48 @@ def test_trainer_steps_with_the_hashgrid_network_match_oracle():
         assert set(nonzero) <= set(np.nonzero(touched)[0]), f"step {k}: a gradient outside the touched entries"
         assert not g[n_hash + n_head:].any()
     tr.teardown()
+
+
+def test_encode_and_backward_edge_cases():
+    """Zero samples (no launch, outputs untouched); a device live count below n (samples past it
+    untouched, no gradient from them); positions outside [0, 1] (clamped to the edge cells, as the
+    oracle does)."""
+    import torch
+    from turbonerf_b200 import hotpath as hp
+    spec = _spec(log2_t=14)
+    lv = _levels(spec)
+    rng = np.random.default_rng(13)
+    n = 4096
+    pos = rng.uniform(-0.25, 1.25, 3 * n).astype(np.float32)
+    n_hash, _ = spec.n_params()
+    params = rng.uniform(-1.0, 1.0, n_hash).astype(np.float32)
+    sentinel = np.full(spec.n_features * n, 7.0, np.float32)
+    # zero samples
+    out = dev(sentinel.copy())
+    hp.hashgrid_encode(spec, dev(pos), dev(params), 0, n, out=out)
+    assert np.array_equal(host(out), sentinel)
+    # outside [0, 1]: clamped cells, bit for bit with the oracle
+    feat = hp.hashgrid_encode(spec, dev(pos), dev(params), n, n)
+    assert_bitwise(host(feat), oracle.hashgrid_encode(lv, spec.log2_hashmap_size, pos, params, n), "clamped features")
+    # a live count below n
+    live = 1000
+    n_dev = torch.tensor([live], dtype=torch.int32, device="cuda")
+    out = dev(sentinel.copy())
+    hp.hashgrid_encode(spec, dev(pos), dev(params), n, n, n_dev=n_dev, out=out)
+    got = host(out).reshape(spec.n_features, n)
+    ref = oracle.hashgrid_encode(lv, spec.log2_hashmap_size, pos, params, n).reshape(spec.n_features, n)
+    assert_bitwise(got[:, :live].ravel(), ref[:, :live].ravel(), "live features")
+    assert (got[:, live:] == 7.0).all(), "features past the live count were written"
+    dfeat = rng.normal(0.0, 1.0, spec.n_features * n).astype(np.float32)
+    grads = dev(np.zeros(n_hash, np.float32))
+    bits, lst, count = hp.hashgrid_backward(spec, dev(pos), dev(dfeat), grads, n, n, n_dev=n_dev)
+    d_live = dfeat.reshape(spec.n_features, n).copy()
+    d_live[:, live:] = 0.0
+    ref_g, touched = oracle.hashgrid_backward(lv, spec.log2_hashmap_size, pos[:].copy(), d_live.ravel().astype(np.float64),
+                                              n)
+    _, touched_live = oracle.hashgrid_backward(
+        lv, spec.log2_hashmap_size, np.ascontiguousarray(pos.reshape(3, n)[:, :live]).ravel(),
+        np.ascontiguousarray(d_live[:, :live]).ravel().astype(np.float64), live)
+    assert_norm_close(host(grads).astype(np.float64), ref_g, 1e-5, "gradients of the live samples")
+    k = int(host(count)[0])
+    assert np.array_equal(np.sort(host(lst)[:k].view(np.uint32)), np.nonzero(touched_live)[0].astype(np.uint32))

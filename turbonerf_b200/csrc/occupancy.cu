@@ -83,10 +83,11 @@ __device__ __forceinline__ float settle(float v, float decay) { return signbit(v
 
 // Issues every level's 16-byte load of the thread's four cells before using any of them, so
 // each thread keeps n_levels loads in flight. WRITE_DENSITY stores the settled densities;
-// WRITE_BITS rebuilds the bitfield (and counts its set bits). The one-pass update does both; the
-// split update runs a bits-only pass first (what the next march waits for) and the density
-// write-back after it, beside the march.
-template <bool WRITE_DENSITY, bool WRITE_BITS>
+// WRITE_BITS rebuilds the bitfield; COUNT counts the set bits of the settled densities. The
+// one-pass update does all three; the split update runs a bits-only pass first (what the next
+// march waits for) and the density write-back after it, beside the march; an update whose bits
+// were computed ahead (occ_bits_*_kernel) writes the densities and counts.
+template <bool WRITE_DENSITY, bool WRITE_BITS, bool COUNT = WRITE_BITS>
 __global__ void __launch_bounds__(256)
 occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, uint8_t* __restrict__ bits,
                  float decay, float threshold, uint32_t* __restrict__ n_occupied) {
@@ -118,7 +119,7 @@ occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, ui
         if (WRITE_BITS) reinterpret_cast<uint32_t*>(bits)[i] = packed;
         cnt = __popc(packed);
     }
-    if (WRITE_BITS && n_occupied) {
+    if (COUNT && n_occupied) {
         cnt = warp_sum(cnt);
         __shared__ uint32_t ws[8];
         if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = cnt;
@@ -129,6 +130,50 @@ occ_sweep_kernel(uint32_t volume4, int n_levels, float* __restrict__ density, ui
             if (t) atomicAdd(n_occupied, t);
         }
     }
+}
+
+// The bitfield an occupancy update will write, computed before it without changing the
+// densities (which must be settled, as they are between steps): every cell's decayed density
+// against the threshold, then the queried cells the update raises or-ed in. A selected query
+// (k, cell, sigma) leaves max(decay d, sigma, ...) at the cell, above the threshold exactly when
+// one of its max(decay d, sigma) is, so the bits equal the update's bit for bit.
+__global__ void __launch_bounds__(256)
+occ_bits_decayed_kernel(uint32_t volume4, int n_levels, const float* __restrict__ density,
+                        uint8_t* __restrict__ bits, float decay, float threshold) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= volume4) return;
+    const float4* d4 = reinterpret_cast<const float4*>(density);
+    float4 v[MAX_LEVELS];
+#pragma unroll
+    for (int k = 0; k < MAX_LEVELS; ++k)
+        if (k < n_levels) v[k] = d4[(size_t)k * volume4 + i];
+    uint32_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+#pragma unroll
+    for (int k = 0; k < MAX_LEVELS; ++k) {
+        if (k < n_levels) {
+            b0 |= (uint32_t)(v[k].x * decay > threshold) << k;
+            b1 |= (uint32_t)(v[k].y * decay > threshold) << k;
+            b2 |= (uint32_t)(v[k].z * decay > threshold) << k;
+            b3 |= (uint32_t)(v[k].w * decay > threshold) << k;
+        }
+    }
+    reinterpret_cast<uint32_t*>(bits)[i] = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+}
+
+__global__ void occ_bits_raise_kernel(uint32_t n, uint32_t volume, int n_levels, const float* __restrict__ density,
+                                      const uint8_t* __restrict__ sel_bits, uint8_t* __restrict__ bits,
+                                      const int32_t* __restrict__ levels, const uint32_t* __restrict__ cells,
+                                      const float* __restrict__ values, const float* __restrict__ rand_select,
+                                      int act, const uint32_t* __restrict__ sample_all_dev, float decay,
+                                      float threshold) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    const int k = levels[u];
+    const uint32_t idx = cells[u];
+    if (k < 0 || k >= n_levels || idx >= volume) return;
+    if (!selected((int)*sample_all_dev, rand_select, u, sel_bits, idx, k)) return;
+    const float v = fmaxf(density[(size_t)k * volume + idx] * decay, occ_sigma(act, values[u]));
+    if (v > threshold) atomicOr(reinterpret_cast<uint32_t*>(bits) + (idx >> 2), (1u << k) << (8u * (idx & 3u)));
 }
 
 __global__ void popcount_kernel(uint64_t n_words, const uint32_t* __restrict__ words, uint64_t n_tail,
@@ -268,9 +313,11 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
                             uint8_t* bitfield, uint32_t n_updates, const int32_t* levels, const uint32_t* cells,
                             const float* values, const float* rand_select, int activation, int sample_all,
                             const uint32_t* sample_all_dev, const uint32_t* n_dev, float decay, float threshold,
-                            uint32_t* n_occupied_dev, uint8_t* bitfield_out, cudaEvent_t bits_done) {
+                            uint32_t* n_occupied_dev, uint8_t* bitfield_out, cudaEvent_t bits_done,
+                            bool bits_ready) {
     // bits_done: split update; the event is recorded once the bitfield is rebuilt, before the
-    // settled densities are written back
+    // settled densities are written back. bits_ready: bitfield_out already holds the update's
+    // bits (launch_occupancy_bits_ahead); the update writes the densities and counts the bits.
     const bool split = bits_done != nullptr;
     TN_NONNULL(ctx);
     int st = validate_grid(grid);
@@ -298,6 +345,12 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
         if (st != TN_OK) return st;
     }
     const uint32_t v4 = volume / 4;
+    if (bits_ready) {
+        occ_sweep_kernel<true, false, true><<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density,
+                                                                                 bitfield_out, decay, threshold,
+                                                                                 n_occupied_dev);
+        return check_launch("tn_occupancy_update(densities, count)");
+    }
     if (!split) {
         occ_sweep_kernel<true, true><<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out,
                                                                            decay, threshold, n_occupied_dev);
@@ -312,6 +365,29 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
     occ_sweep_kernel<true, false><<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out,
                                                                         decay, threshold, nullptr);
     return check_launch("tn_occupancy_update(densities)");
+}
+
+int launch_occupancy_bits_ahead(cudaStream_t stream, const tn_grid_desc* grid, const float* density,
+                                const uint8_t* bitfield, uint8_t* bitfield_out, uint32_t n_updates,
+                                const int32_t* levels, const uint32_t* cells, const float* values,
+                                const float* rand_select, int activation, const uint32_t* sample_all_dev, float decay,
+                                float threshold) {
+    int st = validate_grid(grid);
+    if (st != TN_OK) return st;
+    TN_NONNULL(density); TN_NONNULL(bitfield); TN_NONNULL(bitfield_out); TN_NONNULL(sample_all_dev);
+    TN_REQUIRE(((uintptr_t)density & 15u) == 0 && ((uintptr_t)bitfield_out & 3u) == 0, TN_E_INVALID,
+               "occupancy bits ahead: density must be 16-byte and bitfield 4-byte aligned");
+    const uint32_t volume = (uint32_t)grid->resolution * grid->resolution * grid->resolution;
+    const uint32_t v4 = volume / 4;
+    occ_bits_decayed_kernel<<<(v4 + 255) / 256, 256, 0, stream>>>(v4, grid->n_levels, density, bitfield_out, decay,
+                                                                   threshold);
+    st = check_launch("occupancy bits ahead (decayed)");
+    if (st != TN_OK || n_updates == 0) return st;
+    occ_bits_raise_kernel<<<(n_updates + 255) / 256, 256, 0, stream>>>(n_updates, volume, grid->n_levels, density,
+                                                                       bitfield, bitfield_out, levels, cells, values,
+                                                                       rand_select, activation, sample_all_dev, decay,
+                                                                       threshold);
+    return check_launch("occupancy bits ahead (raised)");
 }
 
 }  // namespace tn

@@ -122,7 +122,15 @@ int launch_occupancy_update(tn_ctx* ctx, cudaStream_t stream, const tn_grid_desc
                             const float* values, const float* rand_select, int activation, int sample_all,
                             const uint32_t* sample_all_dev, const uint32_t* n_dev, float decay, float threshold,
                             uint32_t* n_occupied_dev, uint8_t* bitfield_out = nullptr,
-                            cudaEvent_t bits_done = nullptr);
+                            cudaEvent_t bits_done = nullptr, bool bits_ready = false);
+// The bitfield launch_occupancy_update will write into bitfield_out, computed before it from
+// settled densities without changing them (the selection rule reads `bitfield`, the policy
+// *sample_all_dev); equal to the update's bits bit for bit.
+int launch_occupancy_bits_ahead(cudaStream_t stream, const tn_grid_desc* grid, const float* density,
+                                const uint8_t* bitfield, uint8_t* bitfield_out, uint32_t n_updates,
+                                const int32_t* levels, const uint32_t* cells, const float* values,
+                                const float* rand_select, int activation, const uint32_t* sample_all_dev, float decay,
+                                float threshold);
 int launch_occupancy_scatter(cudaStream_t stream, const tn_grid_desc* grid, float* density, const uint8_t* bitfield,
                              uint32_t n_updates, const int32_t* levels, const uint32_t* cells, const float* values,
                              const float* rand_select, int activation, int sample_all, float decay);

@@ -10,10 +10,16 @@
 // (emit, network forward, losses, network backward, Adam, and the step's occupancy update).
 // The march count is bound by the latency of its longest ray (a dependent chain of a few
 // hundred steps), not by bandwidth, and fills only part of the GPU; so each step's tail runs
-// beside the next step's head: the next step's rays and count start as soon as this step's
-// occupancy update has rewritten the bitfield (the count must see the updated grid, as in the
-// reference's order), on count_rays_per_block-ray blocks that each hold an SM alone (see
-// exclusive_smem), while Adam runs on the other side_sms SMs. The two steps in flight use two
+// beside the next step's head: the next step's rays and count start at once, on
+// count_rays_per_block-ray blocks that each hold an SM alone (see exclusive_smem), while Adam
+// runs on the other side_sms SMs. The count must see the bitfield of this step's occupancy
+// update, as in the reference's order; the tail before this one computed it already, once the
+// grid had settled and this step's occupancy query was made: the update leaves every cell at
+// max(decay * density, the values of its selected queries), so its bits are the decayed grid
+// against the threshold with the selected queried cells above it or-ed in (exact, as a
+// comparison of the same products). The update itself then only writes the densities back.
+// The first tail of a run (no tail before it) rebuilds the bitfield first and starts the
+// count after it. The two steps in flight use two
 // sets of ray buffers and two march contexts (slots, per-block scan totals, error word). Every
 // step computes what the in-order schedule computes, bit for bit: the head of step N+1 reads
 // only its own rays and the grid after step N's update, and the tail of step N reads only its
@@ -52,7 +58,8 @@ struct StepState {
     uint32_t n_occupied;
     float loss_sums[2];
     uint32_t err;          // error bits of the completed steps not yet read (TN_FLAG_*)
-    uint32_t pad[3];
+    uint32_t next_sample_all;  // the selection policy of the step after the running one
+    uint32_t pad[2];
 };
 
 // End of a step's tail: its batch cut becomes the state's, the totals grow, and the error bits
@@ -71,6 +78,7 @@ __global__ void step_begin_kernel(StepState* s, float base_lr, float lr_decay) {
     s->cur_step = k;
     s->lr = base_lr / (1.0f + lr_decay * (float)k);
     s->sample_all = k < 256u ? 1u : 0u;
+    s->next_sample_all = k + 1u < 256u ? 1u : 0u;
     s->step_count = k + 1u;
 }
 
@@ -180,10 +188,16 @@ struct tn_trainer {
     int32_t ds_w = 0, ds_h = 0;
     float alpha_threshold = 1.0f, alpha_probability = 1.0f;
     cudaEvent_t ev_staged[2] = {nullptr, nullptr};
-    // [kind][ray source: own, caller][ray set of the tail, or of the head for K_H]
-    cudaGraph_t graph[K_KINDS][2][2] = {};
-    cudaGraphExec_t graph_exec[K_KINDS][2][2] = {};
-    bool warm[K_KINDS][2][2] = {};        // ran once eagerly (lazy resources initialised)
+    // [kind][ray source: own, caller][ray set of the tail, or of the head for K_H][bits of the
+    // tail's occupancy update computed ahead]
+    cudaGraph_t graph[K_KINDS][2][2][2] = {};
+    cudaGraphExec_t graph_exec[K_KINDS][2][2][2] = {};
+    bool warm[K_KINDS][2][2][2] = {};     // ran once eagerly (lazy resources initialised)
+    // bits_ahead[s]: the bitfield the occupancy update of the step in set s writes is already in
+    // tail_bits(s), computed by the tail before it (its head then marches without waiting for
+    // the update); set by a tail with a next step, consumed by that step's tail, cleared when a
+    // head computed ahead is dropped
+    bool bits_ahead[2] = {false, false};
     uint32_t graph_kernels[K_KINDS][2] = {};  // kernels captured in one graph of each kind and ray source
     uint32_t graph_nodes[K_KINDS][2] = {};
     uint32_t fused_steps_enqueued = 0;
@@ -264,14 +278,28 @@ static int enqueue_occupancy_query(tn_trainer* tr, cudaStream_t s, const tn_grid
 // rule reads the bitfield the step marched on), bitfield rebuild into the step's output bitfield.
 // With bits_done the rebuild runs first and records the event, and the decayed densities are
 // written back after it (the next step's march waits only for the bits).
+// With bits_ready the step's output bitfield was computed ahead (enqueue_occupancy_bits_ahead)
+// and the update only writes the densities back and counts.
 static int enqueue_occupancy_update(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, int pi,
-                                    cudaEvent_t bits_done = nullptr) {
+                                    cudaEvent_t bits_done = nullptr, bool bits_ready = false) {
     const tn_trainer_desc& d = tr->d;
     RaySet& p = tr->set[pi];
     return launch_occupancy_update(p.ctx, s, &grid, tr->density, tr->head_bits(pi), tr->M, p.occ_levels, p.occ_cells,
                                    p.occ_values, p.occ_rsel, tr->net.activation, 0, &tr->state->sample_all, nullptr,
                                    d.occupancy_decay, d.occupancy_threshold, &tr->state->n_occupied,
-                                   tr->tail_bits(pi), bits_done);
+                                   tr->tail_bits(pi), bits_done, bits_ready);
+}
+
+// The bitfield the occupancy update of the step in set qi will write, from its query (already in
+// set qi) and the settled densities, into the step's output bitfield; the step's selection
+// policy is the state's next_sample_all (the running step's step_begin has run, the step's has
+// not). Nothing changes the densities or the query before that update runs.
+static int enqueue_occupancy_bits_ahead(tn_trainer* tr, cudaStream_t s, const tn_grid_desc& grid, int qi) {
+    const tn_trainer_desc& d = tr->d;
+    RaySet& q = tr->set[qi];
+    return launch_occupancy_bits_ahead(s, &grid, tr->density, tr->head_bits(qi), tr->tail_bits(qi), tr->M,
+                                       q.occ_levels, q.occ_cells, q.occ_values, q.occ_rsel, tr->net.activation,
+                                       &tr->state->next_sample_all, d.occupancy_decay, d.occupancy_threshold);
 }
 
 // Head of a step: its rays (own, or the caller's already in set q, clipped to the box) and the
@@ -299,33 +327,39 @@ static int enqueue_head(tn_trainer* tr, cudaStream_t s, bool external, int qi) {
 
 // Tail of the step whose head is in set pi: step_begin, emit, network forward, the fused losses,
 // network backward and Adam; on the second stream the step's occupancy update (from the query
-// made with its head), which rebuilds the step's output bitfield while the emit pass still reads
-// the one the count used. With next >= 0 the head of the following step (rays from
-// next_external / own rays) runs on the third stream into set next once the occupancy update is
-// done, Adam keeps to side_sms SMs beside it, and the following step's occupancy query runs
-// after Adam (the density network reads the updated parameters). ring >= 0 copies the finished
-// step's state into that pinned slot before the head is joined.
+// made with its head), which writes the step's output bitfield while the emit pass still reads
+// the one the count used (or only the densities, when the bitfield was computed ahead). With
+// next >= 0 the head of the following step (rays from next_external / own rays) runs on the
+// third stream into set next, its count once the output bitfield is there, Adam keeps to
+// side_sms SMs beside it, and the following step's occupancy query runs after Adam (the
+// density network reads the updated parameters), followed by the bitfield its update will
+// write. ring >= 0 copies the finished step's state into that pinned slot before the head is
+// joined.
 static int enqueue_tail(tn_trainer* tr, int pi, int next, bool next_external, int ring) {
     const tn_trainer_desc& d = tr->d;
     cudaStream_t s = tr->stream, so = tr->aux, cs = tr->cstream;
     const tn_grid_desc grid = tr->grid();
     const tn_march_desc march = tr->march();
     const bool occ = tr->M > 0;
+    const bool ahead = occ && tr->bits_ahead[pi];
     RaySet& p = tr->set[pi];
     step_begin_kernel<<<1, 1, 0, s>>>(tr->state, d.learning_rate, d.learning_rate_decay);
     int st = check_launch("step_begin");
     if (st == TN_OK && (occ || next >= 0)) st = cuda_status(cudaEventRecord(tr->ev_fork, s), "fork");
-    // the occupancy update; beside a next head, split: ev_occ once the bitfield is rebuilt
+    // the occupancy update; its bitfield computed ahead by the previous tail, or beside a next
+    // head split: ev_occ once the bitfield is rebuilt
     if (st == TN_OK && occ) {
         st = cuda_status(cudaStreamWaitEvent(so, tr->ev_fork, 0), "fork");
-        if (st == TN_OK) st = enqueue_occupancy_update(tr, so, grid, pi, next >= 0 ? tr->ev_occ : nullptr);
+        if (st == TN_OK)
+            st = enqueue_occupancy_update(tr, so, grid, pi, next >= 0 && !ahead ? tr->ev_occ : nullptr, ahead);
         if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_occ_all, so), "occupancy done");
     }
-    // the next step's head: its rays at once, its march count on the rebuilt grid
+    // the next step's head: its rays at once, its march count on the step's output bitfield
+    // (ready at once when it was computed ahead)
     if (st == TN_OK && next >= 0) {
         st = cuda_status(cudaStreamWaitEvent(cs, tr->ev_fork, 0), "head start");
         if (st == TN_OK) st = enqueue_head_rays(tr, cs, next_external, next);
-        if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(cs, tr->ev_occ, 0), "grid rebuilt");
+        if (st == TN_OK && occ && !ahead) st = cuda_status(cudaStreamWaitEvent(cs, tr->ev_occ, 0), "grid rebuilt");
         if (st == TN_OK) st = enqueue_head_count(tr, cs, next);
         if (st == TN_OK) st = cuda_status(cudaEventRecord(tr->ev_head, cs), "head done");
     }
@@ -360,6 +394,8 @@ static int enqueue_tail(tn_trainer* tr, int pi, int next, bool next_external, in
     if (st == TN_OK && occ) st = cuda_status(cudaStreamWaitEvent(s, tr->ev_occ_all, 0), "occupancy joined");
     // the following step's occupancy query, keyed by its index (step_count after this step_begin)
     if (st == TN_OK && occ && next >= 0) st = enqueue_occupancy_query(tr, s, grid, tr->set[next], &tr->state->step_count);
+    // and the bitfield its occupancy update will write, so that the head after it need not wait
+    if (st == TN_OK && occ && next >= 0) st = enqueue_occupancy_bits_ahead(tr, s, grid, next);
     if (st == TN_OK) {
         step_end_kernel<<<1, 1, 0, s>>>(tr->state, info, p.ctx->flags);
         st = check_launch("step_end");
@@ -440,6 +476,15 @@ static int enqueue_profiled_step(tn_trainer* tr, int pi, cudaEvent_t* ev) {
 // initialises every lazily created resource); later runs replay a graph captured once.
 static int enqueue_kind(tn_trainer* tr, int kind, bool external, int p, int ring) {
     const int src = external ? 1 : 0;
+    // a head run here queries afresh, so only a lone tail (K_TH, K_T) finds its set's bits
+    // computed ahead; a tail consumes them, and a tail with a next step computes the next's
+    if (kind == K_H || kind == K_HT) tr->bits_ahead[p] = false;
+    const int ahead = tr->M > 0 && tr->bits_ahead[p] ? 1 : 0;
+    auto advance = [&](int st) -> int {
+        if (st == TN_OK && kind != K_H) tr->bits_ahead[p] = false;
+        if (st == TN_OK && kind == K_TH && tr->M > 0) tr->bits_ahead[p ^ 1] = true;
+        return st;
+    };
     // a head without a tail before it also makes its step's occupancy query (a tail runs the
     // next step's query after its Adam update); before its step_begin, the step's key is
     // step_count
@@ -461,11 +506,11 @@ static int enqueue_kind(tn_trainer* tr, int kind, bool external, int p, int ring
         }
     };
     // a ring copy is baked into a graph: the pipelined caller-ray steps copy into slot p
-    if (!tr->d.use_cuda_graph || !tr->warm[kind][src][p] || (ring >= 0 && ring != p)) {
-        tr->warm[kind][src][p] = true;
-        return body();
+    if (!tr->d.use_cuda_graph || !tr->warm[kind][src][p][ahead] || (ring >= 0 && ring != p)) {
+        tr->warm[kind][src][p][ahead] = true;
+        return advance(body());
     }
-    cudaGraphExec_t& ex = tr->graph_exec[kind][src][p];
+    cudaGraphExec_t& ex = tr->graph_exec[kind][src][p][ahead];
     if (!ex) {
         int st = cuda_status(cudaStreamBeginCapture(tr->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (st != TN_OK) return st;
@@ -482,7 +527,7 @@ static int enqueue_kind(tn_trainer* tr, int kind, bool external, int p, int ring
             if (g) cudaGraphDestroy(g);
             return st;
         }
-        tr->graph[kind][src][p] = g;
+        tr->graph[kind][src][p][ahead] = g;
         size_t n_nodes = 0;
         cudaGraphGetNodes(g, nullptr, &n_nodes);
         std::vector<cudaGraphNode_t> nodes(n_nodes);
@@ -496,7 +541,7 @@ static int enqueue_kind(tn_trainer* tr, int kind, bool external, int p, int ring
         tr->graph_kernels[kind][src] = kernels;
         tr->graph_nodes[kind][src] = (uint32_t)n_nodes;
     }
-    return cuda_status(cudaGraphLaunch(ex, tr->stream), "graph launch");
+    return advance(cuda_status(cudaGraphLaunch(ex, tr->stream), "graph launch"));
 }
 
 // Drops a head computed ahead from own rays (what it read is about to change, or the next
@@ -505,6 +550,7 @@ static int enqueue_kind(tn_trainer* tr, int kind, bool external, int p, int ring
 static int drop_spec(tn_trainer* tr) {
     if (!tr->spec_own) return TN_OK;
     tr->spec_own = false;
+    tr->bits_ahead[0] = tr->bits_ahead[1] = false;  // the dropped step's update never runs
     int st = cuda_status(cudaStreamSynchronize(tr->stream), "drop head");
     if (st == TN_OK)
         st = cuda_status(cudaMemsetAsync(tr->set[tr->cur ^ 1].ctx->flags, 0, sizeof(uint32_t), tr->stream),
@@ -818,7 +864,8 @@ int tn_trainer_set_synthetic_field(tn_trainer* tr, uint32_t n_blobs, const float
     bool captured = false;
     for (auto& k : tr->graph_exec)
         for (auto& r : k)
-            for (auto& e : r) captured = captured || e != nullptr;
+            for (auto& q : r)
+                for (auto& e : q) captured = captured || e != nullptr;
     TN_REQUIRE(!captured, TN_E_STATE, "the field must be set before the first captured step");
     if (tr->synth.blobs) cudaFree(tr->synth.blobs);
     if (tr->synth.waves) cudaFree(tr->synth.waves);
@@ -1083,13 +1130,14 @@ int tn_trainer_profile_step(tn_trainer* tr, float* stage_ms, uint32_t max_stages
 static void drop_graphs(tn_trainer* tr) {
     for (int k = 0; k < K_KINDS; ++k)
         for (int r = 0; r < 2; ++r)
-            for (int p = 0; p < 2; ++p) {
-                if (tr->graph_exec[k][r][p]) cudaGraphExecDestroy(tr->graph_exec[k][r][p]);
-                if (tr->graph[k][r][p]) cudaGraphDestroy(tr->graph[k][r][p]);
-                tr->graph_exec[k][r][p] = nullptr;
-                tr->graph[k][r][p] = nullptr;
-                tr->warm[k][r][p] = false;
-            }
+            for (int p = 0; p < 2; ++p)
+                for (int a = 0; a < 2; ++a) {
+                    if (tr->graph_exec[k][r][p][a]) cudaGraphExecDestroy(tr->graph_exec[k][r][p][a]);
+                    if (tr->graph[k][r][p][a]) cudaGraphDestroy(tr->graph[k][r][p][a]);
+                    tr->graph_exec[k][r][p][a] = nullptr;
+                    tr->graph[k][r][p][a] = nullptr;
+                    tr->warm[k][r][p][a] = false;
+                }
 }
 
 int tn_trainer_set_dataset(tn_trainer* tr, uint32_t n_images, int32_t width, int32_t height, const tn_camera* cameras,
