@@ -446,17 +446,29 @@ __device__ uint32_t count_ray_loop(const MarchArgs& a, const CountGrid& cg, cons
     const uint32_t res = 1u << cg.res_shift;
     uint32_t n = 0, iters = 0;
     float t = r.t;
+    // Level prediction: the cell lookup and the DDA skip of an iteration run at the level of the
+    // previous iteration (kp), while the iteration's own level is found beside them; when the two
+    // differ (a ray changes level a handful of times) the iteration is discarded without moving
+    // and runs again at the new level. The level choice is then off the chain from t to the next
+    // t, and every iteration that counts used the level the reference's loop uses.
+    int kp;
+    {
+        float x, y, z;
+        ray_point(r, t, x, y, z);
+        const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));
+        kp = count_level<NL>(m, get_dt(t, a.cone, a.dt_min, a.dt_max), cg.half0_bits, cg.cell0_bits, cg.n_levels);
+    }
+    float ils = __fmul_rn(cg.inv_ls0, pow2i(-kp)), kc = __fmul_rn(cg.cell0, pow2i(kp));
     // the iteration guard is part of the loop condition (no branch with a side effect in the
     // body, which stays one straight block); the flag is raised after the loop
     const uint32_t max_iters = a.max_iters;
     while ((t <= t_lim) & (iters < max_iters)) {
-        ++iters;
         float x, y, z;
         ray_point(r, t, x, y, z);
         const float dt = get_dt(t, a.cone, a.dt_min, a.dt_max);
         const float m = fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z)));
         const int k = count_level<NL>(m, dt, cg.half0_bits, cg.cell0_bits, cg.n_levels);
-        const float ils = __fmul_rn(cg.inv_ls0, pow2i(-k));
+        const bool same_level = k == kp;
         const float fx = __fmul_rn(__fadd_rn(__fmul_rn(x, ils), 0.5f), cg.res_f);
         const float fy = __fmul_rn(__fadd_rn(__fmul_rn(y, ils), 0.5f), cg.res_f);
         const float fz = __fmul_rn(__fadd_rn(__fmul_rn(z, ils), 0.5f), cg.res_f);
@@ -465,13 +477,12 @@ __device__ uint32_t count_ray_loop(const MarchArgs& a, const CountGrid& cg, cons
         bool occ;
         if (MIP) {
             const uint32_t coarse = mip[(((((cz >> 2) << cs) | (cy >> 2)) << cs) | (cx >> 2))];
-            const uint32_t word = ((coarse >> k) & 1u) ? __ldg(cg.planes + k * cg.plane_words + (idx >> 5)) : 0u;
+            const uint32_t word = ((coarse >> kp) & 1u) ? __ldg(cg.planes + kp * cg.plane_words + (idx >> 5)) : 0u;
             occ = (word >> (idx & 31u)) & 1u;
         } else {
-            occ = (__ldg(cg.bits + idx) >> k) & 1u;
+            occ = (__ldg(cg.bits + idx) >> kp) & 1u;
         }
         // DDA skip to the next cell boundary: t_target / dt_min rounded up (to a float), times dt_min
-        const float kc = __fmul_rn(cg.cell0, pow2i(k));
         const float tx = axis_dt(fx, hx, r.idx, kc);
         const float ty = axis_dt(fy, hy, r.idy, kc);
         const float tz = axis_dt(fz, hz, r.idz, kc);
@@ -482,8 +493,13 @@ __device__ uint32_t count_ray_loop(const MarchArgs& a, const CountGrid& cg, cons
         // the successor carries no branch
         if (n < slot_cap) slots[n] = t;
         const float t_occ = __fadd_rn(t, dt);
-        t = occ ? t_occ : t_skip;
-        n += occ ? 1u : 0u;
+        const float t_next = occ ? t_occ : t_skip;
+        t = same_level ? t_next : t;
+        n += (same_level & occ) ? 1u : 0u;
+        iters += same_level ? 1u : 0u;
+        kp = k;
+        ils = __fmul_rn(cg.inv_ls0, pow2i(-k));
+        kc = __fmul_rn(cg.cell0, pow2i(k));
         if (LIMIT && n >= max_steps) break;
     }
     if (iters >= max_iters && t <= t_lim && !(LIMIT && n >= max_steps)) raise_flag(flags, ERR_GUARD);
