@@ -520,6 +520,61 @@ __device__ __forceinline__ void load_tile(const Samples& S, uint32_t s0, const b
     }
 }
 
+// One lane's K samples of the five sample arrays as loaded (16-byte groups), held in registers
+// while the tile before them is computed, so that their load latency hides behind that work.
+template <int K>
+struct RawTile {
+    float4 a[K / 4], b[K / 4], r[K / 4], g[K / 4], c[K / 4];
+};
+
+// Loads the 16-byte groups of the lane's K samples from s0 (a multiple of 4) that hold a sample of
+// `im` (bit q: sample s0 + q lies in the warp's range); the other groups read as zero.
+template <int K>
+__device__ __forceinline__ void load_raw(const Samples& S, uint32_t s0, uint32_t im, RawTile<K>& t) {
+#pragma unroll
+    for (int v = 0; v < K / 4; ++v) {
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        t.a[v] = t.b[v] = t.r[v] = t.g[v] = t.c[v] = z;
+        if ((im >> (4 * v)) & 15u) {
+            const uint32_t sv = s0 + 4u * v;
+            t.a[v] = *reinterpret_cast<const float4*>(S.density + sv);
+            t.b[v] = *reinterpret_cast<const float4*>(S.dt + sv);
+            t.r[v] = *reinterpret_cast<const float4*>(S.rgb + sv);
+            t.g[v] = *reinterpret_cast<const float4*>(S.rgb + S.ss + sv);
+            t.c[v] = *reinterpret_cast<const float4*>(S.rgb + 2 * (size_t)S.ss + sv);
+        }
+    }
+}
+
+// load_tile's outputs from a raw tile: samples outside `in` read as zero.
+template <int K, int ACT>
+__device__ __forceinline__ void unpack_tile(const RawTile<K>& t, const bool (&in)[K], float (&sig)[K],
+                                            float (&dtv)[K], float (&cr)[K], float (&cg)[K], float (&cb)[K]) {
+#pragma unroll
+    for (int v = 0; v < K / 4; ++v) {
+        const float av[4] = {t.a[v].x, t.a[v].y, t.a[v].z, t.a[v].w}, bv[4] = {t.b[v].x, t.b[v].y, t.b[v].z, t.b[v].w},
+                    rv[4] = {t.r[v].x, t.r[v].y, t.r[v].z, t.r[v].w}, gv[4] = {t.g[v].x, t.g[v].y, t.g[v].z, t.g[v].w},
+                    cv[4] = {t.c[v].x, t.c[v].y, t.c[v].z, t.c[v].w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int q = 4 * v + k;
+            sig[q] = in[q] ? act_sigma(ACT, av[k]) : 0.0f;
+            dtv[q] = in[q] ? bv[k] : 0.0f;
+            cr[q] = in[q] ? rv[k] : 0.0f;
+            cg[q] = in[q] ? gv[k] : 0.0f;
+            cb[q] = in[q] ? cv[k] : 0.0f;
+        }
+    }
+}
+
+// Bits of the lane's K samples from s0 that lie in [s_begin, s_end).
+template <int K>
+__device__ __forceinline__ uint32_t tile_range_mask(uint32_t s0, uint32_t s_begin, uint32_t s_end) {
+    const uint32_t lo = s_begin > s0 ? min(s_begin - s0, (uint32_t)K) : 0u;
+    const uint32_t hi = s_end > s0 ? min(s_end - s0, (uint32_t)K) : 0u;
+    return ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+}
+
 // L2 prefetch of one tile of samples [s, s + 32 K) of the five sample arrays (density, dt and the
 // three rgb planes), one 128-byte line per lane for the first 5 * 32 K / 32 lanes: the next tile's
 // loads then find their lines in L2 instead of DRAM. Lines past the arrays' end are not touched.
@@ -615,20 +670,38 @@ __device__ __forceinline__ void composite_fwd_group(const Samples& S, uint32_t r
     __syncwarp();
     const uint32_t my_off = lane < nne ? t_off[lane] : 0u;
     float cx = 0.0f, c3[3] = {0.0f, 0.0f, 0.0f};  // depth and colour sums of the ray open at the tile start
-    for (uint32_t base = VEC ? (s_begin & ~3u) : s_begin; base < s_end; base += WARP * K) {
-        if (base + WARP * K < s_end) prefetch_tile<K>(S, base + WARP * K, lane);
+    constexpr uint32_t SPAN = WARP * K;
+    const uint32_t b_first = VEC ? (s_begin & ~3u) : s_begin;
+    // with 16-byte loads the next tile's samples are loaded before this tile is computed (cur, nxt)
+    // and the third tile from here prefetched into L2 (the distance measured best)
+    RawTile<K> cur, nxt;
+    if (VEC) {
+        const uint32_t s0f = b_first + (uint32_t)lane * K;
+        load_raw<K>(S, s0f, tile_range_mask<K>(s0f, s_begin, s_end), cur);
+    }
+    for (uint32_t base = b_first; base < s_end; base += SPAN) {
+        if (VEC) {
+            const uint32_t s0n = base + SPAN + (uint32_t)lane * K;
+            if (base + SPAN < s_end) load_raw<K>(S, s0n, tile_range_mask<K>(s0n, s_begin, s_end), nxt);
+            if (base + 3 * SPAN < s_end) prefetch_tile<K>(S, base + 3 * SPAN, lane);
+        } else if (base + SPAN < s_end) {
+            prefetch_tile<K>(S, base + SPAN, lane);
+        }
         const uint32_t win = tile_head_bits<K>(t_head, base, my_off, nne, s_end, lane);
         constexpr uint32_t LANE_BITS = (1u << K) - 1u;
         const uint32_t hm = win & LANE_BITS, lm = (win >> 1) & LANE_BITS;  // ray starts; ray ends
         const uint32_t s0 = base + (uint32_t)lane * K;
-        const uint32_t lo = s_begin > s0 ? min(s_begin - s0, (uint32_t)K) : 0u;
-        const uint32_t hi = s_end > s0 ? min(s_end - s0, (uint32_t)K) : 0u;
-        const uint32_t im = ((1u << hi) - 1u) & ~((1u << lo) - 1u);  // samples inside [s_begin, s_end)
+        const uint32_t im = tile_range_mask<K>(s0, s_begin, s_end);  // samples inside [s_begin, s_end)
         bool in[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) in[q] = (im >> q) & 1u;
         float x[K], dtv[K], cr[K], cg[K], cb[K];
-        load_tile<K, VEC, ACT>(S, s0, in, x, dtv, cr, cg, cb);
+        if (VEC) {
+            unpack_tile<K, ACT>(cur, in, x, dtv, cr, cg, cb);
+            cur = nxt;
+        } else {
+            load_tile<K, false, ACT>(S, s0, in, x, dtv, cr, cg, cb);
+        }
 #pragma unroll
         for (int q = 0; q < K; ++q) x[q] *= dtv[q];
         // optical depth: the lane's aggregate from its last ray start, one segmented scan
@@ -715,7 +788,7 @@ __device__ __forceinline__ void composite_fwd_group(const Samples& S, uint32_t r
 }
 
 template <int K, bool VEC, int ACT, bool STORE>
-__global__ void __launch_bounds__(LOSS_THREADS, 3)
+__global__ void __launch_bounds__(LOSS_THREADS, 2)
 composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float depth_max,
                            float* __restrict__ rgba, float* __restrict__ depth, uint32_t* __restrict__ n_used,
@@ -773,16 +846,29 @@ __device__ __forceinline__ void composite_bwd_group(const Samples& S, uint32_t r
     const uint32_t span = WARP * K;
     const uint32_t n_tiles = (s_end - b0 + span - 1) / span;
     float cx = 0.0f, cu = 0.0f;  // suffix sums of x and w u of the ray open at the tile end
+    // with 16-byte loads the next tile's samples (the one below) are loaded before this tile is
+    // computed (cur, nxt); an L2 prefetch further ahead measured slower here (its instructions
+    // cost more than it saves)
+    RawTile<K> cur, nxt;
+    if (VEC) {
+        const uint32_t s0l = b0 + (n_tiles - 1) * span + (uint32_t)lane * K;
+        load_raw<K>(S, s0l, tile_range_mask<K>(s0l, s_begin, s_end), cur);
+    }
     for (int t = (int)n_tiles - 1; t >= 0; --t) {
         const uint32_t base = b0 + (uint32_t)t * span;
-        if (t > 0) prefetch_tile<K>(S, base - span, lane);
+        if (VEC) {
+            if (t > 0) {
+                const uint32_t s0n = base - span + (uint32_t)lane * K;
+                load_raw<K>(S, s0n, tile_range_mask<K>(s0n, s_begin, s_end), nxt);
+            }
+        } else if (t > 0) {
+            prefetch_tile<K>(S, base - span, lane);
+        }
         const uint32_t win = tile_head_bits<K>(t_head, base, my_off, nne, s_end, lane);
         constexpr uint32_t LANE_BITS = (1u << K) - 1u;
         const uint32_t hm = win & LANE_BITS, lm = (win >> 1) & LANE_BITS;  // ray starts; ray ends
         const uint32_t s0 = base + (uint32_t)lane * K;
-        const uint32_t lo = s_begin > s0 ? min(s_begin - s0, (uint32_t)K) : 0u;
-        const uint32_t hi = s_end > s0 ? min(s_end - s0, (uint32_t)K) : 0u;
-        const uint32_t im = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+        const uint32_t im = tile_range_mask<K>(s0, s_begin, s_end);
         const int k0 = ray_ordinal(t_off, nne, s0);
         bool in[K], valid[K];
         float4 g[K];
@@ -795,7 +881,12 @@ __device__ __forceinline__ void composite_bwd_group(const Samples& S, uint32_t r
             g[q] = t_g[k];
         }
         float x[K], dtv[K], cr[K], cg[K], cb[K];
-        load_tile<K, VEC, ACT>(S, s0, valid, x, dtv, cr, cg, cb);
+        if (VEC) {
+            unpack_tile<K, ACT>(cur, valid, x, dtv, cr, cg, cb);
+            cur = nxt;
+        } else {
+            load_tile<K, false, ACT>(S, s0, valid, x, dtv, cr, cg, cb);
+        }
         float sig[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) {
@@ -880,7 +971,7 @@ __device__ __forceinline__ void composite_bwd_group(const Samples& S, uint32_t r
 }
 
 template <int K, bool VEC, int ACT>
-__global__ void __launch_bounds__(LOSS_THREADS, 4)
+__global__ void __launch_bounds__(LOSS_THREADS, 3)
 composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
                            const float* __restrict__ depth, const uint32_t* __restrict__ n_used,
