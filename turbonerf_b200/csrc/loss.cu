@@ -633,8 +633,8 @@ __device__ __forceinline__ int ray_ordinal(const uint32_t* off, int nne, uint32_
 // Ray boundaries come from the tile's head bits (one word per 32 samples, built once per tile):
 // a lane tests bits instead of searching the ray table per sample, and one segment plan serves
 // the optical-depth scan and the colour scan. The alpha of a ray is 1 - exp(-d) at its
-// terminating sample (the sum of its weights, without rounding accumulated over the samples),
-// stored with the depth and the sample count there; its colour sums are stored at its last sample
+// terminating sample (the sum of its weights, without rounding accumulated over the samples;
+// `opacity`, a few 1e-7 relative), stored with the depth and the sample count there; its colour sums are stored at its last sample
 // (the ray open at the lane's start, after the colour scan).
 // One group of the forward tiles: rays [r0, r0 + nr) (consecutive samples), walked in tiles of
 // 32 K samples. t_off, t_rid and t_head are the warp's tables.
@@ -722,6 +722,8 @@ __device__ __forceinline__ void composite_fwd_group(const Samples& S, uint32_t r
         float a3[3] = {0.0f, 0.0f, 0.0f};
         float f3[3] = {0.0f, 0.0f, 0.0f};
         bool first_end = false;  // the ray open at the lane's start ends in the lane
+        uint32_t term_bits = 0u;  // the lane's terminating samples
+        float run_q[K];           // the optical depth after each sample
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             const bool h = (hm >> q) & 1u;
@@ -742,26 +744,34 @@ __device__ __forceinline__ void composite_fwd_group(const Samples& S, uint32_t r
             a3[1] = fmaf(w, cg[q], a3[1]);
             a3[2] = fmaf(w, cb[q], a3[2]);
             const bool last = in[q] && ((lm >> q) & 1u);
-            const bool term = comp && (run > depth_max || last);  // the ray's terminating sample
-            if (term || last) {  // in-range samples: at or after the warp's first ray start
-                const int k = k0 + __popc(hm & ((2u << q) - 2u));
-                const uint32_t r = t_rid[k];
-                if (term) {  // depth, samples used, alpha
-                    if (depth) depth[r] = run;
-                    if (n_used) n_used[r] = s0 + q - t_off[k] + 1u;
-                    rgba[r + 3 * (size_t)rs] = -expm1f(-run);
-                }
-                if (last) {
-                    if ((hm & ((2u << q) - 1u)) == 0u) {
-                        first_end = true;  // the ray began in an earlier lane: completed after the colour scan
+            // the ray's terminating sample: its depth, samples used and alpha are stored after the
+            // loop (term_bits, run_q), so that the loop carries no branch for them
+            const bool term = comp && (run > depth_max || last);
+            term_bits |= (uint32_t)term << q;
+            run_q[q] = run;
+            if (last) {  // an in-range sample: at or after the warp's first ray start
+                if ((hm & ((2u << q) - 1u)) == 0u) {
+                    first_end = true;  // the ray began in an earlier lane: completed after the colour scan
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) f3[c] = a3[c];
-                    } else {
-                        rgba[r] = a3[0]; rgba[r + rs] = a3[1]; rgba[r + 2 * (size_t)rs] = a3[2];
-                    }
+                    for (int c = 0; c < 3; ++c) f3[c] = a3[c];
+                } else {
+                    const uint32_t r = t_rid[k0 + __popc(hm & ((2u << q) - 2u))];
+                    rgba[r] = a3[0]; rgba[r + rs] = a3[1]; rgba[r + 2 * (size_t)rs] = a3[2];
                 }
             }
             tb = tn;
+        }
+        while (term_bits) {
+            const int q = __ffs(term_bits) - 1;
+            term_bits &= term_bits - 1u;
+            float d = run_q[0];
+#pragma unroll
+            for (int j = 1; j < K; ++j) d = q == j ? run_q[j] : d;
+            const int k = k0 + __popc(hm & ((2u << q) - 2u));
+            const uint32_t r = t_rid[k];
+            if (depth) depth[r] = d;
+            if (n_used) n_used[r] = s0 + q - t_off[k] + 1u;
+            rgba[r + 3 * (size_t)rs] = opacity(d);
         }
         // colour sums of the ray open at each lane's end, over the lanes
         if (lane == 0 && !cut) {
