@@ -75,6 +75,53 @@ def test_composite_forward_and_vjp(mean, n_samples):
     assert ctx.check() == 0
 
 
+def test_composite_clustered_empty_and_long_rays():
+    """The tile kernels split a batch between warps by samples: a warp takes the rays whose first
+    sample lies in its share, in groups of up to 32. Runs of hundreds of rays without samples (all
+    at one offset, so one warp takes them all, over several groups), runs of one-sample rays,
+    rays of up to 2,000 samples spanning many warps' shares, and empty rays at the batch's end:
+    every ray is composited and differentiated as by the oracle, and empty rays get zeros."""
+    from turbonerf_b200 import hotpath as hp
+    rng = np.random.default_rng(0x7C1)
+    parts = []
+    for i in range(40):
+        parts.append(np.zeros(int(rng.integers(50, 400)), np.uint32))
+        parts.append(rng.integers(1, 3, int(rng.integers(10, 200))).astype(np.uint32))
+        if i % 7 == 0:
+            parts.append(rng.integers(500, 2000, 2).astype(np.uint32))
+    parts.append(np.zeros(300, np.uint32))
+    counts = np.concatenate(parts)
+    n = len(counts)
+    offsets = np.zeros(n, np.uint32)
+    offsets[1:] = np.cumsum(counts[:-1], dtype=np.uint64).astype(np.uint32)
+    ss = int(counts.sum())
+    ss += (-ss) % 4
+    sigma = np.clip(np.exp(rng.normal(0.0, 2.0, ss)), 0.0, 1e4).astype(np.float32)
+    rgb = (1.0 / (1.0 + np.exp(-rng.normal(0.0, 1.0, 3 * ss)))).astype(np.float32)
+    dt = (rng.uniform(0.5, 2.0, ss) * float(scenes.MIN_STEP_SIZE)).astype(np.float32)
+    ctx = hp.Context()
+    rb = hp.ray_batch(i32(counts), i32(offsets), n, n, ss)
+    out = hp.composite_fwd(ctx, rb, dev(sigma), dev(rgb), dev(dt))
+    used = host(out["n_used"]).view(np.uint32)
+    n_alt, alt, over = oracle.cut_branches(counts, offsets, sigma, dt, band=CUT_BAND)
+    assert over == 0
+    assert_legal_cut(used, n_alt, alt)
+    ref_rgba, _ = oracle.composite_fwd(counts, offsets, sigma, rgb, dt, n, ss, fixed_used=used)
+    _rgb_ok(ref_rgba, host(out["rgba"]), n, None)
+    empty = counts == 0
+    for c in range(4):
+        assert np.all(host(out["rgba"])[c * n:(c + 1) * n][empty] == 0.0)
+    g = rng.normal(size=4 * n).astype(np.float32)
+    dd, drgb = hp.composite_bwd(ctx, rb, dev(sigma), dev(rgb), dev(dt), out["depth"], out["n_used"], dev(g))
+    ref_dd, ref_drgb = oracle.composite_vjp(counts, offsets, sigma, rgb, dt, g.astype(np.float64), n, ss,
+                                            fixed_used=used)
+    assert_per_ray_norm_close(host(dd), ref_dd, counts, offsets, RTOL_GRAD, "dL/dsigma")
+    for c in range(3):
+        assert_per_ray_norm_close(host(drgb)[c * ss:(c + 1) * ss], ref_drgb[c * ss:(c + 1) * ss], counts, offsets,
+                                  RTOL_GRAD, f"dL/drgb[{c}]")
+    assert ctx.check() == 0
+
+
 def _recon_reference(sb, dens, act, gpu, grad_scale=1.0):
     """The oracle's reconstruction fwd/bwd at every legitimate set of cuts, assembled ray by
     ray from the branch closest to the GPU's outputs (gpu: dict of host arrays)."""

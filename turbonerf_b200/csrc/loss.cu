@@ -390,6 +390,54 @@ __device__ __forceinline__ uint32_t live_rays(uint32_t n_rays, const uint32_t* n
     return n_dev ? min(*n_dev, n_rays) : n_rays;
 }
 
+// Two lower bounds at once over ascending offsets: the first i < n with off[i] >= va (lanes
+// 0-15) and >= vb (lanes 16-31), n where there is none. Each half probes 16 positions a round and
+// keeps the sub-range where the offsets cross its value; every lane of the warp runs every round.
+__device__ uint2 warp_lower_bounds(const uint32_t* __restrict__ off, uint32_t n, uint32_t va, uint32_t vb, int lane) {
+    const int half = lane >> 4, j = lane & 15;
+    const uint32_t v = half ? vb : va;
+    uint32_t lo = 0, hi = n;  // the answer lies in [lo, hi]; hi == n or off[hi] >= v
+    for (;;) {
+        const bool active = hi - lo > 16u;
+        if (__ballot_sync(FULL_MASK, active) == 0u) break;
+        uint32_t step = 0;
+        bool pred = false;
+        if (active) {
+            step = (hi - lo + 15u) / 16u;
+            pred = off[min(lo + (uint32_t)(j + 1) * step, hi) - 1u] >= v;
+        }
+        const unsigned m = (__ballot_sync(FULL_MASK, pred) >> (16 * half)) & 0xFFFFu;
+        if (active) {
+            if (m == 0u) {
+                lo = hi;
+            } else {
+                const uint32_t js = (uint32_t)(__ffs(m) - 1);
+                const uint32_t nlo = lo + js * step;
+                hi = min(lo + (js + 1u) * step, hi) - 1u;
+                lo = nlo;
+            }
+        }
+    }
+    const bool pred = lo + (uint32_t)j < hi && off[lo + (uint32_t)j] >= v;
+    const unsigned m = (__ballot_sync(FULL_MASK, pred) >> (16 * half)) & 0xFFFFu;
+    const uint32_t ans = m ? lo + (uint32_t)(__ffs(m) - 1) : hi;
+    return make_uint2(__shfl_sync(FULL_MASK, ans, 0), __shfl_sync(FULL_MASK, ans, 16));
+}
+
+// The rays of warp w of W under a sample-balanced split: those whose first sample lies in
+// [w S / W, (w + 1) S / W), S the batch's samples (offsets ascending); the last warp also takes
+// the rays without samples at the end.
+__device__ __forceinline__ uint2 balanced_rays(const uint32_t* __restrict__ counts,
+                                               const uint32_t* __restrict__ offsets, uint32_t n_live, uint32_t w,
+                                               uint32_t W, int lane) {
+    const uint32_t total = offsets[n_live - 1] + counts[n_live - 1];
+    const uint32_t va = (uint32_t)((uint64_t)total * w / W), vb = (uint32_t)((uint64_t)total * (w + 1) / W);
+    uint2 r = warp_lower_bounds(offsets, n_live, va, vb, lane);
+    if (w == 0) r.x = 0;
+    if (w + 1 == W) r.y = n_live;
+    return r;
+}
+
 // ---- kernels ----------------------------------------------------------------------------
 // ---- sample tiles over several rays (the compositor's launch form) -------------------------
 // Each warp owns `rpw` consecutive rays, whose samples are one contiguous range (offsets are the
@@ -797,9 +845,11 @@ __device__ __forceinline__ void composite_fwd_group(const Samples& S, uint32_t r
     }
 }
 
+// The tile kernels launch one wave of resident warps; each warp takes the rays whose first sample
+// lies in its equal share of the batch's samples (balanced_rays), in groups of up to 32 rays.
 template <int K, bool VEC, int ACT, bool STORE>
 __global__ void __launch_bounds__(LOSS_THREADS, 2)
-composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
+composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets, float depth_max,
                            float* __restrict__ rgba, float* __restrict__ depth, uint32_t* __restrict__ n_used,
                            float* __restrict__ t_out, float* __restrict__ w_out) {
@@ -807,10 +857,14 @@ composite_fwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
     __shared__ uint32_t t_off[LOSS_WARPS][WARP], t_rid[LOSS_WARPS][WARP], t_head[LOSS_WARPS][K + 1];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_live = live_rays(n_rays, n_dev);
-    const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
-    if (r0 >= n_live) return;  // whole warps leave together
-    composite_fwd_group<K, VEC, ACT, STORE>(S, r0, (int)min(rpw, n_live - r0), rs, counts, offsets, depth_max, rgba,
-                                            depth, n_used, t_out, w_out, t_off[wid], t_rid[wid], t_head[wid], lane);
+    if (n_live == 0) return;
+    const uint2 rr = balanced_rays(counts, offsets, n_live, blockIdx.x * LOSS_WARPS + wid, gridDim.x * LOSS_WARPS, lane);
+    for (uint32_t r0 = rr.x; r0 < rr.y; r0 += WARP) {
+        composite_fwd_group<K, VEC, ACT, STORE>(S, r0, (int)min((uint32_t)WARP, rr.y - r0), rs, counts, offsets,
+                                                depth_max, rgba, depth, n_used, t_out, w_out, t_off[wid], t_rid[wid],
+                                                t_head[wid], lane);
+        __syncwarp();  // the warp's tables are reused by the next group
+    }
 }
 
 // Compositor VJP over the rays of each warp (semantics of composite_vjp_ray): tiles from the end
@@ -982,7 +1036,7 @@ __device__ __forceinline__ void composite_bwd_group(const Samples& S, uint32_t r
 
 template <int K, bool VEC, int ACT>
 __global__ void __launch_bounds__(LOSS_THREADS, 3)
-composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs, uint32_t rpw,
+composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, uint32_t rs,
                            const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
                            const float* __restrict__ depth, const uint32_t* __restrict__ n_used,
                            const float* __restrict__ grad_rgba, float* __restrict__ dd, float* __restrict__ drgb) {
@@ -992,10 +1046,14 @@ composite_bwd_tiles_kernel(Samples S, uint32_t n_rays, const uint32_t* n_dev, ui
     __shared__ float4 t_g[LOSS_WARPS][WARP];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_live = live_rays(n_rays, n_dev);
-    const uint32_t r0 = (blockIdx.x * LOSS_WARPS + wid) * rpw;
-    if (r0 >= n_live) return;
-    composite_bwd_group<K, VEC, ACT>(S, r0, (int)min(rpw, n_live - r0), rs, counts, offsets, depth, n_used, grad_rgba,
-                                     dd, drgb, t_off[wid], t_lim[wid], t_dep[wid], t_g[wid], t_head[wid], lane);
+    if (n_live == 0) return;
+    const uint2 rr = balanced_rays(counts, offsets, n_live, blockIdx.x * LOSS_WARPS + wid, gridDim.x * LOSS_WARPS, lane);
+    for (uint32_t r0 = rr.x; r0 < rr.y; r0 += WARP) {
+        composite_bwd_group<K, VEC, ACT>(S, r0, (int)min((uint32_t)WARP, rr.y - r0), rs, counts, offsets, depth, n_used,
+                                         grad_rgba, dd, drgb, t_off[wid], t_lim[wid], t_dep[wid], t_g[wid],
+                                         t_head[wid], lane);
+        __syncwarp();
+    }
 }
 
 // ---- distortion loss over sample tiles ------------------------------------------------------
@@ -2409,6 +2467,16 @@ static bool tile_vec(const Samples& S, const void* a, const void* b) {
     return (m & 15u) == 0 && (S.ss & 3u) == 0;
 }
 
+// One wave of resident warps for a sample-balanced launch, at least eight rays a warp on average.
+static int balanced_grid(uint32_t n_rays, const void* kernel) {
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, LOSS_THREADS, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const uint32_t wave = (uint32_t)num_sms() * (uint32_t)per_sm;
+    const uint32_t want = (std::max(1u, n_rays / 8u) + LOSS_WARPS - 1) / LOSS_WARPS;
+    return (int)std::max(1u, std::min(wave, want));
+}
+
 static int tile_grid(uint32_t n_rays, uint32_t rpw) {
     const uint32_t warps = (n_rays + rpw - 1) / rpw;
     return (int)((warps + LOSS_WARPS - 1) / LOSS_WARPS);
@@ -2421,12 +2489,11 @@ static void launch_composite_fwd_tiles(cudaStream_t stream, const tn_ray_batch* 
                                        float* w_out) {
     const float depth_max = min_t > 0.0f ? -logf(min_t) : INFINITY;
     const bool vec = tile_vec(S, t_out, w_out), store = t_out != nullptr;
-    const uint32_t rpw = tile_rays_per_warp(
-        b, vec ? (const void*)composite_fwd_tiles_kernel<CT_K, true, 0, false> : (const void*)composite_fwd_tiles_kernel<CT_K, false, 0, false>, 0, CT_K);
-    const int grid = tile_grid(b->n_rays, rpw);
+    const int grid = balanced_grid(b->n_rays, vec ? (const void*)composite_fwd_tiles_kernel<CT_K, true, 0, false>
+                                                  : (const void*)composite_fwd_tiles_kernel<CT_K, false, 0, false>);
 #define TN_FWD_TILES(V, A, ST)                                                                                  \
     composite_fwd_tiles_kernel<CT_K, V, A, ST><<<grid, LOSS_THREADS, 0, stream>>>(                              \
-        S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth_max, rgba, depth, n_used,  \
+        S, b->n_rays, b->n_rays_dev, b->ray_stride, b->counts, b->offsets, depth_max, rgba, depth, n_used,       \
         t_out, w_out)
     const int key = (vec ? 4 : 0) | (S.act ? 2 : 0) | (store ? 1 : 0);
     switch (key) {
@@ -2446,12 +2513,11 @@ static void launch_composite_bwd_tiles(cudaStream_t stream, const tn_ray_batch* 
                                        const float* depth, const uint32_t* n_used, const float* grad_rgba, float* dd,
                                        float* drgb) {
     const bool vec = tile_vec(S, dd, drgb);
-    const uint32_t rpw = tile_rays_per_warp(
-        b, vec ? (const void*)composite_bwd_tiles_kernel<CV_K, true, 0> : (const void*)composite_bwd_tiles_kernel<CV_K, false, 0>, 0, CV_K);
-    const int grid = tile_grid(b->n_rays, rpw);
+    const int grid = balanced_grid(b->n_rays, vec ? (const void*)composite_bwd_tiles_kernel<CV_K, true, 0>
+                                                  : (const void*)composite_bwd_tiles_kernel<CV_K, false, 0>);
 #define TN_BWD_TILES(V, A)                                                                                      \
     composite_bwd_tiles_kernel<CV_K, V, A><<<grid, LOSS_THREADS, 0, stream>>>(                                  \
-        S, b->n_rays, b->n_rays_dev, b->ray_stride, rpw, b->counts, b->offsets, depth, n_used, grad_rgba, dd,    \
+        S, b->n_rays, b->n_rays_dev, b->ray_stride, b->counts, b->offsets, depth, n_used, grad_rgba, dd,         \
         drgb)
     const int key = (vec ? 2 : 0) | (S.act ? 1 : 0);
     switch (key) {
