@@ -195,11 +195,11 @@ STAGES = ["rays", "march_count", "march_emit", "network_forward", "losses", "net
 
 # DRAM bytes (read + write) of one launch of each stage's main kernel on this workload, measured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass, after the warm-up steps).
-NCU_TRAFFIC = {"march_count": 1_007_616, "march_emit": 1_285_376, "losses": 9_637_888, "adam": 304_766_208,
+NCU_TRAFFIC = {"march_count": 1_138_944, "march_emit": 1_285_376, "losses": 9_637_888, "adam": 304_766_208,
                "occupancy": 50_338_304}
 # The same for the compositor tile kernels on the 2^22-sample batch (the `--workload compositor`
 # capture: DRAM read + write of the first forward and the first VJP launch).
-NCU_TRAFFIC_COMPOSITE = {"composite_fwd_tiles": 87_864_576, "composite_bwd_tiles": 117_784_064}
+NCU_TRAFFIC_COMPOSITE = {"composite_fwd_tiles": 87_796_224, "composite_bwd_tiles": 113_915_904}
 
 
 class L2Flush:
