@@ -440,8 +440,10 @@ __device__ __forceinline__ uint2 balanced_rays(const uint32_t* __restrict__ coun
 
 // ---- kernels ----------------------------------------------------------------------------
 // ---- sample tiles over several rays (the compositor's launch form) -------------------------
-// Each warp owns `rpw` consecutive rays, whose samples are one contiguous range (offsets are the
-// exclusive scan of the counts), and walks that range in tiles of 32 * K samples, lane l owning
+// Each warp owns a run of consecutive rays (`rpw` of them in the distortion tiles; the rays that
+// start in its share of the samples in the compositor tiles, balanced_rays), whose samples are one
+// contiguous range (offsets are the exclusive scan of the counts), and walks that range in tiles
+// of 32 * K samples, lane l owning
 // the K consecutive samples [base + K l, base + K l + K). Short rays share a tile and long rays
 // span several; every running sum along a ray is a segmented sum: inside a lane, then one
 // segmented warp scan of the lane aggregates, then a carry into the next tile. The loads of a
