@@ -278,7 +278,7 @@ int tn_compact_nonzero(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32
 int tn_autotune_compact(tn_ctx* ctx, tn_stream_t stream, uint32_t n, const uint32_t* values, int32_t* out,
                         uint32_t* count_dev, tn_tune_report* report);
 
-/* ---- compositor (a warp per ray, warp-shuffle scans) ----------------------------- */
+/* ---- compositor (sample tiles over runs of rays, segmented warp scans) ------------ */
 /* Forward (reference density_to_ray_rgba_forward, training-kernels-fused.cuh:227-264):
  * rgba[4][ray_stride]; optional per-ray saved state for the backward: depth[ray]
  * (optical depth up to the transmittance cut) and n_used[ray] (samples composited). */
